@@ -1,0 +1,365 @@
+"""Benchmark of the per-Newton-iteration IPC contact pipeline on B200.
+
+One step = one Newton iteration's contact block through the public API
+(ipc_warp_b200.pipeline.ContactPipeline.iteration): BVH refit, EE + PT
+candidate detection, narrow phase (force + 16 Hessian triplets per record),
+BSR assembly, barrier energy and the CCD step bound, on the rod-bundle scene
+of the rod-twist configuration (16 rods of 4x4x256 hex cells, 5 tets/cell,
+102,800 vertices) in its wound contact state: facing rod sides 0.5 dhat apart
+(dhat = 1e-3 rod width).  Synthetic, seeded inputs.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+The reference arm times the CPU oracle's restatement of the same pipeline
+(the reference itself is Warp + an empty ipctkwp submodule and cannot run).
+For N > 1 every rank runs an independent replica (the reference path is a
+single-GPU simulator); value = pairs processed by all ranks / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Newton step ms, learned-PCG vs cuDSS at rel res 1e-6; contact pairs/s, %HBM"
+WORKLOAD = "rod_twist_16rods_4x4x256_wound_contact_state"
+
+
+def scene():
+    from ipc_warp_b200 import scenes
+
+    return scenes.rod_bundle(n_rods_side=4, cells=(4, 4, 256), width=0.1, gap_over_dhat=0.5,
+                             jitter_over_dhat=0.05, seed=1, kappa=1e4)
+
+
+def newton_direction(sc, seed=2):
+    """Seeded stand-in for a Newton step: neighbours approach by ~dhat."""
+    rng = np.random.default_rng(seed)
+    dx = rng.normal(scale=0.3 * sc.dhat, size=sc.x.shape)
+    width = sc.meta["width"]
+    centre = sc.x.reshape(-1, 3).mean(0)
+    # squeeze the bundle toward its axis (x -= dx)
+    dx[:, :2] += 0.02 * (sc.x[:, :2] - centre[:2]) / width * sc.dhat
+    return dx
+
+
+# ------------------------------------------------------------------ timing
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [c.strip() for c in line.split(",")]
+            if len(f) >= 9 and f[1].replace(".", "").isdigit():
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit()),
+                "reasons": reasons}
+
+
+def flush_l2(buf):
+    buf.add_(1.0)  # 256 MiB write > 126 MB L2
+
+
+def count_kernels(fn):
+    """Number of this library's kernels one call of fn launches."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        fn()
+        torch.cuda.synchronize()
+    names = [e.name for e in prof.events() if e.device_type.name == "CUDA"]
+    ours = [n for n in names if "ipcb" in n]
+    return len(ours), sorted(set(ours))
+
+
+# ---------------------------------------------------------------- roofline
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# algorithmic bytes per pair of the narrow-phase kernel (float32 records):
+# record 24 + positions 48 + 16 triplets (4+4+36) 704 + force 48; EE adds rest positions 48
+NARROW_BYTES = {"pt": 824, "ee": 872}
+
+
+def stage_times(pipe, dx, reps, torch):
+    """Per-stage device times (ms, mean over reps) on the launching stream."""
+    from ipc_warp_b200.dynamic_contacts import contact_hessian_ee, contact_hessian_pt
+
+    st = torch.cuda.current_stream()
+    acc = {}
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(st)
+        return e
+
+    n_ee, n_pt = pipe.n_contacts, pipe.n_contacts_pt
+    t = pipe.collision_triplets
+    for _ in range(reps):
+        marks = [("start", ev())]
+        pipe.update_bvh()
+        marks.append(("refit", ev()))
+        pipe._launch_dcd("ee")
+        marks.append(("dcd_ee", ev()))
+        pipe._launch_dcd("pt")
+        marks.append(("dcd_pt", ev()))
+        pipe.b.zero_()
+        contact_hessian_ee(None, pipe.soup, pipe.contacts_new, t, pipe.b, pipe.contact_stiffness, n=n_ee)
+        marks.append(("narrow_ee", ev()))
+        contact_hessian_pt(None, pipe.soup, pipe.contacts_pt, t, pipe.b, n_ee, pipe.contact_stiffness, n=n_pt)
+        marks.append(("narrow_pt", ev()))
+        from ipc_warp_b200.bsr import bsr_from_triplets
+
+        bsr_from_triplets(pipe.soup.n_verts, pipe.soup.n_verts, t.rows, t.cols, t.vals, count=(n_ee + n_pt) * 16,
+                          out=pipe.collision_hessian)
+        marks.append(("bsr", ev()))
+        pipe.compute_collision_energy(detect=False)
+        marks.append(("energy", ev()))
+        pipe.collision_free_step(dx)
+        marks.append(("ccd", ev()))
+        torch.cuda.synchronize()
+        for (a, ea), (b, eb) in zip(marks[:-1], marks[1:]):
+            acc[b] = acc.get(b, 0.0) + ea.elapsed_time(eb) / reps
+    return acc
+
+
+# ------------------------------------------------------------- CPU oracle
+def cpu_pipeline(sc, dx, reps):
+    """One pass of the oracle's restatement: DCD EE + PT, narrow phase
+    (analytic subspace route), energy, scene TOI.  Returns (pairs, seconds/pass)."""
+    from oracle import pyoracle as po
+
+    x32 = sc.x.astype(np.float32)
+    x1 = x32 - dx.astype(np.float32)
+    th = np.float32(sc.thickness)
+    times = []
+    pairs = 0
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        ee = po.dcd_ee(x32, sc.edges, sc.body, th, cap=1 << 21)
+        pt = po.dcd_pt(x32, sc.triangles, sc.body, th, cap=1 << 21)
+        l0e = np.full(len(ee), th * np.float32(2), np.float32)
+        l0p = np.full(len(pt), th * np.float32(2), np.float32)
+        po.narrow("ee", ee[:, :4], l0e, x32, sc.xcs.astype(np.float32), sc.kappa, mode=1)
+        po.narrow("pt", pt[:, :4], l0p, x32, None, sc.kappa, mode=1)
+        po.scene_toi(x32, x1, sc.edges, sc.triangles, sc.body)
+        times.append(time.perf_counter() - t0)
+        pairs = len(ee) + len(pt)
+    return pairs, statistics.mean(times)
+
+
+def run_reference(args):
+    """CPU arm: the oracle pipeline on all host threads, K timed passes."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sc = scene()
+    dx = newton_direction(sc)
+    cores = os.cpu_count()
+    cpu_pipeline(sc, dx, max(args.warmup, 1))
+    pairs, sec = cpu_pipeline(sc, dx, args.steps)
+    value = pairs / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "verts": sc.n_verts, "edges": sc.n_edges, "tris": sc.n_tris,
+                   "dhat": sc.dhat, "pairs": pairs, "threads": cores},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": "port",
+                         "sample": "full workload, one DCD+narrow+energy+CCD pass per step (C++ oracle, OpenMP)"},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    from ipc_warp_b200.pipeline import ContactPipeline
+
+    sc = scene()
+    dx_np = newton_direction(sc)
+    pipe = ContactPipeline.from_scene(sc, dtype=torch.float32, device=dev)
+    dx = torch.tensor(dx_np, dtype=torch.float32, device=dev)
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def step():
+        return pipe.iteration(dx)
+
+    for _ in range(max(args.warmup, 3)):
+        r = step()
+    torch.cuda.synchronize()
+    pairs = r.n_ee + r.n_pt
+
+    # ---- device-resident timing: K steps, L2 flushed between steps
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    evs = []
+    for _ in range(args.steps):
+        flush_l2(flush)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        step()
+        e.record()
+        evs.append((s, e))
+    barrier()
+    clocks = sampler.stop()
+    total_ms = sum(s.elapsed_time(e) for s, e in evs)
+
+    # ---- end to end: pinned host inputs copied in, results read back
+    xh = torch.tensor(sc.x, dtype=torch.float32).pin_memory()
+    dxh = dx.cpu().pin_memory()
+    bh = torch.empty_like(pipe.b, device="cpu").pin_memory()
+    dx_dev = torch.empty_like(dx)
+    e2e_ev = []
+    barrier()
+    for _ in range(args.steps):
+        flush_l2(flush)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        pipe.soup.x_transformed.copy_(xh, non_blocking=True)
+        dx_dev.copy_(dxh, non_blocking=True)
+        pipe.iteration(dx_dev)
+        bh.copy_(pipe.b, non_blocking=True)
+        e.record()
+        e2e_ev.append((s, e))
+    barrier()
+    e2e_ms = sum(s.elapsed_time(e) for s, e in e2e_ev)
+    h2d = xh.numel() * 4 + dxh.numel() * 4
+    d2h = bh.numel() * 4 + 8 + 4 + 8  # force, energy, toi, counts
+
+    if world > 1:
+        t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_ms = float(t[0]), float(t[1])
+
+    # ---- roofline of the dominant kernel and kernel count (rank 0, untimed)
+    out = None
+    if rank == 0:
+        st = stage_times(pipe, dx, 5, torch)
+        n_launch, names = count_kernels(step)
+        peak, peak_kind = peaks()
+        n_ee, n_pt = pipe.n_contacts, pipe.n_contacts_pt
+        narrow_ms = st["narrow_ee"] + st["narrow_pt"]
+        algo = n_ee * NARROW_BYTES["ee"] + n_pt * NARROW_BYTES["pt"]
+        achieved = algo / (narrow_ms * 1e-3) / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "narrow_traffic.json")
+        if os.path.exists(tp):
+            traffic = json.load(open(tp)).get("bytes_per_launch")
+        cpu_pairs, cpu_sec = cpu_pipeline(sc, dx_np, 3)
+        ms = total_ms / args.steps
+        out = {
+            "metric": METRIC,
+            "value": world * pairs * args.steps / (total_ms * 1e-3),
+            "unit": "pairs/s",
+            "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "verts": sc.n_verts, "edges": sc.n_edges, "tris": sc.n_tris,
+                       "dhat": sc.dhat, "n_ee": n_ee, "n_pt": n_pt, "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"replicas x{world}",
+                       "stage_ms": {k: round(v, 4) for k, v in st.items()}},
+            "roofline": {"kernel": "k_contact_hessian (EE + PT)", "bound": "hbm", "achieved": achieved,
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic,
+                         "algorithmic_bytes": algo},
+            "cpu_baseline": {"value": cpu_pairs / cpu_sec, "unit": "pairs/s", "cores": os.cpu_count(),
+                             "kind": "port",
+                             "sample": "full workload, 3 passes of the C++ oracle pipeline (DCD+narrow+energy+CCD)"},
+            "e2e": {"value": world * pairs * args.steps / (e2e_ms * 1e-3), "unit": "pairs/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": n_launch * args.steps,
+            "kernels": names,
+            "clocks": clocks,
+        }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,174 @@
+/* ipc_warp_b200 C ABI: the per-Newton-iteration IPC contact pipeline on one
+ * B200 (sm_100a).
+ *
+ * Conventions
+ *  - Every pointer is a device pointer unless stated otherwise; structs
+ *    (ipcb_soup, ipcb_lbvh, ipcb_contacts) are passed by host pointer.
+ *  - Positions are AoS scalar[3*V] like the reference's wp.array(dtype=vec3);
+ *    `fp64` selects double (the reference's USE_FLOAT32=False build) or float.
+ *  - Functions enqueue work on `stream` (a cudaStream_t) and never
+ *    synchronize.  They return IPCB_OK or an IPCB_E* code for bad arguments or
+ *    a failed launch.  Device-side conditions are reported through device
+ *    words the caller reads: contact counts above capacity (overflow: grow
+ *    the list and relaunch, as contact.py:523-537,698-723 does) and status
+ *    words for bounded loops that ran out (IPCB_STATUS_*).
+ *  - Scratch memory is caller-provided: query the size with the *_workspace
+ *    function, pass a device block of at least that many bytes.
+ */
+#ifndef IPCB_H
+#define IPCB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* ipcb_stream; /* cudaStream_t */
+
+enum {
+  IPCB_OK = 0,
+  IPCB_E_ARG = 1,    /* invalid argument (null pointer, negative size, small workspace) */
+  IPCB_E_CUDA = 2,   /* a launch or runtime call failed */
+};
+
+/* status-word bits written by device code (OR-ed) */
+enum {
+  IPCB_STATUS_STACK = 1,    /* BVH traversal stack full: result incomplete */
+  IPCB_STATUS_ROOT_ITERS = 2 /* cubic root refinement hit its iteration bound */
+};
+
+/* Geometry: the reference Soup (fem/geometry.py:165-171) plus positions. */
+typedef struct {
+  int n_verts, n_edges, n_tris;
+  int fp64;              /* scalar type of x / xcs: 0 float, 1 double */
+  const void* x;         /* scalar[3*n_verts]   soup.x_transformed  */
+  const void* xcs;       /* scalar[3*n_verts]   soup.xcs (rest)     */
+  const int* edges;      /* int32[2*n_edges]    soup.edges          */
+  const int* triangles;  /* int32[3*n_tris]     soup.triangles      */
+  const int* body;       /* int32[n_verts]      soup.body           */
+} ipcb_soup;
+
+/* Contact list: the reference Contacts/XConstraint (contact.py:61-80) as
+ * columns.  Record k: a1a2b1b2[4k..4k+3], e0e1[2k..2k+1], l0[k], alpha[k],
+ * lam[k] (scalar = float or double as the soup).  *cnt counts every accepted
+ * pair, also those beyond capacity. */
+typedef struct {
+  int* a1a2b1b2;  /* int32[4*capacity], 16-byte aligned */
+  int* e0e1;      /* int32[2*capacity] */
+  void* l0;       /* scalar[capacity] */
+  void* alpha;    /* scalar[capacity] */
+  void* lam;      /* scalar[capacity] */
+  int* cnt;       /* int32[1] */
+  int capacity;
+} ipcb_contacts;
+
+/* Linear BVH over n boxes.  Memory is one caller block carved by
+ * ipcb_lbvh_bind.  nodes: 4 float4 per internal node: (L.lo, Lcode),
+ * (L.hi, -), (R.lo, Rcode), (R.hi, -); code >= 0 internal node, < 0 leaf
+ * ~primitive. */
+typedef struct {
+  int n;          /* leaves currently built */
+  int capacity;   /* leaves the memory was bound for */
+  void* nodes;    /* float4[4*max(capacity-1,1)] */
+  int* parent;    /* int32[2*capacity]: internal j at j, leaf slot k at capacity+k; (parent<<1)|side */
+  int* sorted;    /* int32[capacity]: primitive of each leaf slot (Morton order) */
+  unsigned* keys; /* uint32[capacity]: sorted Morton codes */
+  unsigned* flags;/* uint32[capacity]: refit arrival counters (zero between calls) */
+} ipcb_lbvh;
+
+int ipcb_version(void);
+const char* ipcb_last_error(void);
+
+/* ---- device radix sort (also used inside build and BSR assembly) ---- */
+size_t ipcb_sort_workspace_u32(int n);
+size_t ipcb_sort_workspace_u64(int n);
+/* Stable sort by the low end_bit bits of keys, values permuted alongside. */
+int ipcb_sort_pairs_u32(unsigned* keys, int* vals, int n, int end_bit, void* ws, size_t ws_bytes, ipcb_stream s);
+int ipcb_sort_pairs_u64(unsigned long long* keys, int* vals, int n, int end_bit, void* ws, size_t ws_bytes,
+                        ipcb_stream s);
+
+/* ---- LBVH (replaces wp.Bvh / wp.Mesh build and .refit(): contact.py:464-483, 672-677) ---- */
+size_t ipcb_lbvh_bytes(int capacity);
+int ipcb_lbvh_bind(ipcb_lbvh* bvh, void* mem, int capacity);
+size_t ipcb_lbvh_build_workspace(int n);
+/* 30-bit Morton codes of box centres, radix sort, Karras hierarchy in one
+ * kernel, then a bottom-up refit.  lower/upper: float[3n]. */
+int ipcb_lbvh_build(ipcb_lbvh* bvh, const float* lower, const float* upper, int n, void* ws, size_t ws_bytes,
+                    ipcb_stream s);
+/* Recompute node boxes for new leaf boxes, same topology (atomic bottom-up). */
+int ipcb_lbvh_refit(const ipcb_lbvh* bvh, const float* lower, const float* upper, ipcb_stream s);
+
+/* ---- boxes (contact.py:30-52, ccd/ccd.py:166-210) ---- */
+/* x4 = float4(x) (the reference's float32 mesh copy, contact.py:44-47, as 16-byte records) */
+int ipcb_pack_positions(const ipcb_soup* soup, float* x4, ipcb_stream s);
+/* edge AABBs of x4 padded by pad (edge_aabb, contact.py:30-37) */
+int ipcb_edge_aabbs(const ipcb_soup* soup, const float* x4, float pad, float* lower, float* upper, ipcb_stream s);
+/* triangle AABBs of x4 padded by pad (wp.Mesh bounds, contact.py:479,677) */
+int ipcb_triangle_aabbs(const ipcb_soup* soup, const float* x4, float pad, float* lower, float* upper,
+                        ipcb_stream s);
+/* x1 = x - dx in the soup scalar (_add_dx, contact.py:49-52) */
+int ipcb_add_dx(const ipcb_soup* soup, const void* dx, void* x1, ipcb_stream s);
+/* swept boxes of (x, x1) padded, rounded outward to float (ccd.py:166-210) */
+int ipcb_swept_edge_aabbs(const ipcb_soup* soup, const void* x1, double pad, float* lower, float* upper,
+                          ipcb_stream s);
+int ipcb_swept_triangle_aabbs(const ipcb_soup* soup, const void* x1, double pad, float* lower, float* upper,
+                              ipcb_stream s);
+
+/* ---- DCD broad phase (contact.py:199-228 edge_edge_collision, 304-336 point_triangle_collision) ----
+ * Appends every pair with float32 closest distance < 2*thickness that passes
+ * the reference filters.  The caller zeroes out->cnt first.  query_pad is the
+ * query-box inflation (the reference uses thickness+buffer for EE against
+ * boxes already inflated by the same, 2*(thickness+buffer) for PT against
+ * tight triangle boxes); any pad >= the reference's keeps the candidate set. */
+int ipcb_dcd_ee(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* edge_bvh, float thickness, float query_pad,
+                int exclude_same_body, ipcb_contacts* out, int* status, ipcb_stream s);
+/* query_order: optional int32[n_verts] vertex visiting order (NULL = 0..V-1) */
+int ipcb_dcd_pt(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* tri_bvh, float thickness, float query_pad,
+                int exclude_same_body, const int* query_order, ipcb_contacts* out, int* status, ipcb_stream s);
+
+/* ---- narrow phase (dynamic_contacts.py:152-246 contact_hessian_ee/pt, 375-398 energy) ----
+ * kind 0 = EE list, 1 = PT list.  n >= 0: number of records; n < 0: read
+ * min(*list->cnt, capacity) on the device (graph-capturable).
+ * Writes 16 triplets per record at (offset + k)*16 + ii*4 + jj: rows/cols
+ * int32, vals scalar[9] row-major; inactive records (dist >= l0) get zero
+ * blocks at (0,0).  b (scalar[3V]) accumulates the force -dE/dx. */
+int ipcb_contact_hessian(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, int offset, double kappa,
+                         int* rows, int* cols, void* vals, void* b, ipcb_stream s);
+/* energy (double) += sum of the barrier energy of the list */
+int ipcb_contact_energy(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, double kappa,
+                        double* energy, ipcb_stream s);
+
+/* ---- CCD (ccd/ccd.py:360-427 point_triangle_toi / edge_edge_toi) ----
+ * Cubic coplanarity TOI in double for every candidate whose swept boxes
+ * overlap; toi (scalar[1], caller sets 1) gets the minimum root < 1,
+ * rounded toward zero when stored as float. */
+int ipcb_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* swept_edge_bvh, const float* lower,
+                       const float* upper, int exclude_same_body, void* toi, int* status, ipcb_stream s);
+int ipcb_point_triangle_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* swept_tri_bvh, double pad,
+                            int exclude_same_body, void* toi, int* status, ipcb_stream s);
+/* per-pair collision time of n explicit pairs (kind 0 EE, 1 PT); p_t0/p_t1:
+ * double[n*12] (4 points each) -> t double[n] (ee/pt_collision_time, ccd.py:304-357) */
+int ipcb_collision_time(int kind, int n, const double* p_t0, const double* p_t1, double* t, int* status,
+                        ipcb_stream s);
+/* cubic_roots (cubic_roots.py:96-193) of n cubics coef double[4n] on [x0,x1] */
+int ipcb_cubic_roots(int n, const double* coef, double x0, double x1, double* roots, int* n_roots, int* status,
+                     ipcb_stream s);
+
+/* ---- BSR assembly (warp.sparse.bsr_from_triplets, dynamic_contacts.py:290-297) ----
+ * Canonical 3x3-block CSR from triplets: sort by (row, col), sum duplicates,
+ * drop triplets whose 9 values are all zero.  offsets int32[nrow+1],
+ * columns int32[>= n_trip], values scalar[9*n_trip]; *nnz gets the block count. */
+size_t ipcb_bsr_workspace(int n_trip, int nrow, int ncol);
+int ipcb_bsr_from_triplets(int nrow, int ncol, int n_trip, const int* rows, const int* cols, const void* vals,
+                           int fp64, int* offsets, int* columns, void* values, int* nnz, void* ws, size_t ws_bytes,
+                           ipcb_stream s);
+/* y = alpha*A*x + beta*y for a 3x3 BSR (bsr_mv) */
+int ipcb_bsr_mv(int nrow, const int* offsets, const int* columns, const void* values, int fp64, const void* x,
+                void* y, double alpha, double beta, ipcb_stream s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IPCB_H */

@@ -1,0 +1,115 @@
+"""ctypes binding of libipcb200.so (include/ipcb.h).
+
+The library is required: there is no CPU fallback.  Importing this module
+loads it; any call that launches work needs a CUDA device and raises if the
+library is missing or a call reports an error.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libipcb200.so")
+
+c_int, c_float, c_double, c_size_t, c_void_p = ctypes.c_int, ctypes.c_float, ctypes.c_double, ctypes.c_size_t, ctypes.c_void_p
+P = c_void_p
+
+
+class Soup(ctypes.Structure):
+    _fields_ = [("n_verts", c_int), ("n_edges", c_int), ("n_tris", c_int), ("fp64", c_int),
+                ("x", P), ("xcs", P), ("edges", P), ("triangles", P), ("body", P)]
+
+
+class Contacts(ctypes.Structure):
+    _fields_ = [("a1a2b1b2", P), ("e0e1", P), ("l0", P), ("alpha", P), ("lam", P), ("cnt", P),
+                ("capacity", c_int)]
+
+
+class Lbvh(ctypes.Structure):
+    _fields_ = [("n", c_int), ("capacity", c_int), ("nodes", P), ("parent", P), ("sorted", P), ("keys", P),
+                ("flags", P)]
+
+
+SP, CP, BP = ctypes.POINTER(Soup), ctypes.POINTER(Contacts), ctypes.POINTER(Lbvh)
+
+# name -> (restype, argtypes); every symbol here is declared in include/ipcb.h
+SIGNATURES = {
+    "ipcb_version": (c_int, []),
+    "ipcb_last_error": (ctypes.c_char_p, []),
+    "ipcb_sort_workspace_u32": (c_size_t, [c_int]),
+    "ipcb_sort_workspace_u64": (c_size_t, [c_int]),
+    "ipcb_sort_pairs_u32": (c_int, [P, P, c_int, c_int, P, c_size_t, P]),
+    "ipcb_sort_pairs_u64": (c_int, [P, P, c_int, c_int, P, c_size_t, P]),
+    "ipcb_lbvh_bytes": (c_size_t, [c_int]),
+    "ipcb_lbvh_bind": (c_int, [BP, P, c_int]),
+    "ipcb_lbvh_build_workspace": (c_size_t, [c_int]),
+    "ipcb_lbvh_build": (c_int, [BP, P, P, c_int, P, c_size_t, P]),
+    "ipcb_lbvh_refit": (c_int, [BP, P, P, P]),
+    "ipcb_pack_positions": (c_int, [SP, P, P]),
+    "ipcb_edge_aabbs": (c_int, [SP, P, c_float, P, P, P]),
+    "ipcb_triangle_aabbs": (c_int, [SP, P, c_float, P, P, P]),
+    "ipcb_add_dx": (c_int, [SP, P, P, P]),
+    "ipcb_swept_edge_aabbs": (c_int, [SP, P, c_double, P, P, P]),
+    "ipcb_swept_triangle_aabbs": (c_int, [SP, P, c_double, P, P, P]),
+    "ipcb_dcd_ee": (c_int, [SP, P, BP, c_float, c_float, c_int, CP, P, P]),
+    "ipcb_dcd_pt": (c_int, [SP, P, BP, c_float, c_float, c_int, P, CP, P, P]),
+    "ipcb_contact_hessian": (c_int, [c_int, SP, CP, c_int, c_int, c_double, P, P, P, P, P]),
+    "ipcb_contact_energy": (c_int, [c_int, SP, CP, c_int, c_double, P, P]),
+    "ipcb_edge_edge_toi": (c_int, [SP, P, BP, P, P, c_int, P, P, P]),
+    "ipcb_point_triangle_toi": (c_int, [SP, P, BP, c_double, c_int, P, P, P]),
+    "ipcb_collision_time": (c_int, [c_int, c_int, P, P, P, P, P]),
+    "ipcb_cubic_roots": (c_int, [c_int, P, c_double, c_double, P, P, P, P]),
+    "ipcb_bsr_workspace": (c_size_t, [c_int, c_int, c_int]),
+    "ipcb_bsr_from_triplets": (c_int, [c_int, c_int, c_int, P, P, P, c_int, P, P, P, P, P, c_size_t, P]),
+    "ipcb_bsr_mv": (c_int, [c_int, P, P, P, c_int, P, P, c_double, c_double, P]),
+}
+
+
+class NativeError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise NativeError(
+                f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+                "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def call(name: str, *args):
+    """Invoke a C-ABI entry point; raise on a non-zero return code."""
+    rc = getattr(lib(), name)(*args)
+    if rc != 0:
+        msg = lib().ipcb_last_error()
+        raise NativeError(f"{name} returned {rc}: {msg.decode() if msg else ''}")
+    return rc
+
+
+def size(name: str, *args) -> int:
+    return int(getattr(lib(), name)(*args))
+
+
+def ptr(t) -> int:
+    """Device pointer of a torch tensor (None -> NULL)."""
+    return None if t is None else t.data_ptr()
+
+
+def stream_handle(stream=None):
+    import torch
+
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return c_void_p(s.cuda_stream)

@@ -1,0 +1,492 @@
+// Continuous collision detection: swept boxes, coplanarity-cubic time of
+// impact (ccd/ccd.py:166-427, ccd/cubic_roots.py:7-193), all root arithmetic
+// in double.  This file is compiled with -fmad=false: every operation rounds
+// on its own, in source order, so the TOI is reproducible bit for bit by a
+// plain IEEE evaluation.
+#include "common.cuh"
+#include "lbvh.cuh"
+
+namespace ipcb {
+int check_launch(const char* where);
+
+namespace {
+
+constexpr int kFindIters = 200;  // bound on the bracketed Newton/bisection loop
+constexpr double kXError = 1e-10;  // cubic_roots.py:4
+
+struct Q4 {
+  double c[4];
+};
+struct D3v {
+  double v[3];
+};
+
+IPCB_D double evaluate(const Q4& p, double x) { return p.c[0] + x * (p.c[1] + x * (p.c[2] + x * p.c[3])); }
+IPCB_D double multi_sign(double a, double b) { return b < 0.0 ? -a : a; }
+IPCB_D bool diff_sign(double y0, double yr) { return y0 * yr < 0.0; }
+IPCB_D double dmin(double a, double b) { return a < b ? a : b; }
+IPCB_D double dmax(double a, double b) { return a > b ? a : b; }
+
+IPCB_D D3v deflate(const Q4& p, double root) {
+  D3v d;
+  d.v[2] = p.c[3];
+  d.v[1] = p.c[2] + root * d.v[2];
+  d.v[0] = p.c[1] + root * d.v[1];
+  return d;
+}
+
+IPCB_D double find_closed(const Q4& p, const Q4& dp, double x0, double x1, double y0, double y1, int& status) {
+  (void)y1;
+  double xr = (x0 + x1) / 2.0;
+  double yr = evaluate(p, xr);
+  double xb0 = x0, xb1 = x1;
+  if (x1 - x0 <= kXError * 2.0) return xr;
+  for (int it = 0;; ++it) {
+    if (it >= kFindIters) {
+      status |= IPCB_STATUS_ROOT_ITERS;
+      break;
+    }
+    if (diff_sign(y0, yr)) xb1 = xr;
+    else xb0 = xr;
+    double dy = evaluate(dp, xr);
+    double dx = yr / dy;
+    double xn = xr - dx;
+    if (xn > xb0 && xn < xb1) {
+      double step = fabs(xr - xn);
+      xr = xn;
+      if (step > kXError) yr = evaluate(p, xr);
+      else break;
+    } else {
+      xr = (xb0 + xb1) / 2.0;
+      yr = evaluate(p, xr);
+      if (xb0 == xr || xb1 == xr || xb1 - xb0 <= 2.0 * kXError) break;
+    }
+  }
+  return xr;
+}
+
+IPCB_D int quadratic_roots(const D3v& q, double x0, double x1, double* roots) {
+  double c = q.v[0], b = q.v[1], a = q.v[2];
+  double delta = b * b - 4.0 * a * c;
+  int ret = 0;
+  roots[0] = roots[1] = 0.0;
+  if (delta > 0.0) {
+    double d = sqrt(delta);
+    double qq = -(b + multi_sign(d, b)) * 0.5;
+    double rv0 = qq / a, rv1 = c / qq;
+    double xa = dmin(rv0, rv1), xb = dmax(rv0, rv1);
+    if (xa >= x0 && xa <= x1) roots[ret++] = xa;
+    if (xb >= x0 && xb <= x1) roots[ret++] = xb;
+  } else if (delta < 0.0) {
+    ret = 0;
+  } else {
+    double r0 = -0.5 * b / a;
+    roots[0] = r0;
+    if (r0 >= x0 && r0 <= x1) ret = 1;
+  }
+  return ret;
+}
+
+// cubic_roots.py:96-193: real roots in [x0, x1], ascending.
+IPCB_D int cubic_roots(const Q4& p, double x0, double x1, double* roots, int& status) {
+  roots[0] = roots[1] = roots[2] = 0.0;
+  double y0 = evaluate(p, x0), y1 = evaluate(p, x1);
+  double a = p.c[3] * 3.0, b_2 = p.c[2], c = p.c[1];
+  Q4 dp{{c, 2.0 * b_2, a, 0.0}};
+  double delta_4 = b_2 * b_2 - a * c;
+  double q2[2];
+  if (delta_4 > 0.0) {
+    double d_2 = sqrt(delta_4);
+    double q = -(b_2 + multi_sign(d_2, b_2));
+    double rv0 = q / a, rv1 = c / q;
+    double xa = dmin(rv0, rv1), xb = dmax(rv0, rv1);
+    if (diff_sign(y0, y1)) {
+      if (xa >= x1 || xb <= x0 || (xa <= x0 && xb >= x1)) {
+        roots[0] = find_closed(p, dp, x0, x1, y0, y1, status);
+        return 1;
+      }
+    } else {
+      if (xa >= x1 || xb <= x0 || (xa <= x0 && xb >= x1)) return 0;
+    }
+    if (xa > x0) {
+      double ya = evaluate(p, xa);
+      if (diff_sign(y0, ya)) {
+        roots[0] = find_closed(p, dp, x0, xa, y0, ya, status);
+        if (diff_sign(ya, y1) || (xb < x1 && diff_sign(ya, evaluate(p, xb)))) {
+          int r = quadratic_roots(deflate(p, roots[0]), xa, x1, q2);
+          roots[1] = q2[0];
+          roots[2] = q2[1];
+          return r + 1;
+        }
+        return 1;
+      }
+      if (xb < x1) {
+        double yb = evaluate(p, xb);
+        if (diff_sign(ya, yb)) {
+          roots[0] = find_closed(p, dp, xa, xb, ya, yb, status);
+          if (diff_sign(yb, y1)) {
+            int r = quadratic_roots(deflate(p, roots[0]), xb, x1, q2);
+            roots[1] = q2[0];
+            roots[2] = q2[1];
+            return r + 1;
+          }
+          return 1;
+        }
+        if (diff_sign(yb, y1)) {
+          roots[0] = find_closed(p, dp, xb, x1, yb, y1, status);
+          return 1;
+        }
+      } else if (diff_sign(ya, y1)) {
+        roots[0] = find_closed(p, dp, xa, x1, ya, y1, status);
+        return 1;
+      }
+    } else {
+      double yb = evaluate(p, xb);
+      if (diff_sign(y0, yb)) {
+        roots[0] = find_closed(p, dp, x0, xb, y0, yb, status);
+        if (diff_sign(yb, y1)) {
+          int r = quadratic_roots(deflate(p, roots[0]), xb, x1, q2);
+          roots[1] = q2[0];
+          roots[2] = q2[1];
+          return r + 1;
+        }
+        return 1;
+      }
+      if (diff_sign(yb, y1)) {
+        roots[0] = find_closed(p, dp, xb, x1, yb, y1, status);
+        return 1;
+      }
+    }
+    return 0;
+  }
+  if (diff_sign(y0, y1)) {
+    roots[0] = find_closed(p, dp, x0, x1, y0, y1, status);
+    return 1;
+  }
+  return 0;
+}
+
+// ccd.py:293-300: coefficients of prod_k (b_k + t a_k), ascending powers
+IPCB_D Q4 cubic_binomial(double a0, double a1, double a2, double b0, double b1, double b2) {
+  Q4 r;
+  r.c[0] = b0 * b1 * b2;
+  r.c[1] = a0 * b1 * b2 + b0 * b1 * a2 + b0 * a1 * b2;
+  r.c[2] = a0 * a1 * b2 + a0 * b1 * a2 + b0 * a1 * a2;
+  r.c[3] = a0 * a1 * a2;
+  return r;
+}
+
+// det(B + t A) for 3x3 matrices given by columns (ccd.py:252-290)
+IPCB_D Q4 det_polynomial(const d3* A, const d3* B) {
+  // M[r][c] = col_c[r]
+  auto m = [](const d3* C, int r, int c) -> double { return r == 0 ? C[c].x : (r == 1 ? C[c].y : C[c].z); };
+  Q4 pos{{0, 0, 0, 0}}, neg{{0, 0, 0, 0}};
+  const int P[3][3][2] = {{{0, 0}, {1, 1}, {2, 2}}, {{0, 1}, {1, 2}, {2, 0}}, {{0, 2}, {1, 0}, {2, 1}}};
+  const int N[3][3][2] = {{{0, 0}, {1, 2}, {2, 1}}, {{0, 1}, {1, 0}, {2, 2}}, {{0, 2}, {1, 1}, {2, 0}}};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    Q4 t = cubic_binomial(m(A, P[k][0][0], P[k][0][1]), m(A, P[k][1][0], P[k][1][1]), m(A, P[k][2][0], P[k][2][1]),
+                          m(B, P[k][0][0], P[k][0][1]), m(B, P[k][1][0], P[k][1][1]), m(B, P[k][2][0], P[k][2][1]));
+#pragma unroll
+    for (int q = 0; q < 4; ++q) pos.c[q] = pos.c[q] + t.c[q];
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    Q4 t = cubic_binomial(m(A, N[k][0][0], N[k][0][1]), m(A, N[k][1][0], N[k][1][1]), m(A, N[k][2][0], N[k][2][1]),
+                          m(B, N[k][0][0], N[k][0][1]), m(B, N[k][1][0], N[k][1][1]), m(B, N[k][2][0], N[k][2][1]));
+#pragma unroll
+    for (int q = 0; q < 4; ++q) neg.c[q] = neg.c[q] + t.c[q];
+  }
+  Q4 r;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) r.c[q] = pos.c[q] - neg.c[q];
+  return r;
+}
+
+// ccd.py:226-249: roots in [0,1] of det[p1-p0 ...] coplanarity polynomial
+IPCB_D int coplanar_roots(const d3* p0, const d3* p1, double* roots, int& status) {
+  const int cols[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
+  Q4 acc{{0, 0, 0, 0}};
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    d3 A[3], B[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      B[c] = p0[cols[m][c]];
+      A[c] = p1[cols[m][c]] - p0[cols[m][c]];
+    }
+    Q4 d = det_polynomial(A, B);
+    double sg = (m & 1) ? -1.0 : 1.0;
+    if (m == 0) acc = d;
+    else
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc.c[q] = sg > 0 ? acc.c[q] + d.c[q] : acc.c[q] - d.c[q];
+  }
+  return cubic_roots(acc, 0.0, 1.0, roots, status);
+}
+
+IPCB_D d3 lerp(d3 a, d3 b, double t) { return a * (1.0 - t) + b * t; }
+
+// Least-squares coordinates of the coplanar configuration (ipctkwp
+// beta_gamma_pt/ee, restated): PT solves x0 - x1 = beta e1 + gamma e2,
+// EE solves x2 - x0 = beta ea + gamma eb.
+IPCB_D void solve2(double a11, double a12, double a22, double b1, double b2, double& be, double& ga) {
+  double det = a11 * a22 - a12 * a12;
+  be = (b1 * a22 - a12 * b2) / det;
+  ga = (a11 * b2 - a12 * b1) / det;
+}
+
+IPCB_D bool verify_pt(const d3* x) {
+  d3 e1 = x[2] - x[1], e2 = x[3] - x[1], w = x[0] - x[1];
+  double be, ga;
+  solve2(dot(e1, e1), dot(e1, e2), dot(e2, e2), dot(e1, w), dot(e2, w), be, ga);
+  const double tol = 1e-8;
+  return be >= -tol && ga >= -tol && be + ga <= 1.0 + tol;
+}
+
+IPCB_D bool verify_ee(const d3* x) {
+  d3 ea = x[1] - x[0], eb = x[3] - x[2], w = x[2] - x[0];
+  double be, ga;
+  solve2(dot(ea, ea), dot(ea, eb), dot(eb, eb), dot(ea, w), dot(eb, w), be, ga);
+  const double tol = 1e-8;
+  return be >= -tol && be <= 1.0 + tol && -ga >= -tol && -ga <= 1.0 + tol;
+}
+
+// ccd.py:304-357
+template <int KIND>
+IPCB_D double collision_time(const d3* p0, const d3* p1, int& status) {
+  double roots[3];
+  int nr = coplanar_roots(p0, p1, roots, status);
+  double root = 1.0;
+  bool ok = false;
+  for (int i = 0; i < nr; ++i) {
+    root = roots[i];
+    d3 xt[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) xt[k] = lerp(p0[k], p1[k], root);
+    ok = KIND == 0 ? verify_ee(xt) : verify_pt(xt);
+    if (ok) break;
+  }
+  return ok ? root : 1.0;
+}
+
+template <class S>
+IPCB_D d3 ld(const S* __restrict__ x, int i) {
+  return mk3((double)__ldg(x + 3 * i), (double)__ldg(x + 3 * i + 1), (double)__ldg(x + 3 * i + 2));
+}
+
+IPCB_D void store_toi(float* toi, double t) { atomic_min_nonneg(toi, __double2float_rz(t)); }
+IPCB_D void store_toi(double* toi, double t) { atomic_min_nonneg(toi, t); }
+
+template <class S>
+__global__ void k_add_dx(const S* __restrict__ x, const S* __restrict__ dx, S* __restrict__ x1, int n3) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n3) x1[i] = x[i] - dx[i];
+}
+
+template <class S, int NV>
+__global__ void k_swept(const S* __restrict__ x0, const S* __restrict__ x1, const int* __restrict__ prims, int n,
+                        double pad, float* __restrict__ lo, float* __restrict__ hi) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    int k = __ldg(prims + NV * i + v);
+    d3 a = ld(x0, k), b = ld(x1, k);
+    mn[0] = dmin(mn[0], dmin(a.x, b.x)); mx[0] = dmax(mx[0], dmax(a.x, b.x));
+    mn[1] = dmin(mn[1], dmin(a.y, b.y)); mx[1] = dmax(mx[1], dmax(a.y, b.y));
+    mn[2] = dmin(mn[2], dmin(a.z, b.z)); mx[2] = dmax(mx[2], dmax(a.z, b.z));
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    lo[3 * i + k] = __double2float_rd(mn[k] - pad);
+    hi[3 * i + k] = __double2float_ru(mx[k] + pad);
+  }
+}
+
+template <class S>
+__global__ void __launch_bounds__(128) k_ee_toi(const S* __restrict__ x0, const S* __restrict__ x1,
+                                                const int* __restrict__ edges, const int* __restrict__ body,
+                                                const float4* __restrict__ nodes, const int* __restrict__ order, int n,
+                                                const float* __restrict__ lo, const float* __restrict__ hi,
+                                                int exclude, S* toi, int* status) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int i = __ldg(order + t);
+  int2 ea = __ldg(reinterpret_cast<const int2*>(edges) + i);
+  int bi = exclude ? __ldg(body + ea.x) : 0;
+  f3 qlo = mk3(__ldg(lo + 3 * i), __ldg(lo + 3 * i + 1), __ldg(lo + 3 * i + 2));
+  f3 qhi = mk3(__ldg(hi + 3 * i), __ldg(hi + 3 * i + 1), __ldg(hi + 3 * i + 2));
+  int st = 0;
+  bool ok = traverse(nodes, n, qlo, qhi, [&](int j) {
+    if (!(i < j)) return;
+    int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + j);
+    if (ea.x == eb.x || ea.x == eb.y || ea.y == eb.x || ea.y == eb.y) return;
+    if (exclude && bi == __ldg(body + eb.x)) return;
+    d3 p0[4] = {ld(x0, ea.x), ld(x0, ea.y), ld(x0, eb.x), ld(x0, eb.y)};
+    d3 p1[4] = {ld(x1, ea.x), ld(x1, ea.y), ld(x1, eb.x), ld(x1, eb.y)};
+    double tt = collision_time<0>(p0, p1, st);
+    if (tt < 1.0) store_toi(toi, tt);
+  });
+  if (!ok) st |= IPCB_STATUS_STACK;
+  if (st) atomicOr(status, st);
+}
+
+template <class S>
+__global__ void __launch_bounds__(128) k_pt_toi(const S* __restrict__ x0, const S* __restrict__ x1,
+                                                const int* __restrict__ tris, const int* __restrict__ body,
+                                                const float4* __restrict__ nodes, int n_tris, int nv, double pad,
+                                                int exclude, S* toi, int* status) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  d3 a = ld(x0, i), b = ld(x1, i);
+  f3 qlo = mk3(__double2float_rd(dmin(a.x, b.x) - pad), __double2float_rd(dmin(a.y, b.y) - pad),
+               __double2float_rd(dmin(a.z, b.z) - pad));
+  f3 qhi = mk3(__double2float_ru(dmax(a.x, b.x) + pad), __double2float_ru(dmax(a.y, b.y) + pad),
+               __double2float_ru(dmax(a.z, b.z) + pad));
+  int bi = exclude ? __ldg(body + i) : 0;
+  int st = 0;
+  bool ok = traverse(nodes, n_tris, qlo, qhi, [&](int j) {
+    int t0 = __ldg(tris + 3 * j), t1 = __ldg(tris + 3 * j + 1), t2 = __ldg(tris + 3 * j + 2);
+    if (i == t0 || i == t1 || i == t2) return;
+    if (exclude && bi == __ldg(body + t0)) return;
+    d3 p0[4] = {a, ld(x0, t0), ld(x0, t1), ld(x0, t2)};
+    d3 p1[4] = {b, ld(x1, t0), ld(x1, t1), ld(x1, t2)};
+    double tt = collision_time<1>(p0, p1, st);
+    if (tt < 1.0) store_toi(toi, tt);
+  });
+  if (!ok) st |= IPCB_STATUS_STACK;
+  if (st) atomicOr(status, st);
+}
+
+__global__ void k_pair_time(int kind, int n, const double* __restrict__ a, const double* __restrict__ b,
+                            double* __restrict__ t, int* status) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  d3 p0[4], p1[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    p0[k] = mk3(a[12 * i + 3 * k], a[12 * i + 3 * k + 1], a[12 * i + 3 * k + 2]);
+    p1[k] = mk3(b[12 * i + 3 * k], b[12 * i + 3 * k + 1], b[12 * i + 3 * k + 2]);
+  }
+  int st = 0;
+  t[i] = kind == 0 ? collision_time<0>(p0, p1, st) : collision_time<1>(p0, p1, st);
+  if (st) atomicOr(status, st);
+}
+
+__global__ void k_cubic(int n, const double* __restrict__ coef, double x0, double x1, double* __restrict__ roots,
+                        int* __restrict__ nr, int* status) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Q4 p{{coef[4 * i], coef[4 * i + 1], coef[4 * i + 2], coef[4 * i + 3]}};
+  int st = 0;
+  double r[3];
+  nr[i] = cubic_roots(p, x0, x1, r, st);
+  roots[3 * i] = r[0];
+  roots[3 * i + 1] = r[1];
+  roots[3 * i + 2] = r[2];
+  if (st) atomicOr(status, st);
+}
+
+}  // namespace
+}  // namespace ipcb
+
+using namespace ipcb;
+
+extern "C" {
+
+int ipcb_add_dx(const ipcb_soup* soup, const void* dx, void* x1, ipcb_stream s) {
+  if (!soup || !dx || !x1) return IPCB_E_ARG;
+  int n3 = 3 * soup->n_verts;
+  if (n3 == 0) return IPCB_OK;
+  if (soup->fp64)
+    k_add_dx<double><<<div_up(n3, 256), 256, 0, (cudaStream_t)s>>>((const double*)soup->x, (const double*)dx,
+                                                                   (double*)x1, n3);
+  else
+    k_add_dx<float><<<div_up(n3, 256), 256, 0, (cudaStream_t)s>>>((const float*)soup->x, (const float*)dx,
+                                                                  (float*)x1, n3);
+  return check_launch("ipcb_add_dx");
+}
+
+int ipcb_swept_edge_aabbs(const ipcb_soup* soup, const void* x1, double pad, float* lower, float* upper,
+                          ipcb_stream s) {
+  if (!soup || !x1 || !lower || !upper) return IPCB_E_ARG;
+  int n = soup->n_edges;
+  if (n == 0) return IPCB_OK;
+  if (soup->fp64)
+    k_swept<double, 2><<<div_up(n, 256), 256, 0, (cudaStream_t)s>>>((const double*)soup->x, (const double*)x1,
+                                                                    soup->edges, n, pad, lower, upper);
+  else
+    k_swept<float, 2><<<div_up(n, 256), 256, 0, (cudaStream_t)s>>>((const float*)soup->x, (const float*)x1,
+                                                                   soup->edges, n, pad, lower, upper);
+  return check_launch("ipcb_swept_edge_aabbs");
+}
+
+int ipcb_swept_triangle_aabbs(const ipcb_soup* soup, const void* x1, double pad, float* lower, float* upper,
+                              ipcb_stream s) {
+  if (!soup || !x1 || !lower || !upper) return IPCB_E_ARG;
+  int n = soup->n_tris;
+  if (n == 0) return IPCB_OK;
+  if (soup->fp64)
+    k_swept<double, 3><<<div_up(n, 256), 256, 0, (cudaStream_t)s>>>((const double*)soup->x, (const double*)x1,
+                                                                    soup->triangles, n, pad, lower, upper);
+  else
+    k_swept<float, 3><<<div_up(n, 256), 256, 0, (cudaStream_t)s>>>((const float*)soup->x, (const float*)x1,
+                                                                   soup->triangles, n, pad, lower, upper);
+  return check_launch("ipcb_swept_triangle_aabbs");
+}
+
+int ipcb_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, const float* lower,
+                       const float* upper, int exclude_same_body, void* toi, int* status, ipcb_stream s) {
+  if (!soup || !x1 || !bvh || !lower || !upper || !toi || !status || bvh->n != soup->n_edges) return IPCB_E_ARG;
+  int n = soup->n_edges;
+  if (n == 0) return IPCB_OK;
+  dim3 g(div_up(n, 128));
+  if (soup->fp64)
+    k_ee_toi<double><<<g, 128, 0, (cudaStream_t)s>>>((const double*)soup->x, (const double*)x1, soup->edges,
+                                                     soup->body, (const float4*)bvh->nodes, bvh->sorted, n, lower,
+                                                     upper, exclude_same_body, (double*)toi, status);
+  else
+    k_ee_toi<float><<<g, 128, 0, (cudaStream_t)s>>>((const float*)soup->x, (const float*)x1, soup->edges,
+                                                    soup->body, (const float4*)bvh->nodes, bvh->sorted, n, lower,
+                                                    upper, exclude_same_body, (float*)toi, status);
+  return check_launch("ipcb_edge_edge_toi");
+}
+
+int ipcb_point_triangle_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, double pad,
+                            int exclude_same_body, void* toi, int* status, ipcb_stream s) {
+  if (!soup || !x1 || !bvh || !toi || !status || bvh->n != soup->n_tris) return IPCB_E_ARG;
+  int nv = soup->n_verts;
+  if (nv == 0 || soup->n_tris == 0) return IPCB_OK;
+  dim3 g(div_up(nv, 128));
+  if (soup->fp64)
+    k_pt_toi<double><<<g, 128, 0, (cudaStream_t)s>>>((const double*)soup->x, (const double*)x1, soup->triangles,
+                                                     soup->body, (const float4*)bvh->nodes, soup->n_tris, nv, pad,
+                                                     exclude_same_body, (double*)toi, status);
+  else
+    k_pt_toi<float><<<g, 128, 0, (cudaStream_t)s>>>((const float*)soup->x, (const float*)x1, soup->triangles,
+                                                    soup->body, (const float4*)bvh->nodes, soup->n_tris, nv, pad,
+                                                    exclude_same_body, (float*)toi, status);
+  return check_launch("ipcb_point_triangle_toi");
+}
+
+int ipcb_collision_time(int kind, int n, const double* p_t0, const double* p_t1, double* t, int* status,
+                        ipcb_stream s) {
+  if (n < 0 || (kind != 0 && kind != 1)) return IPCB_E_ARG;
+  if (n == 0) return IPCB_OK;
+  if (!p_t0 || !p_t1 || !t || !status) return IPCB_E_ARG;
+  k_pair_time<<<div_up(n, 128), 128, 0, (cudaStream_t)s>>>(kind, n, p_t0, p_t1, t, status);
+  return check_launch("ipcb_collision_time");
+}
+
+int ipcb_cubic_roots(int n, const double* coef, double x0, double x1, double* roots, int* n_roots, int* status,
+                     ipcb_stream s) {
+  if (n < 0) return IPCB_E_ARG;
+  if (n == 0) return IPCB_OK;
+  if (!coef || !roots || !n_roots || !status) return IPCB_E_ARG;
+  k_cubic<<<div_up(n, 128), 128, 0, (cudaStream_t)s>>>(n, coef, x0, x1, roots, n_roots, status);
+  return check_launch("ipcb_cubic_roots");
+}
+
+}  // extern "C"

@@ -1,0 +1,265 @@
+// LBVH build and refit (Karras 2012, "Maximizing parallelism in the
+// construction of BVHs, octrees, and k-d trees") and the exported radix sort.
+#include <cstdio>
+#include <cstring>
+
+#include "common.cuh"
+#include "lbvh.cuh"
+#include "sort.cuh"
+
+namespace ipcb {
+
+static thread_local char g_err[256] = "";
+void set_error(const char* where, cudaError_t e) {
+  snprintf(g_err, sizeof(g_err), "%s: %s", where, cudaGetErrorString(e));
+}
+void set_error_msg(const char* msg) { snprintf(g_err, sizeof(g_err), "%s", msg); }
+const char* last_error() { return g_err; }
+
+int check_launch(const char* where) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error(where, e);
+    return IPCB_E_CUDA;
+  }
+  return IPCB_OK;
+}
+
+namespace {
+
+// 10-bit spread: b9..b0 -> b9 0 0 b8 0 0 ... b0
+IPCB_D unsigned spread10(unsigned v) {
+  v = (v * 0x00010001u) & 0xFF0000FFu;
+  v = (v * 0x00000101u) & 0x0F00F00Fu;
+  v = (v * 0x00000011u) & 0xC30C30C3u;
+  v = (v * 0x00000005u) & 0x49249249u;
+  return v;
+}
+
+__global__ void k_centre_bounds(const float* __restrict__ lo, const float* __restrict__ hi, int n,
+                                unsigned* __restrict__ bounds) {
+  float mn[3] = {3.4e38f, 3.4e38f, 3.4e38f}, mx[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      float c = 0.5f * (lo[3 * i + k] + hi[3 * i + k]);
+      mn[k] = fminf(mn[k], c);
+      mx[k] = fmaxf(mx[k], c);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[k] = fminf(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+      mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      atomicMin(bounds + k, f2ord(mn[k]));
+      atomicMax(bounds + 3 + k, f2ord(mx[k]));
+    }
+  }
+}
+
+__global__ void k_morton(const float* __restrict__ lo, const float* __restrict__ hi, int n,
+                         const unsigned* __restrict__ bounds, unsigned* __restrict__ keys, int* __restrict__ vals) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned code = 0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float bmin = ord2f(bounds[k]), bmax = ord2f(bounds[3 + k]);
+    float ext = bmax - bmin;
+    float c = 0.5f * (lo[3 * i + k] + hi[3 * i + k]);
+    float u = ext > 0.f ? (c - bmin) / ext : 0.5f;
+    unsigned q = (unsigned)fminf(fmaxf(u * 1024.f, 0.f), 1023.f);
+    code |= spread10(q) << (2 - k);
+  }
+  keys[i] = code;
+  vals[i] = i;
+}
+
+// common-prefix length of sorted keys i and j, ties broken by index
+IPCB_D int delta(const unsigned* __restrict__ k, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  unsigned a = k[i], b = k[j];
+  if (a == b) return 32 + __clz((unsigned)(i ^ j));
+  return __clz(a ^ b);
+}
+
+// One thread per internal node: range, split, child codes and parents.
+__global__ void k_karras(const unsigned* __restrict__ keys, const int* __restrict__ sorted, int n,
+                         float4* __restrict__ nodes, int* __restrict__ parent, int cap) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+  int dmin = delta(keys, n, i, i - d);
+  int lmax = 2;
+  while (delta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int t = lmax >> 1; t >= 1; t >>= 1)
+    if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+  int j = i + l * d;
+  int dnode = delta(keys, n, i, j);
+  int s = 0;
+  for (int div = 2;; div <<= 1) {
+    int t = (l + div - 1) / div;
+    if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+    if (t <= 1) break;
+  }
+  int g = i + s * d + min(d, 0);
+  int first = min(i, j), last = max(i, j);
+  int lcode, rcode;
+  if (first == g) {
+    lcode = ~sorted[g];
+    parent[cap + g] = (i << 1) | 0;
+  } else {
+    lcode = g;
+    parent[g] = (i << 1) | 0;
+  }
+  if (last == g + 1) {
+    rcode = ~sorted[g + 1];
+    parent[cap + g + 1] = (i << 1) | 1;
+  } else {
+    rcode = g + 1;
+    parent[g + 1] = (i << 1) | 1;
+  }
+  nodes[4 * i + 0].w = __int_as_float(lcode);
+  nodes[4 * i + 2].w = __int_as_float(rcode);
+}
+
+// Bottom-up refit: a leaf writes its box into its parent's slot; the second
+// child to arrive at a node merges both slots and continues upward.
+__global__ void k_refit(const float* __restrict__ lo, const float* __restrict__ hi, int n,
+                        const int* __restrict__ sorted, const int* __restrict__ parent, int cap,
+                        float4* __restrict__ nodes, unsigned* __restrict__ flags) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int prim = sorted[k];
+  float3 bl = make_float3(lo[3 * prim], lo[3 * prim + 1], lo[3 * prim + 2]);
+  float3 bh = make_float3(hi[3 * prim], hi[3 * prim + 1], hi[3 * prim + 2]);
+  int code = ~prim;
+  if (n == 1) {
+    nodes[0] = make_float4(bl.x, bl.y, bl.z, __int_as_float(code));
+    nodes[1] = make_float4(bh.x, bh.y, bh.z, 0.f);
+    nodes[2] = make_float4(3.4e38f, 3.4e38f, 3.4e38f, __int_as_float(code));
+    nodes[3] = make_float4(-3.4e38f, -3.4e38f, -3.4e38f, 0.f);
+    return;
+  }
+  int par = parent[cap + k];
+  // Depth is bounded by the 30 Morton bits plus 32 index bits of the
+  // tie-break; the loop bound only guards against a corrupted parent array.
+  for (int level = 0; level < 128; ++level) {
+    int node = par >> 1, side = par & 1;
+    __stcg(nodes + 4 * node + 2 * side, make_float4(bl.x, bl.y, bl.z, __int_as_float(code)));
+    __stcg(nodes + 4 * node + 2 * side + 1, make_float4(bh.x, bh.y, bh.z, 0.f));
+    __threadfence();
+    unsigned old = atomicAdd(flags + node, 1u);
+    if (old == 0) return;
+    flags[node] = 0;
+    float4 sl = __ldcg(nodes + 4 * node + 2 * (1 - side));
+    float4 sh = __ldcg(nodes + 4 * node + 2 * (1 - side) + 1);
+    bl = make_float3(fminf(bl.x, sl.x), fminf(bl.y, sl.y), fminf(bl.z, sl.z));
+    bh = make_float3(fmaxf(bh.x, sh.x), fmaxf(bh.y, sh.y), fmaxf(bh.z, sh.z));
+    if (node == 0) return;
+    code = node;
+    par = parent[node];
+  }
+}
+
+inline size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+}  // namespace
+}  // namespace ipcb
+
+using namespace ipcb;
+
+extern "C" {
+
+int ipcb_version(void) { return 1; }
+const char* ipcb_last_error(void) { return ipcb::last_error(); }
+
+size_t ipcb_sort_workspace_u32(int n) { return sort::workspace_bytes<unsigned>(n < 1 ? 1 : n); }
+size_t ipcb_sort_workspace_u64(int n) { return sort::workspace_bytes<unsigned long long>(n < 1 ? 1 : n); }
+
+int ipcb_sort_pairs_u32(unsigned* keys, int* vals, int n, int end_bit, void* ws, size_t ws_bytes, ipcb_stream s) {
+  if (n < 0 || end_bit < 0 || end_bit > 32) return IPCB_E_ARG;
+  if (n <= 1) return IPCB_OK;
+  if (!keys || !vals || !ws || ws_bytes < sort::workspace_bytes<unsigned>(n)) return IPCB_E_ARG;
+  sort::sort_pairs<unsigned>(keys, vals, n, end_bit, ws, ws_bytes, (cudaStream_t)s);
+  return check_launch("ipcb_sort_pairs_u32");
+}
+
+int ipcb_sort_pairs_u64(unsigned long long* keys, int* vals, int n, int end_bit, void* ws, size_t ws_bytes,
+                        ipcb_stream s) {
+  if (n < 0 || end_bit < 0 || end_bit > 64) return IPCB_E_ARG;
+  if (n <= 1) return IPCB_OK;
+  if (!keys || !vals || !ws || ws_bytes < sort::workspace_bytes<unsigned long long>(n)) return IPCB_E_ARG;
+  sort::sort_pairs<unsigned long long>(keys, vals, n, end_bit, ws, ws_bytes, (cudaStream_t)s);
+  return check_launch("ipcb_sort_pairs_u64");
+}
+
+size_t ipcb_lbvh_bytes(int capacity) {
+  if (capacity < 1) capacity = 1;
+  size_t c = (size_t)capacity;
+  size_t nn = c > 1 ? c - 1 : 1;
+  return al256(nn * 4 * 16) + al256(2 * c * 4) + al256(c * 4) + al256(c * 4) + al256(c * 4);
+}
+
+int ipcb_lbvh_bind(ipcb_lbvh* bvh, void* mem, int capacity) {
+  if (!bvh || !mem || capacity < 1) return IPCB_E_ARG;
+  size_t c = (size_t)capacity;
+  size_t nn = c > 1 ? c - 1 : 1;
+  char* p = (char*)mem;
+  bvh->n = 0;
+  bvh->capacity = capacity;
+  bvh->nodes = p;
+  p += al256(nn * 4 * 16);
+  bvh->parent = (int*)p;
+  p += al256(2 * c * 4);
+  bvh->sorted = (int*)p;
+  p += al256(c * 4);
+  bvh->keys = (unsigned*)p;
+  p += al256(c * 4);
+  bvh->flags = (unsigned*)p;
+  return IPCB_OK;
+}
+
+size_t ipcb_lbvh_build_workspace(int n) { return 256 + sort::workspace_bytes<unsigned>(n < 1 ? 1 : n); }
+
+int ipcb_lbvh_build(ipcb_lbvh* bvh, const float* lower, const float* upper, int n, void* ws, size_t ws_bytes,
+                    ipcb_stream s) {
+  if (!bvh || n < 0 || n > bvh->capacity) return IPCB_E_ARG;
+  cudaStream_t st = (cudaStream_t)s;
+  bvh->n = n;
+  if (n == 0) return IPCB_OK;
+  if (!lower || !upper || !ws || ws_bytes < ipcb_lbvh_build_workspace(n)) return IPCB_E_ARG;
+  unsigned* bounds = (unsigned*)ws;
+  void* sws = (char*)ws + 256;
+  cudaMemsetAsync(bounds, 0xff, 3 * sizeof(unsigned), st);
+  cudaMemsetAsync(bounds + 3, 0x00, 3 * sizeof(unsigned), st);
+  cudaMemsetAsync(bvh->flags, 0, (size_t)n * sizeof(unsigned), st);
+  int nb = min(div_up(n, 256), 148 * 8);
+  k_centre_bounds<<<nb, 256, 0, st>>>(lower, upper, n, bounds);
+  k_morton<<<div_up(n, 256), 256, 0, st>>>(lower, upper, n, bounds, bvh->keys, bvh->sorted);
+  sort::sort_pairs<unsigned>(bvh->keys, bvh->sorted, n, 30, sws, ws_bytes - 256, st);
+  if (n > 1)
+    k_karras<<<div_up(n - 1, 256), 256, 0, st>>>(bvh->keys, bvh->sorted, n, (float4*)bvh->nodes, bvh->parent,
+                                                  bvh->capacity);
+  k_refit<<<div_up(n, 256), 256, 0, st>>>(lower, upper, n, bvh->sorted, bvh->parent, bvh->capacity,
+                                           (float4*)bvh->nodes, bvh->flags);
+  return check_launch("ipcb_lbvh_build");
+}
+
+int ipcb_lbvh_refit(const ipcb_lbvh* bvh, const float* lower, const float* upper, ipcb_stream s) {
+  if (!bvh || bvh->n < 0) return IPCB_E_ARG;
+  if (bvh->n == 0) return IPCB_OK;
+  if (!lower || !upper) return IPCB_E_ARG;
+  k_refit<<<div_up(bvh->n, 256), 256, 0, (cudaStream_t)s>>>(lower, upper, bvh->n, bvh->sorted, bvh->parent,
+                                                            bvh->capacity, (float4*)bvh->nodes, bvh->flags);
+  return check_launch("ipcb_lbvh_refit");
+}
+
+}  // extern "C"

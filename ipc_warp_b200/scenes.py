@@ -1,0 +1,210 @@
+"""Synthetic scenes for the contact pipeline (host-side numpy, not timed).
+
+The reference loads its meshes from `.tobj`/`.obj` files through libigl
+(fem/geometry.py:165-276); the scenes the benchmarks name are not shipped with
+it, so they are generated here from seeded parameters.  The output follows the
+reference `Soup` layout (fem/geometry.py:165-171):
+
+* ``x``          float[V,3]  world positions (``soup.x_transformed``)
+* ``xcs``        float[V,3]  rest positions
+* ``edges``      int32[2E]   flat surface edges (igl.edges of the surface faces)
+* ``triangles``  int32[3T]   flat outward-oriented surface triangles
+* ``body``       int32[V]    body index per vertex
+* ``tets``       int32[n_tets,4]
+
+Hex cells are split into 5 tetrahedra with the split mirrored on alternating
+cells so that neighbouring cells share face diagonals.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# Corner (dx, dy, dz) bits of a hex cell.
+_CORNERS = np.array([[i & 1, (i >> 1) & 1, (i >> 2) & 1] for i in range(8)], dtype=np.int64)
+
+
+def _corner_id(bits):
+    return bits[0] | (bits[1] << 1) | (bits[2] << 2)
+
+
+def _five_tet_split(parity: int):
+    """Return the 5 tets (as corner ids) of a hex cell.
+
+    parity 0: centre tet on the even corners {000,110,101,011};
+    parity 1: centre tet on the odd corners {100,010,001,111}.
+    Each remaining tet joins one corner of the other class with its 3
+    axis neighbours.
+    """
+    even = [0b000, 0b011, 0b101, 0b110]
+    odd = [0b001, 0b010, 0b100, 0b111]
+    centre, tips = (even, odd) if parity == 0 else (odd, even)
+    tets = [list(centre)]
+    for t in tips:
+        nb = [t ^ 1, t ^ 2, t ^ 4]
+        tets.append([t] + nb)
+    return tets
+
+
+@dataclass
+class Mesh:
+    x: np.ndarray
+    tets: np.ndarray
+    triangles: np.ndarray  # [T,3]
+    edges: np.ndarray      # [E,2]
+
+
+def hex_grid_tets(nx: int, ny: int, nz: int, size=(1.0, 1.0, 1.0)) -> Mesh:
+    """Tetrahedralised box with (nx,ny,nz) cells spanning [0,size]."""
+    sx, sy, sz = size
+    gx, gy, gz = np.meshgrid(
+        np.linspace(0.0, sx, nx + 1), np.linspace(0.0, sy, ny + 1), np.linspace(0.0, sz, nz + 1),
+        indexing="ij",
+    )
+    x = np.stack([gx.ravel(), gy.ravel(), gz.ravel()], axis=1)
+
+    def vid(i, j, k):
+        return (i * (ny + 1) + j) * (nz + 1) + k
+
+    tets = []
+    splits = [_five_tet_split(0), _five_tet_split(1)]
+    for i in range(nx):
+        for j in range(ny):
+            for k in range(nz):
+                cid = [vid(i + b[0], j + b[1], k + b[2]) for b in _CORNERS]
+                for t in splits[(i + j + k) & 1]:
+                    tets.append([cid[c] for c in t])
+    tets = np.asarray(tets, dtype=np.int64)
+    # orient every tet positively
+    a, b, c, d = (x[tets[:, q]] for q in range(4))
+    vol = np.einsum("ij,ij->i", np.cross(b - a, c - a), d - a)
+    flip = vol < 0
+    tets[flip, 1], tets[flip, 2] = tets[flip, 2].copy(), tets[flip, 1].copy()
+    tris = boundary_faces(tets)
+    edges = surface_edges(tris)
+    return Mesh(x=x, tets=tets, triangles=tris, edges=edges)
+
+
+def boundary_faces(tets: np.ndarray) -> np.ndarray:
+    """Faces used by exactly one tet, oriented with outward normals
+    (positive tets: face opposite vertex q is wound away from it)."""
+    # faces of a positively oriented tet (a,b,c,d), outward
+    local = np.array([[1, 2, 3], [0, 3, 2], [0, 1, 3], [0, 2, 1]])
+    faces = tets[:, local].reshape(-1, 3)
+    key = np.sort(faces, axis=1)
+    _, inv, cnt = np.unique(key, axis=0, return_inverse=True, return_counts=True)
+    return faces[cnt[inv.ravel()] == 1].astype(np.int64)
+
+
+def surface_edges(tris: np.ndarray) -> np.ndarray:
+    e = np.concatenate([tris[:, [0, 1]], tris[:, [1, 2]], tris[:, [2, 0]]])
+    e = np.sort(e, axis=1)
+    return np.unique(e, axis=0).astype(np.int64)
+
+
+def rot_z(deg: float) -> np.ndarray:
+    t = np.deg2rad(deg)
+    c, s = np.cos(t), np.sin(t)
+    return np.array([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]])
+
+
+@dataclass
+class Scene:
+    name: str
+    x: np.ndarray
+    xcs: np.ndarray
+    edges: np.ndarray
+    triangles: np.ndarray
+    body: np.ndarray
+    tets: np.ndarray
+    dhat: float
+    kappa: float
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n_verts(self):
+        return self.x.shape[0]
+
+    @property
+    def n_edges(self):
+        return self.edges.shape[0] // 2
+
+    @property
+    def n_tris(self):
+        return self.triangles.shape[0] // 3
+
+    @property
+    def thickness(self):
+        """The reference's ``_thickness``: dhat = l0 = 2 * _thickness (contact.py:180)."""
+        return 0.5 * self.dhat
+
+
+def assemble(meshes, name, dhat, kappa, meta=None) -> Scene:
+    xs, es, ts, bs, tets = [], [], [], [], []
+    off = 0
+    for b, m in enumerate(meshes):
+        xs.append(m.x)
+        es.append(m.edges + off)
+        ts.append(m.triangles + off)
+        tets.append(m.tets + off)
+        bs.append(np.full(m.x.shape[0], b, dtype=np.int32))
+        off += m.x.shape[0]
+    x = np.concatenate(xs)
+    return Scene(
+        name=name,
+        x=x.copy(),
+        xcs=x.copy(),
+        edges=np.concatenate(es).astype(np.int32).ravel(),
+        triangles=np.concatenate(ts).astype(np.int32).ravel(),
+        body=np.concatenate(bs).astype(np.int32),
+        tets=np.concatenate(tets).astype(np.int32),
+        dhat=float(dhat),
+        kappa=float(kappa),
+        meta=meta or {},
+    )
+
+
+def two_cubes(n: int = 8, gap: float = 1e-3, angle_deg: float = 15.0, jitter: float = 1e-5,
+              seed: int = 0, dhat: float = 1e-3, kappa: float = 1e4) -> Scene:
+    """Two tetrahedralised unit cubes; the upper one is rotated about z and its
+    lowest vertex sits ``gap`` above the lower cube's top face (y-up)."""
+    rng = np.random.default_rng(seed)
+    lo = hex_grid_tets(n, n, n)
+    up = hex_grid_tets(n, n, n)
+    c = np.array([0.5, 0.5, 0.5])
+    up.x = (up.x - c) @ rot_z(angle_deg).T + c
+    up.x[:, 1] += 1.0 + gap - up.x[:, 1].min()
+    sc = assemble([lo, up], f"two_cubes_{n}", dhat, kappa, {"gap": gap, "angle_deg": angle_deg})
+    sc.x += rng.uniform(-jitter, jitter, size=sc.x.shape)
+    sc.xcs = sc.x.copy()
+    return sc
+
+
+def rod_bundle(n_rods_side: int = 4, cells=(4, 4, 256), width: float = 0.1, spacing: float = 1.2,
+               gap_over_dhat: float | None = None, jitter_over_dhat: float = 0.05, seed: int = 1,
+               dhat_over_width: float = 1e-3, kappa: float = 1e4) -> Scene:
+    """``n_rods_side``^2 parallel square rods (cells[0] x cells[1] x cells[2] hex
+    cells, 5 tets/cell) along z.  By default they sit at ``spacing`` x width
+    centre distance, as in the rod-twist setup.  With ``gap_over_dhat`` the
+    bundle is packed so that facing rod surfaces are ``gap_over_dhat * dhat``
+    apart: the wound contact state of the twist, where every facing pair of
+    rod sides is inside the barrier.  Alternate rods are shifted along the
+    axis by 0.37 cells so grids are not aligned."""
+    rng = np.random.default_rng(seed)
+    cx, cy, cz = cells
+    length = width * cz / cx
+    dhat = dhat_over_width * width
+    meshes = []
+    pitch = spacing * width if gap_over_dhat is None else width + gap_over_dhat * dhat
+    cell = width / cx
+    for a in range(n_rods_side):
+        for b in range(n_rods_side):
+            m = hex_grid_tets(cx, cy, cz, size=(width, width, length))
+            m.x = m.x + np.array([a * pitch, b * pitch, 0.37 * cell * ((a + b) & 1)])
+            meshes.append(m)
+    sc = assemble(meshes, f"rods_{n_rods_side}x{n_rods_side}_{cx}x{cy}x{cz}", dhat, kappa,
+                  {"width": width, "pitch": pitch})
+    sc.x += rng.uniform(-jitter_over_dhat * dhat, jitter_over_dhat * dhat, size=sc.x.shape)
+    sc.xcs = sc.x.copy()
+    return sc

@@ -1,0 +1,38 @@
+"""The C-ABI library loads without a GPU and exports every symbol that
+include/ipcb.h declares (no compute calls here)."""
+import ctypes
+import os
+import re
+
+from ipc_warp_b200 import _native
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "ipcb.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(ipcb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_header_symbols():
+    lib = ctypes.CDLL(_native.LIB_PATH)
+    syms = header_symbols()
+    assert len(syms) >= 25
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_binding_table_covers_header():
+    assert sorted(_native.SIGNATURES) == header_symbols()
+
+
+def test_sizes_and_args_without_gpu():
+    L = _native.lib()
+    assert L.ipcb_version() == 1
+    assert L.ipcb_lbvh_bytes(1000) > 1000 * 64
+    assert L.ipcb_sort_workspace_u32(10) > 0
+    assert L.ipcb_bsr_workspace(100, 10, 10) > 100 * 8
+    # argument validation happens before any launch
+    assert L.ipcb_sort_pairs_u32(None, None, -1, 8, None, 0, None) == 1
+    assert L.ipcb_contact_hessian(5, None, None, 0, 0, 1.0, None, None, None, None, None) == 1

@@ -1,0 +1,45 @@
+"""BSR assembly against scipy (gpu)."""
+import numpy as np
+import pytest
+import torch
+
+from ipc_warp_b200.bsr import bsr_from_triplets, bsr_mv, scipy_from_triplets
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n_trip,nrow", [(0, 5), (1, 1), (1000, 50), (200_000, 30_000), (70_000, 100_000)])
+@pytest.mark.parametrize("fp64", [False, True])
+def test_bsr_from_triplets(cuda, n_trip, nrow, fp64):
+    rng = np.random.default_rng(n_trip + nrow)
+    dt = np.float64 if fp64 else np.float32
+    rows = rng.integers(0, nrow, size=n_trip).astype(np.int32)
+    cols = np.clip(rows + rng.integers(-3, 4, size=n_trip), 0, nrow - 1).astype(np.int32)
+    vals = rng.normal(size=(n_trip, 3, 3)).astype(dt)
+    if n_trip > 10:
+        vals[::9] = 0.0  # pruned
+    tr = lambda a: torch.tensor(a, device=cuda)
+    A = bsr_from_triplets(nrow, nrow, tr(rows), tr(cols), tr(vals))
+    ref = scipy_from_triplets(nrow, nrow, rows, cols, vals)
+    got = A.to_scipy().tocsr()
+    # pattern: one block per distinct nonzero (row, col)
+    keep = np.any(vals != 0, axis=(1, 2))
+    uniq = np.unique(rows[keep].astype(np.int64) * nrow + cols[keep])
+    assert A.nnz_sync() == len(uniq)
+    offs = A.offsets.cpu().numpy()
+    assert offs[0] == 0 and offs[-1] == len(uniq) and np.all(np.diff(offs) >= 0)
+    colsA = A.columns[: len(uniq)].cpu().numpy()
+    for r in range(min(nrow, 200)):
+        seg = colsA[offs[r]:offs[r + 1]]
+        assert np.all(np.diff(seg) > 0)
+    d = (got - ref)
+    tol = 1e-12 if fp64 else 1e-5
+    assert (abs(d).max() if d.nnz else 0.0) <= tol * max(abs(ref).max() if ref.nnz else 1.0, 1.0)
+    # deterministic: same input, same bits
+    B = bsr_from_triplets(nrow, nrow, tr(rows), tr(cols), tr(vals))
+    assert torch.equal(A.values[: A.nnz_sync()], B.values[: B.nnz_sync()])
+    # SpMV
+    x = rng.normal(size=(nrow, 3)).astype(dt)
+    y = bsr_mv(A, tr(x)).cpu().numpy().ravel()
+    yref = ref @ x.ravel().astype(np.float64)
+    assert np.abs(y - yref).max() <= (1e-10 if fp64 else 1e-4) * max(np.abs(yref).max(), 1.0)
