@@ -252,6 +252,11 @@ def run_ours(args):
         r = step()
     torch.cuda.synchronize()
     pairs = r.n_ee + r.n_pt
+    if args.profile_only:
+        for _ in range(args.steps):
+            step()
+        torch.cuda.synchronize()
+        return
 
     # ---- device-resident timing: K steps, L2 flushed between steps
     def barrier():
@@ -354,6 +359,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--profile-only", action="store_true",
+                    help="warmup + K steps only (for ncu launch lists); prints nothing")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

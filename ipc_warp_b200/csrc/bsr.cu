@@ -1,10 +1,18 @@
 // 3x3-block CSR assembly from triplets (the contract of warp.sparse
 // bsr_from_triplets as used at dynamic_contacts.py:290-297 and
-// time_integrator_base.py:413-426): key = (row, col), device radix sort,
-// segment heads, prefix sum, then one thread per unique block sums its
-// segment in sorted (= input) order, so the result is deterministic.
+// time_integrator_base.py:413-426).
+//
+// Row buckets instead of a global (row, col) key sort:
+//   1. count valid triplets per row (atomics), exclusive scan -> row starts
+//   2. scatter triplet ids into their row bucket
+//   3. one warp per row: rank its entries by (col, triplet id) -- the id
+//      breaks ties, so duplicates are summed in input order and the result is
+//      deterministic -- and count the distinct columns
+//   4. scan the per-row distinct counts -> offsets, nnz
+//   5. one warp per row: write sorted columns and the summed 3x3 blocks
+// Triplets whose block is all zero or whose index is outside the matrix are
+// dropped (warp's prune_numerical_zeros behaviour for the former).
 #include "common.cuh"
-#include "sort.cuh"
 
 namespace ipcb {
 int check_launch(const char* where);
@@ -12,47 +20,37 @@ int check_launch(const char* where);
 namespace {
 
 constexpr int kScanBlock = 1024;
+constexpr int kWarpsPerBlock = 8;
 
-inline int bits_for(int v) {  // bits to represent 0..v
-  int b = 1;
-  while ((1LL << b) <= (long long)v) ++b;
-  return b;
-}
 inline size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// Triplets with an all-zero block or an index outside the matrix get the
-// sentinel key (sorted last, dropped).
 template <class S>
-__global__ void k_keys(int n, const int* __restrict__ rows, const int* __restrict__ cols, const S* __restrict__ vals,
-                       int nrow, int ncol, int colbits, unsigned long long sentinel,
-                       unsigned long long* __restrict__ keys, int* __restrict__ idx) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
+IPCB_D bool valid_triplet(int t, const int* __restrict__ rows, const int* __restrict__ cols,
+                          const S* __restrict__ vals, int nrow, int ncol) {
+  int r = rows[t], c = cols[t];
+  if (r < 0 || r >= nrow || c < 0 || c >= ncol) return false;
   bool nz = false;
 #pragma unroll
   for (int k = 0; k < 9; ++k) nz |= vals[9LL * t + k] != S(0);
-  int r = rows[t], c = cols[t];
-  bool inside = r >= 0 && r < nrow && c >= 0 && c < ncol;
-  keys[t] = (nz && inside) ? (((unsigned long long)r << colbits) | (unsigned long long)c) : sentinel;
-  idx[t] = t;
+  return nz;
 }
 
-// heads[t] = 1 at the first element of each non-sentinel key run
-__global__ void k_heads(int n, const unsigned long long* __restrict__ keys, unsigned long long sentinel,
-                        int* __restrict__ heads) {
+template <class S>
+__global__ void k_row_count(int n, const int* __restrict__ rows, const int* __restrict__ cols,
+                            const S* __restrict__ vals, int nrow, int ncol, int* __restrict__ row_cnt) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  unsigned long long k = keys[t];
-  heads[t] = (k != sentinel && (t == 0 || keys[t - 1] != k)) ? 1 : 0;
+  if (valid_triplet(t, rows, cols, vals, nrow, ncol)) atomicAdd(row_cnt + rows[t], 1);
 }
 
-// block-local exclusive scan; block totals to sums[]
-__global__ void __launch_bounds__(kScanBlock) k_scan_local(int n, int* __restrict__ a, unsigned* __restrict__ sums) {
+// Exclusive scan, phase 1: per-block scan in place, block totals to sums.
+__global__ void __launch_bounds__(kScanBlock) k_scan_local(int n, int* __restrict__ a, int* __restrict__ sums) {
   __shared__ int s[kScanBlock / 32];
   int t = blockIdx.x * kScanBlock + threadIdx.x;
   int v = t < n ? a[t] : 0;
   int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int x = v;
+#pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     int y = __shfl_up_sync(0xffffffffu, x, o);
     if (lane >= o) x += y;
@@ -61,6 +59,7 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_local(int n, int* __restric
   __syncthreads();
   if (w == 0) {
     int y = s[lane];
+#pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       int z = __shfl_up_sync(0xffffffffu, y, o);
       if (lane >= o) y += z;
@@ -70,67 +69,171 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_local(int n, int* __restric
   __syncthreads();
   int excl = x - v + (w > 0 ? s[w - 1] : 0);
   if (t < n) a[t] = excl;
-  if (threadIdx.x == kScanBlock - 1) sums[blockIdx.x] = (unsigned)(excl + v);
+  if (threadIdx.x == kScanBlock - 1) sums[blockIdx.x] = excl + v;
 }
 
-__global__ void k_scan_add(int n, int* __restrict__ a, const unsigned* __restrict__ sums) {
-  int t = blockIdx.x * kScanBlock + threadIdx.x;
-  if (t < n) a[t] += (int)sums[blockIdx.x];
-}
-
-__global__ void k_segments(int n, const unsigned long long* __restrict__ keys, unsigned long long sentinel,
-                           const int* __restrict__ heads_scanned, int colbits, int* __restrict__ seg_start,
-                           int* __restrict__ seg_row, int* __restrict__ columns, int* __restrict__ nnz) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  unsigned long long k = keys[t];
-  bool head = k != sentinel && (t == 0 || keys[t - 1] != k);
-  int u = heads_scanned[t];
-  if (head) {
-    seg_start[u] = t;
-    seg_row[u] = (int)(k >> colbits);
-    columns[u] = (int)(k & ((1ULL << colbits) - 1ULL));
+// phase 2: exclusive scan of the block totals (one block, looping)
+__global__ void __launch_bounds__(kScanBlock) k_scan_sums(int nb, int* __restrict__ sums, int* __restrict__ total) {
+  __shared__ int s[kScanBlock / 32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nb; base += kScanBlock) {
+    int t = base + threadIdx.x;
+    int v = t < nb ? sums[t] : 0;
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      int y = s[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int z = __shfl_up_sync(0xffffffffu, y, o);
+        if (lane >= o) y += z;
+      }
+      s[lane] = y;
+    }
+    __syncthreads();
+    int excl = x - v + (w > 0 ? s[w - 1] : 0) + carry;
+    if (t < nb) sums[t] = excl;
+    __syncthreads();
+    if (threadIdx.x == kScanBlock - 1) carry = excl + v;
+    __syncthreads();
   }
-  bool last_valid = k != sentinel && (t == n - 1 || keys[t + 1] == sentinel);
-  if (last_valid) *nnz = u + 1;
-  if (t == 0 && k == sentinel) *nnz = 0;
+  if (threadIdx.x == 0 && total) *total = carry;
+}
+
+// phase 3: add the scanned block totals
+__global__ void k_scan_add(int n, int* __restrict__ a, const int* __restrict__ sums) {
+  int t = blockIdx.x * kScanBlock + threadIdx.x;
+  if (t < n) a[t] += sums[blockIdx.x];
+}
+
+// exclusive scan of a[0..n) in place; *total = sum (device)
+void exclusive_scan(int* a, int n, int* sums, int* total, cudaStream_t st) {
+  int nb = div_up(n, kScanBlock);
+  k_scan_local<<<nb, kScanBlock, 0, st>>>(n, a, sums);
+  k_scan_sums<<<1, kScanBlock, 0, st>>>(nb, sums, total);
+  k_scan_add<<<nb, kScanBlock, 0, st>>>(n, a, sums);
 }
 
 template <class S>
-__global__ void k_reduce(int n, const unsigned long long* __restrict__ keys, const int* __restrict__ perm,
-                         const int* __restrict__ seg_start, const int* __restrict__ nnz, const S* __restrict__ vals,
-                         S* __restrict__ values) {
-  int u = blockIdx.x * blockDim.x + threadIdx.x;
-  if (u >= *nnz) return;
-  int t = seg_start[u];
-  unsigned long long k = keys[t];
-  S acc[9];
-#pragma unroll
-  for (int q = 0; q < 9; ++q) acc[q] = S(0);
-  for (; t < n && keys[t] == k; ++t) {
-    const S* v = vals + 9LL * perm[t];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) acc[q] += v[q];
-  }
-#pragma unroll
-  for (int q = 0; q < 9; ++q) values[9LL * u + q] = acc[q];
+__global__ void k_row_scatter(int n, const int* __restrict__ rows, const int* __restrict__ cols,
+                              const S* __restrict__ vals, int nrow, int ncol, const int* __restrict__ row_start,
+                              int* __restrict__ cursor, int* __restrict__ bucket) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  if (!valid_triplet(t, rows, cols, vals, nrow, ncol)) return;
+  int r = rows[t];
+  int pos = row_start[r] + atomicAdd(cursor + r, 1);
+  bucket[pos] = t;
 }
 
-__global__ void k_offsets(int cap, int nrow, const int* __restrict__ seg_row, const int* __restrict__ nnz,
-                          int* __restrict__ offsets) {
-  int u = blockIdx.x * blockDim.x + threadIdx.x;
-  int m = *nnz;
-  if (m == 0) {
-    for (int r = u; r <= nrow; r += gridDim.x * blockDim.x) offsets[r] = 0;
-    return;
+// (col, id) as one 64-bit ordering key
+IPCB_D unsigned long long ckey(const int* __restrict__ cols, int t) {
+  return ((unsigned long long)(unsigned)cols[t] << 32) | (unsigned)t;
+}
+
+constexpr int kRowCap = 256;  // entries a warp ranks from shared memory
+
+// Warp per row: sort the row's bucket by (col, id) by ranking (rank = number
+// of smaller keys; keys are distinct because ids are) and count the distinct
+// columns.  Rows longer than kRowCap rank from global memory.
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_row_sort(int nrow, const int* __restrict__ cols,
+                                                                  const int* __restrict__ row_start,
+                                                                  int* __restrict__ bucket, int* __restrict__ tmp,
+                                                                  int* __restrict__ row_nnz) {
+  __shared__ unsigned long long sk[kWarpsPerBlock][kRowCap];
+  const int wib = threadIdx.x >> 5;
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= nrow) return;
+  int b = row_start[warp], e = row_start[warp + 1], L = e - b;
+  if (L <= kRowCap) {
+    for (int i = lane; i < L; i += 32) sk[wib][i] = ckey(cols, bucket[b + i]);
+    __syncwarp();
+    for (int i = lane; i < L; i += 32) {
+      unsigned long long ki = sk[wib][i];
+      int rank = 0;
+      for (int j = 0; j < L; ++j) rank += sk[wib][j] < ki;
+      tmp[b + rank] = (int)(unsigned)(ki & 0xffffffffULL);
+    }
+  } else {
+    for (int i = lane; i < L; i += 32) {
+      unsigned long long ki = ckey(cols, bucket[b + i]);
+      int rank = 0;
+      for (int j = 0; j < L; ++j) rank += ckey(cols, bucket[b + j]) < ki;
+      tmp[b + rank] = bucket[b + i];
+    }
   }
-  if (u >= m) return;
-  int r = seg_row[u];
-  int rp = u == 0 ? -1 : seg_row[u - 1];
-  for (int rr = rp + 1; rr <= r; ++rr) offsets[rr] = u;
-  if (u == m - 1)
-    for (int rr = r + 1; rr <= nrow; ++rr) offsets[rr] = m;
-  (void)cap;
+  __syncwarp();
+  int distinct = 0;
+  for (int i = lane; i < L; i += 32) {
+    int t = tmp[b + i];
+    bucket[b + i] = t;
+    distinct += (i == 0 || cols[tmp[b + i - 1]] != cols[t]) ? 1 : 0;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) distinct += __shfl_xor_sync(0xffffffffu, distinct, o);
+  if (lane == 0) row_nnz[warp] = distinct;
+}
+
+// Warp per row over the sorted bucket: the first entry of each run of equal
+// columns sums the run in order (deterministic) and writes one block; the
+// run's output slot is the number of run heads before it (ballot prefix).
+template <class S>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_row_emit(int nrow, const int* __restrict__ cols,
+                                                                  const S* __restrict__ vals,
+                                                                  const int* __restrict__ row_start,
+                                                                  const int* __restrict__ bucket,
+                                                                  const int* __restrict__ offsets,
+                                                                  int* __restrict__ columns, S* __restrict__ values) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= nrow) return;
+  int b = row_start[warp], e = row_start[warp + 1], L = e - b;
+  int out = offsets[warp];
+  const unsigned le = 0xffffffffu >> (31 - lane);
+  int carry = 0;
+  for (int base = 0; base < L; base += 32) {
+    int i = base + lane;
+    bool in = i < L;
+    int t = in ? bucket[b + i] : 0;
+    int c = in ? cols[t] : 0;
+    bool head = in && (i == 0 || cols[bucket[b + i - 1]] != c);
+    unsigned m = __ballot_sync(0xffffffffu, head);
+    if (head) {
+      int u = carry + __popc(m & le) - 1;
+      S acc[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) acc[q] = S(0);
+      for (int j = i; j < L; ++j) {
+        int tj = bucket[b + j];
+        if (cols[tj] != c) break;
+        const S* v = vals + 9LL * tj;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) acc[q] += v[q];
+      }
+      columns[out + u] = c;
+#pragma unroll
+      for (int q = 0; q < 9; ++q) values[9LL * (out + u) + q] = acc[q];
+    }
+    carry += __popc(m);
+  }
+}
+
+__global__ void k_finish_offsets(int nrow, int* __restrict__ offsets, const int* __restrict__ total,
+                                 int* __restrict__ nnz) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    offsets[nrow] = *total;
+    *nnz = *total;
+  }
 }
 
 template <class S>
@@ -158,6 +261,32 @@ __global__ void k_bsr_mv(int nrow, const int* __restrict__ off, const int* __res
   }
 }
 
+template <class S>
+int assemble(int nrow, int ncol, int n, const int* rows, const int* cols, const S* vals, int* offsets, int* columns,
+             S* values, int* nnz, void* ws, cudaStream_t st) {
+  size_t R = (size_t)nrow + 1, N = (size_t)n;
+  size_t nbr = (size_t)div_up((int)R, kScanBlock);
+  char* p = (char*)ws;
+  int* row_start = (int*)p; p += al(R * 4);
+  int* cursor = (int*)p; p += al(R * 4);
+  int* sums = (int*)p; p += al((nbr + 1) * 4);
+  int* total = (int*)p; p += 256;
+  int* bucket = (int*)p; p += al(N * 4);
+  int* tmp = (int*)p;
+  cudaMemsetAsync(row_start, 0, R * sizeof(int), st);
+  cudaMemsetAsync(cursor, 0, R * sizeof(int), st);
+  int g = div_up(n, 256);
+  k_row_count<S><<<g, 256, 0, st>>>(n, rows, cols, vals, nrow, ncol, row_start);
+  exclusive_scan(row_start, (int)R, sums, total, st);  // row_start[nrow] = valid count
+  k_row_scatter<S><<<g, 256, 0, st>>>(n, rows, cols, vals, nrow, ncol, row_start, cursor, bucket);
+  int gw = div_up(nrow, kWarpsPerBlock);
+  k_row_sort<<<gw, kWarpsPerBlock * 32, 0, st>>>(nrow, cols, row_start, bucket, tmp, offsets);
+  exclusive_scan(offsets, nrow, sums, total, st);
+  k_finish_offsets<<<1, 32, 0, st>>>(nrow, offsets, total, nnz);
+  k_row_emit<S><<<gw, kWarpsPerBlock * 32, 0, st>>>(nrow, cols, vals, row_start, bucket, offsets, columns, values);
+  return check_launch("ipcb_bsr_from_triplets");
+}
+
 }  // namespace
 }  // namespace ipcb
 
@@ -166,11 +295,10 @@ using namespace ipcb;
 extern "C" {
 
 size_t ipcb_bsr_workspace(int n_trip, int nrow, int ncol) {
-  (void)nrow;
   (void)ncol;
-  size_t n = (size_t)(n_trip > 0 ? n_trip : 1);
-  size_t nb = (n + kScanBlock - 1) / kScanBlock;
-  return al(n * 8) + al(n * 4) * 4 + al(nb * 4) + 256 + sort::workspace_bytes<unsigned long long>((int)n);
+  size_t R = (size_t)(nrow > 0 ? nrow : 0) + 1, N = (size_t)(n_trip > 0 ? n_trip : 1);
+  size_t nbr = (R + kScanBlock - 1) / kScanBlock;
+  return 2 * al(R * 4) + al((nbr + 1) * 4) + 256 + 2 * al(N * 4);
 }
 
 int ipcb_bsr_from_triplets(int nrow, int ncol, int n_trip, const int* rows, const int* cols, const void* vals,
@@ -178,47 +306,18 @@ int ipcb_bsr_from_triplets(int nrow, int ncol, int n_trip, const int* rows, cons
                            ipcb_stream s) {
   if (nrow < 0 || ncol < 0 || n_trip < 0 || !offsets || !nnz) return IPCB_E_ARG;
   cudaStream_t st = (cudaStream_t)s;
-  if (n_trip == 0) {
+  if (n_trip == 0 || nrow == 0) {
     cudaMemsetAsync(offsets, 0, (size_t)(nrow + 1) * sizeof(int), st);
     cudaMemsetAsync(nnz, 0, sizeof(int), st);
     return check_launch("ipcb_bsr_from_triplets");
   }
   if (!rows || !cols || !vals || !columns || !values || !ws || ws_bytes < ipcb_bsr_workspace(n_trip, nrow, ncol))
     return IPCB_E_ARG;
-  int colbits = bits_for(ncol > 0 ? ncol - 1 : 0);
-  int rowbits = bits_for(nrow);
-  if (colbits + rowbits > 62) return IPCB_E_ARG;
-  unsigned long long sentinel = (unsigned long long)nrow << colbits;
-  size_t n = (size_t)n_trip, nb = (n + kScanBlock - 1) / kScanBlock;
-  char* p = (char*)ws;
-  unsigned long long* keys = (unsigned long long*)p; p += al(n * 8);
-  int* perm = (int*)p; p += al(n * 4);
-  int* heads = (int*)p; p += al(n * 4);
-  int* seg_start = (int*)p; p += al(n * 4);
-  int* seg_row = (int*)p; p += al(n * 4);
-  unsigned* sums = (unsigned*)p; p += al(nb * 4);
-  p += 256;
-  void* sws = p;
-  size_t sws_bytes = ws_bytes - (size_t)(p - (char*)ws);
-  int g = div_up(n_trip, 256);
   if (fp64)
-    k_keys<double><<<g, 256, 0, st>>>(n_trip, rows, cols, (const double*)vals, nrow, ncol, colbits, sentinel, keys, perm);
-  else
-    k_keys<float><<<g, 256, 0, st>>>(n_trip, rows, cols, (const float*)vals, nrow, ncol, colbits, sentinel, keys, perm);
-  sort::sort_pairs<unsigned long long>(keys, perm, n_trip, colbits + rowbits, sws, sws_bytes, st);
-  k_heads<<<g, 256, 0, st>>>(n_trip, keys, sentinel, heads);
-  k_scan_local<<<(int)nb, kScanBlock, 0, st>>>(n_trip, heads, sums);
-  if (nb > 1) {
-    sort::k_scan<<<1, 1024, 0, st>>>(sums, (int)nb);
-    k_scan_add<<<(int)nb, kScanBlock, 0, st>>>(n_trip, heads, sums);
-  }
-  k_segments<<<g, 256, 0, st>>>(n_trip, keys, sentinel, heads, colbits, seg_start, seg_row, columns, nnz);
-  if (fp64)
-    k_reduce<double><<<g, 256, 0, st>>>(n_trip, keys, perm, seg_start, nnz, (const double*)vals, (double*)values);
-  else
-    k_reduce<float><<<g, 256, 0, st>>>(n_trip, keys, perm, seg_start, nnz, (const float*)vals, (float*)values);
-  k_offsets<<<g, 256, 0, st>>>(n_trip, nrow, seg_row, nnz, offsets);
-  return check_launch("ipcb_bsr_from_triplets");
+    return assemble<double>(nrow, ncol, n_trip, rows, cols, (const double*)vals, offsets, columns, (double*)values,
+                            nnz, ws, st);
+  return assemble<float>(nrow, ncol, n_trip, rows, cols, (const float*)vals, offsets, columns, (float*)values, nnz,
+                         ws, st);
 }
 
 int ipcb_bsr_mv(int nrow, const int* offsets, const int* columns, const void* values, int fp64, const void* x,
