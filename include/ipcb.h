@@ -143,11 +143,15 @@ int ipcb_contact_energy(int kind, const ipcb_soup* soup, const ipcb_contacts* li
 /* ---- CCD (ccd/ccd.py:360-427 point_triangle_toi / edge_edge_toi) ----
  * Cubic coplanarity TOI in double for every candidate whose swept boxes
  * overlap; toi (scalar[1], caller sets 1) gets the minimum root < 1,
- * rounded toward zero when stored as float. */
+ * rounded toward zero when stored as float.  The workspace stages candidate
+ * pairs (ipcb_toi_workspace(capacity) bytes, int32 count first); pairs that
+ * do not fit are solved during traversal, so any capacity >= 0 is correct. */
+size_t ipcb_toi_workspace(int capacity);
 int ipcb_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* swept_edge_bvh, const float* lower,
-                       const float* upper, int exclude_same_body, void* toi, int* status, ipcb_stream s);
+                       const float* upper, int exclude_same_body, void* toi, int* status, void* ws, size_t ws_bytes,
+                       ipcb_stream s);
 int ipcb_point_triangle_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* swept_tri_bvh, double pad,
-                            int exclude_same_body, void* toi, int* status, ipcb_stream s);
+                            int exclude_same_body, void* toi, int* status, void* ws, size_t ws_bytes, ipcb_stream s);
 /* per-pair collision time of n explicit pairs (kind 0 EE, 1 PT); p_t0/p_t1:
  * double[n*12] (4 points each) -> t double[n] (ee/pt_collision_time, ccd.py:304-357) */
 int ipcb_collision_time(int kind, int n, const double* p_t0, const double* p_t1, double* t, int* status,

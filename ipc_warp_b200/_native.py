@@ -56,8 +56,9 @@ SIGNATURES = {
     "ipcb_dcd_pt": (c_int, [SP, P, BP, c_float, c_float, c_int, P, CP, P, P]),
     "ipcb_contact_hessian": (c_int, [c_int, SP, CP, c_int, c_int, c_double, P, P, P, P, P]),
     "ipcb_contact_energy": (c_int, [c_int, SP, CP, c_int, c_double, P, P]),
-    "ipcb_edge_edge_toi": (c_int, [SP, P, BP, P, P, c_int, P, P, P]),
-    "ipcb_point_triangle_toi": (c_int, [SP, P, BP, c_double, c_int, P, P, P]),
+    "ipcb_toi_workspace": (c_size_t, [c_int]),
+    "ipcb_edge_edge_toi": (c_int, [SP, P, BP, P, P, c_int, P, P, P, c_size_t, P]),
+    "ipcb_point_triangle_toi": (c_int, [SP, P, BP, c_double, c_int, P, P, P, c_size_t, P]),
     "ipcb_collision_time": (c_int, [c_int, c_int, P, P, P, P, P]),
     "ipcb_cubic_roots": (c_int, [c_int, P, c_double, c_double, P, P, P, P]),
     "ipcb_bsr_workspace": (c_size_t, [c_int, c_int, c_int]),

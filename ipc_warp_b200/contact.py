@@ -151,6 +151,9 @@ class ContactSolverBase:
         self.n_contacts = 0
         self.n_contacts_pt = 0
         self._status = torch.zeros(1, dtype=torch.int32, device=dev)
+        # CCD candidate staging (pairs beyond capacity are still solved, inline)
+        cap = max(1 << 20, 4 * max(n_edges, n_nodes))
+        self._toi_ws = torch.empty(N.size("ipcb_toi_workspace", cap), dtype=torch.uint8, device=dev)
         self._counts_host = torch.zeros(2, dtype=torch.int32).pin_memory() if dev.type == "cuda" else None
 
     # --------------------------------------------------------------- hooks
@@ -260,14 +263,14 @@ class ContactSolverBase:
         self._status.zero_()
         N.call("ipcb_edge_edge_toi", ctypes.byref(soup), N.ptr(self.ccd_x1), ctypes.byref(self.ccd_edge_bvh.c),
                N.ptr(self.ccd_edge_lower), N.ptr(self.ccd_edge_upper), int(self.disable_self_collision),
-               N.ptr(self.ccd_toi), N.ptr(self._status), s)
+               N.ptr(self.ccd_toi), N.ptr(self._status), N.ptr(self._toi_ws), self._toi_ws.numel(), s)
         if self.has_triangles:
             N.call("ipcb_swept_triangle_aabbs", ctypes.byref(soup), N.ptr(self.ccd_x1), pad,
                    N.ptr(self.ccd_triangle_lower), N.ptr(self.ccd_triangle_upper), s)
             self.ccd_triangle_bvh.rebuild()
             N.call("ipcb_point_triangle_toi", ctypes.byref(soup), N.ptr(self.ccd_x1),
                    ctypes.byref(self.ccd_triangle_bvh.c), pad, int(self.disable_self_collision),
-                   N.ptr(self.ccd_toi), N.ptr(self._status), s)
+                   N.ptr(self.ccd_toi), N.ptr(self._status), N.ptr(self._toi_ws), self._toi_ws.numel(), s)
         toi = float(self.ccd_toi.item())
         return 0.9 * toi if toi < 1.0 else 1.0
 

@@ -5,21 +5,22 @@
 // Row buckets instead of a global (row, col) key sort:
 //   1. count valid triplets per row (atomics), exclusive scan -> row starts
 //   2. scatter triplet ids into their row bucket
-//   3. one warp per row: rank its entries by (col, triplet id) -- the id
-//      breaks ties, so duplicates are summed in input order and the result is
-//      deterministic -- and count the distinct columns
+//   3. one warp per row: bitonic-sort its entries by (col, triplet id) in
+//      shared memory -- the id breaks ties, so the order, and with it every
+//      sum, is fixed by the input -- and count the distinct columns
 //   4. scan the per-row distinct counts -> offsets, nnz
-//   5. one warp per row: write sorted columns and the summed 3x3 blocks
+//   5. one warp per row: segmented reduction over the sorted entries, one
+//      3x3 block per distinct column
 // Triplets whose block is all zero or whose index is outside the matrix are
 // dropped (warp's prune_numerical_zeros behaviour for the former).
 #include "common.cuh"
+#include "scan.cuh"
 
 namespace ipcb {
 int check_launch(const char* where);
 
 namespace {
 
-constexpr int kScanBlock = 1024;
 constexpr int kWarpsPerBlock = 8;
 
 inline size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -43,86 +44,6 @@ __global__ void k_row_count(int n, const int* __restrict__ rows, const int* __re
   if (valid_triplet(t, rows, cols, vals, nrow, ncol)) atomicAdd(row_cnt + rows[t], 1);
 }
 
-// Exclusive scan, phase 1: per-block scan in place, block totals to sums.
-__global__ void __launch_bounds__(kScanBlock) k_scan_local(int n, int* __restrict__ a, int* __restrict__ sums) {
-  __shared__ int s[kScanBlock / 32];
-  int t = blockIdx.x * kScanBlock + threadIdx.x;
-  int v = t < n ? a[t] : 0;
-  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) s[w] = x;
-  __syncthreads();
-  if (w == 0) {
-    int y = s[lane];
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int z = __shfl_up_sync(0xffffffffu, y, o);
-      if (lane >= o) y += z;
-    }
-    s[lane] = y;
-  }
-  __syncthreads();
-  int excl = x - v + (w > 0 ? s[w - 1] : 0);
-  if (t < n) a[t] = excl;
-  if (threadIdx.x == kScanBlock - 1) sums[blockIdx.x] = excl + v;
-}
-
-// phase 2: exclusive scan of the block totals (one block, looping)
-__global__ void __launch_bounds__(kScanBlock) k_scan_sums(int nb, int* __restrict__ sums, int* __restrict__ total) {
-  __shared__ int s[kScanBlock / 32];
-  __shared__ int carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
-  for (int base = 0; base < nb; base += kScanBlock) {
-    int t = base + threadIdx.x;
-    int v = t < nb ? sums[t] : 0;
-    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    if (lane == 31) s[w] = x;
-    __syncthreads();
-    if (w == 0) {
-      int y = s[lane];
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        int z = __shfl_up_sync(0xffffffffu, y, o);
-        if (lane >= o) y += z;
-      }
-      s[lane] = y;
-    }
-    __syncthreads();
-    int excl = x - v + (w > 0 ? s[w - 1] : 0) + carry;
-    if (t < nb) sums[t] = excl;
-    __syncthreads();
-    if (threadIdx.x == kScanBlock - 1) carry = excl + v;
-    __syncthreads();
-  }
-  if (threadIdx.x == 0 && total) *total = carry;
-}
-
-// phase 3: add the scanned block totals
-__global__ void k_scan_add(int n, int* __restrict__ a, const int* __restrict__ sums) {
-  int t = blockIdx.x * kScanBlock + threadIdx.x;
-  if (t < n) a[t] += sums[blockIdx.x];
-}
-
-// exclusive scan of a[0..n) in place; *total = sum (device)
-void exclusive_scan(int* a, int n, int* sums, int* total, cudaStream_t st) {
-  int nb = div_up(n, kScanBlock);
-  k_scan_local<<<nb, kScanBlock, 0, st>>>(n, a, sums);
-  k_scan_sums<<<1, kScanBlock, 0, st>>>(nb, sums, total);
-  k_scan_add<<<nb, kScanBlock, 0, st>>>(n, a, sums);
-}
-
 template <class S>
 __global__ void k_row_scatter(int n, const int* __restrict__ rows, const int* __restrict__ cols,
                               const S* __restrict__ vals, int nrow, int ncol, const int* __restrict__ row_start,
@@ -140,30 +61,45 @@ IPCB_D unsigned long long ckey(const int* __restrict__ cols, int t) {
   return ((unsigned long long)(unsigned)cols[t] << 32) | (unsigned)t;
 }
 
-constexpr int kRowCap = 256;  // entries a warp ranks from shared memory
+constexpr int kRowCap = 1024;      // entries a warp sorts in shared memory
+constexpr int kSortWarps = 4;      // warps (rows) per block in k_row_sort
 
-// Warp per row: sort the row's bucket by (col, id) by ranking (rank = number
-// of smaller keys; keys are distinct because ids are) and count the distinct
-// columns.  Rows longer than kRowCap rank from global memory.
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_row_sort(int nrow, const int* __restrict__ cols,
-                                                                  const int* __restrict__ row_start,
-                                                                  int* __restrict__ bucket, int* __restrict__ tmp,
-                                                                  int* __restrict__ row_nnz) {
-  __shared__ unsigned long long sk[kWarpsPerBlock][kRowCap];
+// Warp per row: sort the row's bucket by (col, id), keys distinct, then count
+// distinct columns.  Rows up to kRowCap entries use a bitonic network in
+// shared memory; longer rows rank each entry against the row in global memory.
+__global__ void __launch_bounds__(kSortWarps * 32) k_row_sort(int nrow, const int* __restrict__ cols,
+                                                              const int* __restrict__ row_start,
+                                                              int* __restrict__ bucket, int* __restrict__ tmp,
+                                                              int* __restrict__ row_nnz) {
+  __shared__ unsigned long long sk[kSortWarps][kRowCap];
   const int wib = threadIdx.x >> 5;
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (warp >= nrow) return;
   int b = row_start[warp], e = row_start[warp + 1], L = e - b;
   if (L <= kRowCap) {
-    for (int i = lane; i < L; i += 32) sk[wib][i] = ckey(cols, bucket[b + i]);
+    int P = 1;
+    while (P < L) P <<= 1;
+    unsigned long long* k = sk[wib];
+    for (int i = lane; i < P; i += 32) k[i] = i < L ? ckey(cols, bucket[b + i]) : ~0ULL;
     __syncwarp();
-    for (int i = lane; i < L; i += 32) {
-      unsigned long long ki = sk[wib][i];
-      int rank = 0;
-      for (int j = 0; j < L; ++j) rank += sk[wib][j] < ki;
-      tmp[b + rank] = (int)(unsigned)(ki & 0xffffffffULL);
+    for (int sz = 2; sz <= P; sz <<= 1) {
+      for (int st = sz >> 1; st > 0; st >>= 1) {
+        for (int i = lane; i < P; i += 32) {
+          int l = i ^ st;
+          if (l > i) {
+            unsigned long long a = k[i], c = k[l];
+            bool up = (i & sz) == 0;
+            if ((a > c) == up) {
+              k[i] = c;
+              k[l] = a;
+            }
+          }
+        }
+        __syncwarp();
+      }
     }
+    for (int i = lane; i < L; i += 32) tmp[b + i] = (int)(unsigned)(k[i] & 0xffffffffULL);
   } else {
     for (int i = lane; i < L; i += 32) {
       unsigned long long ki = ckey(cols, bucket[b + i]);
@@ -184,9 +120,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_row_sort(int nrow, cons
   if (lane == 0) row_nnz[warp] = distinct;
 }
 
-// Warp per row over the sorted bucket: the first entry of each run of equal
-// columns sums the run in order (deterministic) and writes one block; the
-// run's output slot is the number of run heads before it (ballot prefix).
+// Warp per row over the sorted bucket, 32 entries at a time: a segmented
+// inclusive scan (segments = runs of equal column) of the 9 block values;
+// the last entry of each run writes the block.  A run that crosses a chunk
+// boundary is carried into the next chunk.  The combination order is fixed
+// by the sorted order, so results are deterministic.
 template <class S>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_row_emit(int nrow, const int* __restrict__ cols,
                                                                   const S* __restrict__ vals,
@@ -200,31 +138,51 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_row_emit(int nrow, cons
   int b = row_start[warp], e = row_start[warp + 1], L = e - b;
   int out = offsets[warp];
   const unsigned le = 0xffffffffu >> (31 - lane);
-  int carry = 0;
+  int runs_before = 0;  // heads in earlier chunks
+  int prev_col = -1;    // column of the last entry of the previous chunk
+  S carry[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) carry[q] = S(0);
   for (int base = 0; base < L; base += 32) {
     int i = base + lane;
     bool in = i < L;
     int t = in ? bucket[b + i] : 0;
-    int c = in ? cols[t] : 0;
-    bool head = in && (i == 0 || cols[bucket[b + i - 1]] != c);
-    unsigned m = __ballot_sync(0xffffffffu, head);
-    if (head) {
-      int u = carry + __popc(m & le) - 1;
-      S acc[9];
+    int c = in ? cols[t] : -1;
+    int cprev = __shfl_up_sync(0xffffffffu, c, 1);
+    if (lane == 0) cprev = prev_col;
+    bool head = in && (i == 0 || c != cprev);
+    int cnext = __shfl_down_sync(0xffffffffu, c, 1);
+    if (lane == 31) cnext = (i + 1 < L) ? cols[bucket[b + i + 1]] : -2;
+    bool tail = in && (i == L - 1 || cnext != c);
+    S v[9];
 #pragma unroll
-      for (int q = 0; q < 9; ++q) acc[q] = S(0);
-      for (int j = i; j < L; ++j) {
-        int tj = bucket[b + j];
-        if (cols[tj] != c) break;
-        const S* v = vals + 9LL * tj;
+    for (int q = 0; q < 9; ++q) v[q] = in ? vals[9LL * t + q] : S(0);
+    if (lane == 0 && in && !head) {
 #pragma unroll
-        for (int q = 0; q < 9; ++q) acc[q] += v[q];
+      for (int q = 0; q < 9; ++q) v[q] = carry[q] + v[q];
+    }
+    int f = head ? 1 : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int nf = __shfl_up_sync(0xffffffffu, f, o);
+#pragma unroll
+      for (int q = 0; q < 9; ++q) {
+        S nv = __shfl_up_sync(0xffffffffu, v[q], o);
+        if (lane >= o && !f) v[q] = nv + v[q];
       }
+      if (lane >= o) f |= nf;
+    }
+    unsigned hm = __ballot_sync(0xffffffffu, head);
+    int u = runs_before + __popc(hm & le) - 1;
+    if (tail) {
       columns[out + u] = c;
 #pragma unroll
-      for (int q = 0; q < 9; ++q) values[9LL * (out + u) + q] = acc[q];
+      for (int q = 0; q < 9; ++q) values[9LL * (out + u) + q] = v[q];
     }
-    carry += __popc(m);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) carry[q] = __shfl_sync(0xffffffffu, v[q], 31);
+    prev_col = __shfl_sync(0xffffffffu, c, 31);
+    runs_before += __popc(hm);
   }
 }
 
@@ -265,23 +223,22 @@ template <class S>
 int assemble(int nrow, int ncol, int n, const int* rows, const int* cols, const S* vals, int* offsets, int* columns,
              S* values, int* nnz, void* ws, cudaStream_t st) {
   size_t R = (size_t)nrow + 1, N = (size_t)n;
-  size_t nbr = (size_t)div_up((int)R, kScanBlock);
   char* p = (char*)ws;
   int* row_start = (int*)p; p += al(R * 4);
   int* cursor = (int*)p; p += al(R * 4);
-  int* sums = (int*)p; p += al((nbr + 1) * 4);
   int* total = (int*)p; p += 256;
   int* bucket = (int*)p; p += al(N * 4);
-  int* tmp = (int*)p;
+  int* tmp = (int*)p; p += al(N * 4);
+  void* scratch = p;
   cudaMemsetAsync(row_start, 0, R * sizeof(int), st);
   cudaMemsetAsync(cursor, 0, R * sizeof(int), st);
   int g = div_up(n, 256);
   k_row_count<S><<<g, 256, 0, st>>>(n, rows, cols, vals, nrow, ncol, row_start);
-  exclusive_scan(row_start, (int)R, sums, total, st);  // row_start[nrow] = valid count
+  scan::exclusive<int>(row_start, (int)R, scratch, total, st);  // row_start[nrow] = valid count
   k_row_scatter<S><<<g, 256, 0, st>>>(n, rows, cols, vals, nrow, ncol, row_start, cursor, bucket);
+  k_row_sort<<<div_up(nrow, kSortWarps), kSortWarps * 32, 0, st>>>(nrow, cols, row_start, bucket, tmp, offsets);
+  scan::exclusive<int>(offsets, nrow, scratch, total, st);
   int gw = div_up(nrow, kWarpsPerBlock);
-  k_row_sort<<<gw, kWarpsPerBlock * 32, 0, st>>>(nrow, cols, row_start, bucket, tmp, offsets);
-  exclusive_scan(offsets, nrow, sums, total, st);
   k_finish_offsets<<<1, 32, 0, st>>>(nrow, offsets, total, nnz);
   k_row_emit<S><<<gw, kWarpsPerBlock * 32, 0, st>>>(nrow, cols, vals, row_start, bucket, offsets, columns, values);
   return check_launch("ipcb_bsr_from_triplets");
@@ -297,8 +254,7 @@ extern "C" {
 size_t ipcb_bsr_workspace(int n_trip, int nrow, int ncol) {
   (void)ncol;
   size_t R = (size_t)(nrow > 0 ? nrow : 0) + 1, N = (size_t)(n_trip > 0 ? n_trip : 1);
-  size_t nbr = (R + kScanBlock - 1) / kScanBlock;
-  return 2 * al(R * 4) + al((nbr + 1) * 4) + 256 + 2 * al(N * 4);
+  return 2 * al(R * 4) + 256 + 2 * al(N * 4) + scan::scratch_bytes((int)R);
 }
 
 int ipcb_bsr_from_triplets(int nrow, int ncol, int n_trip, const int* rows, const int* cols, const void* vals,

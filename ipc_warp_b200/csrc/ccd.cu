@@ -3,8 +3,12 @@
 // in double.  This file is compiled with -fmad=false: every operation rounds
 // on its own, in source order, so the TOI is reproducible bit for bit by a
 // plain IEEE evaluation.
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "lbvh.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace ipcb {
 int check_launch(const char* where);
@@ -305,12 +309,49 @@ __global__ void k_swept(const S* __restrict__ x0, const S* __restrict__ x1, cons
   }
 }
 
+// Candidate pairs are staged in a list so the cubic solves run one pair per
+// thread (balanced) instead of inside divergent traversal loops.  Workspace:
+// [count int32 | pad to 256 B | int2 pairs[capacity]].  A pair that finds
+// the list full is solved in the traversal thread, so the result never
+// depends on the capacity.
+struct CandList {
+  int* count;
+  int2* pairs;
+  int capacity;
+};
+
+IPCB_D bool push_candidate(const CandList& L, int a, int b) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  int base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(L.count, (int)g.size());
+  int slot = g.shfl(base, 0) + (int)g.thread_rank();
+  if (slot < L.capacity) {
+    L.pairs[slot] = make_int2(a, b);
+    return true;
+  }
+  return false;
+}
+
 template <class S>
-__global__ void __launch_bounds__(128) k_ee_toi(const S* __restrict__ x0, const S* __restrict__ x1,
-                                                const int* __restrict__ edges, const int* __restrict__ body,
-                                                const float4* __restrict__ nodes, const int* __restrict__ order, int n,
-                                                const float* __restrict__ lo, const float* __restrict__ hi,
-                                                int exclude, S* toi, int* status) {
+IPCB_D double ee_pair_time(const S* __restrict__ x0, const S* __restrict__ x1, int2 ea, int2 eb, int& st) {
+  d3 p0[4] = {ld(x0, ea.x), ld(x0, ea.y), ld(x0, eb.x), ld(x0, eb.y)};
+  d3 p1[4] = {ld(x1, ea.x), ld(x1, ea.y), ld(x1, eb.x), ld(x1, eb.y)};
+  return collision_time<0>(p0, p1, st);
+}
+
+template <class S>
+IPCB_D double pt_pair_time(const S* __restrict__ x0, const S* __restrict__ x1, int v, int3 t, int& st) {
+  d3 p0[4] = {ld(x0, v), ld(x0, t.x), ld(x0, t.y), ld(x0, t.z)};
+  d3 p1[4] = {ld(x1, v), ld(x1, t.x), ld(x1, t.y), ld(x1, t.z)};
+  return collision_time<1>(p0, p1, st);
+}
+
+template <class S>
+__global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, const S* __restrict__ x1,
+                                                    const int* __restrict__ edges, const int* __restrict__ body,
+                                                    const float4* __restrict__ nodes, const int* __restrict__ order,
+                                                    int n, const float* __restrict__ lo, const float* __restrict__ hi,
+                                                    int exclude, CandList cand, S* toi, int* status) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   int i = __ldg(order + t);
@@ -324,20 +365,20 @@ __global__ void __launch_bounds__(128) k_ee_toi(const S* __restrict__ x0, const 
     int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + j);
     if (ea.x == eb.x || ea.x == eb.y || ea.y == eb.x || ea.y == eb.y) return;
     if (exclude && bi == __ldg(body + eb.x)) return;
-    d3 p0[4] = {ld(x0, ea.x), ld(x0, ea.y), ld(x0, eb.x), ld(x0, eb.y)};
-    d3 p1[4] = {ld(x1, ea.x), ld(x1, ea.y), ld(x1, eb.x), ld(x1, eb.y)};
-    double tt = collision_time<0>(p0, p1, st);
-    if (tt < 1.0) store_toi(toi, tt);
+    if (!push_candidate(cand, i, j)) {
+      double tt = ee_pair_time(x0, x1, ea, eb, st);
+      if (tt < 1.0) store_toi(toi, tt);
+    }
   });
   if (!ok) st |= IPCB_STATUS_STACK;
   if (st) atomicOr(status, st);
 }
 
 template <class S>
-__global__ void __launch_bounds__(128) k_pt_toi(const S* __restrict__ x0, const S* __restrict__ x1,
-                                                const int* __restrict__ tris, const int* __restrict__ body,
-                                                const float4* __restrict__ nodes, int n_tris, int nv, double pad,
-                                                int exclude, S* toi, int* status) {
+__global__ void __launch_bounds__(128) k_pt_collect(const S* __restrict__ x0, const S* __restrict__ x1,
+                                                    const int* __restrict__ tris, const int* __restrict__ body,
+                                                    const float4* __restrict__ nodes, int n_tris, int nv, double pad,
+                                                    int exclude, CandList cand, S* toi, int* status) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
   d3 a = ld(x0, i), b = ld(x1, i);
@@ -348,16 +389,48 @@ __global__ void __launch_bounds__(128) k_pt_toi(const S* __restrict__ x0, const 
   int bi = exclude ? __ldg(body + i) : 0;
   int st = 0;
   bool ok = traverse(nodes, n_tris, qlo, qhi, [&](int j) {
-    int t0 = __ldg(tris + 3 * j), t1 = __ldg(tris + 3 * j + 1), t2 = __ldg(tris + 3 * j + 2);
-    if (i == t0 || i == t1 || i == t2) return;
-    if (exclude && bi == __ldg(body + t0)) return;
-    d3 p0[4] = {a, ld(x0, t0), ld(x0, t1), ld(x0, t2)};
-    d3 p1[4] = {b, ld(x1, t0), ld(x1, t1), ld(x1, t2)};
-    double tt = collision_time<1>(p0, p1, st);
-    if (tt < 1.0) store_toi(toi, tt);
+    int3 tj = make_int3(__ldg(tris + 3 * j), __ldg(tris + 3 * j + 1), __ldg(tris + 3 * j + 2));
+    if (i == tj.x || i == tj.y || i == tj.z) return;
+    if (exclude && bi == __ldg(body + tj.x)) return;
+    if (!push_candidate(cand, i, j)) {
+      double tt = pt_pair_time(x0, x1, i, tj, st);
+      if (tt < 1.0) store_toi(toi, tt);
+    }
   });
   if (!ok) st |= IPCB_STATUS_STACK;
   if (st) atomicOr(status, st);
+}
+
+// one thread per staged candidate; kind 0 EE (edge, edge), 1 PT (vertex, triangle)
+template <class S, int KIND>
+__global__ void __launch_bounds__(128) k_cand_toi(const S* __restrict__ x0, const S* __restrict__ x1,
+                                                  const int* __restrict__ prims, CandList cand, S* toi,
+                                                  int* status) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  int n = min(*cand.count, cand.capacity);
+  if (k >= n) return;
+  int2 pr = cand.pairs[k];
+  int st = 0;
+  double tt;
+  if (KIND == 0) {
+    int2 ea = __ldg(reinterpret_cast<const int2*>(prims) + pr.x);
+    int2 eb = __ldg(reinterpret_cast<const int2*>(prims) + pr.y);
+    tt = ee_pair_time(x0, x1, ea, eb, st);
+  } else {
+    int3 tj = make_int3(__ldg(prims + 3 * pr.y), __ldg(prims + 3 * pr.y + 1), __ldg(prims + 3 * pr.y + 2));
+    tt = pt_pair_time(x0, x1, pr.x, tj, st);
+  }
+  if (tt < 1.0) store_toi(toi, tt);
+  if (st) atomicOr(status, st);
+}
+
+inline CandList cand_list(void* ws, size_t ws_bytes) {
+  CandList c;
+  c.count = (int*)ws;
+  c.pairs = (int2*)((char*)ws + 256);
+  size_t cap = ws_bytes > 256 ? (ws_bytes - 256) / sizeof(int2) : 0;
+  c.capacity = cap > 0x7fffffff ? 0x7fffffff : (int)cap;
+  return c;
 }
 
 __global__ void k_pair_time(int kind, int n, const double* __restrict__ a, const double* __restrict__ b,
@@ -437,37 +510,64 @@ int ipcb_swept_triangle_aabbs(const ipcb_soup* soup, const void* x1, double pad,
   return check_launch("ipcb_swept_triangle_aabbs");
 }
 
+size_t ipcb_toi_workspace(int capacity) { return 256 + (size_t)(capacity > 0 ? capacity : 0) * sizeof(int2); }
+
 int ipcb_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, const float* lower,
-                       const float* upper, int exclude_same_body, void* toi, int* status, ipcb_stream s) {
-  if (!soup || !x1 || !bvh || !lower || !upper || !toi || !status || bvh->n != soup->n_edges) return IPCB_E_ARG;
+                       const float* upper, int exclude_same_body, void* toi, int* status, void* ws, size_t ws_bytes,
+                       ipcb_stream s) {
+  if (!soup || !x1 || !bvh || !lower || !upper || !toi || !status || !ws || ws_bytes < 256 ||
+      bvh->n != soup->n_edges)
+    return IPCB_E_ARG;
   int n = soup->n_edges;
   if (n == 0) return IPCB_OK;
-  dim3 g(div_up(n, 128));
-  if (soup->fp64)
-    k_ee_toi<double><<<g, 128, 0, (cudaStream_t)s>>>((const double*)soup->x, (const double*)x1, soup->edges,
-                                                     soup->body, (const float4*)bvh->nodes, bvh->sorted, n, lower,
-                                                     upper, exclude_same_body, (double*)toi, status);
-  else
-    k_ee_toi<float><<<g, 128, 0, (cudaStream_t)s>>>((const float*)soup->x, (const float*)x1, soup->edges,
-                                                    soup->body, (const float4*)bvh->nodes, bvh->sorted, n, lower,
-                                                    upper, exclude_same_body, (float*)toi, status);
+  cudaStream_t st = (cudaStream_t)s;
+  CandList c = cand_list(ws, ws_bytes);
+  cudaMemsetAsync(c.count, 0, sizeof(int), st);
+  dim3 g(div_up(n, 128)), gc(div_up(c.capacity > 0 ? c.capacity : 1, 128));
+  if (soup->fp64) {
+    k_ee_collect<double><<<g, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, soup->body,
+                                            (const float4*)bvh->nodes, bvh->sorted, n, lower, upper,
+                                            exclude_same_body, c, (double*)toi, status);
+    if (c.capacity)
+      k_cand_toi<double, 0><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, c,
+                                                (double*)toi, status);
+  } else {
+    k_ee_collect<float><<<g, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, soup->body,
+                                           (const float4*)bvh->nodes, bvh->sorted, n, lower, upper,
+                                           exclude_same_body, c, (float*)toi, status);
+    if (c.capacity)
+      k_cand_toi<float, 0><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, c,
+                                               (float*)toi, status);
+  }
   return check_launch("ipcb_edge_edge_toi");
 }
 
 int ipcb_point_triangle_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, double pad,
-                            int exclude_same_body, void* toi, int* status, ipcb_stream s) {
-  if (!soup || !x1 || !bvh || !toi || !status || bvh->n != soup->n_tris) return IPCB_E_ARG;
+                            int exclude_same_body, void* toi, int* status, void* ws, size_t ws_bytes,
+                            ipcb_stream s) {
+  if (!soup || !x1 || !bvh || !toi || !status || !ws || ws_bytes < 256 || bvh->n != soup->n_tris)
+    return IPCB_E_ARG;
   int nv = soup->n_verts;
   if (nv == 0 || soup->n_tris == 0) return IPCB_OK;
-  dim3 g(div_up(nv, 128));
-  if (soup->fp64)
-    k_pt_toi<double><<<g, 128, 0, (cudaStream_t)s>>>((const double*)soup->x, (const double*)x1, soup->triangles,
-                                                     soup->body, (const float4*)bvh->nodes, soup->n_tris, nv, pad,
-                                                     exclude_same_body, (double*)toi, status);
-  else
-    k_pt_toi<float><<<g, 128, 0, (cudaStream_t)s>>>((const float*)soup->x, (const float*)x1, soup->triangles,
-                                                    soup->body, (const float4*)bvh->nodes, soup->n_tris, nv, pad,
-                                                    exclude_same_body, (float*)toi, status);
+  cudaStream_t st = (cudaStream_t)s;
+  CandList c = cand_list(ws, ws_bytes);
+  cudaMemsetAsync(c.count, 0, sizeof(int), st);
+  dim3 g(div_up(nv, 128)), gc(div_up(c.capacity > 0 ? c.capacity : 1, 128));
+  if (soup->fp64) {
+    k_pt_collect<double><<<g, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, soup->body,
+                                            (const float4*)bvh->nodes, soup->n_tris, nv, pad, exclude_same_body, c,
+                                            (double*)toi, status);
+    if (c.capacity)
+      k_cand_toi<double, 1><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, c,
+                                                (double*)toi, status);
+  } else {
+    k_pt_collect<float><<<g, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, soup->body,
+                                           (const float4*)bvh->nodes, soup->n_tris, nv, pad, exclude_same_body, c,
+                                           (float*)toi, status);
+    if (c.capacity)
+      k_cand_toi<float, 1><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, c,
+                                               (float*)toi, status);
+  }
   return check_launch("ipcb_point_triangle_toi");
 }
 

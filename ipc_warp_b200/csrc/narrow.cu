@@ -98,28 +98,28 @@ struct Feature {
 
 IPCB_D d3 dnorm(d3 a) { return a * (1.0 / sqrt(dot(a, a))); }
 
+// register-resident selection of x[s] for a runtime slot s
+IPCB_D d3 pick(const d3* x, int s) { return s == 0 ? x[0] : (s == 1 ? x[1] : (s == 2 ? x[2] : x[3])); }
+
 IPCB_D void feature_pp(Feature& f, const d3* x, int sa, int sb) {
   f.np = 0;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) f.c[k] = 0.0;
-  f.c[sa] = 1.0;
-  f.c[sb] = -1.0;
-  f.r = x[sa] - x[sb];
+  for (int k = 0; k < 4; ++k) f.c[k] = k == sa ? 1.0 : (k == sb ? -1.0 : 0.0);
+  f.r = pick(x, sa) - pick(x, sb);
 }
 
 IPCB_D void feature_pe(Feature& f, const d3* x, int sp, int s0, int s1) {
   f.np = 1;
-  d3 p = x[sp], e0 = x[s0], e1 = x[s1], e = e1 - e0;
+  d3 p = pick(x, sp), e0 = pick(x, s0), e1 = pick(x, s1), e = e1 - e0;
   double t = dot(p - e0, e) / dot(e, e);
   d3 r = p - e0 - e * t;
   double rl = sqrt(dot(r, r));
 #pragma unroll
-  for (int k = 0; k < 4; ++k) f.c[k] = f.D[0][k] = f.D[1][k] = 0.0;
-  f.c[sp] = 1.0;
-  f.c[s0] = -(1.0 - t);
-  f.c[s1] = -t;
-  f.D[0][s0] = 1.0;
-  f.D[0][s1] = -1.0;
+  for (int k = 0; k < 4; ++k) {
+    f.c[k] = k == sp ? 1.0 : (k == s0 ? -(1.0 - t) : (k == s1 ? -t : 0.0));
+    f.D[0][k] = k == s0 ? 1.0 : (k == s1 ? -1.0 : 0.0);
+    f.D[1][k] = 0.0;
+  }
   f.E[0] = e0 - e1;
   f.rho = rl;
   f.n = r * (1.0 / rl);
@@ -355,40 +355,66 @@ IPCB_D S ee_eps_x(const S* __restrict__ xcs, int4 id) {
   return xmul(xmul(S(1.0e-3), edot(ea, ea)), edot(eb, eb));
 }
 
-template <class S>
-IPCB_D void write_zero(int* rows, int* cols, S* vals, long long base) {
+// 16-byte stores of n (multiple of 16 bytes) values; dst 16-byte aligned
+IPCB_D void store16(float* dst, const float* v, int n) {
 #pragma unroll
-  for (int k = 0; k < 16; ++k) {
-    rows[base + k] = 0;
-    cols[base + k] = 0;
-  }
+  for (int k = 0; k < n; k += 4) *reinterpret_cast<float4*>(dst + k) = make_float4(v[k], v[k + 1], v[k + 2], v[k + 3]);
+}
+IPCB_D void store16(double* dst, const double* v, int n) {
 #pragma unroll
-  for (int k = 0; k < 144; ++k) vals[9 * base + k] = S(0);
+  for (int k = 0; k < n; k += 2) *reinterpret_cast<double2*>(dst + k) = make_double2(v[k], v[k + 1]);
 }
 
+// inactive record: zero blocks at (0, 0) (the reference's zero-initialised
+// triplet arrays)
+template <class S>
+IPCB_D void write_zero(int* rows, int* cols, S* vals, long long base) {
+  int4 z = make_int4(0, 0, 0, 0);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    reinterpret_cast<int4*>(rows + base)[k] = z;
+    reinterpret_cast<int4*>(cols + base)[k] = z;
+  }
+  S zv[72];
+#pragma unroll
+  for (int k = 0; k < 72; ++k) zv[k] = S(0);
+  store16(vals + 9 * base, zv, 72);
+  store16(vals + 9 * base + 72, zv, 72);
+}
+
+// 16 blocks of H = sum_m w_m h_m h_m^T; the record's 144 values are
+// contiguous and 16-byte aligned (576 B per record in float), written as two
+// halves of 8 blocks with vector stores.
 template <class S, class T>
 IPCB_D void write_blocks(const int4 id, int* rows, int* cols, S* vals, long long base, const T (&h)[kMaxH][12],
                          const T (&w)[kMaxH], int nh) {
   const int vid[4] = {id.x, id.y, id.z, id.w};
 #pragma unroll
-  for (int ii = 0; ii < 4; ++ii)
+  for (int ii = 0; ii < 4; ++ii) {
+    reinterpret_cast<int4*>(rows + base)[ii] = make_int4(vid[ii], vid[ii], vid[ii], vid[ii]);
+    reinterpret_cast<int4*>(cols + base)[ii] = make_int4(vid[0], vid[1], vid[2], vid[3]);
+  }
 #pragma unroll
-    for (int jj = 0; jj < 4; ++jj) {
-      long long k = base + ii * 4 + jj;
-      rows[k] = vid[ii];
-      cols[k] = vid[jj];
-      S* out = vals + 9 * k;
+  for (int half = 0; half < 2; ++half) {
+    S buf[72];
 #pragma unroll
-      for (int a = 0; a < 3; ++a)
+    for (int i2 = 0; i2 < 2; ++i2) {
+      const int ii = 2 * half + i2;
 #pragma unroll
-        for (int b = 0; b < 3; ++b) {
-          T v = T(0);
+      for (int jj = 0; jj < 4; ++jj)
 #pragma unroll
-          for (int m = 0; m < kMaxH; ++m)
-            if (m < nh) v += w[m] * h[m][3 * ii + a] * h[m][3 * jj + b];
-          out[3 * a + b] = S(v);
-        }
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) {
+            T v = T(0);
+#pragma unroll
+            for (int m = 0; m < kMaxH; ++m)
+              if (m < nh) v += w[m] * h[m][3 * ii + a] * h[m][3 * jj + b];
+            buf[(i2 * 4 + jj) * 9 + 3 * a + b] = S(v);
+          }
     }
+    store16(vals + 9 * base + 72 * half, buf, 72);
+  }
 }
 
 template <class S>

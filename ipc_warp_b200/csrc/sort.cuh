@@ -1,12 +1,13 @@
 // Stable LSD radix sort of (key, value) pairs, 8-bit digits.
 //
-// One pass = histogram per 2048-key tile -> exclusive scan of the
+// One pass = histogram per 2048-key tile -> device-wide exclusive scan of the
 // digit-major [256][tiles] table -> stable scatter.  Inside a tile, ranks are
 // found 256 keys at a time with __match_any_sync (lanes sharing a digit) and
 // a per-warp shared-memory prefix, so equal digits keep input order.
 // Workspace: alternate key/value buffers and the [256][tiles] table.
 #pragma once
 #include "common.cuh"
+#include "scan.cuh"
 
 namespace ipcb {
 namespace sort {
@@ -22,7 +23,7 @@ inline size_t workspace_bytes(int n) {
   size_t a = ((size_t)n * sizeof(K) + 255) & ~(size_t)255;
   size_t b = ((size_t)n * sizeof(int) + 255) & ~(size_t)255;
   size_t c = ((size_t)256 * tiles(n > 0 ? n : 1) * sizeof(unsigned) + 255) & ~(size_t)255;
-  return a + b + c;
+  return a + b + c + scan::scratch_bytes(256 * tiles(n > 0 ? n : 1));
 }
 
 template <class K>
@@ -39,30 +40,6 @@ __global__ void __launch_bounds__(kThreads) k_hist(const K* __restrict__ keys, i
   }
   __syncthreads();
   table[threadIdx.x * nt + blockIdx.x] = h[threadIdx.x];
-}
-
-// Exclusive scan of m entries in place, one block of 1024 threads.
-static __global__ void __launch_bounds__(1024) k_scan(unsigned* __restrict__ a, int m) {
-  __shared__ unsigned s[1024];
-  int t = threadIdx.x;
-  int chunk = (m + 1023) / 1024;
-  int b = t * chunk, e = min(m, b + chunk);
-  unsigned sum = 0;
-  for (int i = b; i < e; ++i) sum += a[i];
-  s[t] = sum;
-  __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    unsigned v = t >= off ? s[t - off] : 0u;
-    __syncthreads();
-    s[t] += v;
-    __syncthreads();
-  }
-  unsigned run = s[t] - sum;
-  for (int i = b; i < e; ++i) {
-    unsigned v = a[i];
-    a[i] = run;
-    run += v;
-  }
 }
 
 template <class K, class V>
@@ -121,6 +98,8 @@ inline cudaError_t sort_pairs(K* keys, int* vals, int n, int end_bit, void* ws, 
   p += ((size_t)n * sizeof(int) + 255) & ~(size_t)255;
   unsigned* table = (unsigned*)p;
   int nt = tiles(n);
+  p += ((size_t)256 * nt * sizeof(unsigned) + 255) & ~(size_t)255;
+  void* scan_scratch = p;
   K* kin = keys;
   int* vin = vals;
   K* kout = kalt;
@@ -129,7 +108,7 @@ inline cudaError_t sort_pairs(K* keys, int* vals, int n, int end_bit, void* ws, 
   for (int ps = 0; ps < passes; ++ps) {
     int shift = ps * 8;
     k_hist<K><<<nt, kThreads, 0, s>>>(kin, n, shift, nt, table);
-    k_scan<<<1, 1024, 0, s>>>(table, 256 * nt);
+    scan::exclusive<unsigned>(table, 256 * nt, scan_scratch, nullptr, s);
     k_scatter<K, int><<<nt, kThreads, 0, s>>>(kin, vin, kout, vout, n, shift, nt, table);
     K* tk = kin; kin = kout; kout = tk;
     int* tv = vin; vin = vout; vout = tv;
