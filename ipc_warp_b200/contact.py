@@ -130,9 +130,11 @@ class ContactSolverBase:
         self.bvh_edges_upper = torch.zeros((n_edges, 3), **f32)
         self.compute_edge_aabbs()
         self.bvh_edges = Bvh(self.bvh_edges_lower, self.bvh_edges_upper)
+        # CCD boxes are refit into the DCD hierarchies (same primitives, same
+        # topology); detect_collision refits them back before every query.
         self.ccd_edge_lower = torch.zeros((n_edges, 3), **f32)
         self.ccd_edge_upper = torch.zeros((n_edges, 3), **f32)
-        self.ccd_edge_bvh = Bvh(self.ccd_edge_lower, self.ccd_edge_upper)
+        self.ccd_edge_bvh = self.bvh_edges
         self.ccd_toi = torch.ones(1, dtype=dtype, device=dev)
         self.ccd_x1 = torch.zeros_like(soup.x_transformed)
         self.has_triangles = n_tris > 0
@@ -143,7 +145,7 @@ class ContactSolverBase:
             self.tri_mesh = Bvh(self.tri_lower, self.tri_upper)
             self.ccd_triangle_lower = torch.zeros((n_tris, 3), **f32)
             self.ccd_triangle_upper = torch.zeros((n_tris, 3), **f32)
-            self.ccd_triangle_bvh = Bvh(self.ccd_triangle_lower, self.ccd_triangle_upper)
+            self.ccd_triangle_bvh = self.tri_mesh
         self.contacts_new = Contacts(contact_volume, dtype, dev)
         self.contacts_pt = Contacts(contact_volume, dtype, dev)
         self.contacts_list_new = self.contacts_new
@@ -178,12 +180,23 @@ class ContactSolverBase:
                N.ptr(self.tri_lower), N.ptr(self.tri_upper), N.stream_handle())
 
     def update_bvh(self):
-        """contact.py:672-677: edge boxes + refit, float32 mesh copy + refit."""
+        """contact.py:672-677: edge boxes + refit, float32 mesh copy + refit.
+        With ``bvh_rebuild_interval`` = k > 0 the hierarchies are rebuilt
+        (new Morton order) every k-th call instead of refit."""
         self.compute_edge_aabbs()
-        self.bvh_edges.refit()
+        k = getattr(self, "bvh_rebuild_interval", 0)
+        self._bvh_calls = getattr(self, "_bvh_calls", 0) + 1
+        rebuild = k > 0 and self._bvh_calls % k == 0
+        if rebuild:
+            self.bvh_edges.rebuild()
+        else:
+            self.bvh_edges.refit()
         if self.has_triangles:
             self._triangle_aabbs()
-            self.tri_mesh.refit()
+            if rebuild:
+                self.tri_mesh.rebuild()
+            else:
+                self.tri_mesh.refit()
 
     # ----------------------------------------------------------------- DCD
     def _grow_contact_list(self, contacts: Contacts, required: int, point_triangle: bool = False):
@@ -258,7 +271,7 @@ class ContactSolverBase:
         N.call("ipcb_add_dx", ctypes.byref(soup), N.ptr(dx), N.ptr(self.ccd_x1), s)
         N.call("ipcb_swept_edge_aabbs", ctypes.byref(soup), N.ptr(self.ccd_x1), pad, N.ptr(self.ccd_edge_lower),
                N.ptr(self.ccd_edge_upper), s)
-        self.ccd_edge_bvh.rebuild()
+        self.ccd_edge_bvh.refit(self.ccd_edge_lower, self.ccd_edge_upper)
         self.ccd_toi.fill_(1.0)
         self._status.zero_()
         N.call("ipcb_edge_edge_toi", ctypes.byref(soup), N.ptr(self.ccd_x1), ctypes.byref(self.ccd_edge_bvh.c),
@@ -267,7 +280,7 @@ class ContactSolverBase:
         if self.has_triangles:
             N.call("ipcb_swept_triangle_aabbs", ctypes.byref(soup), N.ptr(self.ccd_x1), pad,
                    N.ptr(self.ccd_triangle_lower), N.ptr(self.ccd_triangle_upper), s)
-            self.ccd_triangle_bvh.rebuild()
+            self.ccd_triangle_bvh.refit(self.ccd_triangle_lower, self.ccd_triangle_upper)
             N.call("ipcb_point_triangle_toi", ctypes.byref(soup), N.ptr(self.ccd_x1),
                    ctypes.byref(self.ccd_triangle_bvh.c), pad, int(self.disable_self_collision),
                    N.ptr(self.ccd_toi), N.ptr(self._status), N.ptr(self._toi_ws), self._toi_ws.numel(), s)

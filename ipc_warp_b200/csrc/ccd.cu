@@ -332,10 +332,105 @@ IPCB_D bool push_candidate(const CandList& L, int a, int b) {
   return false;
 }
 
+// ---- exact skip of pairs that cannot reach contact within the step ----
+// The primitives move linearly, so their distance obeys
+//   d(t) >= d(0) - t * (max_a |dx_a - m| + max_b |dx_b - m|)
+// for any common translation m (the vertex-mean here).  A verified root needs
+// the primitives to touch up to the barycentric tolerance of the root check
+// (1e-8 in parameter units), so a pair with d(0) - motion above a margin of
+// 1e-6 (1 + extent) returns 1 from the cubic path; skipping it does not change
+// the TOI.
+IPCB_D double seg_seg_dist(d3 p1, d3 q1, d3 p2, d3 q2) {
+  d3 d1 = q1 - p1, d2 = q2 - p2, r = p1 - p2;
+  double a = dot(d1, d1), e = dot(d2, d2), f = dot(d2, r);
+  double s = 0, t = 0;
+  if (a <= 1e-30 && e <= 1e-30) {
+  } else if (a <= 1e-30) {
+    t = fmin(fmax(f / e, 0.0), 1.0);
+  } else {
+    double c = dot(d1, r);
+    if (e <= 1e-30) {
+      s = fmin(fmax(-c / a, 0.0), 1.0);
+    } else {
+      double b = dot(d1, d2), den = a * e - b * b;
+      s = den > 0 ? fmin(fmax((b * f - c * e) / den, 0.0), 1.0) : 0.0;
+      t = (b * s + f) / e;
+      if (t < 0) {
+        t = 0;
+        s = fmin(fmax(-c / a, 0.0), 1.0);
+      } else if (t > 1) {
+        t = 1;
+        s = fmin(fmax((b - c) / a, 0.0), 1.0);
+      }
+    }
+  }
+  d3 w = (p1 + d1 * s) - (p2 + d2 * t);
+  return sqrt(dot(w, w));
+}
+
+IPCB_D double pt_dist(d3 p, d3 a, d3 b, d3 c) {
+  d3 ab = b - a, ac = c - a, ap = p - a;
+  double d1 = dot(ab, ap), d2 = dot(ac, ap);
+  if (d1 <= 0 && d2 <= 0) return sqrt(dot(ap, ap));
+  d3 bp = p - b;
+  double d3v = dot(ab, bp), d4 = dot(ac, bp);
+  if (d3v >= 0 && d4 <= d3v) return sqrt(dot(bp, bp));
+  double vc = d1 * d4 - d3v * d2;
+  if (vc <= 0 && d1 >= 0 && d3v <= 0) {
+    d3 w = p - (a + ab * (d1 / (d1 - d3v)));
+    return sqrt(dot(w, w));
+  }
+  d3 cp = p - c;
+  double d5 = dot(ab, cp), d6 = dot(ac, cp);
+  if (d6 >= 0 && d5 <= d6) return sqrt(dot(cp, cp));
+  double vb = d5 * d2 - d1 * d6;
+  if (vb <= 0 && d2 >= 0 && d6 <= 0) {
+    d3 w = p - (a + ac * (d2 / (d2 - d6)));
+    return sqrt(dot(w, w));
+  }
+  double va = d3v * d6 - d5 * d4;
+  if (va <= 0 && (d4 - d3v) >= 0 && (d5 - d6) >= 0) {
+    d3 w = p - (b + (c - b) * ((d4 - d3v) / ((d4 - d3v) + (d5 - d6))));
+    return sqrt(dot(w, w));
+  }
+  double den = va + vb + vc;
+  if (!(fabs(den) > 0)) {  // degenerate triangle: distance to its edges
+    return fmin(seg_seg_dist(p, p, a, b), fmin(seg_seg_dist(p, p, a, c), seg_seg_dist(p, p, b, c)));
+  }
+  d3 w = p - (a + ab * (vb / den) + ac * (vc / den));
+  return sqrt(dot(w, w));
+}
+
+// KIND 0: (a0, a1 | b0, b1); KIND 1: (p | t0, t1, t2)
+template <int KIND>
+IPCB_D bool cannot_touch(const d3* p0, const d3* p1) {
+  d3 dx[4];
+  d3 m = mk3(0.0, 0.0, 0.0);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    dx[k] = p1[k] - p0[k];
+    m = m + dx[k];
+  }
+  m = m * 0.25;
+  double ma = 0, mb = 0, ext = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    d3 u = dx[k] - m;
+    double l = sqrt(dot(u, u));
+    if ((KIND == 0 && k < 2) || (KIND == 1 && k < 1)) ma = fmax(ma, l);
+    else mb = fmax(mb, l);
+    ext = fmax(ext, fmax(fabs(p0[k].x), fmax(fabs(p0[k].y), fabs(p0[k].z))));
+    ext = fmax(ext, fmax(fabs(p1[k].x), fmax(fabs(p1[k].y), fabs(p1[k].z))));
+  }
+  double d0 = KIND == 0 ? seg_seg_dist(p0[0], p0[1], p0[2], p0[3]) : pt_dist(p0[0], p0[1], p0[2], p0[3]);
+  return d0 - (ma + mb) > 1e-6 * (1.0 + ext);
+}
+
 template <class S>
 IPCB_D double ee_pair_time(const S* __restrict__ x0, const S* __restrict__ x1, int2 ea, int2 eb, int& st) {
   d3 p0[4] = {ld(x0, ea.x), ld(x0, ea.y), ld(x0, eb.x), ld(x0, eb.y)};
   d3 p1[4] = {ld(x1, ea.x), ld(x1, ea.y), ld(x1, eb.x), ld(x1, eb.y)};
+  if (cannot_touch<0>(p0, p1)) return 1.0;
   return collision_time<0>(p0, p1, st);
 }
 
@@ -343,6 +438,7 @@ template <class S>
 IPCB_D double pt_pair_time(const S* __restrict__ x0, const S* __restrict__ x1, int v, int3 t, int& st) {
   d3 p0[4] = {ld(x0, v), ld(x0, t.x), ld(x0, t.y), ld(x0, t.z)};
   d3 p1[4] = {ld(x1, v), ld(x1, t.x), ld(x1, t.y), ld(x1, t.z)};
+  if (cannot_touch<1>(p0, p1)) return 1.0;
   return collision_time<1>(p0, p1, st);
 }
 

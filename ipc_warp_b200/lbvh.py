@@ -63,9 +63,13 @@ class Bvh:
         N.call("ipcb_lbvh_build", ctypes.byref(self.c), N.ptr(self.lower), N.ptr(self.upper), n,
                N.ptr(self._ws), self._ws.numel(), N.stream_handle(stream))
 
-    def refit(self, stream=None):
-        N.call("ipcb_lbvh_refit", ctypes.byref(self.c), N.ptr(self.lower), N.ptr(self.upper),
-               N.stream_handle(stream))
+    def refit(self, lower: torch.Tensor | None = None, upper: torch.Tensor | None = None, stream=None):
+        """Recompute node boxes keeping the topology; by default from the
+        bound box arrays, or from other (n, 3) boxes of the same primitives."""
+        lo = self.lower if lower is None else lower
+        hi = self.upper if upper is None else upper
+        assert lo.shape[0] == self.c.n and hi.shape[0] == self.c.n
+        N.call("ipcb_lbvh_refit", ctypes.byref(self.c), N.ptr(lo), N.ptr(hi), N.stream_handle(stream))
 
 
 def sort_pairs(keys: torch.Tensor, vals: torch.Tensor, end_bit: int, stream=None) -> None:
