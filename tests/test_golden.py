@@ -1,0 +1,77 @@
+"""The oracle against golden vectors produced by running the reference's own
+functions (tests/golden/make_golden.py).  CPU only."""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import rel_err, sort_records
+from oracle import pyoracle as po
+
+G = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    return np.load(os.path.join(G, name))
+
+
+def test_closest_point_triangle_bit_exact():
+    d = load("closest_point_triangle.npz")
+    P = d["pts"]
+    uvd, ty = po.closest_point_triangle(P[:, 0], P[:, 1], P[:, 2], P[:, 3])
+    assert np.array_equal(ty, d["type"])
+    assert np.array_equal(uvd, d["uvd"])
+
+
+def test_cubic_roots_bit_exact():
+    d = load("cubic_roots.npz")
+    nr, roots, st = po.cubic_roots(d["coef"], 0.0, 1.0)
+    assert st == 0
+    assert np.array_equal(nr, d["n_roots"])
+    for i in range(len(nr)):
+        assert np.array_equal(roots[i, :nr[i]], d["roots"][i, :nr[i]]), i
+
+
+def test_collision_time_bit_exact():
+    d = load("collision_time.npz")
+    assert np.array_equal(po.collision_time("ee", d["p0"], d["p1"]), d["t_ee"])
+    assert np.array_equal(po.collision_time("pt", d["p0"], d["p1"]), d["t_pt"])
+    assert (d["t_ee"] < 1).sum() > 20 and (d["t_pt"] < 1).sum() > 20
+
+
+@pytest.mark.parametrize("exclude", [0, 1])
+def test_dcd_candidates_match_reference(exclude):
+    d = load("dcd_two_cubes_3.npz")
+    ee = po.dcd_ee(d["x"], d["edges"], d["body"], d["thickness"], bool(exclude))
+    pt = po.dcd_pt(d["x"], d["triangles"], d["body"], d["thickness"], bool(exclude))
+    assert len(d[f"ee_{exclude}"]) > 0 and len(d[f"pt_{exclude}"]) > 0
+    assert np.array_equal(sort_records(ee), sort_records(d[f"ee_{exclude}"]))
+    assert np.array_equal(sort_records(pt), sort_records(d[f"pt_{exclude}"]))
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_narrow_phase_matches_reference_composition(mode):
+    """Per-record Hessian blocks, the accumulated force and the energies in
+    the double build (tolerance 1e-10 relative, per record / overall)."""
+    d = load("narrow_fp64.npz")
+    x, xcs, kappa, l0 = d["x"], d["xcs"], float(d["kappa"]), float(d["l0"])
+    force = np.zeros_like(x)
+    off = 0
+    for kind, rec, e_ref in (("ee", d["ee"], d["e_ee"]), ("pt", d["pt"], d["e_pt"])):
+        n = len(rec)
+        F, H, E, act = po.narrow(kind, rec[:, :4], np.full(n, l0), x, xcs, kappa, fp64=True, mode=mode)
+        for p in range(n):
+            blk = d["vals"][(off + p) * 16:(off + p + 1) * 16]
+            Href = np.zeros((12, 12))
+            for ii in range(4):
+                for jj in range(4):
+                    Href[3 * ii:3 * ii + 3, 3 * jj:3 * jj + 3] = blk[ii * 4 + jj]
+            if not act[p]:
+                assert not np.any(Href)
+                continue
+            assert rel_err(H[p], Href) < 1e-10, (kind, p)
+            for k in range(4):
+                force[rec[p, k]] += F[p, 3 * k:3 * k + 3]
+        assert abs(E.sum() - e_ref) <= 1e-10 * abs(e_ref)
+        off += n
+    assert rel_err(force, d["force"]) < 1e-10
