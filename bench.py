@@ -67,11 +67,12 @@ class ClockSampler:
         self.path = None
 
     def start(self):
+        """Sample every 50 ms from before the warm-up to after the e2e loop."""
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
@@ -129,6 +130,9 @@ def peaks():
 # algorithmic bytes per pair of the narrow-phase kernel (float32 records):
 # record 24 + positions 48 + 16 triplets (4+4+36) 704 + force 48; EE adds rest positions 48
 NARROW_BYTES = {"pt": 824, "ee": 872}
+# dram__bytes_read.sum + dram__bytes_write.sum of the EE + PT narrow-phase launches
+# of one step on this workload (ncu, profiles/k_contact_hessian_rod_bundle.md)
+NARROW_DRAM_BYTES_PER_STEP = 447.4e6
 
 
 def stage_times(pipe, dx, reps, torch):
@@ -248,6 +252,9 @@ def run_ours(args):
     def step():
         return pipe.iteration(dx)
 
+    sampler = ClockSampler(local)
+    if not args.profile_only:
+        sampler.start()
     for _ in range(max(args.warmup, 3)):
         r = step()
     torch.cuda.synchronize()
@@ -264,8 +271,6 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    sampler = ClockSampler(local)
-    sampler.start()
     barrier()
     evs = []
     for _ in range(args.steps):
@@ -276,7 +281,6 @@ def run_ours(args):
         e.record()
         evs.append((s, e))
     barrier()
-    clocks = sampler.stop()
     total_ms = sum(s.elapsed_time(e) for s, e in evs)
 
     # ---- end to end: pinned host inputs copied in, results read back
@@ -297,6 +301,7 @@ def run_ours(args):
         e.record()
         e2e_ev.append((s, e))
     barrier()
+    clocks = sampler.stop()
     e2e_ms = sum(s.elapsed_time(e) for s, e in e2e_ev)
     h2d = xh.numel() * 4 + dxh.numel() * 4
     d2h = bh.numel() * 4 + 8 + 4 + 8  # force, energy, toi, counts
@@ -316,10 +321,7 @@ def run_ours(args):
         narrow_ms = st["narrow_ee"] + st["narrow_pt"]
         algo = n_ee * NARROW_BYTES["ee"] + n_pt * NARROW_BYTES["pt"]
         achieved = algo / (narrow_ms * 1e-3) / 1e9
-        traffic = None
-        tp = os.path.join(ROOT, "profiles", "narrow_traffic.json")
-        if os.path.exists(tp):
-            traffic = json.load(open(tp)).get("bytes_per_launch")
+        traffic = NARROW_DRAM_BYTES_PER_STEP
         cpu_pairs, cpu_sec = cpu_pipeline(sc, dx_np, 3)
         ms = total_ms / args.steps
         out = {
@@ -356,7 +358,7 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--profile-only", action="store_true",
