@@ -100,6 +100,22 @@ int ipcb_lbvh_build(ipcb_lbvh* bvh, const float* lower, const float* upper, int 
 /* Recompute node boxes for new leaf boxes, same topology (atomic bottom-up). */
 int ipcb_lbvh_refit(const ipcb_lbvh* bvh, const float* lower, const float* upper, ipcb_stream s);
 
+/* LBVH build that allocates nothing.  No counterpart in the reference: it
+ * serves callers that cannot call cudaMalloc while a step runs (an allocation
+ * may synchronise the device; a host framework may own all device memory in
+ * its own pool; a JNI/FFI binding may only pass buffers it already holds).
+ * Same result as ipcb_lbvh_build; the build scratch is a file-scope
+ * __device__ array of ipcb_lbvh_build_noalloc_scratch_bytes() (about 2.2 MB)
+ * that every GPU loading the library keeps until exit, so n is limited to
+ * IPCB_LBVH_NOALLOC_MAX_PRIMS (larger n returns IPCB_E_ARG).  The first call
+ * on a device looks the array's device address up (cudaGetSymbolAddress) with
+ * that device current: make that first call before any stream capture.  All
+ * calls share the one array, so calls that overlap on the GPU race; the build
+ * clears what must start at zero, and the array keeps the last call's data. */
+#define IPCB_LBVH_NOALLOC_MAX_PRIMS (1 << 18)
+size_t ipcb_lbvh_build_noalloc_scratch_bytes(void);
+int ipcb_lbvh_build_noalloc(ipcb_lbvh* bvh, const float* lower, const float* upper, int n, ipcb_stream s);
+
 /* ---- boxes (contact.py:30-52, ccd/ccd.py:166-210) ---- */
 /* x4 = float4(x) (the reference's float32 mesh copy, contact.py:44-47, as 16-byte records) */
 int ipcb_pack_positions(const ipcb_soup* soup, float* x4, ipcb_stream s);

@@ -46,6 +46,8 @@ SIGNATURES = {
     "ipcb_lbvh_build_workspace": (c_size_t, [c_int]),
     "ipcb_lbvh_build": (c_int, [BP, P, P, c_int, P, c_size_t, P]),
     "ipcb_lbvh_refit": (c_int, [BP, P, P, P]),
+    "ipcb_lbvh_build_noalloc_scratch_bytes": (c_size_t, []),
+    "ipcb_lbvh_build_noalloc": (c_int, [BP, P, P, c_int, P]),
     "ipcb_pack_positions": (c_int, [SP, P, P]),
     "ipcb_edge_aabbs": (c_int, [SP, P, c_float, P, P, P]),
     "ipcb_triangle_aabbs": (c_int, [SP, P, c_float, P, P, P]),
