@@ -36,7 +36,8 @@ enum {
 /* status-word bits written by device code (OR-ed) */
 enum {
   IPCB_STATUS_STACK = 1,    /* BVH traversal stack full: result incomplete */
-  IPCB_STATUS_ROOT_ITERS = 2 /* cubic root refinement hit its iteration bound */
+  IPCB_STATUS_ROOT_ITERS = 2, /* cubic root refinement hit its iteration bound */
+  IPCB_STATUS_ROW_OVERFLOW = 4 /* contact BSR: a row has more distinct columns than one warp handles */
 };
 
 /* Geometry: the reference Soup (fem/geometry.py:165-171) plus positions. */
@@ -184,6 +185,17 @@ size_t ipcb_bsr_workspace(int n_trip, int nrow, int ncol);
 int ipcb_bsr_from_triplets(int nrow, int ncol, int n_trip, const int* rows, const int* cols, const void* vals,
                            int fp64, int* offsets, int* columns, void* values, int* nnz, void* ws, size_t ws_bytes,
                            ipcb_stream s);
+/* The same BSR for the contact Hessian, assembled from the EE and PT lists
+ * and their triplet values (16 blocks per record, EE records first, as
+ * ipcb_contact_hessian writes them) instead of from generic triplets: the
+ * records' structure (one row and 4 columns per (record, slot)) replaces the
+ * per-triplet bucketing.  Deterministic.  If a row has more than 128 distinct
+ * columns, *status gets IPCB_STATUS_ROW_OVERFLOW and the caller must use
+ * ipcb_bsr_from_triplets instead. */
+size_t ipcb_contact_bsr_workspace(int n_records, int n_verts);
+int ipcb_contact_bsr(const ipcb_contacts* ee, int n_ee, const ipcb_contacts* pt, int n_pt, int n_verts,
+                     const void* vals, int fp64, int* offsets, int* columns, void* values, int* nnz, int* status,
+                     void* ws, size_t ws_bytes, ipcb_stream s);
 /* y = alpha*A*x + beta*y for a 3x3 BSR (bsr_mv) */
 int ipcb_bsr_mv(int nrow, const int* offsets, const int* columns, const void* values, int fp64, const void* x,
                 void* y, double alpha, double beta, ipcb_stream s);

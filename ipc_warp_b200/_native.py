@@ -66,6 +66,8 @@ SIGNATURES = {
     "ipcb_bsr_workspace": (c_size_t, [c_int, c_int, c_int]),
     "ipcb_bsr_from_triplets": (c_int, [c_int, c_int, c_int, P, P, P, c_int, P, P, P, P, P, c_size_t, P]),
     "ipcb_bsr_mv": (c_int, [c_int, P, P, P, c_int, P, P, c_double, c_double, P]),
+    "ipcb_contact_bsr_workspace": (c_size_t, [c_int, c_int]),
+    "ipcb_contact_bsr": (c_int, [CP, c_int, CP, c_int, c_int, P, c_int, P, P, P, P, P, P, c_size_t, P]),
 }
 
 

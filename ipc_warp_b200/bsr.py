@@ -74,6 +74,26 @@ def bsr_from_triplets(nrow: int, ncol: int, rows: torch.Tensor, cols: torch.Tens
     return out
 
 
+def contact_bsr(ee, n_ee: int, pt, n_pt: int, n_verts: int, vals: torch.Tensor,
+                out: BsrMatrix | None = None, status: torch.Tensor | None = None) -> tuple[BsrMatrix, int]:
+    """BSR of the contact Hessian from the EE/PT lists and their triplet
+    values (16 blocks per record, EE first).  Returns (matrix, status);
+    status has IPCB_STATUS_ROW_OVERFLOW (4) set when a row had too many
+    distinct columns for the fast path (the matrix is then incomplete)."""
+    dtype, dev = vals.dtype, vals.device
+    cap = max(16 * (n_ee + n_pt), 1)
+    if out is None or out.columns.shape[0] < cap or out.nrow != n_verts or out.dtype != dtype:
+        out = BsrMatrix(n_verts, n_verts, cap, dtype, dev)
+    st = torch.zeros(1, dtype=torch.int32, device=dev) if status is None else status.zero_()
+    ws = torch.empty(N.size("ipcb_contact_bsr_workspace", n_ee + n_pt, n_verts), dtype=torch.uint8, device=dev)
+    import ctypes
+
+    N.call("ipcb_contact_bsr", ctypes.byref(ee.c_struct()), n_ee, ctypes.byref(pt.c_struct()), n_pt, n_verts,
+           N.ptr(vals), int(dtype == torch.float64), N.ptr(out.offsets), N.ptr(out.columns), N.ptr(out.values),
+           N.ptr(out.nnz_dev), N.ptr(st), N.ptr(ws), ws.numel(), N.stream_handle())
+    return out, int(st.item())
+
+
 def bsr_axpy(x: BsrMatrix, y: BsrMatrix, alpha: float = 1.0, beta: float = 1.0) -> BsrMatrix:
     """y = alpha * x + beta * y on the union pattern (returns the new y)."""
     tx, ty = x.triplets(), y.triplets()

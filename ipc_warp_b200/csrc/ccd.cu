@@ -320,17 +320,6 @@ struct CandList {
   int capacity;
 };
 
-IPCB_D bool push_candidate(const CandList& L, int a, int b) {
-  cg::coalesced_group g = cg::coalesced_threads();
-  int base = 0;
-  if (g.thread_rank() == 0) base = atomicAdd(L.count, (int)g.size());
-  int slot = g.shfl(base, 0) + (int)g.thread_rank();
-  if (slot < L.capacity) {
-    L.pairs[slot] = make_int2(a, b);
-    return true;
-  }
-  return false;
-}
 
 // ---- exact skip of pairs that cannot reach contact within the step ----
 // The primitives move linearly, so their distance obeys
@@ -442,6 +431,32 @@ IPCB_D double pt_pair_time(const S* __restrict__ x0, const S* __restrict__ x1, i
   return collision_time<1>(p0, p1, st);
 }
 
+constexpr int kQueue = 32;  // per-thread queue of filtered leaf hits
+
+IPCB_D int warp_max(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// converged push: one ballot and one atomicAdd per warp; returns false for a
+// lane whose pair did not fit (the caller solves it in place)
+IPCB_D bool push_converged(const CandList& L, bool has, int a, int b) {
+  const unsigned lane = threadIdx.x & 31;
+  unsigned m = __ballot_sync(0xffffffffu, has);
+  int base = 0;
+  if (lane == 0 && m) base = atomicAdd(L.count, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  int slot = base + __popc(m & ((1u << lane) - 1u));
+  if (has && slot < L.capacity) {
+    L.pairs[slot] = make_int2(a, b);
+    return true;
+  }
+  return !has;
+}
+
+// Traversal applies the cheap filters and queues leaves; the warp then pushes
+// the queued pairs converged (divergent pushes would serialise on the count).
 template <class S>
 __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, const S* __restrict__ x1,
                                                     const int* __restrict__ edges, const int* __restrict__ body,
@@ -449,24 +464,40 @@ __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, co
                                                     int n, const float* __restrict__ lo, const float* __restrict__ hi,
                                                     int exclude, CandList cand, S* toi, int* status) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  int i = __ldg(order + t);
+  bool active = t < n;
+  int i = active ? __ldg(order + t) : 0;
   int2 ea = __ldg(reinterpret_cast<const int2*>(edges) + i);
   int bi = exclude ? __ldg(body + ea.x) : 0;
-  f3 qlo = mk3(__ldg(lo + 3 * i), __ldg(lo + 3 * i + 1), __ldg(lo + 3 * i + 2));
-  f3 qhi = mk3(__ldg(hi + 3 * i), __ldg(hi + 3 * i + 1), __ldg(hi + 3 * i + 2));
   int st = 0;
-  bool ok = traverse(nodes, n, qlo, qhi, [&](int j) {
-    if (!(i < j)) return;
-    int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + j);
-    if (ea.x == eb.x || ea.x == eb.y || ea.y == eb.x || ea.y == eb.y) return;
-    if (exclude && bi == __ldg(body + eb.x)) return;
-    if (!push_candidate(cand, i, j)) {
+  int q[kQueue];
+  int nq = 0;
+  if (active) {
+    f3 qlo = mk3(__ldg(lo + 3 * i), __ldg(lo + 3 * i + 1), __ldg(lo + 3 * i + 2));
+    f3 qhi = mk3(__ldg(hi + 3 * i), __ldg(hi + 3 * i + 1), __ldg(hi + 3 * i + 2));
+    bool ok = traverse(nodes, n, qlo, qhi, [&](int j) {
+      if (!(i < j)) return;
+      int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + j);
+      if (ea.x == eb.x || ea.x == eb.y || ea.y == eb.x || ea.y == eb.y) return;
+      if (exclude && bi == __ldg(body + eb.x)) return;
+      if (nq < kQueue) {
+        q[nq++] = j;
+      } else {
+        double tt = ee_pair_time(x0, x1, ea, eb, st);
+        if (tt < 1.0) store_toi(toi, tt);
+      }
+    });
+    if (!ok) st |= IPCB_STATUS_STACK;
+  }
+  int rounds = warp_max(nq);
+  for (int k = 0; k < rounds; ++k) {
+    bool has = k < nq;
+    int j = has ? q[k] : 0;
+    if (!push_converged(cand, has, i, j)) {
+      int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + j);
       double tt = ee_pair_time(x0, x1, ea, eb, st);
       if (tt < 1.0) store_toi(toi, tt);
     }
-  });
-  if (!ok) st |= IPCB_STATUS_STACK;
+  }
   if (st) atomicOr(status, st);
 }
 
@@ -475,25 +506,42 @@ __global__ void __launch_bounds__(128) k_pt_collect(const S* __restrict__ x0, co
                                                     const int* __restrict__ tris, const int* __restrict__ body,
                                                     const float4* __restrict__ nodes, int n_tris, int nv, double pad,
                                                     int exclude, CandList cand, S* toi, int* status) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nv) return;
+  int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  bool active = i0 < nv;
+  int i = active ? i0 : 0;
   d3 a = ld(x0, i), b = ld(x1, i);
-  f3 qlo = mk3(__double2float_rd(dmin(a.x, b.x) - pad), __double2float_rd(dmin(a.y, b.y) - pad),
-               __double2float_rd(dmin(a.z, b.z) - pad));
-  f3 qhi = mk3(__double2float_ru(dmax(a.x, b.x) + pad), __double2float_ru(dmax(a.y, b.y) + pad),
-               __double2float_ru(dmax(a.z, b.z) + pad));
   int bi = exclude ? __ldg(body + i) : 0;
   int st = 0;
-  bool ok = traverse(nodes, n_tris, qlo, qhi, [&](int j) {
-    int3 tj = make_int3(__ldg(tris + 3 * j), __ldg(tris + 3 * j + 1), __ldg(tris + 3 * j + 2));
-    if (i == tj.x || i == tj.y || i == tj.z) return;
-    if (exclude && bi == __ldg(body + tj.x)) return;
-    if (!push_candidate(cand, i, j)) {
+  int q[kQueue];
+  int nq = 0;
+  if (active) {
+    f3 qlo = mk3(__double2float_rd(dmin(a.x, b.x) - pad), __double2float_rd(dmin(a.y, b.y) - pad),
+                 __double2float_rd(dmin(a.z, b.z) - pad));
+    f3 qhi = mk3(__double2float_ru(dmax(a.x, b.x) + pad), __double2float_ru(dmax(a.y, b.y) + pad),
+                 __double2float_ru(dmax(a.z, b.z) + pad));
+    bool ok = traverse(nodes, n_tris, qlo, qhi, [&](int j) {
+      int3 tj = make_int3(__ldg(tris + 3 * j), __ldg(tris + 3 * j + 1), __ldg(tris + 3 * j + 2));
+      if (i == tj.x || i == tj.y || i == tj.z) return;
+      if (exclude && bi == __ldg(body + tj.x)) return;
+      if (nq < kQueue) {
+        q[nq++] = j;
+      } else {
+        double tt = pt_pair_time(x0, x1, i, tj, st);
+        if (tt < 1.0) store_toi(toi, tt);
+      }
+    });
+    if (!ok) st |= IPCB_STATUS_STACK;
+  }
+  int rounds = warp_max(nq);
+  for (int k = 0; k < rounds; ++k) {
+    bool has = k < nq;
+    int j = has ? q[k] : 0;
+    if (!push_converged(cand, has, i, j)) {
+      int3 tj = make_int3(__ldg(tris + 3 * j), __ldg(tris + 3 * j + 1), __ldg(tris + 3 * j + 2));
       double tt = pt_pair_time(x0, x1, i, tj, st);
       if (tt < 1.0) store_toi(toi, tt);
     }
-  });
-  if (!ok) st |= IPCB_STATUS_STACK;
+  }
   if (st) atomicOr(status, st);
 }
 

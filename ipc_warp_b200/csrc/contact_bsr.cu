@@ -1,0 +1,255 @@
+// BSR assembly of the contact Hessian straight from the contact lists and
+// their 16 triplet blocks per record (the result of
+// bsr_from_triplets(rows, cols, vals) at dynamic_contacts.py:290-296, all-zero
+// blocks dropped).  The generic assembly (bsr.cu) buckets all 16 triplets of
+// a record by row; here the unit is a (record, slot ii) quad: one row
+// (vertex ii of the record) and 4 consecutive blocks (columns = the record's 4
+// vertices).  A row's distinct columns are few (tens), so:
+//   1. key every quad by its row; stable radix sort (order = (row, quad id))
+//   2. pass A, warp per row: insert the columns of non-zero blocks into a
+//      shared-memory hash, sort the distinct columns, count them
+//   3. scan the counts -> offsets
+//   4. pass B, warp per row: lane k owns the row's distinct columns k, k+32,
+//      ...; every lane walks the row's quads in order and the owner of each
+//      block's column adds it, so each sum runs in input order (deterministic)
+// A row with more than kHash distinct columns sets IPCB_STATUS_ROW_OVERFLOW
+// (the host then uses the generic assembly).
+#include "common.cuh"
+#include "scan.cuh"
+#include "sort.cuh"
+
+namespace ipcb {
+int check_launch(const char* where);
+
+namespace {
+
+constexpr int kHash = 128;     // distinct columns per row handled by one warp
+constexpr int kOwn = kHash / 32;
+constexpr int kWarps = 4;
+
+inline size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
+
+IPCB_D int4 record_ids(const int* __restrict__ ee, int n_ee, const int* __restrict__ pt, int p) {
+  return p < n_ee ? __ldg(reinterpret_cast<const int4*>(ee) + p) : __ldg(reinterpret_cast<const int4*>(pt) + (p - n_ee));
+}
+IPCB_D int comp(int4 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
+
+template <class S>
+IPCB_D bool block_nonzero(const S* __restrict__ b) {
+  bool nz = false;
+#pragma unroll
+  for (int q = 0; q < 9; ++q) nz |= b[q] != S(0);
+  return nz;
+}
+
+__global__ void k_quad_keys(int nq, const int* __restrict__ ee, int n_ee, const int* __restrict__ pt,
+                            unsigned* __restrict__ keys, int* __restrict__ ids, int* __restrict__ row_cnt) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nq) return;
+  int4 v = record_ids(ee, n_ee, pt, q >> 2);
+  int row = comp(v, q & 3);
+  keys[q] = (unsigned)row;
+  ids[q] = q;
+  atomicAdd(row_cnt + row, 1);
+}
+
+// insert c into the warp's open-addressing table (keys -1 = empty)
+IPCB_D bool hash_insert(int* tab, int c) {
+  unsigned h = ((unsigned)c * 2654435761u) & (kHash - 1);
+  for (int probe = 0; probe < kHash; ++probe) {
+    int old = atomicCAS(tab + h, -1, c);
+    if (old == -1 || old == c) return true;
+    h = (h + 1) & (kHash - 1);
+  }
+  return false;
+}
+
+template <class S>
+__global__ void __launch_bounds__(kWarps * 32) k_row_columns(int nrow, const int* __restrict__ qstart,
+                                                             const int* __restrict__ qids, const int* __restrict__ ee,
+                                                             int n_ee, const int* __restrict__ pt,
+                                                             const S* __restrict__ vals, int* __restrict__ tmpcols,
+                                                             int* __restrict__ row_nnz, int* __restrict__ status) {
+  __shared__ int tab[kWarps][kHash];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int row = blockIdx.x * kWarps + w;
+  if (row >= nrow) return;
+  int b = qstart[row], e = qstart[row + 1];
+  if (b == e) {
+    if (lane == 0) row_nnz[row] = 0;
+    return;
+  }
+  for (int k = lane; k < kHash; k += 32) tab[w][k] = -1;
+  __syncwarp();
+  bool ok = true;
+  for (int i = b + lane; i < e; i += 32) {
+    int q = qids[i];
+    int4 v = record_ids(ee, n_ee, pt, q >> 2);
+    const S* blk = vals + 36LL * q;  // 4 blocks (ii, jj = 0..3) of 9 values
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj)
+      if (block_nonzero(blk + 9 * jj)) ok &= hash_insert(tab[w], comp(v, jj));
+  }
+  __syncwarp();
+  // compact the occupied slots to the front (stable), pad with INT_MAX, then
+  // bitonic-sort the first P >= cnt entries
+  const unsigned lt = (1u << lane) - 1u;
+  int dest[kOwn], colv[kOwn];
+  int cnt = 0;
+#pragma unroll
+  for (int r = 0; r < kOwn; ++r) {
+    int c = tab[w][r * 32 + lane];
+    unsigned m = __ballot_sync(0xffffffffu, c >= 0);
+    dest[r] = c >= 0 ? cnt + __popc(m & lt) : -1;
+    colv[r] = c;
+    cnt += __popc(m);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int r = 0; r < kOwn; ++r) tab[w][r * 32 + lane] = 0x7fffffff;
+  __syncwarp();
+#pragma unroll
+  for (int r = 0; r < kOwn; ++r)
+    if (dest[r] >= 0) tab[w][dest[r]] = colv[r];
+  __syncwarp();
+  int P = 1;
+  while (P < cnt) P <<= 1;
+  for (int sz = 2; sz <= P; sz <<= 1)
+    for (int st = sz >> 1; st > 0; st >>= 1) {
+      for (int i = lane; i < P; i += 32) {
+        int l = i ^ st;
+        if (l > i) {
+          int a = tab[w][i], c = tab[w][l];
+          bool up = (i & sz) == 0;
+          if ((a > c) == up) {
+            tab[w][i] = c;
+            tab[w][l] = a;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  int base4 = 4 * b;  // the row may use up to 4 columns per quad
+  for (int k = lane; k < cnt; k += 32) tmpcols[base4 + k] = tab[w][k];
+  unsigned bad = __ballot_sync(0xffffffffu, !ok);
+  if (lane == 0) {
+    row_nnz[row] = cnt;
+    if (bad) atomicOr(status, IPCB_STATUS_ROW_OVERFLOW);
+  }
+}
+
+template <class S>
+__global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int* __restrict__ qstart,
+                                                            const int* __restrict__ qids, const int* __restrict__ ee,
+                                                            int n_ee, const int* __restrict__ pt,
+                                                            const S* __restrict__ vals,
+                                                            const int* __restrict__ tmpcols,
+                                                            const int* __restrict__ offsets, int* __restrict__ columns,
+                                                            S* __restrict__ values) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int row = blockIdx.x * kWarps + w;
+  if (row >= nrow) return;
+  int b = qstart[row], e = qstart[row + 1];
+  if (b == e) return;
+  int out = offsets[row], cnt = offsets[row + 1] - out;
+  int own[kOwn];
+  S acc[kOwn][9];
+#pragma unroll
+  for (int r = 0; r < kOwn; ++r) {
+    int k = r * 32 + lane;
+    own[r] = k < cnt ? tmpcols[4 * b + k] : -1;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) acc[r][q] = S(0);
+  }
+  for (int i = b; i < e; ++i) {
+    int q = qids[i];
+    int4 v = record_ids(ee, n_ee, pt, q >> 2);
+    const S* blk = vals + 36LL * q;
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      int c = comp(v, jj);
+#pragma unroll
+      for (int r = 0; r < kOwn; ++r)
+        if (own[r] == c) {
+#pragma unroll
+          for (int t = 0; t < 9; ++t) acc[r][t] += blk[9 * jj + t];
+        }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kOwn; ++r) {
+    int k = r * 32 + lane;
+    if (k < cnt) {
+      columns[out + k] = own[r];
+#pragma unroll
+      for (int t = 0; t < 9; ++t) values[9LL * (out + k) + t] = acc[r][t];
+    }
+  }
+}
+
+__global__ void k_total(int nrow, int* __restrict__ offsets, const int* __restrict__ total, int* __restrict__ nnz) {
+  offsets[nrow] = *total;
+  *nnz = *total;
+}
+
+template <class S>
+int assemble(int n_ee, int n_pt, int nv, const int* ee, const int* pt, const S* vals, int* offsets, int* columns,
+             S* values, int* nnz, int* status, void* ws, cudaStream_t st) {
+  int P = n_ee + n_pt, nq = 4 * P;
+  size_t NQ = (size_t)nq, R = (size_t)nv + 1;
+  char* p = (char*)ws;
+  unsigned* keys = (unsigned*)p; p += al(NQ * 4);
+  int* ids = (int*)p; p += al(NQ * 4);
+  int* qstart = (int*)p; p += al(R * 4);
+  int* tmpcols = (int*)p; p += al(NQ * 4 * 4);
+  int* total = (int*)p; p += 256;
+  void* scratch = p; p += scan::scratch_bytes((int)R);
+  void* sws = p;
+  cudaMemsetAsync(qstart, 0, R * sizeof(int), st);
+  k_quad_keys<<<div_up(nq, 256), 256, 0, st>>>(nq, ee, n_ee, pt, keys, ids, qstart);
+  int bits = 1;
+  while ((1LL << bits) < (long long)nv) ++bits;
+  sort::sort_pairs<unsigned>(keys, ids, nq, bits, sws, sort::workspace_bytes<unsigned>(nq), st);
+  scan::exclusive<int>(qstart, (int)R, scratch, total, st);
+  int g = div_up(nv, kWarps);
+  k_row_columns<S><<<g, kWarps * 32, 0, st>>>(nv, qstart, ids, ee, n_ee, pt, vals, tmpcols, offsets, status);
+  scan::exclusive<int>(offsets, nv, scratch, total, st);
+  k_total<<<1, 1, 0, st>>>(nv, offsets, total, nnz);
+  k_row_values<S><<<g, kWarps * 32, 0, st>>>(nv, qstart, ids, ee, n_ee, pt, vals, tmpcols, offsets, columns, values);
+  return check_launch("ipcb_contact_bsr");
+}
+
+}  // namespace
+}  // namespace ipcb
+
+using namespace ipcb;
+
+extern "C" {
+
+size_t ipcb_contact_bsr_workspace(int n_records, int n_verts) {
+  size_t NQ = 4 * (size_t)(n_records > 0 ? n_records : 1), R = (size_t)(n_verts > 0 ? n_verts : 0) + 1;
+  return al(NQ * 4) * 2 + al(R * 4) + al(NQ * 16) + 256 + scan::scratch_bytes((int)R) +
+         sort::workspace_bytes<unsigned>((int)NQ);
+}
+
+int ipcb_contact_bsr(const ipcb_contacts* ee, int n_ee, const ipcb_contacts* pt, int n_pt, int n_verts,
+                     const void* vals, int fp64, int* offsets, int* columns, void* values, int* nnz, int* status,
+                     void* ws, size_t ws_bytes, ipcb_stream s) {
+  if (!ee || !pt || n_ee < 0 || n_pt < 0 || n_verts < 0 || !offsets || !nnz || !status) return IPCB_E_ARG;
+  if (n_ee > ee->capacity || n_pt > pt->capacity || (long long)4 * (n_ee + n_pt) > 0x7fffffff) return IPCB_E_ARG;
+  cudaStream_t st = (cudaStream_t)s;
+  if (n_ee + n_pt == 0 || n_verts == 0) {
+    cudaMemsetAsync(offsets, 0, (size_t)(n_verts + 1) * sizeof(int), st);
+    cudaMemsetAsync(nnz, 0, sizeof(int), st);
+    return check_launch("ipcb_contact_bsr");
+  }
+  if (!vals || !columns || !values || !ws || ws_bytes < ipcb_contact_bsr_workspace(n_ee + n_pt, n_verts))
+    return IPCB_E_ARG;
+  if (fp64)
+    return assemble<double>(n_ee, n_pt, n_verts, ee->a1a2b1b2, pt->a1a2b1b2, (const double*)vals, offsets, columns,
+                            (double*)values, nnz, status, ws, st);
+  return assemble<float>(n_ee, n_pt, n_verts, ee->a1a2b1b2, pt->a1a2b1b2, (const float*)vals, offsets, columns,
+                         (float*)values, nnz, status, ws, st);
+}
+
+}  // extern "C"

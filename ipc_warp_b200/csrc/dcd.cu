@@ -47,14 +47,10 @@ __global__ void k_tri_aabbs(const float4* __restrict__ x4, const int* __restrict
   hi[3 * i + 2] = fmaxf(fmaxf(a.z, b.z), c.z) + pad;
 }
 
-// Append one record with a warp-aggregated atomic (one atomicAdd per group of
-// lanes that accept at the same time), as contact.py:171-183 append().
+constexpr int kQueue = 32;  // per-thread queue of filtered leaf hits
+
 template <class S>
-IPCB_D void append(const ipcb_contacts& c, int a1, int a2, int b1, int b2, int e0, int e1, S l0) {
-  cg::coalesced_group g = cg::coalesced_threads();
-  int base = 0;
-  if (g.thread_rank() == 0) base = atomicAdd(c.cnt, (int)g.size());
-  int slot = g.shfl(base, 0) + (int)g.thread_rank();
+IPCB_D void write_record(const ipcb_contacts& c, int slot, int a1, int a2, int b1, int b2, int e0, int e1, S l0) {
   if (slot < c.capacity) {
     reinterpret_cast<int4*>(c.a1a2b1b2)[slot] = make_int4(a1, a2, b1, b2);
     reinterpret_cast<int2*>(c.e0e1)[slot] = make_int2(e0, e1);
@@ -64,32 +60,77 @@ IPCB_D void append(const ipcb_contacts& c, int a1, int a2, int b1, int b2, int e
   }
 }
 
+// Append from inside divergent code (rare path: a full queue).
+template <class S>
+IPCB_D void append_divergent(const ipcb_contacts& c, int a1, int a2, int b1, int b2, int e0, int e1, S l0) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  int base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(c.cnt, (int)g.size());
+  write_record<S>(c, g.shfl(base, 0) + (int)g.thread_rank(), a1, a2, b1, b2, e0, e1, l0);
+}
+
+// Append from converged code: one ballot and one atomicAdd per warp.
+IPCB_D int warp_reserve(int* cnt, bool accept) {
+  const unsigned lane = threadIdx.x & 31;
+  unsigned m = __ballot_sync(0xffffffffu, accept);
+  int base = 0;
+  if (lane == 0 && m) base = atomicAdd(cnt, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  return base + __popc(m & ((1u << lane) - 1u));
+}
+
+IPCB_D int warp_max(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
 // One thread per edge, visiting edges in the BVH leaf (Morton) order so a
-// warp's queries walk neighbouring subtrees.
+// warp's queries walk neighbouring subtrees.  Traversal only applies the cheap
+// filters and queues the surviving leaves; the exact closest-point test and
+// the append run afterwards with the warp converged.
 template <class S>
 __global__ void __launch_bounds__(128) k_dcd_ee(const float4* __restrict__ x4, const int* __restrict__ edges,
                                                 const int* __restrict__ body, const float4* __restrict__ nodes,
                                                 const int* __restrict__ order, int n, float thickness, float qpad,
                                                 int exclude, ipcb_contacts out, int* status) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  int i = __ldg(order + t);
-  int2 ea = __ldg(reinterpret_cast<const int2*>(edges) + i);
+  bool active = t < n;
+  int i = active ? __ldg(order + t) : 0;
+  int2 ea = active ? __ldg(reinterpret_cast<const int2*>(edges) + i) : make_int2(0, 0);
   f3 p1 = load4(x4, ea.x), p2 = load4(x4, ea.y);
   int bi = exclude ? __ldg(body + ea.x) : 0;
-  f3 qlo = mk3(fminf(p1.x, p2.x) - qpad, fminf(p1.y, p2.y) - qpad, fminf(p1.z, p2.z) - qpad);
-  f3 qhi = mk3(fmaxf(p1.x, p2.x) + qpad, fmaxf(p1.y, p2.y) + qpad, fmaxf(p1.z, p2.z) + qpad);
   const float l0f = xmul(thickness, 2.0f);
   const S l0 = S(thickness) * S(2.0);
-  bool ok = traverse(nodes, n, qlo, qhi, [&](int j) {
-    if (!(i < j)) return;
-    int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + j);
-    if (ea.x == eb.x || ea.x == eb.y || ea.y == eb.x || ea.y == eb.y) return;
-    if (exclude && bi == __ldg(body + eb.x)) return;
-    CPEE r = closest_point_edge_edge(p1, p2, load4(x4, eb.x), load4(x4, eb.y), 1.0e-6f);
-    if (r.d < l0f) append<S>(out, ea.x, ea.y, eb.x, eb.y, i, j, l0);
-  });
-  if (!ok) atomicOr(status, IPCB_STATUS_STACK);
+  int q[kQueue];
+  int nq = 0;
+  if (active) {
+    f3 qlo = mk3(fminf(p1.x, p2.x) - qpad, fminf(p1.y, p2.y) - qpad, fminf(p1.z, p2.z) - qpad);
+    f3 qhi = mk3(fmaxf(p1.x, p2.x) + qpad, fmaxf(p1.y, p2.y) + qpad, fmaxf(p1.z, p2.z) + qpad);
+    bool ok = traverse(nodes, n, qlo, qhi, [&](int j) {
+      if (!(i < j)) return;
+      int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + j);
+      if (ea.x == eb.x || ea.x == eb.y || ea.y == eb.x || ea.y == eb.y) return;
+      if (exclude && bi == __ldg(body + eb.x)) return;
+      if (nq < kQueue) {
+        q[nq++] = j;
+      } else {
+        CPEE r = closest_point_edge_edge(p1, p2, load4(x4, eb.x), load4(x4, eb.y), 1.0e-6f);
+        if (r.d < l0f) append_divergent<S>(out, ea.x, ea.y, eb.x, eb.y, i, j, l0);
+      }
+    });
+    if (!ok) atomicOr(status, IPCB_STATUS_STACK);
+  }
+  int rounds = warp_max(nq);
+  for (int k = 0; k < rounds; ++k) {
+    bool has = k < nq;
+    int j = has ? q[k] : 0;
+    int2 eb = has ? __ldg(reinterpret_cast<const int2*>(edges) + j) : make_int2(0, 0);
+    bool accept = false;
+    if (has) accept = closest_point_edge_edge(p1, p2, load4(x4, eb.x), load4(x4, eb.y), 1.0e-6f).d < l0f;
+    int slot = warp_reserve(out.cnt, accept);
+    if (accept) write_record<S>(out, slot, ea.x, ea.y, eb.x, eb.y, i, j, l0);
+  }
 }
 
 template <class S>
@@ -98,21 +139,40 @@ __global__ void __launch_bounds__(128) k_dcd_pt(const float4* __restrict__ x4, c
                                                 int n_tris, const int* __restrict__ order, int nv, float thickness,
                                                 float qpad, int exclude, ipcb_contacts out, int* status) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nv) return;
-  int i = order ? __ldg(order + t) : t;
+  bool active = t < nv;
+  int i = active ? (order ? __ldg(order + t) : t) : 0;
   f3 p = load4(x4, i);
   int bi = exclude ? __ldg(body + i) : 0;
-  f3 qlo = mk3(p.x - qpad, p.y - qpad, p.z - qpad), qhi = mk3(p.x + qpad, p.y + qpad, p.z + qpad);
   const float l0f = xmul(thickness, 2.0f);
   const S l0 = S(thickness) * S(2.0);
-  bool ok = traverse(nodes, n_tris, qlo, qhi, [&](int j) {
-    int t0 = __ldg(tris + 3 * j), t1 = __ldg(tris + 3 * j + 1), t2 = __ldg(tris + 3 * j + 2);
-    if (t0 == i || t1 == i || t2 == i) return;
-    if (exclude && bi == __ldg(body + t0)) return;
-    CPT r = closest_point_triangle(p, load4(x4, t0), load4(x4, t1), load4(x4, t2));
-    if (r.d < l0f) append<S>(out, i, t1, t0, t2, i, j, l0);  // (p, tri[1], tri[0], tri[2])
-  });
-  if (!ok) atomicOr(status, IPCB_STATUS_STACK);
+  int q[kQueue];
+  int nq = 0;
+  if (active) {
+    f3 qlo = mk3(p.x - qpad, p.y - qpad, p.z - qpad), qhi = mk3(p.x + qpad, p.y + qpad, p.z + qpad);
+    bool ok = traverse(nodes, n_tris, qlo, qhi, [&](int j) {
+      int t0 = __ldg(tris + 3 * j), t1 = __ldg(tris + 3 * j + 1), t2 = __ldg(tris + 3 * j + 2);
+      if (t0 == i || t1 == i || t2 == i) return;
+      if (exclude && bi == __ldg(body + t0)) return;
+      if (nq < kQueue) {
+        q[nq++] = j;
+      } else {
+        CPT r = closest_point_triangle(p, load4(x4, t0), load4(x4, t1), load4(x4, t2));
+        if (r.d < l0f) append_divergent<S>(out, i, t1, t0, t2, i, j, l0);
+      }
+    });
+    if (!ok) atomicOr(status, IPCB_STATUS_STACK);
+  }
+  int rounds = warp_max(nq);
+  for (int k = 0; k < rounds; ++k) {
+    bool has = k < nq;
+    int j = has ? q[k] : 0;
+    int t0 = has ? __ldg(tris + 3 * j) : 0, t1 = has ? __ldg(tris + 3 * j + 1) : 0,
+        t2 = has ? __ldg(tris + 3 * j + 2) : 0;
+    bool accept = false;
+    if (has) accept = closest_point_triangle(p, load4(x4, t0), load4(x4, t1), load4(x4, t2)).d < l0f;
+    int slot = warp_reserve(out.cnt, accept);
+    if (accept) write_record<S>(out, slot, i, t1, t0, t2, i, j, l0);  // (p, tri[1], tri[0], tri[2])
+  }
 }
 
 }  // namespace

@@ -18,7 +18,7 @@ import ctypes
 import torch
 
 from . import _native as N
-from .bsr import BsrMatrix, Triplets, bsr_from_triplets
+from .bsr import BsrMatrix, Triplets, bsr_from_triplets, contact_bsr
 from .contact import ContactSolverBase, Contacts, Soup
 
 
@@ -87,9 +87,13 @@ class ContactBarrierMixin(ContactSolverBase):
                 contact_hessian_ee(states, self.soup, self.contacts_new, t, self.b, kappa, n=n_ee)
             if n_pt:
                 contact_hessian_pt(states, self.soup, self.contacts_pt, t, self.b, n_ee, kappa, n=n_pt)
-            self.collision_hessian = bsr_from_triplets(self.soup.n_verts, self.soup.n_verts, t.rows, t.cols, t.vals,
-                                                       count=nnz,
-                                                       out=getattr(self, "collision_hessian", None))
+            prev = getattr(self, "collision_hessian", None)
+            H, status = contact_bsr(self.contacts_new, n_ee, self.contacts_pt, n_pt, self.soup.n_verts, t.vals,
+                                    out=prev)
+            if status & 4:  # a row with too many distinct columns: generic assembly
+                H = bsr_from_triplets(self.soup.n_verts, self.soup.n_verts, t.rows, t.cols, t.vals, count=nnz,
+                                      out=H)
+            self.collision_hessian = H
         return self.collision_hessian
 
     def compute_collision_energy(self, detect: bool = True) -> float:

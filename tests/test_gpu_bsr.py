@@ -43,3 +43,36 @@ def test_bsr_from_triplets(cuda, n_trip, nrow, fp64):
     y = bsr_mv(A, tr(x)).cpu().numpy().ravel()
     yref = ref @ x.ravel().astype(np.float64)
     assert np.abs(y - yref).max() <= (1e-10 if fp64 else 1e-4) * max(np.abs(yref).max(), 1.0)
+
+
+@pytest.mark.parametrize("idx", range(4))
+@pytest.mark.parametrize("fp64", [False, True])
+def test_contact_bsr_equals_generic_assembly(cuda, idx, fp64):
+    """The record-structured assembly and the generic triplet assembly give
+    the same matrix bit for bit (both sum each block's contributions in
+    record order)."""
+    from helpers import small_scenes
+    from ipc_warp_b200.bsr import contact_bsr
+    from test_gpu_dcd import make_solver
+    from test_gpu_narrow import run_gpu
+
+    sc = small_scenes()[idx]
+    s = make_solver(sc, torch.float64 if fp64 else torch.float32)
+    s.detect_collision()
+    from ipc_warp_b200.bsr import Triplets
+    from ipc_warp_b200.dynamic_contacts import contact_hessian_ee, contact_hessian_pt
+
+    n_ee, n_pt = s.n_contacts, s.n_contacts_pt
+    t = Triplets.zeros((n_ee + n_pt) * 16, s.soup.xcs.dtype, s.device)
+    b = torch.zeros_like(s.soup.x_transformed)
+    contact_hessian_ee(None, s.soup, s.contacts_new, t, b, 1e4, n=n_ee)
+    contact_hessian_pt(None, s.soup, s.contacts_pt, t, b, n_ee, 1e4, n=n_pt)
+    nv = s.soup.n_verts
+    A = bsr_from_triplets(nv, nv, t.rows, t.cols, t.vals)
+    B, status = contact_bsr(s.contacts_new, n_ee, s.contacts_pt, n_pt, nv, t.vals)
+    assert status == 0
+    nnz = A.nnz_sync()
+    assert B.nnz_sync() == nnz > 0
+    assert torch.equal(A.offsets, B.offsets)
+    assert torch.equal(A.columns[:nnz], B.columns[:nnz])
+    assert torch.equal(A.values[:nnz], B.values[:nnz])
