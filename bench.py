@@ -162,10 +162,10 @@ def stage_times(pipe, dx, reps, torch):
         marks.append(("narrow_ee", ev()))
         contact_hessian_pt(None, pipe.soup, pipe.contacts_pt, t, pipe.b, n_ee, pipe.contact_stiffness, n=n_pt)
         marks.append(("narrow_pt", ev()))
-        from ipc_warp_b200.bsr import bsr_from_triplets
+        from ipc_warp_b200.bsr import contact_bsr
 
-        bsr_from_triplets(pipe.soup.n_verts, pipe.soup.n_verts, t.rows, t.cols, t.vals, count=(n_ee + n_pt) * 16,
-                          out=pipe.collision_hessian)
+        contact_bsr(pipe.contacts_new, n_ee, pipe.contacts_pt, n_pt, pipe.soup.n_verts, t.vals,
+                    out=pipe.collision_hessian)
         marks.append(("bsr", ev()))
         pipe.compute_collision_energy(detect=False)
         marks.append(("energy", ev()))
