@@ -164,7 +164,7 @@ def stage_times(pipe, dx, reps, torch):
         marks.append(("narrow_pt", ev()))
         from ipc_warp_b200.bsr import contact_bsr
 
-        contact_bsr(pipe.contacts_new, n_ee, pipe.contacts_pt, n_pt, pipe.soup.n_verts, t.vals,
+        contact_bsr(pipe.contacts_new, n_ee, pipe.contacts_pt, n_pt, pipe.soup.n_verts, t,
                     out=pipe.collision_hessian)
         marks.append(("bsr", ev()))
         pipe.compute_collision_energy(detect=False)

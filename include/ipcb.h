@@ -150,9 +150,11 @@ int ipcb_dcd_pt(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* tri_bvh
  * min(*list->cnt, capacity) on the device (graph-capturable).
  * Writes 16 triplets per record at (offset + k)*16 + ii*4 + jj: rows/cols
  * int32, vals scalar[9] row-major; inactive records (dist >= l0) get zero
- * blocks at (0,0).  b (scalar[3V]) accumulates the force -dE/dx. */
+ * blocks at (0,0).  b (scalar[3V]) accumulates the force -dE/dx.
+ * block_mask (optional, uint16[offset + n]): bit ii*4+jj set when block
+ * (ii, jj) of the record has a non-zero entry (read by ipcb_contact_bsr). */
 int ipcb_contact_hessian(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, int offset, double kappa,
-                         int* rows, int* cols, void* vals, void* b, ipcb_stream s);
+                         int* rows, int* cols, void* vals, void* b, unsigned short* block_mask, ipcb_stream s);
 /* energy (double) += sum of the barrier energy of the list */
 int ipcb_contact_energy(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, double kappa,
                         double* energy, ipcb_stream s);
@@ -185,17 +187,18 @@ size_t ipcb_bsr_workspace(int n_trip, int nrow, int ncol);
 int ipcb_bsr_from_triplets(int nrow, int ncol, int n_trip, const int* rows, const int* cols, const void* vals,
                            int fp64, int* offsets, int* columns, void* values, int* nnz, void* ws, size_t ws_bytes,
                            ipcb_stream s);
-/* The same BSR for the contact Hessian, assembled from the EE and PT lists
- * and their triplet values (16 blocks per record, EE records first, as
- * ipcb_contact_hessian writes them) instead of from generic triplets: the
+/* The same BSR for the contact Hessian, assembled from the EE and PT lists,
+ * their triplet values (16 blocks per record, EE records first, as
+ * ipcb_contact_hessian writes them) and block masks instead of from generic
+ * triplets: the
  * records' structure (one row and 4 columns per (record, slot)) replaces the
  * per-triplet bucketing.  Deterministic.  If a row has more than 128 distinct
  * columns, *status gets IPCB_STATUS_ROW_OVERFLOW and the caller must use
  * ipcb_bsr_from_triplets instead. */
 size_t ipcb_contact_bsr_workspace(int n_records, int n_verts);
 int ipcb_contact_bsr(const ipcb_contacts* ee, int n_ee, const ipcb_contacts* pt, int n_pt, int n_verts,
-                     const void* vals, int fp64, int* offsets, int* columns, void* values, int* nnz, int* status,
-                     void* ws, size_t ws_bytes, ipcb_stream s);
+                     const void* vals, const unsigned short* block_mask, int fp64, int* offsets, int* columns,
+                     void* values, int* nnz, int* status, void* ws, size_t ws_bytes, ipcb_stream s);
 /* y = alpha*A*x + beta*y for a 3x3 BSR (bsr_mv) */
 int ipcb_bsr_mv(int nrow, const int* offsets, const int* columns, const void* values, int fp64, const void* x,
                 void* y, double alpha, double beta, ipcb_stream s);

@@ -56,7 +56,7 @@ SIGNATURES = {
     "ipcb_swept_triangle_aabbs": (c_int, [SP, P, c_double, P, P, P]),
     "ipcb_dcd_ee": (c_int, [SP, P, BP, c_float, c_float, c_int, CP, P, P]),
     "ipcb_dcd_pt": (c_int, [SP, P, BP, c_float, c_float, c_int, P, CP, P, P]),
-    "ipcb_contact_hessian": (c_int, [c_int, SP, CP, c_int, c_int, c_double, P, P, P, P, P]),
+    "ipcb_contact_hessian": (c_int, [c_int, SP, CP, c_int, c_int, c_double, P, P, P, P, P, P]),
     "ipcb_contact_energy": (c_int, [c_int, SP, CP, c_int, c_double, P, P]),
     "ipcb_toi_workspace": (c_size_t, [c_int]),
     "ipcb_edge_edge_toi": (c_int, [SP, P, BP, P, P, c_int, P, P, P, c_size_t, P]),
@@ -67,7 +67,7 @@ SIGNATURES = {
     "ipcb_bsr_from_triplets": (c_int, [c_int, c_int, c_int, P, P, P, c_int, P, P, P, P, P, c_size_t, P]),
     "ipcb_bsr_mv": (c_int, [c_int, P, P, P, c_int, P, P, c_double, c_double, P]),
     "ipcb_contact_bsr_workspace": (c_size_t, [c_int, c_int]),
-    "ipcb_contact_bsr": (c_int, [CP, c_int, CP, c_int, c_int, P, c_int, P, P, P, P, P, P, c_size_t, P]),
+    "ipcb_contact_bsr": (c_int, [CP, c_int, CP, c_int, c_int, P, P, c_int, P, P, P, P, P, P, c_size_t, P]),
 }
 
 

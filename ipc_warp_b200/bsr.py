@@ -21,12 +21,16 @@ class Triplets:
     rows: torch.Tensor  # int32 (n,)
     cols: torch.Tensor  # int32 (n,)
     vals: torch.Tensor  # scalar (n, 3, 3)
+    # contact triplets only: per record (16 triplets) a 16-bit mask of the
+    # blocks with a non-zero entry, int16 (n // 16,)
+    mask: torch.Tensor | None = None
 
     @staticmethod
     def zeros(n: int, dtype, device) -> "Triplets":
         return Triplets(torch.zeros(n, dtype=torch.int32, device=device),
                         torch.zeros(n, dtype=torch.int32, device=device),
-                        torch.zeros((n, 3, 3), dtype=dtype, device=device))
+                        torch.zeros((n, 3, 3), dtype=dtype, device=device),
+                        torch.zeros(max(n // 16, 1), dtype=torch.int16, device=device))
 
 
 class BsrMatrix:
@@ -74,12 +78,13 @@ def bsr_from_triplets(nrow: int, ncol: int, rows: torch.Tensor, cols: torch.Tens
     return out
 
 
-def contact_bsr(ee, n_ee: int, pt, n_pt: int, n_verts: int, vals: torch.Tensor,
+def contact_bsr(ee, n_ee: int, pt, n_pt: int, n_verts: int, trip: Triplets,
                 out: BsrMatrix | None = None, status: torch.Tensor | None = None) -> tuple[BsrMatrix, int]:
-    """BSR of the contact Hessian from the EE/PT lists and their triplet
-    values (16 blocks per record, EE first).  Returns (matrix, status);
+    """BSR of the contact Hessian from the EE/PT lists and their triplets
+    (16 blocks per record, EE first, with block masks).  Returns (matrix, status);
     status has IPCB_STATUS_ROW_OVERFLOW (4) set when a row had too many
     distinct columns for the fast path (the matrix is then incomplete)."""
+    vals = trip.vals
     dtype, dev = vals.dtype, vals.device
     cap = max(16 * (n_ee + n_pt), 1)
     if out is None or out.columns.shape[0] < cap or out.nrow != n_verts or out.dtype != dtype:
@@ -89,7 +94,8 @@ def contact_bsr(ee, n_ee: int, pt, n_pt: int, n_verts: int, vals: torch.Tensor,
     import ctypes
 
     N.call("ipcb_contact_bsr", ctypes.byref(ee.c_struct()), n_ee, ctypes.byref(pt.c_struct()), n_pt, n_verts,
-           N.ptr(vals), int(dtype == torch.float64), N.ptr(out.offsets), N.ptr(out.columns), N.ptr(out.values),
+           N.ptr(vals), N.ptr(trip.mask), int(dtype == torch.float64), N.ptr(out.offsets), N.ptr(out.columns),
+           N.ptr(out.values),
            N.ptr(out.nnz_dev), N.ptr(st), N.ptr(ws), ws.numel(), N.stream_handle())
     return out, int(st.item())
 

@@ -6,12 +6,15 @@
 // (vertex ii of the record) and 4 consecutive blocks (columns = the record's 4
 // vertices).  A row's distinct columns are few (tens), so:
 //   1. key every quad by its row; stable radix sort (order = (row, quad id))
-//   2. pass A, warp per row: insert the columns of non-zero blocks into a
-//      shared-memory hash, sort the distinct columns, count them
+//   2. pass A, warp per row: insert the columns of the non-zero blocks (the
+//      narrow phase's per-record block masks) into a shared-memory hash, sort
+//      the distinct columns, count them
 //   3. scan the counts -> offsets
 //   4. pass B, warp per row: lane k owns the row's distinct columns k, k+32,
-//      ...; every lane walks the row's quads in order and the owner of each
-//      block's column adds it, so each sum runs in input order (deterministic)
+//      ...; the row's quads are staged 32 at a time in shared memory (ids,
+//      masks, 4 blocks) with coalesced vector loads, then every lane walks them
+//      in order and the owner of each block's column adds it, so each sum runs
+//      in input order (deterministic)
 // A row with more than kHash distinct columns sets IPCB_STATUS_ROW_OVERFLOW
 // (the host then uses the generic assembly).
 #include "common.cuh"
@@ -33,14 +36,6 @@ IPCB_D int4 record_ids(const int* __restrict__ ee, int n_ee, const int* __restri
   return p < n_ee ? __ldg(reinterpret_cast<const int4*>(ee) + p) : __ldg(reinterpret_cast<const int4*>(pt) + (p - n_ee));
 }
 IPCB_D int comp(int4 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
-
-template <class S>
-IPCB_D bool block_nonzero(const S* __restrict__ b) {
-  bool nz = false;
-#pragma unroll
-  for (int q = 0; q < 9; ++q) nz |= b[q] != S(0);
-  return nz;
-}
 
 __global__ void k_quad_keys(int nq, const int* __restrict__ ee, int n_ee, const int* __restrict__ pt,
                             unsigned* __restrict__ keys, int* __restrict__ ids, int* __restrict__ row_cnt) {
@@ -64,12 +59,12 @@ IPCB_D bool hash_insert(int* tab, int c) {
   return false;
 }
 
-template <class S>
 __global__ void __launch_bounds__(kWarps * 32) k_row_columns(int nrow, const int* __restrict__ qstart,
                                                              const int* __restrict__ qids, const int* __restrict__ ee,
                                                              int n_ee, const int* __restrict__ pt,
-                                                             const S* __restrict__ vals, int* __restrict__ tmpcols,
-                                                             int* __restrict__ row_nnz, int* __restrict__ status) {
+                                                             const unsigned short* __restrict__ bmask,
+                                                             int* __restrict__ tmpcols, int* __restrict__ row_nnz,
+                                                             int* __restrict__ status) {
   __shared__ int tab[kWarps][kHash];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int row = blockIdx.x * kWarps + w;
@@ -85,10 +80,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_columns(int nrow, const int
   for (int i = b + lane; i < e; i += 32) {
     int q = qids[i];
     int4 v = record_ids(ee, n_ee, pt, q >> 2);
-    const S* blk = vals + 36LL * q;  // 4 blocks (ii, jj = 0..3) of 9 values
+    unsigned m = (bmask[q >> 2] >> (4 * (q & 3))) & 0xFu;  // blocks (ii, jj = 0..3)
 #pragma unroll
     for (int jj = 0; jj < 4; ++jj)
-      if (block_nonzero(blk + 9 * jj)) ok &= hash_insert(tab[w], comp(v, jj));
+      if ((m >> jj) & 1u) ok &= hash_insert(tab[w], comp(v, jj));
   }
   __syncwarp();
   // compact the occupied slots to the front (stable), pad with INT_MAX, then
@@ -138,14 +133,27 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_columns(int nrow, const int
   }
 }
 
+IPCB_D void copy36(float* dst, const float* __restrict__ src) {
+#pragma unroll
+  for (int k = 0; k < 36; k += 4) *reinterpret_cast<float4*>(dst + k) = __ldg(reinterpret_cast<const float4*>(src + k));
+}
+IPCB_D void copy36(double* dst, const double* __restrict__ src) {
+#pragma unroll
+  for (int k = 0; k < 36; k += 2) *reinterpret_cast<double2*>(dst + k) = __ldg(reinterpret_cast<const double2*>(src + k));
+}
+
 template <class S>
 __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int* __restrict__ qstart,
                                                             const int* __restrict__ qids, const int* __restrict__ ee,
                                                             int n_ee, const int* __restrict__ pt,
+                                                            const unsigned short* __restrict__ bmask,
                                                             const S* __restrict__ vals,
                                                             const int* __restrict__ tmpcols,
                                                             const int* __restrict__ offsets, int* __restrict__ columns,
                                                             S* __restrict__ values) {
+  __shared__ __align__(16) S sv[kWarps][32][36];
+  __shared__ int4 sid[kWarps][32];
+  __shared__ unsigned char smk[kWarps][32];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int row = blockIdx.x * kWarps + w;
   if (row >= nrow) return;
@@ -161,20 +169,32 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int*
 #pragma unroll
     for (int q = 0; q < 9; ++q) acc[r][q] = S(0);
   }
-  for (int i = b; i < e; ++i) {
-    int q = qids[i];
-    int4 v = record_ids(ee, n_ee, pt, q >> 2);
-    const S* blk = vals + 36LL * q;
-#pragma unroll
-    for (int jj = 0; jj < 4; ++jj) {
-      int c = comp(v, jj);
-#pragma unroll
-      for (int r = 0; r < kOwn; ++r)
-        if (own[r] == c) {
-#pragma unroll
-          for (int t = 0; t < 9; ++t) acc[r][t] += blk[9 * jj + t];
-        }
+  for (int base = b; base < e; base += 32) {
+    int i = base + lane;
+    if (i < e) {
+      int q = qids[i];
+      sid[w][lane] = record_ids(ee, n_ee, pt, q >> 2);
+      smk[w][lane] = (unsigned char)((bmask[q >> 2] >> (4 * (q & 3))) & 0xFu);
+      copy36(sv[w][lane], vals + 36LL * q);
     }
+    __syncwarp();
+    int n = min(32, e - base);
+    for (int k = 0; k < n; ++k) {
+      int4 v = sid[w][k];
+      unsigned m = smk[w][k];
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        if (!((m >> jj) & 1u)) continue;
+        int c = comp(v, jj);
+#pragma unroll
+        for (int r = 0; r < kOwn; ++r)
+          if (own[r] == c) {
+#pragma unroll
+            for (int t = 0; t < 9; ++t) acc[r][t] += sv[w][k][9 * jj + t];
+          }
+      }
+    }
+    __syncwarp();
   }
 #pragma unroll
   for (int r = 0; r < kOwn; ++r) {
@@ -193,8 +213,8 @@ __global__ void k_total(int nrow, int* __restrict__ offsets, const int* __restri
 }
 
 template <class S>
-int assemble(int n_ee, int n_pt, int nv, const int* ee, const int* pt, const S* vals, int* offsets, int* columns,
-             S* values, int* nnz, int* status, void* ws, cudaStream_t st) {
+int assemble(int n_ee, int n_pt, int nv, const int* ee, const int* pt, const S* vals, const unsigned short* bmask,
+             int* offsets, int* columns, S* values, int* nnz, int* status, void* ws, cudaStream_t st) {
   int P = n_ee + n_pt, nq = 4 * P;
   size_t NQ = (size_t)nq, R = (size_t)nv + 1;
   char* p = (char*)ws;
@@ -212,10 +232,11 @@ int assemble(int n_ee, int n_pt, int nv, const int* ee, const int* pt, const S* 
   sort::sort_pairs<unsigned>(keys, ids, nq, bits, sws, sort::workspace_bytes<unsigned>(nq), st);
   scan::exclusive<int>(qstart, (int)R, scratch, total, st);
   int g = div_up(nv, kWarps);
-  k_row_columns<S><<<g, kWarps * 32, 0, st>>>(nv, qstart, ids, ee, n_ee, pt, vals, tmpcols, offsets, status);
+  k_row_columns<<<g, kWarps * 32, 0, st>>>(nv, qstart, ids, ee, n_ee, pt, bmask, tmpcols, offsets, status);
   scan::exclusive<int>(offsets, nv, scratch, total, st);
   k_total<<<1, 1, 0, st>>>(nv, offsets, total, nnz);
-  k_row_values<S><<<g, kWarps * 32, 0, st>>>(nv, qstart, ids, ee, n_ee, pt, vals, tmpcols, offsets, columns, values);
+  k_row_values<S><<<g, kWarps * 32, 0, st>>>(nv, qstart, ids, ee, n_ee, pt, bmask, vals, tmpcols, offsets, columns,
+                                             values);
   return check_launch("ipcb_contact_bsr");
 }
 
@@ -233,8 +254,8 @@ size_t ipcb_contact_bsr_workspace(int n_records, int n_verts) {
 }
 
 int ipcb_contact_bsr(const ipcb_contacts* ee, int n_ee, const ipcb_contacts* pt, int n_pt, int n_verts,
-                     const void* vals, int fp64, int* offsets, int* columns, void* values, int* nnz, int* status,
-                     void* ws, size_t ws_bytes, ipcb_stream s) {
+                     const void* vals, const unsigned short* block_mask, int fp64, int* offsets, int* columns,
+                     void* values, int* nnz, int* status, void* ws, size_t ws_bytes, ipcb_stream s) {
   if (!ee || !pt || n_ee < 0 || n_pt < 0 || n_verts < 0 || !offsets || !nnz || !status) return IPCB_E_ARG;
   if (n_ee > ee->capacity || n_pt > pt->capacity || (long long)4 * (n_ee + n_pt) > 0x7fffffff) return IPCB_E_ARG;
   cudaStream_t st = (cudaStream_t)s;
@@ -243,13 +264,14 @@ int ipcb_contact_bsr(const ipcb_contacts* ee, int n_ee, const ipcb_contacts* pt,
     cudaMemsetAsync(nnz, 0, sizeof(int), st);
     return check_launch("ipcb_contact_bsr");
   }
-  if (!vals || !columns || !values || !ws || ws_bytes < ipcb_contact_bsr_workspace(n_ee + n_pt, n_verts))
+  if (!vals || !block_mask || !columns || !values || !ws ||
+      ws_bytes < ipcb_contact_bsr_workspace(n_ee + n_pt, n_verts))
     return IPCB_E_ARG;
   if (fp64)
-    return assemble<double>(n_ee, n_pt, n_verts, ee->a1a2b1b2, pt->a1a2b1b2, (const double*)vals, offsets, columns,
-                            (double*)values, nnz, status, ws, st);
-  return assemble<float>(n_ee, n_pt, n_verts, ee->a1a2b1b2, pt->a1a2b1b2, (const float*)vals, offsets, columns,
-                         (float*)values, nnz, status, ws, st);
+    return assemble<double>(n_ee, n_pt, n_verts, ee->a1a2b1b2, pt->a1a2b1b2, (const double*)vals, block_mask,
+                            offsets, columns, (double*)values, nnz, status, ws, st);
+  return assemble<float>(n_ee, n_pt, n_verts, ee->a1a2b1b2, pt->a1a2b1b2, (const float*)vals, block_mask, offsets,
+                         columns, (float*)values, nnz, status, ws, st);
 }
 
 }  // extern "C"

@@ -386,8 +386,9 @@ IPCB_D void write_zero(int* rows, int* cols, S* vals, long long base) {
 // contiguous and 16-byte aligned (576 B per record in float), written as two
 // halves of 8 blocks with vector stores.
 template <class S, class T>
-IPCB_D void write_blocks(const int4 id, int* rows, int* cols, S* vals, long long base, const T (&h)[kMaxH][12],
-                         const T (&w)[kMaxH], int nh) {
+IPCB_D unsigned write_blocks(const int4 id, int* rows, int* cols, S* vals, long long base, const T (&h)[kMaxH][12],
+                             const T (&w)[kMaxH], int nh) {
+  unsigned mask = 0;
   const int vid[4] = {id.x, id.y, id.z, id.w};
 #pragma unroll
   for (int ii = 0; ii < 4; ++ii) {
@@ -411,10 +412,12 @@ IPCB_D void write_blocks(const int4 id, int* rows, int* cols, S* vals, long long
             for (int m = 0; m < kMaxH; ++m)
               if (m < nh) v += w[m] * h[m][3 * ii + a] * h[m][3 * jj + b];
             buf[(i2 * 4 + jj) * 9 + 3 * a + b] = S(v);
+            if (S(v) != S(0)) mask |= 1u << (ii * 4 + jj);
           }
     }
     store16(vals + 9 * base + 72 * half, buf, 72);
   }
+  return mask;
 }
 
 template <class S>
@@ -447,7 +450,8 @@ template <class S, int KIND>
 __global__ void __launch_bounds__(128) k_contact_hessian(const S* __restrict__ x, const S* __restrict__ xcs,
                                                          ipcb_contacts L, int n, int offset, double kappa,
                                                          int* __restrict__ rows, int* __restrict__ cols,
-                                                         S* __restrict__ vals, S* __restrict__ bforce) {
+                                                         S* __restrict__ vals, S* __restrict__ bforce,
+                                                         unsigned short* __restrict__ block_mask) {
   typedef S T;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int cnt = list_count<S>(L, n);
@@ -463,6 +467,7 @@ __global__ void __launch_bounds__(128) k_contact_hessian(const S* __restrict__ x
   else dist = closest_point_triangle(xf[0], xf[1], xf[2], xf[3]).d;
   if (!(S(dist) < l0)) {
     write_zero<S>(rows, cols, vals, base);
+    if (block_mask) block_mask[offset + i] = 0;
     return;
   }
   Feature f;
@@ -506,7 +511,8 @@ __global__ void __launch_bounds__(128) k_contact_hessian(const S* __restrict__ x
 #pragma unroll
     for (int k = 0; k < 12; ++k) fc[k] = -br.db * g[k];
   }
-  write_blocks<S, T>(id, rows, cols, vals, base, h, w, nh);
+  unsigned mask = write_blocks<S, T>(id, rows, cols, vals, base, h, w, nh);
+  if (block_mask) block_mask[offset + i] = (unsigned short)mask;
   add_force<S>(bforce, id, fc);
 }
 
@@ -554,16 +560,16 @@ __global__ void __launch_bounds__(256) k_contact_energy(const S* __restrict__ x,
 
 template <class S>
 int launch_hessian(int kind, const ipcb_soup* soup, const ipcb_contacts* L, int n, int offset, double kappa,
-                   int* rows, int* cols, void* vals, void* b, cudaStream_t st) {
+                   int* rows, int* cols, void* vals, void* b, unsigned short* mask, cudaStream_t st) {
   int threads = n >= 0 ? n : L->capacity;
   if (threads == 0) return IPCB_OK;
   dim3 grid(div_up(threads, 128));
   if (kind == 0)
     k_contact_hessian<S, 0><<<grid, 128, 0, st>>>((const S*)soup->x, (const S*)soup->xcs, *L, n, offset, kappa, rows,
-                                                  cols, (S*)vals, (S*)b);
+                                                  cols, (S*)vals, (S*)b, mask);
   else
     k_contact_hessian<S, 1><<<grid, 128, 0, st>>>((const S*)soup->x, (const S*)soup->xcs, *L, n, offset, kappa, rows,
-                                                  cols, (S*)vals, (S*)b);
+                                                  cols, (S*)vals, (S*)b, mask);
   return check_launch("ipcb_contact_hessian");
 }
 
@@ -588,11 +594,12 @@ using namespace ipcb;
 extern "C" {
 
 int ipcb_contact_hessian(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, int offset, double kappa,
-                         int* rows, int* cols, void* vals, void* b, ipcb_stream s) {
+                         int* rows, int* cols, void* vals, void* b, unsigned short* block_mask, ipcb_stream s) {
   if (!soup || !list || !rows || !cols || !vals || !b || (kind != 0 && kind != 1) || offset < 0) return IPCB_E_ARG;
   if (n > list->capacity) return IPCB_E_ARG;
-  if (soup->fp64) return launch_hessian<double>(kind, soup, list, n, offset, kappa, rows, cols, vals, b, (cudaStream_t)s);
-  return launch_hessian<float>(kind, soup, list, n, offset, kappa, rows, cols, vals, b, (cudaStream_t)s);
+  if (soup->fp64)
+    return launch_hessian<double>(kind, soup, list, n, offset, kappa, rows, cols, vals, b, block_mask, (cudaStream_t)s);
+  return launch_hessian<float>(kind, soup, list, n, offset, kappa, rows, cols, vals, b, block_mask, (cudaStream_t)s);
 }
 
 int ipcb_contact_energy(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, double kappa,

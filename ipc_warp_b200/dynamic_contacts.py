@@ -32,7 +32,7 @@ def contact_hessian_ee(states, soup: Soup, contacts: Contacts, triplets: Triplet
     n = min(_count(contacts, n), contacts.capacity)
     N.call("ipcb_contact_hessian", 0, ctypes.byref(soup.c_struct()), ctypes.byref(contacts.c_struct()), n, 0,
            float(kappa), N.ptr(triplets.rows), N.ptr(triplets.cols), N.ptr(triplets.vals), N.ptr(b),
-           N.stream_handle())
+           N.ptr(triplets.mask), N.stream_handle())
 
 
 def contact_hessian_pt(states, soup: Soup, contacts: Contacts, triplets: Triplets, b: torch.Tensor, offset: int,
@@ -41,7 +41,7 @@ def contact_hessian_pt(states, soup: Soup, contacts: Contacts, triplets: Triplet
     n = min(_count(contacts, n), contacts.capacity)
     N.call("ipcb_contact_hessian", 1, ctypes.byref(soup.c_struct()), ctypes.byref(contacts.c_struct()), n,
            int(offset), float(kappa), N.ptr(triplets.rows), N.ptr(triplets.cols), N.ptr(triplets.vals), N.ptr(b),
-           N.stream_handle())
+           N.ptr(triplets.mask), N.stream_handle())
 
 
 def contact_energy_ee(states, soup: Soup, contacts: Contacts, e: torch.Tensor, kappa: float, n: int | None = None):
@@ -88,8 +88,7 @@ class ContactBarrierMixin(ContactSolverBase):
             if n_pt:
                 contact_hessian_pt(states, self.soup, self.contacts_pt, t, self.b, n_ee, kappa, n=n_pt)
             prev = getattr(self, "collision_hessian", None)
-            H, status = contact_bsr(self.contacts_new, n_ee, self.contacts_pt, n_pt, self.soup.n_verts, t.vals,
-                                    out=prev)
+            H, status = contact_bsr(self.contacts_new, n_ee, self.contacts_pt, n_pt, self.soup.n_verts, t, out=prev)
             if status & 4:  # a row with too many distinct columns: generic assembly
                 H = bsr_from_triplets(self.soup.n_verts, self.soup.n_verts, t.rows, t.cols, t.vals, count=nnz,
                                       out=H)

@@ -35,4 +35,4 @@ def test_sizes_and_args_without_gpu():
     assert L.ipcb_bsr_workspace(100, 10, 10) > 100 * 8
     # argument validation happens before any launch
     assert L.ipcb_sort_pairs_u32(None, None, -1, 8, None, 0, None) == 1
-    assert L.ipcb_contact_hessian(5, None, None, 0, 0, 1.0, None, None, None, None, None) == 1
+    assert L.ipcb_contact_hessian(5, None, None, 0, 0, 1.0, None, None, None, None, None, None) == 1

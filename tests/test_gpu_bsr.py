@@ -69,10 +69,14 @@ def test_contact_bsr_equals_generic_assembly(cuda, idx, fp64):
     contact_hessian_pt(None, s.soup, s.contacts_pt, t, b, n_ee, 1e4, n=n_pt)
     nv = s.soup.n_verts
     A = bsr_from_triplets(nv, nv, t.rows, t.cols, t.vals)
-    B, status = contact_bsr(s.contacts_new, n_ee, s.contacts_pt, n_pt, nv, t.vals)
+    B, status = contact_bsr(s.contacts_new, n_ee, s.contacts_pt, n_pt, nv, t)
     assert status == 0
     nnz = A.nnz_sync()
     assert B.nnz_sync() == nnz > 0
     assert torch.equal(A.offsets, B.offsets)
     assert torch.equal(A.columns[:nnz], B.columns[:nnz])
-    assert torch.equal(A.values[:nnz], B.values[:nnz])
+    # same blocks; the generic path sums each run with a warp tree, this one
+    # sequentially, so values agree to rounding
+    a, bb = A.values[:nnz].double(), B.values[:nnz].double()
+    tol = 1e-12 if fp64 else 2e-6
+    assert ((a - bb).abs().amax(dim=(1, 2)) <= tol * a.abs().amax(dim=(1, 2)).clamp_min(1e-300)).all()
