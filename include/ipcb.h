@@ -77,6 +77,7 @@ typedef struct {
   int* sorted;    /* int32[capacity]: primitive of each leaf slot (Morton order) */
   unsigned* keys; /* uint32[capacity]: sorted Morton codes */
   unsigned* flags;/* uint32[capacity]: refit arrival counters (zero between calls) */
+  void* wide;     /* float4[8*max(capacity-1,1)]: 4-wide view rebuilt by build/refit (queries use it) */
 } ipcb_lbvh;
 
 int ipcb_version(void);

@@ -28,7 +28,7 @@ class Contacts(ctypes.Structure):
 
 class Lbvh(ctypes.Structure):
     _fields_ = [("n", c_int), ("capacity", c_int), ("nodes", P), ("parent", P), ("sorted", P), ("keys", P),
-                ("flags", P)]
+                ("flags", P), ("wide", P)]
 
 
 SP, CP, BP = ctypes.POINTER(Soup), ctypes.POINTER(Contacts), ctypes.POINTER(Lbvh)

@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, co
   if (active) {
     f3 qlo = mk3(__ldg(lo + 3 * i), __ldg(lo + 3 * i + 1), __ldg(lo + 3 * i + 2));
     f3 qhi = mk3(__ldg(hi + 3 * i), __ldg(hi + 3 * i + 1), __ldg(hi + 3 * i + 2));
-    bool ok = traverse(nodes, n, qlo, qhi, [&](int j) {
+    bool ok = traverse4(nodes, n, qlo, qhi, [&](int j) {
       if (!(i < j)) return;
       int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + j);
       if (ea.x == eb.x || ea.x == eb.y || ea.y == eb.x || ea.y == eb.y) return;
@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(128) k_pt_collect(const S* __restrict__ x0, co
                  __double2float_rd(dmin(a.z, b.z) - pad));
     f3 qhi = mk3(__double2float_ru(dmax(a.x, b.x) + pad), __double2float_ru(dmax(a.y, b.y) + pad),
                  __double2float_ru(dmax(a.z, b.z) + pad));
-    bool ok = traverse(nodes, n_tris, qlo, qhi, [&](int j) {
+    bool ok = traverse4(nodes, n_tris, qlo, qhi, [&](int j) {
       int3 tj = make_int3(__ldg(tris + 3 * j), __ldg(tris + 3 * j + 1), __ldg(tris + 3 * j + 2));
       if (i == tj.x || i == tj.y || i == tj.z) return;
       if (exclude && bi == __ldg(body + tj.x)) return;
@@ -670,14 +670,14 @@ int ipcb_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* b
   dim3 g(div_up(n, 128)), gc(div_up(c.capacity > 0 ? c.capacity : 1, 128));
   if (soup->fp64) {
     k_ee_collect<double><<<g, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, soup->body,
-                                            (const float4*)bvh->nodes, bvh->sorted, n, lower, upper,
+                                            (const float4*)bvh->wide, bvh->sorted, n, lower, upper,
                                             exclude_same_body, c, (double*)toi, status);
     if (c.capacity)
       k_cand_toi<double, 0><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, c,
                                                 (double*)toi, status);
   } else {
     k_ee_collect<float><<<g, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, soup->body,
-                                           (const float4*)bvh->nodes, bvh->sorted, n, lower, upper,
+                                           (const float4*)bvh->wide, bvh->sorted, n, lower, upper,
                                            exclude_same_body, c, (float*)toi, status);
     if (c.capacity)
       k_cand_toi<float, 0><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, c,
@@ -699,14 +699,14 @@ int ipcb_point_triangle_toi(const ipcb_soup* soup, const void* x1, const ipcb_lb
   dim3 g(div_up(nv, 128)), gc(div_up(c.capacity > 0 ? c.capacity : 1, 128));
   if (soup->fp64) {
     k_pt_collect<double><<<g, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, soup->body,
-                                            (const float4*)bvh->nodes, soup->n_tris, nv, pad, exclude_same_body, c,
+                                            (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude_same_body, c,
                                             (double*)toi, status);
     if (c.capacity)
       k_cand_toi<double, 1><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, c,
                                                 (double*)toi, status);
   } else {
     k_pt_collect<float><<<g, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, soup->body,
-                                           (const float4*)bvh->nodes, soup->n_tris, nv, pad, exclude_same_body, c,
+                                           (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude_same_body, c,
                                            (float*)toi, status);
     if (c.capacity)
       k_cand_toi<float, 1><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, c,

@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(128) k_dcd_ee(const float4* __restrict__ x4, c
   if (active) {
     f3 qlo = mk3(fminf(p1.x, p2.x) - qpad, fminf(p1.y, p2.y) - qpad, fminf(p1.z, p2.z) - qpad);
     f3 qhi = mk3(fmaxf(p1.x, p2.x) + qpad, fmaxf(p1.y, p2.y) + qpad, fmaxf(p1.z, p2.z) + qpad);
-    bool ok = traverse(nodes, n, qlo, qhi, [&](int j) {
+    bool ok = traverse4(nodes, n, qlo, qhi, [&](int j) {
       if (!(i < j)) return;
       int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + j);
       if (ea.x == eb.x || ea.x == eb.y || ea.y == eb.x || ea.y == eb.y) return;
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(128) k_dcd_pt(const float4* __restrict__ x4, c
   int nq = 0;
   if (active) {
     f3 qlo = mk3(p.x - qpad, p.y - qpad, p.z - qpad), qhi = mk3(p.x + qpad, p.y + qpad, p.z + qpad);
-    bool ok = traverse(nodes, n_tris, qlo, qhi, [&](int j) {
+    bool ok = traverse4(nodes, n_tris, qlo, qhi, [&](int j) {
       int t0 = __ldg(tris + 3 * j), t1 = __ldg(tris + 3 * j + 1), t2 = __ldg(tris + 3 * j + 2);
       if (t0 == i || t1 == i || t2 == i) return;
       if (exclude && bi == __ldg(body + t0)) return;
@@ -218,11 +218,11 @@ int ipcb_dcd_ee(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* bvh, fl
   dim3 grid(div_up(n, 128));
   if (soup->fp64)
     k_dcd_ee<double><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->edges, soup->body,
-                                                        (const float4*)bvh->nodes, bvh->sorted, n, thickness,
+                                                        (const float4*)bvh->wide, bvh->sorted, n, thickness,
                                                         query_pad, exclude_same_body, *out, status);
   else
     k_dcd_ee<float><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->edges, soup->body,
-                                                       (const float4*)bvh->nodes, bvh->sorted, n, thickness,
+                                                       (const float4*)bvh->wide, bvh->sorted, n, thickness,
                                                        query_pad, exclude_same_body, *out, status);
   return check_launch("ipcb_dcd_ee");
 }
@@ -235,11 +235,11 @@ int ipcb_dcd_pt(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* bvh, fl
   dim3 grid(div_up(nv, 128));
   if (soup->fp64)
     k_dcd_pt<double><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->triangles, soup->body,
-                                                        (const float4*)bvh->nodes, soup->n_tris, query_order, nv,
+                                                        (const float4*)bvh->wide, soup->n_tris, query_order, nv,
                                                         thickness, query_pad, exclude_same_body, *out, status);
   else
     k_dcd_pt<float><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->triangles, soup->body,
-                                                       (const float4*)bvh->nodes, soup->n_tris, query_order, nv,
+                                                       (const float4*)bvh->wide, soup->n_tris, query_order, nv,
                                                        thickness, query_pad, exclude_same_body, *out, status);
   return check_launch("ipcb_dcd_pt");
 }

@@ -169,6 +169,47 @@ __global__ void k_refit(const float* __restrict__ lo, const float* __restrict__ 
   }
 }
 
+// Gather the 4-wide view (see traverse4) from the refit binary nodes.
+__global__ void k_widen(const float4* __restrict__ nodes, int n_int, float4* __restrict__ wide) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n_int) return;
+  float lo[4][3], hi[4][3];
+  int code[4];
+  int m = 0;
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    float4 slo = __ldcg(nodes + 4 * b + 2 * side), shi = __ldcg(nodes + 4 * b + 2 * side + 1);
+    int c = __float_as_int(slo.w);
+    if (c < 0) {
+      lo[m][0] = slo.x; lo[m][1] = slo.y; lo[m][2] = slo.z;
+      hi[m][0] = shi.x; hi[m][1] = shi.y; hi[m][2] = shi.z;
+      code[m++] = c;
+    } else {
+#pragma unroll
+      for (int s2 = 0; s2 < 2; ++s2) {
+        float4 glo = __ldcg(nodes + 4 * c + 2 * s2), ghi = __ldcg(nodes + 4 * c + 2 * s2 + 1);
+        lo[m][0] = glo.x; lo[m][1] = glo.y; lo[m][2] = glo.z;
+        hi[m][0] = ghi.x; hi[m][1] = ghi.y; hi[m][2] = ghi.z;
+        code[m++] = __float_as_int(glo.w);
+      }
+    }
+  }
+  for (int k = m; k < 4; ++k) {
+    lo[k][0] = lo[k][1] = lo[k][2] = 3.4e38f;
+    hi[k][0] = hi[k][1] = hi[k][2] = -3.4e38f;
+    code[k] = -1;
+  }
+  float4* w = wide + 8 * b;
+  w[0] = make_float4(lo[0][0], lo[1][0], lo[2][0], lo[3][0]);
+  w[1] = make_float4(lo[0][1], lo[1][1], lo[2][1], lo[3][1]);
+  w[2] = make_float4(lo[0][2], lo[1][2], lo[2][2], lo[3][2]);
+  w[3] = make_float4(hi[0][0], hi[1][0], hi[2][0], hi[3][0]);
+  w[4] = make_float4(hi[0][1], hi[1][1], hi[2][1], hi[3][1]);
+  w[5] = make_float4(hi[0][2], hi[1][2], hi[2][2], hi[3][2]);
+  *reinterpret_cast<int4*>(w + 6) = make_int4(code[0], code[1], code[2], code[3]);
+  w[7] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
 inline size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 }  // namespace
@@ -205,7 +246,7 @@ size_t ipcb_lbvh_bytes(int capacity) {
   if (capacity < 1) capacity = 1;
   size_t c = (size_t)capacity;
   size_t nn = c > 1 ? c - 1 : 1;
-  return al256(nn * 4 * 16) + al256(2 * c * 4) + al256(c * 4) + al256(c * 4) + al256(c * 4);
+  return al256(nn * 4 * 16) + al256(2 * c * 4) + al256(c * 4) + al256(c * 4) + al256(c * 4) + al256(nn * 8 * 16);
 }
 
 int ipcb_lbvh_bind(ipcb_lbvh* bvh, void* mem, int capacity) {
@@ -224,6 +265,8 @@ int ipcb_lbvh_bind(ipcb_lbvh* bvh, void* mem, int capacity) {
   bvh->keys = (unsigned*)p;
   p += al256(c * 4);
   bvh->flags = (unsigned*)p;
+  p += al256(c * 4);
+  bvh->wide = p;
   return IPCB_OK;
 }
 
@@ -250,6 +293,8 @@ int ipcb_lbvh_build(ipcb_lbvh* bvh, const float* lower, const float* upper, int 
                                                   bvh->capacity);
   k_refit<<<div_up(n, 256), 256, 0, st>>>(lower, upper, n, bvh->sorted, bvh->parent, bvh->capacity,
                                            (float4*)bvh->nodes, bvh->flags);
+  int n_int = n > 1 ? n - 1 : 1;
+  k_widen<<<div_up(n_int, 256), 256, 0, st>>>((const float4*)bvh->nodes, n_int, (float4*)bvh->wide);
   return check_launch("ipcb_lbvh_build");
 }
 
@@ -259,6 +304,8 @@ int ipcb_lbvh_refit(const ipcb_lbvh* bvh, const float* lower, const float* upper
   if (!lower || !upper) return IPCB_E_ARG;
   k_refit<<<div_up(bvh->n, 256), 256, 0, (cudaStream_t)s>>>(lower, upper, bvh->n, bvh->sorted, bvh->parent,
                                                             bvh->capacity, (float4*)bvh->nodes, bvh->flags);
+  int n_int = bvh->n > 1 ? bvh->n - 1 : 1;
+  k_widen<<<div_up(n_int, 256), 256, 0, (cudaStream_t)s>>>((const float4*)bvh->nodes, n_int, (float4*)bvh->wide);
   return check_launch("ipcb_lbvh_refit");
 }
 

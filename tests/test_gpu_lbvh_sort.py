@@ -70,6 +70,39 @@ def _check_tree(bvh, lo, hi):
     if n >= 2:
         visit(0)
         assert np.all(seen == 1)
+    _check_wide(bvh, lo, hi)
+
+
+def _check_wide(bvh, lo, hi):
+    """4-wide view: from wide node 0 every leaf is reached exactly once and
+    each slot box is the union of the leaves below it."""
+    import torch
+
+    n = lo.shape[0]
+    m = max(n - 1, 1)
+    W = bvh._view(bvh.c.wide, 32 * m, torch.float32).view(m, 8, 4).cpu().numpy()
+    Wi = W.view(np.int32)
+    seen = np.zeros(n, dtype=np.int64)
+
+    def visit(node):
+        leaves = []
+        for k in range(4):
+            blo = np.array([W[node, 0, k], W[node, 1, k], W[node, 2, k]])
+            bhi = np.array([W[node, 3, k], W[node, 4, k], W[node, 5, k]])
+            c = int(Wi[node, 6, k])
+            if blo[0] > bhi[0]:  # empty slot
+                continue
+            if c < 0:
+                seen[~c] += 1
+                sub = [~c]
+            else:
+                sub = visit(c)
+            assert np.array_equal(blo, lo[sub].min(axis=0)) and np.array_equal(bhi, hi[sub].max(axis=0))
+            leaves += sub
+        return leaves
+
+    visit(0)
+    assert np.all(seen == 1)
 
 
 @pytest.mark.parametrize("n", [2, 3, 17, 4096])
