@@ -180,6 +180,19 @@ int ipcb_collision_time(int kind, int n, const double* p_t0, const double* p_t1,
 int ipcb_cubic_roots(int n, const double* coef, double x0, double x1, double* roots, int* n_roots, int* status,
                      ipcb_stream s);
 
+/* ---- FEM elastic term (fem/fem.py:22-34 compute_Dm, 139-203 tet_kernel_sparse;
+ *      time_integrator_base.py:124-137 compute_Psi) ----
+ * material: 0 stable Neo-Hookean (fem/snh.py), 1 Neo-Hookean (fem/neo_hookean.py),
+ * 2 St. Venant-Kirchhoff (fem/stvk.py); Lame mu, lam.  tets int32[4n].
+ * rest: Bm = Dm^-1 (scalar[9n] row-major), W = |det Dm|/6.
+ * hessian: 16 triplets per tet at tet*16 + i*4 + j (K_ij, not projected,
+ * as the reference) and the nodal forces added to b.  energy += sum W psi(F). */
+int ipcb_tet_rest(int fp64, const void* xcs, const int* tets, int n_tets, void* Bm, void* W, ipcb_stream s);
+int ipcb_tet_hessian(int material, int fp64, const void* x, const int* tets, int n_tets, const void* Bm, const void* W,
+                     double mu, double lam, int* rows, int* cols, void* vals, void* b, ipcb_stream s);
+int ipcb_tet_energy(int material, int fp64, const void* x, const int* tets, int n_tets, const void* Bm, const void* W,
+                    double mu, double lam, double* energy, ipcb_stream s);
+
 /* ---- BSR assembly (warp.sparse.bsr_from_triplets, dynamic_contacts.py:290-297) ----
  * Canonical 3x3-block CSR from triplets: sort by (row, col), sum duplicates,
  * drop triplets whose 9 values are all zero.  offsets int32[nrow+1],

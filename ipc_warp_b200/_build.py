@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(LIB_DIR, "libipcb200.so")
 OBJ_DIR = os.path.join(HERE, "csrc", "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["lbvh.cu", "dcd.cu", "narrow.cu", "ccd.cu", "bsr.cu", "contact_bsr.cu", "noalloc.cu"]
+SOURCES = ["lbvh.cu", "dcd.cu", "narrow.cu", "ccd.cu", "bsr.cu", "contact_bsr.cu", "fem.cu", "noalloc.cu"]
 NOFMAD = {"ccd.cu"}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -68,10 +68,12 @@ class ContactBarrierMixin(ContactSolverBase):
     def line_search_upper_bound(self):
         return self.collision_free_step(self.states.dx)
 
-    def compute_contact_hessian(self, detect: bool = True) -> BsrMatrix:
+    def compute_contact_hessian(self, detect: bool = True, build_bsr: bool = True) -> BsrMatrix | None:
         """The contact block of compute_A (dynamic_contacts.py:275-297):
         detect, then 16 triplets per record and b += force; returns the
-        canonical BSR of the contact Hessian (not yet scaled by h^2)."""
+        canonical BSR of the contact Hessian (not yet scaled by h^2), or None
+        with ``build_bsr=False`` (the caller assembles ``collision_triplets``
+        together with its own terms)."""
         if detect:
             with self.profile_timer("detect collision"):
                 self.detect_collision()
@@ -87,6 +89,8 @@ class ContactBarrierMixin(ContactSolverBase):
                 contact_hessian_ee(states, self.soup, self.contacts_new, t, self.b, kappa, n=n_ee)
             if n_pt:
                 contact_hessian_pt(states, self.soup, self.contacts_pt, t, self.b, n_ee, kappa, n=n_pt)
+            if not build_bsr:
+                return None
             prev = getattr(self, "collision_hessian", None)
             H, status = contact_bsr(self.contacts_new, n_ee, self.contacts_pt, n_pt, self.soup.n_verts, t, out=prev)
             if status & 4:  # a row with too many distinct columns: generic assembly

@@ -1,0 +1,270 @@
+"""Implicit-Euler Newton integrator with IPC contact: the time integrator of
+time_integrator_base.py:375-546 (``RodBCBase.step``, ``compute_A``,
+``compute_rhs``, ``solve``, ``line_search``) and the contact parts of
+``RodComplexBC`` (dynamic_contacts.py:249-308), on the GPU kernels of this
+package.
+
+Per Newton iteration:
+  A  = M + h^2 (K + C) + h^2 k_att I_fixed          (BSR, one assembly)
+  b  = -h^2 (f_elastic + f_contact) + M (x - x~) + h^2 k_att (x - x_target)_fixed
+  A dx = b  by PCG (relative residual ``tol``, ``maxiter``; block-Jacobi or a
+            learned preconditioner), direct solve when PCG misses the tolerance
+  x -= alpha dx, alpha from the CCD bound and backtracking on the total energy
+  E = h^2 Psi + 1/2 |x - x~|_M^2 + h^2 B_contact + 1/2 h^2 k_att |x - x_target|^2
+(energies and the convergence norm max|dx| in double).  x~ = x0 + h xdot + h^2 g.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _native as N
+from . import contact as contact_mod
+from .bsr import BsrMatrix, Triplets, bsr_from_triplets, bsr_mv
+from .contact import Soup
+from .dynamic_contacts import ContactBarrierMixin
+
+MATERIALS = {"snh": 0, "neo_hookean": 1, "nh": 1, "stvk": 2}
+
+
+def lame(E: float, nu: float):
+    return E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu))
+
+
+@dataclass
+class NewtonState:
+    """fem/params.py:43-50."""
+    x: torch.Tensor
+    x0: torch.Tensor
+    dx: torch.Tensor
+    xdot: torch.Tensor
+
+
+@dataclass
+class StepStats:
+    newton_iterations: int = 0
+    pcg_iterations: list = field(default_factory=list)
+    fallbacks: int = 0
+    alphas: list = field(default_factory=list)
+    energies: list = field(default_factory=list)
+    norms: list = field(default_factory=list)
+
+
+class BlockJacobi:
+    """Inverse of the 3x3 diagonal blocks of a BSR matrix."""
+
+    def __init__(self, A: BsrMatrix):
+        nnz = A.nnz_sync()
+        rows = torch.repeat_interleave(torch.arange(A.nrow, device=A.device),
+                                       (A.offsets[1:] - A.offsets[:-1]).long())
+        diag = rows == A.columns[:nnz].long()
+        D = torch.zeros((A.nrow, 3, 3), dtype=torch.float64, device=A.device)
+        D[rows[diag]] = A.values[:nnz][diag].double()
+        eye = torch.eye(3, dtype=torch.float64, device=A.device)
+        D = torch.where(D.abs().sum(dim=(1, 2), keepdim=True) > 0, D, eye)
+        self.Dinv = torch.linalg.inv(D).to(A.dtype)
+
+    def __call__(self, r: torch.Tensor) -> torch.Tensor:
+        return torch.bmm(self.Dinv, r.unsqueeze(-1)).squeeze(-1)
+
+
+def pcg(A: BsrMatrix, b: torch.Tensor, precond, tol: float = 1e-6, maxiter: int = 200):
+    """Preconditioned CG on the (V, 3) block vector b; dot products in double.
+    Returns (x, iterations, relative residual)."""
+    x = torch.zeros_like(b)
+    r = b.clone()
+    bn = float(torch.linalg.vector_norm(b.double()))
+    if bn == 0.0:
+        return x, 0, 0.0
+    z = precond(r)
+    p = z.clone()
+    rz = float((r.double() * z.double()).sum())
+    Ap = torch.empty_like(b)
+    rel = 1.0
+    for it in range(1, maxiter + 1):
+        bsr_mv(A, p, Ap)
+        pAp = float((p.double() * Ap.double()).sum())
+        if not (pAp > 0.0):
+            return x, it, float("nan")
+        a = rz / pAp
+        x.add_(p, alpha=a)
+        r.sub_(Ap, alpha=a)
+        rel = float(torch.linalg.vector_norm(r.double())) / bn
+        if rel <= tol:
+            return x, it, rel
+        z = precond(r)
+        rz_new = float((r.double() * z.double()).sum())
+        p.mul_(rz_new / rz).add_(z)
+        rz = rz_new
+    return x, maxiter, rel
+
+
+class FEMContactSolver(ContactBarrierMixin):
+    """Deformable bodies (tet FEM) with IPC contact: RodComplexBC on the GPU."""
+
+    def __init__(self, scene, *, material: str = "neo_hookean", E: float = 1e5, nu: float = 0.4, rho: float = 1000.0,
+                 gravity=(0.0, -9.8, 0.0), h: float = 1e-2, fixed: np.ndarray | None = None,
+                 attachment_stiffness: float = 1e11, dtype=torch.float32, device="cuda", vel_tol: float = 5e-2,
+                 max_newton: int = 100, tol: float = 1e-4, maxiter: int = 200, exclude_same_body: bool = False):
+        self.h = float(h)
+        self.material = MATERIALS[material]
+        self.mu, self.lam = lame(E, nu)
+        self.dtype = dtype
+        self.device = torch.device(device)
+        self.vel_tol, self.max_newton = vel_tol, max_newton
+        self.tol, self.maxiter = tol, maxiter
+        self.contact_stiffness = float(scene.kappa)
+        contact_mod._thickness = 0.5 * scene.dhat
+        contact_mod.buffer = 0.5 * scene.dhat
+        self.soup = Soup.from_numpy(scene.x, scene.edges, scene.triangles, scene.body, xcs=scene.xcs,
+                                    device=self.device, dtype=dtype)
+        V = self.soup.n_verts
+        self.tets = torch.as_tensor(scene.tets, dtype=torch.int32, device=self.device).contiguous()
+        self.n_tets = self.tets.shape[0]
+        self.Bm = torch.zeros((self.n_tets, 3, 3), dtype=dtype, device=self.device)
+        self.W = torch.zeros(self.n_tets, dtype=dtype, device=self.device)
+        fp64 = int(dtype == torch.float64)
+        N.call("ipcb_tet_rest", fp64, N.ptr(self.soup.xcs), N.ptr(self.tets), self.n_tets, N.ptr(self.Bm), N.ptr(self.W),
+               N.stream_handle())
+        # lumped mass: rho * volume / 4 per tet vertex
+        w = self.W.double().cpu().numpy()
+        m = np.zeros(V)
+        np.add.at(m, scene.tets.reshape(-1), np.repeat(rho * w / 4.0, 4))
+        m[m == 0] = rho * (w.mean() if len(w) else 1.0) / 4.0
+        self.mass = torch.tensor(m, dtype=torch.float64, device=self.device)
+        self.gravity = torch.tensor(gravity, dtype=torch.float64, device=self.device)
+        x = self.soup.x_transformed
+        self.states = NewtonState(x=x, x0=x.clone(), dx=torch.zeros_like(x), xdot=torch.zeros_like(x))
+        self.b = torch.zeros_like(x)
+        self.fixed = torch.zeros(V, dtype=torch.bool, device=self.device)
+        if fixed is not None:
+            self.fixed = torch.as_tensor(fixed, dtype=torch.bool, device=self.device)
+        self.x_target = self.soup.xcs.clone()
+        self.k_att = float(attachment_stiffness)
+        ContactBarrierMixin.__init__(self)
+        self.disable_self_collision = exclude_same_body
+        self._elastic = Triplets.zeros(16 * self.n_tets, dtype, self.device)
+        self.precond_factory = BlockJacobi
+        self.direct_solver = None  # callable(A, b) -> x, set to use a direct fallback
+        self.frame = 0
+        self.stats = StepStats()
+
+    # ----------------------------------------------------------- energies
+    def x_tilde(self) -> torch.Tensor:
+        h = self.h
+        return self.states.x0.double() + h * self.states.xdot.double() + h * h * self.gravity
+
+    def elastic_energy(self) -> float:
+        e = torch.zeros(1, dtype=torch.float64, device=self.device)
+        N.call("ipcb_tet_energy", self.material, int(self.dtype == torch.float64), N.ptr(self.states.x),
+               N.ptr(self.tets), self.n_tets, N.ptr(self.Bm), N.ptr(self.W), self.mu, self.lam, N.ptr(e),
+               N.stream_handle())
+        return float(e.item())
+
+    def total_energy(self) -> float:
+        """h^2 Psi + inertia + h^2 contact + attachment, in double (line search)."""
+        h2 = self.h * self.h
+        x = self.states.x.double()
+        d = x - self.x_tilde()
+        inertia = 0.5 * float((self.mass[:, None] * d * d).sum())
+        att = 0.0
+        if bool(self.fixed.any()):
+            r = (x - self.x_target.double())[self.fixed]
+            att = 0.5 * self.k_att * h2 * float((r * r).sum())
+        return h2 * self.elastic_energy() + inertia + self.compute_collision_energy() + att
+
+    # ------------------------------------------------------------ system
+    def compute_A(self) -> BsrMatrix:
+        """time_integrator_base.py:406-426 + dynamic_contacts.py:275-297."""
+        h2 = self.h * self.h
+        V = self.soup.n_verts
+        self.b.zero_()
+        t = self._elastic
+        N.call("ipcb_tet_hessian", self.material, int(self.dtype == torch.float64), N.ptr(self.states.x),
+               N.ptr(self.tets), self.n_tets, N.ptr(self.Bm), N.ptr(self.W), self.mu, self.lam, N.ptr(t.rows),
+               N.ptr(t.cols), N.ptr(t.vals), N.ptr(self.b), N.stream_handle())
+        self.compute_contact_hessian(detect=True, build_bsr=False)
+        nc = 16 * (self.n_contacts + self.n_contacts_pt)
+        ct = self.collision_triplets
+        idx = torch.arange(V, dtype=torch.int32, device=self.device)
+        eye = torch.eye(3, dtype=self.dtype, device=self.device)
+        diag = self.mass.to(self.dtype)[:, None, None] * eye
+        if bool(self.fixed.any()):
+            diag = diag + (h2 * self.k_att) * self.fixed.to(self.dtype)[:, None, None] * eye
+        rows = torch.cat([idx, t.rows, ct.rows[:nc]])
+        cols = torch.cat([idx, t.cols, ct.cols[:nc]])
+        vals = torch.cat([diag, t.vals * h2, ct.vals[:nc] * h2])
+        self.A = bsr_from_triplets(V, V, rows, cols, vals, out=getattr(self, "A", None))
+        return self.A
+
+    def compute_rhs(self) -> torch.Tensor:
+        """time_integrator_base.py:82-91,428-438: gradient of the total energy."""
+        h2 = self.h * self.h
+        x = self.states.x.double()
+        g = -h2 * self.b.double() + self.mass[:, None] * (x - self.x_tilde())
+        if bool(self.fixed.any()):
+            g = g + (h2 * self.k_att) * self.fixed.double()[:, None] * (x - self.x_target.double())
+        self.rhs = g.to(self.dtype)
+        return self.rhs
+
+    def solve(self) -> torch.Tensor:
+        P = self.precond_factory(self.A)
+        dx, its, rel = pcg(self.A, self.rhs, P, self.tol, self.maxiter)
+        self.stats.pcg_iterations.append(its)
+        if not (rel <= self.tol) and self.direct_solver is not None:
+            dx = self.direct_solver(self.A, self.rhs)
+            self.stats.fallbacks += 1
+        self.states.dx = dx
+        return dx
+
+    def line_search(self) -> float:
+        """time_integrator_base.py:514-546 with the CCD bound."""
+        x_tmp = self.states.x.clone()
+        E0 = self.total_energy()
+        ub = self.collision_free_step(self.states.dx)
+        alpha = ub
+        accepted = False
+        E1 = math.inf
+        eps = 1.1920928955078125e-7 if self.dtype == torch.float32 else 2.220446049250313e-16
+        for _ in range(64):
+            self.states.x.copy_(x_tmp - alpha * self.states.dx)
+            E1 = self.total_energy()
+            if math.isfinite(E1) and E1 < E0:
+                accepted = True
+                break
+            alpha *= 0.5
+            if alpha <= eps * max(1.0, ub):
+                break
+        if not accepted:
+            self.states.x.copy_(x_tmp)
+            alpha = 0.0
+        self.stats.energies.append((E0, E1))
+        return alpha
+
+    def newton_iteration(self) -> tuple[float, float]:
+        self.compute_A()
+        self.compute_rhs()
+        self.solve()
+        alpha = self.line_search()
+        norm = float(self.states.dx.double().abs().max()) if alpha > 0 else 0.0
+        return alpha, norm
+
+    def step(self) -> StepStats:
+        """time_integrator_base.py:375-401."""
+        self.stats = StepStats()
+        for it in range(self.max_newton):
+            alpha, norm = self.newton_iteration()
+            self.stats.newton_iterations = it + 1
+            self.stats.alphas.append(alpha)
+            self.stats.norms.append(norm)
+            if alpha == 0.0 or norm <= self.vel_tol * self.h:
+                break
+        x = self.states.x
+        self.states.xdot.copy_((x - self.states.x0) / self.h)
+        self.states.x0.copy_(x)
+        self.frame += 1
+        return self.stats

@@ -977,6 +977,106 @@ double scene_toi(int nv, const S* x0, const S* x1, int ne, const int* edges, int
   return b;
 }
 
+
+// ------------------------------------------------------------------- FEM
+// fem/fem.py:22-34, 139-203; fem/snh.py, neo_hookean.py, stvk.py (double)
+struct M3d {
+  double a[3][3];
+};
+M3d mz() { M3d m; std::memset(&m, 0, sizeof(m)); return m; }
+M3d mm(const M3d& x, const M3d& y) {
+  M3d r = mz();
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) for (int k = 0; k < 3; ++k) r.a[i][j] += x.a[i][k] * y.a[k][j];
+  return r;
+}
+M3d mt(const M3d& x) { M3d r; for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) r.a[i][j] = x.a[j][i]; return r; }
+M3d lin(double a, const M3d& x, double b, const M3d& y) {
+  M3d r; for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) r.a[i][j] = a * x.a[i][j] + b * y.a[i][j]; return r;
+}
+double dd(const M3d& x, const M3d& y) { double s = 0; for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) s += x.a[i][j] * y.a[i][j]; return s; }
+double det(const M3d& m) {
+  return m.a[0][0] * (m.a[1][1] * m.a[2][2] - m.a[1][2] * m.a[2][1]) - m.a[0][1] * (m.a[1][0] * m.a[2][2] - m.a[1][2] * m.a[2][0]) +
+         m.a[0][2] * (m.a[1][0] * m.a[2][1] - m.a[1][1] * m.a[2][0]);
+}
+M3d inv(const M3d& m) {
+  double id = 1.0 / det(m);
+  M3d r;
+  r.a[0][0] = (m.a[1][1] * m.a[2][2] - m.a[1][2] * m.a[2][1]) * id; r.a[0][1] = (m.a[0][2] * m.a[2][1] - m.a[0][1] * m.a[2][2]) * id;
+  r.a[0][2] = (m.a[0][1] * m.a[1][2] - m.a[0][2] * m.a[1][1]) * id; r.a[1][0] = (m.a[1][2] * m.a[2][0] - m.a[1][0] * m.a[2][2]) * id;
+  r.a[1][1] = (m.a[0][0] * m.a[2][2] - m.a[0][2] * m.a[2][0]) * id; r.a[1][2] = (m.a[0][2] * m.a[1][0] - m.a[0][0] * m.a[1][2]) * id;
+  r.a[2][0] = (m.a[1][0] * m.a[2][1] - m.a[1][1] * m.a[2][0]) * id; r.a[2][1] = (m.a[0][1] * m.a[2][0] - m.a[0][0] * m.a[2][1]) * id;
+  r.a[2][2] = (m.a[0][0] * m.a[1][1] - m.a[0][1] * m.a[1][0]) * id;
+  return r;
+}
+V3<double> colm(const M3d& m, int j) { return mk(m.a[0][j], m.a[1][j], m.a[2][j]); }
+M3d cols3(V3<double> c0, V3<double> c1, V3<double> c2) {
+  M3d r;
+  double v[3][3] = {{c0.x, c1.x, c2.x}, {c0.y, c1.y, c2.y}, {c0.z, c1.z, c2.z}};
+  std::memcpy(r.a, v, sizeof(v));
+  return r;
+}
+M3d cof(const M3d& F) {
+  V3<double> f0 = colm(F, 0), f1 = colm(F, 1), f2 = colm(F, 2);
+  return cols3(cross(f1, f2), cross(f2, f0), cross(f0, f1));
+}
+M3d green(const M3d& F) {
+  M3d E = mm(mt(F), F);
+  for (int i = 0; i < 3; ++i) E.a[i][i] -= 1.0;
+  return lin(0.5, E, 0.0, E);
+}
+double fem_psi(int mat, const M3d& F, double mu, double lam) {
+  if (mat == 0) {
+    double smu = 4.0 / 3.0 * mu, slam = lam + 5.0 / 6.0 * mu, alpha = 1.0 + 0.75 * smu / slam;
+    double Ic = dd(F, F), Ja = det(F) - alpha;
+    return 0.5 * (slam * Ja * Ja + smu * (Ic - 3.0) - smu * std::log(Ic + 1.0));
+  }
+  if (mat == 1) {
+    double lJ = std::log(det(F));
+    return mu * 0.5 * (dd(F, F) - 3.0) - mu * lJ + lam * 0.5 * lJ * lJ;
+  }
+  M3d E = green(F);
+  double tr = E.a[0][0] + E.a[1][1] + E.a[2][2];
+  return mu * dd(E, E) + lam * 0.5 * tr * tr;
+}
+M3d fem_pk1(int mat, const M3d& F, double mu, double lam) {
+  if (mat == 0) {
+    double smu = 4.0 / 3.0 * mu, slam = lam + 5.0 / 6.0 * mu, alpha = 1.0 + 0.75 * smu / slam;
+    double Ic = dd(F, F);
+    return lin(smu * (1.0 - 1.0 / (Ic + 1.0)), F, slam * (det(F) - alpha), cof(F));
+  }
+  if (mat == 1) {
+    M3d FiT = mt(inv(F));
+    return lin(mu, lin(1.0, F, -1.0, FiT), lam * std::log(det(F)), FiT);
+  }
+  M3d E = green(F);
+  double tr = E.a[0][0] + E.a[1][1] + E.a[2][2];
+  M3d S = lin(2.0 * mu, E, 0.0, E);
+  for (int i = 0; i < 3; ++i) S.a[i][i] += lam * tr;
+  return mm(F, S);
+}
+M3d fem_tangent(int mat, const M3d& F, const M3d& dF, double mu, double lam) {
+  if (mat == 0) {
+    double smu = 4.0 / 3.0 * mu, slam = lam + 5.0 / 6.0 * mu, alpha = 1.0 + 0.75 * smu / slam;
+    M3d C = cof(F);
+    double Ic1 = dd(F, F) + 1.0, dIc = 2.0 * dd(F, dF);
+    V3<double> f0 = colm(F, 0), f1 = colm(F, 1), f2 = colm(F, 2), d0 = colm(dF, 0), d1 = colm(dF, 1), d2 = colm(dF, 2);
+    M3d dC = cols3(cross(d1, f2) + cross(f1, d2), cross(d2, f0) + cross(f2, d0), cross(d0, f1) + cross(f0, d1));
+    M3d r = lin(smu * (1.0 - 1.0 / Ic1), dF, smu * dIc / (Ic1 * Ic1), F);
+    r = lin(1.0, r, slam * dd(C, dF), C);
+    return lin(1.0, r, slam * (det(F) - alpha), dC);
+  }
+  if (mat == 1) {
+    M3d Fi = inv(F), FiT = mt(Fi), B = mm(Fi, dF);
+    double lJ = std::log(det(F)), trB = B.a[0][0] + B.a[1][1] + B.a[2][2];
+    return lin(1.0, lin(mu, dF, mu - lam * lJ, mm(mm(FiT, mt(dF)), FiT)), lam * trB, FiT);
+  }
+  M3d E = green(F), dE = mm(mt(dF), F);
+  dE = lin(0.5, dE, 0.5, mt(dE));
+  double trE = E.a[0][0] + E.a[1][1] + E.a[2][2], trdE = dE.a[0][0] + dE.a[1][1] + dE.a[2][2];
+  M3d S = lin(2.0 * mu, E, 0.0, E), dS = lin(2.0 * mu, dE, 0.0, dE);
+  for (int i = 0; i < 3; ++i) { S.a[i][i] += lam * trE; dS.a[i][i] += lam * trdE; }
+  return lin(1.0, mm(dF, S), 1.0, mm(F, dS));
+}
 }  // namespace
 
 // ===================================================================== C ABI
@@ -1140,6 +1240,38 @@ double ora_scene_toi(int fp64, int nv, const void* x0, const void* x1, int ne, c
                   : scene_toi<float>(nv, (const float*)x0, (const float*)x1, ne, edges, nt, tris, body, exclude, st);
   if (status) *status = st;
   return t;
+}
+
+
+// Elastic forces (V x 3, added), 16 blocks per tet (n x 16 x 9) and energy
+// sum W psi for positions x and rest positions xcs (both double).
+double ora_tet(int mat, int nv, const double* x, const double* xcs, int nt, const int* tets, double mu, double lam,
+               double* force, double* blocks) {
+  (void)nv;
+  double energy = 0.0;
+  for (int e = 0; e < nt; ++e) {
+    const int* t = tets + 4 * e;
+    M3d Dm = cols3(load3(xcs, t[0]) - load3(xcs, t[3]), load3(xcs, t[1]) - load3(xcs, t[3]), load3(xcs, t[2]) - load3(xcs, t[3]));
+    M3d B = inv(Dm);
+    double w = std::fabs(det(Dm)) / 6.0;
+    M3d F = mm(cols3(load3(x, t[0]) - load3(x, t[3]), load3(x, t[1]) - load3(x, t[3]), load3(x, t[2]) - load3(x, t[3])), B);
+    energy += w * fem_psi(mat, F, mu, lam);
+    M3d H = lin(-w, mm(fem_pk1(mat, F, mu, lam), mt(B)), 0.0, F);
+    for (int i = 0; i < 4; ++i)
+      for (int l = 0; l < 3; ++l)
+        force[3 * t[i] + l] += i < 3 ? H.a[l][i] : -(H.a[l][0] + H.a[l][1] + H.a[l][2]);
+    for (int j = 0; j < 4; ++j)
+      for (int k = 0; k < 3; ++k) {
+        M3d dDs = mz();
+        if (j < 3) dDs.a[k][j] = -1.0;
+        else dDs.a[k][0] = dDs.a[k][1] = dDs.a[k][2] = 1.0;
+        M3d dH = lin(-w, mm(fem_tangent(mat, F, mm(dDs, B), mu, lam), mt(B)), 0.0, F);
+        for (int i = 0; i < 4; ++i)
+          for (int l = 0; l < 3; ++l)
+            blocks[((size_t)e * 16 + i * 4 + j) * 9 + 3 * l + k] = i < 3 ? dH.a[l][i] : -(dH.a[l][0] + dH.a[l][1] + dH.a[l][2]);
+      }
+  }
+  return energy;
 }
 
 }  // extern "C"

@@ -155,3 +155,17 @@ def scene_toi(x0, x1, edges, triangles, body, exclude_same_body=False, fp64=Fals
     t = f(int(fp64), x0.shape[0], _p(x0), _p(x1), edges.size // 2, _p(edges), triangles.size // 3, _p(triangles),
           _p(body), int(exclude_same_body), _p(st))
     return float(t), int(st[0])
+
+
+def tet(material: int, x, xcs, tets, mu, lam):
+    """Elastic force (V,3), per-tet 16 blocks (n,16,3,3) and energy (double)."""
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
+    xcs = np.ascontiguousarray(xcs, dtype=np.float64).reshape(-1, 3)
+    tets = _i32(tets).reshape(-1, 4)
+    force = np.zeros_like(x)
+    blocks = np.zeros((tets.shape[0], 16, 3, 3))
+    f = lib().ora_tet
+    f.restype = ctypes.c_double
+    e = f(int(material), x.shape[0], _p(x), _p(xcs), tets.shape[0], _p(tets), ctypes.c_double(mu),
+          ctypes.c_double(lam), _p(force), _p(blocks))
+    return force, blocks, float(e)
