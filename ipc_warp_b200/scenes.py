@@ -166,14 +166,17 @@ def assemble(meshes, name, dhat, kappa, meta=None) -> Scene:
 
 
 def two_cubes(n: int = 8, gap: float = 1e-3, angle_deg: float = 15.0, jitter: float = 1e-5,
-              seed: int = 0, dhat: float = 1e-3, kappa: float = 1e4) -> Scene:
-    """Two tetrahedralised unit cubes; the upper one is rotated about z and its
-    lowest vertex sits ``gap`` above the lower cube's top face (y-up)."""
+              seed: int = 0, dhat: float = 1e-3, kappa: float = 1e4, tilt_deg: float = 0.0) -> Scene:
+    """Two tetrahedralised unit cubes; the upper one is rotated about z (then
+    tilted about x by ``tilt_deg``) and its lowest vertex sits ``gap`` above
+    the lower cube's top face (y-up)."""
     rng = np.random.default_rng(seed)
     lo = hex_grid_tets(n, n, n)
     up = hex_grid_tets(n, n, n)
     c = np.array([0.5, 0.5, 0.5])
-    up.x = (up.x - c) @ rot_z(angle_deg).T + c
+    t = np.radians(tilt_deg)
+    rot_x = np.array([[1.0, 0.0, 0.0], [0.0, np.cos(t), -np.sin(t)], [0.0, np.sin(t), np.cos(t)]])
+    up.x = (up.x - c) @ (rot_x @ rot_z(angle_deg)).T + c
     up.x[:, 1] += 1.0 + gap - up.x[:, 1].min()
     sc = assemble([lo, up], f"two_cubes_{n}", dhat, kappa, {"gap": gap, "angle_deg": angle_deg})
     sc.x += rng.uniform(-jitter, jitter, size=sc.x.shape)

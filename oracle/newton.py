@@ -132,8 +132,8 @@ def line_search(p: Problem, x, dx, xt):
     """time_integrator_base.py:514-546 with the CCD bound of
     contact.py:539-585 (0.9 toi when toi < 1)."""
     E0 = energy(p, x, xt)
-    x32 = np.asarray(x, dtype=np.float32)
-    toi, _ = po.scene_toi(x32, (x - dx).astype(np.float32), p.edges, p.triangles, p.body, p.exclude_same_body)
+    toi, _ = po.scene_toi(np.asarray(x, p.dtype), np.asarray(x - dx, p.dtype), p.edges, p.triangles, p.body,
+                          p.exclude_same_body, fp64=p.fp64)
     ub = 0.9 * toi if toi < 1.0 else 1.0
     alpha = ub
     eps = float(np.finfo(p.dtype).eps)

@@ -23,15 +23,16 @@ def _fixed(sc):
     return sc.xcs[:, 1] <= sc.xcs[:, 1].min() + 1e-9
 
 
-def _solver(sc, dtype, material="neo_hookean", **kw):
-    return FEMContactSolver(sc, material=material, E=E_YOUNG, nu=NU, rho=RHO, h=H, fixed=_fixed(sc), dtype=dtype,
-                            **kw)
+def _solver(sc, dtype, material="neo_hookean", E=E_YOUNG, **kw):
+    return FEMContactSolver(sc, material=material, E=E, nu=NU, rho=RHO, h=H, fixed=_fixed(sc), dtype=dtype, **kw)
 
 
-def _problem(sc, fp64, material=1):
-    mu, lam = lame(E_YOUNG, NU)
+def _problem(sc, fp64, material=1, E=E_YOUNG):
+    mu, lam = lame(E, NU)
     return on.Problem(sc.xcs, sc.tets, sc.edges.reshape(-1, 2), sc.triangles.reshape(-1, 3), sc.body,
-                      on.lumped_mass(sc.xcs, sc.tets, RHO), _fixed(sc), sc.xcs.copy(), material, mu, lam, sc.dhat,
+                      on.lumped_mass(sc.xcs, sc.tets, RHO), _fixed(sc),
+                      # the attachment targets are the rest positions in the solver's precision
+                      sc.xcs.astype(np.float64 if fp64 else np.float32).astype(np.float64), material, mu, lam, sc.dhat,
                       sc.kappa, H, 1e11, np.array([0.0, -9.8, 0.0]), fp64=fp64)
 
 
@@ -98,32 +99,68 @@ def test_pcg_direction_matches_direct_solve(cuda):
     assert np.abs(dx.cpu().numpy() - ref).max() <= 1e-7 * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("material", ["snh", "neo_hookean"])
+def test_newton_iteration_matches_oracle(cuda, material):
+    """One Newton iteration in double (matrix, tight PCG solve, CCD bound,
+    backtracking) lands on the oracle's iterate."""
+    sc = _scene(4e-4)
+    m = {"snh": 0, "neo_hookean": 1}[material]
+    s = _solver(sc, torch.float64, material, tol=1e-11, maxiter=5000)
+    x, xdot = _state(sc, seed=5)
+    s.states.x.copy_(torch.tensor(x))
+    s.states.x0.copy_(torch.tensor(sc.xcs))
+    s.states.xdot.copy_(torch.tensor(xdot))
+    alpha, norm = s.newton_iteration()
+    p = _problem(sc, True, m)
+    xt = on.x_tilde(p, sc.xcs, xdot)
+    g, A = on.gradient_hessian(p, x, xt)
+    import scipy.sparse.linalg as spla
+
+    dx = spla.spsolve(A.tocsc(), g.reshape(-1)).reshape(-1, 3)
+    xr, alpha_r, E0, E1 = on.line_search(p, x, dx, xt)
+    assert alpha_r > 0
+    assert abs(alpha - alpha_r) <= 2e-6 * alpha_r
+    assert abs(norm - np.abs(dx).max()) <= 1e-7 * norm
+    assert np.abs(s.states.x.cpu().numpy() - xr).max() <= 1e-8
+    assert abs(s.stats.energies[-1][0] - E0) <= 1e-10 * abs(E0)
+
+
+def _falling_scene():
+    """The upper cube, tilted so that a corner comes down first, falls at
+    0.1 m/s onto the lower one, whose bottom layer is fixed."""
+    return two_cubes(n=3, gap=2e-3, angle_deg=15.0, tilt_deg=7.0, jitter=0.0, seed=0, dhat=1e-3, kappa=1e11)
+
+
 @pytest.mark.parametrize("fp64", [False, True])
 def test_falling_cube_trajectory(cuda, fp64):
-    """The upper cube falls onto the fixed lower one: every accepted line
-    search lowers the total energy, the contact set is never crossed (finite
-    barrier energy at every frame) and, in double, the frames follow the CPU
-    Newton oracle."""
-    sc = _scene(2e-3)
+    """Every accepted line search lowers the total energy, the contact set is
+    never crossed (finite barrier energy at every frame) and, in double, the
+    frames follow the CPU Newton oracle."""
+    sc = _falling_scene()
     dt = torch.float64 if fp64 else torch.float32
+    E = 1e7
     vel_tol = 1e-4 if fp64 else 5e-2
-    s = _solver(sc, dt, vel_tol=vel_tol, tol=1e-10 if fp64 else 1e-4, maxiter=2000 if fp64 else 200)
-    p = _problem(sc, fp64)
-    xr, xdr = sc.xcs.copy(), np.zeros_like(sc.xcs)
+    s = _solver(sc, dt, E=E, vel_tol=vel_tol, tol=1e-10 if fp64 else 1e-4, maxiter=2000 if fp64 else 200)
+    v0 = np.zeros_like(sc.xcs)
+    v0[sc.body == 1, 1] = -0.1
+    s.states.xdot.copy_(torch.tensor(v0, dtype=dt))
+    p = _problem(sc, fp64, E=E)
+    xr, xdr = sc.xcs.copy(), v0.copy()
     had_contact = False
-    for frame in range(5):
+    for frame in range(8):
         st = s.step()
         assert st.newton_iterations < s.max_newton
         for (E0, E1), a in zip(st.energies, st.alphas):
             if a > 0:
                 assert E1 < E0
         x = s.states.x.double().cpu().numpy()
-        E = on.energy(p, x.astype(p.dtype), on.x_tilde(p, x, np.zeros_like(x)))
-        assert math.isfinite(E)
+        Ef = on.energy(p, x.astype(p.dtype), on.x_tilde(p, x, np.zeros_like(x)))
+        assert math.isfinite(Ef)
         had_contact |= (s.n_contacts + s.n_contacts_pt) > 0
         if fp64:
             xr, xdr, _ = on.step(p, xr, xdr, vel_tol=vel_tol)
-            assert np.abs(x - xr).max() <= 2e-5, frame
+            assert np.abs(x - xr).max() <= 1e-5, frame
     assert had_contact
-    # the upper body came down (separation is the finite barrier energy above)
+    # the corner came down onto the lower cube (separation is the finite
+    # barrier energy above)
     assert x[sc.body == 1, 1].min() < sc.xcs[sc.body == 1, 1].min() - 1e-3
