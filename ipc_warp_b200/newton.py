@@ -109,7 +109,8 @@ class FEMContactSolver(ContactBarrierMixin):
     def __init__(self, scene, *, material: str = "neo_hookean", E: float = 1e5, nu: float = 0.4, rho: float = 1000.0,
                  gravity=(0.0, -9.8, 0.0), h: float = 1e-2, fixed: np.ndarray | None = None,
                  attachment_stiffness: float = 1e11, dtype=torch.float32, device="cuda", vel_tol: float = 5e-2,
-                 max_newton: int = 100, tol: float = 1e-4, maxiter: int = 200, exclude_same_body: bool = False):
+                 max_newton: int = 100, tol: float = 1e-4, maxiter: int = 200, exclude_same_body: bool = False,
+                 linear_solver: str = "pcg", direct_fallback: bool = True):
         self.h = float(h)
         self.material = MATERIALS[material]
         self.mu, self.lam = lame(E, nu)
@@ -149,7 +150,11 @@ class FEMContactSolver(ContactBarrierMixin):
         self.disable_self_collision = exclude_same_body
         self._elastic = Triplets.zeros(16 * self.n_tets, dtype, self.device)
         self.precond_factory = BlockJacobi
-        self.direct_solver = None  # callable(A, b) -> x, set to use a direct fallback
+        if linear_solver not in ("pcg", "direct"):
+            raise ValueError(f"unknown linear solver {linear_solver!r}")
+        self.linear_solver = linear_solver
+        self.direct_fallback = direct_fallback
+        self.direct_solver = None  # DirectSolver, created on first use
         self.frame = 0
         self.stats = StepStats()
 
@@ -211,13 +216,26 @@ class FEMContactSolver(ContactBarrierMixin):
         self.rhs = g.to(self.dtype)
         return self.rhs
 
+    def _direct(self):
+        if self.direct_solver is None:
+            from .direct import DirectSolver
+
+            self.direct_solver = DirectSolver("metis")
+        return self.direct_solver
+
     def solve(self) -> torch.Tensor:
-        P = self.precond_factory(self.A)
-        dx, its, rel = pcg(self.A, self.rhs, P, self.tol, self.maxiter)
-        self.stats.pcg_iterations.append(its)
-        if not (rel <= self.tol) and self.direct_solver is not None:
-            dx = self.direct_solver(self.A, self.rhs)
-            self.stats.fallbacks += 1
+        """time_integrator_base.py:502-507: PCG to the relative residual
+        ``tol`` within ``maxiter`` (falling back to the direct solve when it
+        misses), or the direct solve alone (``solve_ldlt``, 470-500)."""
+        if self.linear_solver == "direct":
+            dx = self._direct()(self.A, self.rhs)
+        else:
+            P = self.precond_factory(self.A)
+            dx, its, rel = pcg(self.A, self.rhs, P, self.tol, self.maxiter)
+            self.stats.pcg_iterations.append(its)
+            if not (rel <= self.tol) and self.direct_fallback:
+                dx = self._direct()(self.A, self.rhs)
+                self.stats.fallbacks += 1
         self.states.dx = dx
         return dx
 

@@ -1,5 +1,5 @@
-"""The C-ABI library loads without a GPU and exports every symbol that
-include/ipcb.h declares (no compute calls here)."""
+"""The C-ABI libraries load without a GPU and export every symbol that
+include/ipcb.h and include/ipcb_direct.h declare (no compute calls here)."""
 import ctypes
 import os
 import re
@@ -9,8 +9,8 @@ from ipc_warp_b200 import _native
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def header_symbols():
-    text = open(os.path.join(ROOT, "include", "ipcb.h")).read()
+def header_symbols(header="ipcb.h"):
+    text = open(os.path.join(ROOT, "include", header)).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(ipcb_[a-z0-9_]+)\s*\(", text)))
 
@@ -36,3 +36,16 @@ def test_sizes_and_args_without_gpu():
     # argument validation happens before any launch
     assert L.ipcb_sort_pairs_u32(None, None, -1, 8, None, 0, None) == 1
     assert L.ipcb_contact_hessian(5, None, None, 0, 0, 1.0, None, None, None, None, None, None) == 1
+
+
+def test_direct_library_exports_header_symbols():
+    from ipc_warp_b200 import direct
+
+    lib = direct.lib()
+    syms = header_symbols("ipcb_direct.h")
+    assert len(syms) == 7
+    assert not [s for s in syms if not hasattr(lib, s)]
+    assert sorted(direct.SIGNATURES) == syms
+    # argument validation before any device work
+    assert lib.ipcb_direct_analyze(None, 0, 0, None, None, 0, 0, None) == 1
+    assert lib.ipcb_direct_factor(None, None, None) == 1

@@ -164,3 +164,22 @@ def test_falling_cube_trajectory(cuda, fp64):
     # the corner came down onto the lower cube (separation is the finite
     # barrier energy above)
     assert x[sc.body == 1, 1].min() < sc.xcs[sc.body == 1, 1].min() - 1e-3
+
+
+def test_direct_solver_step_matches_pcg_step(cuda):
+    """The reference's direct path (solve_ldlt) and PCG give the same Newton
+    iterate; a PCG capped at one iteration falls back to the direct solve."""
+    sc = _scene(4e-4)
+    x, xdot = _state(sc, seed=9)
+    out = {}
+    for name, kw in (("direct", dict(linear_solver="direct")), ("pcg", dict(tol=1e-11, maxiter=5000)),
+                     ("fallback", dict(tol=1e-11, maxiter=1))):
+        s = _solver(sc, torch.float64, **kw)
+        s.states.x.copy_(torch.tensor(x))
+        s.states.x0.copy_(torch.tensor(sc.xcs))
+        s.states.xdot.copy_(torch.tensor(xdot))
+        s.newton_iteration()
+        out[name] = (s.states.x.cpu().numpy(), s.stats.fallbacks)
+    assert np.abs(out["direct"][0] - out["pcg"][0]).max() <= 1e-9
+    assert np.abs(out["direct"][0] - out["fallback"][0]).max() <= 1e-12
+    assert out["fallback"][1] == 1 and out["pcg"][1] == 0
