@@ -37,7 +37,8 @@ enum {
 enum {
   IPCB_STATUS_STACK = 1,    /* BVH traversal stack full: result incomplete */
   IPCB_STATUS_ROOT_ITERS = 2, /* cubic root refinement hit its iteration bound */
-  IPCB_STATUS_ROW_OVERFLOW = 4 /* contact BSR: a row has more distinct columns than one warp handles */
+  IPCB_STATUS_ROW_OVERFLOW = 4, /* contact BSR: a row has more distinct columns than one warp handles */
+  IPCB_STATUS_TIMEOUT = 8       /* a bounded wait on the tensor core gave up; outputs are incomplete */
 };
 
 /* Geometry: the reference Soup (fem/geometry.py:165-171) plus positions. */
@@ -216,6 +217,14 @@ int ipcb_contact_bsr(const ipcb_contacts* ee, int n_ee, const ipcb_contacts* pt,
 /* y = alpha*A*x + beta*y for a 3x3 BSR (bsr_mv) */
 int ipcb_bsr_mv(int nrow, const int* offsets, const int* columns, const void* values, int fp64, const void* x,
                 void* y, double alpha, double beta, ipcb_stream s);
+
+/* ---- BF16 tensor-core GEMM (tcgen05, TMEM accumulator) ----
+ * No counterpart in the reference: the building block of the learned
+ * preconditioner's kernels, exported for its own tests and for callers that
+ * need a plain GEMM.  C[M x N] (fp32) = A[M x K] * B[N x K]^T, A and B
+ * row-major bf16; N in {16, 64, 128, 192, 256}, K in {64, 128, 192, 256}.
+ * *status gets IPCB_STATUS_TIMEOUT if a bounded wait gave up. */
+int ipcb_umma_gemm_bf16(int M, int N, int K, const void* A, const void* B, void* C, int* status, ipcb_stream s);
 
 #ifdef __cplusplus
 }

@@ -63,6 +63,7 @@ SIGNATURES = {
     "ipcb_point_triangle_toi": (c_int, [SP, P, BP, c_double, c_int, P, P, P, c_size_t, P]),
     "ipcb_collision_time": (c_int, [c_int, c_int, P, P, P, P, P]),
     "ipcb_cubic_roots": (c_int, [c_int, P, c_double, c_double, P, P, P, P]),
+    "ipcb_umma_gemm_bf16": (c_int, [c_int, c_int, c_int, P, P, P, P, P]),
     "ipcb_tet_rest": (c_int, [c_int, P, P, c_int, P, P, P]),
     "ipcb_tet_hessian": (c_int, [c_int, c_int, P, P, c_int, P, P, c_double, c_double, P, P, P, P, P]),
     "ipcb_tet_energy": (c_int, [c_int, c_int, P, P, c_int, P, P, c_double, c_double, P, P]),
