@@ -218,6 +218,86 @@ int ipcb_contact_bsr(const ipcb_contacts* ee, int n_ee, const ipcb_contacts* pt,
 int ipcb_bsr_mv(int nrow, const int* offsets, const int* columns, const void* values, int fp64, const void* x,
                 void* y, double alpha, double beta, ipcb_stream s);
 
+/* ---- Learned preconditioner: message-passing net -> FSAI factor ----
+ * No counterpart in the reference (its linear solve is cg or cuDSS LDLT,
+ * time_integrator_base.py:470-507).  A 4-layer, width-64 message-passing net
+ * over the 3x3-block graph of a Newton matrix A (canonical BSR: sorted,
+ * structurally symmetric, every diagonal block present) predicts a block
+ * lower-triangular factor G^ on the lower pattern of A, and
+ * M^-1 = S G^T G^ S (S = diag(A)^-1/2 per scalar) preconditions PCG.
+ * Products run on the tensor cores (BF16 operands, FP32 accumulation);
+ * G^ and everything the solve touches are FP32.
+ *
+ * Graph arrays (device, int32): rows[nnz] (row of each block), rev[nnz]
+ * (index of the transposed block), diag[n] (index of (i, i)), lower[n_lower]
+ * (blocks with column <= row, in block order; n_lower = (nnz + n) / 2). */
+#define IPCB_MPNN_WIDTH 64
+#define IPCB_MPNN_IN 16
+#define IPCB_MPNN_LAYERS 4
+#define IPCB_STATUS_PATTERN 16 /* pattern not symmetric / diagonal missing / non-positive diagonal */
+
+typedef struct {
+  int n, nnz, n_lower;
+  const int* offsets; /* int32[n + 1] */
+  const int* columns; /* int32[nnz] */
+  int* rows;
+  int* rev;
+  int* diag;
+  int* lower;
+} ipcb_graph;
+
+/* Parameter layout: FP32 master vector (weights stored in x out, row-major,
+ * then the bias, per linear map: W_hin b_hin W_ein b_ein, per layer
+ * W1 b1 W2 b2, then W_off b_off W_dg b_dg) and the BF16 operand copies the
+ * kernels read (made by ipcb_mpnn_pack). */
+int ipcb_mpnn_param_count(void);
+int ipcb_mpnn_packed_count(void);
+int ipcb_mpnn_pack(const float* params, void* packed, ipcb_stream s);
+
+size_t ipcb_mpnn_graph_workspace(int n);
+int ipcb_mpnn_graph(ipcb_graph* g, int* status, void* ws, size_t ws_bytes, ipcb_stream s);
+/* Scaling s (float[3n]), scaled blocks ahat (float[9 nnz]) and the net's
+ * inputs x (bf16[16 n]) and y (bf16[16 nnz]) from the BSR values. */
+int ipcb_mpnn_features(const ipcb_graph* g, int fp64, const void* values, float* scale, float* ahat, void* x,
+                       void* y, int* status, ipcb_stream s);
+
+/* Activations: bf16 buffers; h[5][n*64], e[5][nnz*64] (layer inputs and the
+ * final state), m[4][nnz*64], a[4][n*64], u[4][n*64]; for inference only
+ * h[0..1] and e[0..1] are used (ping-pong) and m, a, u may be NULL.
+ * agg: float[n*64] scratch.  G: float[9 nnz] written on the lower blocks. */
+typedef struct {
+  void* h;
+  void* e;
+  void* m;
+  void* a;
+  void* u;
+  float* agg;
+  int training;
+} ipcb_mpnn_tape;
+
+int ipcb_mpnn_forward(const ipcb_graph* g, const void* packed, const float* params, const void* x, const void* y,
+                      ipcb_mpnn_tape* tape, float* G, int* status, ipcb_stream s);
+/* Kaporin loss parts of G^ A^ G^T: acc[0] += tr(G^ A^ G^T), acc[1] += sum_i
+ * log|det G^_ii| (double).  With dG != NULL, a second call after the first
+ * has completed writes the loss gradient w.r.t. G^ scaled by `weight`
+ * (bf16[64 n_lower], columns 0..8 for off-diagonal blocks, 16..24 for
+ * diagonal blocks) using T (float[9 nnz] scratch). */
+int ipcb_mpnn_loss(const ipcb_graph* g, const float* ahat, const float* G, float* T, double* acc, void* dG,
+                   double weight, ipcb_stream s);
+size_t ipcb_mpnn_backward_workspace(int n, int nnz, int n_lower);
+/* Gradients of sum(dG * G^) w.r.t. the parameters, added to grad
+ * (float[param_count]).  Needs the training tape of the forward call. */
+int ipcb_mpnn_backward(const ipcb_graph* g, const void* packed, const float* params, const void* x, const void* y,
+                       const ipcb_mpnn_tape* tape, const void* dG, float* grad, int* status, void* ws,
+                       size_t ws_bytes, ipcb_stream s);
+/* One Adam step (bias-corrected, step t >= 1) over n parameters. */
+int ipcb_adam(int n, float* params, const float* grad, float* m, float* v, float lr, float beta1, float beta2,
+              float eps, int t, ipcb_stream s);
+/* z = S G^T G^ S r (r, z: scalar[3n]; fp64 selects double vectors); tmp:
+ * float/double[3n]. */
+int ipcb_fsai_apply(const ipcb_graph* g, const float* G, const float* scale, int fp64, const void* r, void* tmp,
+                    void* z, ipcb_stream s);
+
 /* ---- BF16 tensor-core GEMM (tcgen05, TMEM accumulator) ----
  * No counterpart in the reference: the building block of the learned
  * preconditioner's kernels, exported for its own tests and for callers that

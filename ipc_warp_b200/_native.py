@@ -31,7 +31,17 @@ class Lbvh(ctypes.Structure):
                 ("flags", P), ("wide", P)]
 
 
+class Graph(ctypes.Structure):
+    _fields_ = [("n", c_int), ("nnz", c_int), ("n_lower", c_int), ("offsets", P), ("columns", P), ("rows", P),
+                ("rev", P), ("diag", P), ("lower", P)]
+
+
+class Tape(ctypes.Structure):
+    _fields_ = [("h", P), ("e", P), ("m", P), ("a", P), ("u", P), ("agg", P), ("training", c_int)]
+
+
 SP, CP, BP = ctypes.POINTER(Soup), ctypes.POINTER(Contacts), ctypes.POINTER(Lbvh)
+GP, TP = ctypes.POINTER(Graph), ctypes.POINTER(Tape)
 
 # name -> (restype, argtypes); every symbol here is declared in include/ipcb.h
 SIGNATURES = {
@@ -63,6 +73,18 @@ SIGNATURES = {
     "ipcb_point_triangle_toi": (c_int, [SP, P, BP, c_double, c_int, P, P, P, c_size_t, P]),
     "ipcb_collision_time": (c_int, [c_int, c_int, P, P, P, P, P]),
     "ipcb_cubic_roots": (c_int, [c_int, P, c_double, c_double, P, P, P, P]),
+    "ipcb_mpnn_param_count": (c_int, []),
+    "ipcb_mpnn_packed_count": (c_int, []),
+    "ipcb_mpnn_pack": (c_int, [P, P, P]),
+    "ipcb_mpnn_graph_workspace": (c_size_t, [c_int]),
+    "ipcb_mpnn_graph": (c_int, [GP, P, P, c_size_t, P]),
+    "ipcb_mpnn_features": (c_int, [GP, c_int, P, P, P, P, P, P, P]),
+    "ipcb_mpnn_forward": (c_int, [GP, P, P, P, P, TP, P, P, P]),
+    "ipcb_mpnn_loss": (c_int, [GP, P, P, P, P, P, c_double, P]),
+    "ipcb_mpnn_backward_workspace": (c_size_t, [c_int, c_int, c_int]),
+    "ipcb_mpnn_backward": (c_int, [GP, P, P, P, P, TP, P, P, P, P, c_size_t, P]),
+    "ipcb_adam": (c_int, [c_int, P, P, P, P, c_float, c_float, c_float, c_float, c_int, P]),
+    "ipcb_fsai_apply": (c_int, [GP, P, P, c_int, P, P, P, P]),
     "ipcb_umma_gemm_bf16": (c_int, [c_int, c_int, c_int, P, P, P, P, P]),
     "ipcb_tet_rest": (c_int, [c_int, P, P, c_int, P, P, P]),
     "ipcb_tet_hessian": (c_int, [c_int, c_int, P, P, c_int, P, P, c_double, c_double, P, P, P, P, P]),

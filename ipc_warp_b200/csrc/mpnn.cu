@@ -1,0 +1,1138 @@
+// Learned preconditioner: a message-passing net over the 3x3-block graph of
+// the Newton matrix whose output is an FSAI factor G^ (include/ipcb.h).
+//
+// Every dense product runs on the tensor cores through one templated kernel,
+// k_mlp: a persistent CTA stages 128 rows of its A operand into an SW128
+// K-major shared tile (the "stage" functor gathers them: node states of both
+// endpoints and the edge state for a message, node state and mean message
+// for an update, ...), one thread issues the UMMAs into a TMEM accumulator,
+// and the four warps read their 32 lanes back for a fused epilogue (bias,
+// ReLU, residual, segmented message aggregation, head selection).  Weight
+// gradients use k_wgrad, which stages X^T and dY^T tiles (rows of the batch
+// along K) and keeps the [features x outputs] accumulator in TMEM across all
+// the row tiles a CTA visits, plus a bias row from a column of ones.
+//
+// Storage: node/edge states and messages bf16, accumulation fp32, biases
+// fp32, G^ fp32 (the rounding points of oracle/mpnn.py).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "scan.cuh"
+#include "umma.cuh"
+
+namespace ipcb {
+int check_launch(const char* where);
+void set_error_msg(const char* msg);
+}  // namespace ipcb
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+constexpr int W = IPCB_MPNN_WIDTH;  // 64
+constexpr int IN = IPCB_MPNN_IN;    // 16
+constexpr int LAYERS = IPCB_MPNN_LAYERS;
+constexpr int kThreads = 128;
+
+// ------------------------------------------------------------ parameters
+// FP32 master layout (weights in x out row-major, then bias)
+constexpr int P_WHIN = 0, P_BHIN = P_WHIN + IN * W;
+constexpr int P_WEIN = P_BHIN + W, P_BEIN = P_WEIN + IN * W;
+constexpr int P_LAYER0 = P_BEIN + W;
+constexpr int P_LAYER = 3 * W * W + W + 2 * W * W + W;  // W1 b1 W2 b2
+constexpr int O_W1 = 0, O_B1 = 3 * W * W, O_W2 = O_B1 + W, O_B2 = O_W2 + 2 * W * W;
+constexpr int P_WOFF = P_LAYER0 + LAYERS * P_LAYER, P_BOFF = P_WOFF + W * 9;
+constexpr int P_WDG = P_BOFF + 9, P_BDG = P_WDG + W * 9;
+constexpr int P_COUNT = P_BDG + 9;
+
+// BF16 operand layout (all offsets in elements, multiples of 8)
+constexpr int K_ENC_H = 0;                        // [64 out][64 in]  (in >= 16 zero)
+constexpr int K_ENC_E = K_ENC_H + W * 64;         // [64][64]
+constexpr int K_W1T = K_ENC_E + W * 64;           // LAYERS x [64 out][192 in]
+constexpr int K_W2T = K_W1T + LAYERS * W * 3 * W; // LAYERS x [64 out][128 in]
+constexpr int K_HEADT = K_W2T + LAYERS * W * 2 * W; // [32 out][64 in]: rows 0..8 off, 16..24 diag
+constexpr int K_W1 = K_HEADT + 32 * W;            // LAYERS x [192 in][64 out]
+constexpr int K_W2 = K_W1 + LAYERS * 3 * W * W;   // LAYERS x [128 in][64 out]
+constexpr int K_HEAD = K_W2 + LAYERS * 2 * W * W; // [64 in][64 cols]: cols 0..8 off, 16..24 diag
+constexpr int K_COUNT = K_HEAD + W * 64;
+
+__global__ void k_pack(const float* __restrict__ p, bf16* __restrict__ q) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= K_COUNT) return;
+  float v = 0.f;
+  if (t < K_ENC_E) {  // enc_h^T
+    const int o = (t - K_ENC_H) / 64, k = (t - K_ENC_H) % 64;
+    v = k < IN ? p[P_WHIN + k * W + o] : 0.f;
+  } else if (t < K_W1T) {
+    const int o = (t - K_ENC_E) / 64, k = (t - K_ENC_E) % 64;
+    v = k < IN ? p[P_WEIN + k * W + o] : 0.f;
+  } else if (t < K_W2T) {
+    const int r = t - K_W1T, l = r / (W * 3 * W), o = (r % (W * 3 * W)) / (3 * W), k = r % (3 * W);
+    v = p[P_LAYER0 + l * P_LAYER + O_W1 + k * W + o];
+  } else if (t < K_HEADT) {
+    const int r = t - K_W2T, l = r / (W * 2 * W), o = (r % (W * 2 * W)) / (2 * W), k = r % (2 * W);
+    v = p[P_LAYER0 + l * P_LAYER + O_W2 + k * W + o];
+  } else if (t < K_W1) {
+    const int r = t - K_HEADT, o = r / W, k = r % W;
+    if (o < 9) v = p[P_WOFF + k * 9 + o];
+    else if (o >= 16 && o < 25) v = p[P_WDG + k * 9 + (o - 16)];
+  } else if (t < K_W2) {
+    const int r = t - K_W1, l = r / (3 * W * W), k = (r % (3 * W * W)) / W, o = r % W;
+    v = p[P_LAYER0 + l * P_LAYER + O_W1 + k * W + o];
+  } else if (t < K_HEAD) {
+    const int r = t - K_W2, l = r / (2 * W * W), k = (r % (2 * W * W)) / W, o = r % W;
+    v = p[P_LAYER0 + l * P_LAYER + O_W2 + k * W + o];
+  } else {
+    const int r = t - K_HEAD, k = r / 64, c = r % 64;
+    if (c < 9) v = p[P_WOFF + k * 9 + c];
+    else if (c >= 16 && c < 25) v = p[P_WDG + k * 9 + (c - 16)];
+  }
+  q[t] = __float2bfloat16_rn(v);
+}
+
+// ------------------------------------------------------------ helpers
+__device__ __forceinline__ float bfr(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+__device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
+  return reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~uintptr_t(1023));
+}
+__device__ __forceinline__ uint4 zero4() { return make_uint4(0, 0, 0, 0); }
+__device__ __forceinline__ uint4 ld4(const bf16* p) { return *reinterpret_cast<const uint4*>(p); }
+
+__device__ __forceinline__ void unpack8(uint4 u, float (&f)[8]) {
+  const __nv_bfloat162* b = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    float2 t = __bfloat1622float2(b[i]);
+    f[2 * i] = t.x;
+    f[2 * i + 1] = t.y;
+  }
+}
+__device__ __forceinline__ uint4 pack8(const float* f) {
+  uint4 u;
+  __nv_bfloat162* b = reinterpret_cast<__nv_bfloat162*>(&u);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) b[i] = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
+  return u;
+}
+
+// ------------------------------------------------------------ stages
+struct StageDense {  // row-major bf16 rows, columns >= kvalid read as zero
+  const bf16* X;
+  int ld, kvalid;
+  __device__ uint4 group(int row, int c, int g) const {
+    const int k = c * 64 + g * 8;
+    return k < kvalid ? ld4(X + (size_t)row * ld + k) : zero4();
+  }
+};
+
+struct StageEdge {  // [h_row | h_col | e] of an edge
+  const bf16 *h, *e;
+  const int *rows, *cols;
+  __device__ uint4 group(int row, int c, int g) const {
+    if (c == 0) return ld4(h + (size_t)__ldg(rows + row) * W + g * 8);
+    if (c == 1) return ld4(h + (size_t)__ldg(cols + row) * W + g * 8);
+    return ld4(e + (size_t)row * W + g * 8);
+  }
+};
+
+struct StageNode {  // [h | bf16(agg / deg)], writing a to the tape
+  const bf16* h;
+  const float* agg;
+  const int* offsets;
+  bf16* a_out;
+  __device__ uint4 group(int row, int c, int g) const {
+    if (c == 0) return ld4(h + (size_t)row * W + g * 8);
+    const float deg = (float)(__ldg(offsets + row + 1) - __ldg(offsets + row));
+    float f[8];
+    const float4* a4 = reinterpret_cast<const float4*>(agg + (size_t)row * W + g * 8);
+    const float4 p = a4[0], q = a4[1];
+    f[0] = p.x / deg; f[1] = p.y / deg; f[2] = p.z / deg; f[3] = p.w / deg;
+    f[4] = q.x / deg; f[5] = q.y / deg; f[6] = q.z / deg; f[7] = q.w / deg;
+    const uint4 u = pack8(f);
+    if (a_out) *reinterpret_cast<uint4*>(a_out + (size_t)row * W + g * 8) = u;
+    return u;
+  }
+};
+
+struct StageGather {  // X[idx[row]] (64 wide)
+  const bf16* X;
+  const int* idx;
+  __device__ uint4 group(int row, int, int g) const { return ld4(X + (size_t)__ldg(idx + row) * W + g * 8); }
+};
+
+// ------------------------------------------------------------ epilogues
+// apply() is called by all 128 threads (valid marks rows inside the batch);
+// `scr` is shared scratch of 128 x 33 floats plus 128 ints.
+struct EpiBiasRelu {
+  const float* b;
+  bf16* out;
+  __device__ void apply(int row, bool valid, int col0, const float (&v)[32], float*, int*) const {
+    if (!valid) return;
+    float o[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) o[i] = fmaxf(v[i] + __ldg(b + col0 + i), 0.f);
+    uint4* dst = reinterpret_cast<uint4*>(out + (size_t)row * W + col0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) dst[q] = pack8(o + 8 * q);
+  }
+};
+
+struct EpiEdge {  // m = relu(v + b1); e_out = e_in + m; agg[row] += m
+  const float* b;
+  const bf16* e_in;
+  bf16* e_out;
+  bf16* m_out;
+  float* agg;
+  const int* rows;
+  __device__ void apply(int row, bool valid, int col0, const float (&v)[32], float* scr, int* srow) const {
+    const int tid = threadIdx.x;
+    float m[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) m[i] = valid ? bfr(fmaxf(v[i] + __ldg(b + col0 + i), 0.f)) : 0.f;
+    if (valid) {
+      const bf16* ei = e_in + (size_t)row * W + col0;
+      float eo[32];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        float f[8];
+        unpack8(ld4(ei + 8 * q), f);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) eo[8 * q + i] = f[i] + m[8 * q + i];
+      }
+      uint4* de = reinterpret_cast<uint4*>(e_out + (size_t)row * W + col0);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) de[q] = pack8(eo + 8 * q);
+      if (m_out) {
+        uint4* dm = reinterpret_cast<uint4*>(m_out + (size_t)row * W + col0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dm[q] = pack8(m + 8 * q);
+      }
+    }
+    // segmented sum over the tile's rows (edges of a row are contiguous)
+#pragma unroll
+    for (int i = 0; i < 32; ++i) scr[tid * 33 + i] = m[i];
+    srow[tid] = valid ? __ldg(rows + row) : -1;
+    __syncthreads();
+    const int col = tid & 31, q = tid >> 5;
+    int cur = -1;
+    float acc = 0.f;
+    for (int r = q * 32; r < q * 32 + 32; ++r) {
+      const int id = srow[r];
+      if (id != cur) {
+        if (cur >= 0) atomicAdd(agg + (size_t)cur * W + col0 + col, acc);
+        cur = id;
+        acc = 0.f;
+      }
+      acc += scr[r * 33 + col];
+    }
+    if (cur >= 0) atomicAdd(agg + (size_t)cur * W + col0 + col, acc);
+    __syncthreads();
+  }
+};
+
+struct EpiNode {  // u = relu(v + b2); h_out = h_in + u
+  const float* b;
+  const bf16* h_in;
+  bf16* h_out;
+  bf16* u_out;
+  __device__ void apply(int row, bool valid, int col0, const float (&v)[32], float*, int*) const {
+    if (!valid) return;
+    float u[32], ho[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) u[i] = bfr(fmaxf(v[i] + __ldg(b + col0 + i), 0.f));
+    const bf16* hi = h_in + (size_t)row * W + col0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      float f[8];
+      unpack8(ld4(hi + 8 * q), f);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) ho[8 * q + i] = f[i] + u[8 * q + i];
+    }
+    uint4* dh = reinterpret_cast<uint4*>(h_out + (size_t)row * W + col0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) dh[q] = pack8(ho + 8 * q);
+    if (u_out) {
+      uint4* du = reinterpret_cast<uint4*>(u_out + (size_t)row * W + col0);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) du[q] = pack8(u + 8 * q);
+    }
+  }
+};
+
+struct EpiHead {  // G^ of a lower block from the off-diagonal or diagonal head
+  const float *b_off, *b_dg;
+  const int *lower, *rows, *cols;
+  float* G;
+  __device__ void apply(int row, bool valid, int col0, const float (&v)[32], float*, int*) const {
+    if (!valid || col0 != 0) return;
+    const int e = __ldg(lower + row);
+    const bool dg = __ldg(rows + e) == __ldg(cols + e);
+    float* g = G + (size_t)e * 9;
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+      g[k] = dg ? v[16 + k] + __ldg(b_dg + k) + ((k % 4) == 0 ? 1.f : 0.f) : v[k] + __ldg(b_off + k);
+  }
+};
+
+struct EpiF32 {  // plain fp32 rows of width ld
+  float* out;
+  int ld;
+  __device__ void apply(int row, bool valid, int col0, const float (&v)[32], float*, int*) const {
+    if (!valid) return;
+    const int n = ld - col0 < 32 ? ld - col0 : 32;
+    float* o = out + (size_t)row * ld + col0;
+    if (n == 32) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) reinterpret_cast<float4*>(o)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    } else {
+      for (int i = 0; i < n; ++i) o[i] = v[i];
+    }
+  }
+};
+
+// ------------------------------------------------------------ k_mlp
+template <int N, int C>
+constexpr size_t mlp_smem() {
+  return 1024 + (size_t)C * 128 * 128 + (size_t)C * N * 128 + 128 * 33 * 4 + 128 * 4;
+}
+
+template <int N, int C, class Stage, class Epi>
+__global__ void __launch_bounds__(kThreads) k_mlp(int rows, Stage st, Epi ep, const bf16* __restrict__ Bw,
+                                                  int* __restrict__ status) {
+  extern __shared__ uint8_t dsmem[];
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tslot;
+  constexpr uint32_t kCols = umma::tmem_cols(N);
+  constexpr int K = 64 * C;
+  uint8_t* sA = align1024(dsmem);
+  uint8_t* sB = sA + C * 128 * 128;
+  float* scr = reinterpret_cast<float*>(sB + C * N * 128);
+  int* srow = reinterpret_cast<int*>(scr + 128 * 33);
+  const int tid = threadIdx.x, warp = tid >> 5;
+
+  for (int idx = tid; idx < N * C * 8; idx += kThreads) {
+    const int r = idx / (C * 8), c = (idx / 8) % C, g = idx % 8;
+    *reinterpret_cast<uint4*>(sB + umma::sw128_group(r, c, g, N)) = ld4(Bw + (size_t)r * K + c * 64 + g * 8);
+  }
+  if (warp == 0) umma::tmem_alloc(&tslot, kCols);
+  if (tid == 0) umma::mbar_init(&mbar, 1);
+  umma::fence_async_smem();
+  umma::fence_before();
+  __syncthreads();
+  umma::fence_after();
+  const uint32_t tmem = tslot;
+  uint32_t phase = 0;
+  int ok = 1;
+  const int ntiles = (rows + 127) / 128;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int row = tile * 128 + tid;
+    const bool valid = row < rows;
+#pragma unroll
+    for (int c = 0; c < C; ++c)
+#pragma unroll
+      for (int g = 0; g < 8; ++g)
+        *reinterpret_cast<uint4*>(sA + umma::sw128_group(tid, c, g, 128)) = valid ? st.group(row, c, g) : zero4();
+    umma::fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after();
+      umma::issue_tile<N, C>(tmem, umma::smem_u32(sA), umma::smem_u32(sB), false, &mbar);
+    }
+    ok = __syncthreads_and(umma::mbar_wait(&mbar, phase) ? 1 : 0);
+    phase ^= 1;
+    if (!ok) break;
+    umma::fence_after();
+#pragma unroll
+    for (int col = 0; col < N; col += 32) {
+      float v[32];
+      umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + col, v);
+      ep.apply(row, valid, col, v, scr, srow);
+    }
+    umma::fence_before();
+    __syncthreads();
+  }
+  if (!ok) {
+    if (tid == 0) atomicOr(status, IPCB_STATUS_TIMEOUT);
+    umma::mbar_wait(&mbar, phase);
+  }
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, kCols);
+}
+
+int g_sms = 0;
+int sm_count() {
+  if (!g_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sms <= 0) g_sms = 148;
+  }
+  return g_sms;
+}
+
+template <int N, int C, class Stage, class Epi>
+int launch_mlp(int rows, const Stage& st, const Epi& ep, const bf16* Bw, int* status, cudaStream_t s,
+               const char* what) {
+  if (rows <= 0) return 0;
+  constexpr size_t smem = mlp_smem<N, C>();
+  auto kern = k_mlp<N, C, Stage, Epi>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    ipcb::set_error_msg(what);
+    return IPCB_E_CUDA;
+  }
+  const int by_tmem = (int)(512 / umma::tmem_cols(N));
+  const int by_smem = (int)((227 * 1024) / (smem + 1024));
+  const int per_sm = by_tmem < by_smem ? by_tmem : by_smem;
+  const int tiles = (rows + 127) / 128;
+  const int cap = sm_count() * (per_sm > 0 ? per_sm : 1);
+  kern<<<tiles < cap ? tiles : cap, kThreads, smem, s>>>(rows, st, ep, Bw, status);
+  return ipcb::check_launch(what);
+}
+
+// ------------------------------------------------------------ k_wgrad
+// dW[f][o] += sum_r X[r][f] dY[r][o] over all rows, plus the bias gradient in
+// row f = kx (a column of ones appended to X).  MT M-tiles of 128 features.
+struct EpiGrad {
+  float* dW;  // [kx][out]
+  float* db;  // [out]
+  int kx, out;
+  __device__ void add(int f, int col0, const float (&v)[32]) const {
+    if (f < kx) {
+      for (int i = 0; i < 32 && col0 + i < out; ++i) atomicAdd(dW + (size_t)f * out + col0 + i, v[i]);
+    } else if (f == kx) {
+      for (int i = 0; i < 32 && col0 + i < out; ++i) atomicAdd(db + col0 + i, v[i]);
+    }
+  }
+};
+
+struct EpiGradHead {  // columns 0..8 -> off-diagonal head, 16..24 -> diagonal head
+  float *dW_off, *db_off, *dW_dg, *db_dg;
+  __device__ void add(int f, int col0, const float (&v)[32]) const {
+    if (col0 != 0 || f > W) return;
+    for (int k = 0; k < 9; ++k) {
+      if (f < W) {
+        atomicAdd(dW_off + f * 9 + k, v[k]);
+        atomicAdd(dW_dg + f * 9 + k, v[16 + k]);
+      } else {
+        atomicAdd(db_off + k, v[k]);
+        atomicAdd(db_dg + k, v[16 + k]);
+      }
+    }
+  }
+};
+
+template <int MT, int N>
+constexpr size_t wgrad_smem() {
+  return 1024 + (size_t)MT * 2 * 128 * 128 + (size_t)2 * N * 128;
+}
+
+template <int MT, int N, class Epi>
+__global__ void __launch_bounds__(kThreads) k_wgrad(int R, const bf16* __restrict__ X, int ldx, int kx,
+                                                    const bf16* __restrict__ dY, int ldy, Epi ep,
+                                                    int* __restrict__ status) {
+  extern __shared__ uint8_t dsmem[];
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tslot;
+  constexpr uint32_t kCols = umma::tmem_cols(MT * N);
+  uint8_t* sA = align1024(dsmem);                // MT x [128 features][128 rows]
+  uint8_t* sB = sA + MT * 2 * 128 * 128;         // [N outputs][128 rows]
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) umma::tmem_alloc(&tslot, kCols);
+  if (tid == 0) umma::mbar_init(&mbar, 1);
+  umma::fence_before();
+  __syncthreads();
+  umma::fence_after();
+  const uint32_t tmem = tslot;
+  uint32_t phase = 0;
+  int ok = 1;
+  bool any = false;
+  const int ntiles = (R + 127) / 128;
+  const bf16 one = __float2bfloat16_rn(1.f), zero = __float2bfloat16_rn(0.f);
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int r = tile * 128 + tid;
+    const bool valid = r < R;
+    // X^T: element (feature f, k = tid)
+    for (int f0 = 0; f0 < MT * 128; f0 += 8) {
+      float xv[8];
+      if (valid && f0 + 8 <= kx) {
+        unpack8(ld4(X + (size_t)r * ldx + f0), xv);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) xv[i] = 0.f;
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int f = f0 + i;
+        bf16 val = f < kx ? __float2bfloat16_rn(xv[i]) : (f == kx && valid ? one : zero);
+        *reinterpret_cast<bf16*>(sA + (f >> 7) * (2 * 128 * 128) + umma::sw128_offset(f & 127, tid, 128)) = val;
+      }
+    }
+    for (int o0 = 0; o0 < N; o0 += 8) {
+      float yv[8];
+      if (valid) unpack8(ld4(dY + (size_t)r * ldy + o0), yv);
+      else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) yv[i] = 0.f;
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+        *reinterpret_cast<bf16*>(sB + umma::sw128_offset(o0 + i, tid, N)) = __float2bfloat16_rn(yv[i]);
+    }
+    umma::fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after();
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt)
+        umma::issue<N, 2>(tmem + mt * N, umma::smem_u32(sA + mt * 2 * 128 * 128), umma::smem_u32(sB), any);
+      umma::commit(&mbar);
+    }
+    ok = __syncthreads_and(umma::mbar_wait(&mbar, phase) ? 1 : 0);
+    phase ^= 1;
+    if (!ok) break;
+    any = true;
+  }
+  if (!ok) {
+    if (tid == 0) atomicOr(status, IPCB_STATUS_TIMEOUT);
+    umma::mbar_wait(&mbar, phase);
+  } else if (any) {
+    umma::fence_after();
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+      for (int col = 0; col < N; col += 32) {
+        float v[32];
+        umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + mt * N + col, v);
+        ep.add(mt * 128 + tid, col, v);
+      }
+  }
+  umma::fence_before();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, kCols);
+}
+
+template <int MT, int N, class Epi>
+int launch_wgrad(int R, const bf16* X, int ldx, int kx, const bf16* dY, int ldy, const Epi& ep, int* status,
+                 cudaStream_t s, const char* what) {
+  if (R <= 0) return 0;
+  constexpr size_t smem = wgrad_smem<MT, N>();
+  auto kern = k_wgrad<MT, N, Epi>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    ipcb::set_error_msg(what);
+    return IPCB_E_CUDA;
+  }
+  const int tiles = (R + 127) / 128;
+  // few CTAs: each reduces many tiles in TMEM before its atomics
+  const int cap = sm_count();
+  kern<<<tiles < cap ? tiles : cap, kThreads, smem, s>>>(R, X, ldx, kx, dY, ldy, ep, status);
+  return ipcb::check_launch(what);
+}
+
+// ------------------------------------------------------------ graph
+__global__ void k_graph_rows(int n, const int* __restrict__ off, const int* __restrict__ col, int* __restrict__ rows,
+                             int* __restrict__ rev, int* __restrict__ diag, int* __restrict__ lower_count,
+                             int* __restrict__ status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int b = off[i], e = off[i + 1];
+  int d = -1;
+  for (int k = b; k < e; ++k) {
+    rows[k] = i;
+    const int j = col[k];
+    if (j == i) d = k;
+    // transposed block (j, i): binary search in row j
+    int lo = off[j], hi = off[j + 1] - 1, r = -1;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1, c = col[mid];
+      if (c == i) { r = mid; break; }
+      if (c < i) lo = mid + 1; else hi = mid - 1;
+    }
+    rev[k] = r;
+    if (r < 0) atomicOr(status, IPCB_STATUS_PATTERN);
+  }
+  diag[i] = d;
+  if (d < 0) atomicOr(status, IPCB_STATUS_PATTERN);
+  lower_count[i] = d < 0 ? 0 : d - b + 1;
+}
+
+__global__ void k_graph_lower(int n, const int* __restrict__ off, const int* __restrict__ diag,
+                              const int* __restrict__ lower_start, int* __restrict__ lower) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int b = off[i], c = diag[i] < 0 ? 0 : diag[i] - b + 1, s0 = lower_start[i];
+  for (int k = 0; k < c; ++k) lower[s0 + k] = b + k;
+}
+
+// ------------------------------------------------------------ features
+template <class T>
+__global__ void k_scale(int n, const int* __restrict__ diag, const T* __restrict__ vals, float* __restrict__ scale,
+                        int* __restrict__ status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int d = diag[i];
+  for (int a = 0; a < 3; ++a) {
+    double v = d >= 0 ? (double)vals[(size_t)d * 9 + 4 * a] : 0.0;
+    if (!(v > 0.0)) {
+      atomicOr(status, IPCB_STATUS_PATTERN);
+      v = 1.0;
+    }
+    scale[3 * i + a] = (float)(1.0 / sqrt(v));
+  }
+}
+
+template <class T>
+__global__ void k_edge_features(int nnz, const int* __restrict__ rows, const int* __restrict__ cols,
+                                const T* __restrict__ vals, const float* __restrict__ scale, float* __restrict__ ahat,
+                                bf16* __restrict__ y) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nnz) return;
+  const int i = rows[e], j = cols[e];
+  float a[9];
+  double fro = 0.0;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double v = (double)vals[(size_t)e * 9 + 3 * r + c] * (double)scale[3 * i + r] * (double)scale[3 * j + c];
+      a[3 * r + c] = (float)v;
+      fro += v * v;
+    }
+  float f[16];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    ahat[(size_t)e * 9 + k] = a[k];
+    f[k] = a[k];
+  }
+  f[9] = (float)sqrt(fro);
+  f[10] = i == j ? 1.f : 0.f;
+#pragma unroll
+  for (int k = 11; k < 16; ++k) f[k] = 0.f;
+  uint4* dst = reinterpret_cast<uint4*>(y + (size_t)e * 16);
+  dst[0] = pack8(f);
+  dst[1] = pack8(f + 8);
+}
+
+__global__ void k_node_features(int n, const int* __restrict__ off, const int* __restrict__ cols,
+                                const int* __restrict__ diag, const float* __restrict__ ahat, bf16* __restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float f[16];
+  const int d = diag[i];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) f[k] = d >= 0 ? ahat[(size_t)d * 9 + k] : 0.f;
+  const int b = off[i], e = off[i + 1];
+  double rs = 0.0;
+  for (int k = b; k < e; ++k) {
+    if (cols[k] == i) continue;
+    double s = 0.0;
+    for (int q = 0; q < 9; ++q) {
+      const double v = ahat[(size_t)k * 9 + q];
+      s += v * v;
+    }
+    rs += sqrt(s);
+  }
+  f[9] = (float)log1p((double)(e - b));
+  f[10] = (float)rs;
+#pragma unroll
+  for (int k = 11; k < 16; ++k) f[k] = 0.f;
+  uint4* dst = reinterpret_cast<uint4*>(x + (size_t)i * 16);
+  dst[0] = pack8(f);
+  dst[1] = pack8(f + 8);
+}
+
+// ------------------------------------------------------------ loss
+__device__ __forceinline__ int find_col(const int* __restrict__ off, const int* __restrict__ cols, int row, int c) {
+  int lo = off[row], hi = off[row + 1] - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1, v = __ldg(cols + mid);
+    if (v == c) return mid;
+    if (v < c) lo = mid + 1; else hi = mid - 1;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ void mm3_acc(float (&acc)[9], const float* __restrict__ a, const float* __restrict__ b) {
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc[3 * r + c] += a[3 * r] * b[c] + a[3 * r + 1] * b[3 + c] + a[3 * r + 2] * b[6 + c];
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// T_ij = sum_{k <= i} G_ik A^_kj over the lower blocks (i, j); acc[0] += <T, G>
+__global__ void k_fsai_T(int n_lower, const int* __restrict__ lower, const int* __restrict__ rows,
+                         const int* __restrict__ cols, const int* __restrict__ off, const int* __restrict__ diag,
+                         const float* __restrict__ ahat, const float* __restrict__ G, float* __restrict__ T,
+                         double* __restrict__ acc) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  double part = 0.0;
+  if (r < n_lower) {
+    const int e = lower[r], i = rows[e], j = cols[e];
+    float t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int ke = off[i]; ke <= diag[i]; ++ke) {
+      const int k = cols[ke];
+      const int kj = find_col(off, cols, k, j);
+      if (kj >= 0) mm3_acc(t, G + (size_t)ke * 9, ahat + (size_t)kj * 9);
+    }
+    const float* g = G + (size_t)e * 9;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      T[(size_t)e * 9 + q] = t[q];
+      part += (double)t[q] * (double)g[q];
+    }
+  }
+  part = warp_sum(part);
+  if ((threadIdx.x & 31) == 0 && part != 0.0) atomicAdd(acc, part);
+}
+
+__device__ __forceinline__ double det3(const float* g) {
+  return (double)g[0] * ((double)g[4] * g[8] - (double)g[5] * g[7]) -
+         (double)g[1] * ((double)g[3] * g[8] - (double)g[5] * g[6]) +
+         (double)g[2] * ((double)g[3] * g[7] - (double)g[4] * g[6]);
+}
+
+__global__ void k_fsai_logdet(int n, const int* __restrict__ diag, const float* __restrict__ G,
+                              double* __restrict__ acc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double part = 0.0;
+  if (i < n) part = log(fabs(det3(G + (size_t)diag[i] * 9)));
+  part = warp_sum(part);
+  if ((threadIdx.x & 31) == 0) atomicAdd(acc + 1, part);
+}
+
+// dG = weight * (2 T / tr - (2 / N) [diag] G^-T), written bf16 into the
+// padded head layout (columns 0..8 off-diagonal, 16..24 diagonal)
+__global__ void k_fsai_dG(int n_lower, int n, const int* __restrict__ lower, const int* __restrict__ rows,
+                          const int* __restrict__ cols, const float* __restrict__ G, const float* __restrict__ T,
+                          const double* __restrict__ acc, double weight, bf16* __restrict__ dG) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_lower) return;
+  const int e = lower[r];
+  const bool dg = rows[e] == cols[e];
+  const double tr = acc[0];
+  const double N = 3.0 * n;
+  float d[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) d[q] = (float)(weight * 2.0 * (double)T[(size_t)e * 9 + q] / tr);
+  if (dg) {
+    const float* g = G + (size_t)e * 9;
+    const double det = det3(g);
+    // inverse transpose = cofactor matrix / det
+    double cof[9] = {(double)g[4] * g[8] - (double)g[5] * g[7], -((double)g[3] * g[8] - (double)g[5] * g[6]),
+                     (double)g[3] * g[7] - (double)g[4] * g[6], -((double)g[1] * g[8] - (double)g[2] * g[7]),
+                     (double)g[0] * g[8] - (double)g[2] * g[6], -((double)g[0] * g[7] - (double)g[1] * g[6]),
+                     (double)g[1] * g[5] - (double)g[2] * g[4], -((double)g[0] * g[5] - (double)g[2] * g[3]),
+                     (double)g[0] * g[4] - (double)g[1] * g[3]};
+#pragma unroll
+    for (int q = 0; q < 9; ++q) d[q] -= (float)(weight * (2.0 / N) * cof[q] / det);
+  }
+  float row[64];
+#pragma unroll
+  for (int q = 0; q < 64; ++q) row[q] = 0.f;
+#pragma unroll
+  for (int q = 0; q < 9; ++q) row[(dg ? 16 : 0) + q] = d[q];
+  uint4* dst = reinterpret_cast<uint4*>(dG + (size_t)r * 64);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) dst[q] = pack8(row + 8 * q);
+}
+
+// ------------------------------------------------------------ backward helpers
+__global__ void k_gather_rows(int R, const bf16* __restrict__ X, const int* __restrict__ idx, bf16* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // one 16-byte group
+  if (t >= R * 8) return;
+  const int r = t >> 3, g = t & 7;
+  reinterpret_cast<uint4*>(out)[t] = ld4(X + (size_t)idx[r] * W + g * 8);
+}
+
+__global__ void k_edge_x(int nnz, const bf16* __restrict__ h, const bf16* __restrict__ e, const int* __restrict__ rows,
+                         const int* __restrict__ cols, bf16* __restrict__ X) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // 24 groups per edge
+  if (t >= nnz * 24) return;
+  const int k = t / 24, g = t % 24;
+  uint4 v;
+  if (g < 8) v = ld4(h + (size_t)rows[k] * W + g * 8);
+  else if (g < 16) v = ld4(h + (size_t)cols[k] * W + (g - 8) * 8);
+  else v = ld4(e + (size_t)k * W + (g - 16) * 8);
+  reinterpret_cast<uint4*>(X)[t] = v;
+}
+
+__global__ void k_node_x(int n, const bf16* __restrict__ h, const bf16* __restrict__ a, bf16* __restrict__ X) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // 16 groups per node
+  if (t >= n * 16) return;
+  const int i = t / 16, g = t % 16;
+  reinterpret_cast<uint4*>(X)[t] = g < 8 ? ld4(h + (size_t)i * W + g * 8) : ld4(a + (size_t)i * W + (g - 8) * 8);
+}
+
+// out = bf16(d * (act > 0)) over rows x 64
+__global__ void k_relu_grad(long long count, const float* __restrict__ d, const bf16* __restrict__ act,
+                            bf16* __restrict__ out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  out[t] = __float2bfloat16_rn(__bfloat162float(act[t]) > 0.f ? d[t] : 0.f);
+}
+
+// dm = de + da[row]; out = bf16(dm * (m > 0))
+__global__ void k_edge_grad(int nnz, const float* __restrict__ de, const float* __restrict__ da,
+                            const int* __restrict__ rows, const bf16* __restrict__ m, bf16* __restrict__ out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nnz * W) return;
+  const int e = (int)(t / W), c = (int)(t % W);
+  const float dm = de[t] + da[(size_t)rows[e] * W + c];
+  out[t] = __float2bfloat16_rn(__bfloat162float(m[t]) > 0.f ? dm : 0.f);
+}
+
+// dh += dXn[:, :64]; da = dXn[:, 64:] / deg
+__global__ void k_node_post(int n, const int* __restrict__ off, const float* __restrict__ dXn, float* __restrict__ dh,
+                            float* __restrict__ da) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * W) return;
+  const int i = (int)(t / W), c = (int)(t % W);
+  const float deg = (float)(off[i + 1] - off[i]);
+  dh[t] += dXn[(size_t)i * 2 * W + c];
+  da[t] = dXn[(size_t)i * 2 * W + W + c] / deg;
+}
+
+// de += dX[:, 128:192]
+__global__ void k_edge_post_e(int nnz, const float* __restrict__ dX, float* __restrict__ de) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nnz * W) return;
+  const int e = (int)(t / W), c = (int)(t % W);
+  de[t] += dX[(size_t)e * 3 * W + 2 * W + c];
+}
+
+// dh[i] += sum over row i of dX[e][0:64] + dX[rev e][64:128]
+__global__ void k_edge_post_h(int n, const int* __restrict__ off, const int* __restrict__ rev,
+                              const float* __restrict__ dX, float* __restrict__ dh) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * W) return;
+  const int i = (int)(t / W), c = (int)(t % W);
+  float s = 0.f;
+  for (int e = off[i]; e < off[i + 1]; ++e) s += dX[(size_t)e * 3 * W + c] + dX[(size_t)rev[e] * 3 * W + W + c];
+  dh[t] += s;
+}
+
+__global__ void k_scatter_rows(int R, const int* __restrict__ idx, const float* __restrict__ src,
+                               float* __restrict__ dst) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)R * W) return;
+  const int r = (int)(t / W), c = (int)(t % W);
+  dst[(size_t)idx[r] * W + c] = src[t];
+}
+
+__global__ void k_adam(int n, float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// ------------------------------------------------------------ FSAI apply
+template <class T>
+__global__ void k_fsai_y(int n, const int* __restrict__ off, const int* __restrict__ diag, const int* __restrict__ cols,
+                         const float* __restrict__ G, const float* __restrict__ scale, const T* __restrict__ r,
+                         T* __restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  T acc[3] = {0, 0, 0};
+  for (int e = off[i]; e <= diag[i]; ++e) {
+    const int j = cols[e];
+    const float* g = G + (size_t)e * 9;
+    const T t0 = r[3 * j] * (T)scale[3 * j], t1 = r[3 * j + 1] * (T)scale[3 * j + 1],
+            t2 = r[3 * j + 2] * (T)scale[3 * j + 2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) acc[a] += (T)g[3 * a] * t0 + (T)g[3 * a + 1] * t1 + (T)g[3 * a + 2] * t2;
+  }
+  y[3 * i] = acc[0];
+  y[3 * i + 1] = acc[1];
+  y[3 * i + 2] = acc[2];
+}
+
+template <class T>
+__global__ void k_fsai_z(int n, const int* __restrict__ off, const int* __restrict__ diag, const int* __restrict__ cols,
+                         const int* __restrict__ rev, const float* __restrict__ G, const float* __restrict__ scale,
+                         const T* __restrict__ y, T* __restrict__ z) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  T acc[3] = {0, 0, 0};
+  for (int e = diag[j]; e < off[j + 1]; ++e) {
+    const int i = cols[e];  // i >= j: block (i, j) of G^ sits at rev[e]
+    const float* g = G + (size_t)rev[e] * 9;
+    const T y0 = y[3 * i], y1 = y[3 * i + 1], y2 = y[3 * i + 2];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) acc[b] += (T)g[b] * y0 + (T)g[3 + b] * y1 + (T)g[6 + b] * y2;
+  }
+  z[3 * j] = acc[0] * (T)scale[3 * j];
+  z[3 * j + 1] = acc[1] * (T)scale[3 * j + 1];
+  z[3 * j + 2] = acc[2] * (T)scale[3 * j + 2];
+}
+
+inline int grid_for(long long n, int b = 256) { return (int)((n + b - 1) / b); }
+
+struct Carve {
+  uint8_t* p;
+  size_t left;
+  template <class T>
+  T* take(size_t count) {
+    const size_t bytes = (count * sizeof(T) + 255) & ~(size_t)255;
+    if (bytes > left) return nullptr;
+    T* r = reinterpret_cast<T*>(p);
+    p += bytes;
+    left -= bytes;
+    return r;
+  }
+};
+
+bool graph_ok(const ipcb_graph* g) {
+  return g && g->n > 0 && g->nnz >= g->n && g->offsets && g->columns && g->rows && g->rev && g->diag && g->lower &&
+         g->n_lower == (g->nnz + g->n) / 2;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ipcb_mpnn_param_count(void) { return P_COUNT; }
+int ipcb_mpnn_packed_count(void) { return K_COUNT; }
+
+int ipcb_mpnn_pack(const float* params, void* packed, ipcb_stream s) {
+  if (!params || !packed) {
+    ipcb::set_error_msg("mpnn_pack: null pointer");
+    return IPCB_E_ARG;
+  }
+  k_pack<<<grid_for(K_COUNT), 256, 0, (cudaStream_t)s>>>(params, (bf16*)packed);
+  return ipcb::check_launch("ipcb_mpnn_pack");
+}
+
+size_t ipcb_mpnn_graph_workspace(int n) { return 2 * ((size_t)n * 4 + 256) + ipcb::scan::scratch_bytes(n); }
+
+int ipcb_mpnn_graph(ipcb_graph* g, int* status, void* ws, size_t ws_bytes, ipcb_stream s) {
+  if (!graph_ok(g) || !status || !ws || ws_bytes < ipcb_mpnn_graph_workspace(g->n)) {
+    ipcb::set_error_msg("mpnn_graph: bad arguments (n_lower must be (nnz + n) / 2)");
+    return IPCB_E_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)s;
+  Carve c{(uint8_t*)ws, ws_bytes};
+  int* start = c.take<int>(g->n);
+  void* sc = c.take<uint8_t>(ipcb::scan::scratch_bytes(g->n));
+  k_graph_rows<<<grid_for(g->n), 256, 0, st>>>(g->n, g->offsets, g->columns, g->rows, g->rev, g->diag, start, status);
+  ipcb::scan::exclusive(start, g->n, sc, (int*)nullptr, st);
+  k_graph_lower<<<grid_for(g->n), 256, 0, st>>>(g->n, g->offsets, g->diag, start, g->lower);
+  return ipcb::check_launch("ipcb_mpnn_graph");
+}
+
+int ipcb_mpnn_features(const ipcb_graph* g, int fp64, const void* values, float* scale, float* ahat, void* x,
+                       void* y, int* status, ipcb_stream s) {
+  if (!graph_ok(g) || !values || !scale || !ahat || !x || !y || !status) {
+    ipcb::set_error_msg("mpnn_features: bad arguments");
+    return IPCB_E_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)s;
+  if (fp64) {
+    k_scale<double><<<grid_for(g->n), 256, 0, st>>>(g->n, g->diag, (const double*)values, scale, status);
+    k_edge_features<double><<<grid_for(g->nnz), 256, 0, st>>>(g->nnz, g->rows, g->columns, (const double*)values,
+                                                              scale, ahat, (bf16*)y);
+  } else {
+    k_scale<float><<<grid_for(g->n), 256, 0, st>>>(g->n, g->diag, (const float*)values, scale, status);
+    k_edge_features<float><<<grid_for(g->nnz), 256, 0, st>>>(g->nnz, g->rows, g->columns, (const float*)values,
+                                                             scale, ahat, (bf16*)y);
+  }
+  k_node_features<<<grid_for(g->n), 256, 0, st>>>(g->n, g->offsets, g->columns, g->diag, ahat, (bf16*)x);
+  return ipcb::check_launch("ipcb_mpnn_features");
+}
+
+int ipcb_mpnn_forward(const ipcb_graph* g, const void* packed, const float* params, const void* x, const void* y,
+                      ipcb_mpnn_tape* tape, float* G, int* status, ipcb_stream s) {
+  if (!graph_ok(g) || !packed || !params || !x || !y || !tape || !tape->h || !tape->e || !tape->agg || !G ||
+      !status || (tape->training && (!tape->m || !tape->a || !tape->u))) {
+    ipcb::set_error_msg("mpnn_forward: bad arguments");
+    return IPCB_E_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)s;
+  const bf16* P = (const bf16*)packed;
+  const int n = g->n, nnz = g->nnz;
+  const bool tr = tape->training != 0;
+  bf16* H = (bf16*)tape->h;
+  bf16* E = (bf16*)tape->e;
+  auto hbuf = [&](int l) { return H + (size_t)(tr ? l : (l & 1)) * n * W; };
+  auto ebuf = [&](int l) { return E + (size_t)(tr ? l : (l & 1)) * nnz * W; };
+  int rc;
+  rc = launch_mlp<64, 1>(n, StageDense{(const bf16*)x, IN, IN}, EpiBiasRelu{params + P_BHIN, hbuf(0)},
+                         P + K_ENC_H, status, st, "mpnn node encoder");
+  if (rc) return rc;
+  rc = launch_mlp<64, 1>(nnz, StageDense{(const bf16*)y, IN, IN}, EpiBiasRelu{params + P_BEIN, ebuf(0)},
+                         P + K_ENC_E, status, st, "mpnn edge encoder");
+  if (rc) return rc;
+  for (int l = 0; l < LAYERS; ++l) {
+    const float* pl = params + P_LAYER0 + l * P_LAYER;
+    bf16* m = tr ? (bf16*)tape->m + (size_t)l * nnz * W : nullptr;
+    bf16* a = tr ? (bf16*)tape->a + (size_t)l * n * W : nullptr;
+    bf16* u = tr ? (bf16*)tape->u + (size_t)l * n * W : nullptr;
+    if (cudaMemsetAsync(tape->agg, 0, sizeof(float) * n * W, st) != cudaSuccess) return ipcb::check_launch("agg");
+    rc = launch_mlp<64, 3>(nnz, StageEdge{hbuf(l), ebuf(l), g->rows, g->columns},
+                           EpiEdge{pl + O_B1, ebuf(l), ebuf(l + 1), m, tape->agg, g->rows}, P + K_W1T + l * W * 3 * W,
+                           status, st, "mpnn message");
+    if (rc) return rc;
+    rc = launch_mlp<64, 2>(n, StageNode{hbuf(l), tape->agg, g->offsets, a}, EpiNode{pl + O_B2, hbuf(l), hbuf(l + 1), u},
+                           P + K_W2T + l * W * 2 * W, status, st, "mpnn update");
+    if (rc) return rc;
+  }
+  return launch_mlp<32, 1>(g->n_lower, StageGather{ebuf(LAYERS), g->lower},
+                           EpiHead{params + P_BOFF, params + P_BDG, g->lower, g->rows, g->columns, G}, P + K_HEADT,
+                           status, st, "mpnn head");
+}
+
+int ipcb_mpnn_loss(const ipcb_graph* g, const float* ahat, const float* G, float* T, double* acc, void* dG,
+                   double weight, ipcb_stream s) {
+  if (!graph_ok(g) || !ahat || !G || !T || !acc) {
+    ipcb::set_error_msg("mpnn_loss: bad arguments");
+    return IPCB_E_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)s;
+  if (!dG) {
+    k_fsai_T<<<grid_for(g->n_lower), 256, 0, st>>>(g->n_lower, g->lower, g->rows, g->columns, g->offsets, g->diag,
+                                                   ahat, G, T, acc);
+    k_fsai_logdet<<<grid_for(g->n), 256, 0, st>>>(g->n, g->diag, G, acc);
+  } else {
+    k_fsai_dG<<<grid_for(g->n_lower), 256, 0, st>>>(g->n_lower, g->n, g->lower, g->rows, g->columns, G, T, acc,
+                                                    weight, (bf16*)dG);
+  }
+  return ipcb::check_launch("ipcb_mpnn_loss");
+}
+
+size_t ipcb_mpnn_backward_workspace(int n, int nnz, int n_lower) {
+  const size_t big = (size_t)nnz * 3 * W > (size_t)n * 2 * W ? (size_t)nnz * 3 * W : (size_t)n * 2 * W;
+  const size_t rowsmax = (size_t)(nnz > n ? nnz : n);
+  size_t b = 0;
+  auto add = [&](size_t bytes) { b += (bytes + 255) & ~(size_t)255; };
+  add(sizeof(float) * n * W);                 // dh
+  add(sizeof(float) * nnz * W);               // de
+  add(sizeof(float) * n * W);                 // da
+  add(sizeof(float) * (big > (size_t)n_lower * W ? big : (size_t)n_lower * W));  // dX
+  add(sizeof(bf16) * (big > (size_t)n_lower * W ? big : (size_t)n_lower * W));   // X
+  add(sizeof(bf16) * rowsmax * W);            // dY
+  return b + 256;
+}
+
+int ipcb_mpnn_backward(const ipcb_graph* g, const void* packed, const float* params, const void* x, const void* y,
+                       const ipcb_mpnn_tape* tape, const void* dG, float* grad, int* status, void* ws,
+                       size_t ws_bytes, ipcb_stream s) {
+  (void)params;
+  if (!graph_ok(g) || !packed || !x || !y || !tape || !tape->training || !dG || !grad || !status || !ws ||
+      ws_bytes < ipcb_mpnn_backward_workspace(g->n, g->nnz, g->n_lower)) {
+    ipcb::set_error_msg("mpnn_backward: bad arguments");
+    return IPCB_E_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)s;
+  const bf16* P = (const bf16*)packed;
+  const int n = g->n, nnz = g->nnz, L = g->n_lower;
+  const size_t big = (size_t)nnz * 3 * W > (size_t)n * 2 * W ? (size_t)nnz * 3 * W : (size_t)n * 2 * W;
+  const size_t bigl = big > (size_t)L * W ? big : (size_t)L * W;
+  Carve c{(uint8_t*)ws, ws_bytes};
+  float* dh = c.take<float>((size_t)n * W);
+  float* de = c.take<float>((size_t)nnz * W);
+  float* da = c.take<float>((size_t)n * W);
+  float* dX = c.take<float>(bigl);
+  bf16* X = c.take<bf16>(bigl);
+  bf16* dY = c.take<bf16>((size_t)(nnz > n ? nnz : n) * W);
+  const bf16* H = (const bf16*)tape->h;
+  const bf16* E = (const bf16*)tape->e;
+  const bf16* Mt = (const bf16*)tape->m;
+  const bf16* At = (const bf16*)tape->a;
+  const bf16* Ut = (const bf16*)tape->u;
+  const bf16* dGb = (const bf16*)dG;
+  int rc;
+  // head
+  k_gather_rows<<<grid_for((long long)L * 8), 256, 0, st>>>(L, E + (size_t)LAYERS * nnz * W, g->lower, X);
+  rc = launch_wgrad<1, 32>(L, X, W, W, dGb, 64,
+                           EpiGradHead{grad + P_WOFF, grad + P_BOFF, grad + P_WDG, grad + P_BDG}, status, st,
+                           "mpnn head wgrad");
+  if (rc) return rc;
+  rc = launch_mlp<64, 1>(L, StageDense{dGb, 64, 64}, EpiF32{dX, W}, P + K_HEAD, status, st, "mpnn head dx");
+  if (rc) return rc;
+  cudaMemsetAsync(de, 0, sizeof(float) * nnz * W, st);
+  cudaMemsetAsync(dh, 0, sizeof(float) * n * W, st);
+  k_scatter_rows<<<grid_for((long long)L * W), 256, 0, st>>>(L, g->lower, dX, de);
+  for (int l = LAYERS - 1; l >= 0; --l) {
+    const bf16* h = H + (size_t)l * n * W;
+    const bf16* e = E + (size_t)l * nnz * W;
+    const bf16* m = Mt + (size_t)l * nnz * W;
+    const bf16* a = At + (size_t)l * n * W;
+    const bf16* u = Ut + (size_t)l * n * W;
+    float* gl = grad + P_LAYER0 + l * P_LAYER;
+    // node update: h_out = h + relu([h, a] W2 + b2)
+    k_relu_grad<<<grid_for((long long)n * W), 256, 0, st>>>((long long)n * W, dh, u, dY);
+    k_node_x<<<grid_for((long long)n * 16), 256, 0, st>>>(n, h, a, X);
+    rc = launch_wgrad<2, 64>(n, X, 2 * W, 2 * W, dY, W, EpiGrad{gl + O_W2, gl + O_B2, 2 * W, W}, status, st,
+                             "mpnn update wgrad");
+    if (rc) return rc;
+    rc = launch_mlp<128, 1>(n, StageDense{dY, W, W}, EpiF32{dX, 2 * W}, P + K_W2 + l * 2 * W * W, status, st,
+                            "mpnn update dx");
+    if (rc) return rc;
+    k_node_post<<<grid_for((long long)n * W), 256, 0, st>>>(n, g->offsets, dX, dh, da);
+    // message: e_out = e + m, m = relu([h_i, h_j, e] W1 + b1), a = mean m
+    k_edge_grad<<<grid_for((long long)nnz * W), 256, 0, st>>>(nnz, de, da, g->rows, m, dY);
+    k_edge_x<<<grid_for((long long)nnz * 24), 256, 0, st>>>(nnz, h, e, g->rows, g->columns, X);
+    rc = launch_wgrad<2, 64>(nnz, X, 3 * W, 3 * W, dY, W, EpiGrad{gl + O_W1, gl + O_B1, 3 * W, W}, status, st,
+                             "mpnn message wgrad");
+    if (rc) return rc;
+    rc = launch_mlp<192, 1>(nnz, StageDense{dY, W, W}, EpiF32{dX, 3 * W}, P + K_W1 + l * 3 * W * W, status, st,
+                            "mpnn message dx");
+    if (rc) return rc;
+    k_edge_post_e<<<grid_for((long long)nnz * W), 256, 0, st>>>(nnz, dX, de);
+    k_edge_post_h<<<grid_for((long long)n * W), 256, 0, st>>>(n, g->offsets, g->rev, dX, dh);
+  }
+  // encoders
+  k_relu_grad<<<grid_for((long long)n * W), 256, 0, st>>>((long long)n * W, dh, H, dY);
+  rc = launch_wgrad<1, 64>(n, (const bf16*)x, IN, IN, dY, W, EpiGrad{grad + P_WHIN, grad + P_BHIN, IN, W}, status,
+                           st, "mpnn node encoder wgrad");
+  if (rc) return rc;
+  k_relu_grad<<<grid_for((long long)nnz * W), 256, 0, st>>>((long long)nnz * W, de, E, dY);
+  rc = launch_wgrad<1, 64>(nnz, (const bf16*)y, IN, IN, dY, W, EpiGrad{grad + P_WEIN, grad + P_BEIN, IN, W}, status,
+                           st, "mpnn edge encoder wgrad");
+  if (rc) return rc;
+  return ipcb::check_launch("ipcb_mpnn_backward");
+}
+
+int ipcb_adam(int n, float* params, const float* grad, float* m, float* v, float lr, float beta1, float beta2,
+              float eps, int t, ipcb_stream s) {
+  if (n < 0 || !params || !grad || !m || !v || t < 1) {
+    ipcb::set_error_msg("adam: bad arguments");
+    return IPCB_E_ARG;
+  }
+  const float c1 = 1.f - powf(beta1, (float)t), c2 = 1.f - powf(beta2, (float)t);
+  k_adam<<<grid_for(n), 256, 0, (cudaStream_t)s>>>(n, params, grad, m, v, lr, beta1, beta2, eps, c1, c2);
+  return ipcb::check_launch("ipcb_adam");
+}
+
+int ipcb_fsai_apply(const ipcb_graph* g, const float* G, const float* scale, int fp64, const void* r, void* tmp,
+                    void* z, ipcb_stream s) {
+  if (!graph_ok(g) || !G || !scale || !r || !tmp || !z) {
+    ipcb::set_error_msg("fsai_apply: bad arguments");
+    return IPCB_E_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)s;
+  if (fp64) {
+    k_fsai_y<double><<<grid_for(g->n, 128), 128, 0, st>>>(g->n, g->offsets, g->diag, g->columns, G, scale,
+                                                     (const double*)r, (double*)tmp);
+    k_fsai_z<double><<<grid_for(g->n, 128), 128, 0, st>>>(g->n, g->offsets, g->diag, g->columns, g->rev, G, scale,
+                                                     (const double*)tmp, (double*)z);
+  } else {
+    k_fsai_y<float><<<grid_for(g->n, 128), 128, 0, st>>>(g->n, g->offsets, g->diag, g->columns, G, scale, (const float*)r,
+                                                    (float*)tmp);
+    k_fsai_z<float><<<grid_for(g->n, 128), 128, 0, st>>>(g->n, g->offsets, g->diag, g->columns, g->rev, G, scale,
+                                                    (const float*)tmp, (float*)z);
+  }
+  return ipcb::check_launch("ipcb_fsai_apply");
+}
+
+}  // extern "C"

@@ -124,10 +124,9 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 
 // D[128 x N] (+)= A[128 x 64C] * B[N x 64C]^T from SW128 K-major tiles at
 // shared addresses a_base (128 rows) and b_base (N rows).  Issued by one
-// thread; completion is signalled on mbar.
+// thread; the caller commits to an mbarrier afterwards.
 template <int N, int C>
-__device__ __forceinline__ void issue_tile(uint32_t tmem_d, uint32_t a_base, uint32_t b_base, bool accumulate,
-                                           uint64_t* mbar) {
+__device__ __forceinline__ void issue(uint32_t tmem_d, uint32_t a_base, uint32_t b_base, bool accumulate) {
   constexpr uint32_t idesc = idesc_bf16_f32(N);
 #pragma unroll
   for (int c = 0; c < C; ++c)
@@ -137,6 +136,12 @@ __device__ __forceinline__ void issue_tile(uint32_t tmem_d, uint32_t a_base, uin
       const uint64_t b = desc_sw128(b_base + c * N * 128 + s * 32);
       mma_bf16(tmem_d, a, b, idesc, (accumulate || c > 0 || s > 0) ? 1u : 0u);
     }
+}
+
+template <int N, int C>
+__device__ __forceinline__ void issue_tile(uint32_t tmem_d, uint32_t a_base, uint32_t b_base, bool accumulate,
+                                           uint64_t* mbar) {
+  issue<N, C>(tmem_d, a_base, b_base, accumulate);
   commit(mbar);
 }
 

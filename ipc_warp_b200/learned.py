@@ -1,0 +1,256 @@
+"""Learned preconditioner for the Newton PCG solve: a message-passing net
+over the 3x3-block graph of the Newton matrix predicts a factorised sparse
+approximate inverse (FSAI) ``M^-1 = S G^T G S`` on the lower block pattern
+(include/ipcb.h, ipc_warp_b200/csrc/mpnn.cu).
+
+The reference solves the Newton system with cg or cuDSS LDLT
+(time_integrator_base.py:470-507); this preconditioner replaces the
+identity/diagonal one inside PCG, and the direct solve stays the fallback and
+judge (``newton.FEMContactSolver``).  Training is unsupervised: the Kaporin
+condition number of ``G A G^T`` (exactly computable on the pattern of G) is
+minimised with Adam, on Newton systems the simulator itself produces; the
+forward and backward passes run in the package's tcgen05 kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .bsr import BsrMatrix
+
+WIDTH, IN_DIM, LAYERS = 64, 16, 4
+
+
+def _param_sizes():
+    """(name, shape) in the master-vector order of the kernels."""
+    out = [("W_hin", (IN_DIM, WIDTH)), ("b_hin", (WIDTH,)), ("W_ein", (IN_DIM, WIDTH)), ("b_ein", (WIDTH,))]
+    for l in range(LAYERS):
+        out += [(f"W1_{l}", (3 * WIDTH, WIDTH)), (f"b1_{l}", (WIDTH,)), (f"W2_{l}", (2 * WIDTH, WIDTH)),
+                (f"b2_{l}", (WIDTH,))]
+    out += [("W_off", (WIDTH, 9)), ("b_off", (9,)), ("W_dg", (WIDTH, 9)), ("b_dg", (9,))]
+    return out
+
+
+PARAMS = _param_sizes()
+PARAM_COUNT = sum(int(np.prod(s)) for _, s in PARAMS)
+
+
+def flatten(params: dict) -> np.ndarray:
+    return np.concatenate([np.asarray(params[k], np.float64).reshape(-1) for k, _ in PARAMS]).astype(np.float32)
+
+
+def unflatten(vec) -> dict:
+    vec = np.asarray(vec)
+    out, o = {}, 0
+    for k, s in PARAMS:
+        n = int(np.prod(s))
+        out[k] = vec[o:o + n].reshape(s)
+        o += n
+    return out
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-initialised trunk, zero output heads (the net starts as Jacobi)."""
+    rng = np.random.default_rng(seed)
+    p = {}
+    for k, s in PARAMS:
+        if k.startswith("b") or k in ("W_off", "W_dg"):
+            p[k] = np.zeros(s)
+        else:
+            p[k] = rng.normal(scale=math.sqrt(2.0 / s[0]), size=s)
+    return flatten(p)
+
+
+class Graph:
+    """rows / rev / diag / lower of a canonical BSR pattern (device)."""
+
+    def __init__(self, A: BsrMatrix, nnz: int | None = None):
+        self.n = A.nrow
+        self.nnz = A.nnz_sync() if nnz is None else int(nnz)
+        if (self.nnz + self.n) % 2:
+            raise ValueError("pattern is not structurally symmetric")
+        self.n_lower = (self.nnz + self.n) // 2
+        dev = A.device
+        i32 = dict(dtype=torch.int32, device=dev)
+        self.offsets = A.offsets
+        self.columns = A.columns
+        self.rows = torch.empty(self.nnz, **i32)
+        self.rev = torch.empty(self.nnz, **i32)
+        self.diag = torch.empty(self.n, **i32)
+        self.lower = torch.empty(self.n_lower, **i32)
+        self.c = N.Graph(self.n, self.nnz, self.n_lower, N.ptr(self.offsets), N.ptr(self.columns), N.ptr(self.rows),
+                         N.ptr(self.rev), N.ptr(self.diag), N.ptr(self.lower))
+        status = torch.zeros(1, **i32)
+        ws = torch.empty(N.size("ipcb_mpnn_graph_workspace", self.n), dtype=torch.uint8, device=dev)
+        N.call("ipcb_mpnn_graph", ctypes.byref(self.c), N.ptr(status), N.ptr(ws), ws.numel(), N.stream_handle())
+        if int(status.item()) & 16:
+            raise ValueError("pattern is not symmetric or lacks a diagonal block")
+
+
+class Net:
+    """FP32 master parameters and their BF16 operand copies."""
+
+    def __init__(self, params: np.ndarray | None = None, device="cuda", seed: int = 0):
+        assert N.lib().ipcb_mpnn_param_count() == PARAM_COUNT
+        vec = init_params(seed) if params is None else np.asarray(params, np.float32)
+        self.device = torch.device(device)
+        self.params = torch.tensor(vec, dtype=torch.float32, device=self.device)
+        self.packed = torch.empty(N.lib().ipcb_mpnn_packed_count(), dtype=torch.bfloat16, device=self.device)
+        self.pack()
+
+    def pack(self):
+        N.call("ipcb_mpnn_pack", N.ptr(self.params), N.ptr(self.packed), N.stream_handle())
+
+    def save(self, path: str):
+        np.save(path, self.params.cpu().numpy())
+
+    @staticmethod
+    def load(path: str, device="cuda") -> "Net":
+        return Net(np.load(path), device=device)
+
+
+@dataclass
+class System:
+    """One Newton matrix prepared for the net."""
+    A: BsrMatrix
+    graph: Graph
+    scale: torch.Tensor  # float32 (n, 3)
+    ahat: torch.Tensor   # float32 (nnz, 9)
+    x: torch.Tensor      # bf16 (n, 16)
+    y: torch.Tensor      # bf16 (nnz, 16)
+
+    @staticmethod
+    def from_bsr(A: BsrMatrix, graph: Graph | None = None) -> "System":
+        g = graph if graph is not None else Graph(A)
+        dev = A.device
+        f32 = dict(dtype=torch.float32, device=dev)
+        scale = torch.empty((g.n, 3), **f32)
+        ahat = torch.empty((g.nnz, 9), **f32)
+        x = torch.empty((g.n, IN_DIM), dtype=torch.bfloat16, device=dev)
+        y = torch.empty((g.nnz, IN_DIM), dtype=torch.bfloat16, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        N.call("ipcb_mpnn_features", ctypes.byref(g.c), int(A.dtype == torch.float64), N.ptr(A.values), N.ptr(scale),
+               N.ptr(ahat), N.ptr(x), N.ptr(y), N.ptr(status), N.stream_handle())
+        if int(status.item()) & 16:
+            raise ValueError("non-positive diagonal entry")
+        return System(A, g, scale, ahat, x, y)
+
+
+class _Tape:
+    def __init__(self, g: Graph, training: bool, dev):
+        b = dict(dtype=torch.bfloat16, device=dev)
+        nh = LAYERS + 1 if training else 2
+        self.h = torch.empty((nh, g.n, WIDTH), **b)
+        self.e = torch.empty((nh, g.nnz, WIDTH), **b)
+        self.m = torch.empty((LAYERS, g.nnz, WIDTH), **b) if training else None
+        self.a = torch.empty((LAYERS, g.n, WIDTH), **b) if training else None
+        self.u = torch.empty((LAYERS, g.n, WIDTH), **b) if training else None
+        self.agg = torch.empty((g.n, WIDTH), dtype=torch.float32, device=dev)
+        opt = lambda t: N.ptr(t) if t is not None else None
+        self.c = N.Tape(N.ptr(self.h), N.ptr(self.e), opt(self.m), opt(self.a), opt(self.u), N.ptr(self.agg),
+                        int(training))
+
+
+def forward(net: Net, sysm: System, training: bool = False, G: torch.Tensor | None = None):
+    """G^ (float32 (nnz, 3, 3), valid on the lower blocks) and the tape."""
+    g = sysm.graph
+    dev = sysm.A.device
+    tape = _Tape(g, training, dev)
+    G = torch.zeros((g.nnz, 3, 3), dtype=torch.float32, device=dev) if G is None else G
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    N.call("ipcb_mpnn_forward", ctypes.byref(g.c), N.ptr(net.packed), N.ptr(net.params), N.ptr(sysm.x), N.ptr(sysm.y),
+           ctypes.byref(tape.c), N.ptr(G), N.ptr(status), N.stream_handle())
+    if int(status.item()):
+        raise RuntimeError(f"mpnn forward status {int(status.item())}")
+    return G, tape
+
+
+def kaporin(sysm: System, G: torch.Tensor, want_grad: bool = False, weight: float = 1.0):
+    """Loss log(tr(G A^ G^T)/N) - (2/N) sum log|det G_ii| and, optionally,
+    its gradient in the padded bf16 head layout."""
+    g = sysm.graph
+    dev = G.device
+    T = torch.empty((g.nnz, 9), dtype=torch.float32, device=dev)
+    acc = torch.zeros(2, dtype=torch.float64, device=dev)
+    N.call("ipcb_mpnn_loss", ctypes.byref(g.c), N.ptr(sysm.ahat), N.ptr(G), N.ptr(T), N.ptr(acc), None, 0.0,
+           N.stream_handle())
+    dG = None
+    if want_grad:
+        dG = torch.empty((g.n_lower, 64), dtype=torch.bfloat16, device=dev)
+        N.call("ipcb_mpnn_loss", ctypes.byref(g.c), N.ptr(sysm.ahat), N.ptr(G), N.ptr(T), N.ptr(acc), N.ptr(dG),
+               float(weight), N.stream_handle())
+    tr, logdet = acc.tolist()
+    Nd = 3 * g.n
+    return math.log(tr / Nd) - 2.0 * logdet / Nd, dG
+
+
+def backward(net: Net, sysm: System, tape: _Tape, dG: torch.Tensor, grad: torch.Tensor):
+    g = sysm.graph
+    dev = dG.device
+    ws = torch.empty(N.size("ipcb_mpnn_backward_workspace", g.n, g.nnz, g.n_lower), dtype=torch.uint8, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    N.call("ipcb_mpnn_backward", ctypes.byref(g.c), N.ptr(net.packed), N.ptr(net.params), N.ptr(sysm.x),
+           N.ptr(sysm.y), ctypes.byref(tape.c), N.ptr(dG), N.ptr(grad), N.ptr(status), N.ptr(ws), ws.numel(),
+           N.stream_handle())
+    if int(status.item()):
+        raise RuntimeError(f"mpnn backward status {int(status.item())}")
+
+
+class Trainer:
+    """Adam on the Kaporin loss over a list of systems."""
+
+    def __init__(self, net: Net, lr: float = 1e-3, betas=(0.9, 0.999), eps: float = 1e-8):
+        self.net = net
+        self.lr, self.betas, self.eps = lr, betas, eps
+        z = lambda: torch.zeros_like(net.params)
+        self.m, self.v, self.grad = z(), z(), z()
+        self.t = 0
+
+    def step(self, batch: list[System]) -> float:
+        self.grad.zero_()
+        total = 0.0
+        for sysm in batch:
+            G, tape = forward(self.net, sysm, training=True)
+            loss, dG = kaporin(sysm, G, want_grad=True, weight=1.0 / len(batch))
+            backward(self.net, sysm, tape, dG, self.grad)
+            total += loss / len(batch)
+        self.t += 1
+        N.call("ipcb_adam", self.net.params.numel(), N.ptr(self.net.params), N.ptr(self.grad), N.ptr(self.m),
+               N.ptr(self.v), float(self.lr), float(self.betas[0]), float(self.betas[1]), float(self.eps), self.t,
+               N.stream_handle())
+        self.net.pack()
+        return total
+
+
+class LearnedPreconditioner:
+    """z = S G^T G S r for the PCG of newton.py: ``LearnedPreconditioner(net)``
+    is a factory (called with the Newton matrix) like ``BlockJacobi``."""
+
+    def __init__(self, net: Net):
+        self.net = net
+
+    def __call__(self, A: BsrMatrix) -> "_Apply":
+        sysm = System.from_bsr(A)
+        G, _ = forward(self.net, sysm)
+        return _Apply(sysm, G, A.dtype)
+
+
+class _Apply:
+    def __init__(self, sysm: System, G: torch.Tensor, dtype):
+        self.sysm, self.G, self.dtype = sysm, G, dtype
+        self.tmp = torch.empty((sysm.graph.n, 3), dtype=dtype, device=G.device)
+
+    def __call__(self, r: torch.Tensor) -> torch.Tensor:
+        z = torch.empty_like(r)
+        N.call("ipcb_fsai_apply", ctypes.byref(self.sysm.graph.c), N.ptr(self.G), N.ptr(self.sysm.scale),
+               int(self.dtype == torch.float64), N.ptr(r), N.ptr(self.tmp), N.ptr(z), N.stream_handle())
+        return z
+
+
+DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "mpnn_fsai.npy")

@@ -1,0 +1,290 @@
+"""CPU oracle of the learned preconditioner (test infrastructure only; the
+product never imports this module).
+
+The network is a message-passing net over the 3x3-block sparsity graph of a
+Newton matrix A (n block rows, the edges are the stored blocks, self loops
+included, sorted by (row, column)).  It outputs a block lower-triangular
+factor G^ on the lower pattern of A such that M^-1 = S G^T G^ S (S = diag(A)
+^-1/2 per scalar) preconditions A: a factorised sparse approximate inverse
+(FSAI).  Training minimises the Kaporin condition number of G^ A^ G^T
+(A^ = S A S):
+
+  loss = log(tr(G^ A^ G^T) / N) - (2 / N) sum_i log|det G^_ii|,  N = 3 n,
+
+which equals (log K(G^ A^ G^T) + log det A^) / N; it is 0 for G^ = I (Jacobi)
+and needs only products on the pattern of G^.  The reference has no learned
+component (its solve is cg or cuDSS LDLT, time_integrator_base.py:470-507);
+this module restates the algorithm of ipc_warp_b200/csrc/mpnn.cu in float64
+with the same bfloat16 rounding points, so that the device kernels can be
+checked value by value.
+
+Rounding points (as the kernels): inputs x, y, the weights used in the
+products, and the stored activations h, e, m, u and the aggregate a are
+bfloat16; products accumulate in float; biases are float; G^ is float.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+WIDTH = 64
+IN_DIM = 16
+LAYERS = 4
+
+
+ROUND = True  # set False for finite-difference checks of the backward pass
+
+
+def bf16(a):
+    """Round float values to bfloat16 (nearest even), returned as float64."""
+    if not ROUND:
+        return np.asarray(a, dtype=np.float64)
+    a32 = np.ascontiguousarray(a, dtype=np.float32)
+    u = a32.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    out = (r & 0xFFFFFFFF).astype(np.uint32).view(np.float32)
+    return out.astype(np.float64)
+
+
+def relu(a):
+    return np.maximum(a, 0.0)
+
+
+@dataclass
+class Graph:
+    n: int
+    offsets: np.ndarray  # (n+1,)
+    cols: np.ndarray     # (E,)
+    rows: np.ndarray     # (E,)
+    rev: np.ndarray      # (E,) index of (j, i)
+    lower: np.ndarray    # (L,) edge indices with col <= row, in edge order
+    diag: np.ndarray     # (n,) edge index of (i, i)
+
+
+def graph(offsets, cols) -> Graph:
+    offsets = np.asarray(offsets, np.int64)
+    cols = np.asarray(cols, np.int64)
+    n = len(offsets) - 1
+    rows = np.repeat(np.arange(n), np.diff(offsets))
+    key = rows * n + cols
+    order = {int(k): e for e, k in enumerate(key)}
+    rev = np.array([order[int(c) * n + int(r)] for r, c in zip(rows, cols)], np.int64)
+    lower = np.nonzero(cols <= rows)[0]
+    diag = np.array([order[i * n + i] for i in range(n)], np.int64)
+    return Graph(n, offsets, cols, rows, rev, lower, diag)
+
+
+def scaled(g: Graph, vals):
+    """A^ = S A S, S = diag(A)^-1/2 per scalar dof; returns (A^ blocks, s)."""
+    vals = np.asarray(vals, np.float64).reshape(-1, 3, 3)
+    d = np.stack([vals[g.diag][:, a, a] for a in range(3)], axis=1)  # (n, 3)
+    s = 1.0 / np.sqrt(d)
+    Ah = vals * s[g.rows][:, :, None] * s[g.cols][:, None, :]
+    return Ah, s
+
+
+def features(g: Graph, Ah):
+    """Node inputs x (n, 16) and edge inputs y (E, 16), bfloat16."""
+    deg = np.diff(g.offsets).astype(np.float64)
+    fro = np.sqrt((Ah * Ah).sum(axis=(1, 2)))
+    off = np.where(g.cols != g.rows, fro, 0.0)
+    rowsum = np.zeros(g.n)
+    np.add.at(rowsum, g.rows, off)
+    x = np.zeros((g.n, IN_DIM))
+    x[:, :9] = Ah[g.diag].reshape(-1, 9)
+    x[:, 9] = np.log1p(deg)
+    x[:, 10] = rowsum
+    y = np.zeros((len(g.cols), IN_DIM))
+    y[:, :9] = Ah.reshape(-1, 9)
+    y[:, 9] = fro
+    y[:, 10] = (g.cols == g.rows).astype(np.float64)
+    return bf16(x), bf16(y)
+
+
+def init_params(seed=0, zero_head=True):
+    """Weights (in, out) with biases; the output heads start at zero so that
+    the initial factor is G^ = I (Jacobi)."""
+    rng = np.random.default_rng(seed)
+
+    def lin(i, o, scale=None):
+        s = np.sqrt(2.0 / i) if scale is None else scale
+        return rng.normal(scale=s, size=(i, o)), np.zeros(o)
+
+    p = {}
+    p["W_hin"], p["b_hin"] = lin(IN_DIM, WIDTH)
+    p["W_ein"], p["b_ein"] = lin(IN_DIM, WIDTH)
+    for l in range(LAYERS):
+        p[f"W1_{l}"], p[f"b1_{l}"] = lin(3 * WIDTH, WIDTH)
+        p[f"W2_{l}"], p[f"b2_{l}"] = lin(2 * WIDTH, WIDTH)
+    for name in ("off", "dg"):
+        W, b = lin(WIDTH, 9, scale=0.0 if zero_head else 0.05)
+        p[f"W_{name}"], p[f"b_{name}"] = W, b
+    return p
+
+
+PARAM_ORDER = (["W_hin", "b_hin", "W_ein", "b_ein"]
+               + [f"{k}_{l}" for l in range(LAYERS) for k in ("W1", "b1", "W2", "b2")]
+               + ["W_off", "b_off", "W_dg", "b_dg"])
+
+
+def forward(g: Graph, x, y, p, keep=False):
+    """G^ on the lower edges (L, 3, 3); with keep=True also the stored
+    activations for the backward pass."""
+    W = {k: (bf16(v) if k.startswith("W") else v) for k, v in p.items()}
+    deg = np.diff(g.offsets).astype(np.float64)
+    h = bf16(relu(x @ W["W_hin"] + W["b_hin"]))
+    e = bf16(relu(y @ W["W_ein"] + W["b_ein"]))
+    tape = []
+    for l in range(LAYERS):
+        X = np.concatenate([h[g.rows], h[g.cols], e], axis=1)
+        m = bf16(relu(X @ W[f"W1_{l}"] + W[f"b1_{l}"]))
+        agg = np.zeros((g.n, WIDTH))
+        np.add.at(agg, g.rows, m)
+        a = bf16(agg / deg[:, None])
+        Xn = np.concatenate([h, a], axis=1)
+        u = bf16(relu(Xn @ W[f"W2_{l}"] + W[f"b2_{l}"]))
+        tape.append((h, e, m, a, u))
+        e = bf16(e + m)
+        h = bf16(h + u)
+    el = e[g.lower]
+    is_diag = g.cols[g.lower] == g.rows[g.lower]
+    out = np.where(is_diag[:, None], el @ W["W_dg"] + W["b_dg"], el @ W["W_off"] + W["b_off"])
+    G = out.reshape(-1, 3, 3)
+    G[is_diag] += np.eye(3)
+    if keep:
+        return G, dict(tape=tape, h=h, e=e, W=W, is_diag=is_diag)
+    return G
+
+
+def _lower_index(g: Graph):
+    """map (row, col) -> lower slot, and per row the lower slots"""
+    slot = {}
+    for s, e in enumerate(g.lower):
+        slot[(int(g.rows[e]), int(g.cols[e]))] = s
+    return slot
+
+
+def random_spd(nb, seed, band=5, couplings=3):
+    """A symmetric positive definite block matrix with a banded random pattern
+    (diagonal plus PSD pair couplings), as (offsets, cols, vals)."""
+    rng = np.random.default_rng(seed)
+    blocks = {}
+
+    def add(i, j, B):
+        blocks[(i, j)] = blocks.get((i, j), 0.0) + B
+
+    for i in range(nb):
+        add(i, i, np.eye(3) * (0.5 + rng.uniform()) + np.diag(rng.uniform(0, 2, 3)))
+        if i == 0:
+            continue
+        for j in rng.choice(np.arange(max(0, i - band), i), size=min(i, couplings), replace=False):
+            B = rng.normal(size=(3, 3))
+            Gm = B @ B.T
+            add(i, i, Gm)
+            add(int(j), int(j), Gm)
+            add(i, int(j), -0.9 * Gm)
+            add(int(j), i, -0.9 * Gm)
+    keys = sorted(blocks)
+    offsets = np.zeros(nb + 1, np.int64)
+    for (i, _) in keys:
+        offsets[i + 1] += 1
+    offsets = np.cumsum(offsets)
+    cols = np.array([j for (_, j) in keys], np.int64)
+    vals = np.stack([blocks[k] for k in keys])
+    return offsets, cols, vals
+
+
+def loss_and_grad_G(g: Graph, Ah, G):
+    """Kaporin loss of G^ A^ G^T and its gradient w.r.t. G^ (L, 3, 3)."""
+    n = g.n
+    N = 3 * n
+    full = {(int(r), int(c)): e for e, (r, c) in enumerate(zip(g.rows, g.cols))}
+    lower_rows = [[] for _ in range(n)]
+    for s, e in enumerate(g.lower):
+        lower_rows[int(g.rows[e])].append((int(g.cols[e]), s))
+    T = np.zeros_like(G)
+    for i in range(n):
+        for (j, sj) in lower_rows[i]:
+            acc = np.zeros((3, 3))
+            for (k, sk) in lower_rows[i]:
+                e = full.get((k, j))
+                if e is not None:
+                    acc += G[sk] @ Ah[e]
+            T[sj] = acc
+    tr = float((T * G).sum())
+    dsl = [None] * n
+    logdet = 0.0
+    dG = 2.0 * T / tr
+    for i in range(n):
+        s = None
+        for (j, sj) in lower_rows[i]:
+            if j == i:
+                s = sj
+        D = G[s]
+        sign, ld = np.linalg.slogdet(D)
+        logdet += ld
+        dG[s] -= (2.0 / N) * np.linalg.inv(D).T
+    loss = np.log(tr / N) - (2.0 / N) * logdet
+    return loss, dG, tr
+
+
+def backward(g: Graph, x, y, p, dG, cache):
+    """Gradients of sum(dG * G^) w.r.t. every parameter (dict), in float64,
+    with the forward's rounding points held fixed."""
+    W = cache["W"]
+    deg = np.diff(g.offsets).astype(np.float64)
+    is_diag = cache["is_diag"]
+    grads = {k: np.zeros_like(v) for k, v in p.items()}
+    dout = dG.reshape(-1, 9)
+    el = cache["e"][g.lower]
+    grads["W_dg"] = el[is_diag].T @ dout[is_diag]
+    grads["b_dg"] = dout[is_diag].sum(axis=0)
+    grads["W_off"] = el[~is_diag].T @ dout[~is_diag]
+    grads["b_off"] = dout[~is_diag].sum(axis=0)
+    de = np.zeros((len(g.cols), WIDTH))
+    de[g.lower] = np.where(is_diag[:, None], dout @ W["W_dg"].T, dout @ W["W_off"].T)
+    dh = np.zeros((g.n, WIDTH))
+    for l in reversed(range(LAYERS)):
+        h, e, m, a, u = cache["tape"][l]
+        # h_out = h + u ; e_out = e + m
+        du = dh * (u > 0)
+        Xn = np.concatenate([h, a], axis=1)
+        grads[f"W2_{l}"] = Xn.T @ du
+        grads[f"b2_{l}"] = du.sum(axis=0)
+        dXn = du @ W[f"W2_{l}"].T
+        dh_in = dh + dXn[:, :WIDTH]
+        da = dXn[:, WIDTH:]
+        dm = de + (da / deg[:, None])[g.rows]
+        dmp = dm * (m > 0)
+        X = np.concatenate([h[g.rows], h[g.cols], e], axis=1)
+        grads[f"W1_{l}"] = X.T @ dmp
+        grads[f"b1_{l}"] = dmp.sum(axis=0)
+        dX = dmp @ W[f"W1_{l}"].T
+        np.add.at(dh_in, g.rows, dX[:, :WIDTH])
+        np.add.at(dh_in, g.cols, dX[:, WIDTH:2 * WIDTH])
+        de = de + dX[:, 2 * WIDTH:]
+        dh = dh_in
+    h0 = bf16(relu(x @ W["W_hin"] + W["b_hin"]))
+    e0 = bf16(relu(y @ W["W_ein"] + W["b_ein"]))
+    dh0 = dh * (h0 > 0)
+    de0 = de * (e0 > 0)
+    grads["W_hin"] = x.T @ dh0
+    grads["b_hin"] = dh0.sum(axis=0)
+    grads["W_ein"] = y.T @ de0
+    grads["b_ein"] = de0.sum(axis=0)
+    return grads
+
+
+def apply_preconditioner(g: Graph, G, s, r):
+    """z = S G^T G S r for r (n, 3)."""
+    t = s * r
+    y = np.zeros_like(t)
+    for k, e in enumerate(g.lower):
+        i, j = int(g.rows[e]), int(g.cols[e])
+        y[i] += G[k] @ t[j]
+    z = np.zeros_like(t)
+    for k, e in enumerate(g.lower):
+        i, j = int(g.rows[e]), int(g.cols[e])
+        z[j] += G[k].T @ y[i]
+    return s * z
