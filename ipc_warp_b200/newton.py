@@ -110,7 +110,7 @@ class FEMContactSolver(ContactBarrierMixin):
                  gravity=(0.0, -9.8, 0.0), h: float = 1e-2, fixed: np.ndarray | None = None,
                  attachment_stiffness: float = 1e11, dtype=torch.float32, device="cuda", vel_tol: float = 5e-2,
                  max_newton: int = 100, tol: float = 1e-4, maxiter: int = 200, exclude_same_body: bool = False,
-                 linear_solver: str = "pcg", direct_fallback: bool = True):
+                 linear_solver: str = "pcg", direct_fallback: bool = True, preconditioner: str = "jacobi"):
         self.h = float(h)
         self.material = MATERIALS[material]
         self.mu, self.lam = lame(E, nu)
@@ -149,13 +149,24 @@ class FEMContactSolver(ContactBarrierMixin):
         ContactBarrierMixin.__init__(self)
         self.disable_self_collision = exclude_same_body
         self._elastic = Triplets.zeros(16 * self.n_tets, dtype, self.device)
-        self.precond_factory = BlockJacobi
+        if preconditioner == "jacobi":
+            self.precond_factory = BlockJacobi
+        elif preconditioner == "learned":
+            from .learned import DEFAULT_WEIGHTS, LearnedPreconditioner, Net
+
+            self.precond_factory = LearnedPreconditioner(Net.load(DEFAULT_WEIGHTS, device=self.device))
+        else:
+            raise ValueError(f"unknown preconditioner {preconditioner!r}")
         if linear_solver not in ("pcg", "direct"):
             raise ValueError(f"unknown linear solver {linear_solver!r}")
         self.linear_solver = linear_solver
         self.direct_fallback = direct_fallback
         self.direct_solver = None  # DirectSolver, created on first use
         self.frame = 0
+        self.time = 0.0
+        # prescribed boundary (compute_compensation, time_integrator_base.py:440-467):
+        # callable(t) -> (V, 3) attachment targets of the fixed vertices at time t
+        self.boundary = None
         self.stats = StepStats()
 
     # ----------------------------------------------------------- energies
@@ -274,6 +285,8 @@ class FEMContactSolver(ContactBarrierMixin):
     def step(self) -> StepStats:
         """time_integrator_base.py:375-401."""
         self.stats = StepStats()
+        if self.boundary is not None:
+            self.x_target.copy_(torch.as_tensor(self.boundary(self.time + self.h), dtype=self.dtype))
         for it in range(self.max_newton):
             alpha, norm = self.newton_iteration()
             self.stats.newton_iterations = it + 1
@@ -285,4 +298,5 @@ class FEMContactSolver(ContactBarrierMixin):
         self.states.xdot.copy_((x - self.states.x0) / self.h)
         self.states.x0.copy_(x)
         self.frame += 1
+        self.time += self.h
         return self.stats

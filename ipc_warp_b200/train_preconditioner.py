@@ -1,0 +1,143 @@
+"""Train the learned FSAI preconditioner on Newton systems the simulator
+produces, and write its weights.
+
+    python -m ipc_warp_b200.train_preconditioner --out weights.npy
+
+Systems come from two scenes run with ``newton.FEMContactSolver``: two
+neo-Hookean cubes, the upper one falling onto the lower one (the two-cube
+contact setup), and a bundle of StVK rods whose clamped ends counter-rotate
+so that the rods wind together (the rod-twist setup, at a reduced rod
+length).  Every Newton matrix of every step is captured (a copy of the BSR),
+and Adam minimises the mean Kaporin loss over random mini-batches.
+"""
+from __future__ import annotations
+
+import argparse
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import learned as L
+from .bsr import BsrMatrix
+from .newton import FEMContactSolver
+from .scenes import rod_bundle, two_cubes
+
+
+def _copy(A: BsrMatrix) -> BsrMatrix:
+    nnz = A.nnz_sync()
+    B = BsrMatrix(A.nrow, A.ncol, nnz, A.dtype, A.device)
+    B.offsets.copy_(A.offsets)
+    B.columns[:nnz].copy_(A.columns[:nnz])
+    B.values[:nnz].copy_(A.values[:nnz])
+    B.nnz_dev.copy_(A.nnz_dev)
+    return B
+
+
+def capture(solver: FEMContactSolver, steps: int, out: list, limit: int):
+    """Run `steps` time steps, appending a copy of every Newton matrix."""
+    orig = solver.solve
+
+    def solve():
+        if len(out) < limit:
+            out.append(_copy(solver.A))
+        return orig()
+
+    solver.solve = solve
+    try:
+        for _ in range(steps):
+            solver.step()
+    finally:
+        solver.solve = orig
+
+
+def cube_systems(steps: int, seed: int, limit: int, dtype=torch.float32, n: int = 8):
+    sc = two_cubes(n=n, gap=1e-3, angle_deg=15.0, jitter=1e-5, seed=seed, dhat=1e-3, kappa=1e4)
+    fixed = sc.xcs[:, 1] <= sc.xcs[:, 1].min() + 1e-9
+    s = FEMContactSolver(sc, material="neo_hookean", E=1e5, nu=0.4, h=1e-2, fixed=fixed, dtype=dtype, max_newton=20)
+    out = []
+    capture(s, steps, out, limit)
+    return out
+
+
+def twist_targets(sc, omega: float):
+    """Targets of the clamped rod ends: the z-min end turns by +omega t and
+    the z-max end by -omega t about the bundle axis."""
+    x = sc.xcs
+    c = x[:, :2].mean(axis=0)
+    zlo, zhi = x[:, 2].min(), x[:, 2].max()
+    lo = x[:, 2] <= zlo + 1e-9
+    hi = x[:, 2] >= zhi - 1e-9
+
+    def at(t):
+        tgt = x.copy()
+        for mask, sgn in ((lo, 1.0), (hi, -1.0)):
+            a = sgn * omega * t
+            ca, sa = math.cos(a), math.sin(a)
+            d = x[mask, :2] - c
+            tgt[mask, 0] = c[0] + ca * d[:, 0] - sa * d[:, 1]
+            tgt[mask, 1] = c[1] + sa * d[:, 0] + ca * d[:, 1]
+        return tgt
+
+    return lo | hi, at
+
+
+def rod_systems(steps: int, seed: int, limit: int, dtype=torch.float32, side: int = 2, cells=(4, 4, 64),
+                gap_over_dhat: float | None = None):
+    """Twisting rods; with ``gap_over_dhat`` the bundle starts packed with
+    every facing pair of rod sides inside the barrier (contact-heavy
+    systems)."""
+    sc = rod_bundle(n_rods_side=side, cells=cells, seed=seed, kappa=1e4, gap_over_dhat=gap_over_dhat)
+    fixed, at = twist_targets(sc, omega=2.0)
+    s = FEMContactSolver(sc, material="stvk", E=1e6, nu=0.45, h=5e-3, fixed=fixed, gravity=(0.0, 0.0, 0.0),
+                         dtype=dtype, max_newton=20)
+    s.boundary = at
+    out = []
+    capture(s, steps, out, limit)
+    return out
+
+
+def train(systems, steps: int = 400, batch: int = 4, lr: float = 2e-3, seed: int = 0, log_every: int = 50,
+          net: L.Net | None = None):
+    prepared = [L.System.from_bsr(A) for A in systems]
+    net = net or L.Net(seed=seed, device=systems[0].device)
+    tr = L.Trainer(net, lr=lr)
+    rng = np.random.default_rng(seed)
+    history = []
+    for it in range(steps):
+        idx = rng.choice(len(prepared), size=min(batch, len(prepared)), replace=False)
+        loss = tr.step([prepared[i] for i in idx])
+        history.append(loss)
+        if log_every and (it % log_every == 0 or it == steps - 1):
+            print(f"step {it:5d}  kaporin loss {loss:+.5f}", flush=True)
+    return net, history
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=L.DEFAULT_WEIGHTS)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--cube-steps", type=int, default=10)
+    ap.add_argument("--rod-steps", type=int, default=12)
+    ap.add_argument("--limit", type=int, default=120)
+    ap.add_argument("--seed", type=int, default=0)
+    args = ap.parse_args()
+    t0 = time.time()
+    systems = (cube_systems(args.cube_steps, args.seed, args.limit)
+               + rod_systems(args.rod_steps, args.seed + 1, args.limit)
+               + rod_systems(args.rod_steps, args.seed + 2, args.limit, side=3, cells=(4, 4, 32), gap_over_dhat=0.5))
+    print(f"captured {len(systems)} Newton systems in {time.time() - t0:.1f} s", flush=True)
+    t0 = time.time()
+    net, hist = train(systems, steps=args.steps, seed=args.seed)
+    torch.cuda.synchronize()
+    print(f"trained {args.steps} steps in {time.time() - t0:.1f} s; final loss {np.mean(hist[-20:]):+.5f}")
+    import os
+
+    os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
+    net.save(args.out)
+    print(f"wrote {args.out}")
+
+
+if __name__ == "__main__":
+    main()
