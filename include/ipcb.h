@@ -298,6 +298,43 @@ int ipcb_adam(int n, float* params, const float* grad, float* m, float* v, float
 int ipcb_fsai_apply(const ipcb_graph* g, const float* G, const float* scale, int fp64, const void* r, void* tmp,
                     void* z, ipcb_stream s);
 
+/* ---- Device-resident PCG (time_integrator_base.py:502-507, ``cg``) ----
+ * Solves A x = b on the canonical BSR with x0 = 0 to |r| <= tol |b|; the
+ * scalars live in `state` (device), so batches of iterations run without a
+ * host synchronisation (and can be replayed as a CUDA graph); a finished
+ * solve turns further launches into no-ops.  precond 0: block Jacobi (dinv:
+ * inverse diagonal blocks, scalar[9n], from ipcb_block_jacobi); precond 1:
+ * the learned FSAI factor (diag: int32[n] diagonal block indices, g: bf16
+ * [9 nnz] from ipcb_fsai_mirror, scale: float[3n], t: scalar[3n] scratch).
+ * state->status bit 1: breakdown (p.Ap <= 0). */
+typedef struct {
+  double rz, rz_new, pAp, rr, bb, tol2, last_rr;
+  int it, done, maxiter, status;
+} ipcb_pcg_state;
+
+typedef struct {
+  int n, fp64, precond;
+  const int* offsets;
+  const int* columns;
+  const void* values;
+  const void* dinv;
+  const int* diag;
+  const void* g;
+  const float* scale;
+  const void* b;
+  void *x, *r, *z, *p, *q, *t;
+  ipcb_pcg_state* state;
+} ipcb_pcg;
+
+int ipcb_pcg_start(const ipcb_pcg* P, double tol, int maxiter, ipcb_stream s);
+int ipcb_pcg_iterate(const ipcb_pcg* P, int k, ipcb_stream s);
+/* Inverse diagonal blocks (diag may be NULL: found by a row scan). */
+int ipcb_block_jacobi(int n, const int* offsets, const int* columns, const int* diag, const void* values, int fp64,
+                      void* dinv, int* status, ipcb_stream s);
+/* bf16 copy of the FSAI factor for the apply: lower and diagonal blocks as
+ * they are, upper slots holding the transposed lower block. */
+int ipcb_fsai_mirror(const ipcb_graph* g, const float* G, void* gh, ipcb_stream s);
+
 /* ---- BF16 tensor-core GEMM (tcgen05, TMEM accumulator) ----
  * No counterpart in the reference: the building block of the learned
  * preconditioner's kernels, exported for its own tests and for callers that

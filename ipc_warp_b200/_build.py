@@ -22,7 +22,7 @@ DIRECT_LIB_PATH = os.path.join(LIB_DIR, "libipcb200_direct.so")
 OBJ_DIR = os.path.join(HERE, "csrc", "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["lbvh.cu", "dcd.cu", "narrow.cu", "ccd.cu", "bsr.cu", "contact_bsr.cu", "fem.cu", "umma_gemm.cu", "mpnn.cu",
+SOURCES = ["lbvh.cu", "dcd.cu", "narrow.cu", "ccd.cu", "bsr.cu", "contact_bsr.cu", "fem.cu", "umma_gemm.cu", "mpnn.cu", "pcg.cu",
            "noalloc.cu"]
 NOFMAD = {"ccd.cu"}
 DIRECT_SOURCES = ["direct.cu"]

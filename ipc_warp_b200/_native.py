@@ -40,6 +40,18 @@ class Tape(ctypes.Structure):
     _fields_ = [("h", P), ("e", P), ("m", P), ("a", P), ("u", P), ("agg", P), ("training", c_int)]
 
 
+class PcgState(ctypes.Structure):
+    _fields_ = [("rz", c_double), ("rz_new", c_double), ("pAp", c_double), ("rr", c_double), ("bb", c_double),
+                ("tol2", c_double), ("last_rr", c_double), ("it", c_int), ("done", c_int), ("maxiter", c_int),
+                ("status", c_int)]
+
+
+class Pcg(ctypes.Structure):
+    _fields_ = [("n", c_int), ("fp64", c_int), ("precond", c_int), ("offsets", P), ("columns", P), ("values", P),
+                ("dinv", P), ("diag", P), ("g", P), ("scale", P), ("b", P), ("x", P), ("r", P), ("z", P), ("p", P),
+                ("q", P), ("t", P), ("state", P)]
+
+
 SP, CP, BP = ctypes.POINTER(Soup), ctypes.POINTER(Contacts), ctypes.POINTER(Lbvh)
 GP, TP = ctypes.POINTER(Graph), ctypes.POINTER(Tape)
 
@@ -85,6 +97,10 @@ SIGNATURES = {
     "ipcb_mpnn_backward": (c_int, [GP, P, P, P, P, TP, P, P, P, P, c_size_t, P]),
     "ipcb_adam": (c_int, [c_int, P, P, P, P, c_float, c_float, c_float, c_float, c_int, P]),
     "ipcb_fsai_apply": (c_int, [GP, P, P, c_int, P, P, P, P]),
+    "ipcb_pcg_start": (c_int, [ctypes.POINTER(Pcg), c_double, c_int, P]),
+    "ipcb_pcg_iterate": (c_int, [ctypes.POINTER(Pcg), c_int, P]),
+    "ipcb_block_jacobi": (c_int, [c_int, P, P, P, P, c_int, P, P, P]),
+    "ipcb_fsai_mirror": (c_int, [GP, P, P, P]),
     "ipcb_umma_gemm_bf16": (c_int, [c_int, c_int, c_int, P, P, P, P, P]),
     "ipcb_tet_rest": (c_int, [c_int, P, P, c_int, P, P, P]),
     "ipcb_tet_hessian": (c_int, [c_int, c_int, P, P, c_int, P, P, c_double, c_double, P, P, P, P, P]),

