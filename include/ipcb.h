@@ -222,11 +222,15 @@ int ipcb_bsr_mv(int nrow, const int* offsets, const int* columns, const void* va
  * No counterpart in the reference (its linear solve is cg or cuDSS LDLT,
  * time_integrator_base.py:470-507).  A 4-layer, width-64 message-passing net
  * over the 3x3-block graph of a Newton matrix A (canonical BSR: sorted,
- * structurally symmetric, every diagonal block present) predicts a block
- * lower-triangular factor G^ on the lower pattern of A, and
- * M^-1 = S G^T G^ S (S = diag(A)^-1/2 per scalar) preconditions PCG.
- * Products run on the tensor cores (BF16 operands, FP32 accumulation);
- * G^ and everything the solve touches are FP32.
+ * structurally symmetric, every diagonal block present) predicts the row
+ * directions H of a block lower-triangular factor on the lower pattern of A;
+ * ipcb_fsai_normalize scales each block row exactly (G^_i = C_i^-1 H_i with
+ * C_i C_i^T = M_i = H_i A^ H_i^T, A^ = S A S, S = diag(A)^-1/2 per scalar), so
+ * every diagonal block of G^ A^ G^T is I, and M^-1 = S G^T G^ S
+ * preconditions PCG.  The training loss is (1/N) sum_i log det M_i (the
+ * Kaporin condition number of the normalised factor, up to a constant).
+ * Products run on the tensor cores (BF16 operands, FP32 accumulation); H, G^
+ * and everything the solve touches are FP32.
  *
  * Graph arrays (device, int32): rows[nnz] (row of each block), rev[nnz]
  * (index of the transposed block), diag[n] (index of (i, i)), lower[n_lower]
@@ -248,7 +252,7 @@ typedef struct {
 
 /* Parameter layout: FP32 master vector (weights stored in x out, row-major,
  * then the bias, per linear map: W_hin b_hin W_ein b_ein, per layer
- * W1 b1 W2 b2, then W_off b_off W_dg b_dg) and the BF16 operand copies the
+ * W1 b1 W2 b2, then the head W_off b_off) and the BF16 operand copies the
  * kernels read (made by ipcb_mpnn_pack). */
 int ipcb_mpnn_param_count(void);
 int ipcb_mpnn_packed_count(void);
@@ -264,7 +268,7 @@ int ipcb_mpnn_features(const ipcb_graph* g, int fp64, const void* values, float*
 /* Activations: bf16 buffers; h[5][n*64], e[5][nnz*64] (layer inputs and the
  * final state), m[4][nnz*64], a[4][n*64], u[4][n*64]; for inference only
  * h[0..1] and e[0..1] are used (ping-pong) and m, a, u may be NULL.
- * agg: float[n*64] scratch.  G: float[9 nnz] written on the lower blocks. */
+ * agg: float[n*64] scratch. */
 typedef struct {
   void* h;
   void* e;
@@ -275,17 +279,26 @@ typedef struct {
   int training;
 } ipcb_mpnn_tape;
 
-int ipcb_mpnn_forward(const ipcb_graph* g, const void* packed, const float* params, const void* x, const void* y,
-                      ipcb_mpnn_tape* tape, float* G, int* status, ipcb_stream s);
-/* Kaporin loss parts of G^ A^ G^T: acc[0] += tr(G^ A^ G^T), acc[1] += sum_i
- * log|det G^_ii| (double).  With dG != NULL, a second call after the first
- * has completed writes the loss gradient w.r.t. G^ scaled by `weight`
- * (bf16[64 n_lower], columns 0..8 for off-diagonal blocks, 16..24 for
- * diagonal blocks) using T (float[9 nnz] scratch). */
-int ipcb_mpnn_loss(const ipcb_graph* g, const float* ahat, const float* G, float* T, double* acc, void* dG,
-                   double weight, ipcb_stream s);
+/* H: float[9 nnz], written on the lower blocks: H_ii = I and
+ * H_ij = (rho_i out - I) A^_ij, with out the head output read as a 3x3
+ * matrix and rho_i = c / (1 + c) (c: the row's summed |A^_ij|_F, node
+ * feature 10); a zero head gives first-order FSAI (ahat, x from
+ * ipcb_mpnn_features). */
+int ipcb_mpnn_forward(const ipcb_graph* g, const void* packed, const float* params, const float* ahat, const void* x,
+                      const void* y, ipcb_mpnn_tape* tape, float* H, int* status, ipcb_stream s);
+/* G^ (float[9 nnz], lower blocks) from H: T (float[9 nnz] scratch) gets
+ * T_ij = sum_k H_ik A^_kj, minv (float[9 n]) gets M_i^-1, acc[0] (double,
+ * device) += sum_i log det M_i.  A row whose M_i is not positive definite
+ * keeps G^ = H and raises IPCB_STATUS_PATTERN. */
+int ipcb_fsai_normalize(const ipcb_graph* g, const float* ahat, const float* H, float* T, float* minv, float* G,
+                        double* acc, int* status, ipcb_stream s);
+/* Gradient of weight * (1/N) sum_i log det M_i w.r.t. the head outputs,
+ * after ipcb_fsai_normalize: dG bf16[64 n_lower], columns 0..8 (zero rows for
+ * diagonal blocks). */
+int ipcb_mpnn_loss_grad(const ipcb_graph* g, const float* ahat, const void* x, const float* T, const float* minv,
+                        void* dG, double weight, ipcb_stream s);
 size_t ipcb_mpnn_backward_workspace(int n, int nnz, int n_lower);
-/* Gradients of sum(dG * G^) w.r.t. the parameters, added to grad
+/* Gradients of sum(dG * head outputs) w.r.t. the parameters, added to grad
  * (float[param_count]).  Needs the training tape of the forward call. */
 int ipcb_mpnn_backward(const ipcb_graph* g, const void* packed, const float* params, const void* x, const void* y,
                        const ipcb_mpnn_tape* tape, const void* dG, float* grad, int* status, void* ws,

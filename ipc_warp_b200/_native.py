@@ -91,8 +91,9 @@ SIGNATURES = {
     "ipcb_mpnn_graph_workspace": (c_size_t, [c_int]),
     "ipcb_mpnn_graph": (c_int, [GP, P, P, c_size_t, P]),
     "ipcb_mpnn_features": (c_int, [GP, c_int, P, P, P, P, P, P, P]),
-    "ipcb_mpnn_forward": (c_int, [GP, P, P, P, P, TP, P, P, P]),
-    "ipcb_mpnn_loss": (c_int, [GP, P, P, P, P, P, c_double, P]),
+    "ipcb_mpnn_forward": (c_int, [GP, P, P, P, P, P, TP, P, P, P]),
+    "ipcb_fsai_normalize": (c_int, [GP, P, P, P, P, P, P, P, P]),
+    "ipcb_mpnn_loss_grad": (c_int, [GP, P, P, P, P, P, c_double, P]),
     "ipcb_mpnn_backward_workspace": (c_size_t, [c_int, c_int, c_int]),
     "ipcb_mpnn_backward": (c_int, [GP, P, P, P, P, TP, P, P, P, P, c_size_t, P]),
     "ipcb_adam": (c_int, [c_int, P, P, P, P, c_float, c_float, c_float, c_float, c_int, P]),

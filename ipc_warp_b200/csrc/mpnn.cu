@@ -1,5 +1,6 @@
 // Learned preconditioner: a message-passing net over the 3x3-block graph of
-// the Newton matrix whose output is an FSAI factor G^ (include/ipcb.h).
+// the Newton matrix predicts the row directions H of an FSAI factor, and an
+// exact per-row normalisation turns them into G^ (include/ipcb.h).
 //
 // Every dense product runs on the tensor cores through one templated kernel,
 // k_mlp: a persistent CTA stages 128 rows of its A operand into an SW128
@@ -42,18 +43,17 @@ constexpr int P_LAYER0 = P_BEIN + W;
 constexpr int P_LAYER = 3 * W * W + W + 2 * W * W + W;  // W1 b1 W2 b2
 constexpr int O_W1 = 0, O_B1 = 3 * W * W, O_W2 = O_B1 + W, O_B2 = O_W2 + 2 * W * W;
 constexpr int P_WOFF = P_LAYER0 + LAYERS * P_LAYER, P_BOFF = P_WOFF + W * 9;
-constexpr int P_WDG = P_BOFF + 9, P_BDG = P_WDG + W * 9;
-constexpr int P_COUNT = P_BDG + 9;
+constexpr int P_COUNT = P_BOFF + 9;
 
 // BF16 operand layout (all offsets in elements, multiples of 8)
 constexpr int K_ENC_H = 0;                        // [64 out][64 in]  (in >= 16 zero)
 constexpr int K_ENC_E = K_ENC_H + W * 64;         // [64][64]
 constexpr int K_W1T = K_ENC_E + W * 64;           // LAYERS x [64 out][192 in]
 constexpr int K_W2T = K_W1T + LAYERS * W * 3 * W; // LAYERS x [64 out][128 in]
-constexpr int K_HEADT = K_W2T + LAYERS * W * 2 * W; // [32 out][64 in]: rows 0..8 off, 16..24 diag
-constexpr int K_W1 = K_HEADT + 32 * W;            // LAYERS x [192 in][64 out]
+constexpr int K_HEADT = K_W2T + LAYERS * W * 2 * W; // [16 out][64 in]: rows 0..8 the head
+constexpr int K_W1 = K_HEADT + 16 * W;            // LAYERS x [192 in][64 out]
 constexpr int K_W2 = K_W1 + LAYERS * 3 * W * W;   // LAYERS x [128 in][64 out]
-constexpr int K_HEAD = K_W2 + LAYERS * 2 * W * W; // [64 in][64 cols]: cols 0..8 off, 16..24 diag
+constexpr int K_HEAD = K_W2 + LAYERS * 2 * W * W; // [64 in][64 cols]: cols 0..8 the head
 constexpr int K_COUNT = K_HEAD + W * 64;
 
 __global__ void k_pack(const float* __restrict__ p, bf16* __restrict__ q) {
@@ -75,7 +75,6 @@ __global__ void k_pack(const float* __restrict__ p, bf16* __restrict__ q) {
   } else if (t < K_W1) {
     const int r = t - K_HEADT, o = r / W, k = r % W;
     if (o < 9) v = p[P_WOFF + k * 9 + o];
-    else if (o >= 16 && o < 25) v = p[P_WDG + k * 9 + (o - 16)];
   } else if (t < K_W2) {
     const int r = t - K_W1, l = r / (3 * W * W), k = (r % (3 * W * W)) / W, o = r % W;
     v = p[P_LAYER0 + l * P_LAYER + O_W1 + k * W + o];
@@ -85,7 +84,6 @@ __global__ void k_pack(const float* __restrict__ p, bf16* __restrict__ q) {
   } else {
     const int r = t - K_HEAD, k = r / 64, c = r % 64;
     if (c < 9) v = p[P_WOFF + k * 9 + c];
-    else if (c >= 16 && c < 25) v = p[P_WDG + k * 9 + (c - 16)];
   }
   q[t] = __float2bfloat16_rn(v);
 }
@@ -259,18 +257,49 @@ struct EpiNode {  // u = relu(v + b2); h_out = h_in + u
   }
 };
 
-struct EpiHead {  // G^ of a lower block from the off-diagonal or diagonal head
-  const float *b_off, *b_dg;
+__device__ __forceinline__ float block_fro(const float* __restrict__ a) {
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) s += a[k] * a[k];
+  return sqrtf(s);
+}
+
+// rho_i = c / (1 + c), c = sum of |A^_ij|_F over the off-diagonal blocks of
+// row i (node feature 10)
+__device__ __forceinline__ float coupling(const bf16* __restrict__ x, int i) {
+  const float c = __bfloat162float(x[(size_t)i * IN + 10]);
+  return c / (1.f + c);
+}
+
+// Row directions on a lower block (out: the head output read as a 3x3
+// matrix): H_ii = I and H_ij = (rho_i out - I) A^_ij.  A zero head gives
+// first-order FSAI; a weakly coupled row stays at first order, where it is
+// accurate, whatever the head outputs.
+struct EpiHead {
+  const float *b_off, *ahat;
+  const bf16* x;
   const int *lower, *rows, *cols;
-  float* G;
+  float* H;
   __device__ void apply(int row, bool valid, int col0, const float (&v)[32], float*, int*) const {
     if (!valid || col0 != 0) return;
     const int e = __ldg(lower + row);
-    const bool dg = __ldg(rows + e) == __ldg(cols + e);
-    float* g = G + (size_t)e * 9;
+    const int i = __ldg(rows + e);
+    float* h = H + (size_t)e * 9;
+    if (i == __ldg(cols + e)) {
 #pragma unroll
-    for (int k = 0; k < 9; ++k)
-      g[k] = dg ? v[16 + k] + __ldg(b_dg + k) + ((k % 4) == 0 ? 1.f : 0.f) : v[k] + __ldg(b_off + k);
+      for (int k = 0; k < 9; ++k) h[k] = (k % 4) == 0 ? 1.f : 0.f;
+      return;
+    }
+    const float* a = ahat + (size_t)e * 9;
+    const float rho = coupling(x, i);
+    float p[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) p[k] = rho * (v[k] + __ldg(b_off + k)) - ((k % 4) == 0 ? 1.f : 0.f);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        h[3 * r + c] = p[3 * r] * __ldg(a + c) + p[3 * r + 1] * __ldg(a + 3 + c) + p[3 * r + 2] * __ldg(a + 6 + c);
   }
 };
 
@@ -405,18 +434,13 @@ struct EpiGrad {
   }
 };
 
-struct EpiGradHead {  // columns 0..8 -> off-diagonal head, 16..24 -> diagonal head
-  float *dW_off, *db_off, *dW_dg, *db_dg;
+struct EpiGradHead {  // columns 0..8: the head
+  float *dW_off, *db_off;
   __device__ void add(int f, int col0, const float (&v)[32]) const {
     if (col0 != 0 || f > W) return;
     for (int k = 0; k < 9; ++k) {
-      if (f < W) {
-        atomicAdd(dW_off + f * 9 + k, v[k]);
-        atomicAdd(dW_dg + f * 9 + k, v[16 + k]);
-      } else {
-        atomicAdd(db_off + k, v[k]);
-        atomicAdd(db_dg + k, v[16 + k]);
-      }
+      if (f < W) atomicAdd(dW_off + f * 9 + k, v[k]);
+      else atomicAdd(db_off + k, v[k]);
     }
   }
 };
@@ -664,78 +688,113 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// T_ij = sum_{k <= i} G_ik A^_kj over the lower blocks (i, j); acc[0] += <T, G>
+// T_ij = sum_{k <= i} H_ik A^_kj over the lower blocks (i, j)
 __global__ void k_fsai_T(int n_lower, const int* __restrict__ lower, const int* __restrict__ rows,
                          const int* __restrict__ cols, const int* __restrict__ off, const int* __restrict__ diag,
-                         const float* __restrict__ ahat, const float* __restrict__ G, float* __restrict__ T,
-                         double* __restrict__ acc) {
+                         const float* __restrict__ ahat, const float* __restrict__ H, float* __restrict__ T) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  double part = 0.0;
-  if (r < n_lower) {
-    const int e = lower[r], i = rows[e], j = cols[e];
-    float t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int ke = off[i]; ke <= diag[i]; ++ke) {
-      const int k = cols[ke];
-      const int kj = find_col(off, cols, k, j);
-      if (kj >= 0) mm3_acc(t, G + (size_t)ke * 9, ahat + (size_t)kj * 9);
-    }
-    const float* g = G + (size_t)e * 9;
+  if (r >= n_lower) return;
+  const int e = lower[r], i = rows[e], j = cols[e];
+  float t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int ke = off[i]; ke <= diag[i]; ++ke) {
+    const int kj = find_col(off, cols, cols[ke], j);
+    if (kj >= 0) mm3_acc(t, H + (size_t)ke * 9, ahat + (size_t)kj * 9);
+  }
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
-      T[(size_t)e * 9 + q] = t[q];
-      part += (double)t[q] * (double)g[q];
+  for (int q = 0; q < 9; ++q) T[(size_t)e * 9 + q] = t[q];
+}
+
+// Per row: M_i = sum_j T_ij H_ij^T, Cholesky M_i = C C^T, G^_ij = C^-1 H_ij;
+// acc[0] += log det M_i, minv_i = M_i^-1.  A row whose M_i is not positive
+// definite keeps G^ = H and raises IPCB_STATUS_PATTERN.
+__global__ void k_fsai_rows(int n, const int* __restrict__ off, const int* __restrict__ diag,
+                            const float* __restrict__ H, const float* __restrict__ T, float* __restrict__ minv,
+                            float* __restrict__ G, double* __restrict__ acc, int* __restrict__ status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double part = 0.0;
+  if (i < n) {
+    double M[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int e = off[i]; e <= diag[i]; ++e) {
+      const float* t = T + (size_t)e * 9;
+      const float* h = H + (size_t)e * 9;
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          M[3 * r + c] += (double)t[3 * r] * h[3 * c] + (double)t[3 * r + 1] * h[3 * c + 1] +
+                          (double)t[3 * r + 2] * h[3 * c + 2];
+    }
+    // symmetrise, Cholesky
+    const double m00 = M[0], m10 = 0.5 * (M[3] + M[1]), m11 = M[4], m20 = 0.5 * (M[6] + M[2]),
+                 m21 = 0.5 * (M[7] + M[5]), m22 = M[8];
+    bool ok = m00 > 0.0;
+    const double c00 = ok ? sqrt(m00) : 1.0;
+    const double c10 = m10 / c00, c20 = m20 / c00;
+    const double d11 = m11 - c10 * c10;
+    ok = ok && d11 > 0.0;
+    const double c11 = ok ? sqrt(d11) : 1.0;
+    const double c21 = (m21 - c20 * c10) / c11;
+    const double d22 = m22 - c20 * c20 - c21 * c21;
+    ok = ok && d22 > 0.0;
+    const double c22 = ok ? sqrt(d22) : 1.0;
+    double L[9];  // C^-1 (lower triangular)
+    L[0] = 1.0 / c00; L[1] = 0.0; L[2] = 0.0;
+    L[4] = 1.0 / c11; L[3] = -c10 * L[0] / c11; L[5] = 0.0;
+    L[8] = 1.0 / c22; L[6] = -(c20 * L[0] + c21 * L[3]) / c22; L[7] = -c21 * L[4] / c22;
+    if (!ok) {
+      atomicOr(status, IPCB_STATUS_PATTERN);
+      for (int q = 0; q < 9; ++q) L[q] = (q % 4) == 0 ? 1.0 : 0.0;
+    }
+    // M^-1 = L^T L
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        minv[(size_t)i * 9 + 3 * r + c] = (float)(L[r] * L[c] + L[3 + r] * L[3 + c] + L[6 + r] * L[6 + c]);
+    part = ok ? 2.0 * log(c00 * c11 * c22) : 0.0;
+    for (int e = off[i]; e <= diag[i]; ++e) {
+      const float* h = H + (size_t)e * 9;
+      float* g = G + (size_t)e * 9;
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          g[3 * r + c] = (float)(L[3 * r] * h[c] + L[3 * r + 1] * h[3 + c] + L[3 * r + 2] * h[6 + c]);
     }
   }
   part = warp_sum(part);
   if ((threadIdx.x & 31) == 0 && part != 0.0) atomicAdd(acc, part);
 }
 
-__device__ __forceinline__ double det3(const float* g) {
-  return (double)g[0] * ((double)g[4] * g[8] - (double)g[5] * g[7]) -
-         (double)g[1] * ((double)g[3] * g[8] - (double)g[5] * g[6]) +
-         (double)g[2] * ((double)g[3] * g[7] - (double)g[4] * g[6]);
-}
-
-__global__ void k_fsai_logdet(int n, const int* __restrict__ diag, const float* __restrict__ G,
-                              double* __restrict__ acc) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double part = 0.0;
-  if (i < n) part = log(fabs(det3(G + (size_t)diag[i] * 9)));
-  part = warp_sum(part);
-  if ((threadIdx.x & 31) == 0) atomicAdd(acc + 1, part);
-}
-
-// dG = weight * (2 T / tr - (2 / N) [diag] G^-T), written bf16 into the
-// padded head layout (columns 0..8 off-diagonal, 16..24 diagonal)
-__global__ void k_fsai_dG(int n_lower, int n, const int* __restrict__ lower, const int* __restrict__ rows,
-                          const int* __restrict__ cols, const float* __restrict__ G, const float* __restrict__ T,
-                          const double* __restrict__ acc, double weight, bf16* __restrict__ dG) {
+// gradient of weight * (1/N) sum_i log det M_i w.r.t. the head outputs:
+// dH_ij = (2/N) M_i^-1 T_ij, d out = rho_i dH A^T, written bf16 in columns
+// 0..8 of a 64-wide row (zero for diagonal blocks)
+__global__ void k_fsai_dout(int n_lower, int n, const int* __restrict__ lower, const int* __restrict__ rows,
+                            const int* __restrict__ cols, const float* __restrict__ ahat, const bf16* __restrict__ x,
+                            const float* __restrict__ T, const float* __restrict__ minv, double weight,
+                            bf16* __restrict__ dG) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n_lower) return;
-  const int e = lower[r];
-  const bool dg = rows[e] == cols[e];
-  const double tr = acc[0];
-  const double N = 3.0 * n;
-  float d[9];
-#pragma unroll
-  for (int q = 0; q < 9; ++q) d[q] = (float)(weight * 2.0 * (double)T[(size_t)e * 9 + q] / tr);
-  if (dg) {
-    const float* g = G + (size_t)e * 9;
-    const double det = det3(g);
-    // inverse transpose = cofactor matrix / det
-    double cof[9] = {(double)g[4] * g[8] - (double)g[5] * g[7], -((double)g[3] * g[8] - (double)g[5] * g[6]),
-                     (double)g[3] * g[7] - (double)g[4] * g[6], -((double)g[1] * g[8] - (double)g[2] * g[7]),
-                     (double)g[0] * g[8] - (double)g[2] * g[6], -((double)g[0] * g[7] - (double)g[1] * g[6]),
-                     (double)g[1] * g[5] - (double)g[2] * g[4], -((double)g[0] * g[5] - (double)g[2] * g[3]),
-                     (double)g[0] * g[4] - (double)g[1] * g[3]};
-#pragma unroll
-    for (int q = 0; q < 9; ++q) d[q] -= (float)(weight * (2.0 / N) * cof[q] / det);
-  }
+  const int e = lower[r], i = rows[e];
   float row[64];
 #pragma unroll
   for (int q = 0; q < 64; ++q) row[q] = 0.f;
+  if (i != cols[e]) {
+    const float* mi = minv + (size_t)i * 9;
+    const float* t = T + (size_t)e * 9;
+    const float* a = ahat + (size_t)e * 9;
+    const float f = (float)(weight * 2.0 / (3.0 * n)) * coupling(x, i);
+    float dh[9];
 #pragma unroll
-  for (int q = 0; q < 9; ++q) row[(dg ? 16 : 0) + q] = d[q];
+    for (int p = 0; p < 3; ++p)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) dh[3 * p + c] = mi[3 * p] * t[c] + mi[3 * p + 1] * t[3 + c] + mi[3 * p + 2] * t[6 + c];
+#pragma unroll
+    for (int p = 0; p < 3; ++p)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        row[3 * p + c] = f * (dh[3 * p] * a[3 * c] + dh[3 * p + 1] * a[3 * c + 1] + dh[3 * p + 2] * a[3 * c + 2]);
+  }
   uint4* dst = reinterpret_cast<uint4*>(dG + (size_t)r * 64);
 #pragma unroll
   for (int q = 0; q < 8; ++q) dst[q] = pack8(row + 8 * q);
@@ -950,9 +1009,9 @@ int ipcb_mpnn_features(const ipcb_graph* g, int fp64, const void* values, float*
   return ipcb::check_launch("ipcb_mpnn_features");
 }
 
-int ipcb_mpnn_forward(const ipcb_graph* g, const void* packed, const float* params, const void* x, const void* y,
-                      ipcb_mpnn_tape* tape, float* G, int* status, ipcb_stream s) {
-  if (!graph_ok(g) || !packed || !params || !x || !y || !tape || !tape->h || !tape->e || !tape->agg || !G ||
+int ipcb_mpnn_forward(const ipcb_graph* g, const void* packed, const float* params, const float* ahat, const void* x,
+                      const void* y, ipcb_mpnn_tape* tape, float* H, int* status, ipcb_stream s) {
+  if (!graph_ok(g) || !packed || !params || !ahat || !x || !y || !tape || !tape->h || !tape->e || !tape->agg || !H ||
       !status || (tape->training && (!tape->m || !tape->a || !tape->u))) {
     ipcb::set_error_msg("mpnn_forward: bad arguments");
     return IPCB_E_ARG;
@@ -961,10 +1020,10 @@ int ipcb_mpnn_forward(const ipcb_graph* g, const void* packed, const float* para
   const bf16* P = (const bf16*)packed;
   const int n = g->n, nnz = g->nnz;
   const bool tr = tape->training != 0;
-  bf16* H = (bf16*)tape->h;
-  bf16* E = (bf16*)tape->e;
-  auto hbuf = [&](int l) { return H + (size_t)(tr ? l : (l & 1)) * n * W; };
-  auto ebuf = [&](int l) { return E + (size_t)(tr ? l : (l & 1)) * nnz * W; };
+  bf16* Hs = (bf16*)tape->h;
+  bf16* Es = (bf16*)tape->e;
+  auto hbuf = [&](int l) { return Hs + (size_t)(tr ? l : (l & 1)) * n * W; };
+  auto ebuf = [&](int l) { return Es + (size_t)(tr ? l : (l & 1)) * nnz * W; };
   int rc;
   rc = launch_mlp<64, 1>(n, StageDense{(const bf16*)x, IN, IN}, EpiBiasRelu{params + P_BHIN, hbuf(0)},
                          P + K_ENC_H, status, st, "mpnn node encoder");
@@ -986,27 +1045,33 @@ int ipcb_mpnn_forward(const ipcb_graph* g, const void* packed, const float* para
                            P + K_W2T + l * W * 2 * W, status, st, "mpnn update");
     if (rc) return rc;
   }
-  return launch_mlp<32, 1>(g->n_lower, StageGather{ebuf(LAYERS), g->lower},
-                           EpiHead{params + P_BOFF, params + P_BDG, g->lower, g->rows, g->columns, G}, P + K_HEADT,
-                           status, st, "mpnn head");
+  return launch_mlp<16, 1>(g->n_lower, StageGather{ebuf(LAYERS), g->lower},
+                           EpiHead{params + P_BOFF, ahat, (const bf16*)x, g->lower, g->rows, g->columns, H},
+                           P + K_HEADT, status, st, "mpnn head");
 }
 
-int ipcb_mpnn_loss(const ipcb_graph* g, const float* ahat, const float* G, float* T, double* acc, void* dG,
-                   double weight, ipcb_stream s) {
-  if (!graph_ok(g) || !ahat || !G || !T || !acc) {
-    ipcb::set_error_msg("mpnn_loss: bad arguments");
+int ipcb_fsai_normalize(const ipcb_graph* g, const float* ahat, const float* H, float* T, float* minv, float* G,
+                        double* acc, int* status, ipcb_stream s) {
+  if (!graph_ok(g) || !ahat || !H || !T || !minv || !G || !acc || !status) {
+    ipcb::set_error_msg("fsai_normalize: bad arguments");
     return IPCB_E_ARG;
   }
   cudaStream_t st = (cudaStream_t)s;
-  if (!dG) {
-    k_fsai_T<<<grid_for(g->n_lower), 256, 0, st>>>(g->n_lower, g->lower, g->rows, g->columns, g->offsets, g->diag,
-                                                   ahat, G, T, acc);
-    k_fsai_logdet<<<grid_for(g->n), 256, 0, st>>>(g->n, g->diag, G, acc);
-  } else {
-    k_fsai_dG<<<grid_for(g->n_lower), 256, 0, st>>>(g->n_lower, g->n, g->lower, g->rows, g->columns, G, T, acc,
-                                                    weight, (bf16*)dG);
+  k_fsai_T<<<grid_for(g->n_lower), 256, 0, st>>>(g->n_lower, g->lower, g->rows, g->columns, g->offsets, g->diag, ahat,
+                                                 H, T);
+  k_fsai_rows<<<grid_for(g->n), 256, 0, st>>>(g->n, g->offsets, g->diag, H, T, minv, G, acc, status);
+  return ipcb::check_launch("ipcb_fsai_normalize");
+}
+
+int ipcb_mpnn_loss_grad(const ipcb_graph* g, const float* ahat, const void* x, const float* T, const float* minv,
+                        void* dG, double weight, ipcb_stream s) {
+  if (!graph_ok(g) || !ahat || !x || !T || !minv || !dG) {
+    ipcb::set_error_msg("mpnn_loss_grad: bad arguments");
+    return IPCB_E_ARG;
   }
-  return ipcb::check_launch("ipcb_mpnn_loss");
+  k_fsai_dout<<<grid_for(g->n_lower), 256, 0, (cudaStream_t)s>>>(g->n_lower, g->n, g->lower, g->rows, g->columns,
+                                                                  ahat, (const bf16*)x, T, minv, weight, (bf16*)dG);
+  return ipcb::check_launch("ipcb_mpnn_loss_grad");
 }
 
 size_t ipcb_mpnn_backward_workspace(int n, int nnz, int n_lower) {
@@ -1053,8 +1118,7 @@ int ipcb_mpnn_backward(const ipcb_graph* g, const void* packed, const float* par
   int rc;
   // head
   k_gather_rows<<<grid_for((long long)L * 8), 256, 0, st>>>(L, E + (size_t)LAYERS * nnz * W, g->lower, X);
-  rc = launch_wgrad<1, 32>(L, X, W, W, dGb, 64,
-                           EpiGradHead{grad + P_WOFF, grad + P_BOFF, grad + P_WDG, grad + P_BDG}, status, st,
+  rc = launch_wgrad<1, 16>(L, X, W, W, dGb, 64, EpiGradHead{grad + P_WOFF, grad + P_BOFF}, status, st,
                            "mpnn head wgrad");
   if (rc) return rc;
   rc = launch_mlp<64, 1>(L, StageDense{dGb, 64, 64}, EpiF32{dX, W}, P + K_HEAD, status, st, "mpnn head dx");

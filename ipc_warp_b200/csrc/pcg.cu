@@ -11,6 +11,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace ipcb {
@@ -42,60 +44,87 @@ __device__ __forceinline__ double block_sum(double v) {
 template <class T> __device__ __forceinline__ T ldv(const T* p) { return __ldg(p); }
 __device__ __forceinline__ float ldv(const bf16* p) { return __bfloat162float(*p); }
 
-// warp per block row: out_i = sum_k V_k x_{col k} over the row's blocks in
-// [b, e); value index v = lane + 32 t walks the row's 9 (e - b) values
-// contiguously.  transpose_at: block index whose 3x3 is used transposed.
+// Block-row products with 8 lanes per row (4 rows in flight per warp): lane
+// `sub` takes blocks b + sub, b + sub + 8, ... of the row, reads the whole 3x3
+// block (consecutive lanes read consecutive blocks, so a row's values stream
+// contiguously), gathers x of the block's column and accumulates 3 outputs;
+// the 8 lanes then reduce.  xs scales x per scalar (NULL: none);
+// transpose_at: block index used transposed.
+constexpr int kLanes = 8;
+
+template <class T> __device__ __forceinline__ void ld9(const T* __restrict__ v, float (&a)[9]) {
+#pragma unroll
+  for (int q = 0; q < 9; ++q) a[q] = (float)__ldg(v + q);
+}
+__device__ __forceinline__ void ld9(const double* __restrict__ v, double (&a)[9]) {
+#pragma unroll
+  for (int q = 0; q < 9; ++q) a[q] = __ldg(v + q);
+}
+__device__ __forceinline__ void ld9(const bf16* __restrict__ v, float (&a)[9]) {
+#pragma unroll
+  for (int q = 0; q < 9; ++q) a[q] = __bfloat162float(v[q]);
+}
+
 template <class T, class V>
-__device__ __forceinline__ void warp_row_mv(const int* __restrict__ cols, const V* __restrict__ vals, int b, int e,
-                                            const T* __restrict__ x, const float* __restrict__ xs, int transpose_at,
-                                            T& o0, T& o1, T& o2) {
-  const int lane = threadIdx.x & 31;
+__device__ __forceinline__ void row_mv(const int* __restrict__ cols, const V* __restrict__ vals, int b, int e,
+                                       const T* __restrict__ x, const float* __restrict__ xs, int transpose_at,
+                                       T& o0, T& o1, T& o2) {
+  const int sub = threadIdx.x & (kLanes - 1);
+  using A = typename std::conditional<std::is_same<V, double>::value, double, float>::type;
   T a0 = 0, a1 = 0, a2 = 0;
-  const int nv = 9 * (e - b);
-  for (int v = lane; v < nv; v += 32) {
-    const int k = b + v / 9, q = v % 9;
-    int ra = q / 3, cb = q % 3;
+#pragma unroll 2
+  for (int k = b + sub; k < e; k += kLanes) {
     const int c = __ldg(cols + k);
-    if (k == transpose_at) {  // use V^T: entry (ra, cb) of V^T is V(cb, ra)
-      const int t = ra;
-      ra = cb;
-      cb = t;
+    A m[9];
+    ld9(vals + 9LL * k, m);
+    T x0 = x[3 * c], x1 = x[3 * c + 1], x2 = x[3 * c + 2];
+    if (xs) {
+      x0 *= (T)__ldg(xs + 3 * c);
+      x1 *= (T)__ldg(xs + 3 * c + 1);
+      x2 *= (T)__ldg(xs + 3 * c + 2);
     }
-    T xv = x[3 * c + cb];
-    if (xs) xv *= (T)__ldg(xs + 3 * c + cb);
-    const T prod = (T)ldv(vals + 9LL * k + q) * xv;
-    if (ra == 0) a0 += prod;
-    else if (ra == 1) a1 += prod;
-    else a2 += prod;
+    if (k == transpose_at) {
+      a0 += (T)m[0] * x0 + (T)m[3] * x1 + (T)m[6] * x2;
+      a1 += (T)m[1] * x0 + (T)m[4] * x1 + (T)m[7] * x2;
+      a2 += (T)m[2] * x0 + (T)m[5] * x1 + (T)m[8] * x2;
+    } else {
+      a0 += (T)m[0] * x0 + (T)m[1] * x1 + (T)m[2] * x2;
+      a1 += (T)m[3] * x0 + (T)m[4] * x1 + (T)m[5] * x2;
+      a2 += (T)m[6] * x0 + (T)m[7] * x1 + (T)m[8] * x2;
+    }
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    a0 += __shfl_down_sync(0xffffffffu, a0, o);
-    a1 += __shfl_down_sync(0xffffffffu, a1, o);
-    a2 += __shfl_down_sync(0xffffffffu, a2, o);
+  for (int o = kLanes / 2; o > 0; o >>= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+    a2 += __shfl_xor_sync(0xffffffffu, a2, o);
   }
   o0 = a0;
   o1 = a1;
   o2 = a2;
 }
 
-// q = A p ; state.pAp += p.q
+// q = A p ; state.pAp += p.q  (grid-stride row groups: one atomic per block)
 template <class T>
 __global__ void __launch_bounds__(kBlock) k_spmv_dot(int n, const int* __restrict__ off, const int* __restrict__ cols,
                                                      const T* __restrict__ vals, const T* __restrict__ p,
                                                      T* __restrict__ q, ipcb_pcg_state* st) {
   if (st->done) return;
-  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+  const int sub = threadIdx.x & (kLanes - 1);
+  const int groups = (gridDim.x * blockDim.x) / kLanes;
   double part = 0.0;
-  if (row < n) {
+  // every lane of a warp runs the same number of trips (shuffles need all 32)
+  const int trips = (n + groups - 1) / groups;
+  int row = (blockIdx.x * blockDim.x + threadIdx.x) / kLanes;
+  for (int t = 0; t < trips; ++t, row += groups) {
+    const bool ok = row < n;
     T o0, o1, o2;
-    warp_row_mv<T, T>(cols, vals, off[row], off[row + 1], p, nullptr, -1, o0, o1, o2);
-    if (lane == 0) {
+    row_mv<T, T>(cols, vals, ok ? off[row] : 0, ok ? off[row + 1] : 0, p, nullptr, -1, o0, o1, o2);
+    if (ok && sub == 0) {
       q[3 * row] = o0;
       q[3 * row + 1] = o1;
       q[3 * row + 2] = o2;
-      part = (double)p[3 * row] * o0 + (double)p[3 * row + 1] * o1 + (double)p[3 * row + 2] * o2;
+      part += (double)p[3 * row] * o0 + (double)p[3 * row + 1] * o1 + (double)p[3 * row + 2] * o2;
     }
   }
   part = block_sum(part);
@@ -108,14 +137,13 @@ __global__ void __launch_bounds__(kBlock) k_update_xr(int m, T* __restrict__ x, 
                                                       const T* __restrict__ p, const T* __restrict__ q,
                                                       ipcb_pcg_state* st) {
   if (st->done) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const double alpha = st->pAp > 0.0 ? st->rz / st->pAp : 0.0;
   double part = 0.0;
-  if (i < m) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
     x[i] += (T)alpha * p[i];
     const T ri = r[i] - (T)alpha * q[i];
     r[i] = ri;
-    part = (double)ri * ri;
+    part += (double)ri * ri;
   }
   part = block_sum(part);
   if (threadIdx.x == 0) atomicAdd(&st->rr, part);
@@ -126,9 +154,8 @@ template <class T>
 __global__ void __launch_bounds__(kBlock) k_jacobi(int n, const T* __restrict__ dinv, const T* __restrict__ r,
                                                    T* __restrict__ z, ipcb_pcg_state* st) {
   if (st->done) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double part = 0.0;
-  if (i < n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const T* d = dinv + 9LL * i;
     const T r0 = r[3 * i], r1 = r[3 * i + 1], r2 = r[3 * i + 2];
     const T z0 = d[0] * r0 + d[1] * r1 + d[2] * r2;
@@ -137,7 +164,7 @@ __global__ void __launch_bounds__(kBlock) k_jacobi(int n, const T* __restrict__ 
     z[3 * i] = z0;
     z[3 * i + 1] = z1;
     z[3 * i + 2] = z2;
-    part = (double)r0 * z0 + (double)r1 * z1 + (double)r2 * z2;
+    part += (double)r0 * z0 + (double)r1 * z1 + (double)r2 * z2;
   }
   part = block_sum(part);
   if (threadIdx.x == 0) atomicAdd(&st->rz_new, part);
@@ -150,14 +177,19 @@ __global__ void __launch_bounds__(kBlock) k_fsai_lower(int n, const int* __restr
                                                        const float* __restrict__ scale, const T* __restrict__ r,
                                                        T* __restrict__ t, ipcb_pcg_state* st) {
   if (st->done) return;
-  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (row >= n) return;
-  T o0, o1, o2;
-  warp_row_mv<T, bf16>(cols, g, off[row], diag[row] + 1, r, scale, -1, o0, o1, o2);
-  if ((threadIdx.x & 31) == 0) {
-    t[3 * row] = o0;
-    t[3 * row + 1] = o1;
-    t[3 * row + 2] = o2;
+  const int sub = threadIdx.x & (kLanes - 1);
+  const int groups = (gridDim.x * blockDim.x) / kLanes;
+  const int trips = (n + groups - 1) / groups;
+  int row = (blockIdx.x * blockDim.x + threadIdx.x) / kLanes;
+  for (int it = 0; it < trips; ++it, row += groups) {
+    const bool ok = row < n;
+    T o0, o1, o2;
+    row_mv<T, bf16>(cols, g, ok ? off[row] : 0, ok ? diag[row] + 1 : 0, r, scale, -1, o0, o1, o2);
+    if (ok && sub == 0) {
+      t[3 * row] = o0;
+      t[3 * row + 1] = o1;
+      t[3 * row + 2] = o2;
+    }
   }
 }
 
@@ -170,19 +202,22 @@ __global__ void __launch_bounds__(kBlock) k_fsai_upper(int n, const int* __restr
                                                        const T* __restrict__ r, T* __restrict__ z,
                                                        ipcb_pcg_state* st) {
   if (st->done) return;
-  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+  const int sub = threadIdx.x & (kLanes - 1);
+  const int groups = (gridDim.x * blockDim.x) / kLanes;
+  const int trips = (n + groups - 1) / groups;
   double part = 0.0;
-  if (row < n) {
+  int row = (blockIdx.x * blockDim.x + threadIdx.x) / kLanes;
+  for (int it = 0; it < trips; ++it, row += groups) {
+    const bool ok = row < n;
     T o0, o1, o2;
-    const int d = diag[row];
-    warp_row_mv<T, bf16>(cols, g, d, off[row + 1], t, nullptr, d, o0, o1, o2);
-    if (lane == 0) {
+    const int d = ok ? diag[row] : 0;
+    row_mv<T, bf16>(cols, g, d, ok ? off[row + 1] : 0, t, nullptr, d, o0, o1, o2);
+    if (ok && sub == 0) {
       const T z0 = o0 * (T)scale[3 * row], z1 = o1 * (T)scale[3 * row + 1], z2 = o2 * (T)scale[3 * row + 2];
       z[3 * row] = z0;
       z[3 * row + 1] = z1;
       z[3 * row + 2] = z2;
-      part = (double)r[3 * row] * z0 + (double)r[3 * row + 1] * z1 + (double)r[3 * row + 2] * z2;
+      part += (double)r[3 * row] * z0 + (double)r[3 * row + 1] * z1 + (double)r[3 * row + 2] * z2;
     }
   }
   part = block_sum(part);
@@ -290,15 +325,36 @@ __global__ void k_fsai_mirror(int nnz, const int* __restrict__ rows, const int* 
 
 inline int gridn(long long n, int b = kBlock) { return (int)((n + b - 1) / b); }
 
+// row-group kernels loop over rows: a fixed grid of 8 blocks per SM
+int warp_grid(int n) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  const int need = gridn((long long)kLanes * n);
+  return need < 8 * sms ? need : 8 * sms;
+}
+
+// element-wise kernels with a dot product: at most 4 blocks per SM, so that
+// the per-block atomics on the scalar stay few
+int flat_grid(long long m) {
+  const int need = gridn(m);
+  const int cap = 4 * (warp_grid(1 << 30) / 8);
+  return need < cap ? need : cap;
+}
+
 template <class T>
 int precond(const ipcb_pcg* P, cudaStream_t s) {
   const int n = P->n;
   if (P->precond == 0)
-    k_jacobi<T><<<gridn(n), kBlock, 0, s>>>(n, (const T*)P->dinv, (const T*)P->r, (T*)P->z, P->state);
+    k_jacobi<T><<<flat_grid(n), kBlock, 0, s>>>(n, (const T*)P->dinv, (const T*)P->r, (T*)P->z, P->state);
   else {
-    k_fsai_lower<T><<<gridn(32LL * n), kBlock, 0, s>>>(n, P->offsets, P->diag, P->columns, (const bf16*)P->g,
+    k_fsai_lower<T><<<warp_grid(n), kBlock, 0, s>>>(n, P->offsets, P->diag, P->columns, (const bf16*)P->g,
                                                        P->scale, (const T*)P->r, (T*)P->t, P->state);
-    k_fsai_upper<T><<<gridn(32LL * n), kBlock, 0, s>>>(n, P->offsets, P->diag, P->columns, (const bf16*)P->g,
+    k_fsai_upper<T><<<warp_grid(n), kBlock, 0, s>>>(n, P->offsets, P->diag, P->columns, (const bf16*)P->g,
                                                        P->scale, (const T*)P->t, (const T*)P->r, (T*)P->z, P->state);
   }
   return 0;
@@ -319,9 +375,9 @@ template <class T>
 int iterate(const ipcb_pcg* P, int k, cudaStream_t s) {
   const int n = P->n, m = 3 * n;
   for (int it = 0; it < k; ++it) {
-    k_spmv_dot<T><<<gridn(32LL * n), kBlock, 0, s>>>(n, P->offsets, P->columns, (const T*)P->values, (const T*)P->p,
+    k_spmv_dot<T><<<warp_grid(n), kBlock, 0, s>>>(n, P->offsets, P->columns, (const T*)P->values, (const T*)P->p,
                                                      (T*)P->q, P->state);
-    k_update_xr<T><<<gridn(m), kBlock, 0, s>>>(m, (T*)P->x, (T*)P->r, (const T*)P->p, (const T*)P->q, P->state);
+    k_update_xr<T><<<flat_grid(m), kBlock, 0, s>>>(m, (T*)P->x, (T*)P->r, (const T*)P->p, (const T*)P->q, P->state);
     precond<T>(P, s);
     k_update_p<T><<<gridn(m), kBlock, 0, s>>>(m, (const T*)P->z, (T*)P->p, P->state, 0);
     k_finish<<<1, 1, 0, s>>>(P->state, 0);

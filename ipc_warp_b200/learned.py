@@ -33,7 +33,7 @@ def _param_sizes():
     for l in range(LAYERS):
         out += [(f"W1_{l}", (3 * WIDTH, WIDTH)), (f"b1_{l}", (WIDTH,)), (f"W2_{l}", (2 * WIDTH, WIDTH)),
                 (f"b2_{l}", (WIDTH,))]
-    out += [("W_off", (WIDTH, 9)), ("b_off", (9,)), ("W_dg", (WIDTH, 9)), ("b_dg", (9,))]
+    out += [("W_off", (WIDTH, 9)), ("b_off", (9,))]
     return out
 
 
@@ -56,11 +56,12 @@ def unflatten(vec) -> dict:
 
 
 def init_params(seed: int = 0) -> np.ndarray:
-    """He-initialised trunk, zero output heads (the net starts as Jacobi)."""
+    """He-initialised trunk, zero output heads (the net starts as first-order
+    FSAI, G^_ij = -A^_ij)."""
     rng = np.random.default_rng(seed)
     p = {}
     for k, s in PARAMS:
-        if k.startswith("b") or k in ("W_off", "W_dg"):
+        if k.startswith("b") or k == "W_off":
             p[k] = np.zeros(s)
         else:
             p[k] = rng.normal(scale=math.sqrt(2.0 / s[0]), size=s)
@@ -157,40 +158,55 @@ class _Tape:
                         int(training))
 
 
-def forward(net: Net, sysm: System, training: bool = False, G: torch.Tensor | None = None):
-    """G^ (float32 (nnz, 3, 3), valid on the lower blocks) and the tape."""
+def forward(net: Net, sysm: System, training: bool = False):
+    """Row directions H (float32 (nnz, 3, 3), valid on the lower blocks) and
+    the tape."""
     g = sysm.graph
     dev = sysm.A.device
     tape = _Tape(g, training, dev)
-    G = torch.zeros((g.nnz, 3, 3), dtype=torch.float32, device=dev) if G is None else G
+    H = torch.zeros((g.nnz, 3, 3), dtype=torch.float32, device=dev)
     status = torch.zeros(1, dtype=torch.int32, device=dev)
-    N.call("ipcb_mpnn_forward", ctypes.byref(g.c), N.ptr(net.packed), N.ptr(net.params), N.ptr(sysm.x), N.ptr(sysm.y),
-           ctypes.byref(tape.c), N.ptr(G), N.ptr(status), N.stream_handle())
+    N.call("ipcb_mpnn_forward", ctypes.byref(g.c), N.ptr(net.packed), N.ptr(net.params), N.ptr(sysm.ahat),
+           N.ptr(sysm.x), N.ptr(sysm.y), ctypes.byref(tape.c), N.ptr(H), N.ptr(status), N.stream_handle())
     if int(status.item()):
         raise RuntimeError(f"mpnn forward status {int(status.item())}")
-    return G, tape
+    return H, tape
 
 
-def kaporin(sysm: System, G: torch.Tensor, want_grad: bool = False, weight: float = 1.0):
-    """Loss log(tr(G A^ G^T)/N) - (2/N) sum log|det G_ii| and, optionally,
-    its gradient in the padded bf16 head layout."""
+@dataclass
+class Normalized:
+    G: torch.Tensor     # float32 (nnz, 3, 3): the factor on the lower blocks
+    T: torch.Tensor     # float32 (nnz, 9): T_ij = sum_k H_ik A^_kj
+    minv: torch.Tensor  # float32 (n, 9): M_i^-1
+    loss: float         # (1/N) sum_i log det M_i
+    status: int
+
+
+def normalize(sysm: System, H: torch.Tensor) -> Normalized:
+    """Exact row normalisation G^_i = chol(M_i)^-1 H_i and the FSAI loss."""
     g = sysm.graph
-    dev = G.device
+    dev = H.device
+    G = torch.zeros_like(H)
     T = torch.empty((g.nnz, 9), dtype=torch.float32, device=dev)
-    acc = torch.zeros(2, dtype=torch.float64, device=dev)
-    N.call("ipcb_mpnn_loss", ctypes.byref(g.c), N.ptr(sysm.ahat), N.ptr(G), N.ptr(T), N.ptr(acc), None, 0.0,
-           N.stream_handle())
-    dG = None
-    if want_grad:
-        dG = torch.empty((g.n_lower, 64), dtype=torch.bfloat16, device=dev)
-        N.call("ipcb_mpnn_loss", ctypes.byref(g.c), N.ptr(sysm.ahat), N.ptr(G), N.ptr(T), N.ptr(acc), N.ptr(dG),
-               float(weight), N.stream_handle())
-    tr, logdet = acc.tolist()
-    Nd = 3 * g.n
-    return math.log(tr / Nd) - 2.0 * logdet / Nd, dG
+    minv = torch.empty((g.n, 9), dtype=torch.float32, device=dev)
+    acc = torch.zeros(1, dtype=torch.float64, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    N.call("ipcb_fsai_normalize", ctypes.byref(g.c), N.ptr(sysm.ahat), N.ptr(H), N.ptr(T), N.ptr(minv), N.ptr(G),
+           N.ptr(acc), N.ptr(status), N.stream_handle())
+    return Normalized(G, T, minv, float(acc.item()) / (3 * g.n), int(status.item()))
+
+
+def loss_grad(sysm: System, nz: Normalized, weight: float = 1.0) -> torch.Tensor:
+    """Gradient of weight x loss w.r.t. the head outputs (bf16 (L, 64))."""
+    g = sysm.graph
+    dG = torch.empty((g.n_lower, 64), dtype=torch.bfloat16, device=nz.G.device)
+    N.call("ipcb_mpnn_loss_grad", ctypes.byref(g.c), N.ptr(sysm.ahat), N.ptr(sysm.x), N.ptr(nz.T), N.ptr(nz.minv),
+           N.ptr(dG), float(weight), N.stream_handle())
+    return dG
 
 
 def backward(net: Net, sysm: System, tape: _Tape, dG: torch.Tensor, grad: torch.Tensor):
+    """Parameter gradients of sum(dG * head outputs), added to grad."""
     g = sysm.graph
     dev = dG.device
     ws = torch.empty(N.size("ipcb_mpnn_backward_workspace", g.n, g.nnz, g.n_lower), dtype=torch.uint8, device=dev)
@@ -216,10 +232,11 @@ class Trainer:
         self.grad.zero_()
         total = 0.0
         for sysm in batch:
-            G, tape = forward(self.net, sysm, training=True)
-            loss, dG = kaporin(sysm, G, want_grad=True, weight=1.0 / len(batch))
+            H, tape = forward(self.net, sysm, training=True)
+            nz = normalize(sysm, H)
+            dG = loss_grad(sysm, nz, weight=1.0 / len(batch))
             backward(self.net, sysm, tape, dG, self.grad)
-            total += loss / len(batch)
+            total += nz.loss / len(batch)
         self.t += 1
         N.call("ipcb_adam", self.net.params.numel(), N.ptr(self.net.params), N.ptr(self.grad), N.ptr(self.m),
                N.ptr(self.v), float(self.lr), float(self.betas[0]), float(self.betas[1]), float(self.eps), self.t,
@@ -235,10 +252,11 @@ class LearnedFactor:
 
     def __init__(self, net: Net, A: BsrMatrix):
         self.sysm = System.from_bsr(A)
-        G, _ = forward(net, self.sysm)
-        self.G = G
+        H, _ = forward(net, self.sysm)
+        self.G = normalize(self.sysm, H).G
         self.gh = torch.empty((self.sysm.graph.nnz, 9), dtype=torch.bfloat16, device=A.device)
-        N.call("ipcb_fsai_mirror", ctypes.byref(self.sysm.graph.c), N.ptr(G), N.ptr(self.gh), N.stream_handle())
+        N.call("ipcb_fsai_mirror", ctypes.byref(self.sysm.graph.c), N.ptr(self.G), N.ptr(self.gh),
+               N.stream_handle())
 
     def fill(self, P):
         P.diag = N.ptr(self.sysm.graph.diag)
@@ -255,8 +273,8 @@ class LearnedPreconditioner:
 
     def __call__(self, A: BsrMatrix) -> "_Apply":
         sysm = System.from_bsr(A)
-        G, _ = forward(self.net, sysm)
-        return _Apply(sysm, G, A.dtype)
+        H, _ = forward(self.net, sysm)
+        return _Apply(sysm, normalize(sysm, H).G, A.dtype)
 
 
 class _Apply:

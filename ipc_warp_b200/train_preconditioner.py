@@ -110,7 +110,7 @@ def train(systems, steps: int = 400, batch: int = 4, lr: float = 2e-3, seed: int
         loss = tr.step([prepared[i] for i in idx])
         history.append(loss)
         if log_every and (it % log_every == 0 or it == steps - 1):
-            print(f"step {it:5d}  kaporin loss {loss:+.5f}", flush=True)
+            print(f"step {it:5d}  fsai loss {loss:+.5f}", flush=True)
     return net, history
 
 

@@ -3,24 +3,27 @@ product never imports this module).
 
 The network is a message-passing net over the 3x3-block sparsity graph of a
 Newton matrix A (n block rows, the edges are the stored blocks, self loops
-included, sorted by (row, column)).  It outputs a block lower-triangular
-factor G^ on the lower pattern of A such that M^-1 = S G^T G^ S (S = diag(A)
-^-1/2 per scalar) preconditions A: a factorised sparse approximate inverse
-(FSAI).  Training minimises the Kaporin condition number of G^ A^ G^T
-(A^ = S A S):
+included, sorted by (row, column)).  It outputs, on the lower pattern of A,
+the row directions H of a block lower-triangular factorised sparse
+approximate inverse (FSAI): H_ii = I and H_ij = (rho_i out_ij - I) A^_ij,
+with A^ = S A S (S = diag(A)^-1/2 per scalar), out_ij the head output read as
+a 3x3 matrix and rho_i a coupling gate (``coupling``).  Each block row is then
+normalised exactly: with T_ij = sum_k H_ik A^_kj and M_i = sum_j T_ij H_ij^T
+= H_i A^ H_i^T, G^_i = L_i H_i where L_i = chol(M_i)^-1, so that every
+diagonal block of G^ A^ G^T is the identity, and M^-1 = S G^T G^ S
+preconditions A.  For such a factor the Kaporin condition number reduces to
 
-  loss = log(tr(G^ A^ G^T) / N) - (2 / N) sum_i log|det G^_ii|,  N = 3 n,
+  loss = (1 / N) sum_i log det M_i,  N = 3 n,     dloss/dH_ij = (2 / N) M_i^-1 T_ij,
 
-which equals (log K(G^ A^ G^T) + log det A^) / N; it is 0 for G^ = I (Jacobi)
-and needs only products on the pattern of G^.  The reference has no learned
-component (its solve is cg or cuDSS LDLT, time_integrator_base.py:470-507);
-this module restates the algorithm of ipc_warp_b200/csrc/mpnn.cu in float64
-with the same bfloat16 rounding points, so that the device kernels can be
-checked value by value.
+minimised over H by training (the FSAI functional).  The reference has no
+learned component (its solve is cg or cuDSS LDLT,
+time_integrator_base.py:470-507); this module restates the algorithm of
+ipc_warp_b200/csrc/mpnn.cu in float64 with the same bfloat16 rounding points,
+so that the device kernels can be checked value by value.
 
 Rounding points (as the kernels): inputs x, y, the weights used in the
 products, and the stored activations h, e, m, u and the aggregate a are
-bfloat16; products accumulate in float; biases are float; G^ is float.
+bfloat16; products accumulate in float; biases are float; H and G^ are float.
 """
 from __future__ import annotations
 
@@ -103,8 +106,8 @@ def features(g: Graph, Ah):
 
 
 def init_params(seed=0, zero_head=True):
-    """Weights (in, out) with biases; the output heads start at zero so that
-    the initial factor is G^ = I (Jacobi)."""
+    """Weights (in, out) with biases; the output head starts at zero, so that
+    the initial directions are first-order FSAI (H_ij = -A^_ij)."""
     rng = np.random.default_rng(seed)
 
     def lin(i, o, scale=None):
@@ -117,20 +120,20 @@ def init_params(seed=0, zero_head=True):
     for l in range(LAYERS):
         p[f"W1_{l}"], p[f"b1_{l}"] = lin(3 * WIDTH, WIDTH)
         p[f"W2_{l}"], p[f"b2_{l}"] = lin(2 * WIDTH, WIDTH)
-    for name in ("off", "dg"):
-        W, b = lin(WIDTH, 9, scale=0.0 if zero_head else 0.05)
-        p[f"W_{name}"], p[f"b_{name}"] = W, b
+    p["W_off"], p["b_off"] = lin(WIDTH, 9, scale=0.0 if zero_head else 0.05)
     return p
 
 
 PARAM_ORDER = (["W_hin", "b_hin", "W_ein", "b_ein"]
                + [f"{k}_{l}" for l in range(LAYERS) for k in ("W1", "b1", "W2", "b2")]
-               + ["W_off", "b_off", "W_dg", "b_dg"])
+               + ["W_off", "b_off"])
 
 
-def forward(g: Graph, x, y, p, keep=False):
-    """G^ on the lower edges (L, 3, 3); with keep=True also the stored
-    activations for the backward pass."""
+def forward(g: Graph, x, y, p, keep=False, Ah=None):
+    """Row directions H on the lower edges (L, 3, 3): H_ii = I and
+    H_ij = (rho_i out - I) A^_ij (Ah: float32 values as the kernels read
+    them); with keep=True also the stored activations for the backward
+    pass."""
     W = {k: (bf16(v) if k.startswith("W") else v) for k, v in p.items()}
     deg = np.diff(g.offsets).astype(np.float64)
     h = bf16(relu(x @ W["W_hin"] + W["b_hin"]))
@@ -149,20 +152,39 @@ def forward(g: Graph, x, y, p, keep=False):
         h = bf16(h + u)
     el = e[g.lower]
     is_diag = g.cols[g.lower] == g.rows[g.lower]
-    out = np.where(is_diag[:, None], el @ W["W_dg"] + W["b_dg"], el @ W["W_off"] + W["b_off"])
-    G = out.reshape(-1, 3, 3)
-    G[is_diag] += np.eye(3)
+    Al = _lower_blocks(g, Ah)
+    rho = coupling(x)[g.rows[g.lower]]
+    P_off = (el @ W["W_off"] + W["b_off"]).reshape(-1, 3, 3) * rho[:, None, None] - np.eye(3)
+    H = np.where(is_diag[:, None, None], np.eye(3), P_off @ Al)
     if keep:
-        return G, dict(tape=tape, h=h, e=e, W=W, is_diag=is_diag)
-    return G
+        return H, dict(tape=tape, h=h, e=e, W=W, is_diag=is_diag, Al=Al, rho=rho)
+    return H
 
 
-def _lower_index(g: Graph):
-    """map (row, col) -> lower slot, and per row the lower slots"""
-    slot = {}
-    for s, e in enumerate(g.lower):
-        slot[(int(g.rows[e]), int(g.cols[e]))] = s
-    return slot
+def _lower_blocks(g: Graph, Ah):
+    """A^ of the lower blocks as float32 values (identity blocks where A^ is
+    not given)."""
+    if Ah is None:
+        return np.tile(np.eye(3), (len(g.lower), 1, 1))
+    return np.asarray(Ah, np.float32).reshape(-1, 3, 3)[g.lower].astype(np.float64)
+
+
+def head_output_grad(dH, is_diag, Al, rho):
+    """Gradient w.r.t. the head outputs (L, 9) from the gradient w.r.t. H:
+    rho_i dH A^T off the diagonal (H_ij = (rho_i out - I) A^_ij), 0 on it."""
+    dout = np.asarray(dH, np.float64).reshape(-1, 3, 3).copy()
+    dout[~is_diag] = dout[~is_diag] @ np.transpose(Al[~is_diag], (0, 2, 1))
+    dout *= rho[:, None, None]
+    dout[is_diag] = 0.0
+    return dout.reshape(-1, 9)
+
+
+def coupling(x):
+    """rho_i = c / (1 + c), c = sum_j |A^_ij|_F over the off-diagonal blocks
+    of row i (node feature 10, bf16): a row without coupling keeps its
+    first-order directions whatever the head outputs."""
+    c = np.asarray(x, np.float64)[:, 10]
+    return c / (1.0 + c)
 
 
 def random_spd(nb, seed, band=5, couplings=3):
@@ -195,55 +217,77 @@ def random_spd(nb, seed, band=5, couplings=3):
     return offsets, cols, vals
 
 
-def loss_and_grad_G(g: Graph, Ah, G):
-    """Kaporin loss of G^ A^ G^T and its gradient w.r.t. G^ (L, 3, 3)."""
-    n = g.n
-    N = 3 * n
-    full = {(int(r), int(c)): e for e, (r, c) in enumerate(zip(g.rows, g.cols))}
-    lower_rows = [[] for _ in range(n)]
+def _lower_rows(g: Graph):
+    rows = [[] for _ in range(g.n)]
     for s, e in enumerate(g.lower):
-        lower_rows[int(g.rows[e])].append((int(g.cols[e]), s))
-    T = np.zeros_like(G)
-    for i in range(n):
-        for (j, sj) in lower_rows[i]:
+        rows[int(g.rows[e])].append((int(g.cols[e]), s))
+    return rows
+
+
+def products(g: Graph, Ah, H):
+    """T_ij = sum_{k <= i} H_ik A^_kj on the lower pattern (L, 3, 3)."""
+    full = {(int(r), int(c)): e for e, (r, c) in enumerate(zip(g.rows, g.cols))}
+    T = np.zeros_like(H)
+    for i, row in enumerate(_lower_rows(g)):
+        for (j, sj) in row:
             acc = np.zeros((3, 3))
-            for (k, sk) in lower_rows[i]:
+            for (k, sk) in row:
                 e = full.get((k, j))
                 if e is not None:
-                    acc += G[sk] @ Ah[e]
+                    acc += H[sk] @ Ah[e]
             T[sj] = acc
+    return T
+
+
+def normalize(g: Graph, Ah, H):
+    """G^ = L H row by row with L_i = chol(M_i)^-1, M_i = sum_j T_ij H_ij^T;
+    returns (G, loss, dH): loss = (1/N) sum_i log det M_i and its gradient
+    w.r.t. the off-diagonal H_ij, (2/N) M_i^-1 T_ij."""
+    T = products(g, Ah, H)
+    N = 3 * g.n
+    G = np.zeros_like(H)
+    dH = np.zeros_like(H)
+    loss = 0.0
+    for i, row in enumerate(_lower_rows(g)):
+        M = sum(T[s] @ H[s].T for (_, s) in row)
+        M = 0.5 * (M + M.T)
+        C = np.linalg.cholesky(M)
+        Li = np.linalg.inv(C)
+        Mi = np.linalg.inv(M)
+        loss += np.linalg.slogdet(M)[1]
+        for (j, s) in row:
+            G[s] = Li @ H[s]
+            if j != i:
+                dH[s] = (2.0 / N) * Mi @ T[s]
+    return G, loss / N, dH
+
+
+def kaporin(g: Graph, Ah, G):
+    """log(tr(G A^ G^T) / N) - (2/N) sum_i log|det G_ii| of any factor G."""
+    T = products(g, Ah, G)
+    N = 3 * g.n
     tr = float((T * G).sum())
-    dsl = [None] * n
     logdet = 0.0
-    dG = 2.0 * T / tr
-    for i in range(n):
-        s = None
-        for (j, sj) in lower_rows[i]:
+    for i, row in enumerate(_lower_rows(g)):
+        for (j, s) in row:
             if j == i:
-                s = sj
-        D = G[s]
-        sign, ld = np.linalg.slogdet(D)
-        logdet += ld
-        dG[s] -= (2.0 / N) * np.linalg.inv(D).T
-    loss = np.log(tr / N) - (2.0 / N) * logdet
-    return loss, dG, tr
+                logdet += np.linalg.slogdet(G[s])[1]
+    return np.log(tr / N) - (2.0 / N) * logdet
 
 
-def backward(g: Graph, x, y, p, dG, cache):
-    """Gradients of sum(dG * G^) w.r.t. every parameter (dict), in float64,
+def backward(g: Graph, x, y, p, dH, cache):
+    """Gradients of sum(dH * H) w.r.t. every parameter (dict), in float64,
     with the forward's rounding points held fixed."""
     W = cache["W"]
     deg = np.diff(g.offsets).astype(np.float64)
     is_diag = cache["is_diag"]
     grads = {k: np.zeros_like(v) for k, v in p.items()}
-    dout = dG.reshape(-1, 9)
+    dout = head_output_grad(dH, is_diag, cache["Al"], cache["rho"])
     el = cache["e"][g.lower]
-    grads["W_dg"] = el[is_diag].T @ dout[is_diag]
-    grads["b_dg"] = dout[is_diag].sum(axis=0)
-    grads["W_off"] = el[~is_diag].T @ dout[~is_diag]
-    grads["b_off"] = dout[~is_diag].sum(axis=0)
+    grads["W_off"] = el.T @ dout
+    grads["b_off"] = dout.sum(axis=0)
     de = np.zeros((len(g.cols), WIDTH))
-    de[g.lower] = np.where(is_diag[:, None], dout @ W["W_dg"].T, dout @ W["W_off"].T)
+    de[g.lower] = dout @ W["W_off"].T
     dh = np.zeros((g.n, WIDTH))
     for l in reversed(range(LAYERS)):
         h, e, m, a, u = cache["tape"][l]
