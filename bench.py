@@ -177,6 +177,73 @@ def stage_times(pipe, dx, reps, torch):
     return acc
 
 
+# ------------------------------------------------------------- Newton step
+NEWTON_WORKLOAD = "rod_twist_16rods_4x4x256_wound_theta0.3_stvk_dt5e-3"
+
+
+def newton_solver(dev, torch, linear_solver: str, preconditioner: str, theta: float = 0.3):
+    """FEMContactSolver on the rod-twist bundle in a wound state: the
+    cross-sections turned by up to +-theta, the clamped ends advancing by one
+    step of the 2 rad/s counter-rotation (StVK, E = 1e6, nu = 0.45, dt = 5e-3,
+    rel. residual 1e-6)."""
+    from ipc_warp_b200 import scenes
+    from ipc_warp_b200.newton import FEMContactSolver
+
+    sc = scene()
+    fixed, at = scenes.twist_targets(sc, omega=2.0)
+    s = FEMContactSolver(sc, material="stvk", E=1e6, nu=0.45, h=5e-3, fixed=fixed, gravity=(0.0, 0.0, 0.0),
+                         dtype=torch.float32, device=dev, tol=1e-6, maxiter=20000, linear_solver=linear_solver,
+                         preconditioner=preconditioner)
+    x = torch.tensor(scenes.twist_bundle(sc, theta), dtype=torch.float32, device=dev)
+    s.states.x.copy_(x)
+    s.states.x0.copy_(x)
+    tgt = at(0.0)
+    tgt[fixed] = scenes.twist_bundle(sc, theta + 2.0 * 5e-3)[fixed]
+    s.x_target.copy_(torch.tensor(tgt, dtype=torch.float32))
+    return s
+
+
+def newton_step_times(dev, torch, reps: int = 3, direct_reps: int = 1):
+    """ms of one full Newton iteration (compute_A -> rhs -> solve -> line
+    search, CUDA events around it) for learned-PCG, block-Jacobi PCG and the
+    direct Cholesky solve, from the same state."""
+    out = {"workload": NEWTON_WORKLOAD, "rel_res": 1e-6, "ms": {}, "phase_ms": {}, "pcg_iterations": {},
+           "alpha": {}}
+    for name, ls, pc in (("learned_pcg", "pcg", "learned"), ("jacobi_pcg", "pcg", "jacobi"),
+                         ("direct_cholesky", "direct", "jacobi")):
+        s = newton_solver(dev, torch, ls, pc)
+        s.timing = True
+        x0 = s.states.x.clone()
+        n = direct_reps if ls == "direct" else reps
+        times = []
+        for r in range(n + (0 if ls == "direct" else 1)):  # one untimed warm-up for the PCG paths
+            s.states.x.copy_(x0)
+            s.stats.pcg_iterations.clear()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            alpha, _ = s.newton_iteration()
+            b.record()
+            torch.cuda.synchronize()
+            if ls == "direct" or r > 0:
+                times.append(a.elapsed_time(b))
+        out["ms"][name] = statistics.median(times)
+        out["phase_ms"][name] = {k: round(v, 3) for k, v in s.phase_ms.items()}
+        out["pcg_iterations"][name] = s.stats.pcg_iterations[-1] if s.stats.pcg_iterations else None
+        out["alpha"][name] = alpha
+        out["n_contacts"] = s.n_contacts + s.n_contacts_pt
+        del s
+        torch.cuda.empty_cache()
+    ms = out["ms"]
+    out["speedup_learned_vs_direct"] = ms["direct_cholesky"] / ms["learned_pcg"]
+    out["speedup_learned_vs_jacobi"] = ms["jacobi_pcg"] / ms["learned_pcg"]
+    solve = {k: v["solve"] for k, v in out["phase_ms"].items()}
+    out["solve_speedup_learned_vs_direct"] = solve["direct_cholesky"] / solve["learned_pcg"]
+    out["solve_speedup_learned_vs_jacobi"] = solve["jacobi_pcg"] / solve["learned_pcg"]
+    out["direct_solver"] = "cuSOLVER csrchol with METIS ordering (cuDSS is not in this toolkit)"
+    return out
+
+
 # ------------------------------------------------------------- CPU oracle
 def cpu_pipeline(sc, dx, reps):
     """One pass of the oracle's restatement: DCD EE + PT, narrow phase
@@ -323,6 +390,7 @@ def run_ours(args):
         achieved = algo / (narrow_ms * 1e-3) / 1e9
         traffic = NARROW_DRAM_BYTES_PER_STEP
         cpu_pairs, cpu_sec = cpu_pipeline(sc, dx_np, 3)
+        newton = None if args.no_newton else newton_step_times(dev, torch)
         ms = total_ms / args.steps
         out = {
             "metric": METRIC,
@@ -347,6 +415,7 @@ def run_ours(args):
             "gpu_launches": n_launch * args.steps,
             "kernels": names,
             "clocks": clocks,
+            "newton_step": newton,
         }
     if world > 1:
         dist.barrier()
@@ -363,6 +432,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--profile-only", action="store_true",
                     help="warmup + K steps only (for ncu launch lists); prints nothing")
+    ap.add_argument("--no-newton", action="store_true",
+                    help="skip the Newton-step timing (learned-PCG / Jacobi-PCG / direct)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -358,10 +358,27 @@ class FEMContactSolver(ContactBarrierMixin):
         return alpha
 
     def newton_iteration(self) -> tuple[float, float]:
+        """One iteration of RodBCBase.step; with ``self.timing`` set, the
+        device time of each phase (ms) is left in ``self.phase_ms``."""
+        ev = None
+        if getattr(self, "timing", False):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+            ev[0].record()
         self.compute_A()
+        if ev:
+            ev[1].record()
         self.compute_rhs()
+        if ev:
+            ev[2].record()
         self.solve()
+        if ev:
+            ev[3].record()
         alpha = self.line_search()
+        if ev:
+            ev[4].record()
+            torch.cuda.synchronize()
+            self.phase_ms = {k: ev[i].elapsed_time(ev[i + 1]) for i, k in
+                             enumerate(("compute_A", "rhs", "solve", "line_search"))}
         norm = float(self.states.dx.double().abs().max()) if alpha > 0 else 0.0
         return alpha, norm
 

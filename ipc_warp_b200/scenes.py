@@ -211,3 +211,39 @@ def rod_bundle(n_rods_side: int = 4, cells=(4, 4, 256), width: float = 0.1, spac
     sc.x += rng.uniform(-jitter_over_dhat * dhat, jitter_over_dhat * dhat, size=sc.x.shape)
     sc.xcs = sc.x.copy()
     return sc
+
+
+def twist_bundle(sc: Scene, theta: float) -> np.ndarray:
+    """Positions of a rod bundle (rods along z) whose cross-sections are turned
+    rigidly about the bundle axis by theta * (2 (z - z0) / L - 1): a wound
+    state of the rod twist in which facing rod sides keep their gap."""
+    x = sc.xcs.copy()
+    c = x[:, :2].mean(axis=0)
+    z = x[:, 2]
+    th = theta * (2.0 * (z - z.min()) / (z.max() - z.min()) - 1.0)
+    d = x[:, :2] - c
+    x[:, 0] = c[0] + np.cos(th) * d[:, 0] - np.sin(th) * d[:, 1]
+    x[:, 1] = c[1] + np.sin(th) * d[:, 0] + np.cos(th) * d[:, 1]
+    return x
+
+
+def twist_targets(sc: Scene, omega: float):
+    """Clamped ends of the rod twist: returns (fixed mask, targets(t)); the
+    z-min end turns by +omega t and the z-max end by -omega t about the
+    bundle axis."""
+    x = sc.xcs
+    c = x[:, :2].mean(axis=0)
+    lo = x[:, 2] <= x[:, 2].min() + 1e-9
+    hi = x[:, 2] >= x[:, 2].max() - 1e-9
+
+    def at(t):
+        tgt = x.copy()
+        for mask, sgn in ((lo, 1.0), (hi, -1.0)):
+            a = sgn * omega * t
+            ca, sa = np.cos(a), np.sin(a)
+            d = x[mask, :2] - c
+            tgt[mask, 0] = c[0] + ca * d[:, 0] - sa * d[:, 1]
+            tgt[mask, 1] = c[1] + sa * d[:, 0] + ca * d[:, 1]
+        return tgt
+
+    return lo | hi, at

@@ -13,7 +13,6 @@ and Adam minimises the mean Kaporin loss over random mini-batches.
 from __future__ import annotations
 
 import argparse
-import math
 import time
 
 import numpy as np
@@ -22,7 +21,7 @@ import torch
 from . import learned as L
 from .bsr import BsrMatrix
 from .newton import FEMContactSolver
-from .scenes import rod_bundle, two_cubes
+from .scenes import rod_bundle, twist_targets, two_cubes
 
 
 def _copy(A: BsrMatrix) -> BsrMatrix:
@@ -59,28 +58,6 @@ def cube_systems(steps: int, seed: int, limit: int, dtype=torch.float32, n: int 
     out = []
     capture(s, steps, out, limit)
     return out
-
-
-def twist_targets(sc, omega: float):
-    """Targets of the clamped rod ends: the z-min end turns by +omega t and
-    the z-max end by -omega t about the bundle axis."""
-    x = sc.xcs
-    c = x[:, :2].mean(axis=0)
-    zlo, zhi = x[:, 2].min(), x[:, 2].max()
-    lo = x[:, 2] <= zlo + 1e-9
-    hi = x[:, 2] >= zhi - 1e-9
-
-    def at(t):
-        tgt = x.copy()
-        for mask, sgn in ((lo, 1.0), (hi, -1.0)):
-            a = sgn * omega * t
-            ca, sa = math.cos(a), math.sin(a)
-            d = x[mask, :2] - c
-            tgt[mask, 0] = c[0] + ca * d[:, 0] - sa * d[:, 1]
-            tgt[mask, 1] = c[1] + sa * d[:, 0] + ca * d[:, 1]
-        return tgt
-
-    return lo | hi, at
 
 
 def rod_systems(steps: int, seed: int, limit: int, dtype=torch.float32, side: int = 2, cells=(4, 4, 64),
