@@ -267,15 +267,15 @@ int ipcb_mpnn_features(const ipcb_graph* g, int fp64, const void* values, float*
 
 /* Activations: bf16 buffers; h[5][n*64], e[5][nnz*64] (layer inputs and the
  * final state), m[4][nnz*64], a[4][n*64], u[4][n*64]; for inference only
- * h[0..1] and e[0..1] are used (ping-pong) and m, a, u may be NULL.
- * agg: float[n*64] scratch. */
+ * h[0..1], e[0..1] (ping-pong), m[0] and a[0] are used and u may be NULL.
+ * proj: float[n*128] scratch. */
 typedef struct {
   void* h;
   void* e;
   void* m;
   void* a;
   void* u;
-  float* agg;
+  float* proj;
   int training;
 } ipcb_mpnn_tape;
 

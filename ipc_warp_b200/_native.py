@@ -37,7 +37,7 @@ class Graph(ctypes.Structure):
 
 
 class Tape(ctypes.Structure):
-    _fields_ = [("h", P), ("e", P), ("m", P), ("a", P), ("u", P), ("agg", P), ("training", c_int)]
+    _fields_ = [("h", P), ("e", P), ("m", P), ("a", P), ("u", P), ("proj", P), ("training", c_int)]
 
 
 class PcgState(ctypes.Structure):

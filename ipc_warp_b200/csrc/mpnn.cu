@@ -4,11 +4,13 @@
 //
 // Every dense product runs on the tensor cores through one templated kernel,
 // k_mlp: a persistent CTA stages 128 rows of its A operand into an SW128
-// K-major shared tile (the "stage" functor gathers them: node states of both
-// endpoints and the edge state for a message, node state and mean message
-// for an update, ...), one thread issues the UMMAs into a TMEM accumulator,
-// and the four warps read their 32 lanes back for a fused epilogue (bias,
-// ReLU, residual, segmented message aggregation, head selection).  Weight
+// K-major shared tile (the "stage" functor gathers them: the edge state, node
+// state and mean message for an update, ...), one thread issues the UMMAs
+// into a TMEM accumulator, and the four warps read their 32 lanes back for a
+// fused epilogue (bias, ReLU, residual, segmented message aggregation, head).
+// The message map is split by input block, [h_i | h_j | e] W1 = (h W1a)_i +
+// (h W1b)_j + e W1c: the two node projections are one node-sized product and
+// the edge product stages only the 128-byte edge state.  Weight
 // gradients use k_wgrad, which stages X^T and dY^T tiles (rows of the batch
 // along K) and keeps the [features x outputs] accumulator in TMEM across all
 // the row tiles a CTA visits, plus a bias row from a column of ones.
@@ -34,6 +36,10 @@ constexpr int W = IPCB_MPNN_WIDTH;  // 64
 constexpr int IN = IPCB_MPNN_IN;    // 16
 constexpr int LAYERS = IPCB_MPNN_LAYERS;
 constexpr int kThreads = 128;
+// k_mlp: warps 0-3 produce (stage tiles, issue the UMMAs), warps 4-7 drain the
+// accumulators; hardware barrier ids 1 and 2 synchronise each group
+constexpr int kMlpThreads = 256;
+constexpr int kProdBarrier = 1, kEpiBarrier = 2;
 
 // ------------------------------------------------------------ parameters
 // FP32 master layout (weights in x out row-major, then bias)
@@ -48,8 +54,10 @@ constexpr int P_COUNT = P_BOFF + 9;
 // BF16 operand layout (all offsets in elements, multiples of 8)
 constexpr int K_ENC_H = 0;                        // [64 out][64 in]  (in >= 16 zero)
 constexpr int K_ENC_E = K_ENC_H + W * 64;         // [64][64]
-constexpr int K_W1T = K_ENC_E + W * 64;           // LAYERS x [64 out][192 in]
-constexpr int K_W2T = K_W1T + LAYERS * W * 3 * W; // LAYERS x [64 out][128 in]
+// message map split by input block: [h_i | h_j | e] W1 = h_i W1a + h_j W1b + e W1c
+constexpr int K_W1ABT = K_ENC_E + W * 64;         // LAYERS x [128 out (W1a | W1b)][64 in (h)]
+constexpr int K_W1CT = K_W1ABT + LAYERS * 2 * W * W; // LAYERS x [64 out][64 in (e)]
+constexpr int K_W2T = K_W1CT + LAYERS * W * W;    // LAYERS x [64 out][128 in]
 constexpr int K_HEADT = K_W2T + LAYERS * W * 2 * W; // [16 out][64 in]: rows 0..8 the head
 constexpr int K_W1 = K_HEADT + 16 * W;            // LAYERS x [192 in][64 out]
 constexpr int K_W2 = K_W1 + LAYERS * 3 * W * W;   // LAYERS x [128 in][64 out]
@@ -63,12 +71,16 @@ __global__ void k_pack(const float* __restrict__ p, bf16* __restrict__ q) {
   if (t < K_ENC_E) {  // enc_h^T
     const int o = (t - K_ENC_H) / 64, k = (t - K_ENC_H) % 64;
     v = k < IN ? p[P_WHIN + k * W + o] : 0.f;
-  } else if (t < K_W1T) {
+  } else if (t < K_W1ABT) {
     const int o = (t - K_ENC_E) / 64, k = (t - K_ENC_E) % 64;
     v = k < IN ? p[P_WEIN + k * W + o] : 0.f;
+  } else if (t < K_W1CT) {
+    // row o < 64: h_i part (W1 rows 0..63); row 64 + o: h_j part (W1 rows 64..127)
+    const int r = t - K_W1ABT, l = r / (2 * W * W), o = (r % (2 * W * W)) / W, k = r % W;
+    v = p[P_LAYER0 + l * P_LAYER + O_W1 + ((o / W) * W + k) * W + (o % W)];
   } else if (t < K_W2T) {
-    const int r = t - K_W1T, l = r / (W * 3 * W), o = (r % (W * 3 * W)) / (3 * W), k = r % (3 * W);
-    v = p[P_LAYER0 + l * P_LAYER + O_W1 + k * W + o];
+    const int r = t - K_W1CT, l = r / (W * W), o = (r % (W * W)) / W, k = r % W;
+    v = p[P_LAYER0 + l * P_LAYER + O_W1 + (2 * W + k) * W + o];
   } else if (t < K_HEADT) {
     const int r = t - K_W2T, l = r / (W * 2 * W), o = (r % (W * 2 * W)) / (2 * W), k = r % (2 * W);
     v = p[P_LAYER0 + l * P_LAYER + O_W2 + k * W + o];
@@ -123,32 +135,11 @@ struct StageDense {  // row-major bf16 rows, columns >= kvalid read as zero
   }
 };
 
-struct StageEdge {  // [h_row | h_col | e] of an edge
-  const bf16 *h, *e;
-  const int *rows, *cols;
-  __device__ uint4 group(int row, int c, int g) const {
-    if (c == 0) return ld4(h + (size_t)__ldg(rows + row) * W + g * 8);
-    if (c == 1) return ld4(h + (size_t)__ldg(cols + row) * W + g * 8);
-    return ld4(e + (size_t)row * W + g * 8);
-  }
-};
-
-struct StageNode {  // [h | bf16(agg / deg)], writing a to the tape
+struct StageNode {  // [h | a] of a node (a: mean message, from k_mean_messages)
   const bf16* h;
-  const float* agg;
-  const int* offsets;
-  bf16* a_out;
+  const bf16* a;
   __device__ uint4 group(int row, int c, int g) const {
-    if (c == 0) return ld4(h + (size_t)row * W + g * 8);
-    const float deg = (float)(__ldg(offsets + row + 1) - __ldg(offsets + row));
-    float f[8];
-    const float4* a4 = reinterpret_cast<const float4*>(agg + (size_t)row * W + g * 8);
-    const float4 p = a4[0], q = a4[1];
-    f[0] = p.x / deg; f[1] = p.y / deg; f[2] = p.z / deg; f[3] = p.w / deg;
-    f[4] = q.x / deg; f[5] = q.y / deg; f[6] = q.z / deg; f[7] = q.w / deg;
-    const uint4 u = pack8(f);
-    if (a_out) *reinterpret_cast<uint4*>(a_out + (size_t)row * W + g * 8) = u;
-    return u;
+    return ld4((c == 0 ? h : a) + (size_t)row * W + g * 8);
   }
 };
 
@@ -159,110 +150,105 @@ struct StageGather {  // X[idx[row]] (64 wide)
 };
 
 // ------------------------------------------------------------ epilogues
-// apply() is called by all 128 threads (valid marks rows inside the batch);
-// `scr` is shared scratch of 128 x 33 floats plus 128 ints.
-struct EpiBiasRelu {
+// The accumulator tile is moved from TMEM into shared memory (acc: row r at
+// r * stride floats), and each epilogue warp then finishes its 32 rows with
+// rows32(): lane l works on column group l % 8 (8 columns) of row l / 8 of
+// each step of 4 rows, so a row's gathers and stores are contiguous 128- or
+// 256-byte accesses, and the 8 steps are unrolled so that their loads are in
+// flight together.  Per-row indices are loaded once per warp (lane l: row l)
+// and broadcast with shuffles.  tile is the staged A tile (SW128 layout),
+// still intact during the epilogue; nvalid rows of the 32 are inside the
+// batch.
+__device__ __forceinline__ void ld8f(const float* p, float (&f)[8]) {
+  const float4 a = reinterpret_cast<const float4*>(p)[0], b = reinterpret_cast<const float4*>(p)[1];
+  f[0] = a.x; f[1] = a.y; f[2] = a.z; f[3] = a.w; f[4] = b.x; f[5] = b.y; f[6] = b.z; f[7] = b.w;
+}
+__device__ __forceinline__ void ld8s(const float* p, float (&f)[8]) {  // shared, any alignment
+#pragma unroll
+  for (int t = 0; t < 8; ++t) f[t] = p[t];
+}
+
+struct EpiBiasRelu {  // out = bf16(relu(v + b)), 64 columns
   const float* b;
   bf16* out;
-  __device__ void apply(int row, bool valid, int col0, const float (&v)[32], float*, int*) const {
-    if (!valid) return;
-    float o[32];
+  __device__ void rows32(int grow0, int nvalid, const float* acc, int stride, const uint8_t*, int, int lane) const {
+    const int q = lane >> 3, cg = lane & 7;
+    float bb[8];
+    ld8f(b + 8 * cg, bb);
 #pragma unroll
-    for (int i = 0; i < 32; ++i) o[i] = fmaxf(v[i] + __ldg(b + col0 + i), 0.f);
-    uint4* dst = reinterpret_cast<uint4*>(out + (size_t)row * W + col0);
+    for (int it = 0; it < 8; ++it) {
+      const int r = 4 * it + q;
+      if (r >= nvalid) continue;
+      float v[8];
+      ld8s(acc + r * stride + 8 * cg, v);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) dst[q] = pack8(o + 8 * q);
+      for (int t = 0; t < 8; ++t) v[t] = fmaxf(v[t] + bb[t], 0.f);
+      *reinterpret_cast<uint4*>(out + (size_t)(grow0 + r) * W + 8 * cg) = pack8(v);
+    }
   }
 };
 
-struct EpiEdge {  // m = relu(v + b1); e_out = e_in + m; agg[row] += m
+struct EpiEdge {  // m = relu(v + b1 + P_a[i] + P_b[j]); e_out = e_in + m (e_in: the staged tile)
   const float* b;
-  const bf16* e_in;
+  const float* proj;  // [n][128]: columns 0..63 h W1a, 64..127 h W1b
   bf16* e_out;
   bf16* m_out;
-  float* agg;
   const int* rows;
-  __device__ void apply(int row, bool valid, int col0, const float (&v)[32], float* scr, int* srow) const {
-    const int tid = threadIdx.x;
-    float m[32];
+  const int* cols;
+  __device__ void rows32(int grow0, int nvalid, const float* acc, int stride, const uint8_t* tile, int r0,
+                         int lane) const {
+    const int q = lane >> 3, cg = lane & 7;
+    const int my_i = lane < nvalid ? __ldg(rows + grow0 + lane) : 0;
+    const int my_j = lane < nvalid ? __ldg(cols + grow0 + lane) : 0;
+    float bb[8];
+    ld8f(b + 8 * cg, bb);
 #pragma unroll
-    for (int i = 0; i < 32; ++i) m[i] = valid ? bfr(fmaxf(v[i] + __ldg(b + col0 + i), 0.f)) : 0.f;
-    if (valid) {
-      const bf16* ei = e_in + (size_t)row * W + col0;
-      float eo[32];
+    for (int it = 0; it < 8; ++it) {
+      const int r = 4 * it + q;
+      const int i = __shfl_sync(0xffffffffu, my_i, r), j = __shfl_sync(0xffffffffu, my_j, r);
+      if (r >= nvalid) continue;
+      float pa[8], pb[8], v[8], e[8], m[8];
+      ld8f(proj + (size_t)i * 2 * W + 8 * cg, pa);
+      ld8f(proj + (size_t)j * 2 * W + W + 8 * cg, pb);
+      ld8s(acc + r * stride + 8 * cg, v);
+      unpack8(*reinterpret_cast<const uint4*>(tile + umma::sw128_group(r0 + r, 0, cg, 128)), e);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        float f[8];
-        unpack8(ld4(ei + 8 * q), f);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) eo[8 * q + i] = f[i] + m[8 * q + i];
+      for (int t = 0; t < 8; ++t) {
+        m[t] = bfr(fmaxf(v[t] + bb[t] + pa[t] + pb[t], 0.f));
+        e[t] += m[t];
       }
-      uint4* de = reinterpret_cast<uint4*>(e_out + (size_t)row * W + col0);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) de[q] = pack8(eo + 8 * q);
-      if (m_out) {
-        uint4* dm = reinterpret_cast<uint4*>(m_out + (size_t)row * W + col0);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) dm[q] = pack8(m + 8 * q);
-      }
+      *reinterpret_cast<uint4*>(e_out + (size_t)(grow0 + r) * W + 8 * cg) = pack8(e);
+      *reinterpret_cast<uint4*>(m_out + (size_t)(grow0 + r) * W + 8 * cg) = pack8(m);
     }
-    // segmented sum over the tile's rows (edges of a row are contiguous)
-#pragma unroll
-    for (int i = 0; i < 32; ++i) scr[tid * 33 + i] = m[i];
-    srow[tid] = valid ? __ldg(rows + row) : -1;
-    __syncthreads();
-    const int col = tid & 31, q = tid >> 5;
-    int cur = -1;
-    float acc = 0.f;
-    for (int r = q * 32; r < q * 32 + 32; ++r) {
-      const int id = srow[r];
-      if (id != cur) {
-        if (cur >= 0) atomicAdd(agg + (size_t)cur * W + col0 + col, acc);
-        cur = id;
-        acc = 0.f;
-      }
-      acc += scr[r * 33 + col];
-    }
-    if (cur >= 0) atomicAdd(agg + (size_t)cur * W + col0 + col, acc);
-    __syncthreads();
   }
 };
 
-struct EpiNode {  // u = relu(v + b2); h_out = h_in + u
+struct EpiNode {  // u = relu(v + b2); h_out = h_in + u (h_in: chunk 0 of the staged tile)
   const float* b;
-  const bf16* h_in;
   bf16* h_out;
   bf16* u_out;
-  __device__ void apply(int row, bool valid, int col0, const float (&v)[32], float*, int*) const {
-    if (!valid) return;
-    float u[32], ho[32];
+  __device__ void rows32(int grow0, int nvalid, const float* acc, int stride, const uint8_t* tile, int r0,
+                         int lane) const {
+    const int q = lane >> 3, cg = lane & 7;
+    float bb[8];
+    ld8f(b + 8 * cg, bb);
 #pragma unroll
-    for (int i = 0; i < 32; ++i) u[i] = bfr(fmaxf(v[i] + __ldg(b + col0 + i), 0.f));
-    const bf16* hi = h_in + (size_t)row * W + col0;
+    for (int it = 0; it < 8; ++it) {
+      const int r = 4 * it + q;
+      if (r >= nvalid) continue;
+      float v[8], h[8], u[8];
+      ld8s(acc + r * stride + 8 * cg, v);
+      unpack8(*reinterpret_cast<const uint4*>(tile + umma::sw128_group(r0 + r, 0, cg, 128)), h);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      float f[8];
-      unpack8(ld4(hi + 8 * q), f);
-#pragma unroll
-      for (int i = 0; i < 8; ++i) ho[8 * q + i] = f[i] + u[8 * q + i];
-    }
-    uint4* dh = reinterpret_cast<uint4*>(h_out + (size_t)row * W + col0);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) dh[q] = pack8(ho + 8 * q);
-    if (u_out) {
-      uint4* du = reinterpret_cast<uint4*>(u_out + (size_t)row * W + col0);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) du[q] = pack8(u + 8 * q);
+      for (int t = 0; t < 8; ++t) {
+        u[t] = bfr(fmaxf(v[t] + bb[t], 0.f));
+        h[t] += u[t];
+      }
+      *reinterpret_cast<uint4*>(h_out + (size_t)(grow0 + r) * W + 8 * cg) = pack8(h);
+      if (u_out) *reinterpret_cast<uint4*>(u_out + (size_t)(grow0 + r) * W + 8 * cg) = pack8(u);
     }
   }
 };
-
-__device__ __forceinline__ float block_fro(const float* __restrict__ a) {
-  float s = 0.f;
-#pragma unroll
-  for (int k = 0; k < 9; ++k) s += a[k] * a[k];
-  return sqrtf(s);
-}
 
 // rho_i = c / (1 + c), c = sum of |A^_ij|_F over the off-diagonal blocks of
 // row i (node feature 10)
@@ -274,15 +260,15 @@ __device__ __forceinline__ float coupling(const bf16* __restrict__ x, int i) {
 // Row directions on a lower block (out: the head output read as a 3x3
 // matrix): H_ii = I and H_ij = (rho_i out - I) A^_ij.  A zero head gives
 // first-order FSAI; a weakly coupled row stays at first order, where it is
-// accurate, whatever the head outputs.
+// accurate, whatever the head outputs.  One lane per row.
 struct EpiHead {
   const float *b_off, *ahat;
   const bf16* x;
   const int *lower, *rows, *cols;
   float* H;
-  __device__ void apply(int row, bool valid, int col0, const float (&v)[32], float*, int*) const {
-    if (!valid || col0 != 0) return;
-    const int e = __ldg(lower + row);
+  __device__ void rows32(int grow0, int nvalid, const float* acc, int stride, const uint8_t*, int, int lane) const {
+    if (lane >= nvalid) return;
+    const int e = __ldg(lower + grow0 + lane);
     const int i = __ldg(rows + e);
     float* h = H + (size_t)e * 9;
     if (i == __ldg(cols + e)) {
@@ -291,100 +277,162 @@ struct EpiHead {
       return;
     }
     const float* a = ahat + (size_t)e * 9;
+    const float* v = acc + lane * stride;
     const float rho = coupling(x, i);
-    float p[9];
+    float p[9], am[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) p[k] = rho * (v[k] + __ldg(b_off + k)) - ((k % 4) == 0 ? 1.f : 0.f);
+    for (int k = 0; k < 9; ++k) {
+      p[k] = rho * (v[k] + __ldg(b_off + k)) - ((k % 4) == 0 ? 1.f : 0.f);
+      am[k] = __ldg(a + k);
+    }
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
-        h[3 * r + c] = p[3 * r] * __ldg(a + c) + p[3 * r + 1] * __ldg(a + 3 + c) + p[3 * r + 2] * __ldg(a + 6 + c);
+      for (int c = 0; c < 3; ++c) h[3 * r + c] = p[3 * r] * am[c] + p[3 * r + 1] * am[3 + c] + p[3 * r + 2] * am[6 + c];
   }
 };
 
-struct EpiF32 {  // plain fp32 rows of width ld
+struct EpiF32 {  // plain fp32 rows of width ld (lanes across the columns)
   float* out;
   int ld;
-  __device__ void apply(int row, bool valid, int col0, const float (&v)[32], float*, int*) const {
-    if (!valid) return;
-    const int n = ld - col0 < 32 ? ld - col0 : 32;
-    float* o = out + (size_t)row * ld + col0;
-    if (n == 32) {
-#pragma unroll
-      for (int q = 0; q < 8; ++q) reinterpret_cast<float4*>(o)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-    } else {
-      for (int i = 0; i < n; ++i) o[i] = v[i];
+  __device__ void rows32(int grow0, int nvalid, const float* acc, int stride, const uint8_t*, int, int lane) const {
+    for (int r = 0; r < nvalid; ++r) {
+      float* o = out + (size_t)(grow0 + r) * ld;
+      for (int c = lane; c < ld; c += 32) o[c] = acc[r * stride + c];
     }
   }
 };
 
 // ------------------------------------------------------------ k_mlp
+// Warp-specialised persistent product: D = A B^T + epilogue over 128-row
+// tiles of A.  Producer warps (0-3) gather tile k into shared stage k % 2
+// (thread t stages row t), then thread 0 issues the UMMAs into TMEM
+// accumulator k % 2 and commits to mma_done[k % 2]; epilogue warps (4-7) wait
+// for it, read their 32 lanes each (and may read the staged tile) and arrive
+// on acc_free[k % 2].  Stage and accumulator k % 2 are reused for tile k + 2
+// only after that release, so tile k + 1 is gathered and multiplied while
+// tile k is drained.  Every wait is bounded; a wait that
+// gives up raises IPCB_STATUS_TIMEOUT and ends the CTA's loop.
 template <int N, int C>
 constexpr size_t mlp_smem() {
-  return 1024 + (size_t)C * 128 * 128 + (size_t)C * N * 128 + 128 * 33 * 4 + 128 * 4;
+  return 1024 + 2 * (size_t)C * 128 * 128 + (size_t)C * N * 128 + 128 * (size_t)(N + 1) * 4;
 }
 
 template <int N, int C, class Stage, class Epi>
-__global__ void __launch_bounds__(kThreads) k_mlp(int rows, Stage st, Epi ep, const bf16* __restrict__ Bw,
-                                                  int* __restrict__ status) {
+__global__ void __launch_bounds__(kMlpThreads) k_mlp(int rows, Stage st, Epi ep, const bf16* __restrict__ Bw,
+                                                     int* __restrict__ status) {
   extern __shared__ uint8_t dsmem[];
-  __shared__ uint64_t mbar;
+  __shared__ uint64_t mma_done[2], acc_free[2];
   __shared__ uint32_t tslot;
-  constexpr uint32_t kCols = umma::tmem_cols(N);
+  // abort flags, each written only by its own group before that group's barrier
+  __shared__ int prod_abort, epi_abort;
+  // accumulator stride: at least the 32 columns one tcgen05.ld reads
+  constexpr int NA = N < 32 ? 32 : N;
+  constexpr uint32_t kCols = umma::tmem_cols(2 * NA);
+  static_assert(2 * NA <= 512, "two accumulators must fit the 512 TMEM columns");
   constexpr int K = 64 * C;
+  constexpr int kStage = C * 128 * 128;
   uint8_t* sA = align1024(dsmem);
-  uint8_t* sB = sA + C * 128 * 128;
-  float* scr = reinterpret_cast<float*>(sB + C * N * 128);
-  int* srow = reinterpret_cast<int*>(scr + 128 * 33);
-  const int tid = threadIdx.x, warp = tid >> 5;
+  uint8_t* sB = sA + 2 * kStage;
+  float* accs = reinterpret_cast<float*>(sB + C * N * 128);  // [128][N + 1]
+  constexpr int kStride = N + 1;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-  for (int idx = tid; idx < N * C * 8; idx += kThreads) {
+  for (int idx = tid; idx < N * C * 8; idx += kMlpThreads) {
     const int r = idx / (C * 8), c = (idx / 8) % C, g = idx % 8;
     *reinterpret_cast<uint4*>(sB + umma::sw128_group(r, c, g, N)) = ld4(Bw + (size_t)r * K + c * 64 + g * 8);
   }
   if (warp == 0) umma::tmem_alloc(&tslot, kCols);
-  if (tid == 0) umma::mbar_init(&mbar, 1);
+  if (tid == 0) {
+    umma::mbar_init(&mma_done[0], 1);
+    umma::mbar_init(&mma_done[1], 1);
+    umma::mbar_init(&acc_free[0], 128);
+    umma::mbar_init(&acc_free[1], 128);
+    prod_abort = 0;
+    epi_abort = 0;
+  }
   umma::fence_async_smem();
   umma::fence_before();
   __syncthreads();
   umma::fence_after();
   const uint32_t tmem = tslot;
-  uint32_t phase = 0;
-  int ok = 1;
   const int ntiles = (rows + 127) / 128;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int row = tile * 128 + tid;
-    const bool valid = row < rows;
+  const int mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  int issued = 0;  // tiles whose UMMAs thread 0 committed
+
+  if (warp < 4) {
+    for (int k = 0; k < mine; ++k) {
+      const int s = k & 1, use = k >> 1;
+      // stage s is free once the epilogue of tile k - 2 (which reads it) is done
+      if (k >= 2 && !umma::mbar_wait(&acc_free[s], (use - 1) & 1)) prod_abort = 1;
+      umma::named_sync(kProdBarrier, 128);
+      if (prod_abort) break;  // uniform: read after the group barrier
+      // warp w stages rows 32w..32w+31; lanes take consecutive 16-byte groups
+      // of a row, so a warp reads contiguous row spans
+      const int base = (blockIdx.x + k * gridDim.x) * 128 + 32 * warp;
+      uint8_t* a = sA + s * kStage;
+      // all of the warp's loads first, then the shared stores
+      uint4 buf[C][8];
 #pragma unroll
-    for (int c = 0; c < C; ++c)
+      for (int c = 0; c < C; ++c)
 #pragma unroll
-      for (int g = 0; g < 8; ++g)
-        *reinterpret_cast<uint4*>(sA + umma::sw128_group(tid, c, g, 128)) = valid ? st.group(row, c, g) : zero4();
-    umma::fence_async_smem();
-    __syncthreads();
-    if (tid == 0) {
+        for (int it = 0; it < 8; ++it) {
+          const int item = it * 32 + lane, row = base + item / 8;
+          buf[c][it] = row < rows ? st.group(row, c, item % 8) : zero4();
+        }
+#pragma unroll
+      for (int c = 0; c < C; ++c)
+#pragma unroll
+        for (int it = 0; it < 8; ++it) {
+          const int item = it * 32 + lane;
+          *reinterpret_cast<uint4*>(a + umma::sw128_group(32 * warp + item / 8, c, item % 8, 128)) = buf[c][it];
+        }
+      umma::fence_async_smem();
+      umma::named_sync(kProdBarrier, 128);
+      if (tid == 0) {
+        umma::fence_after();
+        umma::issue_tile<N, C>(tmem + s * NA, umma::smem_u32(a), umma::smem_u32(sB), false, &mma_done[s]);
+        issued = k + 1;
+      }
+    }
+  } else {
+    const int et = tid - 128;
+    for (int k = 0; k < mine; ++k) {
+      const int s = k & 1, use = k >> 1;
+      if (!umma::mbar_wait(&mma_done[s], use & 1)) epi_abort = 1;
+      umma::named_sync(kEpiBarrier, 128);
+      if (epi_abort) break;  // uniform: read after the group barrier
       umma::fence_after();
-      umma::issue_tile<N, C>(tmem, umma::smem_u32(sA), umma::smem_u32(sB), false, &mbar);
-    }
-    ok = __syncthreads_and(umma::mbar_wait(&mbar, phase) ? 1 : 0);
-    phase ^= 1;
-    if (!ok) break;
-    umma::fence_after();
+      // TMEM -> shared: thread et owns accumulator row et
 #pragma unroll
-    for (int col = 0; col < N; col += 32) {
-      float v[32];
-      umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + col, v);
-      ep.apply(row, valid, col, v, scr, srow);
+      for (int col = 0; col < N; col += 32) {
+        float v[32];
+        umma::tmem_ld32(tmem + s * NA + ((uint32_t)(32 * (warp - 4)) << 16) + col, v);
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+          if (col + i < N) accs[et * kStride + col + i] = v[i];
+      }
+      umma::fence_before();
+      umma::named_sync(kEpiBarrier, 128);
+      // each epilogue warp finishes 32 rows
+      const int r0 = 32 * (warp - 4);
+      const int grow0 = (blockIdx.x + k * gridDim.x) * 128 + r0;
+      const int nvalid = rows - grow0 < 32 ? rows - grow0 : 32;
+      if (nvalid > 0) ep.rows32(grow0, nvalid, accs + r0 * kStride, kStride, sA + s * kStage, r0, lane);
+      umma::named_sync(kEpiBarrier, 128);
+      umma::mbar_arrive(&acc_free[s]);
     }
-    umma::fence_before();
-    __syncthreads();
-  }
-  if (!ok) {
-    if (tid == 0) atomicOr(status, IPCB_STATUS_TIMEOUT);
-    umma::mbar_wait(&mbar, phase);
   }
   __syncthreads();
+  if (prod_abort || epi_abort) {
+    if (tid == 0) {
+      atomicOr(status, IPCB_STATUS_TIMEOUT);
+      // let UMMAs still in flight finish (bounded) before the TMEM is freed
+      for (int k = issued > 2 ? issued - 2 : 0; k < issued; ++k) umma::mbar_wait(&mma_done[k & 1], (k >> 1) & 1);
+    }
+    __syncthreads();
+  }
+  umma::fence_after();
   if (warp == 0) umma::tmem_dealloc(tmem, kCols);
 }
 
@@ -409,12 +457,12 @@ int launch_mlp(int rows, const Stage& st, const Epi& ep, const bf16* Bw, int* st
     ipcb::set_error_msg(what);
     return IPCB_E_CUDA;
   }
-  const int by_tmem = (int)(512 / umma::tmem_cols(N));
+  const int by_tmem = (int)(512 / umma::tmem_cols(2 * (N < 32 ? 32 : N)));
   const int by_smem = (int)((227 * 1024) / (smem + 1024));
   const int per_sm = by_tmem < by_smem ? by_tmem : by_smem;
   const int tiles = (rows + 127) / 128;
   const int cap = sm_count() * (per_sm > 0 ? per_sm : 1);
-  kern<<<tiles < cap ? tiles : cap, kThreads, smem, s>>>(rows, st, ep, Bw, status);
+  kern<<<tiles < cap ? tiles : cap, kMlpThreads, smem, s>>>(rows, st, ep, Bw, status);
   return ipcb::check_launch(what);
 }
 
@@ -800,6 +848,36 @@ __global__ void k_fsai_dout(int n_lower, int n, const int* __restrict__ lower, c
   for (int q = 0; q < 8; ++q) dst[q] = pack8(row + 8 * q);
 }
 
+// a_i = bf16(sum of the row's messages / deg): a warp per node, lanes = 4 edge
+// slots x 8 column groups, so each step reads four contiguous 128-byte rows
+__global__ void __launch_bounds__(256) k_mean_messages(int n, const int* __restrict__ off, const bf16* __restrict__ m,
+                                                       bf16* __restrict__ a) {
+  const int lane = threadIdx.x & 31, slot = lane >> 3, g = lane & 7;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+    const int b = __ldg(off + i), e = __ldg(off + i + 1);
+    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 4
+    for (int k = b + slot; k < e; k += 4) {
+      float f[8];
+      unpack8(ld4(m + (size_t)k * W + g * 8), f);
+#pragma unroll
+      for (int t = 0; t < 8; ++t) acc[t] += f[t];
+    }
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 8);
+      acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 16);
+    }
+    if (slot == 0) {
+      const float deg = (float)(e - b);
+#pragma unroll
+      for (int t = 0; t < 8; ++t) acc[t] /= deg;
+      *reinterpret_cast<uint4*>(a + (size_t)i * W + g * 8) = pack8(acc);
+    }
+  }
+}
+
 // ------------------------------------------------------------ backward helpers
 __global__ void k_gather_rows(int R, const bf16* __restrict__ X, const int* __restrict__ idx, bf16* __restrict__ out) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;  // one 16-byte group
@@ -1011,8 +1089,8 @@ int ipcb_mpnn_features(const ipcb_graph* g, int fp64, const void* values, float*
 
 int ipcb_mpnn_forward(const ipcb_graph* g, const void* packed, const float* params, const float* ahat, const void* x,
                       const void* y, ipcb_mpnn_tape* tape, float* H, int* status, ipcb_stream s) {
-  if (!graph_ok(g) || !packed || !params || !ahat || !x || !y || !tape || !tape->h || !tape->e || !tape->agg || !H ||
-      !status || (tape->training && (!tape->m || !tape->a || !tape->u))) {
+  if (!graph_ok(g) || !packed || !params || !ahat || !x || !y || !tape || !tape->h || !tape->e || !tape->m ||
+      !tape->a || !tape->proj || !H || !status || (tape->training && !tape->u)) {
     ipcb::set_error_msg("mpnn_forward: bad arguments");
     return IPCB_E_ARG;
   }
@@ -1033,15 +1111,24 @@ int ipcb_mpnn_forward(const ipcb_graph* g, const void* packed, const float* para
   if (rc) return rc;
   for (int l = 0; l < LAYERS; ++l) {
     const float* pl = params + P_LAYER0 + l * P_LAYER;
-    bf16* m = tr ? (bf16*)tape->m + (size_t)l * nnz * W : nullptr;
+    bf16* m = (bf16*)tape->m + (tr ? (size_t)l * nnz * W : 0);  // inference: one buffer
     bf16* a = tr ? (bf16*)tape->a + (size_t)l * n * W : nullptr;
     bf16* u = tr ? (bf16*)tape->u + (size_t)l * n * W : nullptr;
-    if (cudaMemsetAsync(tape->agg, 0, sizeof(float) * n * W, st) != cudaSuccess) return ipcb::check_launch("agg");
-    rc = launch_mlp<64, 3>(nnz, StageEdge{hbuf(l), ebuf(l), g->rows, g->columns},
-                           EpiEdge{pl + O_B1, ebuf(l), ebuf(l + 1), m, tape->agg, g->rows}, P + K_W1T + l * W * 3 * W,
-                           status, st, "mpnn message");
+    // per-node projections of both message endpoints, then the edge product
+    rc = launch_mlp<128, 1>(n, StageDense{hbuf(l), W, W}, EpiF32{tape->proj, 2 * W}, P + K_W1ABT + l * 2 * W * W,
+                            status, st, "mpnn message projection");
     if (rc) return rc;
-    rc = launch_mlp<64, 2>(n, StageNode{hbuf(l), tape->agg, g->offsets, a}, EpiNode{pl + O_B2, hbuf(l), hbuf(l + 1), u},
+    rc = launch_mlp<64, 1>(nnz, StageDense{ebuf(l), W, W},
+                           EpiEdge{pl + O_B1, tape->proj, ebuf(l + 1), m, g->rows, g->columns},
+                           P + K_W1CT + l * W * W, status, st, "mpnn message");
+    if (rc) return rc;
+    bf16* am = tr ? a : (bf16*)tape->a;
+    {
+      const int need = (int)(((long long)n * 32 + 255) / 256);
+      const int cap = 16 * sm_count();
+      k_mean_messages<<<need < cap ? need : cap, 256, 0, st>>>(n, g->offsets, m, am);
+    }
+    rc = launch_mlp<64, 2>(n, StageNode{hbuf(l), am}, EpiNode{pl + O_B2, hbuf(l + 1), u},
                            P + K_W2T + l * W * 2 * W, status, st, "mpnn update");
     if (rc) return rc;
   }

@@ -94,6 +94,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint3
   return false;
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mbar)) : "memory");
+}
+
+// barrier among `count` threads (a multiple of 32) under hardware barrier id
+__device__ __forceinline__ void named_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
 // TMEM allocation by one full warp; the base address is written to *slot.
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(ncols)
@@ -145,6 +154,10 @@ __device__ __forceinline__ void issue_tile(uint32_t tmem_d, uint32_t a_base, uin
   commit(mbar);
 }
 
-__host__ __device__ constexpr uint32_t tmem_cols(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : 256; }
+// TMEM columns to allocate for n accumulator columns (a power of two >= 32,
+// at most the 512 columns of an SM)
+__host__ __device__ constexpr uint32_t tmem_cols(int n) {
+  return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : n <= 256 ? 256 : 512;
+}
 
 }  // namespace umma

@@ -149,12 +149,12 @@ class _Tape:
         nh = LAYERS + 1 if training else 2
         self.h = torch.empty((nh, g.n, WIDTH), **b)
         self.e = torch.empty((nh, g.nnz, WIDTH), **b)
-        self.m = torch.empty((LAYERS, g.nnz, WIDTH), **b) if training else None
-        self.a = torch.empty((LAYERS, g.n, WIDTH), **b) if training else None
+        self.m = torch.empty((LAYERS if training else 1, g.nnz, WIDTH), **b)
+        self.a = torch.empty((LAYERS if training else 1, g.n, WIDTH), **b)
         self.u = torch.empty((LAYERS, g.n, WIDTH), **b) if training else None
-        self.agg = torch.empty((g.n, WIDTH), dtype=torch.float32, device=dev)
+        self.proj = torch.empty((g.n, 2 * WIDTH), dtype=torch.float32, device=dev)
         opt = lambda t: N.ptr(t) if t is not None else None
-        self.c = N.Tape(N.ptr(self.h), N.ptr(self.e), opt(self.m), opt(self.a), opt(self.u), N.ptr(self.agg),
+        self.c = N.Tape(N.ptr(self.h), N.ptr(self.e), N.ptr(self.m), N.ptr(self.a), opt(self.u), N.ptr(self.proj),
                         int(training))
 
 
