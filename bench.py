@@ -234,6 +234,32 @@ def newton_step_times(dev, torch, reps: int = 3, direct_reps: int = 1):
         out["n_contacts"] = s.n_contacts + s.n_contacts_pt
         del s
         torch.cuda.empty_cache()
+    # one whole time step (Newton to convergence, max|dx| <= 5e-2 h as the
+    # reference's default) from the same state; the learned factor is built
+    # once per step and reused by the later iterations of the step
+    out["time_step"] = {}
+    for name, pc, refresh in (("learned_pcg_factor_per_step", "learned", 10 ** 6), ("jacobi_pcg", "jacobi", 1)):
+        s = newton_solver(dev, torch, "pcg", pc)
+        s.precond_refresh = refresh
+        s.max_newton = 60
+        x0 = s.states.x.clone()
+        times = []
+        for r in range(2):
+            s.states.x.copy_(x0)
+            s.states.x0.copy_(x0)
+            s.states.xdot.zero_()
+            s.time = 0.0
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            st = s.step()
+            b.record()
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b))
+        out["time_step"][name] = {"ms": times[-1], "newton_iterations": st.newton_iterations,
+                                  "pcg_iterations": sum(st.pcg_iterations)}
+        del s
+        torch.cuda.empty_cache()
     ms = out["ms"]
     out["speedup_learned_vs_direct"] = ms["direct_cholesky"] / ms["learned_pcg"]
     out["speedup_learned_vs_jacobi"] = ms["jacobi_pcg"] / ms["learned_pcg"]

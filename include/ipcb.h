@@ -318,8 +318,10 @@ int ipcb_fsai_apply(const ipcb_graph* g, const float* G, const float* scale, int
  * solve turns further launches into no-ops.  precond 0: block Jacobi (dinv:
  * inverse diagonal blocks, scalar[9n], from ipcb_block_jacobi); precond 1:
  * the learned FSAI factor (diag: int32[n] diagonal block indices, g: bf16
- * [9 nnz] from ipcb_fsai_mirror, scale: float[3n], t: scalar[3n] scratch).
- * state->status bit 1: breakdown (p.Ap <= 0). */
+ * [9 nnz] from ipcb_fsai_mirror on its own pattern g_offsets / g_columns,
+ * scale: float[3n], t: scalar[3n] scratch).  The factor's pattern may differ
+ * from A's (a factor kept from an earlier Newton matrix is still an SPD
+ * preconditioner).  state->status bit 1: breakdown (p.Ap <= 0). */
 typedef struct {
   double rz, rz_new, pAp, rr, bb, tol2, last_rr;
   int it, done, maxiter, status;
@@ -331,6 +333,8 @@ typedef struct {
   const int* columns;
   const void* values;
   const void* dinv;
+  const int* g_offsets;
+  const int* g_columns;
   const int* diag;
   const void* g;
   const float* scale;

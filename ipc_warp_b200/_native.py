@@ -48,8 +48,8 @@ class PcgState(ctypes.Structure):
 
 class Pcg(ctypes.Structure):
     _fields_ = [("n", c_int), ("fp64", c_int), ("precond", c_int), ("offsets", P), ("columns", P), ("values", P),
-                ("dinv", P), ("diag", P), ("g", P), ("scale", P), ("b", P), ("x", P), ("r", P), ("z", P), ("p", P),
-                ("q", P), ("t", P), ("state", P)]
+                ("dinv", P), ("g_offsets", P), ("g_columns", P), ("diag", P), ("g", P), ("scale", P), ("b", P),
+                ("x", P), ("r", P), ("z", P), ("p", P), ("q", P), ("t", P), ("state", P)]
 
 
 SP, CP, BP = ctypes.POINTER(Soup), ctypes.POINTER(Contacts), ctypes.POINTER(Lbvh)

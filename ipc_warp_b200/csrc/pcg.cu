@@ -352,10 +352,10 @@ int precond(const ipcb_pcg* P, cudaStream_t s) {
   if (P->precond == 0)
     k_jacobi<T><<<flat_grid(n), kBlock, 0, s>>>(n, (const T*)P->dinv, (const T*)P->r, (T*)P->z, P->state);
   else {
-    k_fsai_lower<T><<<warp_grid(n), kBlock, 0, s>>>(n, P->offsets, P->diag, P->columns, (const bf16*)P->g,
-                                                       P->scale, (const T*)P->r, (T*)P->t, P->state);
-    k_fsai_upper<T><<<warp_grid(n), kBlock, 0, s>>>(n, P->offsets, P->diag, P->columns, (const bf16*)P->g,
-                                                       P->scale, (const T*)P->t, (const T*)P->r, (T*)P->z, P->state);
+    k_fsai_lower<T><<<warp_grid(n), kBlock, 0, s>>>(n, P->g_offsets, P->diag, P->g_columns, (const bf16*)P->g,
+                                                   P->scale, (const T*)P->r, (T*)P->t, P->state);
+    k_fsai_upper<T><<<warp_grid(n), kBlock, 0, s>>>(n, P->g_offsets, P->diag, P->g_columns, (const bf16*)P->g,
+                                                   P->scale, (const T*)P->t, (const T*)P->r, (T*)P->z, P->state);
   }
   return 0;
 }
@@ -390,7 +390,7 @@ bool pcg_ok(const ipcb_pcg* P) {
       !P->b || !P->state)
     return false;
   if (P->precond == 0) return P->dinv != nullptr;
-  if (P->precond == 1) return P->diag && P->g && P->scale && P->t;
+  if (P->precond == 1) return P->g_offsets && P->g_columns && P->diag && P->g && P->scale && P->t;
   return false;
 }
 

@@ -251,7 +251,15 @@ class LearnedFactor:
     kind = 1
 
     def __init__(self, net: Net, A: BsrMatrix):
-        self.sysm = System.from_bsr(A)
+        # own copy of the pattern: the factor may outlive this matrix (reuse
+        # across Newton iterations), whose buffers a later assembly overwrites
+        nnz = A.nnz_sync()
+        B = BsrMatrix(A.nrow, A.ncol, nnz, A.dtype, A.device)
+        B.offsets.copy_(A.offsets)
+        B.columns[:nnz].copy_(A.columns[:nnz])
+        B.values[:nnz].copy_(A.values[:nnz])
+        B.nnz_dev.copy_(A.nnz_dev)
+        self.sysm = System.from_bsr(B)
         H, _ = forward(net, self.sysm)
         self.G = normalize(self.sysm, H).G
         self.gh = torch.empty((self.sysm.graph.nnz, 9), dtype=torch.bfloat16, device=A.device)
@@ -259,7 +267,9 @@ class LearnedFactor:
                N.stream_handle())
 
     def fill(self, P):
-        P.diag = N.ptr(self.sysm.graph.diag)
+        g = self.sysm.graph
+        P.g_offsets, P.g_columns = N.ptr(g.offsets), N.ptr(g.columns)
+        P.diag = N.ptr(g.diag)
         P.g = N.ptr(self.gh)
         P.scale = N.ptr(self.sysm.scale)
 

@@ -104,11 +104,14 @@ def pcg(A: BsrMatrix, b: torch.Tensor, precond, tol: float = 1e-6, maxiter: int 
 
 
 class JacobiPrecond:
-    """Block-Jacobi preconditioner for DevicePcg (inverse diagonal blocks)."""
+    """Block-Jacobi preconditioner for DevicePcg (inverse diagonal blocks);
+    ``out`` reuses a buffer, so that a graph-replayed PCG keeps its pointers."""
     kind = 0
 
-    def __init__(self, A: BsrMatrix):
-        self.dinv = torch.empty((A.nrow, 3, 3), dtype=A.dtype, device=A.device)
+    def __init__(self, A: BsrMatrix, out: torch.Tensor | None = None):
+        shape = (A.nrow, 3, 3)
+        ok = out is not None and tuple(out.shape) == shape and out.dtype == A.dtype
+        self.dinv = out if ok else torch.empty(shape, dtype=A.dtype, device=A.device)
         status = torch.zeros(1, dtype=torch.int32, device=A.device)
         N.call("ipcb_block_jacobi", A.nrow, N.ptr(A.offsets), N.ptr(A.columns), None, N.ptr(A.values),
                int(A.dtype == torch.float64), N.ptr(self.dinv), N.ptr(status), N.stream_handle())
@@ -180,7 +183,8 @@ class FEMContactSolver(ContactBarrierMixin):
                  gravity=(0.0, -9.8, 0.0), h: float = 1e-2, fixed: np.ndarray | None = None,
                  attachment_stiffness: float = 1e11, dtype=torch.float32, device="cuda", vel_tol: float = 5e-2,
                  max_newton: int = 100, tol: float = 1e-4, maxiter: int = 200, exclude_same_body: bool = False,
-                 linear_solver: str = "pcg", direct_fallback: bool = True, preconditioner: str = "jacobi"):
+                 linear_solver: str = "pcg", direct_fallback: bool = True, preconditioner: str = "jacobi",
+                 precond_refresh: int = 1):
         self.h = float(h)
         self.material = MATERIALS[material]
         self.mu, self.lam = lame(E, nu)
@@ -223,7 +227,14 @@ class FEMContactSolver(ContactBarrierMixin):
         # the same preconditioner for DevicePcg
         if preconditioner == "jacobi":
             self.precond_factory = BlockJacobi
-            self.device_precond = JacobiPrecond
+            self._dinv = None
+
+            def jacobi(A):
+                p = JacobiPrecond(A, self._dinv)
+                self._dinv = p.dinv
+                return p
+
+            self.device_precond = jacobi
         elif preconditioner == "learned":
             from .learned import DEFAULT_WEIGHTS, LearnedFactor, LearnedPreconditioner, Net
 
@@ -234,6 +245,12 @@ class FEMContactSolver(ContactBarrierMixin):
             raise ValueError(f"unknown preconditioner {preconditioner!r}")
         self.host_pcg = False
         self.device_pcg = DevicePcg()
+        # the learned factor is rebuilt every `precond_refresh` Newton
+        # iterations (and at the first iteration of a step); in between the
+        # previous factor preconditions the new matrix
+        self.precond_refresh = max(int(precond_refresh), 1)
+        self._precond = None
+        self._precond_age = 0
         if linear_solver not in ("pcg", "direct"):
             raise ValueError(f"unknown linear solver {linear_solver!r}")
         self.linear_solver = linear_solver
@@ -321,8 +338,12 @@ class FEMContactSolver(ContactBarrierMixin):
             if self.host_pcg:
                 dx, its, rel = pcg(self.A, self.rhs, self.precond_factory(self.A), self.tol, self.maxiter)
             else:
-                x, its, rel, status = self.device_pcg.solve(self.A, self.rhs, self.device_precond(self.A), self.tol,
-                                                            self.maxiter)
+                if self._precond is None or self._precond_age >= self.precond_refresh or \
+                        getattr(self._precond, "kind", 0) == 0:
+                    self._precond = self.device_precond(self.A)
+                    self._precond_age = 0
+                self._precond_age += 1
+                x, its, rel, status = self.device_pcg.solve(self.A, self.rhs, self._precond, self.tol, self.maxiter)
                 dx = x.clone()
                 if status:
                     rel = float("nan")
@@ -385,6 +406,7 @@ class FEMContactSolver(ContactBarrierMixin):
     def step(self) -> StepStats:
         """time_integrator_base.py:375-401."""
         self.stats = StepStats()
+        self._precond = None  # a fresh factor at the first iteration of every step
         if self.boundary is not None:
             self.x_target.copy_(torch.as_tensor(self.boundary(self.time + self.h), dtype=self.dtype))
         for it in range(self.max_newton):
