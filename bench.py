@@ -270,6 +270,28 @@ def newton_step_times(dev, torch, reps: int = 3, direct_reps: int = 1):
     return out
 
 
+def run_profile_solver(args):
+    """Untimed launches of the Newton solve's kernels on the wound rod bundle
+    (for ncu): two learned-factor builds (MPNN forward, row normalisation,
+    bf16 mirror) and two short PCG solves (learned factor, block Jacobi)."""
+    import torch
+
+    from ipc_warp_b200 import learned as L
+    from ipc_warp_b200.newton import DevicePcg, JacobiPrecond
+
+    dev = torch.device("cuda", 0)
+    s = newton_solver(dev, torch, "pcg", "jacobi")
+    s.compute_A()
+    s.compute_rhs()
+    net = L.Net.load(L.DEFAULT_WEIGHTS, device=dev)
+    for _ in range(2):
+        M = L.LearnedFactor(net, s.A)
+    dp = DevicePcg(batch=4, use_graph=False)
+    dp.solve(s.A, s.rhs, M, 1e-6, 8)
+    dp.solve(s.A, s.rhs, JacobiPrecond(s.A), 1e-6, 8)
+    torch.cuda.synchronize()
+
+
 # ------------------------------------------------------------- CPU oracle
 def cpu_pipeline(sc, dx, reps):
     """One pass of the oracle's restatement: DCD EE + PT, narrow phase
@@ -460,7 +482,12 @@ def main():
                     help="warmup + K steps only (for ncu launch lists); prints nothing")
     ap.add_argument("--no-newton", action="store_true",
                     help="skip the Newton-step timing (learned-PCG / Jacobi-PCG / direct)")
+    ap.add_argument("--profile-solver", action="store_true",
+                    help="untimed Newton-solve kernels only (learned factor + PCG), for ncu; prints nothing")
     args = ap.parse_args()
+    if args.profile_solver:
+        run_profile_solver(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
