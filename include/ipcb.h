@@ -194,6 +194,70 @@ int ipcb_tet_hessian(int material, int fp64, const void* x, const int* tets, int
 int ipcb_tet_energy(int material, int fp64, const void* x, const int* tets, int n_tets, const void* Bm, const void* W,
                     double mu, double lam, double* energy, ipcb_stream s);
 
+/* ---- Body-local (fixed) hierarchies for affine bodies ----
+ * fixed_bvh_contacts.py:32-827 (FixedBodyContactSolver): every body keeps the
+ * hierarchies of its rest-frame edges and triangles, built once; a query
+ * primitive of body a is mapped into body b's rest frame (x_local =
+ * A_b^-1 (x - p_b)) and tested against b's hierarchy, then accepted by the
+ * same exact world-space predicate and append as ipcb_dcd_ee / ipcb_dcd_pt.
+ * q: scalar[12 nb], per body p, A[:,0], A[:,1], A[:,2] (x = p + A r,
+ * affine_body_dynamics.py:1-10).  Per-body primitive lists: the primitives of
+ * body b are ids[off[b] .. off[b+1]); the 4-wide hierarchy of body b
+ * (ipcb_lbvh.wide of a tree built over its rest boxes in that order) is
+ * edge_wide[b] / tri_wide[b].  frames: double[19 nb] scratch (A^-1, p,
+ * |A^-1|_F, then the world boxes), motion: double[3 nb] scratch, written by
+ * the pair culls; int32 grids cap pairs x chunks at 2^31 blocks. */
+#define IPCB_STATUS_SINGULAR 32 /* a body's |det A| < 1e-8: use the dynamic path */
+
+typedef struct {
+  int n_bodies;
+  const float* local_lower;
+  const float* local_upper;
+  const int* edge_off;
+  const int* edge_ids;
+  const int* tri_off;
+  const int* tri_ids;
+  const int* vert_off;
+  const int* vert_ids;
+  const void* const* edge_wide;
+  const void* const* tri_wide;
+  int max_edges, max_tris, max_verts;
+  double* frames;
+  double* motion;
+} ipcb_bodies;
+
+/* Overlapping body pairs (a < b) of the world boxes of the affine bodies,
+ * padded by `padding` (affine_body_aabbs + compact_overlapping_body_pairs,
+ * fixed_bvh_contacts.py:48-99); also fills `frames`.  pairs int2[capacity],
+ * *count may exceed capacity (grow and relaunch). */
+int ipcb_body_pairs(const ipcb_bodies* B, int fp64, const void* q, double padding, int* pairs, int capacity,
+                    int* count, int* status, ipcb_stream s);
+/* EE (source body = pair.x) and PT (both directions) queries of
+ * batched_fixed_bvh_edge_edge_query / _point_triangle_query
+ * (fixed_bvh_contacts.py:295-380): padding |A^-1|_F * 2 thickness. */
+int ipcb_fixed_dcd_ee(const ipcb_soup* soup, const float* x4, const ipcb_bodies* B, const int* pairs, int n_pairs,
+                      float thickness, ipcb_contacts* out, int* status, ipcb_stream s);
+int ipcb_fixed_dcd_pt(const ipcb_soup* soup, const float* x4, const ipcb_bodies* B, const int* pairs, int n_pairs,
+                      float thickness, ipcb_contacts* out, int* status, ipcb_stream s);
+/* Swept body pairs for the step x -= dq (affine_swept_body_aabbs,
+ * fixed_bvh_contacts.py:144-175): boxes of the bodies at q and q - dq, also
+ * `frames` (at q) and `motion` (the target-frame motion extent,
+ * _target_motion_extent 121-141); IPCB_STATUS_SINGULAR when a body's
+ * |det A| < 1e-8 at either end. */
+int ipcb_body_pairs_swept(const ipcb_bodies* B, int fp64, const void* q, const void* dq, double padding, int* pairs,
+                          int capacity, int* count, int* status, ipcb_stream s);
+/* CCD over the fixed hierarchies (batched_fixed_bvh_edge_edge_toi /
+ * _point_triangle_toi, fixed_bvh_contacts.py:178-292): swept local query
+ * boxes inflated by the target's motion extent and |A^-1|_F * pad; the TOI
+ * of each candidate is the same exact computation as ipcb_edge_edge_toi.
+ * fixed: int32[nb] fixed-body flags (an EE query runs from the moving body). */
+int ipcb_fixed_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_bodies* B, const int* fixed,
+                             const int* pairs, int n_pairs, double pad, void* toi, int* status, void* ws,
+                             size_t ws_bytes, ipcb_stream s);
+int ipcb_fixed_point_triangle_toi(const ipcb_soup* soup, const void* x1, const ipcb_bodies* B, const int* pairs,
+                                  int n_pairs, double pad, void* toi, int* status, void* ws, size_t ws_bytes,
+                                  ipcb_stream s);
+
 /* ---- BSR assembly (warp.sparse.bsr_from_triplets, dynamic_contacts.py:290-297) ----
  * Canonical 3x3-block CSR from triplets: sort by (row, col), sum duplicates,
  * drop triplets whose 9 values are all zero.  offsets int32[nrow+1],

@@ -31,6 +31,12 @@ class Lbvh(ctypes.Structure):
                 ("flags", P), ("wide", P)]
 
 
+class Bodies(ctypes.Structure):
+    _fields_ = [("n_bodies", c_int), ("local_lower", P), ("local_upper", P), ("edge_off", P), ("edge_ids", P),
+                ("tri_off", P), ("tri_ids", P), ("vert_off", P), ("vert_ids", P), ("edge_wide", P), ("tri_wide", P),
+                ("max_edges", c_int), ("max_tris", c_int), ("max_verts", c_int), ("frames", P), ("motion", P)]
+
+
 class Graph(ctypes.Structure):
     _fields_ = [("n", c_int), ("nnz", c_int), ("n_lower", c_int), ("offsets", P), ("columns", P), ("rows", P),
                 ("rev", P), ("diag", P), ("lower", P)]
@@ -53,6 +59,7 @@ class Pcg(ctypes.Structure):
 
 
 SP, CP, BP = ctypes.POINTER(Soup), ctypes.POINTER(Contacts), ctypes.POINTER(Lbvh)
+BD = ctypes.POINTER(Bodies)
 GP, TP = ctypes.POINTER(Graph), ctypes.POINTER(Tape)
 
 # name -> (restype, argtypes); every symbol here is declared in include/ipcb.h
@@ -102,6 +109,12 @@ SIGNATURES = {
     "ipcb_pcg_iterate": (c_int, [ctypes.POINTER(Pcg), c_int, P]),
     "ipcb_block_jacobi": (c_int, [c_int, P, P, P, P, c_int, P, P, P]),
     "ipcb_fsai_mirror": (c_int, [GP, P, P, P]),
+    "ipcb_body_pairs": (c_int, [BD, c_int, P, c_double, P, c_int, P, P, P]),
+    "ipcb_fixed_dcd_ee": (c_int, [SP, P, BD, P, c_int, c_float, CP, P, P]),
+    "ipcb_fixed_dcd_pt": (c_int, [SP, P, BD, P, c_int, c_float, CP, P, P]),
+    "ipcb_body_pairs_swept": (c_int, [BD, c_int, P, P, c_double, P, c_int, P, P, P]),
+    "ipcb_fixed_edge_edge_toi": (c_int, [SP, P, BD, P, P, c_int, c_double, P, P, P, c_size_t, P]),
+    "ipcb_fixed_point_triangle_toi": (c_int, [SP, P, BD, P, c_int, c_double, P, P, P, c_size_t, P]),
     "ipcb_umma_gemm_bf16": (c_int, [c_int, c_int, c_int, P, P, P, P, P]),
     "ipcb_tet_rest": (c_int, [c_int, P, P, c_int, P, P, P]),
     "ipcb_tet_hessian": (c_int, [c_int, c_int, P, P, c_int, P, P, c_double, c_double, P, P, P, P, P]),

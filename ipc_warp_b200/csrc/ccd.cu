@@ -5,6 +5,7 @@
 // plain IEEE evaluation.
 #include <cooperative_groups.h>
 
+#include "bodies.cuh"
 #include "common.cuh"
 #include "lbvh.cuh"
 
@@ -568,6 +569,207 @@ __global__ void __launch_bounds__(128) k_cand_toi(const S* __restrict__ x0, cons
   if (st) atomicOr(status, st);
 }
 
+// ---------------------------------------------------------------- fixed bodies
+// frames at q, swept world boxes of the bodies over the step q -> q - dq, the
+// singular test at both ends, and the target-frame motion extent
+// (_target_motion_extent, fixed_bvh_contacts.py:121-141):
+//   d = A0^-1 (A1 - A0), c = A0^-1 (p1 - p0), m = |d mid + c| + |d| ext
+template <class S>
+__global__ void k_body_frames_swept(int nb, const S* __restrict__ q, const S* __restrict__ dq,
+                                    const float* __restrict__ llo, const float* __restrict__ lhi,
+                                    double* __restrict__ frames, double* __restrict__ motion,
+                                    int* __restrict__ status) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  double p0[3], A0[9], p1[3], A1[9], I[9], w0l[3], w0h[3], w1l[3], w1h[3];
+  bodies::load_affine(q, b, p0, A0);
+  for (int k = 0; k < 3; ++k) p1[k] = p0[k] - (double)dq[12 * b + k];
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) A1[3 * r + c] = A0[3 * r + c] - (double)dq[12 * b + 3 + 3 * c + r];
+  const double d0 = bodies::det3(A0), d1 = bodies::det3(A1);
+  if (!(fmin(fabs(d0), fabs(d1)) >= 1e-8)) {
+    atomicOr(status, IPCB_STATUS_SINGULAR);
+    for (int k = 0; k < 9; ++k) I[k] = (k % 4) == 0 ? 1.0 : 0.0;
+  } else {
+    bodies::inverse3(A0, d0, I);
+  }
+  double fro = 0.0;
+  for (int k = 0; k < 9; ++k) {
+    frames[13 * b + k] = I[k];
+    fro += I[k] * I[k];
+  }
+  for (int k = 0; k < 3; ++k) frames[13 * b + 9 + k] = p0[k];
+  frames[13 * b + 12] = sqrt(fro);
+  const float* lo = llo + 3 * b;
+  const float* hi = lhi + 3 * b;
+  bodies::world_box(p0, A0, lo, hi, w0l, w0h);
+  bodies::world_box(p1, A1, lo, hi, w1l, w1h);
+  double* wbox = frames + 13 * (size_t)nb + 6 * b;
+  for (int k = 0; k < 3; ++k) {
+    wbox[k] = fmin(w0l[k], w1l[k]);
+    wbox[3 + k] = fmax(w0h[k], w1h[k]);
+  }
+  double D[9], cvec[3];
+  for (int r = 0; r < 3; ++r) {
+    for (int c = 0; c < 3; ++c) {
+      double acc = 0.0;
+      for (int k = 0; k < 3; ++k) acc += I[3 * r + k] * (A1[3 * k + c] - A0[3 * k + c]);
+      D[3 * r + c] = acc;
+    }
+    cvec[r] = I[3 * r] * (p1[0] - p0[0]) + I[3 * r + 1] * (p1[1] - p0[1]) + I[3 * r + 2] * (p1[2] - p0[2]);
+  }
+  for (int r = 0; r < 3; ++r) {
+    double dc = cvec[r], e = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      const double mid = 0.5 * ((double)lo[k] + (double)hi[k]), ext = 0.5 * ((double)hi[k] - (double)lo[k]);
+      dc += D[3 * r + k] * mid;
+      e += fabs(D[3 * r + k]) * ext;
+    }
+    motion[3 * b + r] = fabs(dc) + e;
+  }
+}
+
+__global__ void k_swept_pair_cull(int nb, const double* __restrict__ wbox, double pad, int2* __restrict__ pairs,
+                                  int capacity, int* __restrict__ count) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = (int)(t / nb), b = (int)(t % nb);
+  bool hit = false;
+  if (a < nb && a < b) {
+    hit = true;
+    for (int k = 0; k < 3; ++k)
+      hit = hit && wbox[6 * a + k] - pad <= wbox[6 * b + 3 + k] && wbox[6 * b + k] - pad <= wbox[6 * a + 3 + k];
+  }
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned m = __ballot_sync(0xffffffffu, hit);
+  int base = 0;
+  if (lane == 0 && m) base = atomicAdd(count, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  const int slot = base + __popc(m & ((1u << lane) - 1u));
+  if (hit && slot < capacity) pairs[slot] = make_int2(a, b);
+}
+
+// swept local box of world points (x0 and x1 of each) in the target frame,
+// inflated by the frame's motion extent and |A^-1|_F pad
+template <class S, int NP>
+IPCB_D void swept_local_box(const bodies::Frame& f, const double* __restrict__ motion, int tb, const S* __restrict__ x0,
+                            const S* __restrict__ x1, const int (&v)[NP], double pad, f3& qlo, f3& qhi) {
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300}, pd[3], a[3];
+  for (int k = 0; k < NP; ++k) {
+    const d3 p = ld(x0, v[k]), r = ld(x1, v[k]);
+    bodies::to_local(f, p.x, p.y, p.z, a);
+    for (int c = 0; c < 3; ++c) {
+      lo[c] = fmin(lo[c], a[c]);
+      hi[c] = fmax(hi[c], a[c]);
+    }
+    bodies::to_local(f, r.x, r.y, r.z, a);
+    for (int c = 0; c < 3; ++c) {
+      lo[c] = fmin(lo[c], a[c]);
+      hi[c] = fmax(hi[c], a[c]);
+    }
+  }
+  for (int c = 0; c < 3; ++c)
+    pd[c] = motion[3 * tb + c] + f.fro * pad + 1e-6 * (1.0 + fmax(fabs(lo[c]), fabs(hi[c])));
+  bodies::float_box(lo, hi, pd, qlo, qhi);
+}
+
+template <class S>
+__global__ void __launch_bounds__(128) k_fixed_ee_collect(const S* __restrict__ x0, const S* __restrict__ x1,
+                                                          const int* __restrict__ edges, ipcb_bodies B,
+                                                          const int* __restrict__ fixed, const int2* __restrict__ pairs,
+                                                          double pad, CandList cand, S* toi, int* status) {
+  const int chunks = (B.max_edges + 127) / 128;
+  const int pair = blockIdx.x / chunks;
+  const int k = (blockIdx.x % chunks) * blockDim.x + threadIdx.x;
+  int2 pr = pairs[pair];
+  if (fixed && fixed[pr.x] != 0 && fixed[pr.y] == 0) pr = make_int2(pr.y, pr.x);  // query from the moving body
+  const int sb = pr.x, tb = pr.y;
+  const int s0 = __ldg(B.edge_off + sb), sn = __ldg(B.edge_off + sb + 1) - s0;
+  const bool active = k < sn;
+  const int i = active ? __ldg(B.edge_ids + s0 + k) : 0;
+  const int2 ea = __ldg(reinterpret_cast<const int2*>(edges) + i);
+  const int t0 = __ldg(B.edge_off + tb), tn = __ldg(B.edge_off + tb + 1) - t0;
+  int st = 0;
+  int q[kQueue];
+  int nq = 0;
+  if (active && tn > 0) {
+    const bodies::Frame f = bodies::load_frame(B.frames, tb);
+    const int v[2] = {ea.x, ea.y};
+    f3 qlo, qhi;
+    swept_local_box<S, 2>(f, B.motion, tb, x0, x1, v, pad, qlo, qhi);
+    const float4* wide = reinterpret_cast<const float4*>(B.edge_wide[tb]);
+    bool ok = traverse4(wide, tn, qlo, qhi, [&](int j) {
+      const int e2 = __ldg(B.edge_ids + t0 + j);
+      if (nq < kQueue) {
+        q[nq++] = e2;
+      } else {
+        const int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + e2);
+        double tt = ee_pair_time(x0, x1, ea, eb, st);
+        if (tt < 1.0) store_toi(toi, tt);
+      }
+    });
+    if (!ok) st |= IPCB_STATUS_STACK;
+  }
+  const int rounds = warp_max(nq);
+  for (int r = 0; r < rounds; ++r) {
+    const bool has = r < nq;
+    const int e2 = has ? q[r] : 0;
+    if (!push_converged(cand, has, i, e2)) {
+      const int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + e2);
+      double tt = ee_pair_time(x0, x1, ea, eb, st);
+      if (tt < 1.0) store_toi(toi, tt);
+    }
+  }
+  if (st) atomicOr(status, st);
+}
+
+template <class S>
+__global__ void __launch_bounds__(128) k_fixed_pt_collect(const S* __restrict__ x0, const S* __restrict__ x1,
+                                                          const int* __restrict__ tris, ipcb_bodies B,
+                                                          const int2* __restrict__ pairs, double pad, CandList cand,
+                                                          S* toi, int* status) {
+  const int chunks = (B.max_verts + 127) / 128;
+  const int pair = blockIdx.x / chunks, dir = blockIdx.y;
+  const int k = (blockIdx.x % chunks) * blockDim.x + threadIdx.x;
+  const int2 pr = pairs[pair];
+  const int sb = dir ? pr.y : pr.x, tb = dir ? pr.x : pr.y;
+  const int s0 = __ldg(B.vert_off + sb), sn = __ldg(B.vert_off + sb + 1) - s0;
+  const bool active = k < sn;
+  const int i = active ? __ldg(B.vert_ids + s0 + k) : 0;
+  const int t0 = __ldg(B.tri_off + tb), tn = __ldg(B.tri_off + tb + 1) - t0;
+  int st = 0;
+  int q[kQueue];
+  int nq = 0;
+  if (active && tn > 0) {
+    const bodies::Frame f = bodies::load_frame(B.frames, tb);
+    const int v[1] = {i};
+    f3 qlo, qhi;
+    swept_local_box<S, 1>(f, B.motion, tb, x0, x1, v, pad, qlo, qhi);
+    const float4* wide = reinterpret_cast<const float4*>(B.tri_wide[tb]);
+    bool ok = traverse4(wide, tn, qlo, qhi, [&](int j) {
+      const int tr = __ldg(B.tri_ids + t0 + j);
+      if (nq < kQueue) {
+        q[nq++] = tr;
+      } else {
+        const int3 tj = make_int3(__ldg(tris + 3 * tr), __ldg(tris + 3 * tr + 1), __ldg(tris + 3 * tr + 2));
+        double tt = pt_pair_time(x0, x1, i, tj, st);
+        if (tt < 1.0) store_toi(toi, tt);
+      }
+    });
+    if (!ok) st |= IPCB_STATUS_STACK;
+  }
+  const int rounds = warp_max(nq);
+  for (int r = 0; r < rounds; ++r) {
+    const bool has = r < nq;
+    const int tr = has ? q[r] : 0;
+    if (!push_converged(cand, has, i, tr)) {
+      const int3 tj = make_int3(__ldg(tris + 3 * tr), __ldg(tris + 3 * tr + 1), __ldg(tris + 3 * tr + 2));
+      double tt = pt_pair_time(x0, x1, i, tj, st);
+      if (tt < 1.0) store_toi(toi, tt);
+    }
+  }
+  if (st) atomicOr(status, st);
+}
+
 inline CandList cand_list(void* ws, size_t ws_bytes) {
   CandList c;
   c.count = (int*)ws;
@@ -731,6 +933,84 @@ int ipcb_cubic_roots(int n, const double* coef, double x0, double x1, double* ro
   if (!coef || !roots || !n_roots || !status) return IPCB_E_ARG;
   k_cubic<<<div_up(n, 128), 128, 0, (cudaStream_t)s>>>(n, coef, x0, x1, roots, n_roots, status);
   return check_launch("ipcb_cubic_roots");
+}
+
+
+static bool bodies_ok(const ipcb_bodies* B) {
+  return B && B->n_bodies > 0 && B->local_lower && B->local_upper && B->edge_off && B->edge_ids && B->tri_off &&
+         B->tri_ids && B->vert_off && B->vert_ids && B->edge_wide && B->tri_wide && B->frames && B->motion;
+}
+
+int ipcb_body_pairs_swept(const ipcb_bodies* B, int fp64, const void* q, const void* dq, double padding, int* pairs,
+                          int capacity, int* count, int* status, ipcb_stream s) {
+  if (!bodies_ok(B) || !q || !dq || !pairs || capacity < 0 || !count || !status) return IPCB_E_ARG;
+  cudaStream_t st = (cudaStream_t)s;
+  const int nb = B->n_bodies;
+  if (fp64)
+    k_body_frames_swept<double><<<div_up(nb, 128), 128, 0, st>>>(nb, (const double*)q, (const double*)dq,
+                                                                  B->local_lower, B->local_upper, B->frames,
+                                                                  B->motion, status);
+  else
+    k_body_frames_swept<float><<<div_up(nb, 128), 128, 0, st>>>(nb, (const float*)q, (const float*)dq,
+                                                                 B->local_lower, B->local_upper, B->frames,
+                                                                 B->motion, status);
+  k_swept_pair_cull<<<div_up((long long)nb * nb, 256), 256, 0, st>>>(nb, B->frames + 13 * (size_t)nb, padding,
+                                                                     (int2*)pairs, capacity, count);
+  return check_launch("ipcb_body_pairs_swept");
+}
+
+int ipcb_fixed_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_bodies* B, const int* fixed,
+                             const int* pairs, int n_pairs, double pad, void* toi, int* status, void* ws,
+                             size_t ws_bytes, ipcb_stream s) {
+  if (!soup || !x1 || !bodies_ok(B) || !pairs || n_pairs < 0 || !toi || !status || !ws || ws_bytes < 256)
+    return IPCB_E_ARG;
+  if (n_pairs == 0 || B->max_edges == 0) return IPCB_OK;
+  cudaStream_t st = (cudaStream_t)s;
+  CandList c = cand_list(ws, ws_bytes);
+  cudaMemsetAsync(c.count, 0, sizeof(int), st);
+  dim3 grid(div_up(B->max_edges, 128) * n_pairs);
+  const int gc = div_up(c.capacity > 0 ? c.capacity : 1, 128);
+  if (soup->fp64) {
+    k_fixed_ee_collect<double><<<grid, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, *B,
+                                                     fixed, (const int2*)pairs, pad, c, (double*)toi, status);
+    if (c.capacity)
+      k_cand_toi<double, 0><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, c,
+                                              (double*)toi, status);
+  } else {
+    k_fixed_ee_collect<float><<<grid, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, *B, fixed,
+                                                    (const int2*)pairs, pad, c, (float*)toi, status);
+    if (c.capacity)
+      k_cand_toi<float, 0><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, c, (float*)toi,
+                                             status);
+  }
+  return check_launch("ipcb_fixed_edge_edge_toi");
+}
+
+int ipcb_fixed_point_triangle_toi(const ipcb_soup* soup, const void* x1, const ipcb_bodies* B, const int* pairs,
+                                  int n_pairs, double pad, void* toi, int* status, void* ws, size_t ws_bytes,
+                                  ipcb_stream s) {
+  if (!soup || !x1 || !bodies_ok(B) || !pairs || n_pairs < 0 || !toi || !status || !ws || ws_bytes < 256)
+    return IPCB_E_ARG;
+  if (n_pairs == 0 || B->max_verts == 0) return IPCB_OK;
+  cudaStream_t st = (cudaStream_t)s;
+  CandList c = cand_list(ws, ws_bytes);
+  cudaMemsetAsync(c.count, 0, sizeof(int), st);
+  dim3 grid(div_up(B->max_verts, 128) * n_pairs, 2);
+  const int gc = div_up(c.capacity > 0 ? c.capacity : 1, 128);
+  if (soup->fp64) {
+    k_fixed_pt_collect<double><<<grid, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, *B,
+                                                     (const int2*)pairs, pad, c, (double*)toi, status);
+    if (c.capacity)
+      k_cand_toi<double, 1><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, c,
+                                              (double*)toi, status);
+  } else {
+    k_fixed_pt_collect<float><<<grid, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, *B,
+                                                    (const int2*)pairs, pad, c, (float*)toi, status);
+    if (c.capacity)
+      k_cand_toi<float, 1><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, c,
+                                             (float*)toi, status);
+  }
+  return check_launch("ipcb_fixed_point_triangle_toi");
 }
 
 }  // extern "C"

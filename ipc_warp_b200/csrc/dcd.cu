@@ -2,6 +2,7 @@
 // (contact.py:30-52, 199-228, 304-336).
 #include <cooperative_groups.h>
 
+#include "bodies.cuh"
 #include "common.cuh"
 #include "geom.cuh"
 #include "lbvh.cuh"
@@ -175,6 +176,161 @@ __global__ void __launch_bounds__(128) k_dcd_pt(const float4* __restrict__ x4, c
   }
 }
 
+// ---------------------------------------------------------------- fixed bodies
+// world boxes of the bodies, frames, and the padded pair cull (a < b)
+template <class S>
+__global__ void k_body_frames(int nb, const S* __restrict__ q, const float* __restrict__ llo,
+                              const float* __restrict__ lhi, double* __restrict__ frames,
+                              double* __restrict__ wbox, int* __restrict__ status) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  double p[3], A[9], I[9], wl[3], wh[3];
+  bodies::load_affine(q, b, p, A);
+  const double det = bodies::det3(A);
+  if (!(fabs(det) >= 1e-8)) {
+    atomicOr(status, IPCB_STATUS_SINGULAR);
+    for (int k = 0; k < 9; ++k) I[k] = (k % 4) == 0 ? 1.0 : 0.0;
+  } else {
+    bodies::inverse3(A, det, I);
+  }
+  double fro = 0.0;
+  for (int k = 0; k < 9; ++k) {
+    frames[13 * b + k] = I[k];
+    fro += I[k] * I[k];
+  }
+  for (int k = 0; k < 3; ++k) frames[13 * b + 9 + k] = p[k];
+  frames[13 * b + 12] = sqrt(fro);
+  bodies::world_box(p, A, llo + 3 * b, lhi + 3 * b, wl, wh);
+  for (int k = 0; k < 3; ++k) {
+    wbox[6 * b + k] = wl[k];
+    wbox[6 * b + 3 + k] = wh[k];
+  }
+}
+
+__global__ void k_body_pair_cull(int nb, const double* __restrict__ wbox, double pad, int2* __restrict__ pairs,
+                                 int capacity, int* __restrict__ count) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = (int)(t / nb), b = (int)(t % nb);
+  bool hit = false;
+  if (a < nb && a < b) {
+    hit = true;
+    for (int k = 0; k < 3; ++k)
+      hit = hit && wbox[6 * a + k] - pad <= wbox[6 * b + 3 + k] && wbox[6 * b + k] - pad <= wbox[6 * a + 3 + k];
+  }
+  const int slot = warp_reserve(count, hit);
+  if (hit && slot < capacity) pairs[slot] = make_int2(a, b);
+}
+
+// one thread per (body pair, source edge of pair.x): the edge mapped into
+// pair.y's frame, padded by |A^-1|_F 2 thickness, against pair.y's hierarchy
+template <class S>
+__global__ void __launch_bounds__(128) k_fixed_dcd_ee(const float4* __restrict__ x4, const int* __restrict__ edges,
+                                                      ipcb_bodies B, const int2* __restrict__ pairs, int n_pairs,
+                                                      float thickness, ipcb_contacts out, int* status) {
+  const int chunks = (B.max_edges + 127) / 128;
+  const int pair = blockIdx.x / chunks;
+  const int k = (blockIdx.x % chunks) * blockDim.x + threadIdx.x;
+  const int2 pr = pairs[pair];
+  const int sb = pr.x, tb = pr.y;
+  const int s0 = __ldg(B.edge_off + sb), sn = __ldg(B.edge_off + sb + 1) - s0;
+  const bool active = k < sn;
+  const int i = active ? __ldg(B.edge_ids + s0 + k) : 0;
+  const int2 ea = active ? __ldg(reinterpret_cast<const int2*>(edges) + i) : make_int2(0, 0);
+  const f3 p1 = load4(x4, ea.x), p2 = load4(x4, ea.y);
+  const float l0f = xmul(thickness, 2.0f);
+  const S l0 = S(thickness) * S(2.0);
+  const int t0 = __ldg(B.edge_off + tb), tn = __ldg(B.edge_off + tb + 1) - t0;
+  int q[kQueue];
+  int nq = 0;
+  if (active && tn > 0) {
+    const bodies::Frame f = bodies::load_frame(B.frames, tb);
+    double a[3], c[3], lo[3], hi[3], pad[3];
+    bodies::to_local(f, p1.x, p1.y, p1.z, a);
+    bodies::to_local(f, p2.x, p2.y, p2.z, c);
+    for (int r = 0; r < 3; ++r) {
+      lo[r] = fmin(a[r], c[r]);
+      hi[r] = fmax(a[r], c[r]);
+      pad[r] = f.fro * 2.0 * (double)thickness + 1e-6 * (1.0 + fmax(fabs(lo[r]), fabs(hi[r])));
+    }
+    f3 qlo, qhi;
+    bodies::float_box(lo, hi, pad, qlo, qhi);
+    const float4* wide = reinterpret_cast<const float4*>(B.edge_wide[tb]);
+    bool ok = traverse4(wide, tn, qlo, qhi, [&](int j) {
+      const int e2 = __ldg(B.edge_ids + t0 + j);
+      if (nq < kQueue) {
+        q[nq++] = e2;
+      } else {
+        const int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + e2);
+        CPEE r = closest_point_edge_edge(p1, p2, load4(x4, eb.x), load4(x4, eb.y), 1.0e-6f);
+        if (r.d < l0f) append_divergent<S>(out, ea.x, ea.y, eb.x, eb.y, i, e2, l0);
+      }
+    });
+    if (!ok) atomicOr(status, IPCB_STATUS_STACK);
+  }
+  const int rounds = warp_max(nq);
+  for (int r = 0; r < rounds; ++r) {
+    const bool has = r < nq;
+    const int e2 = has ? q[r] : 0;
+    const int2 eb = has ? __ldg(reinterpret_cast<const int2*>(edges) + e2) : make_int2(0, 0);
+    bool accept = false;
+    if (has) accept = closest_point_edge_edge(p1, p2, load4(x4, eb.x), load4(x4, eb.y), 1.0e-6f).d < l0f;
+    const int slot = warp_reserve(out.cnt, accept);
+    if (accept) write_record<S>(out, slot, ea.x, ea.y, eb.x, eb.y, i, e2, l0);
+  }
+}
+
+// one thread per (body pair, direction, source vertex)
+template <class S>
+__global__ void __launch_bounds__(128) k_fixed_dcd_pt(const float4* __restrict__ x4, const int* __restrict__ tris,
+                                                      ipcb_bodies B, const int2* __restrict__ pairs, int n_pairs,
+                                                      float thickness, ipcb_contacts out, int* status) {
+  const int chunks = (B.max_verts + 127) / 128;
+  const int pair = blockIdx.x / chunks, dir = blockIdx.y;
+  const int k = (blockIdx.x % chunks) * blockDim.x + threadIdx.x;
+  const int2 pr = pairs[pair];
+  const int sb = dir ? pr.y : pr.x, tb = dir ? pr.x : pr.y;
+  const int s0 = __ldg(B.vert_off + sb), sn = __ldg(B.vert_off + sb + 1) - s0;
+  const bool active = k < sn;
+  const int i = active ? __ldg(B.vert_ids + s0 + k) : 0;
+  const f3 p = load4(x4, i);
+  const float l0f = xmul(thickness, 2.0f);
+  const S l0 = S(thickness) * S(2.0);
+  const int t0 = __ldg(B.tri_off + tb), tn = __ldg(B.tri_off + tb + 1) - t0;
+  int q[kQueue];
+  int nq = 0;
+  if (active && tn > 0) {
+    const bodies::Frame f = bodies::load_frame(B.frames, tb);
+    double a[3], pad[3];
+    bodies::to_local(f, p.x, p.y, p.z, a);
+    for (int r = 0; r < 3; ++r) pad[r] = f.fro * 2.0 * (double)thickness + 1e-6 * (1.0 + fabs(a[r]));
+    f3 qlo, qhi;
+    bodies::float_box(a, a, pad, qlo, qhi);
+    const float4* wide = reinterpret_cast<const float4*>(B.tri_wide[tb]);
+    bool ok = traverse4(wide, tn, qlo, qhi, [&](int j) {
+      const int tr = __ldg(B.tri_ids + t0 + j);
+      if (nq < kQueue) {
+        q[nq++] = tr;
+      } else {
+        const int u0 = __ldg(tris + 3 * tr), u1 = __ldg(tris + 3 * tr + 1), u2 = __ldg(tris + 3 * tr + 2);
+        CPT r = closest_point_triangle(p, load4(x4, u0), load4(x4, u1), load4(x4, u2));
+        if (r.d < l0f) append_divergent<S>(out, i, u1, u0, u2, i, tr, l0);
+      }
+    });
+    if (!ok) atomicOr(status, IPCB_STATUS_STACK);
+  }
+  const int rounds = warp_max(nq);
+  for (int r = 0; r < rounds; ++r) {
+    const bool has = r < nq;
+    const int tr = has ? q[r] : 0;
+    const int u0 = has ? __ldg(tris + 3 * tr) : 0, u1 = has ? __ldg(tris + 3 * tr + 1) : 0,
+              u2 = has ? __ldg(tris + 3 * tr + 2) : 0;
+    bool accept = false;
+    if (has) accept = closest_point_triangle(p, load4(x4, u0), load4(x4, u1), load4(x4, u2)).d < l0f;
+    const int slot = warp_reserve(out.cnt, accept);
+    if (accept) write_record<S>(out, slot, i, u1, u0, u2, i, tr, l0);
+  }
+}
+
 }  // namespace
 }  // namespace ipcb
 
@@ -242,6 +398,56 @@ int ipcb_dcd_pt(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* bvh, fl
                                                        (const float4*)bvh->wide, soup->n_tris, query_order, nv,
                                                        thickness, query_pad, exclude_same_body, *out, status);
   return check_launch("ipcb_dcd_pt");
+}
+
+
+static bool bodies_ok(const ipcb_bodies* B) {
+  return B && B->n_bodies > 0 && B->local_lower && B->local_upper && B->edge_off && B->edge_ids && B->tri_off &&
+         B->tri_ids && B->vert_off && B->vert_ids && B->edge_wide && B->tri_wide && B->frames && B->motion;
+}
+
+int ipcb_body_pairs(const ipcb_bodies* B, int fp64, const void* q, double padding, int* pairs, int capacity,
+                    int* count, int* status, ipcb_stream s) {
+  if (!bodies_ok(B) || !q || !pairs || capacity < 0 || !count || !status) return IPCB_E_ARG;
+  cudaStream_t st = (cudaStream_t)s;
+  const int nb = B->n_bodies;
+  double* wbox = B->frames + 13 * (size_t)nb;  // world boxes: 6 doubles per body after the frames
+  if (fp64)
+    k_body_frames<double><<<div_up(nb, 128), 128, 0, st>>>(nb, (const double*)q, B->local_lower, B->local_upper,
+                                                            B->frames, wbox, status);
+  else
+    k_body_frames<float><<<div_up(nb, 128), 128, 0, st>>>(nb, (const float*)q, B->local_lower, B->local_upper,
+                                                           B->frames, wbox, status);
+  k_body_pair_cull<<<div_up((long long)nb * nb, 256), 256, 0, st>>>(nb, wbox, padding, (int2*)pairs, capacity, count);
+  return check_launch("ipcb_body_pairs");
+}
+
+int ipcb_fixed_dcd_ee(const ipcb_soup* soup, const float* x4, const ipcb_bodies* B, const int* pairs, int n_pairs,
+                      float thickness, ipcb_contacts* out, int* status, ipcb_stream s) {
+  if (!soup || !x4 || !bodies_ok(B) || !pairs || n_pairs < 0 || !out || !status) return IPCB_E_ARG;
+  if (n_pairs == 0 || B->max_edges == 0) return IPCB_OK;
+  dim3 grid(div_up(B->max_edges, 128) * n_pairs);
+  if (soup->fp64)
+    k_fixed_dcd_ee<double><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->edges, *B,
+                                                              (const int2*)pairs, n_pairs, thickness, *out, status);
+  else
+    k_fixed_dcd_ee<float><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->edges, *B,
+                                                             (const int2*)pairs, n_pairs, thickness, *out, status);
+  return check_launch("ipcb_fixed_dcd_ee");
+}
+
+int ipcb_fixed_dcd_pt(const ipcb_soup* soup, const float* x4, const ipcb_bodies* B, const int* pairs, int n_pairs,
+                      float thickness, ipcb_contacts* out, int* status, ipcb_stream s) {
+  if (!soup || !x4 || !bodies_ok(B) || !pairs || n_pairs < 0 || !out || !status) return IPCB_E_ARG;
+  if (n_pairs == 0 || B->max_verts == 0) return IPCB_OK;
+  dim3 grid(div_up(B->max_verts, 128) * n_pairs, 2);
+  if (soup->fp64)
+    k_fixed_dcd_pt<double><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->triangles, *B,
+                                                              (const int2*)pairs, n_pairs, thickness, *out, status);
+  else
+    k_fixed_dcd_pt<float><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->triangles, *B,
+                                                             (const int2*)pairs, n_pairs, thickness, *out, status);
+  return check_launch("ipcb_fixed_dcd_pt");
 }
 
 }  // extern "C"
