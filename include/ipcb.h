@@ -258,6 +258,82 @@ int ipcb_fixed_point_triangle_toi(const ipcb_soup* soup, const void* x1, const i
                                   int n_pairs, double pad, void* toi, int* status, void* ws, size_t ws_bytes,
                                   ipcb_stream s);
 
+/* ---- Affine body dynamics (affine_body_dynamics.py:33-217, 427-505) ----
+ * State of nb affine bodies, every array scalar (fp64 ? double : float):
+ * q, q0, q_tilde, qdot, dx: [12 nb], per body p, a0, a1, a2 (ABDState, 33-39;
+ * x = p + r0 a0 + r1 a1 + r2 a2); mass: [16 nb] scalar moments M_ij of
+ * _build_mass_blocks (344-358, which stores M_ij * I); volume, stiffness:
+ * [nb]; fixed: int32[nb]. */
+typedef struct {
+  int n_bodies;
+  int fp64;
+  void* q;
+  void* q0;
+  void* q_tilde;
+  void* qdot;
+  void* dx;
+  const void* mass;
+  const void* volume;
+  const void* stiffness;
+  const int* fixed;
+} ipcb_abd;
+#define IPCB_ABD_MAX_BODIES 16384 /* reduced-pattern bitmap limit */
+
+/* out[v] = q[b] + r0 q[b+1] + r1 q[b+2] + r2 q[b+3] with b = 4 body[v]:
+ * _sync_affine_vertices (42-48) with q, _affine_vertex_direction (51-57) with dx. */
+int ipcb_abd_map(int fp64, int n_verts, const void* q, const void* rest, const int* body, void* out, ipcb_stream s);
+/* q = q_start - alpha dq (the copy + _affine_add_step of line_search, 60-63, 623-627) */
+int ipcb_abd_step_from(int fp64, int n, const void* q_start, const void* dq, double alpha, void* q, ipcb_stream s);
+/* _prepare_tilde (66-79); gravity: host double[3]; motor_omega scalar[3 nb]
+ * and motor_enabled int32[nb] may be null (no motors). */
+int ipcb_abd_prepare_tilde(const ipcb_abd* abd, double h, const double* gravity, const void* motor_omega,
+                           const int* motor_enabled, ipcb_stream s);
+/* _update_affine_velocity (82-86): qdot = (q - q0) / h, q0 = q */
+int ipcb_abd_update_velocity(const ipcb_abd* abd, double h, ipcb_stream s);
+/* _assemble_body_system (88-141) in the reference layout: 16 triplets per
+ * body at b*16 + i*4 + j (rows/cols int32, vals scalar[9]) and the body
+ * gradient rows [4 nb][3]. */
+int ipcb_abd_body_system(const ipcb_abd* abd, double h2, int* rows, int* cols, void* vals, void* gradient,
+                         ipcb_stream s);
+/* _body_energy (193-217): energies[0] += inertia, energies[1] += orthogonality (double) */
+int ipcb_abd_body_energy(const ipcb_abd* abd, double h2, double* energies, ipcb_stream s);
+/* _reduce_contact_force (144-157): reduced_force[4 nb][3] += J^T f (bodies not fixed) */
+int ipcb_abd_reduce_force(const ipcb_abd* abd, int n_verts, const void* vertex_force, const void* rest,
+                          const int* body, void* reduced_force, ipcb_stream s);
+/* _add_contact_gradient (160-163): gradient -= h2 * force, n scalars */
+int ipcb_abd_add_contact_gradient(int fp64, int n, void* gradient, const void* force, double h2, ipcb_stream s);
+/* _reduce_contact_hessian (166-190): 16 triplets per source block at
+ * src*16 + a*4 + c, zero when either body is fixed. */
+int ipcb_abd_reduce_hessian(const ipcb_abd* abd, int n_src, const int* src_rows, const int* src_cols,
+                            const void* src_vals, const void* rest, const int* body, double scale, int* dst_rows,
+                            int* dst_cols, void* dst_vals, ipcb_stream s);
+/* Block pattern of the reduced matrix without the 16x fan-out: every body's
+ * diagonal 4x4 block plus the 4x4 blocks of each body pair joined by a
+ * contact record (records as ipcb_contact_hessian writes them, 16 triplets
+ * each; block_mask optional; pairs with a fixed body are left out).
+ * body_off int32[nb+1], body_cols int32[pair_capacity] (the sorted body
+ * neighbours, diagonal included), offsets int32[4 nb + 1], columns
+ * int32[16 pair_capacity]; *nnz (device) = 16 * body_off[nb].
+ * IPCB_STATUS_PATTERN when body_off[nb] > pair_capacity (grow, rerun) or a
+ * record spans more than two bodies.  ws: ipcb_abd_pattern_workspace bytes. */
+size_t ipcb_abd_pattern_workspace(int n_bodies);
+int ipcb_abd_pattern(int n_bodies, const int* fixed, const int* body, int n_records, const int* trows,
+                     const int* tcols, const unsigned short* block_mask, int* body_off, int* body_cols,
+                     int pair_capacity, int* offsets, int* columns, int* nnz, int* status, void* ws, size_t ws_bytes,
+                     ipcb_stream s);
+/* The reduced Newton system of AffineBodyDynamics.compute_A (427-505) into
+ * the pattern of ipcb_abd_pattern: values (capacity blocks) = body blocks +
+ * h2 * J^T H_contact J, gradient [4 nb][3] = body gradient - h2 * J^T f.
+ * Records [0, n_ee) are EE records (a1 a2 on one body, b1 b2 on one body),
+ * the rest PT (the point on one body, the triangle on one body).
+ * vertex_force (scalar[3 n_verts], may be null) with reduced_force
+ * (scalar[12 nb], overwritten with J^T f). */
+int ipcb_abd_assemble(const ipcb_abd* abd, double h2, int n_records, int n_ee, const int* trows, const int* tcols,
+                      const void* tvals, const unsigned short* block_mask, const void* rest, const int* body,
+                      const int* body_off, const int* body_cols, const int* offsets, const int* nnz, int capacity,
+                      void* values, void* gradient, int n_verts, const void* vertex_force, void* reduced_force,
+                      int* status, ipcb_stream s);
+
 /* ---- BSR assembly (warp.sparse.bsr_from_triplets, dynamic_contacts.py:290-297) ----
  * Canonical 3x3-block CSR from triplets: sort by (row, col), sum duplicates,
  * drop triplets whose 9 values are all zero.  offsets int32[nrow+1],

@@ -37,6 +37,11 @@ class Bodies(ctypes.Structure):
                 ("max_edges", c_int), ("max_tris", c_int), ("max_verts", c_int), ("frames", P), ("motion", P)]
 
 
+class Abd(ctypes.Structure):
+    _fields_ = [("n_bodies", c_int), ("fp64", c_int), ("q", P), ("q0", P), ("q_tilde", P), ("qdot", P), ("dx", P),
+                ("mass", P), ("volume", P), ("stiffness", P), ("fixed", P)]
+
+
 class Graph(ctypes.Structure):
     _fields_ = [("n", c_int), ("nnz", c_int), ("n_lower", c_int), ("offsets", P), ("columns", P), ("rows", P),
                 ("rev", P), ("diag", P), ("lower", P)]
@@ -60,6 +65,7 @@ class Pcg(ctypes.Structure):
 
 SP, CP, BP = ctypes.POINTER(Soup), ctypes.POINTER(Contacts), ctypes.POINTER(Lbvh)
 BD = ctypes.POINTER(Bodies)
+AB = ctypes.POINTER(Abd)
 GP, TP = ctypes.POINTER(Graph), ctypes.POINTER(Tape)
 
 # name -> (restype, argtypes); every symbol here is declared in include/ipcb.h
@@ -109,6 +115,19 @@ SIGNATURES = {
     "ipcb_pcg_iterate": (c_int, [ctypes.POINTER(Pcg), c_int, P]),
     "ipcb_block_jacobi": (c_int, [c_int, P, P, P, P, c_int, P, P, P]),
     "ipcb_fsai_mirror": (c_int, [GP, P, P, P]),
+    "ipcb_abd_map": (c_int, [c_int, c_int, P, P, P, P, P]),
+    "ipcb_abd_step_from": (c_int, [c_int, c_int, P, P, c_double, P, P]),
+    "ipcb_abd_prepare_tilde": (c_int, [AB, c_double, P, P, P, P]),
+    "ipcb_abd_update_velocity": (c_int, [AB, c_double, P]),
+    "ipcb_abd_body_system": (c_int, [AB, c_double, P, P, P, P, P]),
+    "ipcb_abd_body_energy": (c_int, [AB, c_double, P, P]),
+    "ipcb_abd_reduce_force": (c_int, [AB, c_int, P, P, P, P, P]),
+    "ipcb_abd_add_contact_gradient": (c_int, [c_int, c_int, P, P, c_double, P]),
+    "ipcb_abd_reduce_hessian": (c_int, [AB, c_int, P, P, P, P, P, c_double, P, P, P, P]),
+    "ipcb_abd_pattern_workspace": (c_size_t, [c_int]),
+    "ipcb_abd_pattern": (c_int, [c_int, P, P, c_int, P, P, P, P, P, c_int, P, P, P, P, P, c_size_t, P]),
+    "ipcb_abd_assemble": (c_int, [AB, c_double, c_int, c_int, P, P, P, P, P, P, P, P, P, P, c_int, P, P, c_int, P, P,
+                                  P, P]),
     "ipcb_body_pairs": (c_int, [BD, c_int, P, c_double, P, c_int, P, P, P]),
     "ipcb_fixed_dcd_ee": (c_int, [SP, P, BD, P, c_int, c_float, CP, P, P]),
     "ipcb_fixed_dcd_pt": (c_int, [SP, P, BD, P, c_int, c_float, CP, P, P]),

@@ -247,3 +247,83 @@ def twist_targets(sc: Scene, omega: float):
         return tgt
 
     return lo | hi, at
+
+
+# ------------------------------------------------------------ affine bodies
+def icosphere(subdiv: int = 2, radius: float = 0.5):
+    """Closed triangle sphere (outward faces): a regular icosahedron whose
+    faces are split in four ``subdiv`` times, vertices pushed to the sphere.
+    subdiv 4 gives 2562 vertices / 5120 triangles."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    verts = [np.asarray(p, np.float64) / np.linalg.norm(p) for p in v]
+    faces = [tuple(x) for x in f]
+    for _ in range(subdiv):
+        mid = {}
+
+        def midpoint(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in mid:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                mid[key] = len(verts) - 1
+            return mid[key]
+
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = midpoint(a, b), midpoint(b, c), midpoint(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    return radius * np.array(verts), np.array(faces, dtype=np.int64)
+
+
+def box_surface(n=(4, 4, 4), size=(1.0, 1.0, 1.0)):
+    """Closed triangulated box surface (outward faces, surface vertices only),
+    n cells per side, corner at the origin."""
+    m = hex_grid_tets(*n, size=size)
+    tris = m.triangles
+    used = np.unique(tris)
+    remap = np.full(m.x.shape[0], -1, np.int64)
+    remap[used] = np.arange(len(used))
+    return m.x[used].copy(), remap[tris]
+
+
+def transform(rotation_deg=(0.0, 0.0, 0.0), position=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """4x4 rigid transform: rotations about x, then y, then z (degrees), then
+    the translation."""
+    rx, ry, rz = np.radians(rotation_deg)
+    cx, sx, cy, sy, cz, sz = np.cos(rx), np.sin(rx), np.cos(ry), np.sin(ry), np.cos(rz), np.sin(rz)
+    Rx = np.array([[1, 0, 0], [0, cx, -sx], [0, sx, cx]])
+    Ry = np.array([[cy, 0, sy], [0, 1, 0], [-sy, 0, cy]])
+    Rz = np.array([[cz, -sz, 0], [sz, cz, 0], [0, 0, 1]])
+    T = np.eye(4)
+    T[:3, :3] = Rz @ Ry @ Rx
+    T[:3, 3] = position
+    return T
+
+
+def abd_balls(n_side: int = 2, layers: int = 1, subdiv: int = 2, radius: float = 0.5, gap: float = 2e-3,
+              drop: float = 1e-3, seed: int = 0, ground_cells: int = 8) -> dict:
+    """Affine-body scene: ``n_side`` x ``n_side`` x ``layers`` icospheres in a
+    stacked grid (neighbours ``gap`` apart, randomly turned), the lowest
+    layer ``drop`` above a fixed box slab.  Keyword arguments of
+    :class:`AffineBodyDynamics` (meshes, transforms, fixed_bodies, gravity)."""
+    rng = np.random.default_rng(seed)
+    ball = icosphere(subdiv, radius)
+    pitch = 2.0 * radius + gap
+    meshes, transforms = [], []
+    for k in range(layers):
+        for i in range(n_side):
+            for j in range(n_side):
+                meshes.append(ball)
+                pos = (i * pitch, radius + drop + k * pitch, j * pitch)
+                transforms.append(transform(rng.uniform(0, 360, 3), pos))
+    width = n_side * pitch + 2.0 * radius
+    slab = box_surface((ground_cells, 1, ground_cells), (width, 0.2, width))
+    meshes.append(slab)
+    transforms.append(transform(position=(-1.5 * radius, -0.2, -1.5 * radius)))
+    return dict(meshes=meshes, transforms=transforms, fixed_bodies=[len(meshes) - 1], gravity=(0.0, -9.8, 0.0))
