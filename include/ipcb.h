@@ -334,6 +334,58 @@ int ipcb_abd_assemble(const ipcb_abd* abd, double h2, int n_records, int n_ee, c
                       void* values, void* gradient, int n_verts, const void* vertex_force, void* reduced_force,
                       int* status, ipcb_stream s);
 
+/* ---- Batched Newton terms and fixed-pattern assembly (time_integrator_base.py:403-426,
+ * dynamic_contacts.py:275-297, fem/fem.py:139-203) ----
+ * One persistent launch over all per-iteration terms: the EE records, the PT
+ * records (counts read on the device: min(*cnt, capacity)) and the tets, in
+ * that order, each with the outputs of ipcb_contact_hessian (EE at 0, PT at
+ * offset n_ee) and ipcb_tet_hessian (t_rows/t_cols may be null); forces add
+ * into `force`.  Work is taken from *queue (zeroed by the call) in tiles of
+ * `tile` items per warp; blocks x threads (<= 128, multiple of 32) is the
+ * persistent grid. */
+typedef struct {
+  int fp64;
+  const void* x;
+  const void* xcs;
+  ipcb_contacts ee;
+  ipcb_contacts pt;
+  double kappa;
+  int* c_rows;
+  int* c_cols;
+  void* c_vals;
+  unsigned short* c_mask;
+  int material;
+  const int* tets;
+  int n_tets;
+  const void* Bm;
+  const void* W;
+  double mu, lam;
+  int* t_rows;
+  int* t_cols;
+  void* t_vals;
+  void* force;
+  int* queue;
+} ipcb_terms;
+int ipcb_terms_launch(const ipcb_terms* terms, int blocks, int threads, int tile, ipcb_stream s);
+/* slots[i] = position of block (rows[i], cols[i]) in a BSR pattern, -1 if absent */
+int ipcb_bsr_slots(int nrow, const int* offsets, const int* columns, int n, const int* rows, const int* cols,
+                   int* slots, ipcb_stream s);
+/* Union of two BSR patterns with the same rows: c_off[nrow+1], and per slot
+ * c_rows, c_cols, src_a / src_b (the slot in a / b, -1 if absent); *c_nnz
+ * (device).  IPCB_STATUS_PATTERN when the union exceeds capacity. */
+size_t ipcb_bsr_union_workspace(int nrow);
+int ipcb_bsr_union(int nrow, const int* a_off, const int* a_cols, const int* b_off, const int* b_cols, int* c_off,
+                   int* c_rows, int* c_cols, int* src_a, int* src_b, int capacity, int* c_nnz, int* status, void* ws,
+                   size_t ws_bytes, ipcb_stream s);
+/* Values of the union: slot p = tet_scale * sum of the tet blocks gathered
+ * through gather_off/gather_idx (a CSR from each slot of pattern a to the
+ * triplets landing on it) + diag[row] I on the diagonal (diag may be null)
+ * + contact_scale * contact_vals[src_b[p]]. */
+int ipcb_newton_values(int fp64, const int* nnz, int capacity, const int* c_rows, const int* c_cols, const int* src_a,
+                       const int* src_b, const int* gather_off, const int* gather_idx, const void* tet_vals,
+                       double tet_scale, const void* diag, const void* contact_vals, double contact_scale,
+                       void* values, ipcb_stream s);
+
 /* ---- BSR assembly (warp.sparse.bsr_from_triplets, dynamic_contacts.py:290-297) ----
  * Canonical 3x3-block CSR from triplets: sort by (row, col), sum duplicates,
  * drop triplets whose 9 values are all zero.  offsets int32[nrow+1],

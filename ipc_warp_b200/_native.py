@@ -37,6 +37,13 @@ class Bodies(ctypes.Structure):
                 ("max_edges", c_int), ("max_tris", c_int), ("max_verts", c_int), ("frames", P), ("motion", P)]
 
 
+class Terms(ctypes.Structure):
+    _fields_ = [("fp64", c_int), ("x", P), ("xcs", P), ("ee", Contacts), ("pt", Contacts), ("kappa", c_double),
+                ("c_rows", P), ("c_cols", P), ("c_vals", P), ("c_mask", P), ("material", c_int), ("tets", P),
+                ("n_tets", c_int), ("Bm", P), ("W", P), ("mu", c_double), ("lam", c_double), ("t_rows", P),
+                ("t_cols", P), ("t_vals", P), ("force", P), ("queue", P)]
+
+
 class Abd(ctypes.Structure):
     _fields_ = [("n_bodies", c_int), ("fp64", c_int), ("q", P), ("q0", P), ("q_tilde", P), ("qdot", P), ("dx", P),
                 ("mass", P), ("volume", P), ("stiffness", P), ("fixed", P)]
@@ -115,6 +122,11 @@ SIGNATURES = {
     "ipcb_pcg_iterate": (c_int, [ctypes.POINTER(Pcg), c_int, P]),
     "ipcb_block_jacobi": (c_int, [c_int, P, P, P, P, c_int, P, P, P]),
     "ipcb_fsai_mirror": (c_int, [GP, P, P, P]),
+    "ipcb_terms_launch": (c_int, [ctypes.POINTER(Terms), c_int, c_int, c_int, P]),
+    "ipcb_bsr_slots": (c_int, [c_int, P, P, c_int, P, P, P, P]),
+    "ipcb_bsr_union_workspace": (c_size_t, [c_int]),
+    "ipcb_bsr_union": (c_int, [c_int, P, P, P, P, P, P, P, P, P, c_int, P, P, P, c_size_t, P]),
+    "ipcb_newton_values": (c_int, [c_int, P, c_int, P, P, P, P, P, P, P, c_double, P, P, c_double, P, P]),
     "ipcb_abd_map": (c_int, [c_int, c_int, P, P, P, P, P]),
     "ipcb_abd_step_from": (c_int, [c_int, c_int, P, P, c_double, P, P]),
     "ipcb_abd_prepare_tilde": (c_int, [AB, c_double, P, P, P, P]),

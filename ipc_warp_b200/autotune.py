@@ -1,0 +1,76 @@
+"""Launch-configuration autotuner: times every candidate configuration of a
+kernel once per workload key with CUDA events and keeps the fastest.
+
+``run(cfg)`` launches the kernel with one configuration; ``reset()`` restores
+what a launch accumulates (e.g. zeroes a force array) and is called before
+every timed launch and once more at the end, so the caller relaunches with
+the chosen configuration on clean state.  Results are cached per key in
+memory and, when the environment variable ``IPCB_AUTOTUNE_CACHE`` names a
+JSON file, across processes.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import torch
+
+
+class Autotuner:
+    def __init__(self, name: str, candidates: list[tuple], reps: int = 2):
+        self.name = name
+        self.candidates = list(candidates)
+        self.reps = reps
+        self.best: dict[str, tuple] = {}
+        self.timings: dict[str, dict] = {}
+        self._path = os.environ.get("IPCB_AUTOTUNE_CACHE")
+        if self._path and os.path.exists(self._path):
+            try:
+                with open(self._path) as f:
+                    data = json.load(f).get(name, {})
+                self.best.update({k: tuple(v) for k, v in data.items()})
+            except (OSError, ValueError):
+                pass
+
+    def pick(self, key, run, reset) -> tuple:
+        key = str(key)
+        if key in self.best:
+            return self.best[key]
+        times = {}
+        for cfg in self.candidates:
+            reset()
+            run(cfg)  # warm-up (first launch of this configuration)
+            best = float("inf")
+            for _ in range(self.reps):
+                reset()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                run(cfg)
+                b.record()
+                b.synchronize()
+                best = min(best, a.elapsed_time(b))
+            times[cfg] = best
+        reset()
+        choice = min(times, key=times.get)
+        self.best[key] = choice
+        self.timings[key] = {str(k): v for k, v in times.items()}
+        if self._path:
+            self._save()
+        return choice
+
+    def _save(self):
+        data = {}
+        if os.path.exists(self._path):
+            try:
+                with open(self._path) as f:
+                    data = json.load(f)
+            except (OSError, ValueError):
+                data = {}
+        data[self.name] = {k: list(v) for k, v in self.best.items()}
+        with open(self._path, "w") as f:
+            json.dump(data, f, indent=1)
+
+
+def bucket(n: int) -> int:
+    """Power-of-two bucket of a work size (the autotuner key)."""
+    return 1 << max(int(n) - 1, 0).bit_length()

@@ -68,27 +68,51 @@ def init_params(seed: int = 0) -> np.ndarray:
     return flatten(p)
 
 
+class Pool:
+    """Device buffers reused by name across factor builds, so that a build in
+    the Newton loop allocates nothing once the sizes have been seen (a new
+    allocation can synchronise the device) and the PCG's captured graph keeps
+    its pointers.  A buffer handed out again invalidates its previous user."""
+
+    def __init__(self):
+        self._bufs = {}
+
+    def get(self, name: str, shape, dtype, device) -> torch.Tensor:
+        shape = tuple(int(v) for v in shape)
+        t = self._bufs.get(name)
+        if t is None or t.dtype != dtype or t.device != torch.device(device) or t.numel() < math.prod(shape):
+            t = torch.empty(max(math.prod(shape), 1), dtype=dtype, device=device)
+            self._bufs[name] = t
+        return t[:math.prod(shape)].view(shape)
+
+
+def _alloc(pool: Pool | None, name: str, shape, dtype, device) -> torch.Tensor:
+    if pool is None:
+        return torch.empty(shape, dtype=dtype, device=device)
+    return pool.get(name, shape, dtype, device)
+
+
 class Graph:
     """rows / rev / diag / lower of a canonical BSR pattern (device)."""
 
-    def __init__(self, A: BsrMatrix, nnz: int | None = None):
+    def __init__(self, A: BsrMatrix, nnz: int | None = None, pool: Pool | None = None):
         self.n = A.nrow
         self.nnz = A.nnz_sync() if nnz is None else int(nnz)
         if (self.nnz + self.n) % 2:
             raise ValueError("pattern is not structurally symmetric")
         self.n_lower = (self.nnz + self.n) // 2
         dev = A.device
-        i32 = dict(dtype=torch.int32, device=dev)
         self.offsets = A.offsets
         self.columns = A.columns
-        self.rows = torch.empty(self.nnz, **i32)
-        self.rev = torch.empty(self.nnz, **i32)
-        self.diag = torch.empty(self.n, **i32)
-        self.lower = torch.empty(self.n_lower, **i32)
+        self.rows = _alloc(pool, "g.rows", (self.nnz,), torch.int32, dev)
+        self.rev = _alloc(pool, "g.rev", (self.nnz,), torch.int32, dev)
+        self.diag = _alloc(pool, "g.diag", (self.n,), torch.int32, dev)
+        self.lower = _alloc(pool, "g.lower", (self.n_lower,), torch.int32, dev)
+        i32 = dict(dtype=torch.int32, device=dev)
         self.c = N.Graph(self.n, self.nnz, self.n_lower, N.ptr(self.offsets), N.ptr(self.columns), N.ptr(self.rows),
                          N.ptr(self.rev), N.ptr(self.diag), N.ptr(self.lower))
         status = torch.zeros(1, **i32)
-        ws = torch.empty(N.size("ipcb_mpnn_graph_workspace", self.n), dtype=torch.uint8, device=dev)
+        ws = _alloc(pool, "g.ws", (N.size("ipcb_mpnn_graph_workspace", self.n),), torch.uint8, dev)
         N.call("ipcb_mpnn_graph", ctypes.byref(self.c), N.ptr(status), N.ptr(ws), ws.numel(), N.stream_handle())
         if int(status.item()) & 16:
             raise ValueError("pattern is not symmetric or lacks a diagonal block")
@@ -127,49 +151,53 @@ class System:
     y: torch.Tensor      # bf16 (nnz, 16)
 
     @staticmethod
-    def from_bsr(A: BsrMatrix, graph: Graph | None = None) -> "System":
-        g = graph if graph is not None else Graph(A)
+    def from_bsr(A: BsrMatrix, graph: Graph | None = None, pool: Pool | None = None,
+                 status: torch.Tensor | None = None) -> "System":
+        """With ``status`` given, the feature status is ORed into it and not
+        read here (the caller reads it once)."""
+        g = graph if graph is not None else Graph(A, pool=pool)
         dev = A.device
-        f32 = dict(dtype=torch.float32, device=dev)
-        scale = torch.empty((g.n, 3), **f32)
-        ahat = torch.empty((g.nnz, 9), **f32)
-        x = torch.empty((g.n, IN_DIM), dtype=torch.bfloat16, device=dev)
-        y = torch.empty((g.nnz, IN_DIM), dtype=torch.bfloat16, device=dev)
-        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        scale = _alloc(pool, "s.scale", (g.n, 3), torch.float32, dev)
+        ahat = _alloc(pool, "s.ahat", (g.nnz, 9), torch.float32, dev)
+        x = _alloc(pool, "s.x", (g.n, IN_DIM), torch.bfloat16, dev)
+        y = _alloc(pool, "s.y", (g.nnz, IN_DIM), torch.bfloat16, dev)
+        st = torch.zeros(1, dtype=torch.int32, device=dev) if status is None else status
         N.call("ipcb_mpnn_features", ctypes.byref(g.c), int(A.dtype == torch.float64), N.ptr(A.values), N.ptr(scale),
-               N.ptr(ahat), N.ptr(x), N.ptr(y), N.ptr(status), N.stream_handle())
-        if int(status.item()) & 16:
+               N.ptr(ahat), N.ptr(x), N.ptr(y), N.ptr(st), N.stream_handle())
+        if status is None and int(st.item()) & 16:
             raise ValueError("non-positive diagonal entry")
         return System(A, g, scale, ahat, x, y)
 
 
 class _Tape:
-    def __init__(self, g: Graph, training: bool, dev):
-        b = dict(dtype=torch.bfloat16, device=dev)
+    def __init__(self, g: Graph, training: bool, dev, pool: Pool | None = None):
+        bf = torch.bfloat16
         nh = LAYERS + 1 if training else 2
-        self.h = torch.empty((nh, g.n, WIDTH), **b)
-        self.e = torch.empty((nh, g.nnz, WIDTH), **b)
-        self.m = torch.empty((LAYERS if training else 1, g.nnz, WIDTH), **b)
-        self.a = torch.empty((LAYERS if training else 1, g.n, WIDTH), **b)
-        self.u = torch.empty((LAYERS, g.n, WIDTH), **b) if training else None
-        self.proj = torch.empty((g.n, 2 * WIDTH), dtype=torch.float32, device=dev)
+        self.h = _alloc(pool, "t.h", (nh, g.n, WIDTH), bf, dev)
+        self.e = _alloc(pool, "t.e", (nh, g.nnz, WIDTH), bf, dev)
+        self.m = _alloc(pool, "t.m", (LAYERS if training else 1, g.nnz, WIDTH), bf, dev)
+        self.a = _alloc(pool, "t.a", (LAYERS if training else 1, g.n, WIDTH), bf, dev)
+        self.u = _alloc(pool, "t.u", (LAYERS, g.n, WIDTH), bf, dev) if training else None
+        self.proj = _alloc(pool, "t.proj", (g.n, 2 * WIDTH), torch.float32, dev)
         opt = lambda t: N.ptr(t) if t is not None else None
         self.c = N.Tape(N.ptr(self.h), N.ptr(self.e), N.ptr(self.m), N.ptr(self.a), opt(self.u), N.ptr(self.proj),
                         int(training))
 
 
-def forward(net: Net, sysm: System, training: bool = False):
+def forward(net: Net, sysm: System, training: bool = False, pool: Pool | None = None,
+            status: torch.Tensor | None = None):
     """Row directions H (float32 (nnz, 3, 3), valid on the lower blocks) and
-    the tape."""
+    the tape.  With ``status`` given, the kernel status is ORed into it and
+    not read here."""
     g = sysm.graph
     dev = sysm.A.device
-    tape = _Tape(g, training, dev)
-    H = torch.zeros((g.nnz, 3, 3), dtype=torch.float32, device=dev)
-    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    tape = _Tape(g, training, dev, pool)
+    H = _alloc(pool, "H", (g.nnz, 3, 3), torch.float32, dev).zero_()
+    st = torch.zeros(1, dtype=torch.int32, device=dev) if status is None else status
     N.call("ipcb_mpnn_forward", ctypes.byref(g.c), N.ptr(net.packed), N.ptr(net.params), N.ptr(sysm.ahat),
-           N.ptr(sysm.x), N.ptr(sysm.y), ctypes.byref(tape.c), N.ptr(H), N.ptr(status), N.stream_handle())
-    if int(status.item()):
-        raise RuntimeError(f"mpnn forward status {int(status.item())}")
+           N.ptr(sysm.x), N.ptr(sysm.y), ctypes.byref(tape.c), N.ptr(H), N.ptr(st), N.stream_handle())
+    if status is None and int(st.item()):
+        raise RuntimeError(f"mpnn forward status {int(st.item())}")
     return H, tape
 
 
@@ -182,18 +210,23 @@ class Normalized:
     status: int
 
 
-def normalize(sysm: System, H: torch.Tensor) -> Normalized:
-    """Exact row normalisation G^_i = chol(M_i)^-1 H_i and the FSAI loss."""
+def normalize(sysm: System, H: torch.Tensor, pool: Pool | None = None,
+              status: torch.Tensor | None = None) -> Normalized:
+    """Exact row normalisation G^_i = chol(M_i)^-1 H_i and the FSAI loss.
+    With ``status`` given, nothing is read back (loss and status are left
+    on the device: ``loss`` is then NaN)."""
     g = sysm.graph
     dev = H.device
-    G = torch.zeros_like(H)
-    T = torch.empty((g.nnz, 9), dtype=torch.float32, device=dev)
-    minv = torch.empty((g.n, 9), dtype=torch.float32, device=dev)
+    G = _alloc(pool, "G", tuple(H.shape), torch.float32, dev).zero_()
+    T = _alloc(pool, "T", (g.nnz, 9), torch.float32, dev)
+    minv = _alloc(pool, "minv", (g.n, 9), torch.float32, dev)
     acc = torch.zeros(1, dtype=torch.float64, device=dev)
-    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    st = torch.zeros(1, dtype=torch.int32, device=dev) if status is None else status
     N.call("ipcb_fsai_normalize", ctypes.byref(g.c), N.ptr(sysm.ahat), N.ptr(H), N.ptr(T), N.ptr(minv), N.ptr(G),
-           N.ptr(acc), N.ptr(status), N.stream_handle())
-    return Normalized(G, T, minv, float(acc.item()) / (3 * g.n), int(status.item()))
+           N.ptr(acc), N.ptr(st), N.stream_handle())
+    if status is not None:
+        return Normalized(G, T, minv, float("nan"), 0)
+    return Normalized(G, T, minv, float(acc.item()) / (3 * g.n), int(st.item()))
 
 
 def loss_grad(sysm: System, nz: Normalized, weight: float = 1.0) -> torch.Tensor:
@@ -250,21 +283,36 @@ class LearnedFactor:
     (bf16 blocks, upper slots mirrored)."""
     kind = 1
 
-    def __init__(self, net: Net, A: BsrMatrix):
+    def __init__(self, net: Net, A: BsrMatrix, pool: Pool | None = None):
+        """``pool``: buffers shared with earlier factors (which this build
+        invalidates); the build then allocates nothing once sizes repeat and
+        reads the device twice (the matrix size and one status word)."""
         # own copy of the pattern: the factor may outlive this matrix (reuse
         # across Newton iterations), whose buffers a later assembly overwrites
         nnz = A.nnz_sync()
-        B = BsrMatrix(A.nrow, A.ncol, nnz, A.dtype, A.device)
+        dev = A.device
+        B = BsrMatrix.__new__(BsrMatrix)
+        B.nrow, B.ncol, B.dtype, B.device = A.nrow, A.ncol, A.dtype, dev
+        B.offsets = _alloc(pool, "B.offsets", (A.nrow + 1,), torch.int32, dev)
+        B.columns = _alloc(pool, "B.columns", (max(nnz, 1),), torch.int32, dev)
+        B.values = _alloc(pool, "B.values", (max(nnz, 1), 3, 3), A.dtype, dev)
+        B.nnz_dev = _alloc(pool, "B.nnz", (1,), torch.int32, dev)
         B.offsets.copy_(A.offsets)
         B.columns[:nnz].copy_(A.columns[:nnz])
         B.values[:nnz].copy_(A.values[:nnz])
         B.nnz_dev.copy_(A.nnz_dev)
-        self.sysm = System.from_bsr(B)
-        H, _ = forward(net, self.sysm)
-        self.G = normalize(self.sysm, H).G
-        self.gh = torch.empty((self.sysm.graph.nnz, 9), dtype=torch.bfloat16, device=A.device)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.sysm = System.from_bsr(B, Graph(B, nnz=nnz, pool=pool), pool=pool, status=status)
+        H, _ = forward(net, self.sysm, pool=pool, status=status)
+        self.G = normalize(self.sysm, H, pool=pool, status=status).G
+        self.gh = _alloc(pool, "gh", (self.sysm.graph.nnz, 9), torch.bfloat16, dev)
         N.call("ipcb_fsai_mirror", ctypes.byref(self.sysm.graph.c), N.ptr(self.G), N.ptr(self.gh),
                N.stream_handle())
+        st = int(status.item())
+        if st & 16:
+            raise ValueError("non-positive diagonal entry in the Newton matrix")
+        if st:
+            raise RuntimeError(f"learned factor status {st:#x}")
 
     def fill(self, P):
         g = self.sysm.graph

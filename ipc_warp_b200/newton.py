@@ -24,7 +24,8 @@ import torch
 
 from . import _native as N
 from . import contact as contact_mod
-from .bsr import BsrMatrix, Triplets, bsr_from_triplets, bsr_mv
+from .autotune import Autotuner, bucket
+from .bsr import BsrMatrix, Triplets, bsr_from_triplets, bsr_mv, contact_bsr
 from .contact import Soup
 from .dynamic_contacts import ContactBarrierMixin
 
@@ -184,8 +185,15 @@ class FEMContactSolver(ContactBarrierMixin):
                  attachment_stiffness: float = 1e11, dtype=torch.float32, device="cuda", vel_tol: float = 5e-2,
                  max_newton: int = 100, tol: float = 1e-4, maxiter: int = 200, exclude_same_body: bool = False,
                  linear_solver: str = "pcg", direct_fallback: bool = True, preconditioner: str = "jacobi",
-                 precond_refresh: int = 1):
+                 precond_refresh: int = 1, assembly: str = "queue"):
         self.h = float(h)
+        if assembly not in ("queue", "generic"):
+            raise ValueError(f"unknown assembly {assembly!r}")
+        # "queue": one persistent launch for contact + tet terms and the
+        # fixed-pattern assembly (csrc/terms.cu); "generic": per-term kernels
+        # and a sort-based assembly of all triplets
+        self.assembly = assembly
+        self._static = None
         self.material = MATERIALS[material]
         self.mu, self.lam = lame(E, nu)
         self.dtype = dtype
@@ -240,7 +248,10 @@ class FEMContactSolver(ContactBarrierMixin):
 
             net = Net.load(DEFAULT_WEIGHTS, device=self.device)
             self.precond_factory = LearnedPreconditioner(net)
-            self.device_precond = lambda A: LearnedFactor(net, A)
+            from .learned import Pool
+
+            self._factor_pool = Pool()
+            self.device_precond = lambda A: LearnedFactor(net, A, pool=self._factor_pool)
         else:
             raise ValueError(f"unknown preconditioner {preconditioner!r}")
         self.host_pcg = False
@@ -290,6 +301,12 @@ class FEMContactSolver(ContactBarrierMixin):
     # ------------------------------------------------------------ system
     def compute_A(self) -> BsrMatrix:
         """time_integrator_base.py:406-426 + dynamic_contacts.py:275-297."""
+        if self.assembly == "queue":
+            return self._compute_A_queue()
+        return self._compute_A_generic()
+
+    def _compute_A_generic(self) -> BsrMatrix:
+        """Per-term kernels, then one sort-based assembly of every triplet."""
         h2 = self.h * self.h
         V = self.soup.n_verts
         self.b.zero_()
@@ -310,6 +327,100 @@ class FEMContactSolver(ContactBarrierMixin):
         vals = torch.cat([diag, t.vals * h2, ct.vals[:nc] * h2])
         self.A = bsr_from_triplets(V, V, rows, cols, vals, out=getattr(self, "A", None))
         return self.A
+
+    # ------------------------------------------------ work-queue assembly
+    def _static_pattern(self):
+        """Pattern of M + h^2 K (diagonal + mesh connectivity), built once,
+        with the map from every slot to the tet blocks that land on it."""
+        dev = self.device
+        V, nt = self.soup.n_verts, self.n_tets
+        T = self.tets
+        rows_t = T.repeat_interleave(4, dim=1).reshape(-1).contiguous()
+        cols_t = T.repeat(1, 4).reshape(-1).contiguous()
+        idx = torch.arange(V, dtype=torch.int32, device=dev)
+        rows = torch.cat([idx, rows_t])
+        cols = torch.cat([idx, cols_t])
+        ones = torch.ones((rows.numel(), 3, 3), dtype=self.dtype, device=dev)
+        S = bsr_from_triplets(V, V, rows, cols, ones)
+        nnz = int(S.nnz_dev.item())
+        slots = torch.empty(16 * nt, dtype=torch.int32, device=dev)
+        N.call("ipcb_bsr_slots", V, N.ptr(S.offsets), N.ptr(S.columns), 16 * nt, N.ptr(rows_t), N.ptr(cols_t),
+               N.ptr(slots), N.stream_handle())
+        sl = slots.long()
+        g_idx = torch.argsort(sl, stable=True).to(torch.int32)
+        g_off = torch.zeros(nnz + 1, dtype=torch.int32, device=dev)
+        g_off[1:] = torch.cumsum(torch.bincount(sl, minlength=nnz), 0).to(torch.int32)
+        h2 = self.h * self.h
+        diag = (self.mass + (h2 * self.k_att) * self.fixed.double()).to(self.dtype)
+        self._static = dict(S=S, nnz=nnz, g_off=g_off, g_idx=g_idx, diag=diag, rows_t=rows_t, cols_t=cols_t,
+                            tet_vals=torch.empty((16 * nt, 3, 3), dtype=self.dtype, device=dev),
+                            queue=torch.zeros(1, dtype=torch.int32, device=dev),
+                            status=torch.zeros(1, dtype=torch.int32, device=dev),
+                            ws=torch.empty(N.size("ipcb_bsr_union_workspace", V), dtype=torch.uint8, device=dev))
+        n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+        self._n_sm = n_sm
+        cands = [(bps, th, tile) for (bps, th) in ((1, 128), (2, 128), (2, 64), (4, 64)) for tile in (32, 64, 128, 256)]
+        self._tuner = Autotuner("terms", cands)
+
+    def _launch_terms(self, cfg, Tc):
+        bps, threads, tile = cfg
+        N.call("ipcb_terms_launch", ctypes.byref(Tc), bps * self._n_sm, threads, tile, N.stream_handle())
+
+    def _compute_A_queue(self) -> BsrMatrix:
+        """Contact detection, then one persistent launch for the contact
+        records and the tets (ipcb_terms_launch), the contact BSR, and the
+        union with the fixed elastic pattern with gathered values."""
+        if self._static is None:
+            self._static_pattern()
+        st = self._static
+        h2 = self.h * self.h
+        V = self.soup.n_verts
+        self.b.zero_()
+        with self.profile_timer("detect collision"):
+            self.detect_collision()
+        n_ee, n_pt = self.n_contacts, self.n_contacts_pt
+        nc = 16 * (n_ee + n_pt)
+        if getattr(self, "collision_triplets", None) is None or self.collision_triplets.rows.shape[0] < nc:
+            self.collision_triplets = Triplets.zeros(max(nc, 16), self.dtype, self.device)
+        t = self.collision_triplets
+        Tc = N.Terms(int(self.dtype == torch.float64), N.ptr(self.states.x), N.ptr(self.soup.xcs),
+                     self.contacts_new.c_struct(), self.contacts_pt.c_struct(), float(self.contact_stiffness),
+                     N.ptr(t.rows), N.ptr(t.cols), N.ptr(t.vals), N.ptr(t.mask), self.material, N.ptr(self.tets),
+                     self.n_tets, N.ptr(self.Bm), N.ptr(self.W), self.mu, self.lam, None, None, N.ptr(st["tet_vals"]),
+                     N.ptr(self.b), N.ptr(st["queue"]))
+        key = (int(self.dtype == torch.float64), bucket(n_ee + n_pt), bucket(self.n_tets))
+        cfg = self._tuner.pick(key, lambda c: self._launch_terms(c, Tc), self.b.zero_)
+        self._launch_terms(cfg, Tc)
+        C, cst = contact_bsr(self.contacts_new, n_ee, self.contacts_pt, n_pt, V, t, out=getattr(self, "_C", None),
+                             status=st["status"])
+        self._C = C
+        if cst & 4:  # a row with too many distinct contact columns: sort-based assembly
+            idx = torch.arange(V, dtype=torch.int32, device=self.device)
+            eye = torch.eye(3, dtype=self.dtype, device=self.device)
+            rows = torch.cat([idx, st["rows_t"], t.rows[:nc]])
+            cols = torch.cat([idx, st["cols_t"], t.cols[:nc]])
+            vals = torch.cat([st["diag"][:, None, None] * eye, st["tet_vals"] * h2, t.vals[:nc] * h2])
+            self.A = bsr_from_triplets(V, V, rows, cols, vals)
+            return self.A
+        S = st["S"]
+        cap = st["nnz"] + max(int(C.nnz_dev.item()), 1)  # the union's size bound
+        A = getattr(self, "A", None)
+        if A is None or A.columns.shape[0] < cap or "a_rows" not in st or st["a_rows"].shape[0] < cap:
+            cap = cap + cap // 4
+            A = BsrMatrix(V, V, cap, self.dtype, self.device)
+            for k in ("a_rows", "src_a", "src_b"):
+                st[k] = torch.empty(cap, dtype=torch.int32, device=self.device)
+        cap = min(A.columns.shape[0], st["a_rows"].shape[0])
+        s = N.stream_handle()
+        N.call("ipcb_bsr_union", V, N.ptr(S.offsets), N.ptr(S.columns), N.ptr(C.offsets), N.ptr(C.columns),
+               N.ptr(A.offsets), N.ptr(st["a_rows"]), N.ptr(A.columns), N.ptr(st["src_a"]), N.ptr(st["src_b"]), cap,
+               N.ptr(A.nnz_dev), N.ptr(st["status"]), N.ptr(st["ws"]), st["ws"].numel(), s)
+        N.call("ipcb_newton_values", int(self.dtype == torch.float64), N.ptr(A.nnz_dev), cap, N.ptr(st["a_rows"]),
+               N.ptr(A.columns), N.ptr(st["src_a"]), N.ptr(st["src_b"]), N.ptr(st["g_off"]), N.ptr(st["g_idx"]),
+               N.ptr(st["tet_vals"]), h2, N.ptr(st["diag"]), N.ptr(C.values), h2, N.ptr(A.values), s)
+        self.A = A
+        self.collision_hessian = C
+        return A
 
     def compute_rhs(self) -> torch.Tensor:
         """time_integrator_base.py:82-91,428-438: gradient of the total energy."""

@@ -1,0 +1,111 @@
+"""Batched Newton terms (one persistent work-queue launch over the contact
+records and the tets) and the fixed-pattern assembly against the per-term
+kernels and the sort-based assembly; BSR pattern union against numpy;
+autotuner bookkeeping (gpu)."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import small_scenes
+from ipc_warp_b200 import _native as N
+from ipc_warp_b200.newton import FEMContactSolver
+
+pytestmark = pytest.mark.gpu
+
+
+def _dense(A):
+    nnz = int(A.nnz_dev.item())
+    off = A.offsets.cpu().numpy()
+    cols = A.columns.cpu().numpy()[:nnz]
+    vals = A.values[:nnz].double().cpu().numpy()
+    n = A.nrow
+    D = np.zeros((3 * n, 3 * n))
+    rows = np.repeat(np.arange(n), np.diff(off))
+    for r, c, v in zip(rows, cols, vals):
+        D[3 * r:3 * r + 3, 3 * c:3 * c + 3] += v
+    return D, rows, cols
+
+
+def _solver(sc, dtype, assembly):
+    fixed = sc.xcs[:, 1] <= sc.xcs[:, 1].min() + 1e-9
+    return FEMContactSolver(sc, material="neo_hookean", E=1e6, nu=0.4, rho=1000.0, h=1e-2, fixed=fixed, dtype=dtype,
+                            assembly=assembly)
+
+
+@pytest.mark.parametrize("idx", [0, 1, 2])
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_queue_assembly_equals_generic(cuda, idx, dtype):
+    sc = small_scenes()[idx]
+    rng = np.random.default_rng(idx)
+    x = sc.x + rng.normal(scale=0.05 * sc.dhat, size=sc.x.shape)
+    out = {}
+    for assembly in ("generic", "queue"):
+        s = _solver(sc, dtype, assembly)
+        s.states.x.copy_(torch.tensor(x, dtype=dtype))
+        A = s.compute_A()
+        assert s.n_contacts + s.n_contacts_pt > 0
+        out[assembly] = (_dense(A), s.b.double().cpu().numpy().copy(), s.n_contacts, s.n_contacts_pt)
+    (Dg, rg, cg), bg, *ng = out["generic"]
+    (Dq, rq, cq), bq, *nq = out["queue"]
+    assert ng == nq
+    # identical pattern, values up to the summation order
+    assert np.array_equal(rg, rq) and np.array_equal(cg, cq)
+    tol = 1e-5 if dtype == torch.float32 else 1e-12
+    assert np.abs(Dq - Dg).max() <= tol * np.abs(Dg).max()
+    assert np.abs(bq - bg).max() <= tol * max(np.abs(bg).max(), 1e-30) * 10
+
+
+def test_bsr_union_matches_numpy(cuda):
+    rng = np.random.default_rng(0)
+    n = 300
+
+    def pattern(density):
+        off = [0]
+        cols = []
+        for r in range(n):
+            c = np.sort(rng.choice(n, size=rng.integers(0, int(density * n) + 1), replace=False))
+            cols.extend(c.tolist())
+            off.append(len(cols))
+        return np.array(off, np.int32), np.array(cols, np.int32)
+
+    ao, ac = pattern(0.05)
+    bo, bc = pattern(0.02)
+    t = lambda a: torch.tensor(a, dtype=torch.int32, device=cuda)
+    cap = len(ac) + len(bc)
+    co, crow, ccol, sa, sb = (torch.zeros(k, dtype=torch.int32, device=cuda) for k in (n + 1, cap, cap, cap, cap))
+    nnz = torch.zeros(1, dtype=torch.int32, device=cuda)
+    st = torch.zeros(1, dtype=torch.int32, device=cuda)
+    ws = torch.empty(N.size("ipcb_bsr_union_workspace", n), dtype=torch.uint8, device=cuda)
+    dao, dac, dbo, dbc = t(ao), t(ac), t(bo), t(bc)  # keep the inputs alive until the launch
+    N.call("ipcb_bsr_union", n, N.ptr(dao), N.ptr(dac), N.ptr(dbo), N.ptr(dbc), N.ptr(co), N.ptr(crow),
+           N.ptr(ccol), N.ptr(sa), N.ptr(sb), cap, N.ptr(nnz), N.ptr(st), N.ptr(ws), ws.numel(), N.stream_handle())
+    assert int(st.item()) == 0
+    k = int(nnz.item())
+    co, crow, ccol, sa, sb = (v.cpu().numpy() for v in (co, crow, ccol, sa, sb))
+    for r in range(n):
+        a = ac[ao[r]:ao[r + 1]]
+        b = bc[bo[r]:bo[r + 1]]
+        u = np.union1d(a, b)
+        got = ccol[co[r]:co[r + 1]]
+        assert np.array_equal(got, u)
+        assert np.all(crow[co[r]:co[r + 1]] == r)
+        for p in range(co[r], co[r + 1]):
+            c = ccol[p]
+            assert (sa[p] >= 0) == (c in a) and (sb[p] >= 0) == (c in b)
+            if sa[p] >= 0:
+                assert ac[sa[p]] == c and ao[r] <= sa[p] < ao[r + 1]
+            if sb[p] >= 0:
+                assert bc[sb[p]] == c and bo[r] <= sb[p] < bo[r + 1]
+    assert k == co[n]
+
+
+def test_autotuner_records_every_candidate(cuda):
+    sc = small_scenes()[0]
+    s = _solver(sc, torch.float32, "queue")
+    s.compute_A()
+    (key, times), = s._tuner.timings.items()
+    assert len(times) == len(s._tuner.candidates)
+    assert s._tuner.best[key] in s._tuner.candidates
+    # a second call with the same workload reuses the choice
+    s.compute_A()
+    assert len(s._tuner.timings) == 1
