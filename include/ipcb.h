@@ -82,6 +82,8 @@ typedef struct {
 } ipcb_lbvh;
 
 int ipcb_version(void);
+/* hash of this header at build time; a loader compares it with its header */
+const char* ipcb_abi_hash(void);
 const char* ipcb_last_error(void);
 
 /* ---- device radix sort (also used inside build and BSR assembly) ---- */

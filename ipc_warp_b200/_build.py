@@ -60,13 +60,23 @@ def _deps():
     return files
 
 
+def header_hash(header: str = "ipcb.h") -> str:
+    """Hash of the C-ABI header the library is compiled against; the loader
+    refuses a library whose hash differs from the header next to it."""
+    import hashlib
+
+    with open(os.path.join(INCLUDE, header), "rb") as f:
+        return hashlib.sha1(f.read()).hexdigest()[:16]
+
+
 def _compile(nvcc, sources, verbose):
     procs, objs = [], []
+    abi = header_hash()
     for src in sources:
         obj = os.path.join(OBJ_DIR, src.replace(".cu", ".o"))
         objs.append(obj)
         cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE,
-               "--expt-relaxed-constexpr", "-c", os.path.join(CSRC, src), "-o", obj]
+               "--expt-relaxed-constexpr", f'-DIPCB_ABI_HASH="{abi}"', "-c", os.path.join(CSRC, src), "-o", obj]
         if src in NOFMAD:
             cmd.insert(1, "-fmad=false")
         if src in DIRECT_SOURCES:

@@ -127,6 +127,7 @@ SIGNATURES = {
     "ipcb_bsr_union_workspace": (c_size_t, [c_int]),
     "ipcb_bsr_union": (c_int, [c_int, P, P, P, P, P, P, P, P, P, c_int, P, P, P, c_size_t, P]),
     "ipcb_newton_values": (c_int, [c_int, P, c_int, P, P, P, P, P, P, P, c_double, P, P, c_double, P, P]),
+    "ipcb_abi_hash": (ctypes.c_char_p, []),
     "ipcb_abd_map": (c_int, [c_int, c_int, P, P, P, P, P]),
     "ipcb_abd_step_from": (c_int, [c_int, c_int, P, P, c_double, P, P]),
     "ipcb_abd_prepare_tilde": (c_int, [AB, c_double, P, P, P, P]),
@@ -178,6 +179,16 @@ def lib():
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args
+        header = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "ipcb.h")
+        if os.path.exists(header):
+            import hashlib
+
+            with open(header, "rb") as f:
+                want = hashlib.sha1(f.read()).hexdigest()[:16]
+            have = L.ipcb_abi_hash().decode()
+            if have != want:
+                raise NativeError(f"{LIB_PATH} was built against another include/ipcb.h ({have} != {want}): "
+                                  "rebuild it (`python -c 'import __graft_entry__ as g; g.build()'`)")
         _lib = L
     return _lib
 

@@ -220,6 +220,10 @@ using namespace ipcb;
 extern "C" {
 
 int ipcb_version(void) { return 1; }
+#ifndef IPCB_ABI_HASH
+#define IPCB_ABI_HASH "unknown"
+#endif
+const char* ipcb_abi_hash(void) { return IPCB_ABI_HASH; }
 const char* ipcb_last_error(void) { return ipcb::last_error(); }
 
 size_t ipcb_sort_workspace_u32(int n) { return sort::workspace_bytes<unsigned>(n < 1 ? 1 : n); }
