@@ -388,6 +388,42 @@ int ipcb_newton_values(int fp64, const int* nnz, int capacity, const int* c_rows
                        double tet_scale, const void* diag, const void* contact_vals, double contact_scale,
                        void* values, ipcb_stream s);
 
+/* ---- Device-side line search (time_integrator_base.py:514-546) ----
+ * State of one backtracking search in device memory.  ipcb_ls_begin: E0 from
+ * the energy accumulators acc[3] (acc[0] elastic Psi, acc[1] barrier, acc[2]
+ * inertia + attachment; E = h2 (acc0 + acc1) + acc2), the bound from the CCD
+ * toi (0.9 toi if toi < 1, else 1).  Per trial: ipcb_ls_trial (x = x_tmp -
+ * alpha dx, acc zeroed), the energy kernels, ipcb_ls_accept (accept if E1
+ * finite and < E0, else halve alpha; stops at alpha <= eps max(1, ub), at
+ * max_it trials or when a contact list count exceeds its capacity; sets the
+ * WHILE condition of cond_handle when non-zero).  ipcb_ls_finish restores x
+ * when nothing was accepted. */
+typedef struct {
+  double E0, E1, alpha, ub, eps, alpha_accepted;
+  int it, max_it, accepted, done, overflow, max_ee, max_pt, pad;
+} ipcb_ls_state;
+/* acc += inertia 1/2 m |x - x~|^2 (x~ = x0 + h xdot + h^2 g) + attachment
+ * 1/2 k_att h^2 |x - target|^2 over fixed vertices, in double; fixed: uint8[V]
+ * or null; gravity: host double[3]. */
+int ipcb_ls_inertia(int fp64, int n, const void* x, const void* x0, const void* xdot, const double* gravity, double h,
+                    const double* mass, const unsigned char* fixed, const void* target, double k_att, double* out,
+                    ipcb_stream s);
+int ipcb_ls_begin(ipcb_ls_state* st, const void* toi, int fp64, const double* acc, double h2, double eps, int max_it,
+                  const ipcb_contacts* ee, const ipcb_contacts* pt, ipcb_stream s);
+int ipcb_ls_trial(const ipcb_ls_state* st, int fp64, int n_verts, const void* x_tmp, const void* dx, void* x,
+                  double* acc, ipcb_stream s);
+int ipcb_ls_accept(ipcb_ls_state* st, const double* acc, double h2, const ipcb_contacts* ee, const ipcb_contacts* pt,
+                   unsigned long long cond_handle, ipcb_stream s);
+int ipcb_ls_finish(const ipcb_ls_state* st, int fp64, int n_verts, const void* x_tmp, void* x, ipcb_stream s);
+/* A CUDA graph with one WHILE conditional node: _begin creates it and starts
+ * capturing stream s (not the legacy default stream) into the loop body
+ * (*handle: the condition, 1 at the start of every launch); launches on s
+ * until _end form the body; _launch runs the loop; _destroy frees it. */
+int ipcb_graph_while_begin(void** ctx, unsigned long long* handle, ipcb_stream s);
+int ipcb_graph_while_end(void* ctx, ipcb_stream s);
+int ipcb_graph_launch(void* ctx, ipcb_stream s);
+void ipcb_graph_destroy(void* ctx);
+
 /* ---- BSR assembly (warp.sparse.bsr_from_triplets, dynamic_contacts.py:290-297) ----
  * Canonical 3x3-block CSR from triplets: sort by (row, col), sum duplicates,
  * drop triplets whose 9 values are all zero.  offsets int32[nrow+1],

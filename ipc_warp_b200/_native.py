@@ -44,6 +44,12 @@ class Terms(ctypes.Structure):
                 ("t_cols", P), ("t_vals", P), ("force", P), ("queue", P)]
 
 
+class LsState(ctypes.Structure):
+    _fields_ = [("E0", c_double), ("E1", c_double), ("alpha", c_double), ("ub", c_double), ("eps", c_double),
+                ("alpha_accepted", c_double), ("it", c_int), ("max_it", c_int), ("accepted", c_int), ("done", c_int),
+                ("overflow", c_int), ("max_ee", c_int), ("max_pt", c_int), ("pad", c_int)]
+
+
 class Abd(ctypes.Structure):
     _fields_ = [("n_bodies", c_int), ("fp64", c_int), ("q", P), ("q0", P), ("q_tilde", P), ("qdot", P), ("dx", P),
                 ("mass", P), ("volume", P), ("stiffness", P), ("fixed", P)]
@@ -128,6 +134,15 @@ SIGNATURES = {
     "ipcb_bsr_union": (c_int, [c_int, P, P, P, P, P, P, P, P, P, c_int, P, P, P, c_size_t, P]),
     "ipcb_newton_values": (c_int, [c_int, P, c_int, P, P, P, P, P, P, P, c_double, P, P, c_double, P, P]),
     "ipcb_abi_hash": (ctypes.c_char_p, []),
+    "ipcb_ls_inertia": (c_int, [c_int, c_int, P, P, P, P, c_double, P, P, P, c_double, P, P]),
+    "ipcb_ls_begin": (c_int, [P, P, c_int, P, c_double, c_double, c_int, CP, CP, P]),
+    "ipcb_ls_trial": (c_int, [P, c_int, c_int, P, P, P, P, P]),
+    "ipcb_ls_accept": (c_int, [P, P, c_double, CP, CP, ctypes.c_ulonglong, P]),
+    "ipcb_ls_finish": (c_int, [P, c_int, c_int, P, P, P]),
+    "ipcb_graph_while_begin": (c_int, [ctypes.POINTER(c_void_p), ctypes.POINTER(ctypes.c_ulonglong), P]),
+    "ipcb_graph_while_end": (c_int, [c_void_p, P]),
+    "ipcb_graph_launch": (c_int, [c_void_p, P]),
+    "ipcb_graph_destroy": (None, [c_void_p]),
     "ipcb_abd_map": (c_int, [c_int, c_int, P, P, P, P, P]),
     "ipcb_abd_step_from": (c_int, [c_int, c_int, P, P, c_double, P, P]),
     "ipcb_abd_prepare_tilde": (c_int, [AB, c_double, P, P, P, P]),

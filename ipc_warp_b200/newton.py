@@ -185,8 +185,14 @@ class FEMContactSolver(ContactBarrierMixin):
                  attachment_stiffness: float = 1e11, dtype=torch.float32, device="cuda", vel_tol: float = 5e-2,
                  max_newton: int = 100, tol: float = 1e-4, maxiter: int = 200, exclude_same_body: bool = False,
                  linear_solver: str = "pcg", direct_fallback: bool = True, preconditioner: str = "jacobi",
-                 precond_refresh: int = 1, assembly: str = "queue"):
+                 precond_refresh: int = 1, assembly: str = "queue", line_search_mode: str = "device"):
         self.h = float(h)
+        if line_search_mode not in ("device", "host"):
+            raise ValueError(f"unknown line search mode {line_search_mode!r}")
+        # "device": trials in one CUDA graph WHILE loop, one read per search
+        # (csrc/linesearch.cu); "host": the reference's loop with host reads
+        self.line_search_mode = line_search_mode
+        self._ls = None
         if assembly not in ("queue", "generic"):
             raise ValueError(f"unknown assembly {assembly!r}")
         # "queue": one persistent launch for contact + tet terms and the
@@ -467,6 +473,12 @@ class FEMContactSolver(ContactBarrierMixin):
 
     def line_search(self) -> float:
         """time_integrator_base.py:514-546 with the CCD bound."""
+        if self.line_search_mode == "device":
+            return self._line_search_device()
+        return self._line_search_host()
+
+    def _line_search_host(self) -> float:
+        """The reference's loop: energies and the accept test on the host."""
         x_tmp = self.states.x.clone()
         E0 = self.total_energy()
         ub = self.collision_free_step(self.states.dx)
@@ -488,6 +500,154 @@ class FEMContactSolver(ContactBarrierMixin):
             alpha = 0.0
         self.stats.energies.append((E0, E1))
         return alpha
+
+    # ------------------------------------------------- device line search
+    def _energy_launches(self, acc: torch.Tensor):
+        """Launches (no host reads, graph-capturable) that add the energy terms
+        at the current x into acc: [0] elastic Psi, [1] barrier, [2] inertia +
+        attachment.  Contact lists are refilled by the DCD; their counts stay
+        on the device."""
+        s = N.stream_handle()
+        fp64 = int(self.dtype == torch.float64)
+        kappa = float(self.contact_stiffness)
+        self.update_bvh()
+        self._launch_dcd("ee")
+        if self.has_triangles:
+            self._launch_dcd("pt")
+        soup = self.soup.c_struct()
+        base = acc.data_ptr()
+        N.call("ipcb_contact_energy", 0, ctypes.byref(soup), ctypes.byref(self.contacts_new.c_struct()), -1, kappa,
+               base + 8, s)
+        if self.has_triangles:
+            N.call("ipcb_contact_energy", 1, ctypes.byref(soup), ctypes.byref(self.contacts_pt.c_struct()), -1,
+                   kappa, base + 8, s)
+        N.call("ipcb_tet_energy", self.material, fp64, N.ptr(self.states.x), N.ptr(self.tets), self.n_tets,
+               N.ptr(self.Bm), N.ptr(self.W), self.mu, self.lam, base, s)
+        ls = self._ls
+        N.call("ipcb_ls_inertia", fp64, self.soup.n_verts, N.ptr(self.states.x), N.ptr(self.states.x0),
+               N.ptr(self.states.xdot), ls["gravity"], self.h, N.ptr(self.mass),
+               N.ptr(ls["fixed"]) if ls["any_fixed"] else None, N.ptr(self.x_target), self.k_att, base + 16, s)
+
+    def _ccd_launches(self, dx: torch.Tensor):
+        """collision_free_step without its read: the TOI stays in ccd_toi."""
+        soup = self.soup.c_struct()
+        s = N.stream_handle()
+        pad = 1e-7
+        N.call("ipcb_add_dx", ctypes.byref(soup), N.ptr(dx), N.ptr(self.ccd_x1), s)
+        N.call("ipcb_swept_edge_aabbs", ctypes.byref(soup), N.ptr(self.ccd_x1), pad, N.ptr(self.ccd_edge_lower),
+               N.ptr(self.ccd_edge_upper), s)
+        self.ccd_edge_bvh.refit(self.ccd_edge_lower, self.ccd_edge_upper)
+        self.ccd_toi.fill_(1.0)
+        self._status.zero_()
+        N.call("ipcb_edge_edge_toi", ctypes.byref(soup), N.ptr(self.ccd_x1), ctypes.byref(self.ccd_edge_bvh.c),
+               N.ptr(self.ccd_edge_lower), N.ptr(self.ccd_edge_upper), int(self.disable_self_collision),
+               N.ptr(self.ccd_toi), N.ptr(self._status), N.ptr(self._toi_ws), self._toi_ws.numel(), s)
+        if self.has_triangles:
+            N.call("ipcb_swept_triangle_aabbs", ctypes.byref(soup), N.ptr(self.ccd_x1), pad,
+                   N.ptr(self.ccd_triangle_lower), N.ptr(self.ccd_triangle_upper), s)
+            self.ccd_triangle_bvh.refit(self.ccd_triangle_lower, self.ccd_triangle_upper)
+            N.call("ipcb_point_triangle_toi", ctypes.byref(soup), N.ptr(self.ccd_x1),
+                   ctypes.byref(self.ccd_triangle_bvh.c), pad, int(self.disable_self_collision),
+                   N.ptr(self.ccd_toi), N.ptr(self._status), N.ptr(self._toi_ws), self._toi_ws.numel(), s)
+
+    def _ls_buffers(self):
+        if self._ls is None:
+            dev = self.device
+            self._ls = dict(
+                x_tmp=torch.empty_like(self.states.x), acc=torch.zeros(3, dtype=torch.float64, device=dev),
+                acc0=torch.zeros(3, dtype=torch.float64, device=dev),
+                state=torch.zeros(ctypes.sizeof(N.LsState), dtype=torch.uint8, device=dev),
+                host=torch.zeros(ctypes.sizeof(N.LsState), dtype=torch.uint8).pin_memory(),
+                gravity=(ctypes.c_double * 3)(*self.gravity.double().cpu().tolist()),
+                fixed=self.fixed.to(torch.uint8), any_fixed=bool(self.fixed.any()),
+                stream=torch.cuda.Stream(device=dev), graph=None, key=None)
+        return self._ls
+
+    def _ls_key(self):
+        return (self.states.x.data_ptr(), self.states.dx.data_ptr(), self.states.x0.data_ptr(),
+                self.states.xdot.data_ptr(), self.contacts_new.a1a2b1b2.data_ptr(), self.contacts_new.capacity,
+                self.contacts_pt.a1a2b1b2.data_ptr(), self.contacts_pt.capacity, self.x_target.data_ptr())
+
+    def _ls_graph(self):
+        """The WHILE graph of one trial, captured once per buffer set (on a
+        side stream: the legacy default stream cannot be captured)."""
+        ls = self._ls
+        key = self._ls_key()
+        if ls["graph"] is not None and ls["key"] == key:
+            return ls["graph"]
+        if ls["graph"] is not None:
+            N.lib().ipcb_graph_destroy(ls["graph"])
+            ls["graph"] = None
+        fp64 = int(self.dtype == torch.float64)
+        h2 = self.h * self.h
+        side = ls["stream"]
+        side.wait_stream(torch.cuda.current_stream())
+        ctx, handle = ctypes.c_void_p(), ctypes.c_ulonglong()
+        with torch.cuda.stream(side):
+            s = N.stream_handle()
+            N.call("ipcb_graph_while_begin", ctypes.byref(ctx), ctypes.byref(handle), s)
+            body_ok = False
+            try:
+                N.call("ipcb_ls_trial", N.ptr(ls["state"]), fp64, self.soup.n_verts, N.ptr(ls["x_tmp"]),
+                       N.ptr(self.states.dx), N.ptr(self.states.x), N.ptr(ls["acc"]), s)
+                self._energy_launches(ls["acc"])
+                # the accept kernel is what ends the loop: the body is complete only with it
+                N.call("ipcb_ls_accept", N.ptr(ls["state"]), N.ptr(ls["acc"]), h2,
+                       ctypes.byref(self.contacts_new.c_struct()), ctypes.byref(self.contacts_pt.c_struct()),
+                       handle.value, s)
+                body_ok = True
+            finally:
+                end_rc = N.lib().ipcb_graph_while_end(ctx, s)
+                if not body_ok or end_rc != 0:
+                    N.lib().ipcb_graph_destroy(ctx)
+            if end_rc != 0:
+                raise N.NativeError("ipcb_graph_while_end failed: " + (N.lib().ipcb_last_error() or b"").decode())
+        torch.cuda.current_stream().wait_stream(side)
+        ls["graph"], ls["key"] = ctx, key
+        return ctx
+
+    def _line_search_device(self) -> float:
+        """The reference's search (same E0, bound, halving and accept test)
+        with the trial loop on the device: E0 and the CCD bound are launched,
+        then the WHILE graph runs trials until one is accepted, and the state
+        is read once.  A contact-list overflow during the search grows the
+        lists and reruns it on the host."""
+        ls = self._ls_buffers()
+        fp64 = int(self.dtype == torch.float64)
+        h2 = self.h * self.h
+        s = N.stream_handle()
+        ls["x_tmp"].copy_(self.states.x)
+        ls["acc0"].zero_()
+        self._energy_launches(ls["acc0"])
+        self._ccd_launches(self.states.dx)
+        eps = 1.1920928955078125e-7 if self.dtype == torch.float32 else 2.220446049250313e-16
+        N.call("ipcb_ls_begin", N.ptr(ls["state"]), N.ptr(self.ccd_toi), fp64, N.ptr(ls["acc0"]), h2, eps, 64,
+               ctypes.byref(self.contacts_new.c_struct()), ctypes.byref(self.contacts_pt.c_struct()), s)
+        graph = self._ls_graph()
+        N.call("ipcb_graph_launch", graph, s)
+        N.call("ipcb_ls_finish", N.ptr(ls["state"]), fp64, self.soup.n_verts, N.ptr(ls["x_tmp"]),
+               N.ptr(self.states.x), s)
+        ls["host"].copy_(ls["state"], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        st = N.LsState.from_buffer_copy(ls["host"].numpy().tobytes())
+        if st.overflow:
+            if st.max_ee > self.contacts_new.capacity:
+                self._grow_contact_list(self.contacts_new, st.max_ee)
+            if st.max_pt > self.contacts_pt.capacity:
+                self._grow_contact_list(self.contacts_pt, st.max_pt, point_triangle=True)
+            self.states.x.copy_(ls["x_tmp"])
+            return self._line_search_host()
+        self.stats.energies.append((st.E0, st.E1))
+        self.ls_trials = st.it
+        return st.alpha_accepted if st.accepted else 0.0
+
+    def __del__(self):
+        ls = getattr(self, "_ls", None)
+        if ls and ls.get("graph") is not None:
+            try:
+                N.lib().ipcb_graph_destroy(ls["graph"])
+            except Exception:
+                pass
 
     def newton_iteration(self) -> tuple[float, float]:
         """One iteration of RodBCBase.step; with ``self.timing`` set, the
