@@ -292,6 +292,26 @@ def run_profile_solver(args):
     torch.cuda.synchronize()
 
 
+def run_profile_newton(args):
+    """Untimed Newton iterations on the wound rod bundle (for ncu launch
+    lists): one warm-up iteration, then two more between
+    cudaProfilerStart/Stop, each compute_A (work-queue terms + fixed-pattern
+    assembly), rhs, learned-PCG solve, device line search."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    s = newton_solver(dev, torch, "pcg", "learned")
+    x0 = s.states.x.clone()
+    s.newton_iteration()  # warm-up: autotuning, graph captures, buffer pools
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()  # ncu --profile-from-start off captures from here
+    for _ in range(2):
+        s.states.x.copy_(x0)
+        s.newton_iteration()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+
+
 # ------------------------------------------------------------- CPU oracle
 def cpu_pipeline(sc, dx, reps):
     """One pass of the oracle's restatement: DCD EE + PT, narrow phase
@@ -484,9 +504,14 @@ def main():
                     help="skip the Newton-step timing (learned-PCG / Jacobi-PCG / direct)")
     ap.add_argument("--profile-solver", action="store_true",
                     help="untimed Newton-solve kernels only (learned factor + PCG), for ncu; prints nothing")
+    ap.add_argument("--profile-newton", action="store_true",
+                    help="untimed Newton iterations (learned PCG, device line search), for ncu; prints nothing")
     args = ap.parse_args()
     if args.profile_solver:
         run_profile_solver(args)
+        return
+    if args.profile_newton:
+        run_profile_newton(args)
         return
     if args.impl == "reference":
         run_reference(args)

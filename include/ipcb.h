@@ -175,6 +175,22 @@ int ipcb_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* s
                        ipcb_stream s);
 int ipcb_point_triangle_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* swept_tri_bvh, double pad,
                             int exclude_same_body, void* toi, int* status, void* ws, size_t ws_bytes, ipcb_stream s);
+/* new_intersections (contact.py:587-670; edge_edge_intersections /
+ * point_triangle_intersections 371-442): the CCD queries above that also
+ * append every pair whose time of impact is < 1 to `out` as a record
+ * (append_ccd 186-197: EE a0 a1 b0 b1 with e0e1 = (i, j), i < j; PT the
+ * vertex and the triangle's t0 t1 t2 with e0e1 = (vertex, triangle);
+ * l0 = 2 thickness, alpha = toi, lam = 0), besides the minimum in toi.
+ * *out->cnt counts every such pair; records beyond the capacity are dropped
+ * (grow and relaunch, as the reference). */
+int ipcb_edge_edge_intersections(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* swept_edge_bvh,
+                                 const float* lower, const float* upper, int exclude_same_body, double thickness,
+                                 void* toi, const ipcb_contacts* out, int* status, void* ws, size_t ws_bytes,
+                                 ipcb_stream s);
+int ipcb_point_triangle_intersections(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* swept_tri_bvh,
+                                      double pad, int exclude_same_body, double thickness, void* toi,
+                                      const ipcb_contacts* out, int* status, void* ws, size_t ws_bytes,
+                                      ipcb_stream s);
 /* per-pair collision time of n explicit pairs (kind 0 EE, 1 PT); p_t0/p_t1:
  * double[n*12] (4 points each) -> t double[n] (ee/pt_collision_time, ccd.py:304-357) */
 int ipcb_collision_time(int kind, int n, const double* p_t0, const double* p_t1, double* t, int* status,
@@ -423,6 +439,42 @@ int ipcb_graph_while_begin(void** ctx, unsigned long long* handle, ipcb_stream s
 int ipcb_graph_while_end(void* ctx, ipcb_stream s);
 int ipcb_graph_launch(void* ctx, ipcb_stream s);
 void ipcb_graph_destroy(void* ctx);
+
+/* ---- Hashed active set of the augmented-Lagrangian solver
+ * (augmented_lagrangian.py:105-198 kernels, 506-572 ActiveSet) ----
+ * ALConstraint columns (capacity entries, scalar = fp64 ? double : float)
+ * stored bucket by bucket; bucket b of the key e0e1 (hash_pos: (e0 * 73856093
+ * xor e1 * 19349663) in 32-bit, non-negative, mod table_size) holds entries
+ * cell_start[b] .. cell_start[b+1]; cell_start[table_size] = count. */
+typedef struct {
+  int table_size;
+  int capacity;
+  int* cell_start;   /* int32[table_size + 1] */
+  int* a1a2b1b2;     /* int4[capacity] */
+  int* e0e1;         /* int2[capacity] */
+  void* l0;
+  void* alpha;
+  void* lam;
+  void* gamma;
+  void* slack;
+  void* mollifier;
+  void* d0;
+  int* distance_type;
+  void* grad;        /* scalar[12 capacity] */
+} ipcb_al_set;
+/* accumulate_vertex_toi: vertex_toi[v] = min(vertex_toi[v], alpha) over the
+ * n records' vertices (vertex_toi scalar[V], non-negative on entry) */
+int ipcb_al_vertex_toi(int fp64, const ipcb_contacts* list, int n, void* vertex_toi, ipcb_stream s);
+size_t ipcb_al_workspace(int table_size);
+/* ActiveSet.create_hash: the records kept by filter_accept (alpha <= the
+ * toi of one of its vertices + 1e-12), as fresh constraints (lam 0, gamma 1,
+ * slack 0, mollifier 1, type 0, d0 0, grad 0); n <= set->capacity. */
+int ipcb_al_create(int fp64, ipcb_al_set* set, const ipcb_contacts* list, int n, const void* vertex_toi, void* ws,
+                   size_t ws_bytes, ipcb_stream s);
+/* ActiveSet.merge: dst = the old entries with gamma >= 0.01 and the new
+ * entries whose key is not in old; n_new + n_old <= dst->capacity. */
+int ipcb_al_merge(int fp64, const ipcb_al_set* nw, const ipcb_al_set* old, ipcb_al_set* dst, int n_new, int n_old,
+                  void* ws, size_t ws_bytes, ipcb_stream s);
 
 /* ---- BSR assembly (warp.sparse.bsr_from_triplets, dynamic_contacts.py:290-297) ----
  * Canonical 3x3-block CSR from triplets: sort by (row, col), sum duplicates,

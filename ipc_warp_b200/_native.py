@@ -50,6 +50,12 @@ class LsState(ctypes.Structure):
                 ("overflow", c_int), ("max_ee", c_int), ("max_pt", c_int), ("pad", c_int)]
 
 
+class AlSet(ctypes.Structure):
+    _fields_ = [("table_size", c_int), ("capacity", c_int), ("cell_start", P), ("a1a2b1b2", P), ("e0e1", P),
+                ("l0", P), ("alpha", P), ("lam", P), ("gamma", P), ("slack", P), ("mollifier", P), ("d0", P),
+                ("distance_type", P), ("grad", P)]
+
+
 class Abd(ctypes.Structure):
     _fields_ = [("n_bodies", c_int), ("fp64", c_int), ("q", P), ("q0", P), ("q_tilde", P), ("qdot", P), ("dx", P),
                 ("mass", P), ("volume", P), ("stiffness", P), ("fixed", P)]
@@ -143,6 +149,13 @@ SIGNATURES = {
     "ipcb_graph_while_end": (c_int, [c_void_p, P]),
     "ipcb_graph_launch": (c_int, [c_void_p, P]),
     "ipcb_graph_destroy": (None, [c_void_p]),
+    "ipcb_edge_edge_intersections": (c_int, [SP, P, BP, P, P, c_int, c_double, P, CP, P, P, c_size_t, P]),
+    "ipcb_point_triangle_intersections": (c_int, [SP, P, BP, c_double, c_int, c_double, P, CP, P, P, c_size_t, P]),
+    "ipcb_al_vertex_toi": (c_int, [c_int, CP, c_int, P, P]),
+    "ipcb_al_workspace": (c_size_t, [c_int]),
+    "ipcb_al_create": (c_int, [c_int, ctypes.POINTER(AlSet), CP, c_int, P, P, c_size_t, P]),
+    "ipcb_al_merge": (c_int, [c_int, ctypes.POINTER(AlSet), ctypes.POINTER(AlSet), ctypes.POINTER(AlSet), c_int, c_int,
+                              P, c_size_t, P]),
     "ipcb_abd_map": (c_int, [c_int, c_int, P, P, P, P, P]),
     "ipcb_abd_step_from": (c_int, [c_int, c_int, P, P, c_double, P, P]),
     "ipcb_abd_prepare_tilde": (c_int, [AB, c_double, P, P, P, P]),

@@ -287,6 +287,59 @@ class ContactSolverBase:
         toi = float(self.ccd_toi.item())
         return 0.9 * toi if toi < 1.0 else 1.0
 
+    def new_intersections(self, x0: torch.Tensor, x1: torch.Tensor) -> float:
+        """contact.py:587-670 (the augmented-Lagrangian solver's CCD): every
+        EE / PT pair that collides on the straight path x0 -> x1 becomes a
+        record of ``contacts_new`` / ``contacts_pt`` (alpha = its time of
+        impact); returns 0.9 * toi if toi < 1 else 1.  Lists grow and the
+        query reruns when they overflow, as the reference."""
+        soup = self.soup.c_struct(x0)
+        s = N.stream_handle()
+        pad = 1e-7
+        th = float(_thickness)
+        excl = int(self.disable_self_collision)
+        N.call("ipcb_swept_edge_aabbs", ctypes.byref(soup), N.ptr(x1), pad, N.ptr(self.ccd_edge_lower),
+               N.ptr(self.ccd_edge_upper), s)
+        self.ccd_edge_bvh.refit(self.ccd_edge_lower, self.ccd_edge_upper)
+        self._status.zero_()
+
+        def edges():
+            self.contacts_new.cnt.zero_()
+            self.ccd_toi.fill_(1.0)
+            N.call("ipcb_edge_edge_intersections", ctypes.byref(soup), N.ptr(x1), ctypes.byref(self.ccd_edge_bvh.c),
+                   N.ptr(self.ccd_edge_lower), N.ptr(self.ccd_edge_upper), excl, th, N.ptr(self.ccd_toi),
+                   ctypes.byref(self.contacts_new.c_struct()), N.ptr(self._status), N.ptr(self._toi_ws),
+                   self._toi_ws.numel(), s)
+            return int(self.contacts_new.cnt.item())
+
+        n = edges()
+        if n > self.contacts_new.capacity:
+            self._grow_contact_list(self.contacts_new, n)
+            n = edges()
+        self.n_contacts = n
+        if self.has_triangles:
+            N.call("ipcb_swept_triangle_aabbs", ctypes.byref(soup), N.ptr(x1), pad, N.ptr(self.ccd_triangle_lower),
+                   N.ptr(self.ccd_triangle_upper), s)
+            self.ccd_triangle_bvh.refit(self.ccd_triangle_lower, self.ccd_triangle_upper)
+
+            def points():
+                self.contacts_pt.cnt.zero_()
+                N.call("ipcb_point_triangle_intersections", ctypes.byref(soup), N.ptr(x1),
+                       ctypes.byref(self.ccd_triangle_bvh.c), pad, excl, th, N.ptr(self.ccd_toi),
+                       ctypes.byref(self.contacts_pt.c_struct()), N.ptr(self._status), N.ptr(self._toi_ws),
+                       self._toi_ws.numel(), s)
+                return int(self.contacts_pt.cnt.item())
+
+            n = points()
+            if n > self.contacts_pt.capacity:
+                self._grow_contact_list(self.contacts_pt, n, point_triangle=True)
+                n = points()
+            self.n_contacts_pt = n
+        else:
+            self.n_contacts_pt = 0
+        toi = float(self.ccd_toi.item())
+        return 0.9 * toi if toi < 1.0 else 1.0
+
     @property
     def status(self) -> int:
         """OR of IPCB_STATUS_* bits raised by the last queries."""

@@ -283,6 +283,28 @@ IPCB_D d3 ld(const S* __restrict__ x, int i) {
 IPCB_D void store_toi(float* toi, double t) { atomic_min_nonneg(toi, __double2float_rz(t)); }
 IPCB_D void store_toi(double* toi, double t) { atomic_min_nonneg(toi, t); }
 
+// Optional output of new_intersections (contact.py:587-670): every pair whose
+// time of impact is < 1 is appended as a record (append_ccd, contact.py:186-197:
+// a1a2b1b2, e0e1 = (query primitive, hit primitive), l0 = 2 thickness,
+// alpha = toi, lam = 0); records beyond the capacity are only counted.
+struct Sink {
+  ipcb_contacts L;
+  double l0;
+  int on;
+};
+
+template <class S>
+IPCB_D void sink_append(const Sink& k, int4 ids, int e0, int e1, double t) {
+  if (!k.on) return;
+  const int idx = atomicAdd(k.L.cnt, 1);
+  if (idx >= k.L.capacity) return;
+  reinterpret_cast<int4*>(k.L.a1a2b1b2)[idx] = ids;
+  reinterpret_cast<int2*>(k.L.e0e1)[idx] = make_int2(e0, e1);
+  static_cast<S*>(k.L.l0)[idx] = S(k.l0);
+  static_cast<S*>(k.L.alpha)[idx] = sizeof(S) == 4 ? S(__double2float_rz(t)) : S(t);
+  static_cast<S*>(k.L.lam)[idx] = S(0);
+}
+
 template <class S>
 __global__ void k_add_dx(const S* __restrict__ x, const S* __restrict__ dx, S* __restrict__ x1, int n3) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -463,7 +485,7 @@ __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, co
                                                     const int* __restrict__ edges, const int* __restrict__ body,
                                                     const float4* __restrict__ nodes, const int* __restrict__ order,
                                                     int n, const float* __restrict__ lo, const float* __restrict__ hi,
-                                                    int exclude, CandList cand, S* toi, int* status) {
+                                                    int exclude, CandList cand, S* toi, int* status, Sink sink) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   bool active = t < n;
   int i = active ? __ldg(order + t) : 0;
@@ -484,7 +506,10 @@ __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, co
         q[nq++] = j;
       } else {
         double tt = ee_pair_time(x0, x1, ea, eb, st);
-        if (tt < 1.0) store_toi(toi, tt);
+        if (tt < 1.0) {
+          store_toi(toi, tt);
+          sink_append<S>(sink, make_int4(ea.x, ea.y, eb.x, eb.y), i, j, tt);
+        }
       }
     });
     if (!ok) st |= IPCB_STATUS_STACK;
@@ -496,7 +521,10 @@ __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, co
     if (!push_converged(cand, has, i, j)) {
       int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + j);
       double tt = ee_pair_time(x0, x1, ea, eb, st);
-      if (tt < 1.0) store_toi(toi, tt);
+      if (tt < 1.0) {
+        store_toi(toi, tt);
+        sink_append<S>(sink, make_int4(ea.x, ea.y, eb.x, eb.y), i, j, tt);
+      }
     }
   }
   if (st) atomicOr(status, st);
@@ -506,7 +534,7 @@ template <class S>
 __global__ void __launch_bounds__(128) k_pt_collect(const S* __restrict__ x0, const S* __restrict__ x1,
                                                     const int* __restrict__ tris, const int* __restrict__ body,
                                                     const float4* __restrict__ nodes, int n_tris, int nv, double pad,
-                                                    int exclude, CandList cand, S* toi, int* status) {
+                                                    int exclude, CandList cand, S* toi, int* status, Sink sink) {
   int i0 = blockIdx.x * blockDim.x + threadIdx.x;
   bool active = i0 < nv;
   int i = active ? i0 : 0;
@@ -528,7 +556,10 @@ __global__ void __launch_bounds__(128) k_pt_collect(const S* __restrict__ x0, co
         q[nq++] = j;
       } else {
         double tt = pt_pair_time(x0, x1, i, tj, st);
-        if (tt < 1.0) store_toi(toi, tt);
+        if (tt < 1.0) {
+          store_toi(toi, tt);
+          sink_append<S>(sink, make_int4(i, tj.x, tj.y, tj.z), i, j, tt);
+        }
       }
     });
     if (!ok) st |= IPCB_STATUS_STACK;
@@ -540,7 +571,10 @@ __global__ void __launch_bounds__(128) k_pt_collect(const S* __restrict__ x0, co
     if (!push_converged(cand, has, i, j)) {
       int3 tj = make_int3(__ldg(tris + 3 * j), __ldg(tris + 3 * j + 1), __ldg(tris + 3 * j + 2));
       double tt = pt_pair_time(x0, x1, i, tj, st);
-      if (tt < 1.0) store_toi(toi, tt);
+      if (tt < 1.0) {
+        store_toi(toi, tt);
+        sink_append<S>(sink, make_int4(i, tj.x, tj.y, tj.z), i, j, tt);
+      }
     }
   }
   if (st) atomicOr(status, st);
@@ -550,22 +584,28 @@ __global__ void __launch_bounds__(128) k_pt_collect(const S* __restrict__ x0, co
 template <class S, int KIND>
 __global__ void __launch_bounds__(128) k_cand_toi(const S* __restrict__ x0, const S* __restrict__ x1,
                                                   const int* __restrict__ prims, CandList cand, S* toi,
-                                                  int* status) {
+                                                  int* status, Sink sink) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   int n = min(*cand.count, cand.capacity);
   if (k >= n) return;
   int2 pr = cand.pairs[k];
   int st = 0;
   double tt;
+  int4 ids;
   if (KIND == 0) {
     int2 ea = __ldg(reinterpret_cast<const int2*>(prims) + pr.x);
     int2 eb = __ldg(reinterpret_cast<const int2*>(prims) + pr.y);
     tt = ee_pair_time(x0, x1, ea, eb, st);
+    ids = make_int4(ea.x, ea.y, eb.x, eb.y);
   } else {
     int3 tj = make_int3(__ldg(prims + 3 * pr.y), __ldg(prims + 3 * pr.y + 1), __ldg(prims + 3 * pr.y + 2));
     tt = pt_pair_time(x0, x1, pr.x, tj, st);
+    ids = make_int4(pr.x, tj.x, tj.y, tj.z);
   }
-  if (tt < 1.0) store_toi(toi, tt);
+  if (tt < 1.0) {
+    store_toi(toi, tt);
+    sink_append<S>(sink, ids, pr.x, pr.y, tt);
+  }
   if (st) atomicOr(status, st);
 }
 
@@ -873,17 +913,17 @@ int ipcb_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* b
   if (soup->fp64) {
     k_ee_collect<double><<<g, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, soup->body,
                                             (const float4*)bvh->wide, bvh->sorted, n, lower, upper,
-                                            exclude_same_body, c, (double*)toi, status);
+                                            exclude_same_body, c, (double*)toi, status, Sink{});
     if (c.capacity)
       k_cand_toi<double, 0><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, c,
-                                                (double*)toi, status);
+                                                (double*)toi, status, Sink{});
   } else {
     k_ee_collect<float><<<g, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, soup->body,
                                            (const float4*)bvh->wide, bvh->sorted, n, lower, upper,
-                                           exclude_same_body, c, (float*)toi, status);
+                                           exclude_same_body, c, (float*)toi, status, Sink{});
     if (c.capacity)
       k_cand_toi<float, 0><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, c,
-                                               (float*)toi, status);
+                                               (float*)toi, status, Sink{});
   }
   return check_launch("ipcb_edge_edge_toi");
 }
@@ -902,19 +942,83 @@ int ipcb_point_triangle_toi(const ipcb_soup* soup, const void* x1, const ipcb_lb
   if (soup->fp64) {
     k_pt_collect<double><<<g, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, soup->body,
                                             (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude_same_body, c,
-                                            (double*)toi, status);
+                                            (double*)toi, status, Sink{});
     if (c.capacity)
       k_cand_toi<double, 1><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, c,
-                                                (double*)toi, status);
+                                                (double*)toi, status, Sink{});
   } else {
     k_pt_collect<float><<<g, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, soup->body,
                                            (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude_same_body, c,
-                                           (float*)toi, status);
+                                           (float*)toi, status, Sink{});
     if (c.capacity)
       k_cand_toi<float, 1><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, c,
-                                               (float*)toi, status);
+                                               (float*)toi, status, Sink{});
   }
   return check_launch("ipcb_point_triangle_toi");
+}
+
+int ipcb_edge_edge_intersections(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, const float* lower,
+                                 const float* upper, int exclude_same_body, double thickness, void* toi,
+                                 const ipcb_contacts* out, int* status, void* ws, size_t ws_bytes, ipcb_stream s) {
+  if (!soup || !x1 || !bvh || !lower || !upper || !toi || !out || !out->cnt || !status || !ws || ws_bytes < 256 ||
+      bvh->n != soup->n_edges)
+    return IPCB_E_ARG;
+  if (out->capacity > 0 && (!out->a1a2b1b2 || !out->e0e1 || !out->l0 || !out->alpha || !out->lam)) return IPCB_E_ARG;
+  int n = soup->n_edges;
+  if (n == 0) return IPCB_OK;
+  cudaStream_t st = (cudaStream_t)s;
+  CandList c = cand_list(ws, ws_bytes);
+  cudaMemsetAsync(c.count, 0, sizeof(int), st);
+  const Sink sink{*out, thickness * 2.0, 1};
+  dim3 g(div_up(n, 128)), gc(div_up(c.capacity > 0 ? c.capacity : 1, 128));
+  if (soup->fp64) {
+    k_ee_collect<double><<<g, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, soup->body,
+                                            (const float4*)bvh->wide, bvh->sorted, n, lower, upper,
+                                            exclude_same_body, c, (double*)toi, status, sink);
+    if (c.capacity)
+      k_cand_toi<double, 0><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, c,
+                                                (double*)toi, status, sink);
+  } else {
+    k_ee_collect<float><<<g, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, soup->body,
+                                           (const float4*)bvh->wide, bvh->sorted, n, lower, upper,
+                                           exclude_same_body, c, (float*)toi, status, sink);
+    if (c.capacity)
+      k_cand_toi<float, 0><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, c,
+                                               (float*)toi, status, sink);
+  }
+  return check_launch("ipcb_edge_edge_intersections");
+}
+
+int ipcb_point_triangle_intersections(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, double pad,
+                                      int exclude_same_body, double thickness, void* toi, const ipcb_contacts* out,
+                                      int* status, void* ws, size_t ws_bytes, ipcb_stream s) {
+  if (!soup || !x1 || !bvh || !toi || !out || !out->cnt || !status || !ws || ws_bytes < 256 ||
+      bvh->n != soup->n_tris)
+    return IPCB_E_ARG;
+  if (out->capacity > 0 && (!out->a1a2b1b2 || !out->e0e1 || !out->l0 || !out->alpha || !out->lam)) return IPCB_E_ARG;
+  int nv = soup->n_verts;
+  if (nv == 0 || soup->n_tris == 0) return IPCB_OK;
+  cudaStream_t st = (cudaStream_t)s;
+  CandList c = cand_list(ws, ws_bytes);
+  cudaMemsetAsync(c.count, 0, sizeof(int), st);
+  const Sink sink{*out, thickness * 2.0, 1};
+  dim3 g(div_up(nv, 128)), gc(div_up(c.capacity > 0 ? c.capacity : 1, 128));
+  if (soup->fp64) {
+    k_pt_collect<double><<<g, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, soup->body,
+                                            (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude_same_body, c,
+                                            (double*)toi, status, sink);
+    if (c.capacity)
+      k_cand_toi<double, 1><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, c,
+                                                (double*)toi, status, sink);
+  } else {
+    k_pt_collect<float><<<g, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, soup->body,
+                                           (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude_same_body, c,
+                                           (float*)toi, status, sink);
+    if (c.capacity)
+      k_cand_toi<float, 1><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, c,
+                                               (float*)toi, status, sink);
+  }
+  return check_launch("ipcb_point_triangle_intersections");
 }
 
 int ipcb_collision_time(int kind, int n, const double* p_t0, const double* p_t1, double* t, int* status,
@@ -975,13 +1079,13 @@ int ipcb_fixed_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_b
                                                      fixed, (const int2*)pairs, pad, c, (double*)toi, status);
     if (c.capacity)
       k_cand_toi<double, 0><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, c,
-                                              (double*)toi, status);
+                                              (double*)toi, status, Sink{});
   } else {
     k_fixed_ee_collect<float><<<grid, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, *B, fixed,
                                                     (const int2*)pairs, pad, c, (float*)toi, status);
     if (c.capacity)
       k_cand_toi<float, 0><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, c, (float*)toi,
-                                             status);
+                                             status, Sink{});
   }
   return check_launch("ipcb_fixed_edge_edge_toi");
 }
@@ -1002,13 +1106,13 @@ int ipcb_fixed_point_triangle_toi(const ipcb_soup* soup, const void* x1, const i
                                                      (const int2*)pairs, pad, c, (double*)toi, status);
     if (c.capacity)
       k_cand_toi<double, 1><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, c,
-                                              (double*)toi, status);
+                                              (double*)toi, status, Sink{});
   } else {
     k_fixed_pt_collect<float><<<grid, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, *B,
                                                     (const int2*)pairs, pad, c, (float*)toi, status);
     if (c.capacity)
       k_cand_toi<float, 1><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, c,
-                                             (float*)toi, status);
+                                             (float*)toi, status, Sink{});
   }
   return check_launch("ipcb_fixed_point_triangle_toi");
 }
