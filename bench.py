@@ -35,10 +35,13 @@ METRIC = "Newton step ms, learned-PCG vs cuDSS at rel res 1e-6; contact pairs/s,
 WORKLOAD = "rod_twist_16rods_4x4x256_wound_contact_state"
 
 
+ROD_SIDE = 4  # rods per side of the bundle; --rods N shrinks the workload for profiler captures
+
+
 def scene():
     from ipc_warp_b200 import scenes
 
-    return scenes.rod_bundle(n_rods_side=4, cells=(4, 4, 256), width=0.1, gap_over_dhat=0.5,
+    return scenes.rod_bundle(n_rods_side=ROD_SIDE, cells=(4, 4, 256), width=0.1, gap_over_dhat=0.5,
                              jitter_over_dhat=0.05, seed=1, kappa=1e4)
 
 
@@ -504,9 +507,13 @@ def main():
                     help="skip the Newton-step timing (learned-PCG / Jacobi-PCG / direct)")
     ap.add_argument("--profile-solver", action="store_true",
                     help="untimed Newton-solve kernels only (learned factor + PCG), for ncu; prints nothing")
+    ap.add_argument("--rods", type=int, default=4,
+                    help="rods per side of the bundle (4 = the benchmark workload; smaller for ncu section captures)")
     ap.add_argument("--profile-newton", action="store_true",
                     help="untimed Newton iterations (learned PCG, device line search), for ncu; prints nothing")
     args = ap.parse_args()
+    global ROD_SIDE
+    ROD_SIDE = args.rods
     if args.profile_solver:
         run_profile_solver(args)
         return

@@ -21,7 +21,7 @@ namespace {
 
 // T: arithmetic type of the eigen-solve and of H (float for S=float).
 template <class S, int KIND>
-__global__ void __launch_bounds__(128) k_contact_hessian(const S* __restrict__ x, const S* __restrict__ xcs,
+__global__ void __launch_bounds__(128, 3) k_contact_hessian(const S* __restrict__ x, const S* __restrict__ xcs,
                                                          ipcb_contacts L, int n, int offset, double kappa,
                                                          int* __restrict__ rows, int* __restrict__ cols,
                                                          S* __restrict__ vals, S* __restrict__ bforce,

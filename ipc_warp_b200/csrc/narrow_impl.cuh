@@ -40,30 +40,31 @@ IPCB_D void jacobi(T (&a)[N][N], T (&v)[N][N]) {
       for (int j = i + 1; j < N; ++j) off += a[i][j] * a[i][j];
     }
     if (off <= tiny * dg) break;
+    // cyclic sweep of symmetric rotations: each (p, q) rotation updates the
+    // two pivots in closed form, zeroes a_pq, and rotates the other entries
+    // of rows/columns p and q once (a is kept symmetric)
 #pragma unroll
     for (int p = 0; p < N - 1; ++p)
 #pragma unroll
       for (int q = p + 1; q < N; ++q) {
-        T apq = a[p][q];
+        const T apq = a[p][q];
         if (apq != T(0)) {
-          T theta = (a[q][q] - a[p][p]) / (T(2) * apq);
-          T t = (theta >= T(0) ? T(1) : T(-1)) / (fabs(theta) + sqrt(theta * theta + T(1)));
-          T c = T(1) / sqrt(t * t + T(1)), s = t * c;
+          const T theta = (a[q][q] - a[p][p]) / (T(2) * apq);
+          const T t = (theta >= T(0) ? T(1) : T(-1)) / (fabs(theta) + sqrt(theta * theta + T(1)));
+          const T c = T(1) / sqrt(t * t + T(1)), s = t * c;
+          a[p][p] -= t * apq;
+          a[q][q] += t * apq;
+          a[p][q] = a[q][p] = T(0);
 #pragma unroll
           for (int k = 0; k < N; ++k) {
-            T akp = a[k][p], akq = a[k][q];
-            a[k][p] = c * akp - s * akq;
-            a[k][q] = s * akp + c * akq;
+            if (k == p || k == q) continue;
+            const T akp = a[k][p], akq = a[k][q];
+            a[k][p] = a[p][k] = c * akp - s * akq;
+            a[k][q] = a[q][k] = s * akp + c * akq;
           }
 #pragma unroll
           for (int k = 0; k < N; ++k) {
-            T apk = a[p][k], aqk = a[q][k];
-            a[p][k] = c * apk - s * aqk;
-            a[q][k] = s * apk + c * aqk;
-          }
-#pragma unroll
-          for (int k = 0; k < N; ++k) {
-            T vkp = v[k][p], vkq = v[k][q];
+            const T vkp = v[k][p], vkq = v[k][q];
             v[k][p] = c * vkp - s * vkq;
             v[k][q] = s * vkp + c * vkq;
           }
@@ -382,27 +383,30 @@ IPCB_D unsigned write_blocks(const int4 id, int* rows, int* cols, S* vals, long 
     reinterpret_cast<int4*>(rows + base)[ii] = make_int4(vid[ii], vid[ii], vid[ii], vid[ii]);
     reinterpret_cast<int4*>(cols + base)[ii] = make_int4(vid[0], vid[1], vid[2], vid[3]);
   }
+  // one block row (4 blocks, 144 B in float) at a time: w_m h_m[3 ii + a] is
+  // formed once per row component and the staging buffer stays at 36 values,
+  // which keeps the kernel at <= 168 registers (3 CTAs of 128 per SM)
 #pragma unroll
-  for (int half = 0; half < 2; ++half) {
-    S buf[72];
+  for (int ii = 0; ii < 4; ++ii) {
+    S buf[36];
 #pragma unroll
-    for (int i2 = 0; i2 < 2; ++i2) {
-      const int ii = 2 * half + i2;
+    for (int a = 0; a < 3; ++a) {
+      T wh[kMaxH];
+#pragma unroll
+      for (int m = 0; m < kMaxH; ++m) wh[m] = m < nh ? w[m] * h[m][3 * ii + a] : T(0);
 #pragma unroll
       for (int jj = 0; jj < 4; ++jj)
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          T v = T(0);
 #pragma unroll
-          for (int b = 0; b < 3; ++b) {
-            T v = T(0);
-#pragma unroll
-            for (int m = 0; m < kMaxH; ++m)
-              if (m < nh) v += w[m] * h[m][3 * ii + a] * h[m][3 * jj + b];
-            buf[(i2 * 4 + jj) * 9 + 3 * a + b] = S(v);
-            if (S(v) != S(0)) mask |= 1u << (ii * 4 + jj);
-          }
+          for (int m = 0; m < kMaxH; ++m)
+            if (m < nh) v += wh[m] * h[m][3 * jj + b];  // rows m >= nh of h are not set
+          buf[jj * 9 + 3 * a + b] = S(v);
+          if (S(v) != S(0)) mask |= 1u << (ii * 4 + jj);
+        }
     }
-    store16(vals + 9 * base + 72 * half, buf, 72);
+    store16(vals + 9 * base + 36 * ii, buf, 36);
   }
   return mask;
 }
