@@ -617,8 +617,13 @@ class FEMContactSolver(ContactBarrierMixin):
         h2 = self.h * self.h
         s = N.stream_handle()
         ls["x_tmp"].copy_(self.states.x)
-        ls["acc0"].zero_()
-        self._energy_launches(ls["acc0"])
+        if getattr(self, "_ls_cache", False):
+            # inside a step, x is the point the previous search accepted: its
+            # energy terms are the accepted trial's (as the ABD search caches E0)
+            ls["acc0"].copy_(ls["acc"])
+        else:
+            ls["acc0"].zero_()
+            self._energy_launches(ls["acc0"])
         self._ccd_launches(self.states.dx)
         eps = 1.1920928955078125e-7 if self.dtype == torch.float32 else 2.220446049250313e-16
         N.call("ipcb_ls_begin", N.ptr(ls["state"]), N.ptr(self.ccd_toi), fp64, N.ptr(ls["acc0"]), h2, eps, 64,
@@ -639,6 +644,7 @@ class FEMContactSolver(ContactBarrierMixin):
             return self._line_search_host()
         self.stats.energies.append((st.E0, st.E1))
         self.ls_trials = st.it
+        self._ls_cache = bool(getattr(self, "_in_step", False) and st.accepted)
         return st.alpha_accepted if st.accepted else 0.0
 
     def __del__(self):
@@ -680,13 +686,19 @@ class FEMContactSolver(ContactBarrierMixin):
         self._precond = None  # a fresh factor at the first iteration of every step
         if self.boundary is not None:
             self.x_target.copy_(torch.as_tensor(self.boundary(self.time + self.h), dtype=self.dtype))
-        for it in range(self.max_newton):
-            alpha, norm = self.newton_iteration()
-            self.stats.newton_iterations = it + 1
-            self.stats.alphas.append(alpha)
-            self.stats.norms.append(norm)
-            if alpha == 0.0 or norm <= self.vel_tol * self.h:
-                break
+        # the line search may reuse the energy of the point it accepted last
+        # only between iterations of this step (x~ and the targets are fixed)
+        self._in_step, self._ls_cache = True, False
+        try:
+            for it in range(self.max_newton):
+                alpha, norm = self.newton_iteration()
+                self.stats.newton_iterations = it + 1
+                self.stats.alphas.append(alpha)
+                self.stats.norms.append(norm)
+                if alpha == 0.0 or norm <= self.vel_tol * self.h:
+                    break
+        finally:
+            self._in_step, self._ls_cache = False, False
         x = self.states.x
         self.states.xdot.copy_((x - self.states.x0) / self.h)
         self.states.x0.copy_(x)
