@@ -398,9 +398,11 @@ def run_ours(args):
     torch.cuda.synchronize()
     pairs = r.n_ee + r.n_pt
     if args.profile_only:
+        torch.cuda.profiler.start()  # ncu --profile-from-start off captures the K steps only
         for _ in range(args.steps):
             step()
         torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
         return
 
     # ---- device-resident timing: K steps, L2 flushed between steps

@@ -10,11 +10,9 @@
 //      narrow phase's per-record block masks) into a shared-memory hash, sort
 //      the distinct columns, count them
 //   3. scan the counts -> offsets
-//   4. pass B, warp per row: lane k owns the row's distinct columns k, k+32,
-//      ...; the row's quads are staged 32 at a time in shared memory (ids,
-//      masks, 4 blocks) with coalesced vector loads, then every lane walks them
-//      in order and the owner of each block's column adds it, so each sum runs
-//      in input order (deterministic)
+//   4. pass B, warp per row: the row's blocks 32 at a time, sorted by column
+//      within the warp and reduced by segments (shuffles), one shared-memory
+//      add per column and batch; a fixed order, so deterministic
 // A row with more than kHash distinct columns sets IPCB_STATUS_ROW_OVERFLOW
 // (the host then uses the generic assembly).
 #include "common.cuh"
@@ -133,15 +131,15 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_columns(int nrow, const int
   }
 }
 
-IPCB_D void copy36(float* dst, const float* __restrict__ src) {
-#pragma unroll
-  for (int k = 0; k < 36; k += 4) *reinterpret_cast<float4*>(dst + k) = __ldg(reinterpret_cast<const float4*>(src + k));
-}
-IPCB_D void copy36(double* dst, const double* __restrict__ src) {
-#pragma unroll
-  for (int k = 0; k < 36; k += 2) *reinterpret_cast<double2*>(dst + k) = __ldg(reinterpret_cast<const double2*>(src + k));
-}
-
+// pass B, warp per row: the row's sorted columns and one 9-value
+// accumulator per column in shared memory.  The lanes load the row's blocks
+// 32 at a time (block i = quad i / 4, column slot jj = i % 4), each finds its
+// column's position by binary search, the warp sorts the 32 (position, lane)
+// keys (bitonic, shuffles), gathers the values in that order and forms the
+// segment sums of equal positions (shuffle-down scan); the first lane of each
+// segment adds its sum to the column's accumulator.  Every sum runs in a
+// fixed order (batches in input order, within a batch by lane), so the result
+// is deterministic, and each column takes one shared-memory add per batch.
 template <class S>
 __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int* __restrict__ qstart,
                                                             const int* __restrict__ qids, const int* __restrict__ ee,
@@ -151,59 +149,85 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int*
                                                             const int* __restrict__ tmpcols,
                                                             const int* __restrict__ offsets, int* __restrict__ columns,
                                                             S* __restrict__ values) {
-  __shared__ __align__(16) S sv[kWarps][32][36];
-  __shared__ int4 sid[kWarps][32];
-  __shared__ unsigned char smk[kWarps][32];
+  __shared__ int scol[kWarps][kHash];
+  __shared__ S sacc[kWarps][kHash * 9];
+  const unsigned full = 0xffffffffu;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int row = blockIdx.x * kWarps + w;
   if (row >= nrow) return;
   int b = qstart[row], e = qstart[row + 1];
   if (b == e) return;
-  int out = offsets[row], cnt = offsets[row + 1] - out;
-  int own[kOwn];
-  S acc[kOwn][9];
+  const int out = offsets[row], cnt = min(offsets[row + 1] - out, kHash);
+  for (int k = lane; k < cnt; k += 32) {
+    scol[w][k] = tmpcols[4 * b + k];
 #pragma unroll
-  for (int r = 0; r < kOwn; ++r) {
-    int k = r * 32 + lane;
-    own[r] = k < cnt ? tmpcols[4 * b + k] : -1;
-#pragma unroll
-    for (int q = 0; q < 9; ++q) acc[r][q] = S(0);
+    for (int t = 0; t < 9; ++t) sacc[w][9 * k + t] = S(0);
   }
-  for (int base = b; base < e; base += 32) {
-    int i = base + lane;
-    if (i < e) {
-      int q = qids[i];
-      sid[w][lane] = record_ids(ee, n_ee, pt, q >> 2);
-      smk[w][lane] = (unsigned char)((bmask[q >> 2] >> (4 * (q & 3))) & 0xFu);
-      copy36(sv[w][lane], vals + 36LL * q);
-    }
-    __syncwarp();
-    int n = min(32, e - base);
-    for (int k = 0; k < n; ++k) {
-      int4 v = sid[w][k];
-      unsigned m = smk[w][k];
+  __syncwarp();
+  const int nb = 4 * (e - b);
+  constexpr int kNone = kHash;  // sorts after every real position
+  for (int base = 0; base < nb; base += 32) {
+    const int i = base + lane;
+    int pos = kNone;
+    S v[9];
 #pragma unroll
-      for (int jj = 0; jj < 4; ++jj) {
-        if (!((m >> jj) & 1u)) continue;
-        int c = comp(v, jj);
-#pragma unroll
-        for (int r = 0; r < kOwn; ++r)
-          if (own[r] == c) {
-#pragma unroll
-            for (int t = 0; t < 9; ++t) acc[r][t] += sv[w][k][9 * jj + t];
+    for (int t = 0; t < 9; ++t) v[t] = S(0);
+    if (i < nb) {
+      const int q = __ldg(qids + b + (i >> 2)), jj = i & 3;
+      if ((__ldg(bmask + (q >> 2)) >> (4 * (q & 3) + jj)) & 1u) {
+        const int c = comp(record_ids(ee, n_ee, pt, q >> 2), jj);
+        int lo = 0, hi = cnt - 1;
+        while (lo <= hi) {
+          const int mid = (lo + hi) >> 1, x = scol[w][mid];
+          if (x == c) {
+            pos = mid;
+            break;
           }
+          if (x < c) lo = mid + 1;
+          else hi = mid - 1;
+        }
+        if (pos != kNone) {  // absent only when the row overflowed (status set in pass A)
+          const S* src = vals + 36LL * q + 9 * jj;
+#pragma unroll
+          for (int t = 0; t < 9; ++t) v[t] = __ldg(src + t);
+        }
       }
     }
+    // bitonic sort of (pos, lane) over the warp
+    int key = (pos << 5) | lane;
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1)
+#pragma unroll
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        const int other = __shfl_xor_sync(full, key, stride);
+        const bool up = (lane & size) == 0, lower = (lane & stride) == 0;
+        key = (lower == up) ? min(key, other) : max(key, other);
+      }
+    const int src_lane = key & 31, p = key >> 5;
+    S sv[9];
+#pragma unroll
+    for (int t = 0; t < 9; ++t) sv[t] = __shfl_sync(full, v[t], src_lane);
+    // segment sums toward the first lane of each run of equal positions
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const int op = __shfl_down_sync(full, p, off);
+#pragma unroll
+      for (int t = 0; t < 9; ++t) {
+        const S o = __shfl_down_sync(full, sv[t], off);
+        if (lane + off < 32 && op == p) sv[t] += o;
+      }
+    }
+    const int prev = __shfl_up_sync(full, p, 1);
+    if (p != kNone && (lane == 0 || prev != p)) {
+#pragma unroll
+      for (int t = 0; t < 9; ++t) sacc[w][9 * p + t] += sv[t];
+    }
     __syncwarp();
   }
+  for (int k = lane; k < cnt; k += 32) {
+    columns[out + k] = scol[w][k];
 #pragma unroll
-  for (int r = 0; r < kOwn; ++r) {
-    int k = r * 32 + lane;
-    if (k < cnt) {
-      columns[out + k] = own[r];
-#pragma unroll
-      for (int t = 0; t < 9; ++t) values[9LL * (out + k) + t] = acc[r][t];
-    }
+    for (int t = 0; t < 9; ++t) values[9LL * (out + k) + t] = sacc[w][9 * k + t];
   }
 }
 
