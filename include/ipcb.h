@@ -205,7 +205,8 @@ int ipcb_cubic_roots(int n, const double* coef, double x0, double x1, double* ro
  * 2 St. Venant-Kirchhoff (fem/stvk.py); Lame mu, lam.  tets int32[4n].
  * rest: Bm = Dm^-1 (scalar[9n] row-major), W = |det Dm|/6.
  * hessian: 16 triplets per tet at tet*16 + i*4 + j (K_ij, not projected,
- * as the reference) and the nodal forces added to b.  energy += sum W psi(F). */
+ * as the reference; rows and cols may both be null when the caller keeps the
+ * pattern) and the nodal forces added to b.  energy += sum W psi(F). */
 int ipcb_tet_rest(int fp64, const void* xcs, const int* tets, int n_tets, void* Bm, void* W, ipcb_stream s);
 int ipcb_tet_hessian(int material, int fp64, const void* x, const int* tets, int n_tets, const void* Bm, const void* W,
                      double mu, double lam, int* rows, int* cols, void* vals, void* b, ipcb_stream s);
@@ -359,8 +360,8 @@ int ipcb_abd_assemble(const ipcb_abd* abd, double h2, int n_records, int n_ee, c
  * that order, each with the outputs of ipcb_contact_hessian (EE at 0, PT at
  * offset n_ee) and ipcb_tet_hessian (t_rows/t_cols may be null); forces add
  * into `force`.  Work is taken from *queue (zeroed by the call) in tiles of
- * `tile` items per warp; blocks x threads (<= 128, multiple of 32) is the
- * persistent grid. */
+ * `tile` items per warp (a multiple of 32); blocks x threads (<= 128, multiple
+ * of 32) is the persistent grid, with 145 * 32 scalars of shared memory per warp. */
 typedef struct {
   int fp64;
   const void* x;

@@ -28,7 +28,7 @@ class Autotuner:
             try:
                 with open(self._path) as f:
                     data = json.load(f).get(name, {})
-                self.best.update({k: tuple(v) for k, v in data.items()})
+                self.best.update({k: tuple(v) for k, v in data.items() if tuple(v) in self.candidates})
             except (OSError, ValueError):
                 pass
 

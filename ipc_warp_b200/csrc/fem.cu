@@ -33,14 +33,19 @@ __global__ void k_tet_dm(const S* __restrict__ xcs, const int4* __restrict__ tet
   W[e] = fabs(det3(Dm)) / S(6);
 }
 
+// warps per block of k_tet_hessian: each warp stages 32 tets (145 values each)
+template <class S> __host__ __device__ constexpr int tet_warps() { return sizeof(S) == 4 ? 2 : 1; }
+
 template <class S>
-__global__ void __launch_bounds__(128) k_tet_hessian(int mat, const S* __restrict__ x, const int4* __restrict__ tets,
-                                                     int n, const S* __restrict__ Bm, const S* __restrict__ W, S mu,
-                                                     S lam, int* __restrict__ rows, int* __restrict__ cols,
-                                                     S* __restrict__ vals, S* __restrict__ b) {
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n) return;
-  tet_hessian_item<S>(mat, x, tets, e, Bm, W, mu, lam, rows, cols, vals, b);
+__global__ void __launch_bounds__(64) k_tet_hessian(int mat, const S* __restrict__ x, const int4* __restrict__ tets,
+                                                    int n, const S* __restrict__ Bm, const S* __restrict__ W, S mu,
+                                                    S lam, int* __restrict__ rows, int* __restrict__ cols,
+                                                    S* __restrict__ vals, S* __restrict__ b) {
+  __shared__ S sm[tet_warps<S>()][32 * kTetStage];
+  const int w = threadIdx.x >> 5;
+  const int e0 = (blockIdx.x * tet_warps<S>() + w) * 32;
+  if (e0 >= n) return;
+  tet_hessian_warp<S>(mat, x, tets, e0, n, Bm, W, mu, lam, rows, cols, vals, b, sm[w]);
 }
 
 template <class S>
@@ -90,14 +95,15 @@ int ipcb_tet_hessian(int material, int fp64, const void* x, const int* tets, int
                      double mu, double lam, int* rows, int* cols, void* vals, void* b, ipcb_stream s) {
   if (material < 0 || material > 2 || n_tets < 0) return IPCB_E_ARG;
   if (n_tets == 0) return IPCB_OK;
-  if (!x || !tets || !Bm || !W || !rows || !cols || !vals || !b) return IPCB_E_ARG;
-  dim3 g(div_up(n_tets, 128));
+  if (!x || !tets || !Bm || !W || !vals || !b || (!rows != !cols)) return IPCB_E_ARG;
   if (fp64)
-    k_tet_hessian<double><<<g, 128, 0, (cudaStream_t)s>>>(material, (const double*)x, (const int4*)tets, n_tets,
+    k_tet_hessian<double><<<div_up(n_tets, 32 * tet_warps<double>()), 32 * tet_warps<double>(), 0,
+                            (cudaStream_t)s>>>(material, (const double*)x, (const int4*)tets, n_tets,
                                                           (const double*)Bm, (const double*)W, mu, lam, rows, cols,
                                                           (double*)vals, (double*)b);
   else
-    k_tet_hessian<float><<<g, 128, 0, (cudaStream_t)s>>>(material, (const float*)x, (const int4*)tets, n_tets,
+    k_tet_hessian<float><<<div_up(n_tets, 32 * tet_warps<float>()), 32 * tet_warps<float>(), 0,
+                           (cudaStream_t)s>>>(material, (const float*)x, (const int4*)tets, n_tets,
                                                          (const float*)Bm, (const float*)W, (float)mu, (float)lam,
                                                          rows, cols, (float*)vals, (float*)b);
   return check_launch("ipcb_tet_hessian");

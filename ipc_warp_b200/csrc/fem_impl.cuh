@@ -186,12 +186,12 @@ IPCB_D M3<S> load_bm(const S* __restrict__ Bm, int e) {
   return B;
 }
 
-// One tet of tet_kernel_sparse: 16 blocks at e*16 + i*4 + j (rows/cols
-// skipped when null: a fixed pattern knows them), nodal forces into b.
-template <class S>
-IPCB_D void tet_hessian_item(int mat, const S* __restrict__ x, const int4* __restrict__ tets, int e,
-                             const S* __restrict__ Bm, const S* __restrict__ W, S mu, S lam, int* __restrict__ rows,
-                             int* __restrict__ cols, S* __restrict__ vals, S* __restrict__ b) {
+// The 16 blocks of one tet of tet_kernel_sparse, handed to put(q, l, k, v)
+// with q = i*4 + j the block slot, and the nodal forces into b.
+template <class S, class Put>
+IPCB_D void tet_hessian_blocks(int mat, const S* __restrict__ x, const int4* __restrict__ tets, int e,
+                               const S* __restrict__ Bm, const S* __restrict__ W, S mu, S lam, S* __restrict__ b,
+                               Put&& put) {
   int4 t = tets[e];
   const int vid[4] = {t.x, t.y, t.z, t.w};
   v3<S> p0 = load3(x, t.x), p1 = load3(x, t.y), p2 = load3(x, t.z), p3 = load3(x, t.w);
@@ -207,9 +207,7 @@ IPCB_D void tet_hessian_item(int mat, const S* __restrict__ x, const int4* __res
     atomicAdd(b + 3 * vid[i] + 1, f[i].y);
     atomicAdd(b + 3 * vid[i] + 2, f[i].z);
   }
-  long long base = 16LL * e;
   for (int j = 0; j < 4; ++j) {
-    S blk[4][3][3];  // blk[i][l][k]
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       M3<S> dDs = mzero<S>();
@@ -220,23 +218,67 @@ IPCB_D void tet_hessian_item(int mat, const S* __restrict__ x, const int4* __res
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int l = 0; l < 3; ++l) blk[i][l][k] = dH.a[l][i];
+        for (int l = 0; l < 3; ++l) put(i * 4 + j, l, k, dH.a[l][i]);
 #pragma unroll
-      for (int l = 0; l < 3; ++l) blk[3][l][k] = -(dH.a[l][0] + dH.a[l][1] + dH.a[l][2]);
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      long long q = base + i * 4 + j;
-      if (rows) {
-        rows[q] = vid[i];
-        cols[q] = vid[j];
-      }
-#pragma unroll
-      for (int l = 0; l < 3; ++l)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) vals[9 * q + 3 * l + k] = blk[i][l][k];
+      for (int l = 0; l < 3; ++l) put(12 + j, l, k, -(dH.a[l][0] + dH.a[l][1] + dH.a[l][2]));
     }
   }
+}
+
+// One tet: 16 blocks at e*16 + i*4 + j (rows/cols skipped when null: a fixed
+// pattern knows them), nodal forces into b.
+template <class S>
+IPCB_D void tet_hessian_item(int mat, const S* __restrict__ x, const int4* __restrict__ tets, int e,
+                             const S* __restrict__ Bm, const S* __restrict__ W, S mu, S lam, int* __restrict__ rows,
+                             int* __restrict__ cols, S* __restrict__ vals, S* __restrict__ b) {
+  const long long base = 16LL * e;
+  if (rows) {
+    const int4 t = tets[e];
+    const int vid[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      rows[base + q] = vid[q >> 2];
+      cols[base + q] = vid[q & 3];
+    }
+  }
+  S* out = vals + 9 * base;
+  tet_hessian_blocks<S>(mat, x, tets, e, Bm, W, mu, lam, b,
+                        [&](int q, int l, int k, S v) { out[9 * q + 3 * l + k] = v; });
+}
+
+// Shared-memory stride of one tet's 144 values (odd: conflict-free lanes).
+constexpr int kTetStage = 145;
+
+// The 32 lanes of a warp build tets e0 .. e0+31 (those < n) into the warp's
+// stage sm[32 * kTetStage], then write the tets' contiguous 144-value records
+// (and rows/cols) with coalesced stores.  Called by all 32 lanes.
+template <class S>
+IPCB_D void tet_hessian_warp(int mat, const S* __restrict__ x, const int4* __restrict__ tets, int e0, int n,
+                             const S* __restrict__ Bm, const S* __restrict__ W, S mu, S lam, int* __restrict__ rows,
+                             int* __restrict__ cols, S* __restrict__ vals, S* __restrict__ b, S* sm) {
+  const int lane = threadIdx.x & 31;
+  const int e = e0 + lane;
+  if (e < n) {
+    S* mine = sm + lane * kTetStage;
+    tet_hessian_blocks<S>(mat, x, tets, e, Bm, W, mu, lam, b,
+                          [&](int q, int l, int k, S v) { mine[9 * q + 3 * l + k] = v; });
+  }
+  __syncwarp();
+  const int cnt = n - e0 < 32 ? n - e0 : 32;
+  S* dst = vals + 144LL * e0;
+  for (int idx = lane; idx < cnt * 144; idx += 32) {
+    const int te = idx / 144;
+    dst[idx] = sm[te * kTetStage + (idx - te * 144)];
+  }
+  if (rows) {
+    for (int idx = lane; idx < cnt * 16; idx += 32) {
+      const int4 t = tets[e0 + (idx >> 4)];
+      const int vid[4] = {t.x, t.y, t.z, t.w};
+      rows[16LL * e0 + idx] = vid[(idx >> 2) & 3];
+      cols[16LL * e0 + idx] = vid[idx & 3];
+    }
+  }
+  __syncwarp();
 }
 
 }  // namespace

@@ -5,7 +5,8 @@
 // order EE contact records | PT contact records | tets: a warp takes a tile of
 // consecutive items from a global counter (one atomic per tile) and its lanes
 // run the items' device functions (narrow_impl.cuh contact_hessian_item,
-// fem_impl.cuh tet_hessian_item).  Contact counts are read on the device, so
+// fem_impl.cuh tet_hessian_item); a 32-item chunk of tets only goes through a
+// shared-memory stage so its 576-byte block records are stored coalesced.  Contact counts are read on the device, so
 // the launch needs no host synchronisation and can be graph-captured.  Grid,
 // block and tile sizes are picked by the host autotuner.
 //
@@ -32,8 +33,11 @@ IPCB_D int device_count(const ipcb_contacts& L) {
   return c < L.capacity ? c : L.capacity;
 }
 
+// dynamic shared memory: one 32-tet stage per warp
 template <class S>
 __global__ void __launch_bounds__(128) k_terms(ipcb_terms T, int tile) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  S* stage = reinterpret_cast<S*>(dsm) + (threadIdx.x >> 5) * 32 * kTetStage;
   const int lane = threadIdx.x & 31;
   const int n_ee = device_count(T.ee);
   const int n_pt = device_count(T.pt);
@@ -44,9 +48,17 @@ __global__ void __launch_bounds__(128) k_terms(ipcb_terms T, int tile) {
     if (lane == 0) base = atomicAdd(T.queue, tile);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= total) break;
-    for (int k = lane; k < tile; k += 32) {
-      const long long it = (long long)base + k;
-      if (it >= total) break;
+    for (int k0 = 0; k0 < tile; k0 += 32) {
+      const long long c0 = (long long)base + k0;
+      if (c0 >= total) break;
+      if (c0 >= n_c) {  // a chunk of tets only: staged, coalesced block stores
+        tet_hessian_warp<S>(T.material, (const S*)T.x, (const int4*)T.tets, (int)(c0 - n_c), T.n_tets,
+                            (const S*)T.Bm, (const S*)T.W, S(T.mu), S(T.lam), T.t_rows, T.t_cols, (S*)T.t_vals,
+                            (S*)T.force, stage);
+        continue;
+      }
+      const long long it = c0 + lane;
+      if (it >= total) continue;
       if (it < n_ee)
         contact_hessian_item<S, 0>((const S*)T.x, (const S*)T.xcs, T.ee, (int)it, 0, T.kappa, T.c_rows, T.c_cols,
                                    (S*)T.c_vals, (S*)T.force, T.c_mask);
@@ -160,10 +172,17 @@ int ipcb_terms_launch(const ipcb_terms* T, int blocks, int threads, int tile, ip
   if ((T->ee.capacity > 0 || T->pt.capacity > 0) && (!T->c_rows || !T->c_cols || !T->c_vals || !T->xcs))
     return IPCB_E_ARG;
   if (T->material < 0 || T->material > 2) return IPCB_E_ARG;
+  if (tile % 32) return IPCB_E_ARG;
   cudaStream_t st = (cudaStream_t)s;
   cudaMemsetAsync(T->queue, 0, sizeof(int), st);
-  if (T->fp64) k_terms<double><<<blocks, threads, 0, st>>>(*T, tile);
-  else k_terms<float><<<blocks, threads, 0, st>>>(*T, tile);
+  const size_t smem = (size_t)(threads / 32) * 32 * kTetStage * (T->fp64 ? sizeof(double) : sizeof(float));
+  if (T->fp64) {
+    cudaFuncSetAttribute(k_terms<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_terms<double><<<blocks, threads, smem, st>>>(*T, tile);
+  } else {
+    cudaFuncSetAttribute(k_terms<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_terms<float><<<blocks, threads, smem, st>>>(*T, tile);
+  }
   return check_launch("ipcb_terms_launch");
 }
 

@@ -365,12 +365,32 @@ class FEMContactSolver(ContactBarrierMixin):
                             ws=torch.empty(N.size("ipcb_bsr_union_workspace", V), dtype=torch.uint8, device=dev))
         n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
         self._n_sm = n_sm
-        cands = [(bps, th, tile) for (bps, th) in ((1, 128), (2, 128), (2, 64), (4, 64)) for tile in (32, 64, 128, 256)]
+        # schedules: the per-kind kernels back to back, or the one persistent
+        # work-queue launch at a (blocks/SM, threads, tile) shape; the fastest
+        # per workload bucket wins
+        cands = [("separate",)] + [(bps, th, tile) for (bps, th) in ((1, 128), (2, 128), (2, 64), (4, 64))
+                                   for tile in (32, 64, 128, 256)]
         self._tuner = Autotuner("terms", cands)
 
     def _launch_terms(self, cfg, Tc):
+        s = N.stream_handle()
+        if cfg[0] == "separate":
+            n_ee, n_pt = self.n_contacts, self.n_contacts_pt
+            t = self.collision_triplets
+            if n_ee:
+                N.call("ipcb_contact_hessian", 0, ctypes.byref(self.soup.c_struct()),
+                       ctypes.byref(self.contacts_new.c_struct()), n_ee, 0, float(self.contact_stiffness),
+                       N.ptr(t.rows), N.ptr(t.cols), N.ptr(t.vals), N.ptr(self.b), N.ptr(t.mask), s)
+            if n_pt:
+                N.call("ipcb_contact_hessian", 1, ctypes.byref(self.soup.c_struct()),
+                       ctypes.byref(self.contacts_pt.c_struct()), n_pt, n_ee, float(self.contact_stiffness),
+                       N.ptr(t.rows), N.ptr(t.cols), N.ptr(t.vals), N.ptr(self.b), N.ptr(t.mask), s)
+            N.call("ipcb_tet_hessian", self.material, int(self.dtype == torch.float64), N.ptr(self.states.x),
+                   N.ptr(self.tets), self.n_tets, N.ptr(self.Bm), N.ptr(self.W), self.mu, self.lam, None, None,
+                   N.ptr(self._static["tet_vals"]), N.ptr(self.b), s)
+            return
         bps, threads, tile = cfg
-        N.call("ipcb_terms_launch", ctypes.byref(Tc), bps * self._n_sm, threads, tile, N.stream_handle())
+        N.call("ipcb_terms_launch", ctypes.byref(Tc), bps * self._n_sm, threads, tile, s)
 
     def _compute_A_queue(self) -> BsrMatrix:
         """Contact detection, then one persistent launch for the contact

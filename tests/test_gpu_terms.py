@@ -109,3 +109,24 @@ def test_autotuner_records_every_candidate(cuda):
     # a second call with the same workload reuses the choice
     s.compute_A()
     assert len(s._tuner.timings) == 1
+
+
+@pytest.mark.parametrize("cfg", [("separate",), (2, 128, 64), (4, 64, 32)])
+def test_every_schedule_assembles_the_same_matrix(cuda, cfg):
+    """The per-kind kernels and the persistent work-queue launch (with its
+    staged tet chunks) produce the same matrix and force."""
+    sc = small_scenes()[2]
+    rng = np.random.default_rng(11)
+    x = sc.x + rng.normal(scale=0.05 * sc.dhat, size=sc.x.shape)
+    out = []
+    for assembly in ("generic", "queue"):
+        s = _solver(sc, torch.float64, assembly)
+        s.states.x.copy_(torch.tensor(x, dtype=torch.float64))
+        if assembly == "queue":
+            s._static_pattern()
+            s._tuner.pick = lambda key, run, reset: cfg
+        A = s.compute_A()
+        out.append((_dense(A)[0], s.b.cpu().numpy().copy()))
+    (Dg, bg), (Dq, bq) = out
+    assert np.abs(Dq - Dg).max() <= 1e-12 * np.abs(Dg).max()
+    assert np.abs(bq - bg).max() <= 1e-11 * np.abs(bg).max()
