@@ -499,6 +499,7 @@ class FEMContactSolver(ContactBarrierMixin):
 
     def _line_search_host(self) -> float:
         """The reference's loop: energies and the accept test on the host."""
+        self._lists_at_x = False
         x_tmp = self.states.x.clone()
         E0 = self.total_energy()
         ub = self.collision_free_step(self.states.dx)
@@ -522,18 +523,19 @@ class FEMContactSolver(ContactBarrierMixin):
         return alpha
 
     # ------------------------------------------------- device line search
-    def _energy_launches(self, acc: torch.Tensor):
+    def _energy_launches(self, acc: torch.Tensor, detect: bool = True):
         """Launches (no host reads, graph-capturable) that add the energy terms
         at the current x into acc: [0] elastic Psi, [1] barrier, [2] inertia +
-        attachment.  Contact lists are refilled by the DCD; their counts stay
-        on the device."""
+        attachment.  Contact lists are refilled by the DCD (their counts stay
+        on the device), or, with detect=False, taken as they are."""
         s = N.stream_handle()
         fp64 = int(self.dtype == torch.float64)
         kappa = float(self.contact_stiffness)
-        self.update_bvh()
-        self._launch_dcd("ee")
-        if self.has_triangles:
-            self._launch_dcd("pt")
+        if detect:
+            self.update_bvh()
+            self._launch_dcd("ee")
+            if self.has_triangles:
+                self._launch_dcd("pt")
         soup = self.soup.c_struct()
         base = acc.data_ptr()
         N.call("ipcb_contact_energy", 0, ctypes.byref(soup), ctypes.byref(self.contacts_new.c_struct()), -1, kappa,
@@ -642,8 +644,13 @@ class FEMContactSolver(ContactBarrierMixin):
             # energy terms are the accepted trial's (as the ABD search caches E0)
             ls["acc0"].copy_(ls["acc"])
         else:
+            # within newton_iteration, compute_A has just detected the contacts
+            # at this x: E0 uses its lists (the reference detects again, with
+            # the same result)
+            fresh = getattr(self, "_lists_at_x", False)
             ls["acc0"].zero_()
-            self._energy_launches(ls["acc0"])
+            self._energy_launches(ls["acc0"], detect=not fresh)
+        self._lists_at_x = False
         self._ccd_launches(self.states.dx)
         eps = 1.1920928955078125e-7 if self.dtype == torch.float32 else 2.220446049250313e-16
         N.call("ipcb_ls_begin", N.ptr(ls["state"]), N.ptr(self.ccd_toi), fp64, N.ptr(ls["acc0"]), h2, eps, 64,
@@ -691,6 +698,7 @@ class FEMContactSolver(ContactBarrierMixin):
         self.solve()
         if ev:
             ev[3].record()
+        self._lists_at_x = True  # nothing has moved x since compute_A's detection
         alpha = self.line_search()
         if ev:
             ev[4].record()

@@ -98,3 +98,18 @@ def test_newton_steps_with_device_search(cuda):
         assert all(a > 0 for a in st.alphas[:-1])
         assert st.newton_iterations < s.max_newton
     assert torch.isfinite(s.states.x).all()
+
+
+def test_newton_iteration_reuses_detection_for_e0(cuda):
+    """Inside newton_iteration the device search takes E0's contacts from
+    compute_A's detection; E0 and alpha match a search that detects again."""
+    s = _solver(torch.float64, "device")
+    x0 = s.states.x.clone()
+    alpha, _ = s.newton_iteration()
+    e0_reused = s.stats.energies[-1][0]
+    x1 = s.states.x.clone()
+    s.states.x.copy_(x0)
+    s.line_search_mode = "device"
+    alpha2 = s.line_search()  # direct call: detects at x0 again, same direction
+    assert s.stats.energies[-1][0] == pytest.approx(e0_reused, rel=1e-12)
+    assert alpha2 == alpha and torch.equal(s.states.x, x1)
