@@ -369,8 +369,13 @@ class AffineBodyDynamics(ContactBarrierMixin):
             self.stats.pcg_iterations.append(its)
             dq = x
             if (status or not (rel <= 1e-4)) and self.direct_fallback:
-                dq = self._direct()(self.A, self.reduced_b)
-                self.stats.fallbacks += 1
+                from .direct import DirectSolverError
+
+                try:
+                    dq = self._direct()(self.A, self.reduced_b)
+                    self.stats.fallbacks += 1
+                except DirectSolverError:  # indefinite: keep the PCG iterate
+                    self.stats.direct_failures += 1
         self.abd_states.dx.copy_(dq)
         self._vertex_direction()
         return self.abd_states.dx

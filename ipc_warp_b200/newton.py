@@ -50,6 +50,7 @@ class StepStats:
     newton_iterations: int = 0
     pcg_iterations: list = field(default_factory=list)
     fallbacks: int = 0
+    direct_failures: int = 0
     alphas: list = field(default_factory=list)
     energies: list = field(default_factory=list)
     norms: list = field(default_factory=list)
@@ -484,10 +485,24 @@ class FEMContactSolver(ContactBarrierMixin):
                 dx = x.clone()
                 if status:
                     rel = float("nan")
+                    if status & 1:  # p^T A p <= 0: A is indefinite, the Cholesky fallback cannot succeed
+                        self.stats.direct_failures += 1
+                        self.stats.pcg_iterations.append(its)
+                        self.states.dx = dx
+                        return dx
             self.stats.pcg_iterations.append(its)
             if not (rel <= self.tol) and self.direct_fallback:
-                dx = self._direct()(self.A, self.rhs)
-                self.stats.fallbacks += 1
+                from .direct import DirectSolverError
+
+                try:
+                    dx = self._direct()(self.A, self.rhs)
+                    self.stats.fallbacks += 1
+                except DirectSolverError:
+                    # the Cholesky stand-in needs a positive definite matrix; an
+                    # indefinite one (unprojected elastic Hessian under
+                    # compression) keeps the PCG iterate, as the reference's cg
+                    # returns its last iterate; the line search then tests descent
+                    self.stats.direct_failures += 1
         self.states.dx = dx
         return dx
 
