@@ -365,6 +365,22 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def max_over_ranks(values, device):
+    """Per-rank device timings (ms) -> their maxima over the process group
+    (the slowest replica sets the whole job's time)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
+def job_throughput(world: int, pairs: int, steps: int, total_ms: float) -> float:
+    """Whole-job pairs/s of N replicas that each processed `pairs` per step."""
+    return world * pairs * steps / (total_ms * 1e-3)
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -448,9 +464,7 @@ def run_ours(args):
     d2h = bh.numel() * 4 + 8 + 4 + 8  # force, energy, toi, counts
 
     if world > 1:
-        t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, e2e_ms = float(t[0]), float(t[1])
+        total_ms, e2e_ms = max_over_ranks([total_ms, e2e_ms], dev)
 
     # ---- roofline of the dominant kernel and kernel count (rank 0, untimed)
     out = None
@@ -468,7 +482,7 @@ def run_ours(args):
         ms = total_ms / args.steps
         out = {
             "metric": METRIC,
-            "value": world * pairs * args.steps / (total_ms * 1e-3),
+            "value": job_throughput(world, pairs, args.steps, total_ms),
             "unit": "pairs/s",
             "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -484,7 +498,7 @@ def run_ours(args):
             "cpu_baseline": {"value": cpu_pairs / cpu_sec, "unit": "pairs/s", "cores": os.cpu_count(),
                              "kind": "port",
                              "sample": "full workload, 3 passes of the C++ oracle pipeline (DCD+narrow+energy+CCD)"},
-            "e2e": {"value": world * pairs * args.steps / (e2e_ms * 1e-3), "unit": "pairs/s",
+            "e2e": {"value": job_throughput(world, pairs, args.steps, e2e_ms), "unit": "pairs/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": n_launch * args.steps,
             "kernels": names,
