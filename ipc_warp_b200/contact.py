@@ -153,7 +153,7 @@ class ContactSolverBase:
         self.n_contacts = 0
         self.n_contacts_pt = 0
         self._status = torch.zeros(1, dtype=torch.int32, device=dev)
-        # CCD candidate staging (pairs beyond capacity are still solved, inline)
+        # CCD candidate staging (a query that overflows it is redone inline)
         cap = max(1 << 20, 4 * max(n_edges, n_nodes))
         self._toi_ws = torch.empty(N.size("ipcb_toi_workspace", cap), dtype=torch.uint8, device=dev)
         self._counts_host = torch.zeros(2, dtype=torch.int32).pin_memory() if dev.type == "cuda" else None

@@ -334,11 +334,13 @@ __global__ void k_swept(const S* __restrict__ x0, const S* __restrict__ x1, cons
 
 // Candidate pairs are staged in a list so the cubic solves run one pair per
 // thread (balanced) instead of inside divergent traversal loops.  Workspace:
-// [count int32 | pad to 256 B | int2 pairs[capacity]].  A pair that finds
-// the list full is solved in the traversal thread, so the result never
+// [count int32 | overflow int32 | pad to 256 B | int2 pairs[capacity]].  When
+// a pair finds the list full the overflow flag is raised and an inline pass
+// solves every pair of the query during traversal, so the result never
 // depends on the capacity.
 struct CandList {
   int* count;
+  int* overflow;  // set by a collect pass that dropped pairs (the inline pass then redoes the query)
   int2* pairs;
   int capacity;
 };
@@ -480,12 +482,20 @@ IPCB_D bool push_converged(const CandList& L, bool has, int a, int b) {
 
 // Traversal applies the cheap filters and queues leaves; the warp then pushes
 // the queued pairs converged (divergent pushes would serialise on the count).
-template <class S>
+// FAST: stage pairs only (a lane whose queue is full pushes on its own); a
+// pair that does not fit in the list raises cand.overflow instead of being
+// solved here, which keeps the cubic solver out of this kernel (48 instead of
+// 255 registers).  !FAST (run only
+// when *gate is set, with a zero-capacity list): every pair solved in place.
+template <class S, bool FAST>
 __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, const S* __restrict__ x1,
                                                     const int* __restrict__ edges, const int* __restrict__ body,
                                                     const float4* __restrict__ nodes, const int* __restrict__ order,
                                                     int n, const float* __restrict__ lo, const float* __restrict__ hi,
-                                                    int exclude, CandList cand, S* toi, int* status, Sink sink) {
+                                                    int exclude, CandList cand, S* toi, int* status, Sink sink,
+                                                    const int* gate) {
+  if (gate && *gate == 0) return;
+  bool dropped = false;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   bool active = t < n;
   int i = active ? __ldg(order + t) : 0;
@@ -504,6 +514,10 @@ __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, co
       if (exclude && bi == __ldg(body + eb.x)) return;
       if (nq < kQueue) {
         q[nq++] = j;
+      } else if (FAST) {  // lane queue full: stage this pair directly
+        const int slot = atomicAdd(cand.count, 1);
+        if (slot < cand.capacity) cand.pairs[slot] = make_int2(i, j);
+        else dropped = true;
       } else {
         double tt = ee_pair_time(x0, x1, ea, eb, st);
         if (tt < 1.0) {
@@ -519,6 +533,10 @@ __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, co
     bool has = k < nq;
     int j = has ? q[k] : 0;
     if (!push_converged(cand, has, i, j)) {
+      if (FAST) {
+        dropped = true;
+        continue;
+      }
       int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + j);
       double tt = ee_pair_time(x0, x1, ea, eb, st);
       if (tt < 1.0) {
@@ -527,14 +545,18 @@ __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, co
       }
     }
   }
+  if (dropped) *cand.overflow = 1;
   if (st) atomicOr(status, st);
 }
 
-template <class S>
+template <class S, bool FAST>
 __global__ void __launch_bounds__(128) k_pt_collect(const S* __restrict__ x0, const S* __restrict__ x1,
                                                     const int* __restrict__ tris, const int* __restrict__ body,
                                                     const float4* __restrict__ nodes, int n_tris, int nv, double pad,
-                                                    int exclude, CandList cand, S* toi, int* status, Sink sink) {
+                                                    int exclude, CandList cand, S* toi, int* status, Sink sink,
+                                                    const int* gate) {
+  if (gate && *gate == 0) return;
+  bool dropped = false;
   int i0 = blockIdx.x * blockDim.x + threadIdx.x;
   bool active = i0 < nv;
   int i = active ? i0 : 0;
@@ -554,6 +576,10 @@ __global__ void __launch_bounds__(128) k_pt_collect(const S* __restrict__ x0, co
       if (exclude && bi == __ldg(body + tj.x)) return;
       if (nq < kQueue) {
         q[nq++] = j;
+      } else if (FAST) {  // lane queue full: stage this pair directly
+        const int slot = atomicAdd(cand.count, 1);
+        if (slot < cand.capacity) cand.pairs[slot] = make_int2(i, j);
+        else dropped = true;
       } else {
         double tt = pt_pair_time(x0, x1, i, tj, st);
         if (tt < 1.0) {
@@ -569,6 +595,10 @@ __global__ void __launch_bounds__(128) k_pt_collect(const S* __restrict__ x0, co
     bool has = k < nq;
     int j = has ? q[k] : 0;
     if (!push_converged(cand, has, i, j)) {
+      if (FAST) {
+        dropped = true;
+        continue;
+      }
       int3 tj = make_int3(__ldg(tris + 3 * j), __ldg(tris + 3 * j + 1), __ldg(tris + 3 * j + 2));
       double tt = pt_pair_time(x0, x1, i, tj, st);
       if (tt < 1.0) {
@@ -577,6 +607,7 @@ __global__ void __launch_bounds__(128) k_pt_collect(const S* __restrict__ x0, co
       }
     }
   }
+  if (dropped) *cand.overflow = 1;
   if (st) atomicOr(status, st);
 }
 
@@ -584,7 +615,8 @@ __global__ void __launch_bounds__(128) k_pt_collect(const S* __restrict__ x0, co
 template <class S, int KIND>
 __global__ void __launch_bounds__(128) k_cand_toi(const S* __restrict__ x0, const S* __restrict__ x1,
                                                   const int* __restrict__ prims, CandList cand, S* toi,
-                                                  int* status, Sink sink) {
+                                                  int* status, Sink sink, const int* skip_if) {
+  if (skip_if && *skip_if) return;  // the inline pass redoes every pair
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   int n = min(*cand.count, cand.capacity);
   if (k >= n) return;
@@ -813,6 +845,7 @@ __global__ void __launch_bounds__(128) k_fixed_pt_collect(const S* __restrict__ 
 inline CandList cand_list(void* ws, size_t ws_bytes) {
   CandList c;
   c.count = (int*)ws;
+  c.overflow = (int*)ws + 1;
   c.pairs = (int2*)((char*)ws + 256);
   size_t cap = ws_bytes > 256 ? (ws_bytes - 256) / sizeof(int2) : 0;
   c.capacity = cap > 0x7fffffff ? 0x7fffffff : (int)cap;
@@ -846,6 +879,47 @@ __global__ void k_cubic(int n, const double* __restrict__ coef, double x0, doubl
   roots[3 * i + 1] = r[1];
   roots[3 * i + 2] = r[2];
   if (st) atomicOr(status, st);
+}
+
+// The CCD query of one kind: a staging-only collect pass, the per-candidate
+// TOI pass, and (only when the first pass dropped pairs) an inline pass that
+// solves every pair of the query in place.
+template <class S>
+void run_ee(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, const float* lower, const float* upper,
+            int exclude, CandList c, void* toi, int* status, Sink sink, cudaStream_t st) {
+  const int n = soup->n_edges;
+  const dim3 g(div_up(n, 128)), gc(div_up(c.capacity > 0 ? c.capacity : 1, 128));
+  cudaMemsetAsync(c.count, 0, 2 * sizeof(int), st);
+  k_ee_collect<S, true><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->edges, soup->body,
+                                           (const float4*)bvh->wide, bvh->sorted, n, lower, upper, exclude, c,
+                                           (S*)toi, status, sink, nullptr);
+  if (c.capacity)
+    k_cand_toi<S, 0><<<gc, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->edges, c, (S*)toi, status, sink,
+                                         c.overflow);
+  CandList none = c;
+  none.capacity = 0;
+  k_ee_collect<S, false><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->edges, soup->body,
+                                            (const float4*)bvh->wide, bvh->sorted, n, lower, upper, exclude, none,
+                                            (S*)toi, status, sink, c.overflow);
+}
+
+template <class S>
+void run_pt(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, double pad, int exclude, CandList c,
+            void* toi, int* status, Sink sink, cudaStream_t st) {
+  const int nv = soup->n_verts;
+  const dim3 g(div_up(nv, 128)), gc(div_up(c.capacity > 0 ? c.capacity : 1, 128));
+  cudaMemsetAsync(c.count, 0, 2 * sizeof(int), st);
+  k_pt_collect<S, true><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->triangles, soup->body,
+                                           (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude, c, (S*)toi,
+                                           status, sink, nullptr);
+  if (c.capacity)
+    k_cand_toi<S, 1><<<gc, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->triangles, c, (S*)toi, status, sink,
+                                         c.overflow);
+  CandList none = c;
+  none.capacity = 0;
+  k_pt_collect<S, false><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->triangles, soup->body,
+                                            (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude, none, (S*)toi,
+                                            status, sink, c.overflow);
 }
 
 }  // namespace
@@ -904,27 +978,10 @@ int ipcb_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* b
   if (!soup || !x1 || !bvh || !lower || !upper || !toi || !status || !ws || ws_bytes < 256 ||
       bvh->n != soup->n_edges)
     return IPCB_E_ARG;
-  int n = soup->n_edges;
-  if (n == 0) return IPCB_OK;
-  cudaStream_t st = (cudaStream_t)s;
-  CandList c = cand_list(ws, ws_bytes);
-  cudaMemsetAsync(c.count, 0, sizeof(int), st);
-  dim3 g(div_up(n, 128)), gc(div_up(c.capacity > 0 ? c.capacity : 1, 128));
-  if (soup->fp64) {
-    k_ee_collect<double><<<g, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, soup->body,
-                                            (const float4*)bvh->wide, bvh->sorted, n, lower, upper,
-                                            exclude_same_body, c, (double*)toi, status, Sink{});
-    if (c.capacity)
-      k_cand_toi<double, 0><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, c,
-                                                (double*)toi, status, Sink{});
-  } else {
-    k_ee_collect<float><<<g, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, soup->body,
-                                           (const float4*)bvh->wide, bvh->sorted, n, lower, upper,
-                                           exclude_same_body, c, (float*)toi, status, Sink{});
-    if (c.capacity)
-      k_cand_toi<float, 0><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, c,
-                                               (float*)toi, status, Sink{});
-  }
+  if (soup->n_edges == 0) return IPCB_OK;
+  const CandList c = cand_list(ws, ws_bytes);
+  if (soup->fp64) run_ee<double>(soup, x1, bvh, lower, upper, exclude_same_body, c, toi, status, Sink{}, (cudaStream_t)s);
+  else run_ee<float>(soup, x1, bvh, lower, upper, exclude_same_body, c, toi, status, Sink{}, (cudaStream_t)s);
   return check_launch("ipcb_edge_edge_toi");
 }
 
@@ -933,27 +990,10 @@ int ipcb_point_triangle_toi(const ipcb_soup* soup, const void* x1, const ipcb_lb
                             ipcb_stream s) {
   if (!soup || !x1 || !bvh || !toi || !status || !ws || ws_bytes < 256 || bvh->n != soup->n_tris)
     return IPCB_E_ARG;
-  int nv = soup->n_verts;
-  if (nv == 0 || soup->n_tris == 0) return IPCB_OK;
-  cudaStream_t st = (cudaStream_t)s;
-  CandList c = cand_list(ws, ws_bytes);
-  cudaMemsetAsync(c.count, 0, sizeof(int), st);
-  dim3 g(div_up(nv, 128)), gc(div_up(c.capacity > 0 ? c.capacity : 1, 128));
-  if (soup->fp64) {
-    k_pt_collect<double><<<g, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, soup->body,
-                                            (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude_same_body, c,
-                                            (double*)toi, status, Sink{});
-    if (c.capacity)
-      k_cand_toi<double, 1><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, c,
-                                                (double*)toi, status, Sink{});
-  } else {
-    k_pt_collect<float><<<g, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, soup->body,
-                                           (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude_same_body, c,
-                                           (float*)toi, status, Sink{});
-    if (c.capacity)
-      k_cand_toi<float, 1><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, c,
-                                               (float*)toi, status, Sink{});
-  }
+  if (soup->n_verts == 0 || soup->n_tris == 0) return IPCB_OK;
+  const CandList c = cand_list(ws, ws_bytes);
+  if (soup->fp64) run_pt<double>(soup, x1, bvh, pad, exclude_same_body, c, toi, status, Sink{}, (cudaStream_t)s);
+  else run_pt<float>(soup, x1, bvh, pad, exclude_same_body, c, toi, status, Sink{}, (cudaStream_t)s);
   return check_launch("ipcb_point_triangle_toi");
 }
 
@@ -964,28 +1004,11 @@ int ipcb_edge_edge_intersections(const ipcb_soup* soup, const void* x1, const ip
       bvh->n != soup->n_edges)
     return IPCB_E_ARG;
   if (out->capacity > 0 && (!out->a1a2b1b2 || !out->e0e1 || !out->l0 || !out->alpha || !out->lam)) return IPCB_E_ARG;
-  int n = soup->n_edges;
-  if (n == 0) return IPCB_OK;
-  cudaStream_t st = (cudaStream_t)s;
-  CandList c = cand_list(ws, ws_bytes);
-  cudaMemsetAsync(c.count, 0, sizeof(int), st);
+  if (soup->n_edges == 0) return IPCB_OK;
+  const CandList c = cand_list(ws, ws_bytes);
   const Sink sink{*out, thickness * 2.0, 1};
-  dim3 g(div_up(n, 128)), gc(div_up(c.capacity > 0 ? c.capacity : 1, 128));
-  if (soup->fp64) {
-    k_ee_collect<double><<<g, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, soup->body,
-                                            (const float4*)bvh->wide, bvh->sorted, n, lower, upper,
-                                            exclude_same_body, c, (double*)toi, status, sink);
-    if (c.capacity)
-      k_cand_toi<double, 0><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, c,
-                                                (double*)toi, status, sink);
-  } else {
-    k_ee_collect<float><<<g, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, soup->body,
-                                           (const float4*)bvh->wide, bvh->sorted, n, lower, upper,
-                                           exclude_same_body, c, (float*)toi, status, sink);
-    if (c.capacity)
-      k_cand_toi<float, 0><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, c,
-                                               (float*)toi, status, sink);
-  }
+  if (soup->fp64) run_ee<double>(soup, x1, bvh, lower, upper, exclude_same_body, c, toi, status, sink, (cudaStream_t)s);
+  else run_ee<float>(soup, x1, bvh, lower, upper, exclude_same_body, c, toi, status, sink, (cudaStream_t)s);
   return check_launch("ipcb_edge_edge_intersections");
 }
 
@@ -996,28 +1019,11 @@ int ipcb_point_triangle_intersections(const ipcb_soup* soup, const void* x1, con
       bvh->n != soup->n_tris)
     return IPCB_E_ARG;
   if (out->capacity > 0 && (!out->a1a2b1b2 || !out->e0e1 || !out->l0 || !out->alpha || !out->lam)) return IPCB_E_ARG;
-  int nv = soup->n_verts;
-  if (nv == 0 || soup->n_tris == 0) return IPCB_OK;
-  cudaStream_t st = (cudaStream_t)s;
-  CandList c = cand_list(ws, ws_bytes);
-  cudaMemsetAsync(c.count, 0, sizeof(int), st);
+  if (soup->n_verts == 0 || soup->n_tris == 0) return IPCB_OK;
+  const CandList c = cand_list(ws, ws_bytes);
   const Sink sink{*out, thickness * 2.0, 1};
-  dim3 g(div_up(nv, 128)), gc(div_up(c.capacity > 0 ? c.capacity : 1, 128));
-  if (soup->fp64) {
-    k_pt_collect<double><<<g, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, soup->body,
-                                            (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude_same_body, c,
-                                            (double*)toi, status, sink);
-    if (c.capacity)
-      k_cand_toi<double, 1><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, c,
-                                                (double*)toi, status, sink);
-  } else {
-    k_pt_collect<float><<<g, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, soup->body,
-                                           (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude_same_body, c,
-                                           (float*)toi, status, sink);
-    if (c.capacity)
-      k_cand_toi<float, 1><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, c,
-                                               (float*)toi, status, sink);
-  }
+  if (soup->fp64) run_pt<double>(soup, x1, bvh, pad, exclude_same_body, c, toi, status, sink, (cudaStream_t)s);
+  else run_pt<float>(soup, x1, bvh, pad, exclude_same_body, c, toi, status, sink, (cudaStream_t)s);
   return check_launch("ipcb_point_triangle_intersections");
 }
 
@@ -1079,13 +1085,13 @@ int ipcb_fixed_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_b
                                                      fixed, (const int2*)pairs, pad, c, (double*)toi, status);
     if (c.capacity)
       k_cand_toi<double, 0><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, c,
-                                              (double*)toi, status, Sink{});
+                                              (double*)toi, status, Sink{}, nullptr);
   } else {
     k_fixed_ee_collect<float><<<grid, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, *B, fixed,
                                                     (const int2*)pairs, pad, c, (float*)toi, status);
     if (c.capacity)
       k_cand_toi<float, 0><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->edges, c, (float*)toi,
-                                             status, Sink{});
+                                             status, Sink{}, nullptr);
   }
   return check_launch("ipcb_fixed_edge_edge_toi");
 }
@@ -1106,13 +1112,13 @@ int ipcb_fixed_point_triangle_toi(const ipcb_soup* soup, const void* x1, const i
                                                      (const int2*)pairs, pad, c, (double*)toi, status);
     if (c.capacity)
       k_cand_toi<double, 1><<<gc, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, c,
-                                              (double*)toi, status, Sink{});
+                                              (double*)toi, status, Sink{}, nullptr);
   } else {
     k_fixed_pt_collect<float><<<grid, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, *B,
                                                     (const int2*)pairs, pad, c, (float*)toi, status);
     if (c.capacity)
       k_cand_toi<float, 1><<<gc, 128, 0, st>>>((const float*)soup->x, (const float*)x1, soup->triangles, c,
-                                             (float*)toi, status, Sink{});
+                                             (float*)toi, status, Sink{}, nullptr);
   }
   return check_launch("ipcb_fixed_point_triangle_toi");
 }

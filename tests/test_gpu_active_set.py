@@ -133,3 +133,20 @@ def test_active_set_create_and_merge(cuda, dtype):
     A.merge(B)
     ref = al.merge(old_keys, old_gamma, new_keys, A.hash.table_size)
     assert _bucket_keys(A.hash) == ref
+
+
+def test_new_intersections_with_a_small_candidate_list(cuda):
+    """The in-place pass (taken when staged candidates overflow) appends each
+    colliding pair once, as the staged pass does."""
+    sc = small_scenes()[0]
+    s = _solver(sc, torch.float64)
+    x0 = torch.tensor(sc.x, dtype=torch.float64, device=cuda)
+    x1 = torch.tensor(_motion(sc, 3), dtype=torch.float64, device=cuda)
+    a_full = s.new_intersections(x0, x1)
+    ee_full, _ = _records(s.contacts_new, s.n_contacts)
+    pt_full, _ = _records(s.contacts_pt, s.n_contacts_pt)
+    s._toi_ws = torch.empty(256 + 8 * 8, dtype=torch.uint8, device=cuda)
+    a_small = s.new_intersections(x0, x1)
+    assert a_small == a_full
+    assert np.array_equal(_records(s.contacts_new, s.n_contacts)[0], ee_full)
+    assert np.array_equal(_records(s.contacts_pt, s.n_contacts_pt)[0], pt_full)

@@ -97,3 +97,24 @@ def test_no_motion_gives_one(cuda):
     s = make_solver(sc)
     alpha = s.collision_free_step(torch.zeros_like(s.soup.x_transformed))
     assert alpha == 1.0
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_small_candidate_list_gives_the_same_toi(cuda, fp64):
+    """Candidates that do not fit the staging list send the query to the
+    in-place pass: the bound does not depend on the workspace size."""
+    sc = small_scenes()[1]
+    dtype = torch.float64 if fp64 else torch.float32
+    s = make_solver(sc, dtype)
+    rng = np.random.default_rng(5)
+    dx = np.zeros_like(sc.x)
+    dx[sc.body == 1] += np.array([0.0, 4.0, 0.0]) * sc.dhat
+    dx += rng.normal(scale=0.3 * sc.dhat, size=dx.shape)
+    dxt = torch.tensor(dx, dtype=dtype, device=cuda)
+    full = s.collision_free_step(dxt)
+    toi_full = float(s.ccd_toi.item())
+    s._toi_ws = torch.empty(256 + 8 * 16, dtype=torch.uint8, device=cuda)  # 16 staged pairs
+    small = s.collision_free_step(dxt)
+    assert float(s.ccd_toi.item()) == toi_full and small == full
+    s._toi_ws = torch.empty(256, dtype=torch.uint8, device=cuda)  # nothing staged
+    assert s.collision_free_step(dxt) == full
