@@ -5,26 +5,31 @@
 // a record by row; here the unit is a (record, slot ii) quad: one row
 // (vertex ii of the record) and 4 consecutive blocks (columns = the record's 4
 // vertices).  A row's distinct columns are few (tens), so:
-//   1. key every quad by its row; stable radix sort (order = (row, quad id))
-//   2. pass A, warp per row: insert the columns of the non-zero blocks (the
-//      narrow phase's per-record block masks) into a shared-memory hash, sort
-//      the distinct columns, count them
+//   1. thread per record: count the quads of each row and take each quad's
+//      arrival slot in its row (atomics); scan the counts; scatter the quad
+//      ids to their rows (arrival order)
+//   2. pass A, warp per row: sort the row's quad ids (so the order, and every
+//      sum below, is the same on every run), insert the columns of the
+//      non-zero blocks (the narrow phase's per-record block masks) into a
+//      shared-memory hash, sort the distinct columns, count them, and store
+//      each quad's 4 column positions (one byte each)
 //   3. scan the counts -> offsets
 //   4. pass B, warp per row: the row's blocks 32 at a time, sorted by column
-//      within the warp and reduced by segments (shuffles), one shared-memory
-//      add per column and batch; a fixed order, so deterministic
-// A row with more than kHash distinct columns sets IPCB_STATUS_ROW_OVERFLOW
-// (the host then uses the generic assembly).
+//      position within the warp and reduced by segments (shuffles), one
+//      shared-memory add per column and batch; a fixed order, so deterministic
+// A row with more than kHash distinct columns or more than kMaxQuads quads
+// sets IPCB_STATUS_ROW_OVERFLOW (the host then uses the generic assembly).
 #include "common.cuh"
 #include "scan.cuh"
-#include "sort.cuh"
 
 namespace ipcb {
 int check_launch(const char* where);
 
 namespace {
 
-constexpr int kHash = 128;     // distinct columns per row handled by one warp
+constexpr int kHash = 128;        // distinct columns per row handled by one warp
+constexpr int kMaxQuads = 1024;   // quads per row sorted in one warp's shared memory
+constexpr unsigned kAbsent = 0xffu;  // column position of a zero block
 constexpr int kOwn = kHash / 32;
 constexpr int kWarps = 4;
 
@@ -35,15 +40,46 @@ IPCB_D int4 record_ids(const int* __restrict__ ee, int n_ee, const int* __restri
 }
 IPCB_D int comp(int4 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
 
-__global__ void k_quad_keys(int nq, const int* __restrict__ ee, int n_ee, const int* __restrict__ pt,
-                            unsigned* __restrict__ keys, int* __restrict__ ids, int* __restrict__ row_cnt) {
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nq) return;
-  int4 v = record_ids(ee, n_ee, pt, q >> 2);
-  int row = comp(v, q & 3);
-  keys[q] = (unsigned)row;
-  ids[q] = q;
-  atomicAdd(row_cnt + row, 1);
+__global__ void k_rec_slots(int n_rec, const int* __restrict__ ee, int n_ee, const int* __restrict__ pt,
+                            int4* __restrict__ slots, int* __restrict__ row_cnt) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_rec) return;
+  const int4 v = record_ids(ee, n_ee, pt, p);
+  int4 s;
+  s.x = atomicAdd(row_cnt + v.x, 1);
+  s.y = atomicAdd(row_cnt + v.y, 1);
+  s.z = atomicAdd(row_cnt + v.z, 1);
+  s.w = atomicAdd(row_cnt + v.w, 1);
+  slots[p] = s;
+}
+
+__global__ void k_rec_scatter(int n_rec, const int* __restrict__ ee, int n_ee, const int* __restrict__ pt,
+                              const int4* __restrict__ slots, const int* __restrict__ qstart, int* __restrict__ qids) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_rec) return;
+  const int4 v = record_ids(ee, n_ee, pt, p), s = slots[p];
+  qids[qstart[v.x] + s.x] = 4 * p;
+  qids[qstart[v.y] + s.y] = 4 * p + 1;
+  qids[qstart[v.z] + s.z] = 4 * p + 2;
+  qids[qstart[v.w] + s.w] = 4 * p + 3;
+}
+
+// ascending bitonic sort of a[0, n) in one warp's shared memory, n a power of two
+IPCB_D void warp_sort(int* a, int n, int lane) {
+  for (int sz = 2; sz <= n; sz <<= 1)
+    for (int st = sz >> 1; st > 0; st >>= 1) {
+      for (int i = lane; i < n; i += 32) {
+        const int l = i ^ st;
+        if (l > i) {
+          const int x = a[i], y = a[l];
+          if ((x > y) == ((i & sz) == 0)) {
+            a[i] = y;
+            a[l] = x;
+          }
+        }
+      }
+      __syncwarp();
+    }
 }
 
 // insert c into the warp's open-addressing table (keys -1 = empty)
@@ -58,27 +94,37 @@ IPCB_D bool hash_insert(int* tab, int c) {
 }
 
 __global__ void __launch_bounds__(kWarps * 32) k_row_columns(int nrow, const int* __restrict__ qstart,
-                                                             const int* __restrict__ qids, const int* __restrict__ ee,
+                                                             int* __restrict__ qids, const int* __restrict__ ee,
                                                              int n_ee, const int* __restrict__ pt,
                                                              const unsigned short* __restrict__ bmask,
-                                                             int* __restrict__ tmpcols, int* __restrict__ row_nnz,
-                                                             int* __restrict__ status) {
+                                                             int* __restrict__ tmpcols, unsigned* __restrict__ qpos,
+                                                             int* __restrict__ row_nnz, int* __restrict__ status) {
   __shared__ int tab[kWarps][kHash];
+  __shared__ int sq[kWarps][kMaxQuads];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int row = blockIdx.x * kWarps + w;
   if (row >= nrow) return;
-  int b = qstart[row], e = qstart[row + 1];
-  if (b == e) {
-    if (lane == 0) row_nnz[row] = 0;
+  const int b = qstart[row], n = qstart[row + 1] - b;
+  if (n == 0 || n > kMaxQuads) {
+    if (lane == 0) {
+      row_nnz[row] = 0;
+      if (n) atomicOr(status, IPCB_STATUS_ROW_OVERFLOW);
+    }
     return;
   }
+  // the row's quads in quad-id order
+  int nq2 = 32;
+  while (nq2 < n) nq2 <<= 1;
+  for (int k = lane; k < nq2; k += 32) sq[w][k] = k < n ? qids[b + k] : 0x7fffffff;
   for (int k = lane; k < kHash; k += 32) tab[w][k] = -1;
   __syncwarp();
+  warp_sort(sq[w], nq2, lane);
+  for (int k = lane; k < n; k += 32) qids[b + k] = sq[w][k];
   bool ok = true;
-  for (int i = b + lane; i < e; i += 32) {
-    int q = qids[i];
-    int4 v = record_ids(ee, n_ee, pt, q >> 2);
-    unsigned m = (bmask[q >> 2] >> (4 * (q & 3))) & 0xFu;  // blocks (ii, jj = 0..3)
+  for (int k = lane; k < n; k += 32) {
+    const int q = sq[w][k];
+    const int4 v = record_ids(ee, n_ee, pt, q >> 2);
+    const unsigned m = (__ldg(bmask + (q >> 2)) >> (4 * (q & 3))) & 0xFu;  // blocks (ii, jj = 0..3)
 #pragma unroll
     for (int jj = 0; jj < 4; ++jj)
       if ((m >> jj) & 1u) ok &= hash_insert(tab[w], comp(v, jj));
@@ -107,23 +153,35 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_columns(int nrow, const int
   __syncwarp();
   int P = 1;
   while (P < cnt) P <<= 1;
-  for (int sz = 2; sz <= P; sz <<= 1)
-    for (int st = sz >> 1; st > 0; st >>= 1) {
-      for (int i = lane; i < P; i += 32) {
-        int l = i ^ st;
-        if (l > i) {
-          int a = tab[w][i], c = tab[w][l];
-          bool up = (i & sz) == 0;
-          if ((a > c) == up) {
-            tab[w][i] = c;
-            tab[w][l] = a;
+  warp_sort(tab[w], P, lane);
+  // each quad's 4 column positions (kAbsent for a zero block, or for a column
+  // lost to an overflowing table)
+  for (int k = lane; k < n; k += 32) {
+    const int q = sq[w][k];
+    const int4 v = record_ids(ee, n_ee, pt, q >> 2);
+    const unsigned m = (__ldg(bmask + (q >> 2)) >> (4 * (q & 3))) & 0xFu;
+    unsigned packed = 0;
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      unsigned pos = kAbsent;
+      if ((m >> jj) & 1u) {
+        const int c = comp(v, jj);
+        int lo = 0, hi = cnt - 1;
+        while (lo <= hi) {
+          const int mid = (lo + hi) >> 1, x = tab[w][mid];
+          if (x == c) {
+            pos = (unsigned)mid;
+            break;
           }
+          if (x < c) lo = mid + 1;
+          else hi = mid - 1;
         }
       }
-      __syncwarp();
+      packed |= pos << (8 * jj);
     }
-  int base4 = 4 * b;  // the row may use up to 4 columns per quad
-  for (int k = lane; k < cnt; k += 32) tmpcols[base4 + k] = tab[w][k];
+    qpos[b + k] = packed;
+  }
+  for (int k = lane; k < cnt; k += 32) tmpcols[4LL * b + k] = tab[w][k];
   unsigned bad = __ballot_sync(0xffffffffu, !ok);
   if (lane == 0) {
     row_nnz[row] = cnt;
@@ -131,10 +189,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_columns(int nrow, const int
   }
 }
 
-// pass B, warp per row: the row's sorted columns and one 9-value
-// accumulator per column in shared memory.  The lanes load the row's blocks
-// 32 at a time (block i = quad i / 4, column slot jj = i % 4), each finds its
-// column's position by binary search, the warp sorts the 32 (position, lane)
+// pass B, warp per row: one 9-value accumulator per column in shared memory.
+// The lanes load the row's blocks 32 at a time (block i = quad i / 4, column
+// slot jj = i % 4) with the column positions pass A stored, the warp sorts the 32 (position, lane)
 // keys (bitonic, shuffles), gathers the values in that order and forms the
 // segment sums of equal positions (shuffle-down scan); the first lane of each
 // segment adds its sum to the column's accumulator.  Every sum runs in a
@@ -142,14 +199,12 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_columns(int nrow, const int
 // is deterministic, and each column takes one shared-memory add per batch.
 template <class S>
 __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int* __restrict__ qstart,
-                                                            const int* __restrict__ qids, const int* __restrict__ ee,
-                                                            int n_ee, const int* __restrict__ pt,
-                                                            const unsigned short* __restrict__ bmask,
+                                                            const int* __restrict__ qids,
+                                                            const unsigned* __restrict__ qpos,
                                                             const S* __restrict__ vals,
                                                             const int* __restrict__ tmpcols,
                                                             const int* __restrict__ offsets, int* __restrict__ columns,
                                                             S* __restrict__ values) {
-  __shared__ int scol[kWarps][kHash];
   __shared__ S sacc[kWarps][kHash * 9];
   const unsigned full = 0xffffffffu;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -158,8 +213,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int*
   int b = qstart[row], e = qstart[row + 1];
   if (b == e) return;
   const int out = offsets[row], cnt = min(offsets[row + 1] - out, kHash);
+  if (cnt == 0) return;  // also a row pass A skipped (too many quads): its positions were not written
   for (int k = lane; k < cnt; k += 32) {
-    scol[w][k] = tmpcols[4 * b + k];
 #pragma unroll
     for (int t = 0; t < 9; ++t) sacc[w][9 * k + t] = S(0);
   }
@@ -173,24 +228,14 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int*
 #pragma unroll
     for (int t = 0; t < 9; ++t) v[t] = S(0);
     if (i < nb) {
-      const int q = __ldg(qids + b + (i >> 2)), jj = i & 3;
-      if ((__ldg(bmask + (q >> 2)) >> (4 * (q & 3) + jj)) & 1u) {
-        const int c = comp(record_ids(ee, n_ee, pt, q >> 2), jj);
-        int lo = 0, hi = cnt - 1;
-        while (lo <= hi) {
-          const int mid = (lo + hi) >> 1, x = scol[w][mid];
-          if (x == c) {
-            pos = mid;
-            break;
-          }
-          if (x < c) lo = mid + 1;
-          else hi = mid - 1;
-        }
-        if (pos != kNone) {  // absent only when the row overflowed (status set in pass A)
-          const S* src = vals + 36LL * q + 9 * jj;
+      const int k = i >> 2, jj = i & 3;
+      const int q = __ldg(qids + b + k);
+      const unsigned pk = (__ldg(qpos + b + k) >> (8 * jj)) & 0xffu;
+      if ((int)pk < cnt) {  // kAbsent for a zero block
+        pos = (int)pk;
+        const S* src = vals + 36LL * q + 9 * jj;
 #pragma unroll
-          for (int t = 0; t < 9; ++t) v[t] = __ldg(src + t);
-        }
+        for (int t = 0; t < 9; ++t) v[t] = __ldg(src + t);
       }
     }
     // bitonic sort of (pos, lane) over the warp
@@ -225,7 +270,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int*
     __syncwarp();
   }
   for (int k = lane; k < cnt; k += 32) {
-    columns[out + k] = scol[w][k];
+    columns[out + k] = tmpcols[4LL * b + k];
 #pragma unroll
     for (int t = 0; t < 9; ++t) values[9LL * (out + k) + t] = sacc[w][9 * k + t];
   }
@@ -239,28 +284,25 @@ __global__ void k_total(int nrow, int* __restrict__ offsets, const int* __restri
 template <class S>
 int assemble(int n_ee, int n_pt, int nv, const int* ee, const int* pt, const S* vals, const unsigned short* bmask,
              int* offsets, int* columns, S* values, int* nnz, int* status, void* ws, cudaStream_t st) {
-  int P = n_ee + n_pt, nq = 4 * P;
-  size_t NQ = (size_t)nq, R = (size_t)nv + 1;
+  const int P = n_ee + n_pt;
+  size_t NQ = 4 * (size_t)P, R = (size_t)nv + 1;
   char* p = (char*)ws;
-  unsigned* keys = (unsigned*)p; p += al(NQ * 4);
-  int* ids = (int*)p; p += al(NQ * 4);
+  int4* slots = (int4*)p; p += al(NQ * 4);
+  int* qids = (int*)p; p += al(NQ * 4);
+  unsigned* qpos = (unsigned*)p; p += al(NQ * 4);
   int* qstart = (int*)p; p += al(R * 4);
   int* tmpcols = (int*)p; p += al(NQ * 4 * 4);
   int* total = (int*)p; p += 256;
-  void* scratch = p; p += scan::scratch_bytes((int)R);
-  void* sws = p;
+  void* scratch = p;
   cudaMemsetAsync(qstart, 0, R * sizeof(int), st);
-  k_quad_keys<<<div_up(nq, 256), 256, 0, st>>>(nq, ee, n_ee, pt, keys, ids, qstart);
-  int bits = 1;
-  while ((1LL << bits) < (long long)nv) ++bits;
-  sort::sort_pairs<unsigned>(keys, ids, nq, bits, sws, sort::workspace_bytes<unsigned>(nq), st);
+  k_rec_slots<<<div_up(P, 256), 256, 0, st>>>(P, ee, n_ee, pt, slots, qstart);
   scan::exclusive<int>(qstart, (int)R, scratch, total, st);
+  k_rec_scatter<<<div_up(P, 256), 256, 0, st>>>(P, ee, n_ee, pt, slots, qstart, qids);
   int g = div_up(nv, kWarps);
-  k_row_columns<<<g, kWarps * 32, 0, st>>>(nv, qstart, ids, ee, n_ee, pt, bmask, tmpcols, offsets, status);
+  k_row_columns<<<g, kWarps * 32, 0, st>>>(nv, qstart, qids, ee, n_ee, pt, bmask, tmpcols, qpos, offsets, status);
   scan::exclusive<int>(offsets, nv, scratch, total, st);
   k_total<<<1, 1, 0, st>>>(nv, offsets, total, nnz);
-  k_row_values<S><<<g, kWarps * 32, 0, st>>>(nv, qstart, ids, ee, n_ee, pt, bmask, vals, tmpcols, offsets, columns,
-                                             values);
+  k_row_values<S><<<g, kWarps * 32, 0, st>>>(nv, qstart, qids, qpos, vals, tmpcols, offsets, columns, values);
   return check_launch("ipcb_contact_bsr");
 }
 
@@ -273,8 +315,7 @@ extern "C" {
 
 size_t ipcb_contact_bsr_workspace(int n_records, int n_verts) {
   size_t NQ = 4 * (size_t)(n_records > 0 ? n_records : 1), R = (size_t)(n_verts > 0 ? n_verts : 0) + 1;
-  return al(NQ * 4) * 2 + al(R * 4) + al(NQ * 16) + 256 + scan::scratch_bytes((int)R) +
-         sort::workspace_bytes<unsigned>((int)NQ);
+  return al(NQ * 4) * 3 + al(R * 4) + al(NQ * 16) + 256 + scan::scratch_bytes((int)R);
 }
 
 int ipcb_contact_bsr(const ipcb_contacts* ee, int n_ee, const ipcb_contacts* pt, int n_pt, int n_verts,

@@ -80,3 +80,45 @@ def test_contact_bsr_equals_generic_assembly(cuda, idx, fp64):
     a, bb = A.values[:nnz].double(), B.values[:nnz].double()
     tol = 1e-12 if fp64 else 2e-6
     assert ((a - bb).abs().amax(dim=(1, 2)) <= tol * a.abs().amax(dim=(1, 2)).clamp_min(1e-300)).all()
+    # the per-row bucketing takes slots with atomics; the result is the same bits on every run
+    C, _ = contact_bsr(s.contacts_new, n_ee, s.contacts_pt, n_pt, nv, t)
+    assert torch.equal(B.values[:nnz], C.values[:nnz])
+
+
+@pytest.mark.parametrize("n_hub", [1024, 1025])
+def test_contact_bsr_long_row(cuda, n_hub):
+    """Vertex 0 in n_hub records (one quad each): a row of up to 1024 quads is
+    assembled in one warp and equals the generic assembly; a longer row sets
+    IPCB_STATUS_ROW_OVERFLOW (4) so the caller switches to the generic path."""
+    from ipc_warp_b200.bsr import Triplets, contact_bsr
+    from ipc_warp_b200.contact import Contacts
+
+    rng = np.random.default_rng(n_hub)
+    nv, P = 40, n_hub
+    recs = np.stack([rng.permutation(np.r_[0, rng.choice(np.arange(1, nv), 3, replace=False)]) for _ in range(P)])
+    recs = recs.astype(np.int32)
+    vals = rng.normal(size=(P, 4, 4, 3, 3)).astype(np.float32)
+    vals[rng.random((P, 4, 4)) < 0.2] = 0.0  # zero blocks are dropped
+    mask = (np.abs(vals).reshape(P, 16, 9).max(-1) > 0).astype(np.uint32) @ (1 << np.arange(16, dtype=np.uint32))
+    rows = np.repeat(recs, 4, axis=1).reshape(-1)  # triplet 16p + 4ii + jj: row recs[p, ii]
+    cols = np.tile(recs, (1, 4)).reshape(-1)       # column recs[p, jj]
+    ee = Contacts(P, torch.float32, cuda)
+    ee.a1a2b1b2.copy_(torch.tensor(recs))
+    ee.cnt.fill_(P)
+    pt = Contacts(1, torch.float32, cuda)
+    tr = lambda a: torch.tensor(a, device=cuda)
+    t = Triplets(tr(rows.astype(np.int32)), tr(cols.astype(np.int32)), tr(vals.reshape(-1, 3, 3)),
+                 tr(mask.astype(np.uint16).view(np.int16)))
+    B, status = contact_bsr(ee, P, pt, 0, nv, t)
+    if n_hub > 1024:
+        assert status & 4
+        return
+    assert status == 0
+    A = bsr_from_triplets(nv, nv, t.rows, t.cols, t.vals)
+    nnz = A.nnz_sync()
+    assert B.nnz_sync() == nnz > 0
+    assert torch.equal(A.offsets, B.offsets) and torch.equal(A.columns[:nnz], B.columns[:nnz])
+    a, bb = A.values[:nnz].double(), B.values[:nnz].double()
+    assert ((a - bb).abs().amax(dim=(1, 2)) <= 2e-5 * a.abs().amax(dim=(1, 2)).clamp_min(1e-30)).all()
+    C, _ = contact_bsr(ee, P, pt, 0, nv, t)
+    assert torch.equal(B.values[:nnz], C.values[:nnz])
