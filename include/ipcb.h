@@ -491,9 +491,8 @@ int ipcb_bsr_from_triplets(int nrow, int ncol, int n_trip, const int* rows, cons
  * triplets: the
  * records' structure (one row and 4 columns per (record, slot)) replaces the
  * per-triplet bucketing.  Deterministic.  If a row has more than 128 distinct
- * columns or appears in more than 1024 (record, slot) pairs, *status gets
- * IPCB_STATUS_ROW_OVERFLOW and the caller must use ipcb_bsr_from_triplets
- * instead. */
+ * columns, *status gets IPCB_STATUS_ROW_OVERFLOW and the caller must use
+ * ipcb_bsr_from_triplets instead. */
 size_t ipcb_contact_bsr_workspace(int n_records, int n_verts);
 int ipcb_contact_bsr(const ipcb_contacts* ee, int n_ee, const ipcb_contacts* pt, int n_pt, int n_verts,
                      const void* vals, const unsigned short* block_mask, int fp64, int* offsets, int* columns,

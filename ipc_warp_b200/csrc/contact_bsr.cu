@@ -17,8 +17,8 @@
 //   4. pass B, warp per row: the row's blocks 32 at a time, sorted by column
 //      position within the warp and reduced by segments (shuffles), one
 //      shared-memory add per column and batch; a fixed order, so deterministic
-// A row with more than kHash distinct columns or more than kMaxQuads quads
-// sets IPCB_STATUS_ROW_OVERFLOW (the host then uses the generic assembly).
+// A row with more than kHash distinct columns sets IPCB_STATUS_ROW_OVERFLOW
+// (the host then uses the generic assembly).
 #include "common.cuh"
 #include "scan.cuh"
 
@@ -28,7 +28,7 @@ int check_launch(const char* where);
 namespace {
 
 constexpr int kHash = 128;        // distinct columns per row handled by one warp
-constexpr int kMaxQuads = 1024;   // quads per row sorted in one warp's shared memory
+constexpr int kSmemQuads = 256;   // quads per row sorted in shared memory (longer rows: in global scratch)
 constexpr unsigned kAbsent = 0xffu;  // column position of a zero block
 constexpr int kOwn = kHash / 32;
 constexpr int kWarps = 4;
@@ -82,107 +82,122 @@ IPCB_D void warp_sort(int* a, int n, int lane) {
     }
 }
 
-// insert c into the warp's open-addressing table (keys -1 = empty)
-IPCB_D bool hash_insert(int* tab, int c) {
+// insert c into the warp's open-addressing table (keys -1 = empty); returns
+// the slot, or -1 when the table is full
+IPCB_D int hash_insert(int* tab, int c) {
   unsigned h = ((unsigned)c * 2654435761u) & (kHash - 1);
   for (int probe = 0; probe < kHash; ++probe) {
     int old = atomicCAS(tab + h, -1, c);
-    if (old == -1 || old == c) return true;
+    if (old == -1 || old == c) return (int)h;
     h = (h + 1) & (kHash - 1);
   }
-  return false;
+  return -1;
 }
 
+IPCB_D int hash_find(const int* tab, int c) {
+  unsigned h = ((unsigned)c * 2654435761u) & (kHash - 1);
+  for (int probe = 0; probe < kHash; ++probe) {
+    const int k = tab[h];
+    if (k == c) return (int)h;
+    if (k == -1) return -1;
+    h = (h + 1) & (kHash - 1);
+  }
+  return -1;
+}
+
+IPCB_D unsigned quad_mask(const unsigned short* __restrict__ bmask, int q) {
+  return (__ldg(bmask + (q >> 2)) >> (4 * (q & 3))) & 0xFu;  // blocks (ii = q & 3, jj = 0..3)
+}
+
+// pass A, warp per row.  The row's quad ids are sorted in shared memory (rows
+// of more than kSmemQuads quads: in their own tmpcols range past the kHash
+// column entries, 4 ints per quad reserved there), the distinct columns of
+// the non-zero blocks go through a shared-memory hash, are compacted and
+// sorted, and every quad gets its 4 column positions through a slot ->
+// position table.
 __global__ void __launch_bounds__(kWarps * 32) k_row_columns(int nrow, const int* __restrict__ qstart,
                                                              int* __restrict__ qids, const int* __restrict__ ee,
                                                              int n_ee, const int* __restrict__ pt,
                                                              const unsigned short* __restrict__ bmask,
                                                              int* __restrict__ tmpcols, unsigned* __restrict__ qpos,
                                                              int* __restrict__ row_nnz, int* __restrict__ status) {
+  __shared__ int sq[kWarps][kSmemQuads];
   __shared__ int tab[kWarps][kHash];
-  __shared__ int sq[kWarps][kMaxQuads];
+  __shared__ int scol[kWarps][kHash];
+  __shared__ unsigned char slot_pos[kWarps][kHash];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int row = blockIdx.x * kWarps + w;
   if (row >= nrow) return;
   const int b = qstart[row], n = qstart[row + 1] - b;
-  if (n == 0 || n > kMaxQuads) {
-    if (lane == 0) {
-      row_nnz[row] = 0;
-      if (n) atomicOr(status, IPCB_STATUS_ROW_OVERFLOW);
-    }
+  if (n == 0) {
+    if (lane == 0) row_nnz[row] = 0;
     return;
   }
   // the row's quads in quad-id order
   int nq2 = 32;
   while (nq2 < n) nq2 <<= 1;
-  for (int k = lane; k < nq2; k += 32) sq[w][k] = k < n ? qids[b + k] : 0x7fffffff;
-  for (int k = lane; k < kHash; k += 32) tab[w][k] = -1;
-  __syncwarp();
-  warp_sort(sq[w], nq2, lane);
-  for (int k = lane; k < n; k += 32) qids[b + k] = sq[w][k];
-  bool ok = true;
-  for (int k = lane; k < n; k += 32) {
-    const int q = sq[w][k];
-    const int4 v = record_ids(ee, n_ee, pt, q >> 2);
-    const unsigned m = (__ldg(bmask + (q >> 2)) >> (4 * (q & 3))) & 0xFu;  // blocks (ii, jj = 0..3)
-#pragma unroll
-    for (int jj = 0; jj < 4; ++jj)
-      if ((m >> jj) & 1u) ok &= hash_insert(tab[w], comp(v, jj));
+  int* buf = n <= kSmemQuads ? sq[w] : tmpcols + 4LL * b + kHash;  // nq2 <= 2n <= 4n - kHash there
+  for (int k = lane; k < nq2; k += 32) buf[k] = k < n ? qids[b + k] : 0x7fffffff;
+  for (int k = lane; k < kHash; k += 32) {
+    tab[w][k] = -1;
+    scol[w][k] = 0x7fffffff;
   }
   __syncwarp();
-  // compact the occupied slots to the front (stable), pad with INT_MAX, then
-  // bitonic-sort the first P >= cnt entries
+  warp_sort(buf, nq2, lane);
+  for (int k = lane; k < n; k += 32) qids[b + k] = buf[k];
+  // distinct columns; the first quad of each lane keeps its 4 slots
+  bool ok = true;
+  int slot0[4] = {-1, -1, -1, -1};
+  for (int k = lane; k < n; k += 32) {
+    const int q = buf[k];
+    const int4 v = record_ids(ee, n_ee, pt, q >> 2);
+    const unsigned m = quad_mask(bmask, q);
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj)
+      if ((m >> jj) & 1u) {
+        const int h = hash_insert(tab[w], comp(v, jj));
+        ok &= h >= 0;
+        if (k == lane) slot0[jj] = h;
+      }
+  }
+  __syncwarp();
+  // compact the occupied slots (stable) and sort them
   const unsigned lt = (1u << lane) - 1u;
-  int dest[kOwn], colv[kOwn];
   int cnt = 0;
 #pragma unroll
   for (int r = 0; r < kOwn; ++r) {
-    int c = tab[w][r * 32 + lane];
-    unsigned m = __ballot_sync(0xffffffffu, c >= 0);
-    dest[r] = c >= 0 ? cnt + __popc(m & lt) : -1;
-    colv[r] = c;
+    const int c = tab[w][r * 32 + lane];
+    const unsigned m = __ballot_sync(0xffffffffu, c >= 0);
+    if (c >= 0) scol[w][cnt + __popc(m & lt)] = c;
     cnt += __popc(m);
   }
   __syncwarp();
-#pragma unroll
-  for (int r = 0; r < kOwn; ++r) tab[w][r * 32 + lane] = 0x7fffffff;
-  __syncwarp();
-#pragma unroll
-  for (int r = 0; r < kOwn; ++r)
-    if (dest[r] >= 0) tab[w][dest[r]] = colv[r];
-  __syncwarp();
   int P = 1;
   while (P < cnt) P <<= 1;
-  warp_sort(tab[w], P, lane);
+  warp_sort(scol[w], P, lane);
+  for (int k = lane; k < cnt; k += 32) slot_pos[w][hash_find(tab[w], scol[w][k])] = (unsigned char)k;
+  __syncwarp();
   // each quad's 4 column positions (kAbsent for a zero block, or for a column
-  // lost to an overflowing table)
+  // lost to a full table)
   for (int k = lane; k < n; k += 32) {
-    const int q = sq[w][k];
-    const int4 v = record_ids(ee, n_ee, pt, q >> 2);
-    const unsigned m = (__ldg(bmask + (q >> 2)) >> (4 * (q & 3))) & 0xFu;
     unsigned packed = 0;
+    if (k == lane) {
 #pragma unroll
-    for (int jj = 0; jj < 4; ++jj) {
-      unsigned pos = kAbsent;
-      if ((m >> jj) & 1u) {
-        const int c = comp(v, jj);
-        int lo = 0, hi = cnt - 1;
-        while (lo <= hi) {
-          const int mid = (lo + hi) >> 1, x = tab[w][mid];
-          if (x == c) {
-            pos = (unsigned)mid;
-            break;
-          }
-          if (x < c) lo = mid + 1;
-          else hi = mid - 1;
-        }
+      for (int jj = 0; jj < 4; ++jj) packed |= (slot0[jj] >= 0 ? (unsigned)slot_pos[w][slot0[jj]] : kAbsent) << (8 * jj);
+    } else {
+      const int q = buf[k];
+      const int4 v = record_ids(ee, n_ee, pt, q >> 2);
+      const unsigned m = quad_mask(bmask, q);
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        const int h = (m >> jj) & 1u ? hash_find(tab[w], comp(v, jj)) : -1;
+        packed |= (h >= 0 ? (unsigned)slot_pos[w][h] : kAbsent) << (8 * jj);
       }
-      packed |= pos << (8 * jj);
     }
     qpos[b + k] = packed;
   }
-  for (int k = lane; k < cnt; k += 32) tmpcols[4LL * b + k] = tab[w][k];
-  unsigned bad = __ballot_sync(0xffffffffu, !ok);
+  for (int k = lane; k < cnt; k += 32) tmpcols[4LL * b + k] = scol[w][k];
+  const unsigned bad = __ballot_sync(0xffffffffu, !ok);
   if (lane == 0) {
     row_nnz[row] = cnt;
     if (bad) atomicOr(status, IPCB_STATUS_ROW_OVERFLOW);

@@ -85,16 +85,17 @@ def test_contact_bsr_equals_generic_assembly(cuda, idx, fp64):
     assert torch.equal(B.values[:nnz], C.values[:nnz])
 
 
-@pytest.mark.parametrize("n_hub", [1024, 1025])
-def test_contact_bsr_long_row(cuda, n_hub):
-    """Vertex 0 in n_hub records (one quad each): a row of up to 1024 quads is
-    assembled in one warp and equals the generic assembly; a longer row sets
+@pytest.mark.parametrize("n_hub,nv", [(256, 40), (257, 40), (3000, 40), (400, 300)])
+def test_contact_bsr_long_row(cuda, n_hub, nv):
+    """Vertex 0 in n_hub records (one quad each): a long row (its quads sorted
+    in shared memory up to 256, past that in the row's own scratch) equals the
+    generic assembly; a row with more than 128 distinct columns sets
     IPCB_STATUS_ROW_OVERFLOW (4) so the caller switches to the generic path."""
     from ipc_warp_b200.bsr import Triplets, contact_bsr
     from ipc_warp_b200.contact import Contacts
 
     rng = np.random.default_rng(n_hub)
-    nv, P = 40, n_hub
+    P = n_hub
     recs = np.stack([rng.permutation(np.r_[0, rng.choice(np.arange(1, nv), 3, replace=False)]) for _ in range(P)])
     recs = recs.astype(np.int32)
     vals = rng.normal(size=(P, 4, 4, 3, 3)).astype(np.float32)
@@ -110,7 +111,7 @@ def test_contact_bsr_long_row(cuda, n_hub):
     t = Triplets(tr(rows.astype(np.int32)), tr(cols.astype(np.int32)), tr(vals.reshape(-1, 3, 3)),
                  tr(mask.astype(np.uint16).view(np.int16)))
     B, status = contact_bsr(ee, P, pt, 0, nv, t)
-    if n_hub > 1024:
+    if nv > 129:
         assert status & 4
         return
     assert status == 0
