@@ -159,6 +159,12 @@ int ipcb_dcd_pt(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* tri_bvh
  * (ii, jj) of the record has a non-zero entry (read by ipcb_contact_bsr). */
 int ipcb_contact_hessian(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, int offset, double kappa,
                          int* rows, int* cols, void* vals, void* b, unsigned short* block_mask, ipcb_stream s);
+/* The same with the record offset taken on the device: records go at
+ * (min(*offset_count, offset) + k)*16, so a PT list can follow the EE list's
+ * device-side count without a host read (offset = the EE list's capacity). */
+int ipcb_contact_hessian_after(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, int offset,
+                               const int* offset_count, double kappa, int* rows, int* cols, void* vals, void* b,
+                               unsigned short* block_mask, ipcb_stream s);
 /* energy (double) += sum of the barrier energy of the list */
 int ipcb_contact_energy(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, double kappa,
                         double* energy, ipcb_stream s);
@@ -492,7 +498,11 @@ int ipcb_bsr_from_triplets(int nrow, int ncol, int n_trip, const int* rows, cons
  * records' structure (one row and 4 columns per (record, slot)) replaces the
  * per-triplet bucketing.  Deterministic.  If a row has more than 128 distinct
  * columns, *status gets IPCB_STATUS_ROW_OVERFLOW and the caller must use
- * ipcb_bsr_from_triplets instead. */
+ * ipcb_bsr_from_triplets instead.  n_ee < 0 (n_pt < 0): that list's count is
+ * min(*cnt, capacity), read on the device (the PT records then follow that
+ * many EE records, as ipcb_contact_hessian_after writes them); the
+ * workspace and the capacity of columns/values are sized for the
+ * capacities. */
 size_t ipcb_contact_bsr_workspace(int n_records, int n_verts);
 int ipcb_contact_bsr(const ipcb_contacts* ee, int n_ee, const ipcb_contacts* pt, int n_pt, int n_verts,
                      const void* vals, const unsigned short* block_mask, int fp64, int* offsets, int* columns,

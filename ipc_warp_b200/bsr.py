@@ -42,6 +42,7 @@ class BsrMatrix:
         self.columns = torch.zeros(cap, dtype=torch.int32, device=device)
         self.values = torch.zeros((cap, 3, 3), dtype=dtype, device=device)
         self.nnz_dev = torch.zeros(1, dtype=torch.int32, device=device)
+        self._ws = None  # contact_bsr workspace, kept between calls
 
     @property
     def shape(self):
@@ -78,26 +79,35 @@ def bsr_from_triplets(nrow: int, ncol: int, rows: torch.Tensor, cols: torch.Tens
     return out
 
 
-def contact_bsr(ee, n_ee: int, pt, n_pt: int, n_verts: int, trip: Triplets,
-                out: BsrMatrix | None = None, status: torch.Tensor | None = None) -> tuple[BsrMatrix, int]:
+def contact_bsr(ee, n_ee: int | None, pt, n_pt: int | None, n_verts: int, trip: Triplets,
+                out: BsrMatrix | None = None, status: torch.Tensor | None = None,
+                read_status: bool = True) -> tuple[BsrMatrix, int | None]:
     """BSR of the contact Hessian from the EE/PT lists and their triplets
     (16 blocks per record, EE first, with block masks).  Returns (matrix, status);
     status has IPCB_STATUS_ROW_OVERFLOW (4) set when a row had too many
-    distinct columns for the fast path (the matrix is then incomplete)."""
+    distinct columns for the fast path (the matrix is then incomplete).
+    n_ee / n_pt None: the lists' counts are read on the device (sizes follow
+    the capacities).  read_status=False: no host read; the status stays in
+    ``status`` (device) and None is returned in its place."""
     vals = trip.vals
     dtype, dev = vals.dtype, vals.device
-    cap = max(16 * (n_ee + n_pt), 1)
+    ne = ee.capacity if n_ee is None else n_ee
+    npt = pt.capacity if n_pt is None else n_pt
+    cap = max(16 * (ne + npt), 1)
     if out is None or out.columns.shape[0] < cap or out.nrow != n_verts or out.dtype != dtype:
         out = BsrMatrix(n_verts, n_verts, cap, dtype, dev)
     st = torch.zeros(1, dtype=torch.int32, device=dev) if status is None else status.zero_()
-    ws = torch.empty(N.size("ipcb_contact_bsr_workspace", n_ee + n_pt, n_verts), dtype=torch.uint8, device=dev)
+    nbytes = N.size("ipcb_contact_bsr_workspace", ne + npt, n_verts)
+    ws = getattr(out, "_ws", None)
+    if ws is None or ws.numel() < nbytes:
+        ws = out._ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
     import ctypes
 
-    N.call("ipcb_contact_bsr", ctypes.byref(ee.c_struct()), n_ee, ctypes.byref(pt.c_struct()), n_pt, n_verts,
+    N.call("ipcb_contact_bsr", ctypes.byref(ee.c_struct()), -1 if n_ee is None else n_ee,
+           ctypes.byref(pt.c_struct()), -1 if n_pt is None else n_pt, n_verts,
            N.ptr(vals), N.ptr(trip.mask), int(dtype == torch.float64), N.ptr(out.offsets), N.ptr(out.columns),
-           N.ptr(out.values),
-           N.ptr(out.nnz_dev), N.ptr(st), N.ptr(ws), ws.numel(), N.stream_handle())
-    return out, int(st.item())
+           N.ptr(out.values), N.ptr(out.nnz_dev), N.ptr(st), N.ptr(ws), ws.numel(), N.stream_handle())
+    return out, (int(st.item()) if read_status else None)
 
 
 def bsr_axpy(x: BsrMatrix, y: BsrMatrix, alpha: float = 1.0, beta: float = 1.0) -> BsrMatrix:

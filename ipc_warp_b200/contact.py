@@ -265,6 +265,12 @@ class ContactSolverBase:
     def collision_free_step(self, dx: torch.Tensor) -> float:
         """contact.py:539-585: conservative CCD bound for x -= alpha * dx;
         returns 0.9 * toi if toi < 1 else 1."""
+        self._launch_ccd(dx)
+        toi = float(self.ccd_toi.item())
+        return 0.9 * toi if toi < 1.0 else 1.0
+
+    def _launch_ccd(self, dx: torch.Tensor):
+        """The CCD queries of collision_free_step; the TOI stays in ccd_toi."""
         soup = self.soup.c_struct()
         s = N.stream_handle()
         pad = 1e-7
@@ -284,8 +290,6 @@ class ContactSolverBase:
             N.call("ipcb_point_triangle_toi", ctypes.byref(soup), N.ptr(self.ccd_x1),
                    ctypes.byref(self.ccd_triangle_bvh.c), pad, int(self.disable_self_collision),
                    N.ptr(self.ccd_toi), N.ptr(self._status), N.ptr(self._toi_ws), self._toi_ws.numel(), s)
-        toi = float(self.ccd_toi.item())
-        return 0.9 * toi if toi < 1.0 else 1.0
 
     def new_intersections(self, x0: torch.Tensor, x1: torch.Tensor) -> float:
         """contact.py:587-670 (the augmented-Lagrangian solver's CCD): every

@@ -40,10 +40,18 @@ IPCB_D int4 record_ids(const int* __restrict__ ee, int n_ee, const int* __restri
 }
 IPCB_D int comp(int4 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
 
-__global__ void k_rec_slots(int n_rec, const int* __restrict__ ee, int n_ee, const int* __restrict__ pt,
+// nrec = {EE records, PT records}: host values, or min(*cnt, capacity) of
+// the lists read on the device (graph-capturable; no host read of the counts)
+__global__ void k_counts(const int* __restrict__ ee_cnt, int ee_n, const int* __restrict__ pt_cnt, int pt_n,
+                         int* __restrict__ nrec) {
+  nrec[0] = ee_cnt ? min(max(*ee_cnt, 0), ee_n) : ee_n;
+  nrec[1] = pt_cnt ? min(max(*pt_cnt, 0), pt_n) : pt_n;
+}
+
+__global__ void k_rec_slots(const int* __restrict__ nrec, const int* __restrict__ ee, const int* __restrict__ pt,
                             int4* __restrict__ slots, int* __restrict__ row_cnt) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n_rec) return;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x, n_ee = nrec[0];
+  if (p >= n_ee + nrec[1]) return;
   const int4 v = record_ids(ee, n_ee, pt, p);
   int4 s;
   s.x = atomicAdd(row_cnt + v.x, 1);
@@ -53,10 +61,10 @@ __global__ void k_rec_slots(int n_rec, const int* __restrict__ ee, int n_ee, con
   slots[p] = s;
 }
 
-__global__ void k_rec_scatter(int n_rec, const int* __restrict__ ee, int n_ee, const int* __restrict__ pt,
+__global__ void k_rec_scatter(const int* __restrict__ nrec, const int* __restrict__ ee, const int* __restrict__ pt,
                               const int4* __restrict__ slots, const int* __restrict__ qstart, int* __restrict__ qids) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n_rec) return;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x, n_ee = nrec[0];
+  if (p >= n_ee + nrec[1]) return;
   const int4 v = record_ids(ee, n_ee, pt, p), s = slots[p];
   qids[qstart[v.x] + s.x] = 4 * p;
   qids[qstart[v.y] + s.y] = 4 * p + 1;
@@ -117,7 +125,7 @@ IPCB_D unsigned quad_mask(const unsigned short* __restrict__ bmask, int q) {
 // position table.
 __global__ void __launch_bounds__(kWarps * 32) k_row_columns(int nrow, const int* __restrict__ qstart,
                                                              int* __restrict__ qids, const int* __restrict__ ee,
-                                                             int n_ee, const int* __restrict__ pt,
+                                                             const int* __restrict__ nrec, const int* __restrict__ pt,
                                                              const unsigned short* __restrict__ bmask,
                                                              int* __restrict__ tmpcols, unsigned* __restrict__ qpos,
                                                              int* __restrict__ row_nnz, int* __restrict__ status) {
@@ -133,6 +141,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_columns(int nrow, const int
     if (lane == 0) row_nnz[row] = 0;
     return;
   }
+  const int n_ee = nrec[0];
   // the row's quads in quad-id order
   int nq2 = 32;
   while (nq2 < n) nq2 <<= 1;
@@ -297,9 +306,10 @@ __global__ void k_total(int nrow, int* __restrict__ offsets, const int* __restri
 }
 
 template <class S>
-int assemble(int n_ee, int n_pt, int nv, const int* ee, const int* pt, const S* vals, const unsigned short* bmask,
-             int* offsets, int* columns, S* values, int* nnz, int* status, void* ws, cudaStream_t st) {
-  const int P = n_ee + n_pt;
+int assemble(int n_ee, int n_pt, const int* ee_cnt, const int* pt_cnt, int nv, const int* ee, const int* pt,
+             const S* vals, const unsigned short* bmask, int* offsets, int* columns, S* values, int* nnz, int* status,
+             void* ws, cudaStream_t st) {
+  const int P = n_ee + n_pt;  // records, or their bound when the counts are read on the device
   size_t NQ = 4 * (size_t)P, R = (size_t)nv + 1;
   char* p = (char*)ws;
   int4* slots = (int4*)p; p += al(NQ * 4);
@@ -308,13 +318,15 @@ int assemble(int n_ee, int n_pt, int nv, const int* ee, const int* pt, const S* 
   int* qstart = (int*)p; p += al(R * 4);
   int* tmpcols = (int*)p; p += al(NQ * 4 * 4);
   int* total = (int*)p; p += 256;
+  int* nrec = (int*)p; p += 256;
   void* scratch = p;
   cudaMemsetAsync(qstart, 0, R * sizeof(int), st);
-  k_rec_slots<<<div_up(P, 256), 256, 0, st>>>(P, ee, n_ee, pt, slots, qstart);
+  k_counts<<<1, 1, 0, st>>>(ee_cnt, n_ee, pt_cnt, n_pt, nrec);
+  k_rec_slots<<<div_up(P, 256), 256, 0, st>>>(nrec, ee, pt, slots, qstart);
   scan::exclusive<int>(qstart, (int)R, scratch, total, st);
-  k_rec_scatter<<<div_up(P, 256), 256, 0, st>>>(P, ee, n_ee, pt, slots, qstart, qids);
+  k_rec_scatter<<<div_up(P, 256), 256, 0, st>>>(nrec, ee, pt, slots, qstart, qids);
   int g = div_up(nv, kWarps);
-  k_row_columns<<<g, kWarps * 32, 0, st>>>(nv, qstart, qids, ee, n_ee, pt, bmask, tmpcols, qpos, offsets, status);
+  k_row_columns<<<g, kWarps * 32, 0, st>>>(nv, qstart, qids, ee, nrec, pt, bmask, tmpcols, qpos, offsets, status);
   scan::exclusive<int>(offsets, nv, scratch, total, st);
   k_total<<<1, 1, 0, st>>>(nv, offsets, total, nnz);
   k_row_values<S><<<g, kWarps * 32, 0, st>>>(nv, qstart, qids, qpos, vals, tmpcols, offsets, columns, values);
@@ -330,13 +342,19 @@ extern "C" {
 
 size_t ipcb_contact_bsr_workspace(int n_records, int n_verts) {
   size_t NQ = 4 * (size_t)(n_records > 0 ? n_records : 1), R = (size_t)(n_verts > 0 ? n_verts : 0) + 1;
-  return al(NQ * 4) * 3 + al(R * 4) + al(NQ * 16) + 256 + scan::scratch_bytes((int)R);
+  return al(NQ * 4) * 3 + al(R * 4) + al(NQ * 16) + 512 + scan::scratch_bytes((int)R);
 }
 
 int ipcb_contact_bsr(const ipcb_contacts* ee, int n_ee, const ipcb_contacts* pt, int n_pt, int n_verts,
                      const void* vals, const unsigned short* block_mask, int fp64, int* offsets, int* columns,
                      void* values, int* nnz, int* status, void* ws, size_t ws_bytes, ipcb_stream s) {
-  if (!ee || !pt || n_ee < 0 || n_pt < 0 || n_verts < 0 || !offsets || !nnz || !status) return IPCB_E_ARG;
+  if (!ee || !pt || n_verts < 0 || !offsets || !nnz || !status) return IPCB_E_ARG;
+  // a negative count: min(*cnt, capacity) of that list, read on the device
+  const int* ee_cnt = n_ee < 0 ? ee->cnt : nullptr;
+  const int* pt_cnt = n_pt < 0 ? pt->cnt : nullptr;
+  if ((n_ee < 0 && !ee_cnt) || (n_pt < 0 && !pt_cnt)) return IPCB_E_ARG;
+  if (n_ee < 0) n_ee = ee->capacity;
+  if (n_pt < 0) n_pt = pt->capacity;
   if (n_ee > ee->capacity || n_pt > pt->capacity || (long long)4 * (n_ee + n_pt) > 0x7fffffff) return IPCB_E_ARG;
   cudaStream_t st = (cudaStream_t)s;
   if (n_ee + n_pt == 0 || n_verts == 0) {
@@ -348,10 +366,10 @@ int ipcb_contact_bsr(const ipcb_contacts* ee, int n_ee, const ipcb_contacts* pt,
       ws_bytes < ipcb_contact_bsr_workspace(n_ee + n_pt, n_verts))
     return IPCB_E_ARG;
   if (fp64)
-    return assemble<double>(n_ee, n_pt, n_verts, ee->a1a2b1b2, pt->a1a2b1b2, (const double*)vals, block_mask,
-                            offsets, columns, (double*)values, nnz, status, ws, st);
-  return assemble<float>(n_ee, n_pt, n_verts, ee->a1a2b1b2, pt->a1a2b1b2, (const float*)vals, block_mask, offsets,
-                         columns, (float*)values, nnz, status, ws, st);
+    return assemble<double>(n_ee, n_pt, ee_cnt, pt_cnt, n_verts, ee->a1a2b1b2, pt->a1a2b1b2, (const double*)vals,
+                            block_mask, offsets, columns, (double*)values, nnz, status, ws, st);
+  return assemble<float>(n_ee, n_pt, ee_cnt, pt_cnt, n_verts, ee->a1a2b1b2, pt->a1a2b1b2, (const float*)vals,
+                         block_mask, offsets, columns, (float*)values, nnz, status, ws, st);
 }
 
 }  // extern "C"

@@ -22,14 +22,17 @@ namespace {
 // T: arithmetic type of the eigen-solve and of H (float for S=float).
 template <class S, int KIND>
 __global__ void __launch_bounds__(128, 3) k_contact_hessian(const S* __restrict__ x, const S* __restrict__ xcs,
-                                                         ipcb_contacts L, int n, int offset, double kappa,
+                                                         ipcb_contacts L, int n, int offset,
+                                                         const int* __restrict__ offset_dev, double kappa,
                                                          int* __restrict__ rows, int* __restrict__ cols,
                                                          S* __restrict__ vals, S* __restrict__ bforce,
                                                          unsigned short* __restrict__ block_mask) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int cnt = list_count<S>(L, n);
   if (i >= cnt) return;
-  contact_hessian_item<S, KIND>(x, xcs, L, i, offset, kappa, rows, cols, vals, bforce, block_mask);
+  // offset_dev: the records follow another list's min(count, offset) records
+  const int off = offset_dev ? min(*offset_dev, offset) : offset;
+  contact_hessian_item<S, KIND>(x, xcs, L, i, off, kappa, rows, cols, vals, bforce, block_mask);
 }
 
 template <class S, int KIND>
@@ -75,17 +78,19 @@ __global__ void __launch_bounds__(256) k_contact_energy(const S* __restrict__ x,
 }
 
 template <class S>
-int launch_hessian(int kind, const ipcb_soup* soup, const ipcb_contacts* L, int n, int offset, double kappa,
-                   int* rows, int* cols, void* vals, void* b, unsigned short* mask, cudaStream_t st) {
+int launch_hessian(int kind, const ipcb_soup* soup, const ipcb_contacts* L, int n, int offset, const int* offset_dev,
+                   double kappa, int* rows, int* cols, void* vals, void* b, unsigned short* mask, cudaStream_t st) {
   int threads = n >= 0 ? n : L->capacity;
   if (threads == 0) return IPCB_OK;
   dim3 grid(div_up(threads, 128));
+  const S* x = (const S*)soup->x;
+  const S* xcs = (const S*)soup->xcs;
   if (kind == 0)
-    k_contact_hessian<S, 0><<<grid, 128, 0, st>>>((const S*)soup->x, (const S*)soup->xcs, *L, n, offset, kappa, rows,
-                                                  cols, (S*)vals, (S*)b, mask);
+    k_contact_hessian<S, 0><<<grid, 128, 0, st>>>(x, xcs, *L, n, offset, offset_dev, kappa, rows, cols, (S*)vals,
+                                                  (S*)b, mask);
   else
-    k_contact_hessian<S, 1><<<grid, 128, 0, st>>>((const S*)soup->x, (const S*)soup->xcs, *L, n, offset, kappa, rows,
-                                                  cols, (S*)vals, (S*)b, mask);
+    k_contact_hessian<S, 1><<<grid, 128, 0, st>>>(x, xcs, *L, n, offset, offset_dev, kappa, rows, cols, (S*)vals,
+                                                  (S*)b, mask);
   return check_launch("ipcb_contact_hessian");
 }
 
@@ -111,11 +116,19 @@ extern "C" {
 
 int ipcb_contact_hessian(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, int offset, double kappa,
                          int* rows, int* cols, void* vals, void* b, unsigned short* block_mask, ipcb_stream s) {
+  return ipcb_contact_hessian_after(kind, soup, list, n, offset, nullptr, kappa, rows, cols, vals, b, block_mask, s);
+}
+
+int ipcb_contact_hessian_after(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, int offset,
+                               const int* offset_count, double kappa, int* rows, int* cols, void* vals, void* b,
+                               unsigned short* block_mask, ipcb_stream s) {
   if (!soup || !list || !rows || !cols || !vals || !b || (kind != 0 && kind != 1) || offset < 0) return IPCB_E_ARG;
   if (n > list->capacity) return IPCB_E_ARG;
   if (soup->fp64)
-    return launch_hessian<double>(kind, soup, list, n, offset, kappa, rows, cols, vals, b, block_mask, (cudaStream_t)s);
-  return launch_hessian<float>(kind, soup, list, n, offset, kappa, rows, cols, vals, b, block_mask, (cudaStream_t)s);
+    return launch_hessian<double>(kind, soup, list, n, offset, offset_count, kappa, rows, cols, vals, b, block_mask,
+                                  (cudaStream_t)s);
+  return launch_hessian<float>(kind, soup, list, n, offset, offset_count, kappa, rows, cols, vals, b, block_mask,
+                               (cudaStream_t)s);
 }
 
 int ipcb_contact_energy(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, double kappa,

@@ -44,6 +44,16 @@ def contact_hessian_pt(states, soup: Soup, contacts: Contacts, triplets: Triplet
            N.ptr(triplets.mask), N.stream_handle())
 
 
+def contact_hessian_pt_after(states, soup: Soup, contacts: Contacts, triplets: Triplets, b: torch.Tensor,
+                             ee: Contacts, kappa: float):
+    """contact_hessian_pt with both counts read on the device: the PT records
+    go right after the EE list's min(count, capacity) records, as
+    contact_hessian_pt(..., offset=n_ee) puts them, without a host read."""
+    N.call("ipcb_contact_hessian_after", 1, ctypes.byref(soup.c_struct()), ctypes.byref(contacts.c_struct()), -1,
+           ee.capacity, N.ptr(ee.cnt), float(kappa), N.ptr(triplets.rows), N.ptr(triplets.cols),
+           N.ptr(triplets.vals), N.ptr(b), N.ptr(triplets.mask), N.stream_handle())
+
+
 def contact_energy_ee(states, soup: Soup, contacts: Contacts, e: torch.Tensor, kappa: float, n: int | None = None):
     """dynamic_contacts.py:374-388; e is a float64 (1,) accumulator."""
     n = min(_count(contacts, n), contacts.capacity)

@@ -20,7 +20,9 @@ import torch
 
 from . import contact
 from .contact import Soup
-from .dynamic_contacts import ContactBarrierMixin
+from .bsr import Triplets, contact_bsr
+from .dynamic_contacts import (ContactBarrierMixin, contact_energy_ee, contact_energy_pt, contact_hessian_ee,
+                               contact_hessian_pt_after)
 
 
 @dataclass
@@ -51,6 +53,13 @@ class ContactPipeline(ContactBarrierMixin):
         self.disable_self_collision = exclude_same_body
         self.collision_triplets = None
         self.collision_hessian = None
+        dev = soup.x_transformed.device
+        self._bsr_status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self._energy = torch.zeros(1, dtype=torch.float64, device=dev)
+        pin = dev.type == "cuda"
+        self._readback = {"counts": torch.zeros(3, dtype=torch.int32, pin_memory=pin),
+                          "energy": torch.zeros(1, dtype=torch.float64, pin_memory=pin),
+                          "toi": torch.zeros(1, dtype=soup.x_transformed.dtype, pin_memory=pin)}
 
     @staticmethod
     def from_scene(scene, dtype=None, device="cuda", exclude_same_body=False) -> "ContactPipeline":
@@ -59,8 +68,58 @@ class ContactPipeline(ContactBarrierMixin):
         return ContactPipeline(soup, scene.dhat, scene.kappa, exclude_same_body=exclude_same_body)
 
     def iteration(self, dx: torch.Tensor | None = None) -> IterationResult:
+        """One Newton iteration's contact work.  On a GPU every stage is
+        enqueued without a host read (list counts taken on the device, PT
+        records placed after the EE count, the contact BSR sized for the
+        list capacities) and the counts, the BSR status, the energy and the
+        TOI come back in one read at the end.  A list that overflowed or a
+        BSR row with too many columns sends the iteration through the
+        step-by-step calls, which grow the lists and pick the generic
+        assembly."""
         if dx is not None:
             self.states.dx = dx
+        if self.device.type != "cuda":
+            return self.iteration_stepwise()
+        ee, pt = self.contacts_new, self.contacts_pt
+        self.compute_V(ret=False)
+        self.update_bvh()
+        self._launch_dcd("ee")
+        if self.has_triangles:
+            self._launch_dcd("pt")
+        else:
+            pt.cnt.zero_()
+        cap = ee.capacity + pt.capacity
+        t = self.collision_triplets
+        if t is None or t.rows.shape[0] < 16 * cap:
+            t = self.collision_triplets = Triplets.zeros(16 * cap, self.soup.xcs.dtype, self.device)
+        kappa = float(self.contact_stiffness)
+        self.b.zero_()
+        contact_hessian_ee(self.states, self.soup, ee, t, self.b, kappa, n=-1)
+        contact_hessian_pt_after(self.states, self.soup, pt, t, self.b, ee, kappa)
+        H, _ = contact_bsr(ee, None, pt, None, self.soup.n_verts, t, out=self.collision_hessian,
+                           status=self._bsr_status, read_status=False)
+        self.collision_hessian = H
+        e = self._energy.zero_()
+        contact_energy_ee(self.states, self.soup, ee, e, kappa, n=-1)
+        contact_energy_pt(self.states, self.soup, pt, e, kappa, n=-1)
+        self._launch_ccd(self.states.dx)
+        h = self._readback
+        h["counts"][0:1].copy_(ee.cnt, non_blocking=True)
+        h["counts"][1:2].copy_(pt.cnt, non_blocking=True)
+        h["counts"][2:3].copy_(self._bsr_status, non_blocking=True)
+        h["energy"].copy_(e, non_blocking=True)
+        h["toi"].copy_(self.ccd_toi, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        n_ee, n_pt, st = (int(v) for v in h["counts"])
+        if n_ee > ee.capacity or n_pt > pt.capacity or st & 4:
+            return self.iteration_stepwise()
+        self.n_contacts, self.n_contacts_pt = n_ee, n_pt
+        toi = float(h["toi"][0])
+        return IterationResult(n_ee, n_pt, float(h["energy"][0]) * self.h * self.h, 0.9 * toi if toi < 1.0 else 1.0)
+
+    def iteration_stepwise(self) -> IterationResult:
+        """The same iteration through the public calls, one stage at a time
+        (each reads its counts or result on the host)."""
         self.detect_collision()
         self.b.zero_()
         self.compute_contact_hessian(detect=False)
