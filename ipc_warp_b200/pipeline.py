@@ -57,6 +57,9 @@ class ContactPipeline(ContactBarrierMixin):
         self._bsr_status = torch.zeros(1, dtype=torch.int32, device=dev)
         self._energy = torch.zeros(1, dtype=torch.float64, device=dev)
         pin = dev.type == "cuda"
+        self.use_graph = True
+        self._graph = None
+        self._dx_buf = torch.zeros_like(soup.x_transformed)
         self._readback = {"counts": torch.zeros(3, dtype=torch.int32, pin_memory=pin),
                           "energy": torch.zeros(1, dtype=torch.float64, pin_memory=pin),
                           "toi": torch.zeros(1, dtype=soup.x_transformed.dtype, pin_memory=pin)}
@@ -72,14 +75,53 @@ class ContactPipeline(ContactBarrierMixin):
         enqueued without a host read (list counts taken on the device, PT
         records placed after the EE count, the contact BSR sized for the
         list capacities) and the counts, the BSR status, the energy and the
-        TOI come back in one read at the end.  A list that overflowed or a
-        BSR row with too many columns sends the iteration through the
-        step-by-step calls, which grow the lists and pick the generic
-        assembly."""
+        TOI come back in one read at the end.  After one such iteration the
+        whole sequence is captured in a CUDA graph and replayed (recaptured
+        when a buffer is reallocated).  A list that overflowed or a BSR row
+        with too many columns sends the iteration through the step-by-step
+        calls, which grow the lists and pick the generic assembly."""
         if dx is not None:
             self.states.dx = dx
         if self.device.type != "cuda":
             return self.iteration_stepwise()
+        if self._dx_buf.data_ptr() != self.states.dx.data_ptr():
+            self._dx_buf.copy_(self.states.dx)
+        key = self._graph_key()
+        if self.use_graph and self._graph is not None and self._graph[0] == key:
+            self._graph[1].replay()
+        else:
+            self._enqueue()
+        torch.cuda.current_stream().synchronize()
+        h = self._readback
+        ee, pt = self.contacts_new, self.contacts_pt
+        n_ee, n_pt, st = (int(v) for v in h["counts"])
+        if n_ee > ee.capacity or n_pt > pt.capacity or st & 4:
+            self._graph = None
+            return self.iteration_stepwise()
+        if self.use_graph and (self._graph is None or self._graph[0] != key):
+            self._capture(self._graph_key())  # the eager pass may have (re)allocated buffers
+        self.n_contacts, self.n_contacts_pt = n_ee, n_pt
+        toi = float(h["toi"][0])
+        return IterationResult(n_ee, n_pt, float(h["energy"][0]) * self.h * self.h, 0.9 * toi if toi < 1.0 else 1.0)
+
+    def _graph_key(self):
+        ee, pt, t, H = self.contacts_new, self.contacts_pt, self.collision_triplets, self.collision_hessian
+        return (ee.a1a2b1b2.data_ptr(), ee.capacity, pt.a1a2b1b2.data_ptr(), pt.capacity,
+                None if t is None else t.rows.data_ptr(), None if H is None else H.values.data_ptr(),
+                None if H is None else H._ws.data_ptr(), getattr(self, "bvh_rebuild_interval", 0))
+
+    def _capture(self, key):
+        if key[-1]:  # periodic rebuilds alternate with refits: not one fixed sequence
+            return
+        g = torch.cuda.CUDAGraph()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(g):
+            self._enqueue()
+        self._graph = (key, g)
+
+    def _enqueue(self):
+        """All stages of iteration() on the current stream, ending with the
+        copies of counts, status, energy and TOI into pinned host memory."""
         ee, pt = self.contacts_new, self.contacts_pt
         self.compute_V(ret=False)
         self.update_bvh()
@@ -102,20 +144,13 @@ class ContactPipeline(ContactBarrierMixin):
         e = self._energy.zero_()
         contact_energy_ee(self.states, self.soup, ee, e, kappa, n=-1)
         contact_energy_pt(self.states, self.soup, pt, e, kappa, n=-1)
-        self._launch_ccd(self.states.dx)
+        self._launch_ccd(self._dx_buf)
         h = self._readback
         h["counts"][0:1].copy_(ee.cnt, non_blocking=True)
         h["counts"][1:2].copy_(pt.cnt, non_blocking=True)
         h["counts"][2:3].copy_(self._bsr_status, non_blocking=True)
         h["energy"].copy_(e, non_blocking=True)
         h["toi"].copy_(self.ccd_toi, non_blocking=True)
-        torch.cuda.current_stream().synchronize()
-        n_ee, n_pt, st = (int(v) for v in h["counts"])
-        if n_ee > ee.capacity or n_pt > pt.capacity or st & 4:
-            return self.iteration_stepwise()
-        self.n_contacts, self.n_contacts_pt = n_ee, n_pt
-        toi = float(h["toi"][0])
-        return IterationResult(n_ee, n_pt, float(h["energy"][0]) * self.h * self.h, 0.9 * toi if toi < 1.0 else 1.0)
 
     def iteration_stepwise(self) -> IterationResult:
         """The same iteration through the public calls, one stage at a time

@@ -56,3 +56,20 @@ def test_overflowed_list_falls_back(cuda):
     assert pipe.contacts_new.capacity >= r.n_ee > 1
     assert (r.n_ee, r.n_pt, r.alpha) == (ref.n_ee, ref.n_pt, ref.alpha)
     assert r.energy == pytest.approx(ref.energy, rel=1e-12)
+
+
+def test_graph_replay_equals_stepwise(cuda):
+    """Eager pass, then capture, then replays with a new direction each time."""
+    sc = small_scenes()[3]
+    pipe, dx = _pipe(sc, torch.float32, cuda)
+    for k in range(4):
+        dxk = dx * (1.0 + 0.25 * k)
+        r = pipe.iteration(dxk)
+        o, c, v = _bsr(pipe)
+        ref = pipe.iteration_stepwise()
+        o2, c2, v2 = _bsr(pipe)
+        assert (r.n_ee, r.n_pt, r.alpha) == (ref.n_ee, ref.n_pt, ref.alpha)
+        assert r.energy == pytest.approx(ref.energy, rel=1e-12)
+        assert torch.equal(o, o2) and torch.equal(c, c2)
+        assert ((v - v2).abs() <= 1e-5 * v2.abs().amax(dim=(1, 2), keepdim=True).clamp_min(1e-30)).all()
+    assert pipe._graph is not None  # the later calls replayed it, each against its own direction
