@@ -90,6 +90,55 @@ IPCB_D void warp_sort(int* a, int n, int lane) {
     }
 }
 
+// ascending bitonic sort of 32 E values held E per lane (element e * 32 +
+// lane in v[e]): strides below 32 exchange through shuffles, larger ones
+// between a lane's own registers
+template <int E>
+IPCB_D void reg_sort(int (&v)[E], int lane) {
+  constexpr int N = 32 * E;
+#pragma unroll
+  for (int sz = 2; sz <= N; sz <<= 1)
+#pragma unroll
+    for (int st = sz >> 1; st > 0; st >>= 1) {
+      if (st >= 32) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int f = e ^ (st >> 5);
+          if (f > e) {
+            const bool asc = ((e * 32 + lane) & sz) == 0;
+            const int a = v[e], c = v[f];
+            if (asc ? (a > c) : (a < c)) {
+              v[e] = c;
+              v[f] = a;
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int other = __shfl_xor_sync(0xffffffffu, v[e], st);
+          const bool asc = ((e * 32 + lane) & sz) == 0, lower = (lane & st) == 0;
+          v[e] = (lower == asc) ? min(v[e], other) : max(v[e], other);
+        }
+      }
+    }
+}
+
+// sort the n (<= 32 E) ints at src (INT_MAX past n) in registers; the sorted
+// values go to dst[0, 32 E) (shared memory) and, the first n, back to src
+template <int E>
+IPCB_D void sort_to(int* src, int n, int* dst, int lane) {
+  int v[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) v[e] = e * 32 + lane < n ? src[e * 32 + lane] : 0x7fffffff;
+  reg_sort<E>(v, lane);
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    dst[e * 32 + lane] = v[e];
+    if (src != dst && e * 32 + lane < n) src[e * 32 + lane] = v[e];
+  }
+}
+
 // insert c into the warp's open-addressing table (keys -1 = empty); returns
 // the slot, or -1 when the table is full
 IPCB_D int hash_insert(int* tab, int c) {
@@ -123,12 +172,11 @@ IPCB_D unsigned quad_mask(const unsigned short* __restrict__ bmask, int q) {
 // the non-zero blocks go through a shared-memory hash, are compacted and
 // sorted, and every quad gets its 4 column positions through a slot ->
 // position table.
-__global__ void __launch_bounds__(kWarps * 32) k_row_columns(int nrow, const int* __restrict__ qstart,
-                                                             int* __restrict__ qids, const int* __restrict__ ee,
-                                                             const int* __restrict__ nrec, const int* __restrict__ pt,
-                                                             const unsigned short* __restrict__ bmask,
-                                                             int* __restrict__ tmpcols, unsigned* __restrict__ qpos,
-                                                             int* __restrict__ row_nnz, int* __restrict__ status) {
+__global__ void __launch_bounds__(kWarps * 32, 12)
+    k_row_columns(int nrow, const int* __restrict__ qstart, int* __restrict__ qids, const int* __restrict__ ee,
+                  const int* __restrict__ nrec, const int* __restrict__ pt, const unsigned short* __restrict__ bmask,
+                  int* __restrict__ tmpcols, unsigned* __restrict__ qpos, int* __restrict__ row_nnz,
+                  int* __restrict__ status) {
   __shared__ int sq[kWarps][kSmemQuads];
   __shared__ int tab[kWarps][kHash];
   __shared__ int scol[kWarps][kHash];
@@ -146,14 +194,21 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_columns(int nrow, const int
   int nq2 = 32;
   while (nq2 < n) nq2 <<= 1;
   int* buf = n <= kSmemQuads ? sq[w] : tmpcols + 4LL * b + kHash;  // nq2 <= 2n <= 4n - kHash there
-  for (int k = lane; k < nq2; k += 32) buf[k] = k < n ? qids[b + k] : 0x7fffffff;
   for (int k = lane; k < kHash; k += 32) {
     tab[w][k] = -1;
     scol[w][k] = 0x7fffffff;
   }
+  if (nq2 == 32) sort_to<1>(qids + b, n, buf, lane);
+  else if (nq2 == 64) sort_to<2>(qids + b, n, buf, lane);
+  else if (nq2 == 128) sort_to<4>(qids + b, n, buf, lane);
+  else if (nq2 == 256) sort_to<8>(qids + b, n, buf, lane);
+  else {
+    for (int k = lane; k < nq2; k += 32) buf[k] = k < n ? qids[b + k] : 0x7fffffff;
+    __syncwarp();
+    warp_sort(buf, nq2, lane);
+    for (int k = lane; k < n; k += 32) qids[b + k] = buf[k];
+  }
   __syncwarp();
-  warp_sort(buf, nq2, lane);
-  for (int k = lane; k < n; k += 32) qids[b + k] = buf[k];
   // distinct columns; the first quad of each lane keeps its 4 slots
   bool ok = true;
   int slot0[4] = {-1, -1, -1, -1};
@@ -181,9 +236,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_columns(int nrow, const int
     cnt += __popc(m);
   }
   __syncwarp();
-  int P = 1;
-  while (P < cnt) P <<= 1;
-  warp_sort(scol[w], P, lane);
+  if (cnt <= 32) sort_to<1>(scol[w], 32, scol[w], lane);
+  else if (cnt <= 64) sort_to<2>(scol[w], 64, scol[w], lane);
+  else sort_to<4>(scol[w], 128, scol[w], lane);
+  __syncwarp();
   for (int k = lane; k < cnt; k += 32) slot_pos[w][hash_find(tab[w], scol[w][k])] = (unsigned char)k;
   __syncwarp();
   // each quad's 4 column positions (kAbsent for a zero block, or for a column
@@ -276,9 +332,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int*
     S sv[9];
 #pragma unroll
     for (int t = 0; t < 9; ++t) sv[t] = __shfl_sync(full, v[t], src_lane);
-    // segment sums toward the first lane of each run of equal positions
+    // segment sums toward the first lane of each run of equal positions; a
+    // batch is 8 quads and a quad's 4 columns are distinct, so a run is at
+    // most 8 long and offsets 1, 2, 4 reach all of it
 #pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
+    for (int off = 1; off < 8; off <<= 1) {
       const int op = __shfl_down_sync(full, p, off);
 #pragma unroll
       for (int t = 0; t < 9; ++t) {

@@ -16,6 +16,7 @@ Per Newton iteration:
 from __future__ import annotations
 
 import ctypes
+import gc
 import math
 from dataclasses import dataclass, field
 
@@ -620,6 +621,24 @@ class FEMContactSolver(ContactBarrierMixin):
         side = ls["stream"]
         side.wait_stream(torch.cuda.current_stream())
         ctx, handle = ctypes.c_void_p(), ctypes.c_ulonglong()
+        # as torch.cuda.graph does: collect first and keep the collector off
+        # while capturing, so no tensor freed by a collection (its allocator
+        # may record or query events) touches the capturing stream
+        torch.cuda.synchronize()
+        gc.collect()
+        gc_was_on = gc.isenabled()
+        gc.disable()
+        try:
+            self._capture_trial(side, ctx, handle, fp64, h2)
+        finally:
+            if gc_was_on:
+                gc.enable()
+        torch.cuda.current_stream().wait_stream(side)
+        ls["graph"], ls["key"] = ctx, key
+        return ctx
+
+    def _capture_trial(self, side, ctx, handle, fp64, h2):
+        ls = self._ls
         with torch.cuda.stream(side):
             s = N.stream_handle()
             N.call("ipcb_graph_while_begin", ctypes.byref(ctx), ctypes.byref(handle), s)
@@ -639,9 +658,6 @@ class FEMContactSolver(ContactBarrierMixin):
                     N.lib().ipcb_graph_destroy(ctx)
             if end_rc != 0:
                 raise N.NativeError("ipcb_graph_while_end failed: " + (N.lib().ipcb_last_error() or b"").decode())
-        torch.cuda.current_stream().wait_stream(side)
-        ls["graph"], ls["key"] = ctx, key
-        return ctx
 
     def _line_search_device(self) -> float:
         """The reference's search (same E0, bound, halving and accept test)
