@@ -483,14 +483,13 @@ class FEMContactSolver(ContactBarrierMixin):
                     self._precond_age = 0
                 self._precond_age += 1
                 x, its, rel, status = self.device_pcg.solve(self.A, self.rhs, self._precond, self.tol, self.maxiter)
-                dx = x.clone()
+                dx = x
                 if status:
                     rel = float("nan")
                     if status & 1:  # p^T A p <= 0: A is indefinite, the Cholesky fallback cannot succeed
                         self.stats.direct_failures += 1
                         self.stats.pcg_iterations.append(its)
-                        self.states.dx = dx
-                        return dx
+                        return self._set_dx(dx)
             self.stats.pcg_iterations.append(its)
             if not (rel <= self.tol) and self.direct_fallback:
                 from .direct import DirectSolverError
@@ -504,8 +503,18 @@ class FEMContactSolver(ContactBarrierMixin):
                     # compression) keeps the PCG iterate, as the reference's cg
                     # returns its last iterate; the line search then tests descent
                     self.stats.direct_failures += 1
-        self.states.dx = dx
-        return dx
+        return self._set_dx(dx)
+
+    def _set_dx(self, dx: torch.Tensor) -> torch.Tensor:
+        """states.dx = dx, copied into the existing tensor when it fits, so
+        the captured line-search graph (which holds its address) stays valid."""
+        cur = self.states.dx
+        if cur is not None and cur.shape == dx.shape and cur.dtype == dx.dtype and cur.device == dx.device:
+            if cur.data_ptr() != dx.data_ptr():
+                cur.copy_(dx)
+            return cur
+        self.states.dx = dx.clone()
+        return self.states.dx
 
     def line_search(self) -> float:
         """time_integrator_base.py:514-546 with the CCD bound."""
@@ -621,11 +630,9 @@ class FEMContactSolver(ContactBarrierMixin):
         side = ls["stream"]
         side.wait_stream(torch.cuda.current_stream())
         ctx, handle = ctypes.c_void_p(), ctypes.c_ulonglong()
-        # as torch.cuda.graph does: collect first and keep the collector off
-        # while capturing, so no tensor freed by a collection (its allocator
-        # may record or query events) touches the capturing stream
-        torch.cuda.synchronize()
-        gc.collect()
+        # keep the collector off while capturing, so no tensor freed by a
+        # collection (its allocator may record or query events) touches the
+        # capturing stream
         gc_was_on = gc.isenabled()
         gc.disable()
         try:
