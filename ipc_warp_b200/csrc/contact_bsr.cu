@@ -14,8 +14,8 @@
 //      shared-memory hash, sort the distinct columns, count them, and store
 //      each quad's 4 column positions (one byte each)
 //   3. scan the counts -> offsets
-//   4. pass B, warp per row: the row's blocks 32 at a time, sorted by column
-//      position within the warp and reduced by segments (shuffles), one
+//   4. pass B, warp per row: the row's blocks 32 at a time, grouped by column
+//      position within the warp and summed per group (shuffles), one
 //      shared-memory add per column and batch; a fixed order, so deterministic
 // A row with more than kHash distinct columns sets IPCB_STATUS_ROW_OVERFLOW
 // (the host then uses the generic assembly).
@@ -209,20 +209,34 @@ __global__ void __launch_bounds__(kWarps * 32, 12)
     for (int k = lane; k < n; k += 32) qids[b + k] = buf[k];
   }
   __syncwarp();
-  // distinct columns; the first quad of each lane keeps its 4 slots
+  // distinct columns, 32 quads at a time: lanes holding the same column
+  // (__match_any_sync) let the lowest of them insert it and share its slot;
+  // the first quad of each lane keeps its 4 slots
   bool ok = true;
   int slot0[4] = {-1, -1, -1, -1};
-  for (int k = lane; k < n; k += 32) {
-    const int q = buf[k];
-    const int4 v = record_ids(ee, n_ee, pt, q >> 2);
-    const unsigned m = quad_mask(bmask, q);
+  for (int base = 0; base < n; base += 32) {
+    const int k = base + lane;
+    int4 v = make_int4(0, 0, 0, 0);
+    unsigned m = 0;
+    if (k < n) {
+      const int q = buf[k];
+      v = record_ids(ee, n_ee, pt, q >> 2);
+      m = quad_mask(bmask, q);
+    }
 #pragma unroll
-    for (int jj = 0; jj < 4; ++jj)
-      if ((m >> jj) & 1u) {
-        const int h = hash_insert(tab[w], comp(v, jj));
+    for (int jj = 0; jj < 4; ++jj) {
+      const bool has = (m >> jj) & 1u;
+      const int c = has ? comp(v, jj) : -1;
+      const unsigned peers = __match_any_sync(0xffffffffu, c);
+      const int leader = __ffs(peers) - 1;
+      int h = -1;
+      if (has && lane == leader) h = hash_insert(tab[w], c);
+      h = __shfl_sync(0xffffffffu, h, leader);
+      if (has) {
         ok &= h >= 0;
-        if (k == lane) slot0[jj] = h;
+        if (base == 0) slot0[jj] = h;
       }
+    }
   }
   __syncwarp();
   // compact the occupied slots (stable) and sort them
@@ -271,12 +285,12 @@ __global__ void __launch_bounds__(kWarps * 32, 12)
 
 // pass B, warp per row: one 9-value accumulator per column in shared memory.
 // The lanes load the row's blocks 32 at a time (block i = quad i / 4, column
-// slot jj = i % 4) with the column positions pass A stored, the warp sorts the 32 (position, lane)
-// keys (bitonic, shuffles), gathers the values in that order and forms the
-// segment sums of equal positions (shuffle-down scan); the first lane of each
-// segment adds its sum to the column's accumulator.  Every sum runs in a
-// fixed order (batches in input order, within a batch by lane), so the result
-// is deterministic, and each column takes one shared-memory add per batch.
+// slot jj = i % 4) with the column positions pass A stored, group equal
+// positions (__match_any_sync), sum each group by pointer jumping over its
+// lanes (shuffles), and the group's lowest lane adds the sum to the column's
+// accumulator.  Every sum runs in a fixed order (batches in input order,
+// within a batch a fixed tree over the group's lanes), so the result is
+// deterministic, and each column takes one shared-memory add per batch.
 template <class S>
 __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int* __restrict__ qstart,
                                                             const int* __restrict__ qids,
@@ -300,7 +314,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int*
   }
   __syncwarp();
   const int nb = 4 * (e - b);
-  constexpr int kNone = kHash;  // sorts after every real position
+  constexpr int kNone = kHash;  // no block (past the row, or a zero block)
   for (int base = 0; base < nb; base += 32) {
     const int i = base + lane;
     int pos = kNone;
@@ -318,36 +332,27 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int*
         for (int t = 0; t < 9; ++t) v[t] = __ldg(src + t);
       }
     }
-    // bitonic sort of (pos, lane) over the warp
-    int key = (pos << 5) | lane;
+    // lanes with the same position form a group (at most 8: a batch is 8
+    // quads and a quad's 4 columns are distinct); each lane links to the next
+    // higher lane of its group and three pointer-jumping steps leave the
+    // group's sum, in a fixed order, in its lowest lane
+    const unsigned peers = __match_any_sync(full, pos);
+    const unsigned above = peers & ~((2u << lane) - 1u);
+    int nxt = above ? __ffs(above) - 1 : -1;
 #pragma unroll
-    for (int size = 2; size <= 32; size <<= 1)
-#pragma unroll
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        const int other = __shfl_xor_sync(full, key, stride);
-        const bool up = (lane & size) == 0, lower = (lane & stride) == 0;
-        key = (lower == up) ? min(key, other) : max(key, other);
-      }
-    const int src_lane = key & 31, p = key >> 5;
-    S sv[9];
-#pragma unroll
-    for (int t = 0; t < 9; ++t) sv[t] = __shfl_sync(full, v[t], src_lane);
-    // segment sums toward the first lane of each run of equal positions; a
-    // batch is 8 quads and a quad's 4 columns are distinct, so a run is at
-    // most 8 long and offsets 1, 2, 4 reach all of it
-#pragma unroll
-    for (int off = 1; off < 8; off <<= 1) {
-      const int op = __shfl_down_sync(full, p, off);
+    for (int step = 0; step < 3; ++step) {
+      const int src = nxt >= 0 ? nxt : lane;
 #pragma unroll
       for (int t = 0; t < 9; ++t) {
-        const S o = __shfl_down_sync(full, sv[t], off);
-        if (lane + off < 32 && op == p) sv[t] += o;
+        const S o = __shfl_sync(full, v[t], src);
+        if (nxt >= 0) v[t] += o;
       }
+      const int n2 = __shfl_sync(full, nxt, src);
+      nxt = nxt >= 0 ? n2 : -1;
     }
-    const int prev = __shfl_up_sync(full, p, 1);
-    if (p != kNone && (lane == 0 || prev != p)) {
+    if (pos != kNone && (peers & ((1u << lane) - 1u)) == 0) {
 #pragma unroll
-      for (int t = 0; t < 9; ++t) sacc[w][9 * p + t] += sv[t];
+      for (int t = 0; t < 9; ++t) sacc[w][9 * pos + t] += v[t];
     }
     __syncwarp();
   }
