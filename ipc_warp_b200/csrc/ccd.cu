@@ -507,8 +507,10 @@ __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, co
   if (active) {
     f3 qlo = mk3(__ldg(lo + 3 * i), __ldg(lo + 3 * i + 1), __ldg(lo + 3 * i + 2));
     f3 qhi = mk3(__ldg(hi + 3 * i), __ldg(hi + 3 * i + 1), __ldg(hi + 3 * i + 2));
-    bool ok = traverse4(nodes, n, qlo, qhi, [&](int j) {
-      if (!(i < j)) return;
+    // thread t queries the edge of Morton rank t in its own hierarchy: only
+    // leaves of higher rank are visited, so each pair is met once; it is then
+    // taken as the reference's (lower id, higher id) pair
+    bool ok = traverse4_after(nodes, n, t, qlo, qhi, [&](int j, int) {
       int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + j);
       if (ea.x == eb.x || ea.x == eb.y || ea.y == eb.x || ea.y == eb.y) return;
       if (exclude && bi == __ldg(body + eb.x)) return;
@@ -516,13 +518,15 @@ __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, co
         q[nq++] = j;
       } else if (FAST) {  // lane queue full: stage this pair directly
         const int slot = atomicAdd(cand.count, 1);
-        if (slot < cand.capacity) cand.pairs[slot] = make_int2(i, j);
+        if (slot < cand.capacity) cand.pairs[slot] = make_int2(min(i, j), max(i, j));
         else dropped = true;
       } else {
-        double tt = ee_pair_time(x0, x1, ea, eb, st);
+        const bool fwd = i < j;
+        const int2 e_lo = fwd ? ea : eb, e_hi = fwd ? eb : ea;
+        double tt = ee_pair_time(x0, x1, e_lo, e_hi, st);
         if (tt < 1.0) {
           store_toi(toi, tt);
-          sink_append<S>(sink, make_int4(ea.x, ea.y, eb.x, eb.y), i, j, tt);
+          sink_append<S>(sink, make_int4(e_lo.x, e_lo.y, e_hi.x, e_hi.y), min(i, j), max(i, j), tt);
         }
       }
     });
@@ -532,16 +536,18 @@ __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, co
   for (int k = 0; k < rounds; ++k) {
     bool has = k < nq;
     int j = has ? q[k] : 0;
-    if (!push_converged(cand, has, i, j)) {
+    if (!push_converged(cand, has, min(i, j), max(i, j))) {
       if (FAST) {
         dropped = true;
         continue;
       }
       int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + j);
-      double tt = ee_pair_time(x0, x1, ea, eb, st);
+      const bool fwd = i < j;
+      const int2 e_lo = fwd ? ea : eb, e_hi = fwd ? eb : ea;
+      double tt = ee_pair_time(x0, x1, e_lo, e_hi, st);
       if (tt < 1.0) {
         store_toi(toi, tt);
-        sink_append<S>(sink, make_int4(ea.x, ea.y, eb.x, eb.y), i, j, tt);
+        sink_append<S>(sink, make_int4(e_lo.x, e_lo.y, e_hi.x, e_hi.y), min(i, j), max(i, j), tt);
       }
     }
   }

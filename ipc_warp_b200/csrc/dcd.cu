@@ -108,16 +108,21 @@ __global__ void __launch_bounds__(128) k_dcd_ee(const float4* __restrict__ x4, c
   if (active) {
     f3 qlo = mk3(fminf(p1.x, p2.x) - qpad, fminf(p1.y, p2.y) - qpad, fminf(p1.z, p2.z) - qpad);
     f3 qhi = mk3(fmaxf(p1.x, p2.x) + qpad, fmaxf(p1.y, p2.y) + qpad, fmaxf(p1.z, p2.z) + qpad);
-    bool ok = traverse4(nodes, n, qlo, qhi, [&](int j) {
-      if (!(i < j)) return;
+    // the hierarchy is over the queries themselves: thread t is the edge of
+    // Morton rank t, so only leaves of higher rank are visited and each pair
+    // is met once; it is then stated as the reference's (lower id, higher id)
+    bool ok = traverse4_after(nodes, n, t, qlo, qhi, [&](int j, int) {
       int2 eb = __ldg(reinterpret_cast<const int2*>(edges) + j);
       if (ea.x == eb.x || ea.x == eb.y || ea.y == eb.x || ea.y == eb.y) return;
       if (exclude && bi == __ldg(body + eb.x)) return;
       if (nq < kQueue) {
         q[nq++] = j;
-      } else {
+      } else if (i < j) {
         CPEE r = closest_point_edge_edge(p1, p2, load4(x4, eb.x), load4(x4, eb.y), 1.0e-6f);
         if (r.d < l0f) append_divergent<S>(out, ea.x, ea.y, eb.x, eb.y, i, j, l0);
+      } else {
+        CPEE r = closest_point_edge_edge(load4(x4, eb.x), load4(x4, eb.y), p1, p2, 1.0e-6f);
+        if (r.d < l0f) append_divergent<S>(out, eb.x, eb.y, ea.x, ea.y, j, i, l0);
       }
     });
     if (!ok) atomicOr(status, IPCB_STATUS_STACK);
@@ -127,10 +132,16 @@ __global__ void __launch_bounds__(128) k_dcd_ee(const float4* __restrict__ x4, c
     bool has = k < nq;
     int j = has ? q[k] : 0;
     int2 eb = has ? __ldg(reinterpret_cast<const int2*>(edges) + j) : make_int2(0, 0);
+    // (lower id, higher id): the reference's orientation and argument order
+    const bool fwd = i < j;
+    const int lo_id = fwd ? i : j, hi_id = fwd ? j : i;
+    const int2 e_lo = fwd ? ea : eb, e_hi = fwd ? eb : ea;
     bool accept = false;
-    if (has) accept = closest_point_edge_edge(p1, p2, load4(x4, eb.x), load4(x4, eb.y), 1.0e-6f).d < l0f;
+    if (has)
+      accept = closest_point_edge_edge(load4(x4, e_lo.x), load4(x4, e_lo.y), load4(x4, e_hi.x), load4(x4, e_hi.y),
+                                       1.0e-6f).d < l0f;
     int slot = warp_reserve(out.cnt, accept);
-    if (accept) write_record<S>(out, slot, ea.x, ea.y, eb.x, eb.y, i, j, l0);
+    if (accept) write_record<S>(out, slot, e_lo.x, e_lo.y, e_hi.x, e_hi.y, lo_id, hi_id, l0);
   }
 }
 

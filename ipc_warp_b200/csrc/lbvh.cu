@@ -131,7 +131,9 @@ __global__ void k_karras(const unsigned* __restrict__ keys, const int* __restric
 }
 
 // Bottom-up refit: a leaf writes its box into its parent's slot; the second
-// child to arrive at a node merges both slots and continues upward.
+// child to arrive at a node merges both slots and continues upward.  The .w
+// of a slot's hi entry carries the largest leaf rank (position in Morton
+// order) below the slot: a node's is its right child's.
 __global__ void k_refit(const float* __restrict__ lo, const float* __restrict__ hi, int n,
                         const int* __restrict__ sorted, const int* __restrict__ parent, int cap,
                         float4* __restrict__ nodes, unsigned* __restrict__ flags) {
@@ -143,24 +145,26 @@ __global__ void k_refit(const float* __restrict__ lo, const float* __restrict__ 
   int code = ~prim;
   if (n == 1) {
     nodes[0] = make_float4(bl.x, bl.y, bl.z, __int_as_float(code));
-    nodes[1] = make_float4(bh.x, bh.y, bh.z, 0.f);
+    nodes[1] = make_float4(bh.x, bh.y, bh.z, __int_as_float(0));
     nodes[2] = make_float4(3.4e38f, 3.4e38f, 3.4e38f, __int_as_float(code));
-    nodes[3] = make_float4(-3.4e38f, -3.4e38f, -3.4e38f, 0.f);
+    nodes[3] = make_float4(-3.4e38f, -3.4e38f, -3.4e38f, __int_as_float(-1));
     return;
   }
   int par = parent[cap + k];
+  int last = k;  // largest leaf rank below the subtree being carried up
   // Depth is bounded by the 30 Morton bits plus 32 index bits of the
   // tie-break; the loop bound only guards against a corrupted parent array.
   for (int level = 0; level < 128; ++level) {
     int node = par >> 1, side = par & 1;
     __stcg(nodes + 4 * node + 2 * side, make_float4(bl.x, bl.y, bl.z, __int_as_float(code)));
-    __stcg(nodes + 4 * node + 2 * side + 1, make_float4(bh.x, bh.y, bh.z, 0.f));
+    __stcg(nodes + 4 * node + 2 * side + 1, make_float4(bh.x, bh.y, bh.z, __int_as_float(last)));
     __threadfence();
     unsigned old = atomicAdd(flags + node, 1u);
     if (old == 0) return;
     flags[node] = 0;
     float4 sl = __ldcg(nodes + 4 * node + 2 * (1 - side));
     float4 sh = __ldcg(nodes + 4 * node + 2 * (1 - side) + 1);
+    if (side == 0) last = __float_as_int(sh.w);
     bl = make_float3(fminf(bl.x, sl.x), fminf(bl.y, sl.y), fminf(bl.z, sl.z));
     bh = make_float3(fmaxf(bh.x, sh.x), fmaxf(bh.y, sh.y), fmaxf(bh.z, sh.z));
     if (node == 0) return;
@@ -174,7 +178,7 @@ __global__ void k_widen(const float4* __restrict__ nodes, int n_int, float4* __r
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n_int) return;
   float lo[4][3], hi[4][3];
-  int code[4];
+  int code[4], last[4];
   int m = 0;
 #pragma unroll
   for (int side = 0; side < 2; ++side) {
@@ -183,6 +187,7 @@ __global__ void k_widen(const float4* __restrict__ nodes, int n_int, float4* __r
     if (c < 0) {
       lo[m][0] = slo.x; lo[m][1] = slo.y; lo[m][2] = slo.z;
       hi[m][0] = shi.x; hi[m][1] = shi.y; hi[m][2] = shi.z;
+      last[m] = __float_as_int(shi.w);
       code[m++] = c;
     } else {
 #pragma unroll
@@ -190,6 +195,7 @@ __global__ void k_widen(const float4* __restrict__ nodes, int n_int, float4* __r
         float4 glo = __ldcg(nodes + 4 * c + 2 * s2), ghi = __ldcg(nodes + 4 * c + 2 * s2 + 1);
         lo[m][0] = glo.x; lo[m][1] = glo.y; lo[m][2] = glo.z;
         hi[m][0] = ghi.x; hi[m][1] = ghi.y; hi[m][2] = ghi.z;
+        last[m] = __float_as_int(ghi.w);
         code[m++] = __float_as_int(glo.w);
       }
     }
@@ -198,6 +204,7 @@ __global__ void k_widen(const float4* __restrict__ nodes, int n_int, float4* __r
     lo[k][0] = lo[k][1] = lo[k][2] = 3.4e38f;
     hi[k][0] = hi[k][1] = hi[k][2] = -3.4e38f;
     code[k] = -1;
+    last[k] = -1;
   }
   float4* w = wide + 8 * b;
   w[0] = make_float4(lo[0][0], lo[1][0], lo[2][0], lo[3][0]);
@@ -207,7 +214,7 @@ __global__ void k_widen(const float4* __restrict__ nodes, int n_int, float4* __r
   w[4] = make_float4(hi[0][1], hi[1][1], hi[2][1], hi[3][1]);
   w[5] = make_float4(hi[0][2], hi[1][2], hi[2][2], hi[3][2]);
   *reinterpret_cast<int4*>(w + 6) = make_int4(code[0], code[1], code[2], code[3]);
-  w[7] = make_float4(0.f, 0.f, 0.f, 0.f);
+  *reinterpret_cast<int4*>(w + 7) = make_int4(last[0], last[1], last[2], last[3]);
 }
 
 inline size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }

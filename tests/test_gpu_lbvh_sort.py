@@ -74,14 +74,18 @@ def _check_tree(bvh, lo, hi):
 
 
 def _check_wide(bvh, lo, hi):
-    """4-wide view: from wide node 0 every leaf is reached exactly once and
-    each slot box is the union of the leaves below it."""
+    """4-wide view: from wide node 0 every leaf is reached exactly once, each
+    slot box is the union of the leaves below it, and each slot's last rank
+    is the largest Morton rank below it, the slot covering a contiguous rank
+    range (what the pruned self-queries rely on)."""
     import torch
 
     n = lo.shape[0]
     m = max(n - 1, 1)
     W = bvh._view(bvh.c.wide, 32 * m, torch.float32).view(m, 8, 4).cpu().numpy()
     Wi = W.view(np.int32)
+    rank = np.empty(n, dtype=np.int64)
+    rank[bvh.sorted.cpu().numpy()] = np.arange(n)
     seen = np.zeros(n, dtype=np.int64)
 
     def visit(node):
@@ -98,6 +102,8 @@ def _check_wide(bvh, lo, hi):
             else:
                 sub = visit(c)
             assert np.array_equal(blo, lo[sub].min(axis=0)) and np.array_equal(bhi, hi[sub].max(axis=0))
+            r = np.sort(rank[sub])
+            assert int(Wi[node, 7, k]) == r[-1] and r[-1] - r[0] == len(r) - 1
             leaves += sub
         return leaves
 
