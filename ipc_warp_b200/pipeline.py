@@ -13,11 +13,13 @@ iteration (dynamic_contacts.py:272-308 with contact.py:539-725):
 """
 from __future__ import annotations
 
+import ctypes
 from dataclasses import dataclass
 
 import numpy as np
 import torch
 
+from . import _native as N
 from . import contact
 from .contact import Soup
 from .bsr import Triplets, contact_bsr
@@ -59,6 +61,10 @@ class ContactPipeline(ContactBarrierMixin):
         pin = dev.type == "cuda"
         self.use_graph = True
         self._graph = None
+        if pin:
+            self._side = torch.cuda.Stream(device=dev)
+            self._ee_done = torch.cuda.Event()
+            self._toi_ws_pt = torch.empty_like(self._toi_ws)
         self._dx_buf = torch.zeros_like(soup.x_transformed)
         self._readback = {"counts": torch.zeros(3, dtype=torch.int32, pin_memory=pin),
                           "energy": torch.zeros(1, dtype=torch.float64, pin_memory=pin),
@@ -120,8 +126,82 @@ class ContactPipeline(ContactBarrierMixin):
         self._graph = (key, g)
 
     def _enqueue(self):
-        """All stages of iteration() on the current stream, ending with the
-        copies of counts, status, energy and TOI into pinned host memory."""
+        """All stages of iteration(), ending with the copies of counts,
+        status, energy and TOI into pinned host memory.  The triangle side
+        (box refit, PT query, PT records, swept-box refit, PT TOI) runs on a
+        second stream beside the edge side, so each pair of latency-bound
+        launches overlaps; the streams join before the contact BSR and
+        before the read."""
+        if getattr(self, "bvh_rebuild_interval", 0) or not self.has_triangles:
+            return self._enqueue_serial()
+        ee, pt = self.contacts_new, self.contacts_pt
+        main = torch.cuda.current_stream()
+        side = self._side
+        soup = ctypes.byref(self.soup.c_struct())
+        kappa = float(self.contact_stiffness)
+        cap = ee.capacity + pt.capacity
+        t = self.collision_triplets
+        if t is None or t.rows.shape[0] < 16 * cap:
+            t = self.collision_triplets = Triplets.zeros(16 * cap, self.soup.xcs.dtype, self.device)
+        self.compute_V(ret=False)
+        self._pack()
+        self.b.zero_()
+        side.wait_stream(main)
+        with torch.cuda.stream(side):
+            self._triangle_aabbs()
+            self.tri_mesh.refit()
+            self._launch_dcd("pt")
+        N.call("ipcb_edge_aabbs", soup, N.ptr(self.x4), float(contact._thickness + contact.buffer),
+               N.ptr(self.bvh_edges_lower), N.ptr(self.bvh_edges_upper), N.stream_handle())
+        self.bvh_edges.refit()
+        self._launch_dcd("ee")
+        self._ee_done.record(main)
+        contact_hessian_ee(self.states, self.soup, ee, t, self.b, kappa, n=-1)
+        with torch.cuda.stream(side):
+            side.wait_event(self._ee_done)  # the PT records follow the EE count
+            contact_hessian_pt_after(self.states, self.soup, pt, t, self.b, ee, kappa)
+        main.wait_stream(side)
+        H, _ = contact_bsr(ee, None, pt, None, self.soup.n_verts, t, out=self.collision_hessian,
+                           status=self._bsr_status, read_status=False)
+        self.collision_hessian = H
+        e = self._energy.zero_()
+        contact_energy_ee(self.states, self.soup, ee, e, kappa, n=-1)
+        contact_energy_pt(self.states, self.soup, pt, e, kappa, n=-1)
+        # CCD: the two queries stage candidates in separate workspaces
+        pad = 1e-7
+        N.call("ipcb_add_dx", soup, N.ptr(self._dx_buf), N.ptr(self.ccd_x1), N.stream_handle())
+        self.ccd_toi.fill_(1.0)
+        self._status.zero_()
+        side.wait_stream(main)
+        with torch.cuda.stream(side):
+            s2 = N.stream_handle()
+            N.call("ipcb_swept_triangle_aabbs", soup, N.ptr(self.ccd_x1), pad, N.ptr(self.ccd_triangle_lower),
+                   N.ptr(self.ccd_triangle_upper), s2)
+            self.ccd_triangle_bvh.refit(self.ccd_triangle_lower, self.ccd_triangle_upper)
+            N.call("ipcb_point_triangle_toi", soup, N.ptr(self.ccd_x1), ctypes.byref(self.ccd_triangle_bvh.c), pad,
+                   int(self.disable_self_collision), N.ptr(self.ccd_toi), N.ptr(self._status),
+                   N.ptr(self._toi_ws_pt), self._toi_ws_pt.numel(), s2)
+        s1 = N.stream_handle()
+        N.call("ipcb_swept_edge_aabbs", soup, N.ptr(self.ccd_x1), pad, N.ptr(self.ccd_edge_lower),
+               N.ptr(self.ccd_edge_upper), s1)
+        self.ccd_edge_bvh.refit(self.ccd_edge_lower, self.ccd_edge_upper)
+        N.call("ipcb_edge_edge_toi", soup, N.ptr(self.ccd_x1), ctypes.byref(self.ccd_edge_bvh.c),
+               N.ptr(self.ccd_edge_lower), N.ptr(self.ccd_edge_upper), int(self.disable_self_collision),
+               N.ptr(self.ccd_toi), N.ptr(self._status), N.ptr(self._toi_ws), self._toi_ws.numel(), s1)
+        main.wait_stream(side)
+        self._copy_results(e)
+
+    def _copy_results(self, e):
+        ee, pt = self.contacts_new, self.contacts_pt
+        h = self._readback
+        h["counts"][0:1].copy_(ee.cnt, non_blocking=True)
+        h["counts"][1:2].copy_(pt.cnt, non_blocking=True)
+        h["counts"][2:3].copy_(self._bsr_status, non_blocking=True)
+        h["energy"].copy_(e, non_blocking=True)
+        h["toi"].copy_(self.ccd_toi, non_blocking=True)
+
+    def _enqueue_serial(self):
+        """_enqueue on one stream (periodic BVH rebuilds, or no triangles)."""
         ee, pt = self.contacts_new, self.contacts_pt
         self.compute_V(ret=False)
         self.update_bvh()
@@ -145,12 +225,7 @@ class ContactPipeline(ContactBarrierMixin):
         contact_energy_ee(self.states, self.soup, ee, e, kappa, n=-1)
         contact_energy_pt(self.states, self.soup, pt, e, kappa, n=-1)
         self._launch_ccd(self._dx_buf)
-        h = self._readback
-        h["counts"][0:1].copy_(ee.cnt, non_blocking=True)
-        h["counts"][1:2].copy_(pt.cnt, non_blocking=True)
-        h["counts"][2:3].copy_(self._bsr_status, non_blocking=True)
-        h["energy"].copy_(e, non_blocking=True)
-        h["toi"].copy_(self.ccd_toi, non_blocking=True)
+        self._copy_results(e)
 
     def iteration_stepwise(self) -> IterationResult:
         """The same iteration through the public calls, one stage at a time
