@@ -63,7 +63,10 @@ class ContactPipeline(ContactBarrierMixin):
         self._graph = None
         if pin:
             self._side = torch.cuda.Stream(device=dev)
+            self._ccd_e = torch.cuda.Stream(device=dev)
+            self._ccd_t = torch.cuda.Stream(device=dev)
             self._ee_done = torch.cuda.Event()
+            self._pt_done = torch.cuda.Event()
             self._toi_ws_pt = torch.empty_like(self._toi_ws)
         self._dx_buf = torch.zeros_like(soup.x_transformed)
         self._readback = {"counts": torch.zeros(3, dtype=torch.int32, pin_memory=pin),
@@ -127,18 +130,22 @@ class ContactPipeline(ContactBarrierMixin):
 
     def _enqueue(self):
         """All stages of iteration(), ending with the copies of counts,
-        status, energy and TOI into pinned host memory.  The triangle side
-        (box refit, PT query, PT records, swept-box refit, PT TOI) runs on a
-        second stream beside the edge side, so each pair of latency-bound
-        launches overlaps; the streams join before the contact BSR and
-        before the read."""
+        status, energy and TOI into pinned host memory, on four streams: the
+        triangle side (box refit, PT query, PT records) beside the edge side,
+        and each CCD query (swept boxes, refit, TOI; own candidate workspace)
+        as soon as the discrete query on its hierarchy is done, beside the
+        narrow phase, the contact BSR and the energy.  Nothing after the
+        discrete queries reads the hierarchies, so the CCD refits cannot
+        disturb them; every stream joins the first before the read."""
         if getattr(self, "bvh_rebuild_interval", 0) or not self.has_triangles:
             return self._enqueue_serial()
         ee, pt = self.contacts_new, self.contacts_pt
         main = torch.cuda.current_stream()
-        side = self._side
+        side, ccd_e, ccd_t = self._side, self._ccd_e, self._ccd_t
         soup = ctypes.byref(self.soup.c_struct())
         kappa = float(self.contact_stiffness)
+        excl = int(self.disable_self_collision)
+        pad = 1e-7
         cap = ee.capacity + pt.capacity
         t = self.collision_triplets
         if t is None or t.rows.shape[0] < 16 * cap:
@@ -146,16 +153,38 @@ class ContactPipeline(ContactBarrierMixin):
         self.compute_V(ret=False)
         self._pack()
         self.b.zero_()
+        N.call("ipcb_add_dx", soup, N.ptr(self._dx_buf), N.ptr(self.ccd_x1), N.stream_handle())
+        self.ccd_toi.fill_(1.0)
+        self._status.zero_()
         side.wait_stream(main)
         with torch.cuda.stream(side):
             self._triangle_aabbs()
             self.tri_mesh.refit()
             self._launch_dcd("pt")
+            self._pt_done.record(side)
         N.call("ipcb_edge_aabbs", soup, N.ptr(self.x4), float(contact._thickness + contact.buffer),
                N.ptr(self.bvh_edges_lower), N.ptr(self.bvh_edges_upper), N.stream_handle())
         self.bvh_edges.refit()
         self._launch_dcd("ee")
         self._ee_done.record(main)
+        with torch.cuda.stream(ccd_e):
+            ccd_e.wait_event(self._ee_done)
+            s1 = N.stream_handle()
+            N.call("ipcb_swept_edge_aabbs", soup, N.ptr(self.ccd_x1), pad, N.ptr(self.ccd_edge_lower),
+                   N.ptr(self.ccd_edge_upper), s1)
+            self.ccd_edge_bvh.refit(self.ccd_edge_lower, self.ccd_edge_upper)
+            N.call("ipcb_edge_edge_toi", soup, N.ptr(self.ccd_x1), ctypes.byref(self.ccd_edge_bvh.c),
+                   N.ptr(self.ccd_edge_lower), N.ptr(self.ccd_edge_upper), excl, N.ptr(self.ccd_toi),
+                   N.ptr(self._status), N.ptr(self._toi_ws), self._toi_ws.numel(), s1)
+        with torch.cuda.stream(ccd_t):
+            ccd_t.wait_event(self._pt_done)
+            s2 = N.stream_handle()
+            N.call("ipcb_swept_triangle_aabbs", soup, N.ptr(self.ccd_x1), pad, N.ptr(self.ccd_triangle_lower),
+                   N.ptr(self.ccd_triangle_upper), s2)
+            self.ccd_triangle_bvh.refit(self.ccd_triangle_lower, self.ccd_triangle_upper)
+            N.call("ipcb_point_triangle_toi", soup, N.ptr(self.ccd_x1), ctypes.byref(self.ccd_triangle_bvh.c), pad,
+                   excl, N.ptr(self.ccd_toi), N.ptr(self._status), N.ptr(self._toi_ws_pt),
+                   self._toi_ws_pt.numel(), s2)
         contact_hessian_ee(self.states, self.soup, ee, t, self.b, kappa, n=-1)
         with torch.cuda.stream(side):
             side.wait_event(self._ee_done)  # the PT records follow the EE count
@@ -167,28 +196,8 @@ class ContactPipeline(ContactBarrierMixin):
         e = self._energy.zero_()
         contact_energy_ee(self.states, self.soup, ee, e, kappa, n=-1)
         contact_energy_pt(self.states, self.soup, pt, e, kappa, n=-1)
-        # CCD: the two queries stage candidates in separate workspaces
-        pad = 1e-7
-        N.call("ipcb_add_dx", soup, N.ptr(self._dx_buf), N.ptr(self.ccd_x1), N.stream_handle())
-        self.ccd_toi.fill_(1.0)
-        self._status.zero_()
-        side.wait_stream(main)
-        with torch.cuda.stream(side):
-            s2 = N.stream_handle()
-            N.call("ipcb_swept_triangle_aabbs", soup, N.ptr(self.ccd_x1), pad, N.ptr(self.ccd_triangle_lower),
-                   N.ptr(self.ccd_triangle_upper), s2)
-            self.ccd_triangle_bvh.refit(self.ccd_triangle_lower, self.ccd_triangle_upper)
-            N.call("ipcb_point_triangle_toi", soup, N.ptr(self.ccd_x1), ctypes.byref(self.ccd_triangle_bvh.c), pad,
-                   int(self.disable_self_collision), N.ptr(self.ccd_toi), N.ptr(self._status),
-                   N.ptr(self._toi_ws_pt), self._toi_ws_pt.numel(), s2)
-        s1 = N.stream_handle()
-        N.call("ipcb_swept_edge_aabbs", soup, N.ptr(self.ccd_x1), pad, N.ptr(self.ccd_edge_lower),
-               N.ptr(self.ccd_edge_upper), s1)
-        self.ccd_edge_bvh.refit(self.ccd_edge_lower, self.ccd_edge_upper)
-        N.call("ipcb_edge_edge_toi", soup, N.ptr(self.ccd_x1), ctypes.byref(self.ccd_edge_bvh.c),
-               N.ptr(self.ccd_edge_lower), N.ptr(self.ccd_edge_upper), int(self.disable_self_collision),
-               N.ptr(self.ccd_toi), N.ptr(self._status), N.ptr(self._toi_ws), self._toi_ws.numel(), s1)
-        main.wait_stream(side)
+        main.wait_stream(ccd_e)
+        main.wait_stream(ccd_t)
         self._copy_results(e)
 
     def _copy_results(self, e):
