@@ -27,12 +27,36 @@ __global__ void __launch_bounds__(128, 3) k_contact_hessian(const S* __restrict_
                                                          int* __restrict__ rows, int* __restrict__ cols,
                                                          S* __restrict__ vals, S* __restrict__ bforce,
                                                          unsigned short* __restrict__ block_mask) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int cnt = list_count<S>(L, n);
-  if (i >= cnt) return;
+  // The CTA's 128 records are classified (record_class) and handed to the
+  // threads in class order, so most warps run one path of
+  // contact_hessian_item instead of the union of their records' paths (a
+  // record's outputs go to its own slots; only the order of the force
+  // atomics changes).
+  __shared__ int s_count[4], s_cursor[4], s_order[128];
+  const int cnt = list_count<S>(L, n);
+  const int base = blockIdx.x * 128;
+  if (base >= cnt) return;  // the whole CTA
+  const int tid = threadIdx.x, m = min(128, cnt - base);
+  if (tid < 4) s_count[tid] = 0;
+  __syncthreads();
+  const int cls = tid < m ? record_class<S, KIND>(x, xcs, L, base + tid) : -1;
+  if (cls >= 0) atomicAdd(&s_count[cls], 1);
+  __syncthreads();
+  if (tid == 0) {
+    int run = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      s_cursor[k] = run;
+      run += s_count[k];
+    }
+  }
+  __syncthreads();
+  if (cls >= 0) s_order[atomicAdd(&s_cursor[cls], 1)] = base + tid;
+  __syncthreads();
+  if (tid >= m) return;
   // offset_dev: the records follow another list's min(count, offset) records
   const int off = offset_dev ? min(*offset_dev, offset) : offset;
-  contact_hessian_item<S, KIND>(x, xcs, L, i, off, kappa, rows, cols, vals, bforce, block_mask);
+  contact_hessian_item<S, KIND>(x, xcs, L, s_order[tid], off, kappa, rows, cols, vals, bforce, block_mask);
 }
 
 template <class S, int KIND>

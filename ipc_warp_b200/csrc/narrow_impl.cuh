@@ -436,6 +436,35 @@ IPCB_D void mollifier(const d3* xd, double eps_x, double& mv, double (&gm)[12]) 
   gm[9] = dm * dxb.x; gm[10] = dm * dxb.y; gm[11] = dm * dxb.z;
 }
 
+// Cost class of a record, for giving the records that take the same path
+// through contact_hessian_item to the same warps: 0 inactive (dist >= l0:
+// zero blocks), 1 no eigen-solve (point-point feature, or near-parallel EE
+// edges: mollified gradient term only), 2 the 3x3 restriction (point-edge),
+// 3 the 5x5 restriction (edge-edge, point-triangle).  Mirrors the gate and
+// the feature dispatch of contact_hessian_item.
+template <class S, int KIND>
+IPCB_D int record_class(const S* __restrict__ x, const S* __restrict__ xcs, const ipcb_contacts& L, int i) {
+  const int4 id = __ldg(reinterpret_cast<const int4*>(L.a1a2b1b2) + i);
+  const S l0 = static_cast<const S*>(L.l0)[i];
+  const v3<S> xs[4] = {ldx(x, id.x), ldx(x, id.y), ldx(x, id.z), ldx(x, id.w)};
+  const f3 xf[4] = {to_f(xs[0]), to_f(xs[1]), to_f(xs[2]), to_f(xs[3])};
+  if (KIND == 0) {
+    const CPEE d = closest_point_edge_edge(xf[0], xf[1], xf[2], xf[3], 1.0e-6f);
+    if (!(S(d.d) < l0)) return 0;
+    const S eps_x = ee_eps_x(xcs, id);
+    const v3<S> ea = esub(xs[1], xs[0]), eb = esub(xs[3], xs[2]);
+    const v3<S> cr = ecross(ea, eb);
+    if (eps_x > S(0) && edot(cr, cr) < eps_x) return 1;
+    const S s = S(d.s), t = S(d.t), feps = S(1.0e-6), hi = S(1.0) - S(1.0e-6);
+    const bool sb = s <= feps || s >= hi, tb = t <= feps || t >= hi;
+    return sb && tb ? 1 : (sb || tb ? 2 : 3);
+  } else {
+    const CPT cp = closest_point_triangle(xf[0], xf[1], xf[2], xf[3]);
+    if (!(S(cp.d) < l0)) return 0;
+    return cp.type <= 2 ? 1 : (cp.type <= 5 ? 2 : 3);
+  }
+}
+
 // One record of contact_hessian_ee / _pt: 16 blocks at (offset + i)*16,
 // force into bforce, block mask.  T: arithmetic type of the eigen-solve and
 // of H (float for S=float).
