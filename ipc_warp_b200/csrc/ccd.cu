@@ -484,9 +484,9 @@ IPCB_D bool push_converged(const CandList& L, bool has, int a, int b) {
 // the queued pairs converged (divergent pushes would serialise on the count).
 // FAST: stage pairs only (a lane whose queue is full pushes on its own); a
 // pair that does not fit in the list raises cand.overflow instead of being
-// solved here, which keeps the cubic solver out of this kernel (48 instead of
-// 255 registers).  !FAST (run only
-// when *gate is set, with a zero-capacity list): every pair solved in place.
+// solved here, which keeps the cubic solver out of this kernel (56 instead of
+// 255 registers).  !FAST (run only when *gate is set, with a zero-capacity
+// list): every pair solved in place.
 template <class S, bool FAST>
 __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, const S* __restrict__ x1,
                                                     const int* __restrict__ edges, const int* __restrict__ body,
