@@ -36,6 +36,16 @@ def test_sizes_and_args_without_gpu():
     # argument validation happens before any launch
     assert L.ipcb_sort_pairs_u32(None, None, -1, 8, None, 0, None) == 1
     assert L.ipcb_contact_hessian(5, None, None, 0, 0, 1.0, None, None, None, None, None, None) == 1
+    assert L.ipcb_contact_hessian_after(1, None, None, -1, 0, None, 1.0, None, None, None, None, None, None) == 1
+    # contact BSR: negative counts mean "read on the device" and need the lists' count words
+    assert L.ipcb_contact_bsr_workspace(10, 5) > L.ipcb_contact_bsr_workspace(1, 5)
+    ee = _native.Contacts(None, None, None, None, None, None, 4)  # capacity 4, no count word
+    pt = _native.Contacts(None, None, None, None, None, None, 4)
+    nnz, st = ctypes.c_int(), ctypes.c_int()
+    assert L.ipcb_contact_bsr(ctypes.byref(ee), -1, ctypes.byref(pt), -1, 8, None, None, 0, ctypes.byref(nnz),
+                              None, None, ctypes.byref(nnz), ctypes.byref(st), None, 0, None) == 1
+    assert L.ipcb_contact_bsr(ctypes.byref(ee), 5, ctypes.byref(pt), 0, 8, None, None, 0, ctypes.byref(nnz),
+                              None, None, ctypes.byref(nnz), ctypes.byref(st), None, 0, None) == 1  # 5 > capacity
 
 
 def test_direct_library_exports_header_symbols():
