@@ -134,8 +134,7 @@ def peaks():
 # record 24 + positions 48 + 16 triplets (4+4+36) 704 + force 48; EE adds rest positions 48
 NARROW_BYTES = {"pt": 824, "ee": 872}
 # dram__bytes_read.sum + dram__bytes_write.sum of the EE + PT narrow-phase launches
-# of one step on this workload (one-pass ncu capture of the full workload,
-# profiles/k_contact_hessian_rod_bundle.md)
+# of one step on this workload (one-pass ncu capture of the full workload)
 NARROW_DRAM_BYTES_PER_STEP = 441.4e6
 
 

@@ -112,11 +112,16 @@ int ipcb_lbvh_refit(const ipcb_lbvh* bvh, const float* lower, const float* upper
  * Same result as ipcb_lbvh_build; the build scratch is a file-scope
  * __device__ array of ipcb_lbvh_build_noalloc_scratch_bytes() (about 2.2 MB)
  * that every GPU loading the library keeps until exit, so n is limited to
- * IPCB_LBVH_NOALLOC_MAX_PRIMS (larger n returns IPCB_E_ARG).  The first call
- * on a device looks the array's device address up (cudaGetSymbolAddress) with
- * that device current: make that first call before any stream capture.  All
- * calls share the one array, so calls that overlap on the GPU race; the build
- * clears what must start at zero, and the array keeps the last call's data. */
+ * IPCB_LBVH_NOALLOC_MAX_PRIMS (larger n returns IPCB_E_ARG, as does n above the
+ * hierarchy's capacity, each with its own ipcb_last_error text).  Every call
+ * made outside stream capture looks the array's device address up
+ * (cudaGetSymbolAddress) in the context current on the calling thread, so the
+ * address stays right after cudaDeviceReset or in a non-primary context; a
+ * call inside capture uses the address that the last call outside capture
+ * found for that device ordinal, so make one call on each device before
+ * capturing, and again after a cudaDeviceReset.  All calls share the one
+ * array, so calls that overlap on the GPU race; the build clears what must
+ * start at zero, and the array keeps the last call's data. */
 #define IPCB_LBVH_NOALLOC_MAX_PRIMS (1 << 18)
 size_t ipcb_lbvh_build_noalloc_scratch_bytes(void);
 int ipcb_lbvh_build_noalloc(ipcb_lbvh* bvh, const float* lower, const float* upper, int n, ipcb_stream s);
@@ -415,7 +420,10 @@ int ipcb_newton_values(int fp64, const int* nnz, int capacity, const int* c_rows
  * State of one backtracking search in device memory.  ipcb_ls_begin: E0 from
  * the energy accumulators acc[3] (acc[0] elastic Psi, acc[1] barrier, acc[2]
  * inertia + attachment; E = h2 (acc0 + acc1) + acc2), the bound from the CCD
- * toi (0.9 toi if toi < 1, else 1).  Per trial: ipcb_ls_trial (x = x_tmp -
+ * toi (0.9 toi if toi < 1, else 1).  status (may be null) is the CCD queries'
+ * status word: with IPCB_STATUS_STACK or IPCB_STATUS_ROOT_ITERS set the TOI
+ * is no bound, so the search is refused (refused = the bits, bound 0, one
+ * trial at alpha 0, nothing accepted).  Per trial: ipcb_ls_trial (x = x_tmp -
  * alpha dx, acc zeroed), the energy kernels, ipcb_ls_accept (accept if E1
  * finite and < E0, else halve alpha; stops at alpha <= eps max(1, ub), at
  * max_it trials or when a contact list count exceeds its capacity; sets the
@@ -423,7 +431,7 @@ int ipcb_newton_values(int fp64, const int* nnz, int capacity, const int* c_rows
  * when nothing was accepted. */
 typedef struct {
   double E0, E1, alpha, ub, eps, alpha_accepted;
-  int it, max_it, accepted, done, overflow, max_ee, max_pt, pad;
+  int it, max_it, accepted, done, overflow, max_ee, max_pt, refused;
 } ipcb_ls_state;
 /* acc += inertia 1/2 m |x - x~|^2 (x~ = x0 + h xdot + h^2 g) + attachment
  * 1/2 k_att h^2 |x - target|^2 over fixed vertices, in double; fixed: uint8[V]
@@ -431,8 +439,8 @@ typedef struct {
 int ipcb_ls_inertia(int fp64, int n, const void* x, const void* x0, const void* xdot, const double* gravity, double h,
                     const double* mass, const unsigned char* fixed, const void* target, double k_att, double* out,
                     ipcb_stream s);
-int ipcb_ls_begin(ipcb_ls_state* st, const void* toi, int fp64, const double* acc, double h2, double eps, int max_it,
-                  const ipcb_contacts* ee, const ipcb_contacts* pt, ipcb_stream s);
+int ipcb_ls_begin(ipcb_ls_state* st, const void* toi, int fp64, const int* status, const double* acc, double h2,
+                  double eps, int max_it, const ipcb_contacts* ee, const ipcb_contacts* pt, ipcb_stream s);
 int ipcb_ls_trial(const ipcb_ls_state* st, int fp64, int n_verts, const void* x_tmp, const void* dx, void* x,
                   double* acc, ipcb_stream s);
 int ipcb_ls_accept(ipcb_ls_state* st, const double* acc, double h2, const ipcb_contacts* ee, const ipcb_contacts* pt,

@@ -47,7 +47,7 @@ class Terms(ctypes.Structure):
 class LsState(ctypes.Structure):
     _fields_ = [("E0", c_double), ("E1", c_double), ("alpha", c_double), ("ub", c_double), ("eps", c_double),
                 ("alpha_accepted", c_double), ("it", c_int), ("max_it", c_int), ("accepted", c_int), ("done", c_int),
-                ("overflow", c_int), ("max_ee", c_int), ("max_pt", c_int), ("pad", c_int)]
+                ("overflow", c_int), ("max_ee", c_int), ("max_pt", c_int), ("refused", c_int)]
 
 
 class AlSet(ctypes.Structure):
@@ -142,7 +142,7 @@ SIGNATURES = {
     "ipcb_newton_values": (c_int, [c_int, P, c_int, P, P, P, P, P, P, P, c_double, P, P, c_double, P, P]),
     "ipcb_abi_hash": (ctypes.c_char_p, []),
     "ipcb_ls_inertia": (c_int, [c_int, c_int, P, P, P, P, c_double, P, P, P, c_double, P, P]),
-    "ipcb_ls_begin": (c_int, [P, P, c_int, P, c_double, c_double, c_int, CP, CP, P]),
+    "ipcb_ls_begin": (c_int, [P, P, c_int, P, P, c_double, c_double, c_int, CP, CP, P]),
     "ipcb_ls_trial": (c_int, [P, c_int, c_int, P, P, P, P, P]),
     "ipcb_ls_accept": (c_int, [P, P, c_double, CP, CP, ctypes.c_ulonglong, P]),
     "ipcb_ls_finish": (c_int, [P, c_int, c_int, P, P, P]),

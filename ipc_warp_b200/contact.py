@@ -18,6 +18,7 @@ reference (dhat = l0 = 2 * _thickness, contact.py:180).
 from __future__ import annotations
 
 import ctypes
+import warnings
 from contextlib import nullcontext
 from dataclasses import dataclass
 
@@ -33,6 +34,11 @@ buffer = _thickness
 eps = 1e-6
 disable_self_collision = False
 verbose = False
+
+# IPCB_STATUS_STACK | IPCB_STATUS_ROOT_ITERS: a query that ran out of its
+# traversal stack, its visit bound or its root iterations may have missed an
+# impact, so its TOI is no bound
+QUERY_FAILED = 1 | 2
 
 
 @dataclass
@@ -153,10 +159,12 @@ class ContactSolverBase:
         self.n_contacts = 0
         self.n_contacts_pt = 0
         self._status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.query_status = 0  # status word of the last detect_collision / collision_free_step
+        self.ccd_refusals = 0  # collision_free_step calls refused for a failed query
         # CCD candidate staging (a query that overflows it is redone inline)
         cap = max(1 << 20, 4 * max(n_edges, n_nodes))
         self._toi_ws = torch.empty(N.size("ipcb_toi_workspace", cap), dtype=torch.uint8, device=dev)
-        self._counts_host = torch.zeros(2, dtype=torch.int32).pin_memory() if dev.type == "cuda" else None
+        self._counts_host = torch.zeros(3, dtype=torch.int32).pin_memory() if dev.type == "cuda" else None
 
     # --------------------------------------------------------------- hooks
     def profile_timer(self, name):
@@ -224,19 +232,24 @@ class ContactSolverBase:
                    ctypes.byref(self.contacts_pt.c_struct()), N.ptr(self._status), s)
 
     def _read_counts(self):
+        """One host read of both list counts and the query status word (kept
+        in ``query_status``)."""
         h = self._counts_host
         h[0:1].copy_(self.contacts_new.cnt, non_blocking=True)
         if self.has_triangles:
             h[1:2].copy_(self.contacts_pt.cnt, non_blocking=True)
         else:
             h[1] = 0
+        h[2:3].copy_(self._status, non_blocking=True)
         torch.cuda.current_stream().synchronize()
+        self.query_status = int(h[2])
         return int(h[0]), int(h[1])
 
     def detect_collision(self):
         """contact.py:687-725.  Both queries are launched before the single
         count read; an overflowed list is grown and its query relaunched."""
         self.compute_V(ret=False)
+        self._status.zero_()
         with self.profile_timer("collision BVH refit"):
             self.update_bvh()
         with self.profile_timer("EE collision query"):
@@ -258,6 +271,9 @@ class ContactSolverBase:
         if relaunched:
             n_ee, n_pt = self._read_counts()
         self.n_contacts, self.n_contacts_pt = n_ee, (n_pt if self.has_triangles else 0)
+        if self.query_status & QUERY_FAILED:
+            warnings.warn(f"contact query ran out of its traversal bound (status {self.query_status}): "
+                          "the candidate lists may be incomplete", RuntimeWarning, stacklevel=2)
         if verbose:
             print(f"n ee contacts = {self.n_contacts}\nn pt contacts = {self.n_contacts_pt}")
 
@@ -266,11 +282,28 @@ class ContactSolverBase:
         """contact.py:539-585: conservative CCD bound for x -= alpha * dx;
         returns 0.9 * toi if toi < 1 else 1."""
         self._launch_ccd(dx)
-        toi = float(self.ccd_toi.item())
+        return self._step_bound()
+
+    def _step_bound(self) -> float:
+        """One host read of the TOI and the query status.  The bound is
+        0.9 * toi (1 when nothing collides), or 0 -- no step -- when a query
+        set IPCB_STATUS_STACK or IPCB_STATUS_ROOT_ITERS: such a query may have
+        missed an earlier impact, so its TOI is no bound.  Refusals are
+        counted in ``ccd_refusals``."""
+        toi, status = torch.cat([self.ccd_toi.double(), self._status.double()]).tolist()
+        return self._bound_from(toi, int(status))
+
+    def _bound_from(self, toi: float, status: int) -> float:
+        self.query_status = status
+        if status & QUERY_FAILED:
+            self.ccd_refusals += 1
+            return 0.0
         return 0.9 * toi if toi < 1.0 else 1.0
 
-    def _launch_ccd(self, dx: torch.Tensor):
-        """The CCD queries of collision_free_step; the TOI stays in ccd_toi."""
+    def _launch_ccd(self, dx: torch.Tensor, reset_status: bool = True):
+        """The CCD queries of collision_free_step; the TOI stays in ccd_toi
+        and the queries' status bits in _status (zeroed first unless
+        reset_status is False)."""
         soup = self.soup.c_struct()
         s = N.stream_handle()
         pad = 1e-7
@@ -279,7 +312,8 @@ class ContactSolverBase:
                N.ptr(self.ccd_edge_upper), s)
         self.ccd_edge_bvh.refit(self.ccd_edge_lower, self.ccd_edge_upper)
         self.ccd_toi.fill_(1.0)
-        self._status.zero_()
+        if reset_status:
+            self._status.zero_()
         N.call("ipcb_edge_edge_toi", ctypes.byref(soup), N.ptr(self.ccd_x1), ctypes.byref(self.ccd_edge_bvh.c),
                N.ptr(self.ccd_edge_lower), N.ptr(self.ccd_edge_upper), int(self.disable_self_collision),
                N.ptr(self.ccd_toi), N.ptr(self._status), N.ptr(self._toi_ws), self._toi_ws.numel(), s)
@@ -341,8 +375,7 @@ class ContactSolverBase:
             self.n_contacts_pt = n
         else:
             self.n_contacts_pt = 0
-        toi = float(self.ccd_toi.item())
-        return 0.9 * toi if toi < 1.0 else 1.0
+        return self._step_bound()
 
     @property
     def status(self) -> int:

@@ -14,6 +14,10 @@ void set_error(const char* where, cudaError_t e) {
   snprintf(g_err, sizeof(g_err), "%s: %s", where, cudaGetErrorString(e));
 }
 void set_error_msg(const char* msg) { snprintf(g_err, sizeof(g_err), "%s", msg); }
+static int arg_error(const char* msg) {
+  set_error_msg(msg);
+  return IPCB_E_ARG;
+}
 const char* last_error() { return g_err; }
 
 int check_launch(const char* where) {
@@ -285,11 +289,18 @@ size_t ipcb_lbvh_build_workspace(int n) { return 256 + sort::workspace_bytes<uns
 
 int ipcb_lbvh_build(ipcb_lbvh* bvh, const float* lower, const float* upper, int n, void* ws, size_t ws_bytes,
                     ipcb_stream s) {
-  if (!bvh || n < 0 || n > bvh->capacity) return IPCB_E_ARG;
+  if (!bvh) return arg_error("ipcb_lbvh_build: no hierarchy");
+  if (n < 0) return arg_error("ipcb_lbvh_build: n is negative");
+  if (n > bvh->capacity) return arg_error("ipcb_lbvh_build: n exceeds the hierarchy's capacity");
   cudaStream_t st = (cudaStream_t)s;
+  if (n == 0) {
+    bvh->n = 0;
+    return IPCB_OK;
+  }
+  if (!lower || !upper) return arg_error("ipcb_lbvh_build: null box array");
+  if (!ws || ws_bytes < ipcb_lbvh_build_workspace(n))
+    return arg_error("ipcb_lbvh_build: workspace missing or smaller than ipcb_lbvh_build_workspace(n)");
   bvh->n = n;
-  if (n == 0) return IPCB_OK;
-  if (!lower || !upper || !ws || ws_bytes < ipcb_lbvh_build_workspace(n)) return IPCB_E_ARG;
   unsigned* bounds = (unsigned*)ws;
   void* sws = (char*)ws + 256;
   cudaMemsetAsync(bounds, 0xff, 3 * sizeof(unsigned), st);

@@ -50,10 +50,15 @@ __global__ void k_inertia(int n, const S* __restrict__ x, const S* __restrict__ 
   }
 }
 
-__global__ void k_ls_begin(ipcb_ls_state* st, const void* toi, int fp64, const double* __restrict__ acc, double h2,
-                           double eps, int max_it, ipcb_contacts ee, ipcb_contacts pt) {
+__global__ void k_ls_begin(ipcb_ls_state* st, const void* toi, int fp64, const int* __restrict__ status,
+                           const double* __restrict__ acc, double h2, double eps, int max_it, ipcb_contacts ee,
+                           ipcb_contacts pt) {
   const double t = fp64 ? *(const double*)toi : (double)*(const float*)toi;
-  st->ub = t < 1.0 ? 0.9 * t : 1.0;
+  // a CCD query that ran out of stack, visits or root iterations may have
+  // missed an earlier impact: its TOI is no bound, so no step is taken
+  const int failed = status ? (*status & (IPCB_STATUS_STACK | IPCB_STATUS_ROOT_ITERS)) : 0;
+  st->refused = failed;
+  st->ub = failed ? 0.0 : (t < 1.0 ? 0.9 * t : 1.0);
   st->alpha = st->ub;
   st->eps = eps;
   st->E0 = h2 * (acc[0] + acc[1]) + acc[2];
@@ -89,7 +94,9 @@ __global__ void k_ls_accept(ipcb_ls_state* st, const double* __restrict__ acc, d
   st->E1 = E1;
   st->it += 1;
   int cont = 0;
-  if (over || st->overflow) {
+  if (st->refused) {
+    // the CCD bound was refused: the one trial ran at alpha = 0, nothing is accepted
+  } else if (over || st->overflow) {
     st->overflow = 1;
   } else if (isfinite(E1) && E1 < st->E0) {
     st->accepted = 1;
@@ -142,10 +149,10 @@ int ipcb_ls_inertia(int fp64, int n, const void* x, const void* x0, const void* 
   return check_launch("ipcb_ls_inertia");
 }
 
-int ipcb_ls_begin(ipcb_ls_state* st, const void* toi, int fp64, const double* acc, double h2, double eps, int max_it,
-                  const ipcb_contacts* ee, const ipcb_contacts* pt, ipcb_stream s) {
+int ipcb_ls_begin(ipcb_ls_state* st, const void* toi, int fp64, const int* status, const double* acc, double h2,
+                  double eps, int max_it, const ipcb_contacts* ee, const ipcb_contacts* pt, ipcb_stream s) {
   if (!st || !toi || !acc || max_it <= 0 || !ee || !pt) return IPCB_E_ARG;
-  k_ls_begin<<<1, 1, 0, (cudaStream_t)s>>>(st, toi, fp64, acc, h2, eps, max_it, *ee, *pt);
+  k_ls_begin<<<1, 1, 0, (cudaStream_t)s>>>(st, toi, fp64, status, acc, h2, eps, max_it, *ee, *pt);
   return check_launch("ipcb_ls_begin");
 }
 

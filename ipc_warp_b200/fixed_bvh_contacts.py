@@ -198,5 +198,4 @@ class FixedBodyContactSolver(ContactSolverBase):
             N.call("ipcb_fixed_point_triangle_toi", ctypes.byref(soup), N.ptr(self.ccd_x1),
                    ctypes.byref(self._bodies), N.ptr(self.fixed_body_pairs), n_pairs, 1.0e-7, N.ptr(self.ccd_toi),
                    N.ptr(self._status), N.ptr(ws), ws.numel(), s)
-        toi = float(self.ccd_toi.item())
-        return 0.9 * toi if toi < 1.0 else 1.0
+        return self._step_bound()

@@ -55,6 +55,7 @@ class StepStats:
     alphas: list = field(default_factory=list)
     energies: list = field(default_factory=list)
     norms: list = field(default_factory=list)
+    ccd_refusals: int = 0  # line searches refused because a CCD query ran out of its bounds
 
 
 class BlockJacobi:
@@ -527,7 +528,13 @@ class FEMContactSolver(ContactBarrierMixin):
         self._lists_at_x = False
         x_tmp = self.states.x.clone()
         E0 = self.total_energy()
+        refusals = self.ccd_refusals
         ub = self.collision_free_step(self.states.dx)
+        if self.ccd_refusals != refusals:
+            # a CCD query ran out of its bounds: its TOI is no bound, no step
+            self.stats.ccd_refusals += 1
+            self.stats.energies.append((E0, E0))
+            return 0.0
         alpha = ub
         accepted = False
         E1 = math.inf
@@ -691,7 +698,8 @@ class FEMContactSolver(ContactBarrierMixin):
         self._lists_at_x = False
         self._ccd_launches(self.states.dx)
         eps = 1.1920928955078125e-7 if self.dtype == torch.float32 else 2.220446049250313e-16
-        N.call("ipcb_ls_begin", N.ptr(ls["state"]), N.ptr(self.ccd_toi), fp64, N.ptr(ls["acc0"]), h2, eps, 64,
+        N.call("ipcb_ls_begin", N.ptr(ls["state"]), N.ptr(self.ccd_toi), fp64, N.ptr(self._status),
+               N.ptr(ls["acc0"]), h2, eps, 64,
                ctypes.byref(self.contacts_new.c_struct()), ctypes.byref(self.contacts_pt.c_struct()), s)
         graph = self._ls_graph()
         N.call("ipcb_graph_launch", graph, s)
@@ -707,6 +715,11 @@ class FEMContactSolver(ContactBarrierMixin):
                 self._grow_contact_list(self.contacts_pt, st.max_pt, point_triangle=True)
             self.states.x.copy_(ls["x_tmp"])
             return self._line_search_host()
+        self.query_status = st.refused
+        if st.refused:
+            # a CCD query ran out of its bounds: its TOI is no bound, no step
+            self.ccd_refusals += 1
+            self.stats.ccd_refusals += 1
         self.stats.energies.append((st.E0, st.E1))
         self.ls_trials = st.it
         self._ls_cache = bool(getattr(self, "_in_step", False) and st.accepted)

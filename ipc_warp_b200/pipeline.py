@@ -40,6 +40,7 @@ class IterationResult:
     n_pt: int
     energy: float
     alpha: float
+    status: int = 0  # IPCB_STATUS_* bits of the queries; a failed query gives alpha = 0
 
 
 class ContactPipeline(ContactBarrierMixin):
@@ -69,7 +70,7 @@ class ContactPipeline(ContactBarrierMixin):
             self._pt_done = torch.cuda.Event()
             self._toi_ws_pt = torch.empty_like(self._toi_ws)
         self._dx_buf = torch.zeros_like(soup.x_transformed)
-        self._readback = {"counts": torch.zeros(3, dtype=torch.int32, pin_memory=pin),
+        self._readback = {"counts": torch.zeros(4, dtype=torch.int32, pin_memory=pin),
                           "energy": torch.zeros(1, dtype=torch.float64, pin_memory=pin),
                           "toi": torch.zeros(1, dtype=soup.x_transformed.dtype, pin_memory=pin)}
 
@@ -103,15 +104,15 @@ class ContactPipeline(ContactBarrierMixin):
         torch.cuda.current_stream().synchronize()
         h = self._readback
         ee, pt = self.contacts_new, self.contacts_pt
-        n_ee, n_pt, st = (int(v) for v in h["counts"])
+        n_ee, n_pt, st, qst = (int(v) for v in h["counts"])
         if n_ee > ee.capacity or n_pt > pt.capacity or st & 4:
             self._graph = None
             return self.iteration_stepwise()
         if self.use_graph and (self._graph is None or self._graph[0] != key):
             self._capture(self._graph_key())  # the eager pass may have (re)allocated buffers
         self.n_contacts, self.n_contacts_pt = n_ee, n_pt
-        toi = float(h["toi"][0])
-        return IterationResult(n_ee, n_pt, float(h["energy"][0]) * self.h * self.h, 0.9 * toi if toi < 1.0 else 1.0)
+        alpha = self._bound_from(float(h["toi"][0]), qst)
+        return IterationResult(n_ee, n_pt, float(h["energy"][0]) * self.h * self.h, alpha, qst)
 
     def _graph_key(self):
         ee, pt, t, H = self.contacts_new, self.contacts_pt, self.collision_triplets, self.collision_hessian
@@ -206,6 +207,7 @@ class ContactPipeline(ContactBarrierMixin):
         h["counts"][0:1].copy_(ee.cnt, non_blocking=True)
         h["counts"][1:2].copy_(pt.cnt, non_blocking=True)
         h["counts"][2:3].copy_(self._bsr_status, non_blocking=True)
+        h["counts"][3:4].copy_(self._status, non_blocking=True)
         h["energy"].copy_(e, non_blocking=True)
         h["toi"].copy_(self.ccd_toi, non_blocking=True)
 
@@ -213,6 +215,7 @@ class ContactPipeline(ContactBarrierMixin):
         """_enqueue on one stream (periodic BVH rebuilds, or no triangles)."""
         ee, pt = self.contacts_new, self.contacts_pt
         self.compute_V(ret=False)
+        self._status.zero_()
         self.update_bvh()
         self._launch_dcd("ee")
         if self.has_triangles:
@@ -233,7 +236,7 @@ class ContactPipeline(ContactBarrierMixin):
         e = self._energy.zero_()
         contact_energy_ee(self.states, self.soup, ee, e, kappa, n=-1)
         contact_energy_pt(self.states, self.soup, pt, e, kappa, n=-1)
-        self._launch_ccd(self._dx_buf)
+        self._launch_ccd(self._dx_buf, reset_status=False)
         self._copy_results(e)
 
     def iteration_stepwise(self) -> IterationResult:
@@ -243,8 +246,9 @@ class ContactPipeline(ContactBarrierMixin):
         self.b.zero_()
         self.compute_contact_hessian(detect=False)
         e = self.compute_collision_energy(detect=False)
+        dcd_status = self.query_status
         alpha = self.line_search_upper_bound()
-        return IterationResult(self.n_contacts, self.n_contacts_pt, e, alpha)
+        return IterationResult(self.n_contacts, self.n_contacts_pt, e, alpha, dcd_status | self.query_status)
 
     def set_positions(self, x) -> None:
         if isinstance(x, np.ndarray):

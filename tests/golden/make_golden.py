@@ -337,4 +337,6 @@ def main(ref: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("IPC_WARP_REFERENCE", "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the ipc_warp source tree>")
+    main(sys.argv[1])

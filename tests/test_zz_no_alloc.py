@@ -68,3 +68,36 @@ def test_noalloc_rejects_sizes_above_the_static_limit(cuda):
     rc = N.lib().ipcb_lbvh_build_noalloc(ctypes.byref(bvh), None, None, limit + 1, N.stream_handle())
     assert rc == 1
     assert b"IPCB_LBVH_NOALLOC_MAX_PRIMS" in N.lib().ipcb_last_error()
+
+
+@pytest.mark.parametrize("n", [0, 1])
+def test_noalloc_tiny_sizes_match_regular_build(cuda, n):
+    stream = N.stream_handle()
+    lo = torch.tensor([[0.0, 0.0, 0.0]], device=cuda)
+    hi = torch.tensor([[1.0, 1.0, 1.0]], device=cuda)
+    ref, ref_mem = _bound(1, cuda)
+    ws = torch.empty(N.size("ipcb_lbvh_build_workspace", 1), dtype=torch.uint8, device=cuda)
+    N.call("ipcb_lbvh_build", ctypes.byref(ref), N.ptr(lo), N.ptr(hi), n, N.ptr(ws), ws.numel(), stream)
+    got, got_mem = _bound(1, cuda)
+    rc = N.lib().ipcb_lbvh_build_noalloc(ctypes.byref(got), N.ptr(lo), N.ptr(hi), n, stream)
+    assert rc == 0, N.lib().ipcb_last_error()
+    torch.cuda.synchronize()
+    assert got.n == ref.n == n
+    if n == 1:
+        assert np.array_equal(_arrays(got, got_mem, 1)[1], _arrays(ref, ref_mem, 1)[1])
+
+
+def test_noalloc_rejects_negative_n_and_small_capacity(cuda):
+    bvh, _ = _bound(4, cuda)
+    lo = torch.zeros((8, 3), device=cuda)
+    hi = torch.ones((8, 3), device=cuda)
+    rc = N.lib().ipcb_lbvh_build_noalloc(ctypes.byref(bvh), N.ptr(lo), N.ptr(hi), -1, N.stream_handle())
+    assert rc == 1 and b"negative" in N.lib().ipcb_last_error()
+    rc = N.lib().ipcb_lbvh_build_noalloc(ctypes.byref(bvh), N.ptr(lo), N.ptr(hi), 8, N.stream_handle())
+    assert rc == 1 and b"capacity" in N.lib().ipcb_last_error()
+    assert bvh.n == 0  # a refused call leaves the hierarchy as it was
+    # the allocating build reports its own argument errors the same way
+    ws = torch.empty(N.size("ipcb_lbvh_build_workspace", 8), dtype=torch.uint8, device=cuda)
+    rc = N.lib().ipcb_lbvh_build(ctypes.byref(bvh), N.ptr(lo), N.ptr(hi), 8, N.ptr(ws), ws.numel(),
+                                 N.stream_handle())
+    assert rc == 1 and b"capacity" in N.lib().ipcb_last_error()
