@@ -136,14 +136,17 @@ def test_full_size_parity(cuda, name, dtype):
         touched = np.unique(tr_rows[nz])
         rng = np.random.default_rng(0)
         sample = set(rng.choice(touched, size=min(3000, touched.size), replace=False).tolist())
-        sel = nz & np.isin(tr_rows, list(sample))
-        for r in sample:
-            mine = sel & (tr_rows == r)
+        sel = np.nonzero(nz & np.isin(tr_rows, list(sample)))[0]
+        sel = sel[np.argsort(tr_rows[sel], kind="stable")]
+        starts = np.flatnonzero(np.r_[True, tr_rows[sel][1:] != tr_rows[sel][:-1], True])
+        assert starts.size - 1 == len(sample)
+        for a, z in zip(starts[:-1], starts[1:]):
+            mine = sel[a:z]
+            r = tr_rows[mine[0]]
             uc, inv = np.unique(tr_cols[mine], return_inverse=True)
             ref = np.zeros((uc.size, 3, 3))
             np.add.at(ref, inv, tr_vals[mine])
-            got_cols = cols[offs[r]:offs[r + 1]]
-            assert np.array_equal(got_cols, uc)
+            assert np.array_equal(cols[offs[r]:offs[r + 1]], uc)
             scale = max(np.abs(ref).max(), 1e-300)
             assert np.abs(hv[offs[r]:offs[r + 1]] - ref).max() <= tol * scale
 
