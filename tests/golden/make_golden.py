@@ -254,7 +254,185 @@ def run_dcd(ns, sc, x, exclude):
     return records(ee), records(pt), ee, pt
 
 
-def main(ref: str):
+MATERIAL_FILES = {"snh": ("snh.py", ["reparam", "psi", "partialJpartialF", "PK1", "tangent_stiffness"]),
+                  "neo_hookean": ("neo_hookean.py", ["tangent_stiffness", "PK1", "psi"]),
+                  "stvk": ("stvk.py", ["tangent_stiffness", "psi", "PK1"])}
+
+
+def fem_ns(ref: str, fp64: bool, material: str, mu: float, lam: float) -> dict:
+    """fem/fem.py compute_Dm + tet_kernel_sparse and time_integrator_base.py
+    compute_Psi over one material file (the reference selects the material
+    by import, fem/fem.py:12-14); mu and lam as the material files read them
+    from fem/params.py."""
+    ns = scalar_ns(fp64)
+    ns["mu"], ns["lam"] = ns["scalar"](mu), ns["scalar"](lam)
+    fname, funcs = MATERIAL_FILES[material]
+    load(os.path.join(ref, "fem", fname), funcs, ns)
+    load(os.path.join(ref, "fem", "fem.py"), ["Triplets", "compute_Dm", "tet_kernel_sparse"], ns)
+    load(os.path.join(ref, "time_integrator_base.py"), ["compute_Psi"], ns)
+    return ns
+
+
+def make_fem(ref: str):
+    """F. tet terms (fem/fem.py:22-35,139-203, time_integrator_base.py:125-137)
+    for the three materials in both builds, on a deformed 2x2x2-cell block."""
+    from ipc_warp_b200 import scenes
+
+    rng = np.random.default_rng(77)
+    m = scenes.hex_grid_tets(2, 2, 2, size=(0.2, 0.2, 0.2))
+    xcs = m.x.astype(np.float64)
+    G = np.eye(3) + 0.12 * rng.normal(size=(3, 3))
+    x = xcs @ G.T + 0.004 * rng.normal(size=xcs.shape)
+    tets = m.tets.astype(np.int32)
+    nt = len(tets)
+    E_, nu = 1e5, 0.4
+    mu, lam = E_ / (2 * (1 + nu)), E_ * nu / ((1 + nu) * (1 - 2 * nu))
+    out = {"x": x, "xcs": xcs, "tets": tets, "mu": mu, "lam": lam}
+    for material in MATERIAL_FILES:
+        for fp64 in (True, False):
+            ns = fem_ns(ref, fp64, material, mu, lam)
+            f = ns["scalar"]
+            xs, xr = x.astype(f), xcs.astype(f)
+            geo = types.SimpleNamespace(xcs=xr, T=tets)
+            Bm = np.zeros((nt, 3, 3), f)
+            W = np.zeros(nt, f)
+            wp.launch(ns["compute_Dm"], nt, geo, Bm, W)
+            trip = types.SimpleNamespace(rows=np.zeros(16 * nt, np.int32), cols=np.zeros(16 * nt, np.int32),
+                                         vals=np.zeros((16 * nt, 3, 3), f))
+            b = np.zeros_like(xs)
+            wp.launch(ns["tet_kernel_sparse"], 16 * nt, xs, geo, Bm, W, trip, b)
+            Psi = np.zeros(nt, f)
+            wp.launch(ns["compute_Psi"], nt, xs, geo, Bm, W, Psi)
+            key = f"{material}_{64 if fp64 else 32}"
+            out.update({f"{key}_rows": trip.rows, f"{key}_cols": trip.cols, f"{key}_vals": trip.vals,
+                        f"{key}_force": b, f"{key}_psi": Psi, f"{key}_W": W})
+    np.savez_compressed(os.path.join(HERE, "fem_tets.npz"), **out)
+
+
+def make_abd(ref: str):
+    """G. affine-body kernels (affine_body_dynamics.py:42-217) in both builds:
+    body blocks and gradient, energies, and the vertex -> affine reductions of
+    a contact force and of contact Hessian triplets."""
+    rng = np.random.default_rng(78)
+    nb = 3
+    fixed = np.array([0, 0, 1], np.int32)
+    nv_b = 7
+    body = np.repeat(np.arange(nb), nv_b).astype(np.int32)
+    rest = rng.normal(scale=0.3, size=(nb * nv_b, 3))
+    q = np.zeros((nb, 4, 3))
+    for b in range(nb):
+        Q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+        A = Q @ (np.eye(3) + 0.05 * rng.normal(size=(3, 3)))
+        q[b, 0] = rng.normal(size=3)
+        q[b, 1:] = A.T  # columns a0, a1, a2
+    qt = q + 0.01 * rng.normal(size=q.shape)
+    L = rng.normal(size=(nb, 4, 4))
+    M = np.einsum("bij,bkj->bik", L, L) + 4 * np.eye(4)  # SPD scalar moments
+    volume = rng.uniform(0.5, 1.5, nb)
+    stiffness = rng.uniform(1e3, 1e4, nb)
+    h2 = 1e-4
+    f_vert = rng.normal(size=(nb * nv_b, 3))
+    n_src = 40
+    src_rows = rng.integers(0, nb * nv_b, n_src).astype(np.int32)
+    src_cols = rng.integers(0, nb * nv_b, n_src).astype(np.int32)
+    src_vals = rng.normal(size=(n_src, 3, 3))
+    out = {"q": q, "qt": qt, "M": M, "volume": volume, "stiffness": stiffness, "fixed": fixed, "h2": h2,
+           "rest": rest, "body": body, "f_vert": f_vert, "src_rows": src_rows, "src_cols": src_cols,
+           "src_vals": src_vals, "scale": 0.25}
+    for fp64 in (True, False):
+        ns = scalar_ns(fp64)
+        f = ns["scalar"]
+        load(os.path.join(ref, "affine_body_dynamics.py"),
+             ["ABDState", "_assemble_body_system", "_reduce_contact_force", "_reduce_contact_hessian",
+              "_body_energy"], ns)
+        load(os.path.join(ref, "fem", "fem.py"), ["Triplets"], ns)
+        st = types.SimpleNamespace(q=q.reshape(-1, 3).astype(f), q_tilde=qt.reshape(-1, 3).astype(f))
+        mass = np.einsum("bij,kl->bijkl", M, np.eye(3)).reshape(-1, 3, 3).astype(f)
+        trip = types.SimpleNamespace(rows=np.zeros(16 * nb, np.int32), cols=np.zeros(16 * nb, np.int32),
+                                     vals=np.zeros((16 * nb, 3, 3), f))
+        grad = np.zeros((4 * nb, 3), f)
+        wp.launch(ns["_assemble_body_system"], 16 * nb, st, mass, volume.astype(f), stiffness.astype(f), fixed,
+                  f(h2), trip, grad)
+        inertia, ortho = np.zeros(1, f), np.zeros(1, f)
+        wp.launch(ns["_body_energy"], nb, st, mass, volume.astype(f), stiffness.astype(f), fixed, f(h2), inertia,
+                  ortho)
+        red = np.zeros((4 * nb, 3), f)
+        wp.launch(ns["_reduce_contact_force"], nb * nv_b, f_vert.astype(f), rest.astype(f), body, fixed, red)
+        src = types.SimpleNamespace(rows=src_rows, cols=src_cols, vals=src_vals.astype(f))
+        dst = types.SimpleNamespace(rows=np.zeros(16 * n_src, np.int32), cols=np.zeros(16 * n_src, np.int32),
+                                    vals=np.zeros((16 * n_src, 3, 3), f))
+        wp.launch(ns["_reduce_contact_hessian"], 16 * n_src, src, rest.astype(f), body, fixed, f(0.25), dst)
+        key = "64" if fp64 else "32"
+        out.update({f"rows_{key}": trip.rows, f"cols_{key}": trip.cols, f"vals_{key}": trip.vals,
+                    f"grad_{key}": grad, f"inertia_{key}": inertia[0], f"ortho_{key}": ortho[0],
+                    f"reduced_force_{key}": red, f"dst_rows_{key}": dst.rows, f"dst_cols_{key}": dst.cols,
+                    f"dst_vals_{key}": dst.vals})
+    np.savez_compressed(os.path.join(HERE, "abd_bodies.npz"), **out)
+
+
+def make_fp32(ref: str):
+    """H. the reference's float32 build (scalar_types.py:6, USE_FLOAT32) on the
+    CCD path: per-pair collision times (ccd.py:304-357) and cubic roots
+    (cubic_roots.py:96-193) evaluated in float32, beside the float64 build on
+    the same float32 inputs.  Two sets of motions: the random ones of
+    collision_time.npz, and near-contact motions of unit-scale geometry (a
+    pair dhat = 1e-3 apart closing by 2 dhat), the configurations the scene
+    CCD meets."""
+    from ipc_warp_b200 import scenes
+
+    ns32 = reference_ns(ref, fp64=False)
+    ns64 = reference_ns(ref, fp64=True)
+    ct = np.load(os.path.join(HERE, "collision_time.npz"))
+    rng = np.random.default_rng(79)
+    sets = {}
+    n = 1500
+    sets["random"] = (ct["p0"][:n].astype(np.float32), ct["p1"][:n].astype(np.float32))
+    # near contact: the DCD pairs of a two-cube scene (1 unit cubes, gap 2e-4)
+    # with the upper cube closing by 1e-3 plus 2e-4 noise
+    sc = scenes.two_cubes(n=4, gap=2e-4, angle_deg=30.0, seed=4)
+    x0 = sc.x.astype(np.float32)
+    x1 = x0.copy()
+    x1[sc.body == 1, 1] -= np.float32(1e-3)
+    x1 += rng.normal(scale=2e-4, size=x1.shape).astype(np.float32)
+    ee, pt, _, _ = run_dcd(ns32, scenes.two_cubes(n=4, gap=2e-4, angle_deg=30.0, seed=4), x0, False)
+    for kind, rec in (("ee", ee), ("pt", pt)):
+        ids = rec[:, :4]
+        sets[f"near_{kind}"] = (x0[ids], x1[ids])
+    out = {}
+    for name, (p0, p1) in sets.items():
+        kinds = ("ee", "pt") if name == "random" else (name[-2:],)
+        out[f"{name}_p0"], out[f"{name}_p1"] = p0, p1
+        for kind in kinds:
+            fn = f"{kind}_collision_time"
+            t32 = np.array([ns32[fn](*(ns32["vec3"](v) for v in p0[i]), *(ns32["vec3"](v) for v in p1[i]))
+                            for i in range(len(p0))], np.float32)
+            t64 = np.array([ns64[fn](*(ns64["vec3"](v) for v in p0[i]), *(ns64["vec3"](v) for v in p1[i]))
+                            for i in range(len(p0))], np.float64)
+            out[f"{name}_t_{kind}32"], out[f"{name}_t_{kind}64"] = t32, t64
+    # cubic roots of the float32 coefficients, both builds
+    cr = np.load(os.path.join(HERE, "cubic_roots.npz"))
+    coef = cr["coef"].astype(np.float32)
+    for key, ns in (("32", ns32), ("64", ns64)):
+        nr = np.zeros(len(coef), np.int32)
+        roots = np.zeros((len(coef), 3), ns["scalar"])
+        for i, c in enumerate(coef):
+            k, r = ns["cubic_roots"](ns["vec4"](c), ns["scalar"](0.0), ns["scalar"](1.0))
+            nr[i], roots[i] = k, r
+        out[f"cubic_n_roots_{key}"], out[f"cubic_roots_{key}"] = nr, roots
+    out["cubic_coef32"] = coef
+    np.savez_compressed(os.path.join(HERE, "fp32_build.npz"), **out)
+
+
+def main(ref: str, sections=("A", "B", "C", "D", "E", "F", "G", "H")):
+    if "F" in sections:
+        make_fem(ref)
+    if "G" in sections:
+        make_abd(ref)
+    if "H" in sections:
+        make_fp32(ref)
+    if not set(sections) & set("ABCDE"):
+        print("golden vectors written:", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
+        return
     from ipc_warp_b200 import scenes
 
     rng = np.random.default_rng(2024)
@@ -337,6 +515,6 @@ def main(ref: str):
 
 
 if __name__ == "__main__":
-    if len(sys.argv) != 2:
-        sys.exit("usage: python tests/golden/make_golden.py <path of the ipc_warp source tree>")
-    main(sys.argv[1])
+    if len(sys.argv) < 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the ipc_warp source tree> [sections A..H]")
+    main(sys.argv[1], tuple(sys.argv[2:]) or ("A", "B", "C", "D", "E", "F", "G", "H"))

@@ -202,6 +202,51 @@ def matrix_from_cols(*cols):
     return np.stack(cols, axis=1)
 
 
+def ddot(a, b):
+    """Frobenius product, summed row by row in the matrix's scalar type."""
+    acc = a[0, 0] * b[0, 0]
+    for i in range(a.shape[0]):
+        for j in range(a.shape[1]):
+            if i or j:
+                acc = acc + a[i, j] * b[i, j]
+    return acc
+
+
+def trace(m):
+    acc = m[0, 0]
+    for i in range(1, m.shape[0]):
+        acc = acc + m[i, i]
+    return acc
+
+
+def determinant(m):
+    """3x3 cofactor expansion along the first row, in the scalar type."""
+    return (m[0, 0] * (m[1, 1] * m[2, 2] - m[1, 2] * m[2, 1])
+            - m[0, 1] * (m[1, 0] * m[2, 2] - m[1, 2] * m[2, 0])
+            + m[0, 2] * (m[1, 0] * m[2, 1] - m[1, 1] * m[2, 0]))
+
+
+def inverse(m):
+    """3x3 adjugate over the determinant, in the scalar type."""
+    d = determinant(m)
+    adj = np.empty_like(m)
+    for i in range(3):
+        for j in range(3):
+            r = [k for k in range(3) if k != j]
+            c = [k for k in range(3) if k != i]
+            minor = m[r[0], c[0]] * m[r[1], c[1]] - m[r[0], c[1]] * m[r[1], c[0]]
+            adj[i, j] = minor if (i + j) % 2 == 0 else -minor
+    return adj / d
+
+
+def identity(n=3, dtype=np.float32):
+    return np.eye(n, dtype=dtype)
+
+
+def log(x):
+    return type(x)(math.log(x)) if isinstance(x, np.floating) else math.log(x)
+
+
 def transpose(m):
     return m.T.copy()
 

@@ -75,3 +75,57 @@ def test_narrow_phase_matches_reference_composition(mode):
         assert abs(E.sum() - e_ref) <= 1e-10 * abs(e_ref)
         off += n
     assert rel_err(force, d["force"]) < 1e-10
+
+
+MATERIALS = (("snh", 0), ("neo_hookean", 1), ("stvk", 2))
+
+
+@pytest.mark.parametrize("material,code", MATERIALS)
+@pytest.mark.parametrize("build", [64, 32])
+def test_fem_matches_reference_kernels(material, code, build):
+    """fem/fem.py compute_Dm + tet_kernel_sparse and compute_Psi, run by the
+    reference for each material file: the oracle's blocks, forces and energy
+    in double within 1e-12 of the double build, and within 2e-6 of the float32
+    build (evaluated on the float32-rounded positions)."""
+    d = load("fem_tets.npz")
+    x, xcs, tets = d["x"], d["xcs"], d["tets"]
+    if build == 32:
+        x, xcs = x.astype(np.float32).astype(np.float64), xcs.astype(np.float32).astype(np.float64)
+    force, blocks, energy = po.tet(code, x, xcs, tets, float(d["mu"]), float(d["lam"]))
+    k = f"{material}_{build}"
+    n = len(tets)
+    assert np.array_equal(d[k + "_rows"].reshape(n, 4, 4), np.repeat(tets[:, :, None], 4, axis=2))
+    assert np.array_equal(d[k + "_cols"].reshape(n, 4, 4), np.repeat(tets[:, None, :], 4, axis=1))
+    tol = 1e-12 if build == 64 else 2e-6
+    vals = d[k + "_vals"].astype(np.float64).reshape(n, 16, 3, 3)
+    assert rel_err(blocks, vals) <= tol
+    assert rel_err(force, d[k + "_force"]) <= tol
+    assert abs(energy - d[k + "_psi"].astype(np.float64).sum()) <= tol * abs(energy)
+
+
+@pytest.mark.parametrize("build", ["64", "32"])
+def test_abd_matches_reference_kernels(build):
+    """affine_body_dynamics.py _assemble_body_system, _body_energy,
+    _reduce_contact_force and _reduce_contact_hessian run by the reference:
+    oracle/abd.py within 1e-12 of the double build and 5e-6 of the float32
+    build (the float32 gradient M (q - q~) loses digits to cancellation)."""
+    from oracle import abd as oa
+
+    a = load("abd_bodies.npz")
+    tol = 1e-12 if build == "64" else 5e-6
+    blocks, grad = oa.body_system(a["q"], a["qt"], a["M"], a["volume"], a["stiffness"], a["fixed"], float(a["h2"]))
+    nb = len(a["volume"])
+    rows = np.array([[4 * b + i for i in range(4) for _ in range(4)] for b in range(nb)]).ravel()
+    cols = np.array([[4 * b + j for _ in range(4) for j in range(4)] for b in range(nb)]).ravel()
+    assert np.array_equal(a["rows_" + build], rows) and np.array_equal(a["cols_" + build], cols)
+    assert rel_err(blocks.reshape(-1, 3, 3), a["vals_" + build]) <= tol
+    assert rel_err(grad.reshape(-1, 3), a["grad_" + build]) <= tol
+    inertia, ortho = oa.body_energy(a["q"], a["qt"], a["M"], a["volume"], a["stiffness"], a["fixed"], float(a["h2"]))
+    assert abs(inertia - a["inertia_" + build]) <= tol * abs(inertia)
+    assert abs(ortho - a["ortho_" + build]) <= tol * abs(ortho)
+    red = oa.reduce_force(a["f_vert"], a["rest"], a["body"], a["fixed"], nb)
+    assert rel_err(red.reshape(-1, 3), a["reduced_force_" + build]) <= tol
+    R, C, V = oa.reduce_hessian(a["src_rows"], a["src_cols"], a["src_vals"], a["rest"], a["body"], a["fixed"],
+                                float(a["scale"]))
+    assert np.array_equal(R, a["dst_rows_" + build]) and np.array_equal(C, a["dst_cols_" + build])
+    assert rel_err(V, a["dst_vals_" + build]) <= tol

@@ -82,3 +82,45 @@ def test_tet_rest_volumes(cuda):
     for bi in np.unique(body):
         idx = np.nonzero(np.isin(sc.tets, np.nonzero(body == bi)[0]).all(axis=1))[0]
         assert W.cpu().numpy()[idx].sum() > 0
+
+
+@pytest.mark.parametrize("material,code", [("snh", 0), ("neo_hookean", 1), ("stvk", 2)])
+@pytest.mark.parametrize("fp64", [False, True])
+def test_tet_kernels_match_reference_fixture(cuda, material, code, fp64):
+    """The reference's own compute_Dm, tet_kernel_sparse and compute_Psi
+    (fem/fem.py:22-35,139-203, time_integrator_base.py:125-137), run at
+    fixture time on each material file (tests/golden/fem_tets.npz): the GPU
+    kernels on the same inputs, against the reference build of the same
+    precision (1e-10 double; 2e-5 float)."""
+    import os
+
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "fem_tets.npz"))
+    dt = torch.float64 if fp64 else torch.float32
+    key = f"{material}_{64 if fp64 else 32}"
+    tx = torch.tensor(d["x"], dtype=dt, device=cuda)
+    txcs = torch.tensor(d["xcs"], dtype=dt, device=cuda)
+    tets = torch.tensor(d["tets"], dtype=torch.int32, device=cuda)
+    n = tets.shape[0]
+    mu, lam = float(d["mu"]), float(d["lam"])
+    Bm = torch.zeros((n, 3, 3), dtype=dt, device=cuda)
+    W = torch.zeros(n, dtype=dt, device=cuda)
+    N.call("ipcb_tet_rest", int(fp64), N.ptr(txcs), N.ptr(tets), n, N.ptr(Bm), N.ptr(W), N.stream_handle())
+    rows = torch.full((16 * n,), -1, dtype=torch.int32, device=cuda)
+    cols = torch.full((16 * n,), -1, dtype=torch.int32, device=cuda)
+    vals = torch.zeros((16 * n, 3, 3), dtype=dt, device=cuda)
+    b = torch.zeros_like(tx)
+    N.call("ipcb_tet_hessian", code, int(fp64), N.ptr(tx), N.ptr(tets), n, N.ptr(Bm), N.ptr(W), mu, lam,
+           N.ptr(rows), N.ptr(cols), N.ptr(vals), N.ptr(b), N.stream_handle())
+    e = torch.zeros(1, dtype=torch.float64, device=cuda)
+    N.call("ipcb_tet_energy", code, int(fp64), N.ptr(tx), N.ptr(tets), n, N.ptr(Bm), N.ptr(W), mu, lam,
+           N.ptr(e), N.stream_handle())
+    torch.cuda.synchronize()
+    tol = 1e-10 if fp64 else 2e-5
+    assert np.array_equal(rows.cpu().numpy(), d[key + "_rows"])
+    assert np.array_equal(cols.cpu().numpy(), d[key + "_cols"])
+    ref = d[key + "_vals"].astype(np.float64)
+    assert np.abs(vals.double().cpu().numpy() - ref).max() <= tol * np.abs(ref).max()
+    fr = d[key + "_force"].astype(np.float64)
+    assert np.abs(b.double().cpu().numpy() - fr).max() <= tol * np.abs(fr).max()
+    er = float(d[key + "_psi"].astype(np.float64).sum())
+    assert abs(float(e.item()) - er) <= tol * abs(er)
