@@ -376,10 +376,8 @@ def make_fp32(ref: str):
     (cubic_roots.py:96-193) evaluated in float32, beside the float64 build on
     the same float32 inputs.  Two sets of motions: the random ones of
     collision_time.npz, and near-contact motions of unit-scale geometry (a
-    pair dhat = 1e-3 apart closing by 2 dhat), the configurations the scene
-    CCD meets."""
-    from ipc_warp_b200 import scenes
-
+    pair up to dhat = 1e-3 apart closing by 2 dhat), the configurations the
+    scene CCD meets."""
     ns32 = reference_ns(ref, fp64=False)
     ns64 = reference_ns(ref, fp64=True)
     ct = np.load(os.path.join(HERE, "collision_time.npz"))
@@ -387,17 +385,34 @@ def make_fp32(ref: str):
     sets = {}
     n = 1500
     sets["random"] = (ct["p0"][:n].astype(np.float32), ct["p1"][:n].astype(np.float32))
-    # near contact: the DCD pairs of a two-cube scene (1 unit cubes, gap 2e-4)
-    # with the upper cube closing by 1e-3 plus 2e-4 noise
-    sc = scenes.two_cubes(n=4, gap=2e-4, angle_deg=30.0, seed=4)
-    x0 = sc.x.astype(np.float32)
-    x1 = x0.copy()
-    x1[sc.body == 1, 1] -= np.float32(1e-3)
-    x1 += rng.normal(scale=2e-4, size=x1.shape).astype(np.float32)
-    ee, pt, _, _ = run_dcd(ns32, scenes.two_cubes(n=4, gap=2e-4, angle_deg=30.0, seed=4), x0, False)
-    for kind, rec in (("ee", ee), ("pt", pt)):
-        ids = rec[:, :4]
-        sets[f"near_{kind}"] = (x0[ids], x1[ids])
+    # near contact at unit scale: 0.1-long edges / 0.1-wide triangles whose
+    # centres lie in [-1, 1]^3, a pair placed up to dhat = 1e-3 apart along a
+    # random normal and closing by 2 dhat (plus 0.2 dhat noise) over the step
+    m = 2000
+    c = rng.uniform(-1, 1, size=(m, 1, 3))
+    nrm = rng.normal(size=(m, 1, 3))
+    nrm /= np.linalg.norm(nrm, axis=2, keepdims=True)
+    d0 = rng.uniform(0, 1e-3, size=(m, 1, 1))
+    u = np.cross(nrm, rng.normal(size=(m, 1, 3)))
+    u /= np.linalg.norm(u, axis=2, keepdims=True)
+    v = np.cross(nrm, u)
+    ang = rng.uniform(0, np.pi, size=(m, 1, 1))
+    w = np.cos(ang) * u + np.sin(ang) * v
+    ea = np.concatenate([c - 0.05 * u, c + 0.05 * u], axis=1)
+    eb = np.concatenate([c + d0 * nrm - 0.05 * w, c + d0 * nrm + 0.05 * w], axis=1)
+    p0 = np.concatenate([ea, eb], axis=1)
+    mv = np.zeros_like(p0)
+    mv[:, 2:] = -2e-3 * nrm
+    p1 = p0 + mv + rng.normal(scale=2e-4, size=p0.shape)
+    sets["near_ee"] = (p0.astype(np.float32), p1.astype(np.float32))
+    off = rng.uniform(-0.02, 0.02, size=(m, 1, 2))
+    tri = np.concatenate([c - 0.05 * u - 0.03 * v, c + 0.05 * u - 0.03 * v, c + 0.06 * v], axis=1)
+    pnt = c + d0 * nrm + off[..., :1] * u + off[..., 1:] * v
+    p0 = np.concatenate([pnt, tri], axis=1)
+    mv = np.zeros_like(p0)
+    mv[:, :1] = -2e-3 * nrm
+    p1 = p0 + mv + rng.normal(scale=2e-4, size=p0.shape)
+    sets["near_pt"] = (p0.astype(np.float32), p1.astype(np.float32))
     out = {}
     for name, (p0, p1) in sets.items():
         kinds = ("ee", "pt") if name == "random" else (name[-2:],)

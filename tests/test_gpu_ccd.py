@@ -118,3 +118,21 @@ def test_small_candidate_list_gives_the_same_toi(cuda, fp64):
     assert float(s.ccd_toi.item()) == toi_full and small == full
     s._toi_ws = torch.empty(256, dtype=torch.uint8, device=cuda)  # nothing staged
     assert s.collision_free_step(dxt) == full
+
+
+def test_pair_times_match_reference_float64_build(cuda):
+    """Per-pair times on the float32 inputs of tests/golden/fp32_build.npz
+    (random and near-contact motions) equal the reference's float64 build
+    run at fixture time, bit for bit; the reference's float32 build is
+    compared in test_golden.py."""
+    import os
+
+    from ipc_warp_b200.ccd import collision_time
+
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "fp32_build.npz"))
+    for name, kinds in (("random", ("ee", "pt")), ("near_ee", ("ee",)), ("near_pt", ("pt",))):
+        p0, p1 = d[name + "_p0"].astype(np.float64), d[name + "_p1"].astype(np.float64)
+        for kind in kinds:
+            t, st = collision_time(kind, p0, p1)
+            assert st == 0
+            assert np.array_equal(t.cpu().numpy(), d[f"{name}_t_{kind}64"]), (name, kind)
