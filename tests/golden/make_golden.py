@@ -438,13 +438,55 @@ def make_fp32(ref: str):
     np.savez_compressed(os.path.join(HERE, "fp32_build.npz"), **out)
 
 
-def main(ref: str, sections=("A", "B", "C", "D", "E", "F", "G", "H")):
+def make_narrow32(ref: str):
+    """I. the narrow phase of the reference's float32 build
+    (dynamic_contacts.py:152-246, 375-398 with scalar = float32) on the scene
+    of narrow_fp64.npz rounded to float32."""
+    d = np.load(os.path.join(HERE, "narrow_fp64.npz"))
+    ns32 = reference_ns(ref, fp64=False)
+    x32 = d["x"].astype(np.float32)
+    xcs32 = d["xcs"].astype(np.float32)
+    th = np.float32(d["l0"]) * np.float32(0.5)
+    ns32["_thickness"] = float(th)
+    ns32["buffer"] = float(th)
+    states = types.SimpleNamespace(x=x32)
+    soup = types.SimpleNamespace(edges=d["edges"], triangles=d["triangles"], body=d["body"], x_transformed=x32,
+                                 xcs=xcs32)
+    lists = {}
+    for kind in ("ee", "pt"):
+        rec = d[kind]
+        c = make_contacts(ns32, max(len(rec), 1))
+        for k, r in enumerate(rec):
+            c.list[k] = ns32["XConstraint"](a1a2b1b2=ns32["wp"].vec4i(r[:4]), e0e1=ns32["wp"].vec2i(r[4:]),
+                                            l0=np.float32(2) * th, alpha=np.float32(0), lam=np.float32(0))
+        c.cnt[0] = len(rec)
+        lists[kind] = c
+    n_ee, n_pt = len(d["ee"]), len(d["pt"])
+    kappa = np.float32(d["kappa"])
+    trip = types.SimpleNamespace(rows=np.zeros(16 * (n_ee + n_pt), np.int32),
+                                 cols=np.zeros(16 * (n_ee + n_pt), np.int32),
+                                 vals=np.zeros((16 * (n_ee + n_pt), 3, 3), np.float32))
+    b = np.zeros_like(x32)
+    wp.launch(ns32["contact_hessian_ee"], n_ee, states, soup, lists["ee"].list, trip, b, kappa)
+    wp.launch(ns32["contact_hessian_pt"], n_pt, states, soup, lists["pt"].list, trip, b, n_ee, kappa)
+    e = np.zeros(1, np.float32)
+    wp.launch(ns32["contact_energy_ee"], n_ee, states, soup, lists["ee"].list, e, kappa)
+    e_ee = e[0]
+    e[0] = 0
+    wp.launch(ns32["contact_energy_pt"], n_pt, states, soup, lists["pt"].list, e, kappa)
+    np.savez_compressed(os.path.join(HERE, "narrow_fp32.npz"), x=x32, xcs=xcs32, l0=np.float32(2) * th,
+                        rows=trip.rows, cols=trip.cols, vals=trip.vals, force=b, e_ee=e_ee, e_pt=e[0])
+
+
+def main(ref: str, sections=("A", "B", "C", "D", "E", "F", "G", "H", "I")):
     if "F" in sections:
         make_fem(ref)
     if "G" in sections:
         make_abd(ref)
     if "H" in sections:
         make_fp32(ref)
+    if "I" in sections:
+        make_narrow32(ref)
     if not set(sections) & set("ABCDE"):
         print("golden vectors written:", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
         return
@@ -531,5 +573,5 @@ def main(ref: str, sections=("A", "B", "C", "D", "E", "F", "G", "H")):
 
 if __name__ == "__main__":
     if len(sys.argv) < 2:
-        sys.exit("usage: python tests/golden/make_golden.py <path of the ipc_warp source tree> [sections A..H]")
-    main(sys.argv[1], tuple(sys.argv[2:]) or ("A", "B", "C", "D", "E", "F", "G", "H"))
+        sys.exit("usage: python tests/golden/make_golden.py <path of the ipc_warp source tree> [sections A..I]")
+    main(sys.argv[1], tuple(sys.argv[2:]) or ("A", "B", "C", "D", "E", "F", "G", "H", "I"))

@@ -170,3 +170,31 @@ def test_ccd_float32_build():
     assert st == 0 and np.array_equal(nr, d["cubic_n_roots_64"])
     for i in range(len(nr)):
         assert np.array_equal(roots[i, :nr[i]], d["cubic_roots_64"][i, :nr[i]])
+
+
+def test_narrow_phase_matches_reference_float32_build():
+    """contact_hessian_ee/pt and contact_energy_ee/pt of the reference's
+    float32 build on the narrow_fp64.npz scene rounded to float32
+    (narrow_fp32.npz): the oracle's float mode (float32 gate and features,
+    geometry and barrier in double) within 1e-5 per record, in the force
+    and in the energies -- the float32 tolerance of the north star."""
+    d = load("narrow_fp32.npz")
+    d64 = load("narrow_fp64.npz")
+    x, xcs, l0, kappa = d["x"], d["xcs"], d["l0"], float(d64["kappa"])
+    force = np.zeros(x.shape)
+    off = 0
+    for kind, rec, e_ref in (("ee", d64["ee"], d["e_ee"]), ("pt", d64["pt"], d["e_pt"])):
+        n = len(rec)
+        F, H, E, act = po.narrow(kind, rec[:, :4], np.full(n, l0, np.float32), x, xcs, kappa, fp64=False, mode=0)
+        for p in range(n):
+            Href = d["vals"][(off + p) * 16:(off + p + 1) * 16].astype(np.float64)
+            Href = Href.reshape(4, 4, 3, 3).transpose(0, 2, 1, 3).reshape(12, 12)
+            if not act[p]:
+                assert not np.any(Href)
+                continue
+            assert rel_err(H[p], Href) < 1e-5, (kind, p)
+            for k in range(4):
+                force[rec[p, k]] += F[p, 3 * k:3 * k + 3]
+        assert abs(E.sum() - float(e_ref)) <= 1e-5 * abs(float(e_ref))
+        off += n
+    assert rel_err(force, d["force"]) < 1e-5
