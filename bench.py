@@ -3,10 +3,17 @@
 One step = one Newton iteration's contact block through the public API
 (ipc_warp_b200.pipeline.ContactPipeline.iteration): BVH refit, EE + PT
 candidate detection, narrow phase (force + 16 Hessian triplets per record),
-BSR assembly, barrier energy and the CCD step bound, on the rod-bundle scene
-of the rod-twist configuration (16 rods of 4x4x256 hex cells, 5 tets/cell,
-102,800 vertices) in its wound contact state: facing rod sides 0.5 dhat apart
-(dhat = 1e-3 rod width).  Synthetic, seeded inputs.
+BSR assembly, barrier energy and the CCD step bound.
+
+Workloads (synthetic, seeded; the reference ships none of its scene assets):
+
+* screw_nut (the headline): a bolt and a nut of a 60-degree ISO thread,
+  pitch 0.1 of the 1.0 major radius, 12 turns, about 0.5M surface triangles
+  and 1.23M tets per body, radial clearance 1e-4, dhat 5e-5, the nut pushed
+  onto one flank (gap 0.4 dhat) and driven at 4 rad/s over dt = 2e-3;
+* rod_bundle (a second line): the rod-twist configuration's 16 rods of
+  4x4x256 hex cells, 5 tets/cell (102,800 vertices) in the wound contact
+  state, facing rod sides 0.5 dhat apart (dhat = 1e-3 rod width).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -32,21 +39,36 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Newton step ms, learned-PCG vs cuDSS at rel res 1e-6; contact pairs/s, %HBM"
-WORKLOAD = "rod_twist_16rods_4x4x256_wound_contact_state"
-
+WORKLOADS = {
+    "screw_nut": "screw_nut_iso60_pitch0.1_12turns_0.5Mtris_per_body_loaded_flank_driven_4rad_s",
+    "rod_bundle": "rod_twist_16rods_4x4x256_wound_contact_state",
+}
+HEADLINE = "screw_nut"
 
 ROD_SIDE = 4  # rods per side of the bundle; --rods N shrinks the workload for profiler captures
 
 
-def scene():
+def scene(name: str = HEADLINE):
     from ipc_warp_b200 import scenes
 
+    if name == "screw_nut":
+        return scenes.screw_and_nut()
     return scenes.rod_bundle(n_rods_side=ROD_SIDE, cells=(4, 4, 256), width=0.1, gap_over_dhat=0.5,
                              jitter_over_dhat=0.05, seed=1, kappa=1e4)
 
 
+def direction(sc):
+    """The workload's Newton direction (x1 = x - dx)."""
+    from ipc_warp_b200 import scenes
+
+    if sc.name.startswith("screw_nut"):
+        return scenes.screw_direction(sc)
+    return newton_direction(sc)
+
+
 def newton_direction(sc, seed=2):
-    """Seeded stand-in for a Newton step: neighbours approach by ~dhat."""
+    """Seeded stand-in for a Newton step of the rod bundle: neighbours
+    approach by ~dhat."""
     rng = np.random.default_rng(seed)
     dx = rng.normal(scale=0.3 * sc.dhat, size=sc.x.shape)
     width = sc.meta["width"]
@@ -133,9 +155,10 @@ def peaks():
 # algorithmic bytes per pair of the narrow-phase kernel (float32 records):
 # record 24 + positions 48 + 16 triplets (4+4+36) 704 + force 48; EE adds rest positions 48
 NARROW_BYTES = {"pt": 824, "ee": 872}
-# dram__bytes_read.sum + dram__bytes_write.sum of the EE + PT narrow-phase launches
-# of one step on this workload (one-pass ncu capture of the full workload)
-NARROW_DRAM_BYTES_PER_STEP = 441.4e6
+# dram__bytes_read.sum + dram__bytes_write.sum of the EE + PT narrow-phase
+# launches of one step (one-pass ncu capture of the full workload); None until
+# captured for the current kernels
+NARROW_DRAM_BYTES_PER_STEP = {"rod_bundle": 441.4e6, "screw_nut": None}
 
 
 def stage_times(pipe, dx, reps, torch):
@@ -192,7 +215,7 @@ def newton_solver(dev, torch, linear_solver: str, preconditioner: str, theta: fl
     from ipc_warp_b200 import scenes
     from ipc_warp_b200.newton import FEMContactSolver
 
-    sc = scene()
+    sc = scene("rod_bundle")
     fixed, at = scenes.twist_targets(sc, omega=2.0)
     s = FEMContactSolver(sc, material="stvk", E=1e6, nu=0.45, h=5e-3, fixed=fixed, gravity=(0.0, 0.0, 0.0),
                          dtype=torch.float32, device=dev, tol=1e-6, maxiter=20000, linear_solver=linear_solver,
@@ -318,7 +341,8 @@ def run_profile_newton(args):
 # ------------------------------------------------------------- CPU oracle
 def cpu_pipeline(sc, dx, reps):
     """One pass of the oracle's restatement: DCD EE + PT, narrow phase
-    (analytic subspace route), energy, scene TOI.  Returns (pairs, seconds/pass)."""
+    (analytic subspace route: force, Hessian, energy), contact BSR assembly,
+    scene TOI.  Returns (pairs, seconds/pass)."""
     from oracle import pyoracle as po
 
     x32 = sc.x.astype(np.float32)
@@ -332,8 +356,10 @@ def cpu_pipeline(sc, dx, reps):
         pt = po.dcd_pt(x32, sc.triangles, sc.body, th, cap=1 << 21)
         l0e = np.full(len(ee), th * np.float32(2), np.float32)
         l0p = np.full(len(pt), th * np.float32(2), np.float32)
-        po.narrow("ee", ee[:, :4], l0e, x32, sc.xcs.astype(np.float32), sc.kappa, mode=1)
-        po.narrow("pt", pt[:, :4], l0p, x32, None, sc.kappa, mode=1)
+        _, He, _, _ = po.narrow("ee", ee[:, :4], l0e, x32, sc.xcs.astype(np.float32), sc.kappa, mode=1)
+        _, Hp, _, _ = po.narrow("pt", pt[:, :4], l0p, x32, None, sc.kappa, mode=1)
+        po.contact_bsr(sc.n_verts, np.concatenate([ee[:, :4], pt[:, :4]]), np.concatenate([He, Hp]))
+        del He, Hp
         po.scene_toi(x32, x1, sc.edges, sc.triangles, sc.body)
         times.append(time.perf_counter() - t0)
         pairs = len(ee) + len(pt)
@@ -345,8 +371,8 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    sc = scene()
-    dx = newton_direction(sc)
+    sc = scene(args.workload)
+    dx = direction(sc)
     cores = os.cpu_count()
     cpu_pipeline(sc, dx, max(args.warmup, 1))
     pairs, sec = cpu_pipeline(sc, dx, args.steps)
@@ -355,13 +381,18 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "verts": sc.n_verts, "edges": sc.n_edges, "tris": sc.n_tris,
-                   "dhat": sc.dhat, "pairs": pairs, "threads": cores},
+        "config": workload_config(args.workload, sc, pairs),
         "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": "port",
-                         "sample": "full workload, one DCD+narrow+energy+CCD pass per step (C++ oracle, OpenMP)"},
+                         "sample": "full workload, one DCD+narrow+energy+BSR+CCD pass per step (C++ oracle, OpenMP)"},
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+def workload_config(name, sc, pairs):
+    """The config keys both arms report for a workload."""
+    return {"workload": WORKLOADS[name], "verts": sc.n_verts, "edges": sc.n_edges, "tris": sc.n_tris,
+            "dhat": sc.dhat, "pairs": pairs}
 
 
 def max_over_ranks(values, device):
@@ -380,25 +411,15 @@ def job_throughput(world: int, pairs: int, steps: int, total_ms: float) -> float
     return world * pairs * steps / (total_ms * 1e-3)
 
 
-def run_ours(args):
-    import torch
-    import torch.distributed as dist
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        from datetime import timedelta
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
-
+def measure(name, args, dev, world, rank, torch, dist, full: bool):
+    """Time one workload: K device-timed steps (L2 flushed between steps),
+    then K end-to-end steps with host positions and direction copied in and
+    the force copied out.  With ``full`` (rank 0), also the stage times, the
+    roofline of the narrow phase, the CPU baseline and the kernel count."""
     from ipc_warp_b200.pipeline import ContactPipeline
 
-    sc = scene()
-    dx_np = newton_direction(sc)
+    sc = scene(name)
+    dx_np = direction(sc)
     pipe = ContactPipeline.from_scene(sc, dtype=torch.float32, device=dev)
     dx = torch.tensor(dx_np, dtype=torch.float32, device=dev)
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)
@@ -406,9 +427,6 @@ def run_ours(args):
     def step():
         return pipe.iteration(dx)
 
-    sampler = ClockSampler(local)
-    if not args.profile_only:
-        sampler.start()
     for _ in range(max(args.warmup, 3)):
         r = step()
     torch.cuda.synchronize()
@@ -419,9 +437,8 @@ def run_ours(args):
             step()
         torch.cuda.synchronize()
         torch.cuda.profiler.stop()
-        return
+        return None
 
-    # ---- device-resident timing: K steps, L2 flushed between steps
     def barrier():
         if world > 1:
             dist.barrier()
@@ -457,53 +474,86 @@ def run_ours(args):
         e.record()
         e2e_ev.append((s, e))
     barrier()
-    clocks = sampler.stop()
     e2e_ms = sum(s.elapsed_time(e) for s, e in e2e_ev)
     h2d = xh.numel() * 4 + dxh.numel() * 4
-    d2h = bh.numel() * 4 + 8 + 4 + 8  # force, energy, toi, counts
-
+    d2h = bh.numel() * 4 + 8 + 4 + 16  # force, energy, toi, counts + statuses
     if world > 1:
         total_ms, e2e_ms = max_over_ranks([total_ms, e2e_ms], dev)
+    out = {"workload": WORKLOADS[name], "pairs": pairs, "n_ee": r.n_ee, "n_pt": r.n_pt,
+           "value": job_throughput(world, pairs, args.steps, total_ms), "ms_per_step": total_ms / args.steps,
+           "e2e": {"value": job_throughput(world, pairs, args.steps, e2e_ms), "unit": "pairs/s",
+                   "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+           "sc": sc}
+    if not full:
+        return out
+    ws = [int(v) for v in torch.cat([pipe._toi_ws[:4].view(torch.int32), pipe._toi_ws_pt[:4].view(torch.int32)])]
+    st = stage_times(pipe, dx, 5, torch)
+    n_launch, names = count_kernels(step)
+    peak, peak_kind = peaks()
+    n_ee, n_pt = pipe.n_contacts, pipe.n_contacts_pt
+    narrow_ms = st["narrow_ee"] + st["narrow_pt"]
+    algo = n_ee * NARROW_BYTES["ee"] + n_pt * NARROW_BYTES["pt"]
+    achieved = algo / (narrow_ms * 1e-3) / 1e9
+    cpu_pairs, cpu_sec = cpu_pipeline(sc, dx_np, 3)
+    out.update({
+        "ccd_candidates": ws[0] + ws[1],
+        "stage_ms": {k: round(v, 4) for k, v in st.items()},
+        "roofline": {"kernel": "k_contact_hessian (EE + PT)", "bound": "hbm", "achieved": achieved,
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": NARROW_DRAM_BYTES_PER_STEP[name], "algorithmic_bytes": algo},
+        "cpu_baseline": {"value": cpu_pairs / cpu_sec, "unit": "pairs/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": "full workload, 3 passes of the C++ oracle pipeline (DCD+narrow+energy+BSR+CCD)"},
+        "gpu_launches": n_launch * args.steps, "kernels": names,
+    })
+    return out
 
-    # ---- roofline of the dominant kernel and kernel count (rank 0, untimed)
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    sampler = ClockSampler(local)
+    if not args.profile_only:
+        sampler.start()
+    head = measure(args.workload, args, dev, world, rank, torch, dist, full=rank == 0)
+    if args.profile_only:
+        return
+    second = None
+    if not args.headline_only:
+        other = "rod_bundle" if args.workload != "rod_bundle" else "screw_nut"
+        second = measure(other, args, dev, world, rank, torch, dist, full=rank == 0)
+    clocks = sampler.stop()
     out = None
     if rank == 0:
-        st = stage_times(pipe, dx, 5, torch)
-        n_launch, names = count_kernels(step)
-        peak, peak_kind = peaks()
-        n_ee, n_pt = pipe.n_contacts, pipe.n_contacts_pt
-        narrow_ms = st["narrow_ee"] + st["narrow_pt"]
-        algo = n_ee * NARROW_BYTES["ee"] + n_pt * NARROW_BYTES["pt"]
-        achieved = algo / (narrow_ms * 1e-3) / 1e9
-        traffic = NARROW_DRAM_BYTES_PER_STEP
-        cpu_pairs, cpu_sec = cpu_pipeline(sc, dx_np, 3)
         newton = None if args.no_newton else newton_step_times(dev, torch)
-        ms = total_ms / args.steps
+        sc = head.pop("sc")
+        cfg = workload_config(args.workload, sc, head["pairs"])
+        cfg.update({"n_ee": head["n_ee"], "n_pt": head["n_pt"], "ccd_candidates": head["ccd_candidates"],
+                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
+                    "stage_ms": head["stage_ms"]})
         out = {
-            "metric": METRIC,
-            "value": job_throughput(world, pairs, args.steps, total_ms),
-            "unit": "pairs/s",
-            "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
+            "metric": METRIC, "value": head["value"], "unit": "pairs/s",
+            "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": head["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic",
-            "config": {"workload": WORKLOAD, "verts": sc.n_verts, "edges": sc.n_edges, "tris": sc.n_tris,
-                       "dhat": sc.dhat, "n_ee": n_ee, "n_pt": n_pt, "l2": "flushed between steps (256 MiB write)",
-                       "parallelism": f"replicas x{world}",
-                       "stage_ms": {k: round(v, 4) for k, v in st.items()}},
-            "roofline": {"kernel": "k_contact_hessian (EE + PT)", "bound": "hbm", "achieved": achieved,
-                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic,
-                         "algorithmic_bytes": algo},
-            "cpu_baseline": {"value": cpu_pairs / cpu_sec, "unit": "pairs/s", "cores": os.cpu_count(),
-                             "kind": "port",
-                             "sample": "full workload, 3 passes of the C++ oracle pipeline (DCD+narrow+energy+CCD)"},
-            "e2e": {"value": job_throughput(world, pairs, args.steps, e2e_ms), "unit": "pairs/s",
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": n_launch * args.steps,
-            "kernels": names,
-            "clocks": clocks,
+            "data": "synthetic", "config": cfg, "roofline": head["roofline"], "cpu_baseline": head["cpu_baseline"],
+            "e2e": head["e2e"], "gpu_launches": head["gpu_launches"], "kernels": head["kernels"], "clocks": clocks,
             "newton_step": newton,
         }
+        if second is not None:
+            second.pop("sc")
+            second.pop("kernels", None)
+            out["second_workload"] = second
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -523,6 +573,9 @@ def main():
                     help="skip the Newton-step timing (learned-PCG / Jacobi-PCG / direct)")
     ap.add_argument("--profile-solver", action="store_true",
                     help="untimed Newton-solve kernels only (learned factor + PCG), for ncu; prints nothing")
+    ap.add_argument("--workload", default=HEADLINE, choices=sorted(WORKLOADS),
+                    help="headline workload (the other one is measured as a second line)")
+    ap.add_argument("--headline-only", action="store_true", help="skip the second workload")
     ap.add_argument("--rods", type=int, default=4,
                     help="rods per side of the bundle (4 = the benchmark workload; smaller for ncu section captures)")
     ap.add_argument("--profile-newton", action="store_true",

@@ -74,11 +74,11 @@ class ContactPipeline(ContactBarrierMixin):
                           "energy": torch.zeros(1, dtype=torch.float64, pin_memory=pin),
                           "toi": torch.zeros(1, dtype=soup.x_transformed.dtype, pin_memory=pin)}
 
-    @staticmethod
-    def from_scene(scene, dtype=None, device="cuda", exclude_same_body=False) -> "ContactPipeline":
+    @classmethod
+    def from_scene(cls, scene, dtype=None, device="cuda", exclude_same_body=False) -> "ContactPipeline":
         soup = Soup.from_numpy(scene.x, scene.edges, scene.triangles, scene.body, xcs=scene.xcs, device=device,
                                dtype=dtype)
-        return ContactPipeline(soup, scene.dhat, scene.kappa, exclude_same_body=exclude_same_body)
+        return cls(soup, scene.dhat, scene.kappa, exclude_same_body=exclude_same_body)
 
     def iteration(self, dx: torch.Tensor | None = None) -> IterationResult:
         """One Newton iteration's contact work.  On a GPU every stage is

@@ -327,3 +327,155 @@ def abd_balls(n_side: int = 2, layers: int = 1, subdiv: int = 2, radius: float =
     meshes.append(slab)
     transforms.append(transform(position=(-1.5 * radius, -0.2, -1.5 * radius)))
     return dict(meshes=meshes, transforms=transforms, fixed_bodies=[len(meshes) - 1], gravity=(0.0, -9.8, 0.0))
+
+
+# ------------------------------------------------------------ screw and nut
+def iso_thread_radius(s, major: float, pitch: float):
+    """Radius of a 60-degree ISO metric thread profile at thread phase s
+    (turns; the profile repeats every unit of s): crest flat of pitch/8 at the
+    major radius (centred on s = 0), flanks at 30 degrees from the radial
+    direction over 5 pitch/16 each, root flat of pitch/4; depth 5/8 of the
+    sharp-V height sqrt(3)/2 pitch."""
+    u = np.mod(np.asarray(s, np.float64), 1.0)
+    depth = 5.0 / 16.0 * np.sqrt(3.0) * pitch
+    r = np.full(u.shape, major)
+    down = (u >= 1 / 16) & (u < 6 / 16)
+    r[down] = major - depth * (u[down] - 1 / 16) / (5 / 16)
+    r[(u >= 6 / 16) & (u < 10 / 16)] = major - depth
+    up = (u >= 10 / 16) & (u < 15 / 16)
+    r[up] = major - depth * (15 / 16 - u[up]) / (5 / 16)
+    return r
+
+
+def helical_tube(n_rho: int, n_theta: int, per_pitch: int, turns: int, pitch: float, r_in, r_out,
+                 theta0: float = 0.0) -> Mesh:
+    """Tetrahedralised tube on a helical grid: vertex (i, j, k) at angle
+    theta_j = theta0 + 2 pi j / n_theta, thread phase s_k = k / per_pitch,
+    height z = pitch (s_k + theta_j / 2 pi) and radius interpolated between
+    r_in(s) and r_out(s) by i / n_rho, so grid lines along k follow the
+    helix and every profile corner at a multiple of 1/per_pitch is a grid
+    line.  Around the axis, column n_theta - 1 joins column 0 one turn up
+    (k + per_pitch); cells whose neighbour would lie past the last turn are
+    left out (the ends are helical ramps).  Cells are split into 5 tets with
+    the split alternating in (i + j + k), which matches across the seam when
+    n_theta - per_pitch is even."""
+    assert (n_theta - per_pitch) % 2 == 0, "the 5-tet split needs n_theta - per_pitch even"
+    ns = per_pitch * turns
+    k = np.arange(ns + 1)
+    sk = k / per_pitch
+    ri, ro = np.broadcast_to(r_in(sk), sk.shape), np.broadcast_to(r_out(sk), sk.shape)
+    I, J, K = np.meshgrid(np.arange(n_rho + 1), np.arange(n_theta), k, indexing="ij")
+    rad = ri[K] + (ro[K] - ri[K]) * (I / n_rho)
+    th = theta0 + 2.0 * np.pi * J / n_theta
+    z = pitch * (K / per_pitch + th / (2.0 * np.pi))
+    x = np.stack([rad * np.cos(th), rad * np.sin(th), z], axis=-1).reshape(-1, 3)
+
+    def vid(i, j, kk):
+        return (i * n_theta + j) * (ns + 1) + kk
+
+    ci, cj, ck = np.meshgrid(np.arange(n_rho), np.arange(n_theta), np.arange(ns), indexing="ij")
+    ci, cj, ck = ci.ravel(), cj.ravel(), ck.ravel()
+    corners = []
+    keep = np.ones(ci.shape, bool)
+    for b in _CORNERS:
+        j = cj + b[1]
+        kk = ck + b[2]
+        wrap = j == n_theta
+        j = np.where(wrap, 0, j)
+        kk = np.where(wrap, kk + per_pitch, kk)
+        keep &= kk <= ns
+        corners.append(vid(ci + b[0], j, kk))
+    corners = np.stack(corners, axis=1)[keep]
+    parity = ((ci + cj + ck) & 1)[keep]
+    tets = []
+    for par in (0, 1):
+        cs = corners[parity == par]
+        for t in _five_tet_split(par):
+            tets.append(cs[:, t])
+    tets = np.concatenate(tets).astype(np.int64)
+    a, b_, c, d = (x[tets[:, q]] for q in range(4))
+    vol = np.einsum("ij,ij->i", np.cross(b_ - a, c - a), d - a)
+    flip = vol < 0
+    tets[flip, 1], tets[flip, 2] = tets[flip, 2].copy(), tets[flip, 1].copy()
+    used = np.unique(tets)
+    remap = np.full(x.shape[0], -1, np.int64)
+    remap[used] = np.arange(used.size)
+    x, tets = x[used], remap[tets]
+    tris = boundary_faces_fast(tets)
+    return Mesh(x=x, tets=tets, triangles=tris, edges=surface_edges_fast(tris))
+
+
+def boundary_faces_fast(tets: np.ndarray) -> np.ndarray:
+    """boundary_faces with a packed 63-bit key per face (vertex ids < 2^21)."""
+    local = np.array([[1, 2, 3], [0, 3, 2], [0, 1, 3], [0, 2, 1]])
+    faces = tets[:, local].reshape(-1, 3)
+    assert faces.max() < (1 << 21)
+    srt = np.sort(faces, axis=1).astype(np.int64)
+    key = (srt[:, 0] << 42) | (srt[:, 1] << 21) | srt[:, 2]
+    order = np.argsort(key, kind="stable")
+    ks = key[order]
+    first = np.r_[True, ks[1:] != ks[:-1]]
+    start = np.flatnonzero(first)
+    cnt = np.diff(np.r_[start, ks.size])
+    single = order[start[cnt == 1]]
+    return faces[np.sort(single)].astype(np.int64)
+
+
+def surface_edges_fast(tris: np.ndarray) -> np.ndarray:
+    e = np.concatenate([tris[:, [0, 1]], tris[:, [1, 2]], tris[:, [2, 0]]])
+    e = np.sort(e, axis=1).astype(np.int64)
+    key = np.unique((e[:, 0] << 21) | e[:, 1])
+    return np.stack([key >> 21, key & ((1 << 21) - 1)], axis=1)
+
+
+def screw_and_nut(n_theta: int = 640, per_pitch: int = 16, turns: int = 12, n_rho: int = 2, major: float = 1.0,
+                  pitch: float = 0.1, hole: float = 0.5, nut_outer: float = 1.5, clearance: float = 1e-4,
+                  dhat: float = 5e-5, load_gap_over_dhat: float = 0.4, kappa: float = 1e4,
+                  seed: int = 4) -> Scene:
+    """Bolt and nut of a 60-degree ISO thread (pitch 0.1 of the 1.0 major
+    radius, 12 turns) on the same helical grid (``helical_tube``): the bolt a
+    tube from radius ``hole`` to the thread profile, the nut a tube from the
+    profile plus the radial clearance (1e-4 radius) to ``nut_outer``.  A
+    radial clearance c leaves c sin(30 deg) = c/2 between facing flanks; the
+    nut is then pushed along the axis onto one flank so that flank's gap is
+    ``load_gap_over_dhat`` dhat (the loaded state of a nut driven onto the
+    bolt), which puts the whole loaded flank inside the barrier.  The nut's
+    grid is turned half a column about the axis so its edges cross the
+    bolt's.  Defaults: 640 columns around, 16 rows a pitch, 2 cells through
+    the wall: about 0.5M surface triangles and 1.23M tets per body.  Bolt
+    (body 0) is the affine body and the nut (body 1) the FEM body of the
+    screw-and-nut configuration."""
+    rng = np.random.default_rng(seed)
+    prof = lambda s: iso_thread_radius(s, major, pitch)  # noqa: E731
+    bolt = helical_tube(n_rho, n_theta, per_pitch, turns, pitch, lambda s: np.full_like(s, hole), prof)
+    half = np.pi / n_theta
+    nut = helical_tube(n_rho, n_theta, per_pitch, turns, pitch, lambda s: prof(s) + clearance,
+                       lambda s: np.full_like(s, nut_outer), theta0=half)
+    # both flanks are c/2 from the bolt's; the axial push closes one of them
+    flank_gap = 0.5 * clearance
+    push = (flank_gap - load_gap_over_dhat * dhat) / np.cos(np.pi / 6)
+    nut.x[:, 2] -= push
+    sc = assemble([bolt, nut], f"screw_nut_{n_theta}x{per_pitch * turns}x{n_rho}", dhat, kappa,
+                  {"pitch": pitch, "major": major, "clearance": clearance, "push": push, "n_theta": n_theta,
+                   "per_pitch": per_pitch, "turns": turns})
+    sc.x += rng.uniform(-1e-7, 1e-7, size=sc.x.shape)
+    sc.xcs = sc.x.copy()
+    return sc
+
+
+def screw_direction(sc: Scene, omega: float = 4.0, dt: float = 2e-3, seed: int = 5) -> np.ndarray:
+    """Newton direction of the driven nut (x1 = x - dx): one step of the
+    nut turning at ``omega`` about the axis while held axially, so its
+    loaded flank advances into the bolt's by pitch omega dt / 2 pi; small
+    seeded noise on every vertex."""
+    rng = np.random.default_rng(seed)
+    x = sc.x
+    nut = sc.body == 1
+    a = omega * dt
+    c, s_ = np.cos(a), np.sin(a)
+    x1 = x.copy()
+    x1[nut, 0] = c * x[nut, 0] - s_ * x[nut, 1]
+    x1[nut, 1] = s_ * x[nut, 0] + c * x[nut, 1]
+    dx = x - x1
+    dx += rng.normal(scale=0.05 * sc.dhat, size=dx.shape)
+    return dx

@@ -682,38 +682,74 @@ inline bool overlap(const Box& a, const Box& b) {
          a.lo[2] <= b.hi[2] && b.lo[2] <= a.hi[2];
 }
 
-// Sorted-axis pruning: calls fn(i, j) for every query i and target j whose
-// boxes overlap.  Exactness of the candidate set comes from the predicate; the
-// pruning only has to be conservative.
+// Uniform-grid pruning: calls fn(i, j) once for every query i and target j
+// whose boxes overlap.  Targets are binned into every cell of a uniform grid
+// (cell edge = twice the mean target extent) that their box touches; a query
+// visits the cells its box touches and reports a pair only from the cell that
+// holds the lower corner of the two boxes' intersection, so each pair is
+// reported once.  Exactness of the candidate set comes from the predicate;
+// the pruning only has to be conservative.
 template <class Fn>
 void sweep(const std::vector<Box>& q, const std::vector<Box>& t, Fn&& fn) {
-  int nt = (int)t.size(), nq = (int)q.size();
+  const int nt = (int)t.size(), nq = (int)q.size();
   if (nt == 0 || nq == 0) return;
-  // sweep along the axis with the largest spread of box corners
-  int ax = 0;
-  float best = -1.f;
-  for (int k = 0; k < 3; ++k) {
-    float mn = 3.4e38f, mx = -3.4e38f;
-    for (int j = 0; j < nt; ++j) { mn = std::min(mn, t[j].lo[k]); mx = std::max(mx, t[j].lo[k]); }
-    if (mx - mn > best) { best = mx - mn; ax = k; }
+  float lo[3] = {3.4e38f, 3.4e38f, 3.4e38f}, hi[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+  double ext = 0.0;
+  for (int j = 0; j < nt; ++j)
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], t[j].lo[k]);
+      hi[k] = std::max(hi[k], t[j].hi[k]);
+      ext += (double)t[j].hi[k] - (double)t[j].lo[k];
+    }
+  double h = std::max(2.0 * ext / (3.0 * nt), 1e-30);
+  long long dims[3];
+  for (;;) {  // at most ~64M cells
+    long long tot = 1;
+    for (int k = 0; k < 3; ++k) {
+      dims[k] = std::max(1LL, (long long)std::ceil(((double)hi[k] - lo[k]) / h) + 1);
+      tot *= dims[k];
+    }
+    if (tot <= (1LL << 26)) break;
+    h *= 1.5;
   }
-  std::vector<int> order(nt);
-  for (int j = 0; j < nt; ++j) order[j] = j;
-  std::sort(order.begin(), order.end(), [&](int a, int b) { return t[a].lo[ax] < t[b].lo[ax]; });
-  std::vector<float> lo(nt);
-  float maxw = 0.f;
+  auto cell = [&](float v, int k) -> long long {
+    double c = std::floor(((double)v - lo[k]) / h);
+    return (long long)std::min(std::max(c, 0.0), (double)(dims[k] - 1));
+  };
+  auto key = [&](long long a, long long b, long long c) { return (a * dims[1] + b) * dims[2] + c; };
+  std::vector<std::pair<long long, int>> bins;
+  bins.reserve((size_t)nt * 2);
   for (int j = 0; j < nt; ++j) {
-    lo[j] = t[order[j]].lo[ax];
-    maxw = std::max(maxw, t[order[j]].hi[ax] - t[order[j]].lo[ax]);
+    long long a0 = cell(t[j].lo[0], 0), a1 = cell(t[j].hi[0], 0), b0 = cell(t[j].lo[1], 1),
+              b1 = cell(t[j].hi[1], 1), c0 = cell(t[j].lo[2], 2), c1 = cell(t[j].hi[2], 2);
+    for (long long a = a0; a <= a1; ++a)
+      for (long long b = b0; b <= b1; ++b)
+        for (long long c = c0; c <= c1; ++c) bins.push_back({key(a, b, c), j});
   }
+  std::sort(bins.begin(), bins.end());
+  std::vector<long long> keys(bins.size());
+  for (size_t i = 0; i < bins.size(); ++i) keys[i] = bins[i].first;
 #pragma omp parallel for schedule(dynamic, 256)
   for (int i = 0; i < nq; ++i) {
-    float a = q[i].lo[ax] - maxw, b = q[i].hi[ax];
-    int k = (int)(std::lower_bound(lo.begin(), lo.end(), a) - lo.begin());
-    for (; k < nt && lo[k] <= b; ++k) {
-      int j = order[k];
-      if (overlap(q[i], t[j])) fn(i, j);
-    }
+    const Box& Q = q[i];
+    long long a0 = cell(Q.lo[0], 0), a1 = cell(Q.hi[0], 0), b0 = cell(Q.lo[1], 1), b1 = cell(Q.hi[1], 1),
+              c0 = cell(Q.lo[2], 2), c1 = cell(Q.hi[2], 2);
+    for (long long a = a0; a <= a1; ++a)
+      for (long long b = b0; b <= b1; ++b)
+        for (long long c = c0; c <= c1; ++c) {
+          long long k = key(a, b, c);
+          size_t p = (size_t)(std::lower_bound(keys.begin(), keys.end(), k) - keys.begin());
+          for (; p < keys.size() && keys[p] == k; ++p) {
+            int j = bins[p].second;
+            const Box& T = t[j];
+            if (!overlap(Q, T)) continue;
+            // report from the cell of the intersection's lower corner only
+            if (cell(std::max(Q.lo[0], T.lo[0]), 0) != a || cell(std::max(Q.lo[1], T.lo[1]), 1) != b ||
+                cell(std::max(Q.lo[2], T.lo[2]), 2) != c)
+              continue;
+            fn(i, j);
+          }
+        }
   }
 }
 
@@ -1272,6 +1308,69 @@ double ora_tet(int mat, int nv, const double* x, const double* xcs, int nt, cons
       }
   }
   return energy;
+}
+
+// Contact-block BSR assembly (dynamic_contacts.py:281-297: triplets
+// i*16 + ii*4 + jj of each record -> bsr_from_triplets): record p's 12x12
+// Hessian hess[p] gives 16 blocks keyed (idx[p][ii], idx[p][jj]); all-zero
+// blocks are dropped (warp's prune_numerical_zeros); equal keys are summed in
+// record order.  offsets[nv + 1]; cols/vals sized by the caller (cap blocks).
+// Returns nnz (when > cap nothing past cap is written).
+int ora_contact_bsr(int nv, int n, const int* idx, const double* hess, int* offsets, int* cols, double* vals,
+                    int cap) {
+  std::vector<int> cnt(nv + 1, 0);
+  auto block_nz = [&](long p, int ii, int jj) {
+    const double* H = hess + (size_t)p * 144;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        if (H[(3 * ii + a) * 12 + 3 * jj + b] != 0.0) return true;
+    return false;
+  };
+  for (long p = 0; p < n; ++p)
+    for (int ii = 0; ii < 4; ++ii)
+      for (int jj = 0; jj < 4; ++jj)
+        if (block_nz(p, ii, jj)) cnt[idx[4 * p + ii] + 1]++;
+  for (int r = 0; r < nv; ++r) cnt[r + 1] += cnt[r];
+  std::vector<int> slot(cnt.begin(), cnt.end() - 1);
+  std::vector<int> ids(cnt[nv]);
+  for (long p = 0; p < n; ++p)
+    for (int ii = 0; ii < 4; ++ii)
+      for (int jj = 0; jj < 4; ++jj)
+        if (block_nz(p, ii, jj)) ids[slot[idx[4 * p + ii]]++] = (int)(p * 16 + ii * 4 + jj);
+  auto col_of = [&](int id) { return idx[4 * (id / 16) + (id % 4)]; };
+  std::vector<int> distinct(nv + 1, 0);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int r = 0; r < nv; ++r) {
+    int* b = ids.data() + cnt[r];
+    int* e = ids.data() + cnt[r + 1];
+    std::sort(b, e, [&](int x, int y) { return col_of(x) != col_of(y) ? col_of(x) < col_of(y) : x < y; });
+    int d = 0;
+    for (int* q = b; q < e; ++q)
+      if (q == b || col_of(*q) != col_of(*(q - 1))) ++d;
+    distinct[r + 1] = d;
+  }
+  for (int r = 0; r < nv; ++r) distinct[r + 1] += distinct[r];
+  for (int r = 0; r <= nv; ++r) offsets[r] = distinct[r];
+  const int nnz = distinct[nv];
+  if (nnz > cap) return nnz;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int r = 0; r < nv; ++r) {
+    int o = distinct[r] - 1;
+    for (int q = cnt[r]; q < cnt[r + 1]; ++q) {
+      const int id = ids[q];
+      const long p = id / 16;
+      const int ii = (id / 4) % 4, jj = id % 4;
+      if (q == cnt[r] || col_of(id) != col_of(ids[q - 1])) {
+        ++o;
+        cols[o] = col_of(id);
+        for (int k = 0; k < 9; ++k) vals[(size_t)o * 9 + k] = 0.0;
+      }
+      const double* H = hess + (size_t)p * 144;
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) vals[(size_t)o * 9 + 3 * a + b] += H[(3 * ii + a) * 12 + 3 * jj + b];
+    }
+  }
+  return nnz;
 }
 
 }  // extern "C"

@@ -169,3 +169,17 @@ def tet(material: int, x, xcs, tets, mu, lam):
     e = f(int(material), x.shape[0], _p(x), _p(xcs), tets.shape[0], _p(tets), ctypes.c_double(mu),
           ctypes.c_double(lam), _p(force), _p(blocks))
     return force, blocks, float(e)
+
+
+def contact_bsr(nv, idx, hess):
+    """Contact BSR (offsets, columns, values (nnz, 3, 3)) of records idx (n, 4)
+    with 12x12 Hessians hess (n, 12, 12), dynamic_contacts.py:281-297."""
+    idx = _i32(idx).reshape(-1, 4)
+    hess = np.ascontiguousarray(hess, dtype=np.float64).reshape(-1, 12, 12)
+    n = idx.shape[0]
+    offsets = np.zeros(nv + 1, np.int32)
+    cap = 16 * n
+    cols = np.zeros(max(cap, 1), np.int32)
+    vals = np.zeros((max(cap, 1), 3, 3))
+    nnz = lib().ora_contact_bsr(int(nv), n, _p(idx), _p(hess), _p(offsets), _p(cols), _p(vals), cap)
+    return offsets, cols[:nnz], vals[:nnz]

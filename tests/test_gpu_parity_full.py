@@ -3,8 +3,11 @@
 One ``ContactPipeline.iteration`` -- the benchmark's step -- on the full
 workloads, every output checked against the CPU oracle on the same inputs:
 
+* the screw-and-nut configuration (60-degree thread, pitch 0.1, 12 turns,
+  about 0.5M surface triangles per body, the nut loaded onto one flank,
+  about 345k candidate pairs) with the driven nut's step: the bench workload;
 * the rod-twist bundle in its wound contact state (16 rods of 4x4x256 hex
-  cells, 102,800 vertices, about 739k candidate pairs): the bench workload;
+  cells, 102,800 vertices, about 739k candidate pairs): the second bench line;
 * the two-cube configuration exactly as generated (8^3 cells per cube,
   upper cube turned 15 degrees about z, 1e-3 above the lower one, jitter
   1e-5, dhat 1e-3, kappa 1e4), and the same scene later in its fall, with
@@ -43,8 +46,11 @@ def workload(name):
     if name == "rod_bundle":
         import bench
 
-        sc = bench.scene()
-        return sc, bench.newton_direction(sc)
+        sc = bench.scene("rod_bundle")
+        return sc, bench.direction(sc)
+    if name == "screw_nut":
+        sc = scenes.screw_and_nut()  # the screw-and-nut configuration: 0.5M surface triangles per body
+        return sc, scenes.screw_direction(sc)
     sc = scenes.two_cubes()  # cfg1 as specified
     rng = np.random.default_rng(11)
     up = sc.body == 1
@@ -71,7 +77,8 @@ def records_to_hessians(vals, n, offset):
     return v.transpose(0, 1, 3, 2, 4).reshape(n, 12, 12)
 
 
-@pytest.mark.parametrize("name,dtype", [("rod_bundle", torch.float32), ("rod_bundle", torch.float64),
+@pytest.mark.parametrize("name,dtype", [("screw_nut", torch.float32), ("screw_nut", torch.float64),
+                                        ("rod_bundle", torch.float32), ("rod_bundle", torch.float64),
                                         ("two_cubes", torch.float32), ("two_cubes_falling", torch.float32),
                                         ("two_cubes_falling", torch.float64)])
 def test_full_size_parity(cuda, name, dtype):
@@ -89,6 +96,8 @@ def test_full_size_parity(cuda, name, dtype):
     assert res.n_ee > 0 and res.n_pt > 0  # the jitter brings parts of the lowest edge inside dhat
     if name == "rod_bundle":
         assert res.n_ee + res.n_pt > 700_000
+    if name == "screw_nut":
+        assert res.n_ee + res.n_pt > 300_000
 
     # ---- narrow phase: every record, in chunks
     x = pipe.soup.x_transformed.cpu().numpy()

@@ -175,3 +175,29 @@ def test_known_tois():
     e1 = e0.copy()
     e1[:2, 2] = -3.0
     assert po.collision_time("ee", e0[None], e1[None])[0] == pytest.approx(0.25, abs=1e-9)
+
+
+def test_contact_bsr_equals_scipy_assembly():
+    """The oracle's contact BSR (the CPU baseline's assembly stage) equals
+    scipy's assembly of the records' 16 triplets, all-zero blocks dropped."""
+    import scipy.sparse as sp
+
+    from ipc_warp_b200.bsr import scipy_from_triplets
+
+    rng = np.random.default_rng(0)
+    nv, n = 60, 400
+    idx = rng.integers(0, nv, (n, 4)).astype(np.int32)
+    H = rng.normal(size=(n, 12, 12))
+    H[::7] = 0.0
+    H[3, 0:3, 3:6] = 0.0
+    off, cols, vals = po.contact_bsr(nv, idx, H)
+    rows = np.repeat(idx, 4, axis=1).ravel()
+    cc = np.tile(idx, (1, 4)).ravel()
+    blocks = H.reshape(n, 4, 3, 4, 3).transpose(0, 1, 3, 2, 4).reshape(-1, 3, 3)
+    keep = np.any(blocks != 0, axis=(1, 2))
+    assert len(cols) == len(np.unique(rows[keep].astype(np.int64) * nv + cc[keep]))
+    got = sp.bsr_matrix((vals, cols, off), shape=(3 * nv, 3 * nv))
+    ref = scipy_from_triplets(nv, nv, rows, cc, blocks)
+    assert abs(got - ref).max() <= 1e-13 * abs(ref).max()
+    for r in range(nv):
+        assert np.all(np.diff(cols[off[r]:off[r + 1]]) > 0)
