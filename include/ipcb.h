@@ -170,9 +170,33 @@ int ipcb_contact_hessian(int kind, const ipcb_soup* soup, const ipcb_contacts* l
 int ipcb_contact_hessian_after(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, int offset,
                                const int* offset_count, double kappa, int* rows, int* cols, void* vals, void* b,
                                unsigned short* block_mask, ipcb_stream s);
+/* ipcb_contact_hessian_after with the list's records first put in cost-class
+ * order over the whole list (costliest first: edge-edge / point-triangle
+ * eigen-solve, point-edge, no eigen-solve, inactive), so that nearly every
+ * warp takes one path through the Hessian: a classification kernel caches
+ * each record's float32 distance and feature, a second one writes the order,
+ * then the Hessian kernel runs in that order.  Same outputs (each record
+ * writes its own slots; only the order of the force atomics differs).
+ * ws: ipcb_contact_hessian_workspace(list->capacity) bytes of device memory. */
+size_t ipcb_contact_hessian_workspace(int capacity);
+int ipcb_contact_hessian_sorted(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, int offset,
+                                const int* offset_count, double kappa, int* rows, int* cols, void* vals, void* b,
+                                unsigned short* block_mask, void* ws, size_t ws_bytes, ipcb_stream s);
 /* energy (double) += sum of the barrier energy of the list */
 int ipcb_contact_energy(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, double kappa,
                         double* energy, ipcb_stream s);
+
+/* ---- intersection check of a surface state ----
+ * No single counterpart in the reference: it is the check its trajectories
+ * are judged by (an accepted step leaves no surface edge crossing a surface
+ * triangle).  Every (edge, triangle) pair without a shared vertex whose
+ * segment crosses the triangle's interior (orientation signs in double,
+ * touching and coplanar configurations not counted) adds 1 to *count (caller
+ * zeroes it); the first `capacity` pairs go to pairs (int32[2*capacity]:
+ * edge, triangle).  tri_bvh: the triangle hierarchy refit to soup->x.
+ * IPCB_STATUS_STACK in *status when a traversal ran out of its bound. */
+int ipcb_edge_triangle_crossings(const ipcb_soup* soup, const ipcb_lbvh* tri_bvh, int* count, int* pairs,
+                                 int capacity, int* status, ipcb_stream s);
 
 /* ---- CCD (ccd/ccd.py:360-427 point_triangle_toi / edge_edge_toi) ----
  * Cubic coplanarity TOI in double for every candidate whose swept boxes

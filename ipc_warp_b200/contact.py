@@ -377,6 +377,28 @@ class ContactSolverBase:
             self.n_contacts_pt = 0
         return self._step_bound()
 
+    def edge_triangle_crossings(self, capacity: int = 0):
+        """Intersection check of the current positions: the number of
+        (surface edge, surface triangle) pairs, without a shared vertex, whose
+        segment crosses the triangle (an accepted IPC step leaves none), and
+        up to ``capacity`` of them as an (m, 2) int32 tensor (edge,
+        triangle).  Refits the triangle hierarchy to the positions (the next
+        detect_collision refits it again)."""
+        if not self.has_triangles:
+            return 0, torch.zeros((0, 2), dtype=torch.int32, device=self.device)
+        self._pack()
+        self._triangle_aabbs()
+        self.tri_mesh.refit()
+        count = torch.zeros(1, dtype=torch.int32, device=self.device)
+        pairs = torch.zeros((max(capacity, 1), 2), dtype=torch.int32, device=self.device)
+        st = torch.zeros(1, dtype=torch.int32, device=self.device)
+        N.call("ipcb_edge_triangle_crossings", ctypes.byref(self.soup.c_struct()), ctypes.byref(self.tri_mesh.c),
+               N.ptr(count), N.ptr(pairs), int(capacity), N.ptr(st), N.stream_handle())
+        n, status = (int(v) for v in torch.cat([count, st]).tolist())
+        if status & QUERY_FAILED:
+            raise RuntimeError(f"intersection check ran out of its traversal bound (status {status})")
+        return n, pairs[:min(n, capacity)]
+
     @property
     def status(self) -> int:
         """OR of IPCB_STATUS_* bits raised by the last queries."""

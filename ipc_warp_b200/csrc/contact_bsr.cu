@@ -300,6 +300,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int*
                                                             const int* __restrict__ offsets, int* __restrict__ columns,
                                                             S* __restrict__ values) {
   __shared__ S sacc[kWarps][kHash * 9];
+  // a batch's 8 quads (36 values each, contiguous per quad), loaded with
+  // 16-byte vectors; lane l's block is then at 9 l (conflict-free: 9 is odd)
+  __shared__ __align__(16) S sstage[kWarps][8 * 36];
+  constexpr int kVec = 36 * (int)sizeof(S) / 16;  // 16-byte vectors per quad
   const unsigned full = 0xffffffffu;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int row = blockIdx.x * kWarps + w;
@@ -316,6 +320,14 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int*
   const int nb = 4 * (e - b);
   constexpr int kNone = kHash;  // no block (past the row, or a zero block)
   for (int base = 0; base < nb; base += 32) {
+    const int q0 = base >> 2, nq = min(8, (nb - base) >> 2);
+    for (int u = lane; u < nq * kVec; u += 32) {
+      const int kk = u / kVec, piece = u - kk * kVec;
+      const int q = __ldg(qids + b + q0 + kk);
+      reinterpret_cast<float4*>(&sstage[w][36 * kk])[piece] =
+          __ldg(reinterpret_cast<const float4*>(vals + 36LL * q) + piece);
+    }
+    __syncwarp();
     const int i = base + lane;
     int pos = kNone;
     S v[9];
@@ -323,13 +335,12 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int*
     for (int t = 0; t < 9; ++t) v[t] = S(0);
     if (i < nb) {
       const int k = i >> 2, jj = i & 3;
-      const int q = __ldg(qids + b + k);
       const unsigned pk = (__ldg(qpos + b + k) >> (8 * jj)) & 0xffu;
       if ((int)pk < cnt) {  // kAbsent for a zero block
         pos = (int)pk;
-        const S* src = vals + 36LL * q + 9 * jj;
+        const S* src = &sstage[w][9 * lane];
 #pragma unroll
-        for (int t = 0; t < 9; ++t) v[t] = __ldg(src + t);
+        for (int t = 0; t < 9; ++t) v[t] = src[t];
       }
     }
     // lanes with the same position form a group (at most 8: a batch is 8

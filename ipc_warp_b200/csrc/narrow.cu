@@ -12,6 +12,8 @@
 //      edges are near parallel
 //   5. H = sum_m w_m h_m h_m^T (h_0 = grad, h_e = negative eigenvectors),
 //      written as 16 3x3 triplets; force atomically added to b.
+#include <cstddef>
+
 #include "narrow_impl.cuh"
 
 namespace ipcb {
@@ -27,20 +29,30 @@ __global__ void __launch_bounds__(128, 3) k_contact_hessian(const S* __restrict_
                                                          int* __restrict__ rows, int* __restrict__ cols,
                                                          S* __restrict__ vals, S* __restrict__ bforce,
                                                          unsigned short* __restrict__ block_mask) {
-  // The CTA's 128 records are classified (record_class) and handed to the
-  // threads in class order, so most warps run one path of
-  // contact_hessian_item instead of the union of their records' paths (a
+  // The CTA's 128 records are classified (their float32 part, kept in shared
+  // memory) and handed to the threads in class order, so most warps run one
+  // path of hessian_from instead of the union of their records' paths (a
   // record's outputs go to its own slots; only the order of the force
   // atomics changes).
   __shared__ int s_count[4], s_cursor[4], s_order[128];
+  __shared__ float4 s_pre[128];
   const int cnt = list_count<S>(L, n);
   const int base = blockIdx.x * 128;
   if (base >= cnt) return;  // the whole CTA
   const int tid = threadIdx.x, m = min(128, cnt - base);
   if (tid < 4) s_count[tid] = 0;
   __syncthreads();
-  const int cls = tid < m ? record_class<S, KIND>(x, xcs, L, base + tid) : -1;
-  if (cls >= 0) atomicAdd(&s_count[cls], 1);
+  int cls = -1;
+  if (tid < m) {
+    const int i = base + tid;
+    const int4 id = __ldg(reinterpret_cast<const int4*>(L.a1a2b1b2) + i);
+    const S l0 = static_cast<const S*>(L.l0)[i];
+    const v3<S> xs[4] = {ldx(x, id.x), ldx(x, id.y), ldx(x, id.z), ldx(x, id.w)};
+    const Pre p = predicate<S, KIND>(xcs, id, l0, xs);
+    s_pre[tid] = pack(p);
+    cls = p.cls();
+    atomicAdd(&s_count[cls], 1);
+  }
   __syncthreads();
   if (tid == 0) {
     int run = 0;
@@ -51,12 +63,87 @@ __global__ void __launch_bounds__(128, 3) k_contact_hessian(const S* __restrict_
     }
   }
   __syncthreads();
-  if (cls >= 0) s_order[atomicAdd(&s_cursor[cls], 1)] = base + tid;
+  if (cls >= 0) s_order[atomicAdd(&s_cursor[cls], 1)] = tid;
   __syncthreads();
   if (tid >= m) return;
   // offset_dev: the records follow another list's min(count, offset) records
   const int off = offset_dev ? min(*offset_dev, offset) : offset;
-  contact_hessian_item<S, KIND>(x, xcs, L, s_order[tid], off, kappa, rows, cols, vals, bforce, block_mask);
+  const int t = s_order[tid];
+  hessian_from<S, KIND>(x, xcs, L, base + t, off, kappa, unpack(s_pre[t]), rows, cols, vals, bforce, block_mask);
+}
+
+// ---- class-sorted path: the records of the whole list are put in cost-class
+// order (most expensive first) before the Hessian kernel, so nearly every
+// warp runs one path.  Workspace: [class counts int[4] | cursors int[4] |
+// pad to 256 B | float4 pre[capacity] | int order[capacity]].
+template <class S, int KIND>
+__global__ void __launch_bounds__(256) k_classify(const S* __restrict__ x, const S* __restrict__ xcs, ipcb_contacts L,
+                                                  int n, float4* __restrict__ pre, int* __restrict__ counts) {
+  __shared__ int sc[4];
+  const int cnt = list_count<S>(L, n);
+  if ((int)(blockIdx.x * blockDim.x) >= cnt) return;  // the whole block
+  if (threadIdx.x < 4) sc[threadIdx.x] = 0;
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < cnt) {
+    const int4 id = __ldg(reinterpret_cast<const int4*>(L.a1a2b1b2) + i);
+    const S l0 = static_cast<const S*>(L.l0)[i];
+    const v3<S> xs[4] = {ldx(x, id.x), ldx(x, id.y), ldx(x, id.z), ldx(x, id.w)};
+    const Pre p = predicate<S, KIND>(xcs, id, l0, xs);
+    pre[i] = pack(p);
+    atomicAdd(&sc[p.cls()], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x < 4 && sc[threadIdx.x]) atomicAdd(counts + threadIdx.x, sc[threadIdx.x]);
+}
+
+template <class S>
+__global__ void __launch_bounds__(256) k_class_order(ipcb_contacts L, int n, const float4* __restrict__ pre,
+                                                     const int* __restrict__ counts, int* __restrict__ cursor,
+                                                     int* __restrict__ order) {
+  __shared__ int sc[4], sbase[4];
+  const int cnt = list_count<S>(L, n);
+  if ((int)(blockIdx.x * blockDim.x) >= cnt) return;
+  if (threadIdx.x < 4) sc[threadIdx.x] = 0;
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int cls = -1, local = 0;
+  if (i < cnt) {
+    cls = __float_as_int(pre[i].w) & 3;
+    local = atomicAdd(&sc[cls], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    // classes in the order 3, 2, 1, 0: the costliest records start first
+    const int k = threadIdx.x;
+    int start = 0;
+    for (int c = 3; c > k; --c) start += counts[c];
+    sbase[k] = sc[k] ? start + atomicAdd(cursor + k, sc[k]) : 0;
+  }
+  __syncthreads();
+  if (cls >= 0) order[sbase[cls] + local] = i;
+}
+
+template <class S, int KIND>
+__global__ void __launch_bounds__(128, 3) k_contact_hessian_sorted(const S* __restrict__ x,
+                                                                const S* __restrict__ xcs, ipcb_contacts L, int n,
+                                                                int offset, const int* __restrict__ offset_dev,
+                                                                double kappa, const float4* __restrict__ pre,
+                                                                const int* __restrict__ order,
+                                                                int* __restrict__ rows, int* __restrict__ cols,
+                                                                S* __restrict__ vals, S* __restrict__ bforce,
+                                                                unsigned short* __restrict__ block_mask) {
+  const int cnt = list_count<S>(L, n);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cnt) return;
+  const int i = __ldg(order + t);
+  const int off = offset_dev ? min(*offset_dev, offset) : offset;
+  hessian_from<S, KIND>(x, xcs, L, i, off, kappa, unpack(__ldg(pre + i)), rows, cols, vals, bforce, block_mask);
+}
+
+size_t sorted_workspace(int capacity) {
+  const size_t c = (size_t)(capacity < 1 ? 1 : capacity);
+  return 256 + ((c * 16 + 255) / 256) * 256 + c * 4;
 }
 
 template <class S, int KIND>
@@ -119,6 +206,35 @@ int launch_hessian(int kind, const ipcb_soup* soup, const ipcb_contacts* L, int 
 }
 
 template <class S>
+int launch_hessian_sorted(int kind, const ipcb_soup* soup, const ipcb_contacts* L, int n, int offset,
+                          const int* offset_dev, double kappa, int* rows, int* cols, void* vals, void* b,
+                          unsigned short* mask, void* ws, cudaStream_t st) {
+  int threads = n >= 0 ? n : L->capacity;
+  if (threads == 0) return IPCB_OK;
+  const size_t c = (size_t)(L->capacity < 1 ? 1 : L->capacity);
+  int* counts = (int*)ws;
+  int* cursor = counts + 4;
+  float4* pre = (float4*)((char*)ws + 256);
+  int* order = (int*)((char*)ws + 256 + ((c * 16 + 255) / 256) * 256);
+  cudaMemsetAsync(ws, 0, 8 * sizeof(int), st);
+  const S* x = (const S*)soup->x;
+  const S* xcs = (const S*)soup->xcs;
+  dim3 g256(div_up(threads, 256)), g128(div_up(threads, 128));
+  if (kind == 0) {
+    k_classify<S, 0><<<g256, 256, 0, st>>>(x, xcs, *L, n, pre, counts);
+    k_class_order<S><<<g256, 256, 0, st>>>(*L, n, pre, counts, cursor, order);
+    k_contact_hessian_sorted<S, 0><<<g128, 128, 0, st>>>(x, xcs, *L, n, offset, offset_dev, kappa, pre, order, rows,
+                                                         cols, (S*)vals, (S*)b, mask);
+  } else {
+    k_classify<S, 1><<<g256, 256, 0, st>>>(x, xcs, *L, n, pre, counts);
+    k_class_order<S><<<g256, 256, 0, st>>>(*L, n, pre, counts, cursor, order);
+    k_contact_hessian_sorted<S, 1><<<g128, 128, 0, st>>>(x, xcs, *L, n, offset, offset_dev, kappa, pre, order, rows,
+                                                         cols, (S*)vals, (S*)b, mask);
+  }
+  return check_launch("ipcb_contact_hessian_sorted");
+}
+
+template <class S>
 int launch_energy(int kind, const ipcb_soup* soup, const ipcb_contacts* L, int n, double kappa, double* e,
                   cudaStream_t st) {
   int threads = n >= 0 ? n : L->capacity;
@@ -153,6 +269,20 @@ int ipcb_contact_hessian_after(int kind, const ipcb_soup* soup, const ipcb_conta
                                   (cudaStream_t)s);
   return launch_hessian<float>(kind, soup, list, n, offset, offset_count, kappa, rows, cols, vals, b, block_mask,
                                (cudaStream_t)s);
+}
+
+size_t ipcb_contact_hessian_workspace(int capacity) { return sorted_workspace(capacity); }
+
+int ipcb_contact_hessian_sorted(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, int offset,
+                                const int* offset_count, double kappa, int* rows, int* cols, void* vals, void* b,
+                                unsigned short* block_mask, void* ws, size_t ws_bytes, ipcb_stream s) {
+  if (!soup || !list || !rows || !cols || !vals || !b || (kind != 0 && kind != 1) || offset < 0) return IPCB_E_ARG;
+  if (n > list->capacity || !ws || ws_bytes < sorted_workspace(list->capacity)) return IPCB_E_ARG;
+  if (soup->fp64)
+    return launch_hessian_sorted<double>(kind, soup, list, n, offset, offset_count, kappa, rows, cols, vals, b,
+                                         block_mask, ws, (cudaStream_t)s);
+  return launch_hessian_sorted<float>(kind, soup, list, n, offset, offset_count, kappa, rows, cols, vals, b,
+                                      block_mask, ws, (cudaStream_t)s);
 }
 
 int ipcb_contact_energy(int kind, const ipcb_soup* soup, const ipcb_contacts* list, int n, double kappa,

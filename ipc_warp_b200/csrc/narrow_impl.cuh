@@ -292,9 +292,8 @@ IPCB_D int list_count(const ipcb_contacts& L, int n) {
 // Feature selection for an EE record (dynamic_contacts.py:49-108).  Uses the
 // float32 (s, t) of the segment closest points.
 template <class S>
-IPCB_D void ee_dispatch(Feature& f, const v3<S>* xs, const d3* xd, S parallel_eps) {
-  CPEE dab = closest_point_edge_edge(to_f(xs[0]), to_f(xs[1]), to_f(xs[2]), to_f(xs[3]), 1.0e-6f);
-  S s = S(dab.s), t = S(dab.t);
+IPCB_D void ee_dispatch(Feature& f, const d3* xd, float ds, float dt, bool near_par) {
+  S s = S(ds), t = S(dt);
   const S feps = S(1.0e-6), one = S(1.0), hi = S(1.0) - S(1.0e-6);
   bool sb = s <= feps || s >= hi;
   bool tb = t <= feps || t >= hi;
@@ -310,9 +309,7 @@ IPCB_D void ee_dispatch(Feature& f, const v3<S>* xs, const d3* xd, S parallel_ep
     feature_pe(f, xd, t >= hi ? 3 : 2, 0, 1);
     return;
   }
-  v3<S> ea = esub(xs[1], xs[0]), eb = esub(xs[3], xs[2]);
-  v3<S> cr = ecross(ea, eb);
-  if (parallel_eps > S(0) && edot(cr, cr) < parallel_eps) {
+  if (near_par) {
     S ds0 = s, ds1 = xsub(one, s), dt0 = t, dt1 = xsub(one, t);
     S mn = tmin(tmin(ds0, ds1), tmin(dt0, dt1));
     if (mn == ds0) feature_pe(f, xd, 0, 2, 3);
@@ -324,10 +321,8 @@ IPCB_D void ee_dispatch(Feature& f, const v3<S>* xs, const d3* xd, S parallel_ep
   feature_ee(f, xd);
 }
 
-// dynamic_contacts.py:111-125
-IPCB_D int pt_dispatch(Feature& f, const f3* xf, const d3* xd) {
-  CPT cp = closest_point_triangle(xf[0], xf[1], xf[2], xf[3]);
-  int t = cp.type;
+// dynamic_contacts.py:111-125; t: the closest-point region type of the record
+IPCB_D int pt_dispatch(Feature& f, int t, const d3* xd) {
   if (t <= 2) feature_pp(f, xd, 0, t + 1);
   else if (t == 3) feature_pe(f, xd, 0, 1, 2);
   else if (t == 4) feature_pe(f, xd, 0, 1, 3);
@@ -436,70 +431,84 @@ IPCB_D void mollifier(const d3* xd, double eps_x, double& mv, double (&gm)[12]) 
   gm[9] = dm * dxb.x; gm[10] = dm * dxb.y; gm[11] = dm * dxb.z;
 }
 
-// Cost class of a record, for giving the records that take the same path
-// through contact_hessian_item to the same warps: 0 inactive (dist >= l0:
-// zero blocks), 1 no eigen-solve (point-point feature, or near-parallel EE
-// edges: mollified gradient term only), 2 the 3x3 restriction (point-edge),
-// 3 the 5x5 restriction (edge-edge, point-triangle).  Mirrors the gate and
-// the feature dispatch of contact_hessian_item.
+// The float32 part of a record (the reference's wp.vec3 casts, F9): the
+// closest distance, the segment parameters (EE) or region type (PT), the
+// near-parallel test of the EE mollifier, and the record's cost class, for
+// giving records that take the same path through the Hessian to the same
+// warps: 0 inactive (dist >= l0: zero blocks), 1 no eigen-solve (point-point
+// feature, or near-parallel EE edges: mollified gradient term only), 2 the
+// 3x3 restriction (point-edge), 3 the 5x5 restriction (edge-edge,
+// point-triangle).  Packed in a float4: (dist, s, t, flags) with flags bits
+// 0-1 the class, bit 2 near-parallel, bits 3-5 the PT region type.
+struct Pre {
+  float d, s, t;
+  int flags;
+  IPCB_D int cls() const { return flags & 3; }
+  IPCB_D bool near_par() const { return (flags >> 2) & 1; }
+  IPCB_D int type() const { return (flags >> 3) & 7; }
+};
+IPCB_D float4 pack(const Pre& p) { return make_float4(p.d, p.s, p.t, __int_as_float(p.flags)); }
+IPCB_D Pre unpack(float4 v) { return Pre{v.x, v.y, v.z, __float_as_int(v.w)}; }
+
+template <class S, int KIND>
+IPCB_D Pre predicate(const S* __restrict__ xcs, int4 id, S l0, const v3<S>* xs) {
+  const f3 xf[4] = {to_f(xs[0]), to_f(xs[1]), to_f(xs[2]), to_f(xs[3])};
+  Pre p{0.f, 0.f, 0.f, 0};
+  if (KIND == 0) {
+    const CPEE d = closest_point_edge_edge(xf[0], xf[1], xf[2], xf[3], 1.0e-6f);
+    p.d = d.d;
+    p.s = d.s;
+    p.t = d.t;
+    if (!(S(d.d) < l0)) return p;
+    const S eps_x = ee_eps_x(xcs, id);
+    const v3<S> ea = esub(xs[1], xs[0]), eb = esub(xs[3], xs[2]);
+    const v3<S> cr = ecross(ea, eb);
+    const bool near_par = eps_x > S(0) && edot(cr, cr) < eps_x;
+    const S s = S(d.s), t = S(d.t), feps = S(1.0e-6), hi = S(1.0) - S(1.0e-6);
+    const bool sb = s <= feps || s >= hi, tb = t <= feps || t >= hi;
+    const int cls = near_par ? 1 : (sb && tb ? 1 : (sb || tb ? 2 : 3));
+    p.flags = cls | (near_par ? 4 : 0);
+  } else {
+    const CPT cp = closest_point_triangle(xf[0], xf[1], xf[2], xf[3]);
+    p.d = cp.d;
+    p.flags = cp.type << 3;
+    if (!(S(cp.d) < l0)) return p;
+    p.flags |= cp.type <= 2 ? 1 : (cp.type <= 5 ? 2 : 3);
+  }
+  return p;
+}
+
 template <class S, int KIND>
 IPCB_D int record_class(const S* __restrict__ x, const S* __restrict__ xcs, const ipcb_contacts& L, int i) {
   const int4 id = __ldg(reinterpret_cast<const int4*>(L.a1a2b1b2) + i);
   const S l0 = static_cast<const S*>(L.l0)[i];
   const v3<S> xs[4] = {ldx(x, id.x), ldx(x, id.y), ldx(x, id.z), ldx(x, id.w)};
-  const f3 xf[4] = {to_f(xs[0]), to_f(xs[1]), to_f(xs[2]), to_f(xs[3])};
-  if (KIND == 0) {
-    const CPEE d = closest_point_edge_edge(xf[0], xf[1], xf[2], xf[3], 1.0e-6f);
-    if (!(S(d.d) < l0)) return 0;
-    const S eps_x = ee_eps_x(xcs, id);
-    const v3<S> ea = esub(xs[1], xs[0]), eb = esub(xs[3], xs[2]);
-    const v3<S> cr = ecross(ea, eb);
-    if (eps_x > S(0) && edot(cr, cr) < eps_x) return 1;
-    const S s = S(d.s), t = S(d.t), feps = S(1.0e-6), hi = S(1.0) - S(1.0e-6);
-    const bool sb = s <= feps || s >= hi, tb = t <= feps || t >= hi;
-    return sb && tb ? 1 : (sb || tb ? 2 : 3);
-  } else {
-    const CPT cp = closest_point_triangle(xf[0], xf[1], xf[2], xf[3]);
-    if (!(S(cp.d) < l0)) return 0;
-    return cp.type <= 2 ? 1 : (cp.type <= 5 ? 2 : 3);
-  }
+  return predicate<S, KIND>(xcs, id, l0, xs).cls();
 }
 
-// One record of contact_hessian_ee / _pt: 16 blocks at (offset + i)*16,
-// force into bforce, block mask.  T: arithmetic type of the eigen-solve and
-// of H (float for S=float).
+// One record of contact_hessian_ee / _pt from its float32 part p: 16 blocks
+// at (offset + i)*16, force into bforce, block mask.  T: arithmetic type of
+// the eigen-solve and of H (float for S=float).
 template <class S, int KIND>
-IPCB_D void contact_hessian_item(const S* __restrict__ x, const S* __restrict__ xcs, const ipcb_contacts& L, int i,
-                                 int offset, double kappa, int* __restrict__ rows, int* __restrict__ cols,
-                                 S* __restrict__ vals, S* __restrict__ bforce,
-                                 unsigned short* __restrict__ block_mask) {
+IPCB_D void hessian_from(const S* __restrict__ x, const S* __restrict__ xcs, const ipcb_contacts& L, int i,
+                         int offset, double kappa, const Pre& p, int* __restrict__ rows, int* __restrict__ cols,
+                         S* __restrict__ vals, S* __restrict__ bforce, unsigned short* __restrict__ block_mask) {
   typedef S T;
   long long base = (long long)(offset + i) * 16;
-  int4 id = __ldg(reinterpret_cast<const int4*>(L.a1a2b1b2) + i);
-  S l0 = static_cast<const S*>(L.l0)[i];
-  v3<S> xs[4] = {ldx(x, id.x), ldx(x, id.y), ldx(x, id.z), ldx(x, id.w)};
-  f3 xf[4] = {to_f(xs[0]), to_f(xs[1]), to_f(xs[2]), to_f(xs[3])};
-  d3 xd[4] = {to_d(xs[0]), to_d(xs[1]), to_d(xs[2]), to_d(xs[3])};
-  float dist;
-  if (KIND == 0) dist = closest_point_edge_edge(xf[0], xf[1], xf[2], xf[3], 1.0e-6f).d;
-  else dist = closest_point_triangle(xf[0], xf[1], xf[2], xf[3]).d;
-  if (!(S(dist) < l0)) {
+  if (p.cls() == 0) {
     write_zero<S>(rows, cols, vals, base);
     if (block_mask) block_mask[offset + i] = 0;
     return;
   }
+  int4 id = __ldg(reinterpret_cast<const int4*>(L.a1a2b1b2) + i);
+  S l0 = static_cast<const S*>(L.l0)[i];
+  v3<S> xs[4] = {ldx(x, id.x), ldx(x, id.y), ldx(x, id.z), ldx(x, id.w)};
+  d3 xd[4] = {to_d(xs[0]), to_d(xs[1]), to_d(xs[2]), to_d(xs[3])};
+  const float dist = p.d;
   Feature f;
-  bool near_par = false;
-  S eps_x = S(0);
-  if (KIND == 0) {
-    eps_x = ee_eps_x(xcs, id);
-    v3<S> ea = esub(xs[1], xs[0]), eb = esub(xs[3], xs[2]);
-    v3<S> cr = ecross(ea, eb);
-    near_par = eps_x > S(0) && edot(cr, cr) < eps_x;
-    ee_dispatch<S>(f, xs, xd, eps_x);
-  } else {
-    pt_dispatch(f, xf, xd);
-  }
+  const bool near_par = KIND == 0 && p.near_par();
+  if (KIND == 0) ee_dispatch<S>(f, xd, p.s, p.t, near_par);
+  else pt_dispatch(f, p.type(), xd);
   double d2 = (double)dist * (double)dist, d02 = (double)l0 * (double)l0;
   Barrier br = barrier(d2, d02, kappa);
   T h[kMaxH][12], w[kMaxH];
@@ -518,7 +527,7 @@ IPCB_D void contact_hessian_item(const S* __restrict__ x, const S* __restrict__ 
   int nh = 1;
   if (near_par) {
     double mv, gm[12];
-    mollifier(xd, (double)eps_x, mv, gm);
+    mollifier(xd, (double)ee_eps_x(xcs, id), mv, gm);
     w[0] = T(mv * br.d2b);
 #pragma unroll
     for (int k = 0; k < 12; ++k) fc[k] = -(mv * br.db * g[k] + br.b * gm[k]);
@@ -532,6 +541,19 @@ IPCB_D void contact_hessian_item(const S* __restrict__ x, const S* __restrict__ 
   unsigned mask = write_blocks<S, T>(id, rows, cols, vals, base, h, w, nh);
   if (block_mask) block_mask[offset + i] = (unsigned short)mask;
   add_force<S>(bforce, id, fc);
+}
+
+// One record of contact_hessian_ee / _pt: the float32 part, then the rest.
+template <class S, int KIND>
+IPCB_D void contact_hessian_item(const S* __restrict__ x, const S* __restrict__ xcs, const ipcb_contacts& L, int i,
+                                 int offset, double kappa, int* __restrict__ rows, int* __restrict__ cols,
+                                 S* __restrict__ vals, S* __restrict__ bforce,
+                                 unsigned short* __restrict__ block_mask) {
+  const int4 id = __ldg(reinterpret_cast<const int4*>(L.a1a2b1b2) + i);
+  const S l0 = static_cast<const S*>(L.l0)[i];
+  const v3<S> xs[4] = {ldx(x, id.x), ldx(x, id.y), ldx(x, id.z), ldx(x, id.w)};
+  const Pre p = predicate<S, KIND>(xcs, id, l0, xs);
+  hessian_from<S, KIND>(x, xcs, L, i, offset, kappa, p, rows, cols, vals, bforce, block_mask);
 }
 
 }  // namespace

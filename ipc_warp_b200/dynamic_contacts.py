@@ -26,32 +26,46 @@ def _count(contacts: Contacts, n):
     return int(contacts.cnt.item()) if n is None else int(n)
 
 
+def hessian_workspace(contacts: Contacts, ws: torch.Tensor | None) -> torch.Tensor:
+    """Device workspace of the class-sorted narrow phase for ``contacts``
+    (reused when ``ws`` is large enough)."""
+    need = N.size("ipcb_contact_hessian_workspace", contacts.capacity)
+    if ws is None or ws.numel() < need:
+        ws = torch.empty(need, dtype=torch.uint8, device=contacts.device)
+    return ws
+
+
+def _hessian(kind, soup, contacts, triplets, b, kappa, n, offset, offset_count, ws):
+    args = (kind, ctypes.byref(soup.c_struct()), ctypes.byref(contacts.c_struct()), n, int(offset))
+    tail = (float(kappa), N.ptr(triplets.rows), N.ptr(triplets.cols), N.ptr(triplets.vals), N.ptr(b),
+            N.ptr(triplets.mask))
+    if ws is None:
+        N.call("ipcb_contact_hessian_after", *args, offset_count, *tail, N.stream_handle())
+    else:
+        N.call("ipcb_contact_hessian_sorted", *args, offset_count, *tail, N.ptr(ws), ws.numel(), N.stream_handle())
+
+
 def contact_hessian_ee(states, soup: Soup, contacts: Contacts, triplets: Triplets, b: torch.Tensor, kappa: float,
-                       n: int | None = None):
-    """dynamic_contacts.py:151-207 (EE with mollifier)."""
-    n = min(_count(contacts, n), contacts.capacity)
-    N.call("ipcb_contact_hessian", 0, ctypes.byref(soup.c_struct()), ctypes.byref(contacts.c_struct()), n, 0,
-           float(kappa), N.ptr(triplets.rows), N.ptr(triplets.cols), N.ptr(triplets.vals), N.ptr(b),
-           N.ptr(triplets.mask), N.stream_handle())
+                       n: int | None = None, ws: torch.Tensor | None = None):
+    """dynamic_contacts.py:151-207 (EE with mollifier).  With ``ws``
+    (hessian_workspace) the records run in cost-class order."""
+    n = n if n is not None and n < 0 else min(_count(contacts, n), contacts.capacity)
+    _hessian(0, soup, contacts, triplets, b, kappa, n, 0, None, ws)
 
 
 def contact_hessian_pt(states, soup: Soup, contacts: Contacts, triplets: Triplets, b: torch.Tensor, offset: int,
-                       kappa: float, n: int | None = None):
+                       kappa: float, n: int | None = None, ws: torch.Tensor | None = None):
     """dynamic_contacts.py:209-246 (PT, records at offset)."""
     n = min(_count(contacts, n), contacts.capacity)
-    N.call("ipcb_contact_hessian", 1, ctypes.byref(soup.c_struct()), ctypes.byref(contacts.c_struct()), n,
-           int(offset), float(kappa), N.ptr(triplets.rows), N.ptr(triplets.cols), N.ptr(triplets.vals), N.ptr(b),
-           N.ptr(triplets.mask), N.stream_handle())
+    _hessian(1, soup, contacts, triplets, b, kappa, n, offset, None, ws)
 
 
 def contact_hessian_pt_after(states, soup: Soup, contacts: Contacts, triplets: Triplets, b: torch.Tensor,
-                             ee: Contacts, kappa: float):
+                             ee: Contacts, kappa: float, ws: torch.Tensor | None = None):
     """contact_hessian_pt with both counts read on the device: the PT records
     go right after the EE list's min(count, capacity) records, as
     contact_hessian_pt(..., offset=n_ee) puts them, without a host read."""
-    N.call("ipcb_contact_hessian_after", 1, ctypes.byref(soup.c_struct()), ctypes.byref(contacts.c_struct()), -1,
-           ee.capacity, N.ptr(ee.cnt), float(kappa), N.ptr(triplets.rows), N.ptr(triplets.cols),
-           N.ptr(triplets.vals), N.ptr(b), N.ptr(triplets.mask), N.stream_handle())
+    _hessian(1, soup, contacts, triplets, b, kappa, -1, ee.capacity, N.ptr(ee.cnt), ws)
 
 
 def contact_energy_ee(states, soup: Soup, contacts: Contacts, e: torch.Tensor, kappa: float, n: int | None = None):
@@ -96,9 +110,12 @@ class ContactBarrierMixin(ContactSolverBase):
             states = getattr(self, "states", None)
             kappa = float(self.contact_stiffness)
             if n_ee:
-                contact_hessian_ee(states, self.soup, self.contacts_new, t, self.b, kappa, n=n_ee)
+                self._ws_ee = hessian_workspace(self.contacts_new, getattr(self, "_ws_ee", None))
+                contact_hessian_ee(states, self.soup, self.contacts_new, t, self.b, kappa, n=n_ee, ws=self._ws_ee)
             if n_pt:
-                contact_hessian_pt(states, self.soup, self.contacts_pt, t, self.b, n_ee, kappa, n=n_pt)
+                self._ws_pt = hessian_workspace(self.contacts_pt, getattr(self, "_ws_pt", None))
+                contact_hessian_pt(states, self.soup, self.contacts_pt, t, self.b, n_ee, kappa, n=n_pt,
+                                   ws=self._ws_pt)
             if not build_bsr:
                 return None
             prev = getattr(self, "collision_hessian", None)

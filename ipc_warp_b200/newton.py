@@ -28,7 +28,7 @@ from . import contact as contact_mod
 from .autotune import Autotuner, bucket
 from .bsr import BsrMatrix, Triplets, bsr_from_triplets, bsr_mv, contact_bsr
 from .contact import Soup
-from .dynamic_contacts import ContactBarrierMixin
+from .dynamic_contacts import ContactBarrierMixin, contact_hessian_ee, contact_hessian_pt, hessian_workspace
 
 MATERIALS = {"snh": 0, "neo_hookean": 1, "nh": 1, "stvk": 2}
 
@@ -380,14 +380,14 @@ class FEMContactSolver(ContactBarrierMixin):
         if cfg[0] == "separate":
             n_ee, n_pt = self.n_contacts, self.n_contacts_pt
             t = self.collision_triplets
+            kappa = float(self.contact_stiffness)
             if n_ee:
-                N.call("ipcb_contact_hessian", 0, ctypes.byref(self.soup.c_struct()),
-                       ctypes.byref(self.contacts_new.c_struct()), n_ee, 0, float(self.contact_stiffness),
-                       N.ptr(t.rows), N.ptr(t.cols), N.ptr(t.vals), N.ptr(self.b), N.ptr(t.mask), s)
+                self._ws_ee = hessian_workspace(self.contacts_new, getattr(self, "_ws_ee", None))
+                contact_hessian_ee(None, self.soup, self.contacts_new, t, self.b, kappa, n=n_ee, ws=self._ws_ee)
             if n_pt:
-                N.call("ipcb_contact_hessian", 1, ctypes.byref(self.soup.c_struct()),
-                       ctypes.byref(self.contacts_pt.c_struct()), n_pt, n_ee, float(self.contact_stiffness),
-                       N.ptr(t.rows), N.ptr(t.cols), N.ptr(t.vals), N.ptr(self.b), N.ptr(t.mask), s)
+                self._ws_pt = hessian_workspace(self.contacts_pt, getattr(self, "_ws_pt", None))
+                contact_hessian_pt(None, self.soup, self.contacts_pt, t, self.b, n_ee, kappa, n=n_pt,
+                                   ws=self._ws_pt)
             N.call("ipcb_tet_hessian", self.material, int(self.dtype == torch.float64), N.ptr(self.states.x),
                    N.ptr(self.tets), self.n_tets, N.ptr(self.Bm), N.ptr(self.W), self.mu, self.lam, None, None,
                    N.ptr(self._static["tet_vals"]), N.ptr(self.b), s)

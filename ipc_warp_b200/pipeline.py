@@ -24,7 +24,7 @@ from . import contact
 from .contact import Soup
 from .bsr import Triplets, contact_bsr
 from .dynamic_contacts import (ContactBarrierMixin, contact_energy_ee, contact_energy_pt, contact_hessian_ee,
-                               contact_hessian_pt_after)
+                               contact_hessian_pt_after, hessian_workspace)
 
 
 @dataclass
@@ -116,9 +116,11 @@ class ContactPipeline(ContactBarrierMixin):
 
     def _graph_key(self):
         ee, pt, t, H = self.contacts_new, self.contacts_pt, self.collision_triplets, self.collision_hessian
+        ws = tuple(None if getattr(self, a, None) is None else getattr(self, a).data_ptr()
+                   for a in ("_ws_ee", "_ws_pt"))
         return (ee.a1a2b1b2.data_ptr(), ee.capacity, pt.a1a2b1b2.data_ptr(), pt.capacity,
                 None if t is None else t.rows.data_ptr(), None if H is None else H.values.data_ptr(),
-                None if H is None else H._ws.data_ptr(), getattr(self, "bvh_rebuild_interval", 0))
+                None if H is None else H._ws.data_ptr(), ws, getattr(self, "bvh_rebuild_interval", 0))
 
     def _capture(self, key):
         if key[-1]:  # periodic rebuilds alternate with refits: not one fixed sequence
@@ -151,6 +153,8 @@ class ContactPipeline(ContactBarrierMixin):
         t = self.collision_triplets
         if t is None or t.rows.shape[0] < 16 * cap:
             t = self.collision_triplets = Triplets.zeros(16 * cap, self.soup.xcs.dtype, self.device)
+        self._ws_ee = hessian_workspace(ee, getattr(self, "_ws_ee", None))
+        self._ws_pt = hessian_workspace(pt, getattr(self, "_ws_pt", None))
         self.compute_V(ret=False)
         self._pack()
         self.b.zero_()
@@ -186,10 +190,10 @@ class ContactPipeline(ContactBarrierMixin):
             N.call("ipcb_point_triangle_toi", soup, N.ptr(self.ccd_x1), ctypes.byref(self.ccd_triangle_bvh.c), pad,
                    excl, N.ptr(self.ccd_toi), N.ptr(self._status), N.ptr(self._toi_ws_pt),
                    self._toi_ws_pt.numel(), s2)
-        contact_hessian_ee(self.states, self.soup, ee, t, self.b, kappa, n=-1)
+        contact_hessian_ee(self.states, self.soup, ee, t, self.b, kappa, n=-1, ws=self._ws_ee)
         with torch.cuda.stream(side):
             side.wait_event(self._ee_done)  # the PT records follow the EE count
-            contact_hessian_pt_after(self.states, self.soup, pt, t, self.b, ee, kappa)
+            contact_hessian_pt_after(self.states, self.soup, pt, t, self.b, ee, kappa, ws=self._ws_pt)
         main.wait_stream(side)
         H, _ = contact_bsr(ee, None, pt, None, self.soup.n_verts, t, out=self.collision_hessian,
                            status=self._bsr_status, read_status=False)
@@ -228,8 +232,10 @@ class ContactPipeline(ContactBarrierMixin):
             t = self.collision_triplets = Triplets.zeros(16 * cap, self.soup.xcs.dtype, self.device)
         kappa = float(self.contact_stiffness)
         self.b.zero_()
-        contact_hessian_ee(self.states, self.soup, ee, t, self.b, kappa, n=-1)
-        contact_hessian_pt_after(self.states, self.soup, pt, t, self.b, ee, kappa)
+        self._ws_ee = hessian_workspace(ee, getattr(self, "_ws_ee", None))
+        self._ws_pt = hessian_workspace(pt, getattr(self, "_ws_pt", None))
+        contact_hessian_ee(self.states, self.soup, ee, t, self.b, kappa, n=-1, ws=self._ws_ee)
+        contact_hessian_pt_after(self.states, self.soup, pt, t, self.b, ee, kappa, ws=self._ws_pt)
         H, _ = contact_bsr(ee, None, pt, None, self.soup.n_verts, t, out=self.collision_hessian,
                            status=self._bsr_status, read_status=False)
         self.collision_hessian = H

@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <vector>
 #include <omp.h>
 
@@ -1371,6 +1372,65 @@ int ora_contact_bsr(int nv, int n, const int* idx, const double* hess, int* offs
     }
   }
   return nnz;
+}
+
+// Intersection check (the reference's trajectories must stay intersection
+// free): every (edge, triangle) pair without a shared vertex whose segment
+// strictly crosses the triangle, by orientation signs in double (plain IEEE
+// operations in a fixed order; the product evaluates the same expressions).
+// The sorted-grid pruning over tight boxes is conservative, so the count is
+// that of all E x T pairs.  Returns the count; the first cap pairs go to out.
+static double ora_orient(const double* a, const double* b, const double* c, const double* d) {
+  double u[3], v[3], w[3];
+  for (int k = 0; k < 3; ++k) {
+    u[k] = b[k] - a[k];
+    v[k] = c[k] - a[k];
+    w[k] = d[k] - a[k];
+  }
+  const double cx = v[1] * w[2] - v[2] * w[1], cy = v[2] * w[0] - v[0] * w[2], cz = v[0] * w[1] - v[1] * w[0];
+  return (u[0] * cx + u[1] * cy) + u[2] * cz;
+}
+
+int ora_edge_triangle_crossings(int nv, const double* x, int ne, const int* edges, int nt, const int* tris, int* out,
+                                int cap) {
+  (void)nv;
+  std::vector<Box> eb(ne), tb(nt);
+  for (int e = 0; e < ne; ++e)
+    for (int k = 0; k < 3; ++k) {
+      const double a = x[3 * edges[2 * e] + k], b = x[3 * edges[2 * e + 1] + k];
+      eb[e].lo[k] = std::nextafter((float)std::min(a, b), -3.4e38f);
+      eb[e].hi[k] = std::nextafter((float)std::max(a, b), 3.4e38f);
+    }
+  for (int t = 0; t < nt; ++t)
+    for (int k = 0; k < 3; ++k) {
+      double mn = 1e300, mx = -1e300;
+      for (int v = 0; v < 3; ++v) {
+        mn = std::min(mn, x[3 * tris[3 * t + v] + k]);
+        mx = std::max(mx, x[3 * tris[3 * t + v] + k]);
+      }
+      tb[t].lo[k] = std::nextafter((float)mn, -3.4e38f);
+      tb[t].hi[k] = std::nextafter((float)mx, 3.4e38f);
+    }
+  std::vector<std::pair<int, int>> found;
+  std::mutex mu;
+  sweep(eb, tb, [&](int e, int t) {
+    const int p = edges[2 * e], q = edges[2 * e + 1];
+    const int a = tris[3 * t], b = tris[3 * t + 1], c = tris[3 * t + 2];
+    if (a == p || a == q || b == p || b == q || c == p || c == q) return;
+    const double *P = x + 3 * p, *Q = x + 3 * q, *A = x + 3 * a, *B = x + 3 * b, *C = x + 3 * c;
+    const double o1 = ora_orient(A, B, C, P), o2 = ora_orient(A, B, C, Q);
+    if (!((o1 > 0.0 && o2 < 0.0) || (o1 < 0.0 && o2 > 0.0))) return;
+    const double s1 = ora_orient(P, Q, A, B), s2 = ora_orient(P, Q, B, C), s3 = ora_orient(P, Q, C, A);
+    if (!((s1 > 0.0 && s2 > 0.0 && s3 > 0.0) || (s1 < 0.0 && s2 < 0.0 && s3 < 0.0))) return;
+    std::lock_guard<std::mutex> lock(mu);
+    found.push_back({e, t});
+  });
+  std::sort(found.begin(), found.end());
+  for (int k = 0; k < (int)found.size() && k < cap; ++k) {
+    out[2 * k] = found[k].first;
+    out[2 * k + 1] = found[k].second;
+  }
+  return (int)found.size();
 }
 
 }  // extern "C"

@@ -183,3 +183,14 @@ def contact_bsr(nv, idx, hess):
     vals = np.zeros((max(cap, 1), 3, 3))
     nnz = lib().ora_contact_bsr(int(nv), n, _p(idx), _p(hess), _p(offsets), _p(cols), _p(vals), cap)
     return offsets, cols[:nnz], vals[:nnz]
+
+
+def edge_triangle_crossings(x, edges, triangles, cap=1 << 16):
+    """(count, pairs (m, 2) sorted) of surface edges strictly crossing
+    surface triangles without a shared vertex (the intersection check)."""
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+    edges, triangles = _i32(edges).reshape(-1), _i32(triangles).reshape(-1)
+    out = np.zeros((max(cap, 1), 2), np.int32)
+    n = lib().ora_edge_triangle_crossings(x.size // 3, _p(x), edges.size // 2, _p(edges), triangles.size // 3,
+                                          _p(triangles), _p(out), cap)
+    return n, out[:min(n, cap)]

@@ -89,3 +89,45 @@ def test_hessian_is_psd_and_symmetric(cuda):
             continue
         assert np.allclose(H, H.T, rtol=0, atol=1e-12 * np.abs(H).max())
         assert np.linalg.eigvalsh(H).min() >= -1e-9 * np.abs(H).max()
+
+
+@pytest.mark.parametrize("idx", range(4))
+@pytest.mark.parametrize("fp64", [False, True])
+def test_class_sorted_path_equals_per_cta_path(cuda, idx, fp64):
+    """ipcb_contact_hessian_sorted (records in cost-class order over the whole
+    list) writes the same blocks, rows, columns and masks as the per-CTA
+    ordering, bit for bit; the force differs only by the order of its
+    atomics; its order array is a permutation of the records."""
+    from ipc_warp_b200 import _native as N
+    from ipc_warp_b200.bsr import Triplets
+    from ipc_warp_b200.dynamic_contacts import contact_hessian_ee, contact_hessian_pt, hessian_workspace
+
+    sc = small_scenes()[idx]
+    dtype = torch.float64 if fp64 else torch.float32
+    s = make_solver(sc, dtype)
+    s.detect_collision()
+    n_ee, n_pt = s.n_contacts, s.n_contacts_pt
+    out = []
+    for sorted_path in (False, True):
+        t = Triplets.zeros((n_ee + n_pt) * 16, dtype, s.device)
+        b = torch.zeros_like(s.soup.x_transformed)
+        ws_ee = hessian_workspace(s.contacts_new, None) if sorted_path else None
+        ws_pt = hessian_workspace(s.contacts_pt, None) if sorted_path else None
+        contact_hessian_ee(None, s.soup, s.contacts_new, t, b, 1e4, n=n_ee, ws=ws_ee)
+        contact_hessian_pt(None, s.soup, s.contacts_pt, t, b, n_ee, 1e4, n=n_pt, ws=ws_pt)
+        torch.cuda.synchronize()
+        out.append((t, b))
+        if sorted_path:
+            for ws, n, L in ((ws_ee, n_ee, s.contacts_new), (ws_pt, n_pt, s.contacts_pt)):
+                cap = L.capacity
+                off = 256 + ((cap * 16 + 255) // 256) * 256
+                order = ws[off:off + 4 * n].view(torch.int32).cpu().numpy()
+                assert np.array_equal(np.sort(order), np.arange(n))
+                counts = ws[:16].view(torch.int32).cpu().numpy()
+                assert counts.sum() == n
+    (ta, ba), (tb, bb) = out
+    assert torch.equal(ta.rows, tb.rows) and torch.equal(ta.cols, tb.cols)
+    assert torch.equal(ta.vals, tb.vals) and torch.equal(ta.mask, tb.mask)
+    tol = TOL[fp64]
+    assert rel_err(bb.double().cpu().numpy(), ba.double().cpu().numpy()) <= tol
+    assert N.size("ipcb_contact_hessian_workspace", 1000) >= 256 + 1000 * 20

@@ -201,3 +201,40 @@ def test_contact_bsr_equals_scipy_assembly():
     assert abs(got - ref).max() <= 1e-13 * abs(ref).max()
     for r in range(nv):
         assert np.all(np.diff(cols[off[r]:off[r + 1]]) > 0)
+
+
+def _crossings_brute(x, edges, tris):
+    """All E x T pairs, numpy, the same orientation expressions."""
+    E = edges.reshape(-1, 2)
+    T = tris.reshape(-1, 3)
+
+    def orient(a, b, c, d):
+        u, v, w = b - a, c - a, d - a
+        cx = v[..., 1] * w[..., 2] - v[..., 2] * w[..., 1]
+        cy = v[..., 2] * w[..., 0] - v[..., 0] * w[..., 2]
+        cz = v[..., 0] * w[..., 1] - v[..., 1] * w[..., 0]
+        return (u[..., 0] * cx + u[..., 1] * cy) + u[..., 2] * cz
+
+    P, Q = x[E[:, 0]][:, None], x[E[:, 1]][:, None]
+    A, B, C = x[T[:, 0]][None], x[T[:, 1]][None], x[T[:, 2]][None]
+    o1, o2 = orient(A, B, C, P), orient(A, B, C, Q)
+    s1, s2, s3 = orient(P, Q, A, B), orient(P, Q, B, C), orient(P, Q, C, A)
+    hit = (((o1 > 0) & (o2 < 0)) | ((o1 < 0) & (o2 > 0))) & (((s1 > 0) & (s2 > 0) & (s3 > 0)) |
+                                                         ((s1 < 0) & (s2 < 0) & (s3 < 0)))
+    shared = (E[:, None, :, None] == T[None, :, None, :]).any(axis=(2, 3))
+    hit &= ~shared
+    return np.argwhere(hit).astype(np.int32)
+
+
+def test_edge_triangle_crossings_match_brute_force():
+    from ipc_warp_b200 import scenes
+
+    sc = scenes.two_cubes(n=3, gap=1e-3, angle_deg=20.0, seed=1)
+    n, pairs = po.edge_triangle_crossings(sc.x, sc.edges, sc.triangles)
+    assert n == 0 and len(_crossings_brute(sc.x, sc.edges, sc.triangles)) == 0
+    x = sc.x.copy()
+    x[sc.body == 1, 1] -= 0.15  # the upper cube sinks into the lower one
+    ref = _crossings_brute(x, sc.edges, sc.triangles)
+    n, pairs = po.edge_triangle_crossings(x, sc.edges, sc.triangles)
+    assert n == len(ref) > 20
+    assert np.array_equal(pairs, ref[np.lexsort(ref.T[::-1])])
