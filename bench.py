@@ -46,13 +46,14 @@ WORKLOADS = {
 HEADLINE = "screw_nut"
 
 ROD_SIDE = 4  # rods per side of the bundle; --rods N shrinks the workload for profiler captures
+TURNS = 12  # thread turns of the screw and nut; --turns N shrinks it for profiler captures
 
 
 def scene(name: str = HEADLINE):
     from ipc_warp_b200 import scenes
 
     if name == "screw_nut":
-        return scenes.screw_and_nut()
+        return scenes.screw_and_nut(turns=TURNS)
     return scenes.rod_bundle(n_rods_side=ROD_SIDE, cells=(4, 4, 256), width=0.1, gap_over_dhat=0.5,
                              jitter_over_dhat=0.05, seed=1, kappa=1e4)
 
@@ -576,13 +577,16 @@ def main():
     ap.add_argument("--workload", default=HEADLINE, choices=sorted(WORKLOADS),
                     help="headline workload (the other one is measured as a second line)")
     ap.add_argument("--headline-only", action="store_true", help="skip the second workload")
+    ap.add_argument("--turns", type=int, default=12,
+                    help="thread turns of the screw and nut (12 = the benchmark workload; fewer for ncu captures)")
     ap.add_argument("--rods", type=int, default=4,
                     help="rods per side of the bundle (4 = the benchmark workload; smaller for ncu section captures)")
     ap.add_argument("--profile-newton", action="store_true",
                     help="untimed Newton iterations (learned PCG, device line search), for ncu; prints nothing")
     args = ap.parse_args()
-    global ROD_SIDE
+    global ROD_SIDE, TURNS
     ROD_SIDE = args.rods
+    TURNS = args.turns
     if args.profile_solver:
         run_profile_solver(args)
         return

@@ -415,7 +415,37 @@ IPCB_D double pt_dist(d3 p, d3 a, d3 b, d3 c) {
   return sqrt(dot(w, w));
 }
 
-// KIND 0: (a0, a1 | b0, b1); KIND 1: (p | t0, t1, t2)
+// KIND 0: (a0, a1 | b0, b1); KIND 1: (p | t0, t1, t2).  Lower bound on the
+// time at which the pair can touch: (d(0) - margin) / (relative motion bound),
+// 0 when it already touches, infinity when it does not move.  A verified root
+// at t needs d(t) within the margin, so no root lies below the bound.
+template <int KIND>
+IPCB_D double touch_time_bound(const d3* p0, const d3* p1) {
+  d3 dx[4];
+  d3 m = mk3(0.0, 0.0, 0.0);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    dx[k] = p1[k] - p0[k];
+    m = m + dx[k];
+  }
+  m = m * 0.25;
+  double ma = 0, mb = 0, ext = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    d3 u = dx[k] - m;
+    double l = sqrt(dot(u, u));
+    if ((KIND == 0 && k < 2) || (KIND == 1 && k < 1)) ma = fmax(ma, l);
+    else mb = fmax(mb, l);
+    ext = fmax(ext, fmax(fabs(p0[k].x), fmax(fabs(p0[k].y), fabs(p0[k].z))));
+    ext = fmax(ext, fmax(fabs(p1[k].x), fmax(fabs(p1[k].y), fabs(p1[k].z))));
+  }
+  const double d0 = KIND == 0 ? seg_seg_dist(p0[0], p0[1], p0[2], p0[3]) : pt_dist(p0[0], p0[1], p0[2], p0[3]);
+  const double gap = d0 - 1e-6 * (1.0 + ext);
+  if (!(gap > 0.0)) return 0.0;
+  const double v = ma + mb;
+  return v > 0.0 ? gap / v : INFINITY;
+}
+
 template <int KIND>
 IPCB_D bool cannot_touch(const d3* p0, const d3* p1) {
   d3 dx[4];
@@ -618,31 +648,41 @@ __global__ void __launch_bounds__(128) k_pt_collect(const S* __restrict__ x0, co
 }
 
 // one thread per staged candidate; kind 0 EE (edge, edge), 1 PT (vertex, triangle)
+// One thread per staged pair, grid-stride.  Without a sink only the minimum
+// matters: a pair whose touch-time bound is at or above the TOI stored so far
+// (re-read from L2 for every pair; it only decreases) cannot lower it, so its
+// cubic is not solved -- the result is the same minimum, bit for bit.  With
+// a sink every pair that can touch within the step is solved.
+IPCB_D double current_toi(float* toi) { return (double)__ldcg(toi); }
+IPCB_D double current_toi(double* toi) { return __ldcg(toi); }
+
 template <class S, int KIND>
 __global__ void __launch_bounds__(128) k_cand_toi(const S* __restrict__ x0, const S* __restrict__ x1,
                                                   const int* __restrict__ prims, CandList cand, S* toi,
                                                   int* status, Sink sink, const int* skip_if) {
   if (skip_if && *skip_if) return;  // the inline pass redoes every pair
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  int n = min(*cand.count, cand.capacity);
-  if (k >= n) return;
-  int2 pr = cand.pairs[k];
+  const int n = min(*cand.count, cand.capacity);
   int st = 0;
-  double tt;
-  int4 ids;
-  if (KIND == 0) {
-    int2 ea = __ldg(reinterpret_cast<const int2*>(prims) + pr.x);
-    int2 eb = __ldg(reinterpret_cast<const int2*>(prims) + pr.y);
-    tt = ee_pair_time(x0, x1, ea, eb, st);
-    ids = make_int4(ea.x, ea.y, eb.x, eb.y);
-  } else {
-    int3 tj = make_int3(__ldg(prims + 3 * pr.y), __ldg(prims + 3 * pr.y + 1), __ldg(prims + 3 * pr.y + 2));
-    tt = pt_pair_time(x0, x1, pr.x, tj, st);
-    ids = make_int4(pr.x, tj.x, tj.y, tj.z);
-  }
-  if (tt < 1.0) {
-    store_toi(toi, tt);
-    sink_append<S>(sink, ids, pr.x, pr.y, tt);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int2 pr = cand.pairs[k];
+    int4 ids;
+    if (KIND == 0) {
+      const int2 ea = __ldg(reinterpret_cast<const int2*>(prims) + pr.x);
+      const int2 eb = __ldg(reinterpret_cast<const int2*>(prims) + pr.y);
+      ids = make_int4(ea.x, ea.y, eb.x, eb.y);
+    } else {
+      ids = make_int4(pr.x, __ldg(prims + 3 * pr.y), __ldg(prims + 3 * pr.y + 1), __ldg(prims + 3 * pr.y + 2));
+    }
+    d3 p0[4] = {ld(x0, ids.x), ld(x0, ids.y), ld(x0, ids.z), ld(x0, ids.w)};
+    d3 p1[4] = {ld(x1, ids.x), ld(x1, ids.y), ld(x1, ids.z), ld(x1, ids.w)};
+    const double lb = touch_time_bound<KIND>(p0, p1);
+    if (lb > 1.0) continue;  // cannot touch within the step
+    if (!sink.on && lb >= current_toi(toi)) continue;  // cannot lower the minimum
+    const double tt = collision_time<KIND>(p0, p1, st);
+    if (tt < 1.0) {
+      store_toi(toi, tt);
+      sink_append<S>(sink, ids, pr.x, pr.y, tt);
+    }
   }
   if (st) atomicOr(status, st);
 }
@@ -894,7 +934,9 @@ template <class S>
 void run_ee(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, const float* lower, const float* upper,
             int exclude, CandList c, void* toi, int* status, Sink sink, cudaStream_t st) {
   const int n = soup->n_edges;
-  const dim3 g(div_up(n, 128)), gc(div_up(c.capacity > 0 ? c.capacity : 1, 128));
+  // k_cand_toi is grid-stride: about 14 blocks of 128 per SM, so later pairs
+  // meet an already lowered TOI
+  const dim3 g(div_up(n, 128)), gc(min(div_up(c.capacity > 0 ? c.capacity : 1, 128), 2048));
   cudaMemsetAsync(c.count, 0, 2 * sizeof(int), st);
   k_ee_collect<S, true><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->edges, soup->body,
                                            (const float4*)bvh->wide, bvh->sorted, n, lower, upper, exclude, c,
@@ -913,7 +955,7 @@ template <class S>
 void run_pt(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, double pad, int exclude, CandList c,
             void* toi, int* status, Sink sink, cudaStream_t st) {
   const int nv = soup->n_verts;
-  const dim3 g(div_up(nv, 128)), gc(div_up(c.capacity > 0 ? c.capacity : 1, 128));
+  const dim3 g(div_up(nv, 128)), gc(min(div_up(c.capacity > 0 ? c.capacity : 1, 128), 2048));
   cudaMemsetAsync(c.count, 0, 2 * sizeof(int), st);
   k_pt_collect<S, true><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->triangles, soup->body,
                                            (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude, c, (S*)toi,
@@ -1085,7 +1127,7 @@ int ipcb_fixed_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_b
   CandList c = cand_list(ws, ws_bytes);
   cudaMemsetAsync(c.count, 0, sizeof(int), st);
   dim3 grid(div_up(B->max_edges, 128) * n_pairs);
-  const int gc = div_up(c.capacity > 0 ? c.capacity : 1, 128);
+  const int gc = min(div_up(c.capacity > 0 ? c.capacity : 1, 128), 2048);
   if (soup->fp64) {
     k_fixed_ee_collect<double><<<grid, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->edges, *B,
                                                      fixed, (const int2*)pairs, pad, c, (double*)toi, status);
@@ -1112,7 +1154,7 @@ int ipcb_fixed_point_triangle_toi(const ipcb_soup* soup, const void* x1, const i
   CandList c = cand_list(ws, ws_bytes);
   cudaMemsetAsync(c.count, 0, sizeof(int), st);
   dim3 grid(div_up(B->max_verts, 128) * n_pairs, 2);
-  const int gc = div_up(c.capacity > 0 ? c.capacity : 1, 128);
+  const int gc = min(div_up(c.capacity > 0 ? c.capacity : 1, 128), 2048);
   if (soup->fp64) {
     k_fixed_pt_collect<double><<<grid, 128, 0, st>>>((const double*)soup->x, (const double*)x1, soup->triangles, *B,
                                                      (const int2*)pairs, pad, c, (double*)toi, status);
