@@ -114,8 +114,7 @@ SIGNATURES = {
     "ipcb_contact_hessian_after": (c_int, [c_int, SP, CP, c_int, c_int, P, c_double, P, P, P, P, P, P]),
     "ipcb_contact_hessian_workspace": (c_size_t, [c_int]),
     "ipcb_edge_triangle_crossings": (c_int, [SP, BP, P, P, c_int, P, P]),
-    "ipcb_contact_hessian_sorted": (c_int, [c_int, SP, CP, c_int, c_int, P, c_double, P, P, P, P, P, P, P, c_size_t,
-                                            P]),
+    "ipcb_contact_hessian_sorted": (c_int, [c_int, SP, CP, c_int, c_int, P, c_double, P, P, P, P, P, P, c_size_t, P]),
     "ipcb_contact_energy": (c_int, [c_int, SP, CP, c_int, c_double, P, P]),
     "ipcb_toi_workspace": (c_size_t, [c_int]),
     "ipcb_edge_edge_toi": (c_int, [SP, P, BP, P, P, c_int, P, P, P, c_size_t, P]),

@@ -59,3 +59,21 @@ def test_direct_library_exports_header_symbols():
     # argument validation before any device work
     assert lib.ipcb_direct_analyze(None, 0, 0, None, None, 0, 0, None) == 1
     assert lib.ipcb_direct_factor(None, None, None) == 1
+
+
+def _header_arity(header="ipcb.h"):
+    """{name: number of parameters} from the C declarations."""
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(ipcb_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_binding_argument_counts_match_header():
+    arity = _header_arity()
+    wrong = {name: (len(args), arity[name]) for name, (_, args) in _native.SIGNATURES.items()
+             if name in arity and len(args) != arity[name]}
+    assert not wrong, wrong
