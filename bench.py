@@ -163,7 +163,9 @@ NARROW_DRAM_BYTES_PER_STEP = {"rod_bundle": 441.4e6, "screw_nut": None}
 
 
 def stage_times(pipe, dx, reps, torch):
-    """Per-stage device times (ms, mean over reps) on the launching stream."""
+    """Per-stage device times (ms, mean over reps) on the launching stream;
+    the narrow phase is the class-sorted path the pipeline runs (its two
+    ordering kernels included)."""
     from ipc_warp_b200.dynamic_contacts import contact_hessian_ee, contact_hessian_pt
 
     st = torch.cuda.current_stream()
@@ -185,9 +187,11 @@ def stage_times(pipe, dx, reps, torch):
         pipe._launch_dcd("pt")
         marks.append(("dcd_pt", ev()))
         pipe.b.zero_()
-        contact_hessian_ee(None, pipe.soup, pipe.contacts_new, t, pipe.b, pipe.contact_stiffness, n=n_ee)
+        contact_hessian_ee(None, pipe.soup, pipe.contacts_new, t, pipe.b, pipe.contact_stiffness, n=n_ee,
+                           ws=pipe._ws_ee)
         marks.append(("narrow_ee", ev()))
-        contact_hessian_pt(None, pipe.soup, pipe.contacts_pt, t, pipe.b, n_ee, pipe.contact_stiffness, n=n_pt)
+        contact_hessian_pt(None, pipe.soup, pipe.contacts_pt, t, pipe.b, n_ee, pipe.contact_stiffness, n=n_pt,
+                           ws=pipe._ws_pt)
         marks.append(("narrow_pt", ev()))
         from ipc_warp_b200.bsr import contact_bsr
 

@@ -68,14 +68,20 @@ __global__ void __launch_bounds__(128, 3) k_contact_hessian(const S* __restrict_
   if (tid >= m) return;
   // offset_dev: the records follow another list's min(count, offset) records
   const int off = offset_dev ? min(*offset_dev, offset) : offset;
-  const int t = s_order[tid];
-  hessian_from<S, KIND>(x, xcs, L, base + t, off, kappa, unpack(s_pre[t]), rows, cols, vals, bforce, block_mask);
+  const int t = s_order[tid], i = base + t;
+  const int4 id = __ldg(reinterpret_cast<const int4*>(L.a1a2b1b2) + i);
+  const S l0 = static_cast<const S*>(L.l0)[i];
+  hessian_from<S, KIND>(x, xcs, id, l0, i, off, kappa, unpack(s_pre[t]), rows, cols, vals, bforce, block_mask);
 }
 
 // ---- class-sorted path: the records of the whole list are put in cost-class
 // order (most expensive first) before the Hessian kernel, so nearly every
-// warp runs one path.  Workspace: [class counts int[4] | cursors int[4] |
-// pad to 256 B | float4 pre[capacity] | int order[capacity]].
+// warp runs one path.  The ordering pass also copies each record's float32
+// part, vertex ids and l0 to its sorted position, so the Hessian kernel reads
+// its inputs coalesced and only the positions are gathered.  Workspace:
+// [class counts int[4] | cursors int[4] | pad to 256 B | float4 pre[cap] |
+// int order[cap] | float4 sorted pre[cap] | int4 sorted ids[cap] | S sorted
+// l0[cap]], each array 256-byte aligned.
 template <class S, int KIND>
 __global__ void __launch_bounds__(256) k_classify(const S* __restrict__ x, const S* __restrict__ xcs, ipcb_contacts L,
                                                   int n, float4* __restrict__ pre, int* __restrict__ counts) {
@@ -98,9 +104,35 @@ __global__ void __launch_bounds__(256) k_classify(const S* __restrict__ x, const
 }
 
 template <class S>
-__global__ void __launch_bounds__(256) k_class_order(ipcb_contacts L, int n, const float4* __restrict__ pre,
-                                                     const int* __restrict__ counts, int* __restrict__ cursor,
-                                                     int* __restrict__ order) {
+struct Sorted {
+  float4* pre;
+  int* order;
+  float4* spre;
+  int4* sids;
+  S* sl0;
+};
+
+template <class S>
+IPCB_D Sorted<S> sorted_ws(void* ws, int capacity) {
+  const size_t c = (size_t)(capacity < 1 ? 1 : capacity);
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+  char* p = (char*)ws + 256;
+  Sorted<S> r;
+  r.pre = (float4*)p;
+  p += al(c * 16);
+  r.order = (int*)p;
+  p += al(c * 4);
+  r.spre = (float4*)p;
+  p += al(c * 16);
+  r.sids = (int4*)p;
+  p += al(c * 16);
+  r.sl0 = (S*)p;
+  return r;
+}
+
+template <class S>
+__global__ void __launch_bounds__(256) k_class_order(ipcb_contacts L, int n, const int* __restrict__ counts,
+                                                     int* __restrict__ cursor, Sorted<S> W) {
   __shared__ int sc[4], sbase[4];
   const int cnt = list_count<S>(L, n);
   if ((int)(blockIdx.x * blockDim.x) >= cnt) return;
@@ -108,8 +140,10 @@ __global__ void __launch_bounds__(256) k_class_order(ipcb_contacts L, int n, con
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   int cls = -1, local = 0;
+  float4 pr = make_float4(0.f, 0.f, 0.f, 0.f);
   if (i < cnt) {
-    cls = __float_as_int(pre[i].w) & 3;
+    pr = W.pre[i];
+    cls = __float_as_int(pr.w) & 3;
     local = atomicAdd(&sc[cls], 1);
   }
   __syncthreads();
@@ -121,29 +155,38 @@ __global__ void __launch_bounds__(256) k_class_order(ipcb_contacts L, int n, con
     sbase[k] = sc[k] ? start + atomicAdd(cursor + k, sc[k]) : 0;
   }
   __syncthreads();
-  if (cls >= 0) order[sbase[cls] + local] = i;
+  if (cls >= 0) {
+    const int pos = sbase[cls] + local;
+    W.order[pos] = i;
+    W.spre[pos] = pr;
+    W.sids[pos] = __ldg(reinterpret_cast<const int4*>(L.a1a2b1b2) + i);
+    W.sl0[pos] = static_cast<const S*>(L.l0)[i];
+  }
 }
 
 template <class S, int KIND>
 __global__ void __launch_bounds__(128, 3) k_contact_hessian_sorted(const S* __restrict__ x,
                                                                 const S* __restrict__ xcs, ipcb_contacts L, int n,
                                                                 int offset, const int* __restrict__ offset_dev,
-                                                                double kappa, const float4* __restrict__ pre,
-                                                                const int* __restrict__ order,
+                                                                double kappa, Sorted<S> W,
                                                                 int* __restrict__ rows, int* __restrict__ cols,
                                                                 S* __restrict__ vals, S* __restrict__ bforce,
                                                                 unsigned short* __restrict__ block_mask) {
   const int cnt = list_count<S>(L, n);
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= cnt) return;
-  const int i = __ldg(order + t);
+  const int i = __ldg(W.order + t);
+  const int4 id = __ldg(W.sids + t);
+  const S l0 = __ldg(W.sl0 + t);
   const int off = offset_dev ? min(*offset_dev, offset) : offset;
-  hessian_from<S, KIND>(x, xcs, L, i, off, kappa, unpack(__ldg(pre + i)), rows, cols, vals, bforce, block_mask);
+  hessian_from<S, KIND>(x, xcs, id, l0, i, off, kappa, unpack(__ldg(W.spre + t)), rows, cols, vals, bforce,
+                        block_mask);
 }
 
 size_t sorted_workspace(int capacity) {
   const size_t c = (size_t)(capacity < 1 ? 1 : capacity);
-  return 256 + ((c * 16 + 255) / 256) * 256 + c * 4;
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+  return 256 + al(c * 16) + al(c * 4) + al(c * 16) + al(c * 16) + al(c * 8);
 }
 
 template <class S, int KIND>
@@ -211,25 +254,23 @@ int launch_hessian_sorted(int kind, const ipcb_soup* soup, const ipcb_contacts* 
                           unsigned short* mask, void* ws, cudaStream_t st) {
   int threads = n >= 0 ? n : L->capacity;
   if (threads == 0) return IPCB_OK;
-  const size_t c = (size_t)(L->capacity < 1 ? 1 : L->capacity);
   int* counts = (int*)ws;
   int* cursor = counts + 4;
-  float4* pre = (float4*)((char*)ws + 256);
-  int* order = (int*)((char*)ws + 256 + ((c * 16 + 255) / 256) * 256);
+  const Sorted<S> W = sorted_ws<S>(ws, L->capacity);
   cudaMemsetAsync(ws, 0, 8 * sizeof(int), st);
   const S* x = (const S*)soup->x;
   const S* xcs = (const S*)soup->xcs;
   dim3 g256(div_up(threads, 256)), g128(div_up(threads, 128));
   if (kind == 0) {
-    k_classify<S, 0><<<g256, 256, 0, st>>>(x, xcs, *L, n, pre, counts);
-    k_class_order<S><<<g256, 256, 0, st>>>(*L, n, pre, counts, cursor, order);
-    k_contact_hessian_sorted<S, 0><<<g128, 128, 0, st>>>(x, xcs, *L, n, offset, offset_dev, kappa, pre, order, rows,
-                                                         cols, (S*)vals, (S*)b, mask);
+    k_classify<S, 0><<<g256, 256, 0, st>>>(x, xcs, *L, n, W.pre, counts);
+    k_class_order<S><<<g256, 256, 0, st>>>(*L, n, counts, cursor, W);
+    k_contact_hessian_sorted<S, 0><<<g128, 128, 0, st>>>(x, xcs, *L, n, offset, offset_dev, kappa, W, rows, cols,
+                                                         (S*)vals, (S*)b, mask);
   } else {
-    k_classify<S, 1><<<g256, 256, 0, st>>>(x, xcs, *L, n, pre, counts);
-    k_class_order<S><<<g256, 256, 0, st>>>(*L, n, pre, counts, cursor, order);
-    k_contact_hessian_sorted<S, 1><<<g128, 128, 0, st>>>(x, xcs, *L, n, offset, offset_dev, kappa, pre, order, rows,
-                                                         cols, (S*)vals, (S*)b, mask);
+    k_classify<S, 1><<<g256, 256, 0, st>>>(x, xcs, *L, n, W.pre, counts);
+    k_class_order<S><<<g256, 256, 0, st>>>(*L, n, counts, cursor, W);
+    k_contact_hessian_sorted<S, 1><<<g128, 128, 0, st>>>(x, xcs, *L, n, offset, offset_dev, kappa, W, rows, cols,
+                                                         (S*)vals, (S*)b, mask);
   }
   return check_launch("ipcb_contact_hessian_sorted");
 }

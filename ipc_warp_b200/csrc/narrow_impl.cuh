@@ -489,9 +489,10 @@ IPCB_D int record_class(const S* __restrict__ x, const S* __restrict__ xcs, cons
 // One record of contact_hessian_ee / _pt from its float32 part p: 16 blocks
 // at (offset + i)*16, force into bforce, block mask.  T: arithmetic type of
 // the eigen-solve and of H (float for S=float).
+// record i of the list (vertex ids id, l0); its outputs go to slot offset + i
 template <class S, int KIND>
-IPCB_D void hessian_from(const S* __restrict__ x, const S* __restrict__ xcs, const ipcb_contacts& L, int i,
-                         int offset, double kappa, const Pre& p, int* __restrict__ rows, int* __restrict__ cols,
+IPCB_D void hessian_from(const S* __restrict__ x, const S* __restrict__ xcs, int4 id, S l0, int i, int offset,
+                         double kappa, const Pre& p, int* __restrict__ rows, int* __restrict__ cols,
                          S* __restrict__ vals, S* __restrict__ bforce, unsigned short* __restrict__ block_mask) {
   typedef S T;
   long long base = (long long)(offset + i) * 16;
@@ -500,8 +501,6 @@ IPCB_D void hessian_from(const S* __restrict__ x, const S* __restrict__ xcs, con
     if (block_mask) block_mask[offset + i] = 0;
     return;
   }
-  int4 id = __ldg(reinterpret_cast<const int4*>(L.a1a2b1b2) + i);
-  S l0 = static_cast<const S*>(L.l0)[i];
   v3<S> xs[4] = {ldx(x, id.x), ldx(x, id.y), ldx(x, id.z), ldx(x, id.w)};
   d3 xd[4] = {to_d(xs[0]), to_d(xs[1]), to_d(xs[2]), to_d(xs[3])};
   const float dist = p.d;
@@ -553,7 +552,7 @@ IPCB_D void contact_hessian_item(const S* __restrict__ x, const S* __restrict__ 
   const S l0 = static_cast<const S*>(L.l0)[i];
   const v3<S> xs[4] = {ldx(x, id.x), ldx(x, id.y), ldx(x, id.z), ldx(x, id.w)};
   const Pre p = predicate<S, KIND>(xcs, id, l0, xs);
-  hessian_from<S, KIND>(x, xcs, L, i, offset, kappa, p, rows, cols, vals, bforce, block_mask);
+  hessian_from<S, KIND>(x, xcs, id, l0, i, offset, kappa, p, rows, cols, vals, bforce, block_mask);
 }
 
 }  // namespace

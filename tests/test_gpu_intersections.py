@@ -38,12 +38,17 @@ def test_crossings_match_oracle(cuda, dtype, sink):
 
 
 @pytest.mark.parametrize("idx", range(4))
-def test_contact_scenes_are_intersection_free(cuda, idx):
+def test_contact_scenes_match_oracle(cuda, idx):
+    """The parity scenes: the first three are intersection-free; the fourth
+    (rods 0.3 dhat apart with a 0.2 dhat vertex jitter on both sides)
+    interpenetrates by construction, and the GPU finds the oracle's pairs."""
     sc = small_scenes()[idx]
     pipe = ContactPipeline.from_scene(sc, dtype=torch.float32, device=cuda)
-    n, _ = pipe.edge_triangle_crossings()
-    assert n == 0
-    assert po.edge_triangle_crossings(sc.x.astype(np.float32), sc.edges, sc.triangles)[0] == 0
+    n, pairs = pipe.edge_triangle_crossings(capacity=1 << 16)
+    on, opairs = po.edge_triangle_crossings(sc.x.astype(np.float32), sc.edges, sc.triangles)
+    assert n == on
+    assert np.array_equal(_pairs_sorted(pairs.cpu().numpy()), _pairs_sorted(opairs))
+    assert (n == 0) == (idx < 3)
 
 
 def test_screw_and_nut_is_intersection_free(cuda):
