@@ -148,8 +148,9 @@ IPCB_D void feature_ee(Feature& f, const d3* x) {
 
 // Negative spectral part of hess(d^2) as sum_e lam_e u_e u_e^T; fills h[1..]
 // and w[1..] (w = scale * lam).  Returns the number of vectors written.
-template <class T, int NP>
-IPCB_D int nsd_subspace(const Feature& f, double scale, T (&h)[kMaxH][12], T (&w)[kMaxH]) {
+template <class T, int NP, int MH>
+IPCB_D int nsd_subspace(const Feature& f, double scale, T (&h)[MH][12], T (&w)[MH]) {
+  static_assert(MH >= 2 * NP + 2, "room for the gradient and every eigenvector");
   constexpr int NZ = 1 + NP, NS = 2 * NP + 1;
   double cn = sqrt(f.c[0] * f.c[0] + f.c[1] * f.c[1] + f.c[2] * f.c[2] + f.c[3] * f.c[3]);
   double ch[4], fv[NP][4];
@@ -368,9 +369,9 @@ IPCB_D void write_zero(int* rows, int* cols, S* vals, long long base) {
 // 16 blocks of H = sum_m w_m h_m h_m^T; the record's 144 values are
 // contiguous and 16-byte aligned (576 B per record in float), written as two
 // halves of 8 blocks with vector stores.
-template <class S, class T>
-IPCB_D unsigned write_blocks(const int4 id, int* rows, int* cols, S* vals, long long base, const T (&h)[kMaxH][12],
-                             const T (&w)[kMaxH], int nh) {
+template <class S, class T, int MH>
+IPCB_D unsigned write_blocks(const int4 id, int* rows, int* cols, S* vals, long long base, const T (&h)[MH][12],
+                             const T (&w)[MH], int nh) {
   unsigned mask = 0;
   const int vid[4] = {id.x, id.y, id.z, id.w};
 #pragma unroll
@@ -386,16 +387,16 @@ IPCB_D unsigned write_blocks(const int4 id, int* rows, int* cols, S* vals, long 
     S buf[36];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      T wh[kMaxH];
+      T wh[MH];
 #pragma unroll
-      for (int m = 0; m < kMaxH; ++m) wh[m] = m < nh ? w[m] * h[m][3 * ii + a] : T(0);
+      for (int m = 0; m < MH; ++m) wh[m] = m < nh ? w[m] * h[m][3 * ii + a] : T(0);
 #pragma unroll
       for (int jj = 0; jj < 4; ++jj)
 #pragma unroll
         for (int b = 0; b < 3; ++b) {
           T v = T(0);
 #pragma unroll
-          for (int m = 0; m < kMaxH; ++m)
+          for (int m = 0; m < MH; ++m)
             if (m < nh) v += wh[m] * h[m][3 * jj + b];  // rows m >= nh of h are not set
           buf[jj * 9 + 3 * a + b] = S(v);
           if (S(v) != S(0)) mask |= 1u << (ii * 4 + jj);
@@ -489,14 +490,16 @@ IPCB_D int record_class(const S* __restrict__ x, const S* __restrict__ xcs, cons
 // One record of contact_hessian_ee / _pt from its float32 part p: 16 blocks
 // at (offset + i)*16, force into bforce, block mask.  T: arithmetic type of
 // the eigen-solve and of H (float for S=float).
-// record i of the list (vertex ids id, l0); its outputs go to slot offset + i
-template <class S, int KIND>
+// record i of the list (vertex ids id, l0); its outputs go to slot offset + i.
+// CLS >= 0: the caller guarantees the record's class, and only that class's
+// path is compiled (fewer registers for the cheap classes); CLS = -1: any.
+template <class S, int KIND, int CLS = -1>
 IPCB_D void hessian_from(const S* __restrict__ x, const S* __restrict__ xcs, int4 id, S l0, int i, int offset,
                          double kappa, const Pre& p, int* __restrict__ rows, int* __restrict__ cols,
                          S* __restrict__ vals, S* __restrict__ bforce, unsigned short* __restrict__ block_mask) {
   typedef S T;
   long long base = (long long)(offset + i) * 16;
-  if (p.cls() == 0) {
+  if (CLS == 0 || (CLS < 0 && p.cls() == 0)) {
     write_zero<S>(rows, cols, vals, base);
     if (block_mask) block_mask[offset + i] = 0;
     return;
@@ -510,9 +513,12 @@ IPCB_D void hessian_from(const S* __restrict__ x, const S* __restrict__ xcs, int
   else pt_dispatch(f, p.type(), xd);
   double d2 = (double)dist * (double)dist, d02 = (double)l0 * (double)l0;
   Barrier br = barrier(d2, d02, kappa);
-  T h[kMaxH][12], w[kMaxH];
+  // rank-one terms of H: the gradient, plus up to 3 (point-edge) or 5
+  // (edge-edge, point-triangle) negative eigenvectors
+  constexpr int MH = CLS == 1 ? 1 : (CLS == 2 ? 4 : kMaxH);
+  T h[MH][12], w[MH];
 #pragma unroll
-  for (int m = 0; m < kMaxH; ++m) w[m] = T(0);
+  for (int m = 0; m < MH; ++m) w[m] = T(0);
   double g[12];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
@@ -532,12 +538,16 @@ IPCB_D void hessian_from(const S* __restrict__ x, const S* __restrict__ xcs, int
     for (int k = 0; k < 12; ++k) fc[k] = -(mv * br.db * g[k] + br.b * gm[k]);
   } else {
     w[0] = T(br.d2b);
-    if (f.np == 1) nh = 1 + nsd_subspace<T, 1>(f, br.db, h, w);
-    else if (f.np == 2) nh = 1 + nsd_subspace<T, 2>(f, br.db, h, w);
+    if constexpr (CLS < 0 || CLS == 2) {
+      if (f.np == 1) nh = 1 + nsd_subspace<T, 1, MH>(f, br.db, h, w);
+    }
+    if constexpr (CLS < 0 || CLS == 3) {
+      if (f.np == 2) nh = 1 + nsd_subspace<T, 2, MH>(f, br.db, h, w);
+    }
 #pragma unroll
     for (int k = 0; k < 12; ++k) fc[k] = -br.db * g[k];
   }
-  unsigned mask = write_blocks<S, T>(id, rows, cols, vals, base, h, w, nh);
+  unsigned mask = write_blocks<S, T, MH>(id, rows, cols, vals, base, h, w, nh);
   if (block_mask) block_mask[offset + i] = (unsigned short)mask;
   add_force<S>(bforce, id, fc);
 }
