@@ -112,8 +112,9 @@ struct Sorted {
   S* sl0;
 };
 
+// host side: the device addresses of the workspace's arrays
 template <class S>
-IPCB_D Sorted<S> sorted_ws(void* ws, int capacity) {
+inline Sorted<S> sorted_ws(void* ws, int capacity) {
   const size_t c = (size_t)(capacity < 1 ? 1 : capacity);
   auto al = [](size_t b) { return (b + 255) / 256 * 256; };
   char* p = (char*)ws + 256;
