@@ -165,47 +165,35 @@ __global__ void __launch_bounds__(256) k_class_order(ipcb_contacts L, int n, con
   }
 }
 
-// One kernel per cost class over that class's range of the sorted order
-// (classes 3, 2, 1, 0 from the front), one record per thread; each compiles only its
-// class's path, so the cheap classes run with far fewer registers (more
-// warps in flight for their stores) than the 5x5 eigen-solve.
-template <int CLS>
-struct ClassBounds;
-template <>
-struct ClassBounds<3> {
-  static constexpr int kThreads = 128, kMinBlocks = 3;
-};
-template <>
-struct ClassBounds<2> {
-  static constexpr int kThreads = 128, kMinBlocks = 4;
-};
-template <>
-struct ClassBounds<1> {
-  static constexpr int kThreads = 256, kMinBlocks = 3;
-};
-template <>
-struct ClassBounds<0> {
-  static constexpr int kThreads = 256, kMinBlocks = 4;
-};
-
-template <class S, int KIND, int CLS>
-__global__ void __launch_bounds__(ClassBounds<CLS>::kThreads, ClassBounds<CLS>::kMinBlocks)
-    k_contact_hessian_sorted(const S* __restrict__ x, const S* __restrict__ xcs, int offset,
-                             const int* __restrict__ offset_dev, double kappa, const int* __restrict__ counts,
-                             Sorted<S> W, int* __restrict__ rows, int* __restrict__ cols, S* __restrict__ vals,
-                             S* __restrict__ bforce, unsigned short* __restrict__ block_mask) {
-  int start = 0;
-#pragma unroll
-  for (int c = 3; c > CLS; --c) start += counts[c];
-  const int end = start + counts[CLS];
-  const int t = start + blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= end) return;
+// After the ordering pass, one thread per position of the sorted order; a
+// warp's lanes store their records' blocks together (hessian_from_warp).
+template <class S, int KIND>
+__global__ void __launch_bounds__(128, 3) k_contact_hessian_sorted(const S* __restrict__ x,
+                                                                const S* __restrict__ xcs, ipcb_contacts L, int n,
+                                                                int offset, const int* __restrict__ offset_dev,
+                                                                double kappa, Sorted<S> W,
+                                                                int* __restrict__ rows, int* __restrict__ cols,
+                                                                S* __restrict__ vals, S* __restrict__ bforce,
+                                                                unsigned short* __restrict__ block_mask) {
+  __shared__ __align__(16) S stage[4][32 * 36];
+  const int cnt = list_count<S>(L, n);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int warp_first = t & ~31;
+  if (warp_first >= cnt) return;  // the whole warp
+  const bool active = t < cnt;
   const int off = offset_dev ? min(*offset_dev, offset) : offset;
-  const int i = __ldg(W.order + t);
-  const int4 id = __ldg(W.sids + t);
-  const S l0 = __ldg(W.sl0 + t);
-  hessian_from<S, KIND, CLS>(x, xcs, id, l0, i, off, kappa, unpack(__ldg(W.spre + t)), rows, cols, vals, bforce,
-                             block_mask);
+  int i = 0;
+  int4 id = make_int4(0, 0, 0, 0);
+  S l0 = S(0);
+  Pre p{0.f, 0.f, 0.f, 0};
+  if (active) {
+    i = __ldg(W.order + t);
+    id = __ldg(W.sids + t);
+    l0 = __ldg(W.sl0 + t);
+    p = unpack(__ldg(W.spre + t));
+  }
+  hessian_from_warp<S, KIND>(x, xcs, id, l0, i, off, kappa, p, active, rows, cols, vals, bforce, block_mask,
+                             stage[threadIdx.x >> 5]);
 }
 
 size_t sorted_workspace(int capacity) {
@@ -273,28 +261,6 @@ int launch_hessian(int kind, const ipcb_soup* soup, const ipcb_contacts* L, int 
   return check_launch("ipcb_contact_hessian");
 }
 
-// the class counts are on the device: each class kernel gets a grid for the
-// whole list, and the blocks past its class's records return at once
-template <class S, int KIND, int CLS>
-void launch_class(int threads, const S* x, const S* xcs, int offset, const int* offset_dev, double kappa,
-                  const int* counts, const Sorted<S>& W, int* rows, int* cols, S* vals, S* b, unsigned short* mask,
-                  cudaStream_t st) {
-  constexpr int T = ClassBounds<CLS>::kThreads;
-  const int blocks = div_up(threads, T);
-  k_contact_hessian_sorted<S, KIND, CLS><<<blocks, T, 0, st>>>(x, xcs, offset, offset_dev, kappa, counts, W, rows, cols,
-                                                               vals, b, mask);
-}
-
-template <class S, int KIND>
-void launch_classes(int threads, const S* x, const S* xcs, int offset, const int* offset_dev, double kappa,
-                    const int* counts, const Sorted<S>& W, int* rows, int* cols, S* vals, S* b, unsigned short* mask,
-                    cudaStream_t st) {
-  launch_class<S, KIND, 3>(threads, x, xcs, offset, offset_dev, kappa, counts, W, rows, cols, vals, b, mask, st);
-  launch_class<S, KIND, 2>(threads, x, xcs, offset, offset_dev, kappa, counts, W, rows, cols, vals, b, mask, st);
-  launch_class<S, KIND, 1>(threads, x, xcs, offset, offset_dev, kappa, counts, W, rows, cols, vals, b, mask, st);
-  launch_class<S, KIND, 0>(threads, x, xcs, offset, offset_dev, kappa, counts, W, rows, cols, vals, b, mask, st);
-}
-
 template <class S>
 int launch_hessian_sorted(int kind, const ipcb_soup* soup, const ipcb_contacts* L, int n, int offset,
                           const int* offset_dev, double kappa, int* rows, int* cols, void* vals, void* b,
@@ -307,15 +273,17 @@ int launch_hessian_sorted(int kind, const ipcb_soup* soup, const ipcb_contacts* 
   cudaMemsetAsync(ws, 0, 8 * sizeof(int), st);
   const S* x = (const S*)soup->x;
   const S* xcs = (const S*)soup->xcs;
-  dim3 g256(div_up(threads, 256));
+  dim3 g256(div_up(threads, 256)), g128(div_up(threads, 128));
   if (kind == 0) {
     k_classify<S, 0><<<g256, 256, 0, st>>>(x, xcs, *L, n, W.pre, counts);
     k_class_order<S><<<g256, 256, 0, st>>>(*L, n, counts, cursor, W);
-    launch_classes<S, 0>(threads, x, xcs, offset, offset_dev, kappa, counts, W, rows, cols, (S*)vals, (S*)b, mask, st);
+    k_contact_hessian_sorted<S, 0><<<g128, 128, 0, st>>>(x, xcs, *L, n, offset, offset_dev, kappa, W, rows, cols,
+                                                         (S*)vals, (S*)b, mask);
   } else {
     k_classify<S, 1><<<g256, 256, 0, st>>>(x, xcs, *L, n, W.pre, counts);
     k_class_order<S><<<g256, 256, 0, st>>>(*L, n, counts, cursor, W);
-    launch_classes<S, 1>(threads, x, xcs, offset, offset_dev, kappa, counts, W, rows, cols, (S*)vals, (S*)b, mask, st);
+    k_contact_hessian_sorted<S, 1><<<g128, 128, 0, st>>>(x, xcs, *L, n, offset, offset_dev, kappa, W, rows, cols,
+                                                         (S*)vals, (S*)b, mask);
   }
   return check_launch("ipcb_contact_hessian_sorted");
 }

@@ -490,20 +490,13 @@ IPCB_D int record_class(const S* __restrict__ x, const S* __restrict__ xcs, cons
 // One record of contact_hessian_ee / _pt from its float32 part p: 16 blocks
 // at (offset + i)*16, force into bforce, block mask.  T: arithmetic type of
 // the eigen-solve and of H (float for S=float).
-// record i of the list (vertex ids id, l0); its outputs go to slot offset + i.
-// CLS >= 0: the caller guarantees the record's class, and only that class's
-// path is compiled (fewer registers for the cheap classes); CLS = -1: any.
-template <class S, int KIND, int CLS = -1>
-IPCB_D void hessian_from(const S* __restrict__ x, const S* __restrict__ xcs, int4 id, S l0, int i, int offset,
-                         double kappa, const Pre& p, int* __restrict__ rows, int* __restrict__ cols,
-                         S* __restrict__ vals, S* __restrict__ bforce, unsigned short* __restrict__ block_mask) {
+// Rank-one terms of one active record: H = sum_m w_m h_m h_m^T (the
+// gradient, plus up to 3 (point-edge) or 5 (edge-edge, point-triangle)
+// negative eigenvectors) and the force fc.  Returns the number of terms.
+template <class S, int KIND>
+IPCB_D int hessian_terms(const S* __restrict__ x, const S* __restrict__ xcs, int4 id, S l0, double kappa,
+                         const Pre& p, S (&h)[kMaxH][12], S (&w)[kMaxH], double (&fc)[12]) {
   typedef S T;
-  long long base = (long long)(offset + i) * 16;
-  if (CLS == 0 || (CLS < 0 && p.cls() == 0)) {
-    write_zero<S>(rows, cols, vals, base);
-    if (block_mask) block_mask[offset + i] = 0;
-    return;
-  }
   v3<S> xs[4] = {ldx(x, id.x), ldx(x, id.y), ldx(x, id.z), ldx(x, id.w)};
   d3 xd[4] = {to_d(xs[0]), to_d(xs[1]), to_d(xs[2]), to_d(xs[3])};
   const float dist = p.d;
@@ -513,12 +506,8 @@ IPCB_D void hessian_from(const S* __restrict__ x, const S* __restrict__ xcs, int
   else pt_dispatch(f, p.type(), xd);
   double d2 = (double)dist * (double)dist, d02 = (double)l0 * (double)l0;
   Barrier br = barrier(d2, d02, kappa);
-  // rank-one terms of H: the gradient, plus up to 3 (point-edge) or 5
-  // (edge-edge, point-triangle) negative eigenvectors
-  constexpr int MH = CLS == 1 ? 1 : (CLS == 2 ? 4 : kMaxH);
-  T h[MH][12], w[MH];
 #pragma unroll
-  for (int m = 0; m < MH; ++m) w[m] = T(0);
+  for (int m = 0; m < kMaxH; ++m) w[m] = T(0);
   double g[12];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
@@ -528,7 +517,6 @@ IPCB_D void hessian_from(const S* __restrict__ x, const S* __restrict__ xcs, int
   }
 #pragma unroll
   for (int k = 0; k < 12; ++k) h[0][k] = T(g[k]);
-  double fc[12];
   int nh = 1;
   if (near_par) {
     double mv, gm[12];
@@ -538,18 +526,98 @@ IPCB_D void hessian_from(const S* __restrict__ x, const S* __restrict__ xcs, int
     for (int k = 0; k < 12; ++k) fc[k] = -(mv * br.db * g[k] + br.b * gm[k]);
   } else {
     w[0] = T(br.d2b);
-    if constexpr (CLS < 0 || CLS == 2) {
-      if (f.np == 1) nh = 1 + nsd_subspace<T, 1, MH>(f, br.db, h, w);
-    }
-    if constexpr (CLS < 0 || CLS == 3) {
-      if (f.np == 2) nh = 1 + nsd_subspace<T, 2, MH>(f, br.db, h, w);
-    }
+    if (f.np == 1) nh = 1 + nsd_subspace<T, 1, kMaxH>(f, br.db, h, w);
+    else if (f.np == 2) nh = 1 + nsd_subspace<T, 2, kMaxH>(f, br.db, h, w);
 #pragma unroll
     for (int k = 0; k < 12; ++k) fc[k] = -br.db * g[k];
   }
-  unsigned mask = write_blocks<S, T, MH>(id, rows, cols, vals, base, h, w, nh);
+  return nh;
+}
+
+// record i of the list (vertex ids id, l0); its outputs go to slot offset + i
+template <class S, int KIND>
+IPCB_D void hessian_from(const S* __restrict__ x, const S* __restrict__ xcs, int4 id, S l0, int i, int offset,
+                         double kappa, const Pre& p, int* __restrict__ rows, int* __restrict__ cols,
+                         S* __restrict__ vals, S* __restrict__ bforce, unsigned short* __restrict__ block_mask) {
+  long long base = (long long)(offset + i) * 16;
+  if (p.cls() == 0) {
+    write_zero<S>(rows, cols, vals, base);
+    if (block_mask) block_mask[offset + i] = 0;
+    return;
+  }
+  S h[kMaxH][12], w[kMaxH];
+  double fc[12];
+  const int nh = hessian_terms<S, KIND>(x, xcs, id, l0, kappa, p, h, w, fc);
+  unsigned mask = write_blocks<S, S, kMaxH>(id, rows, cols, vals, base, h, w, nh);
   if (block_mask) block_mask[offset + i] = (unsigned short)mask;
   add_force<S>(bforce, id, fc);
+}
+
+// The same, written by the 32 lanes of a warp together (every lane calls it;
+// a lane without a record passes active = false): each lane forms one block
+// row of its record at a time into the warp's shared-memory stage, then the
+// warp stores the 32 block rows -- each 36 contiguous values -- as runs of
+// 16-byte vectors, instead of every lane storing 16 bytes to 32 different
+// records per instruction.  stage: 32 * 36 values, 16-byte aligned.
+template <class S, int KIND>
+IPCB_D void hessian_from_warp(const S* __restrict__ x, const S* __restrict__ xcs, int4 id, S l0, int i, int offset,
+                              double kappa, const Pre& p, bool active, int* __restrict__ rows,
+                              int* __restrict__ cols, S* __restrict__ vals, S* __restrict__ bforce,
+                              unsigned short* __restrict__ block_mask, S* __restrict__ stage) {
+  constexpr int kVec = 36 * (int)sizeof(S) / 16;  // 16-byte vectors per block row
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const bool live = active && p.cls() != 0;
+  S h[kMaxH][12], w[kMaxH];
+  double fc[12];
+  int nh = 0;
+  if (live) nh = hessian_terms<S, KIND>(x, xcs, id, l0, kappa, p, h, w, fc);
+  const long long base = (long long)(offset + i) * 16;
+  const int4 rid = live ? id : make_int4(0, 0, 0, 0);
+  if (active) {
+    const int vid[4] = {rid.x, rid.y, rid.z, rid.w};
+#pragma unroll
+    for (int ii = 0; ii < 4; ++ii) {
+      reinterpret_cast<int4*>(rows + base)[ii] = make_int4(vid[ii], vid[ii], vid[ii], vid[ii]);
+      reinterpret_cast<int4*>(cols + base)[ii] = make_int4(vid[0], vid[1], vid[2], vid[3]);
+    }
+  }
+  unsigned mask = 0;
+#pragma unroll
+  for (int ii = 0; ii < 4; ++ii) {
+    S buf[36];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      S wh[kMaxH];
+#pragma unroll
+      for (int m = 0; m < kMaxH; ++m) wh[m] = m < nh ? w[m] * h[m][3 * ii + a] : S(0);
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          S v = S(0);
+#pragma unroll
+          for (int m = 0; m < kMaxH; ++m)
+            if (m < nh) v += wh[m] * h[m][3 * jj + b];
+          buf[jj * 9 + 3 * a + b] = v;
+          if (v != S(0)) mask |= 1u << (ii * 4 + jj);
+        }
+    }
+    const float4* st4 = reinterpret_cast<const float4*>(stage);
+    store16(stage + 36 * lane, buf, 36);  // 16-byte aligned: 36 values are 144 (288) bytes
+    __syncwarp(full);
+    // vector u of the warp's 32 * kVec belongs to lane u / kVec's block row
+#pragma unroll
+    for (int r = 0; r < kVec; ++r) {
+      const int u = 32 * r + lane, owner = u / kVec, piece = u - owner * kVec;
+      const long long ob = __shfl_sync(full, base, owner);
+      const bool on = __shfl_sync(full, active, owner);
+      if (on) reinterpret_cast<float4*>(vals + 9 * ob + 36 * ii)[piece] = st4[u];
+    }
+    __syncwarp(full);
+  }
+  if (active && block_mask) block_mask[offset + i] = (unsigned short)mask;
+  if (live) add_force<S>(bforce, id, fc);
 }
 
 // One record of contact_hessian_ee / _pt: the float32 part, then the rest.
