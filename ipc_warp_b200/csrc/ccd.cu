@@ -687,6 +687,130 @@ __global__ void __launch_bounds__(128) k_cand_toi(const S* __restrict__ x0, cons
   if (st) atomicOr(status, st);
 }
 
+// ---- ordered candidate solve (no record sink): the staged pairs' touch-time
+// bounds are computed first by a light kernel and the pairs bucketed by them
+// (32 buckets over [0, 1]; a pair that cannot touch within the step is
+// dropped); the solve then takes the pairs in bucket order, so the pairs that
+// can touch earliest set the TOI first, and a pair whose bound is at or above
+// the TOI stored so far is skipped (it cannot lower the minimum: the result is
+// the same minimum, bit for bit); a warp that meets a bucket starting at or
+// above the stored TOI stops.  Divergence between pruned and solved pairs and
+// the cubic solver's registers stay out of the bound pass.
+constexpr int kBuckets = 32;
+struct CandOrder {
+  int* bcount;   // pairs per bucket
+  int* bcursor;  // fill cursors
+  int* work;     // next position of the ordered solve
+  float* tlb;    // per staged pair: touch-time bound rounded down, or 2 (cannot touch)
+  int* order;    // staged pair indices in bucket order
+};
+
+IPCB_D int bucket_of(float tl) { return min(kBuckets - 1, (int)(tl * (float)kBuckets)); }
+
+template <class S, int KIND>
+__global__ void __launch_bounds__(256) k_cand_bound(const S* __restrict__ x0, const S* __restrict__ x1,
+                                                    const int* __restrict__ prims, CandList cand, CandOrder o,
+                                                    const int* skip_if) {
+  __shared__ int sb[kBuckets];
+  if (skip_if && *skip_if) return;  // the inline pass redoes every pair
+  const int n = min(*cand.count, cand.capacity);
+  if ((int)(blockIdx.x * blockDim.x) >= n) return;
+  if (threadIdx.x < kBuckets) sb[threadIdx.x] = 0;
+  __syncthreads();
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) {
+    const int2 pr = cand.pairs[k];
+    int4 ids;
+    if (KIND == 0) {
+      const int2 ea = __ldg(reinterpret_cast<const int2*>(prims) + pr.x);
+      const int2 eb = __ldg(reinterpret_cast<const int2*>(prims) + pr.y);
+      ids = make_int4(ea.x, ea.y, eb.x, eb.y);
+    } else {
+      ids = make_int4(pr.x, __ldg(prims + 3 * pr.y), __ldg(prims + 3 * pr.y + 1), __ldg(prims + 3 * pr.y + 2));
+    }
+    d3 p0[4] = {ld(x0, ids.x), ld(x0, ids.y), ld(x0, ids.z), ld(x0, ids.w)};
+    d3 p1[4] = {ld(x1, ids.x), ld(x1, ids.y), ld(x1, ids.z), ld(x1, ids.w)};
+    const double lb = touch_time_bound<KIND>(p0, p1);
+    float tl = 2.0f;
+    if (lb <= 1.0) {
+      tl = __double2float_rd(lb);  // not above the bound
+      atomicAdd(&sb[bucket_of(tl)], 1);
+    }
+    o.tlb[k] = tl;
+  }
+  __syncthreads();
+  if (threadIdx.x < kBuckets && sb[threadIdx.x]) atomicAdd(o.bcount + threadIdx.x, sb[threadIdx.x]);
+}
+
+__global__ void __launch_bounds__(256) k_cand_bucket(CandList cand, CandOrder o, const int* skip_if) {
+  __shared__ int sb[kBuckets], sbase[kBuckets];
+  if (skip_if && *skip_if) return;
+  const int n = min(*cand.count, cand.capacity);
+  if ((int)(blockIdx.x * blockDim.x) >= n) return;
+  if (threadIdx.x < kBuckets) sb[threadIdx.x] = 0;
+  __syncthreads();
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  int b = -1, local = 0;
+  if (k < n) {
+    const float tl = o.tlb[k];
+    if (tl <= 1.0f) {
+      b = bucket_of(tl);
+      local = atomicAdd(&sb[b], 1);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < kBuckets) {
+    const int q = threadIdx.x;
+    int start = 0;
+    for (int c = 0; c < q; ++c) start += o.bcount[c];
+    sbase[q] = sb[q] ? start + atomicAdd(o.bcursor + q, sb[q]) : 0;
+  }
+  __syncthreads();
+  if (b >= 0) o.order[sbase[b] + local] = k;
+}
+
+template <class S, int KIND>
+__global__ void __launch_bounds__(128) k_cand_solve(const S* __restrict__ x0, const S* __restrict__ x1,
+                                                    const int* __restrict__ prims, CandList cand, CandOrder o, S* toi,
+                                                    int* status, const int* skip_if) {
+  if (skip_if && *skip_if) return;
+  int total = 0;
+#pragma unroll 1
+  for (int q = 0; q < kBuckets; ++q) total += o.bcount[q];
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  int st = 0;
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(o.work, 32);
+    base = __shfl_sync(full, base, 0);
+    if (base >= total) break;
+    const int item = base + lane;
+    const int k = item < total ? __ldg(o.order + item) : -1;
+    const float tl = k >= 0 ? __ldg(o.tlb + k) : 2.0f;
+    const double cur = current_toi(toi);
+    // the chunk's first pair starts its bucket range: every later pair lies
+    // in this bucket or a later one, so none can lower a TOI at or below it
+    const float first = __shfl_sync(full, tl, 0);
+    if ((double)bucket_of(first) / kBuckets >= cur) break;
+    if (k < 0 || (double)tl >= cur) continue;
+    const int2 pr = cand.pairs[k];
+    int4 ids;
+    if (KIND == 0) {
+      const int2 ea = __ldg(reinterpret_cast<const int2*>(prims) + pr.x);
+      const int2 eb = __ldg(reinterpret_cast<const int2*>(prims) + pr.y);
+      ids = make_int4(ea.x, ea.y, eb.x, eb.y);
+    } else {
+      ids = make_int4(pr.x, __ldg(prims + 3 * pr.y), __ldg(prims + 3 * pr.y + 1), __ldg(prims + 3 * pr.y + 2));
+    }
+    d3 p0[4] = {ld(x0, ids.x), ld(x0, ids.y), ld(x0, ids.z), ld(x0, ids.w)};
+    d3 p1[4] = {ld(x1, ids.x), ld(x1, ids.y), ld(x1, ids.z), ld(x1, ids.w)};
+    const double tt = collision_time<KIND>(p0, p1, st);
+    if (tt < 1.0) store_toi(toi, tt);
+  }
+  if (st) atomicOr(status, st);
+}
+
 // ---------------------------------------------------------------- fixed bodies
 // frames at q, swept world boxes of the bodies over the step q -> q - dq, the
 // singular test at both ends, and the target-frame motion extent
@@ -888,15 +1012,50 @@ __global__ void __launch_bounds__(128) k_fixed_pt_collect(const S* __restrict__ 
   if (st) atomicOr(status, st);
 }
 
+// Candidate workspace: a 512-byte header (count, overflow flag, bucket counts
+// and cursors, work counter), then per staged pair its int2, its touch-time
+// bound (float) and the bucket order (int): 16 bytes a pair.
+constexpr size_t kCandHeader = 512;
+constexpr size_t kCandPerPair = sizeof(int2) + sizeof(float) + sizeof(int);
+
 inline CandList cand_list(void* ws, size_t ws_bytes) {
   CandList c;
   c.count = (int*)ws;
   c.overflow = (int*)ws + 1;
-  c.pairs = (int2*)((char*)ws + 256);
-  size_t cap = ws_bytes > 256 ? (ws_bytes - 256) / sizeof(int2) : 0;
+  c.pairs = (int2*)((char*)ws + kCandHeader);
+  size_t cap = ws_bytes > kCandHeader ? (ws_bytes - kCandHeader) / kCandPerPair : 0;
   c.capacity = cap > 0x7fffffff ? 0x7fffffff : (int)cap;
   return c;
 }
+
+inline CandOrder cand_order(void* ws, const CandList& c) {
+  CandOrder o;
+  int* h = (int*)ws;
+  o.bcount = h + 2;
+  o.bcursor = h + 2 + kBuckets;
+  o.work = h + 2 + 2 * kBuckets;
+  o.tlb = (float*)(c.pairs + c.capacity);
+  o.order = (int*)(o.tlb + c.capacity);
+  return o;
+}
+
+template <class S, int KIND>
+void solve_candidates(const S* x0, const S* x1, const int* prims, void* ws, const CandList& c, S* toi, int* status,
+                      const Sink& sink, cudaStream_t st) {
+  if (!c.capacity) return;
+  if (sink.on) {  // every pair that collides is a record: solve them all
+    const dim3 gc(min(div_up(c.capacity, 128), 2048));
+    k_cand_toi<S, KIND><<<gc, 128, 0, st>>>(x0, x1, prims, c, toi, status, sink, c.overflow);
+    return;
+  }
+  const CandOrder o = cand_order(ws, c);
+  cudaMemsetAsync(o.bcount, 0, (2 * kBuckets + 1) * sizeof(int), st);
+  const dim3 g256(div_up(c.capacity, 256));
+  k_cand_bound<S, KIND><<<g256, 256, 0, st>>>(x0, x1, prims, c, o, c.overflow);
+  k_cand_bucket<<<g256, 256, 0, st>>>(c, o, c.overflow);
+  k_cand_solve<S, KIND><<<148 * 3, 128, 0, st>>>(x0, x1, prims, c, o, toi, status, c.overflow);
+}
+
 
 __global__ void k_pair_time(int kind, int n, const double* __restrict__ a, const double* __restrict__ b,
                             double* __restrict__ t, int* status) {
@@ -934,16 +1093,12 @@ template <class S>
 void run_ee(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, const float* lower, const float* upper,
             int exclude, CandList c, void* toi, int* status, Sink sink, cudaStream_t st) {
   const int n = soup->n_edges;
-  // k_cand_toi is grid-stride: about 14 blocks of 128 per SM, so later pairs
-  // meet an already lowered TOI
-  const dim3 g(div_up(n, 128)), gc(min(div_up(c.capacity > 0 ? c.capacity : 1, 128), 2048));
+  const dim3 g(div_up(n, 128));
   cudaMemsetAsync(c.count, 0, 2 * sizeof(int), st);
   k_ee_collect<S, true><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->edges, soup->body,
                                            (const float4*)bvh->wide, bvh->sorted, n, lower, upper, exclude, c,
                                            (S*)toi, status, sink, nullptr);
-  if (c.capacity)
-    k_cand_toi<S, 0><<<gc, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->edges, c, (S*)toi, status, sink,
-                                         c.overflow);
+  solve_candidates<S, 0>((const S*)soup->x, (const S*)x1, soup->edges, c.count, c, (S*)toi, status, sink, st);
   CandList none = c;
   none.capacity = 0;
   k_ee_collect<S, false><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->edges, soup->body,
@@ -955,14 +1110,12 @@ template <class S>
 void run_pt(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, double pad, int exclude, CandList c,
             void* toi, int* status, Sink sink, cudaStream_t st) {
   const int nv = soup->n_verts;
-  const dim3 g(div_up(nv, 128)), gc(min(div_up(c.capacity > 0 ? c.capacity : 1, 128), 2048));
+  const dim3 g(div_up(nv, 128));
   cudaMemsetAsync(c.count, 0, 2 * sizeof(int), st);
   k_pt_collect<S, true><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->triangles, soup->body,
                                            (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude, c, (S*)toi,
                                            status, sink, nullptr);
-  if (c.capacity)
-    k_cand_toi<S, 1><<<gc, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->triangles, c, (S*)toi, status, sink,
-                                         c.overflow);
+  solve_candidates<S, 1>((const S*)soup->x, (const S*)x1, soup->triangles, c.count, c, (S*)toi, status, sink, st);
   CandList none = c;
   none.capacity = 0;
   k_pt_collect<S, false><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->triangles, soup->body,
@@ -1018,12 +1171,12 @@ int ipcb_swept_triangle_aabbs(const ipcb_soup* soup, const void* x1, double pad,
   return check_launch("ipcb_swept_triangle_aabbs");
 }
 
-size_t ipcb_toi_workspace(int capacity) { return 256 + (size_t)(capacity > 0 ? capacity : 0) * sizeof(int2); }
+size_t ipcb_toi_workspace(int capacity) { return kCandHeader + (size_t)(capacity > 0 ? capacity : 0) * kCandPerPair; }
 
 int ipcb_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, const float* lower,
                        const float* upper, int exclude_same_body, void* toi, int* status, void* ws, size_t ws_bytes,
                        ipcb_stream s) {
-  if (!soup || !x1 || !bvh || !lower || !upper || !toi || !status || !ws || ws_bytes < 256 ||
+  if (!soup || !x1 || !bvh || !lower || !upper || !toi || !status || !ws || ws_bytes < kCandHeader ||
       bvh->n != soup->n_edges)
     return IPCB_E_ARG;
   if (soup->n_edges == 0) return IPCB_OK;
@@ -1036,7 +1189,7 @@ int ipcb_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* b
 int ipcb_point_triangle_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, double pad,
                             int exclude_same_body, void* toi, int* status, void* ws, size_t ws_bytes,
                             ipcb_stream s) {
-  if (!soup || !x1 || !bvh || !toi || !status || !ws || ws_bytes < 256 || bvh->n != soup->n_tris)
+  if (!soup || !x1 || !bvh || !toi || !status || !ws || ws_bytes < kCandHeader || bvh->n != soup->n_tris)
     return IPCB_E_ARG;
   if (soup->n_verts == 0 || soup->n_tris == 0) return IPCB_OK;
   const CandList c = cand_list(ws, ws_bytes);
@@ -1048,7 +1201,7 @@ int ipcb_point_triangle_toi(const ipcb_soup* soup, const void* x1, const ipcb_lb
 int ipcb_edge_edge_intersections(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, const float* lower,
                                  const float* upper, int exclude_same_body, double thickness, void* toi,
                                  const ipcb_contacts* out, int* status, void* ws, size_t ws_bytes, ipcb_stream s) {
-  if (!soup || !x1 || !bvh || !lower || !upper || !toi || !out || !out->cnt || !status || !ws || ws_bytes < 256 ||
+  if (!soup || !x1 || !bvh || !lower || !upper || !toi || !out || !out->cnt || !status || !ws || ws_bytes < kCandHeader ||
       bvh->n != soup->n_edges)
     return IPCB_E_ARG;
   if (out->capacity > 0 && (!out->a1a2b1b2 || !out->e0e1 || !out->l0 || !out->alpha || !out->lam)) return IPCB_E_ARG;
@@ -1063,7 +1216,7 @@ int ipcb_edge_edge_intersections(const ipcb_soup* soup, const void* x1, const ip
 int ipcb_point_triangle_intersections(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, double pad,
                                       int exclude_same_body, double thickness, void* toi, const ipcb_contacts* out,
                                       int* status, void* ws, size_t ws_bytes, ipcb_stream s) {
-  if (!soup || !x1 || !bvh || !toi || !out || !out->cnt || !status || !ws || ws_bytes < 256 ||
+  if (!soup || !x1 || !bvh || !toi || !out || !out->cnt || !status || !ws || ws_bytes < kCandHeader ||
       bvh->n != soup->n_tris)
     return IPCB_E_ARG;
   if (out->capacity > 0 && (!out->a1a2b1b2 || !out->e0e1 || !out->l0 || !out->alpha || !out->lam)) return IPCB_E_ARG;
@@ -1120,7 +1273,7 @@ int ipcb_body_pairs_swept(const ipcb_bodies* B, int fp64, const void* q, const v
 int ipcb_fixed_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_bodies* B, const int* fixed,
                              const int* pairs, int n_pairs, double pad, void* toi, int* status, void* ws,
                              size_t ws_bytes, ipcb_stream s) {
-  if (!soup || !x1 || !bodies_ok(B) || !pairs || n_pairs < 0 || !toi || !status || !ws || ws_bytes < 256)
+  if (!soup || !x1 || !bodies_ok(B) || !pairs || n_pairs < 0 || !toi || !status || !ws || ws_bytes < kCandHeader)
     return IPCB_E_ARG;
   if (n_pairs == 0 || B->max_edges == 0) return IPCB_OK;
   cudaStream_t st = (cudaStream_t)s;
@@ -1147,7 +1300,7 @@ int ipcb_fixed_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_b
 int ipcb_fixed_point_triangle_toi(const ipcb_soup* soup, const void* x1, const ipcb_bodies* B, const int* pairs,
                                   int n_pairs, double pad, void* toi, int* status, void* ws, size_t ws_bytes,
                                   ipcb_stream s) {
-  if (!soup || !x1 || !bodies_ok(B) || !pairs || n_pairs < 0 || !toi || !status || !ws || ws_bytes < 256)
+  if (!soup || !x1 || !bodies_ok(B) || !pairs || n_pairs < 0 || !toi || !status || !ws || ws_bytes < kCandHeader)
     return IPCB_E_ARG;
   if (n_pairs == 0 || B->max_verts == 0) return IPCB_OK;
   cudaStream_t st = (cudaStream_t)s;

@@ -145,7 +145,9 @@ def test_new_intersections_with_a_small_candidate_list(cuda):
     a_full = s.new_intersections(x0, x1)
     ee_full, _ = _records(s.contacts_new, s.n_contacts)
     pt_full, _ = _records(s.contacts_pt, s.n_contacts_pt)
-    s._toi_ws = torch.empty(256 + 8 * 8, dtype=torch.uint8, device=cuda)
+    from ipc_warp_b200 import _native as N
+
+    s._toi_ws = torch.empty(N.size("ipcb_toi_workspace", 8), dtype=torch.uint8, device=cuda)  # 8 staged pairs
     a_small = s.new_intersections(x0, x1)
     assert a_small == a_full
     assert np.array_equal(_records(s.contacts_new, s.n_contacts)[0], ee_full)

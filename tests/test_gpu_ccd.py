@@ -113,10 +113,12 @@ def test_small_candidate_list_gives_the_same_toi(cuda, fp64):
     dxt = torch.tensor(dx, dtype=dtype, device=cuda)
     full = s.collision_free_step(dxt)
     toi_full = float(s.ccd_toi.item())
-    s._toi_ws = torch.empty(256 + 8 * 16, dtype=torch.uint8, device=cuda)  # 16 staged pairs
+    from ipc_warp_b200 import _native as N
+
+    s._toi_ws = torch.empty(N.size("ipcb_toi_workspace", 16), dtype=torch.uint8, device=cuda)  # 16 staged pairs
     small = s.collision_free_step(dxt)
     assert float(s.ccd_toi.item()) == toi_full and small == full
-    s._toi_ws = torch.empty(256, dtype=torch.uint8, device=cuda)  # nothing staged
+    s._toi_ws = torch.empty(N.size("ipcb_toi_workspace", 0), dtype=torch.uint8, device=cuda)  # nothing staged
     assert s.collision_free_step(dxt) == full
 
 
