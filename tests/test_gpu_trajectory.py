@@ -1,0 +1,60 @@
+"""The rod-twist configuration as a trajectory (gpu): 16 rods of 4x4x256 hex
+cells (5 tets/cell, 102,800 vertices) at 1.2 rod widths, ends clamped and
+counter-rotated at 2 rad/s, StVK (E = 1e6, nu = 0.45), dt = 5e-3, dhat =
+1e-3 rod width, 200 steps, in float32 and in float64 (the error oracle).
+
+After every step the surface is checked for edge-triangle crossings (none
+allowed), every step's Newton loop must end before its iteration cap with no
+refused CCD bound, and the rods must come into contact.  The float32 run's
+final positions are compared with the float64 run's; the difference is
+printed and bounded.
+
+The barrier stiffness is scaled to the barrier's energy scale: the IPC
+barrier in squared-distance form has energies of order kappa dhat^4, so with
+dhat = 1e-4 the reference's default kappa = 1e9 gives 1e-7 J -- far below the
+rods' elastic energy: the barrier then lets gaps collapse to the float32
+resolution of the positions and rounding the new positions crosses surfaces.
+kappa = 1e13 (kappa dhat^4 = 1e-3 J) keeps the gaps at a fraction of dhat.
+"""
+import numpy as np
+import pytest
+import torch
+
+from ipc_warp_b200 import scenes
+from ipc_warp_b200.newton import FEMContactSolver
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 200
+KAPPA = 1e13
+
+
+def _run(dtype):
+    sc = scenes.rod_bundle(n_rods_side=4, cells=(4, 4, 256), width=0.1, seed=1, kappa=KAPPA)
+    fixed, at = scenes.twist_targets(sc, omega=2.0)
+    s = FEMContactSolver(sc, material="stvk", E=1e6, nu=0.45, h=5e-3, fixed=fixed, gravity=(0.0, 0.0, 0.0),
+                         dtype=dtype, device="cuda", tol=1e-6, maxiter=20000, linear_solver="pcg",
+                         preconditioner="jacobi", max_newton=100)
+    s.boundary = at
+    assert s.edge_triangle_crossings()[0] == 0
+    max_contacts, iters = 0, []
+    for k in range(STEPS):
+        st = s.step()
+        n, pairs = s.edge_triangle_crossings(capacity=8)
+        assert n == 0, (k, pairs.cpu().numpy())
+        assert st.newton_iterations < s.max_newton, k
+        assert st.ccd_refusals == 0, k
+        iters.append(st.newton_iterations)
+        max_contacts = max(max_contacts, s.n_contacts + s.n_contacts_pt)
+    return s.states.x.double().cpu().numpy(), max_contacts, iters, np.ptp(sc.xcs, axis=0).max()
+
+
+def test_rod_twist_trajectory_float32_against_float64(cuda):
+    x32, c32, it32, extent = _run(torch.float32)
+    x64, c64, it64, _ = _run(torch.float64)
+    assert c32 > 0 and c64 > 0  # the rods touch
+    err = np.abs(x32 - x64).max()
+    print(f"rod twist, {STEPS} steps: float32 vs float64 max |dx| = {err:.3e} ({err / extent:.3e} of the "
+          f"extent); Newton iterations per step float32 max {max(it32)} mean {np.mean(it32):.2f}, float64 max "
+          f"{max(it64)} mean {np.mean(it64):.2f}; contacts up to {c32} / {c64}")
+    assert err <= 1e-3 * extent
