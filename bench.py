@@ -232,7 +232,8 @@ def stage_times(pipe, dx, reps, torch):
 
 
 # ------------------------------------------------------------- Newton step
-NEWTON_WORKLOAD = "rod_twist_16rods_4x4x256_wound_theta0.3_stvk_dt5e-3"
+NEWTON_WORKLOAD = "rod_twist_16rods_4x4x256_wound_theta0.3_stvk_dt5e-3_kappa1e13"
+NEWTON_KAPPA = 1e13
 
 
 def newton_solver(dev, torch, linear_solver: str, preconditioner: str, theta: float = 0.3):
@@ -244,6 +245,9 @@ def newton_solver(dev, torch, linear_solver: str, preconditioner: str, theta: fl
     from ipc_warp_b200.newton import FEMContactSolver
 
     sc = scene("rod_bundle")
+    # barrier stiffness scaled to dhat = 1e-4 (energies of order kappa dhat^4 = 1e-3 J);
+    # the pipeline workload's kappa does not change its work, but a Newton step needs it
+    sc.kappa = NEWTON_KAPPA
     fixed, at = scenes.twist_targets(sc, omega=2.0)
     s = FEMContactSolver(sc, material="stvk", E=1e6, nu=0.45, h=5e-3, fixed=fixed, gravity=(0.0, 0.0, 0.0),
                          dtype=torch.float32, device=dev, tol=1e-6, maxiter=20000, linear_solver=linear_solver,
