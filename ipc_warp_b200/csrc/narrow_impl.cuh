@@ -571,7 +571,10 @@ IPCB_D void hessian_from_warp(const S* __restrict__ x, const S* __restrict__ xcs
   S h[kMaxH][12], w[kMaxH];
   double fc[12];
   int nh = 0;
-  if (live) nh = hessian_terms<S, KIND>(x, xcs, id, l0, kappa, p, h, w, fc);
+  if (live) {
+    nh = hessian_terms<S, KIND>(x, xcs, id, l0, kappa, p, h, w, fc);
+    add_force<S>(bforce, id, fc);  // before the blocks: fc is not live while they are formed
+  }
   const long long base = (long long)(offset + i) * 16;
   const int4 rid = live ? id : make_int4(0, 0, 0, 0);
   if (active) {
@@ -617,7 +620,6 @@ IPCB_D void hessian_from_warp(const S* __restrict__ x, const S* __restrict__ xcs
     __syncwarp(full);
   }
   if (active && block_mask) block_mask[offset + i] = (unsigned short)mask;
-  if (live) add_force<S>(bforce, id, fc);
 }
 
 // One record of contact_hessian_ee / _pt: the float32 part, then the rest.
