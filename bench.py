@@ -158,9 +158,9 @@ def peaks():
 # record 24 + positions 48 + 16 triplets (4+4+36) 704 + force 48; EE adds rest positions 48
 NARROW_BYTES = {"pt": 824, "ee": 872}
 # dram__bytes_read.sum + dram__bytes_write.sum of the EE + PT narrow-phase
-# launches of one step (one-pass ncu capture of the full workload); None until
-# captured for the current kernels
-NARROW_DRAM_BYTES_PER_STEP = {"rod_bundle": 441.4e6, "screw_nut": None}
+# launches (k_contact_hessian_sorted) of one step: one-pass ncu capture of each
+# full workload
+NARROW_DRAM_BYTES_PER_STEP = {"rod_bundle": 464.2e6, "screw_nut": 169.6e6}
 
 
 def stage_times(pipe, dx, reps, torch):

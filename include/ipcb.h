@@ -388,6 +388,43 @@ int ipcb_abd_assemble(const ipcb_abd* abd, double h2, int n_records, int n_ee, c
                       void* values, void* gradient, int n_verts, const void* vertex_force, void* reduced_force,
                       int* status, ipcb_stream s);
 
+/* ---- Mixed FEM + affine-body systems (one Newton solve over tets and affine bodies) ----
+ * Unknowns q: n_fem FEM vertex positions, then p, a0, a1, a2 per affine body
+ * (the q layout of affine_body_dynamics.py:42-48).  Soup vertex v < n_fem is
+ * unknown v; vertex v >= n_fem belongs to body[v - n_fem] with body-local
+ * rest position rest[v] (x = p + A r); fixed bodies (fixed[b] != 0) have no
+ * unknowns.  rest: scalar[3 n_verts] (the soup's xcs). */
+typedef struct {
+  int fp64;
+  int n_fem;
+  int n_verts;
+  int n_bodies;
+  const int* body;  /* int32[n_verts - n_fem] */
+  const int* fixed; /* int32[n_bodies] */
+  const void* rest; /* scalar[3 n_verts] */
+} ipcb_mixed;
+/* x[v] = J_v q: the unknown itself (FEM) or the affine map (_sync_affine_vertices
+ * 42-48 on the body part); also maps a direction dq to the vertex direction. */
+int ipcb_mixed_map(const ipcb_mixed* m, const void* q, void* x, ipcb_stream s);
+/* gradient[unknowns] += scale J^T f (f: scalar[3 n_verts]); fixed bodies get nothing. */
+int ipcb_mixed_reduce_force(const ipcb_mixed* m, const void* vertex_force, double scale, void* gradient,
+                            ipcb_stream s);
+/* Contact Hessian triplets (16 per record, block_mask may be null) -> the
+ * unknown-space triplets of J^T H J times scale, written compactly; *n_out
+ * (device) = their count; IPCB_STATUS_PATTERN in *status when it exceeds
+ * capacity (grow to *n_out and rerun).  ws: ipcb_mixed_hessian_workspace bytes. */
+size_t ipcb_mixed_hessian_workspace(int n_src);
+int ipcb_mixed_reduce_hessian(const ipcb_mixed* m, int n_src, const int* rows, const int* cols, const void* vals,
+                              const unsigned short* block_mask, double scale, int capacity, int* drows, int* dcols,
+                              void* dvals, int* n_out, int* status, void* ws, size_t ws_bytes, ipcb_stream s);
+/* Pins (pendulum rods): body b's local point pin_rest[b] held at world point
+ * pin_target[b] by the energy 0.5 h2 pin_k[b] |x_pin - target|^2 (pin_k 0: no
+ * pin).  Optional outputs: 16 triplets per body (rows/cols/vals, all or none),
+ * gradient += (unknown layout), *energy += (double). */
+int ipcb_mixed_pins(const ipcb_mixed* m, const void* q, const void* pin_rest, const void* pin_target,
+                    const void* pin_k, double h2, int* rows, int* cols, void* vals, void* gradient, double* energy,
+                    ipcb_stream s);
+
 /* ---- Batched Newton terms and fixed-pattern assembly (time_integrator_base.py:403-426,
  * dynamic_contacts.py:275-297, fem/fem.py:139-203) ----
  * One persistent launch over all per-iteration terms: the EE records, the PT

@@ -23,7 +23,7 @@ OBJ_DIR = os.path.join(HERE, "csrc", "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["lbvh.cu", "dcd.cu", "narrow.cu", "ccd.cu", "bsr.cu", "contact_bsr.cu", "fem.cu", "umma_gemm.cu", "mpnn.cu", "pcg.cu",
-           "noalloc.cu", "abd.cu", "terms.cu", "linesearch.cu", "alset.cu", "intersect.cu"]
+           "noalloc.cu", "abd.cu", "terms.cu", "linesearch.cu", "alset.cu", "intersect.cu", "mixed.cu"]
 NOFMAD = {"ccd.cu"}
 DIRECT_SOURCES = ["direct.cu"]
 CUDA_LIB = "/usr/local/cuda/lib64"

@@ -61,6 +61,11 @@ class Abd(ctypes.Structure):
                 ("mass", P), ("volume", P), ("stiffness", P), ("fixed", P)]
 
 
+class Mixed(ctypes.Structure):
+    _fields_ = [("fp64", c_int), ("n_fem", c_int), ("n_verts", c_int), ("n_bodies", c_int), ("body", P),
+                ("fixed", P), ("rest", P)]
+
+
 class Graph(ctypes.Structure):
     _fields_ = [("n", c_int), ("nnz", c_int), ("n_lower", c_int), ("offsets", P), ("columns", P), ("rows", P),
                 ("rev", P), ("diag", P), ("lower", P)]
@@ -85,6 +90,7 @@ class Pcg(ctypes.Structure):
 SP, CP, BP = ctypes.POINTER(Soup), ctypes.POINTER(Contacts), ctypes.POINTER(Lbvh)
 BD = ctypes.POINTER(Bodies)
 AB = ctypes.POINTER(Abd)
+MX = ctypes.POINTER(Mixed)
 GP, TP = ctypes.POINTER(Graph), ctypes.POINTER(Tape)
 
 # name -> (restype, argtypes); every symbol here is declared in include/ipcb.h
@@ -173,6 +179,11 @@ SIGNATURES = {
     "ipcb_abd_pattern": (c_int, [c_int, P, P, c_int, P, P, P, P, P, c_int, P, P, P, P, P, c_size_t, P]),
     "ipcb_abd_assemble": (c_int, [AB, c_double, c_int, c_int, P, P, P, P, P, P, P, P, P, P, c_int, P, P, c_int, P, P,
                                   P, P]),
+    "ipcb_mixed_map": (c_int, [MX, P, P, P]),
+    "ipcb_mixed_reduce_force": (c_int, [MX, P, c_double, P, P]),
+    "ipcb_mixed_hessian_workspace": (c_size_t, [c_int]),
+    "ipcb_mixed_reduce_hessian": (c_int, [MX, c_int, P, P, P, P, c_double, c_int, P, P, P, P, P, P, c_size_t, P]),
+    "ipcb_mixed_pins": (c_int, [MX, P, P, P, P, c_double, P, P, P, P, P, P]),
     "ipcb_body_pairs": (c_int, [BD, c_int, P, c_double, P, c_int, P, P, P]),
     "ipcb_fixed_dcd_ee": (c_int, [SP, P, BD, P, c_int, c_float, CP, P, P]),
     "ipcb_fixed_dcd_pt": (c_int, [SP, P, BD, P, c_int, c_float, CP, P, P]),

@@ -11,6 +11,12 @@
 //   4. scan the per-row distinct counts -> offsets, nnz
 //   5. one warp per row: segmented reduction over the sorted entries, one
 //      3x3 block per distinct column
+// Rows longer than a warp's shared-memory sort (the 12 DOF rows of an affine
+// body collect every contact of the body: 1e4..1e5 entries) are listed by
+// step 3 and handled by one 1024-thread CTA each: a bitonic sort whose
+// stages below 4096 run on shared-memory chunks and whose longer strides
+// run in global memory, and an emit step whose 32 warps take equal slices of
+// the row (a warp owns the runs whose first entry lies in its slice).
 // Triplets whose block is all zero or whose index is outside the matrix are
 // dropped (warp's prune_numerical_zeros behaviour for the former).
 #include "common.cuh"
@@ -66,11 +72,12 @@ constexpr int kSortWarps = 4;      // warps (rows) per block in k_row_sort
 
 // Warp per row: sort the row's bucket by (col, id), keys distinct, then count
 // distinct columns.  Rows up to kRowCap entries use a bitonic network in
-// shared memory; longer rows rank each entry against the row in global memory.
+// shared memory; longer rows are appended to long_rows for k_row_sort_long.
 __global__ void __launch_bounds__(kSortWarps * 32) k_row_sort(int nrow, const int* __restrict__ cols,
                                                               const int* __restrict__ row_start,
                                                               int* __restrict__ bucket, int* __restrict__ tmp,
-                                                              int* __restrict__ row_nnz) {
+                                                              int* __restrict__ row_nnz, int* __restrict__ long_rows,
+                                                              int* __restrict__ n_long) {
   __shared__ unsigned long long sk[kSortWarps][kRowCap];
   const int wib = threadIdx.x >> 5;
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -100,13 +107,12 @@ __global__ void __launch_bounds__(kSortWarps * 32) k_row_sort(int nrow, const in
       }
     }
     for (int i = lane; i < L; i += 32) tmp[b + i] = (int)(unsigned)(k[i] & 0xffffffffULL);
-  } else {
-    for (int i = lane; i < L; i += 32) {
-      unsigned long long ki = ckey(cols, bucket[b + i]);
-      int rank = 0;
-      for (int j = 0; j < L; ++j) rank += ckey(cols, bucket[b + j]) < ki;
-      tmp[b + rank] = bucket[b + i];
+  } else {  // a long row: sorted and counted by k_row_sort_long
+    if (lane == 0) {
+      long_rows[atomicAdd(n_long, 1)] = warp;
+      row_nnz[warp] = 0;
     }
+    return;
   }
   __syncwarp();
   int distinct = 0;
@@ -136,6 +142,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_row_emit(int nrow, cons
   int lane = threadIdx.x & 31;
   if (warp >= nrow) return;
   int b = row_start[warp], e = row_start[warp + 1], L = e - b;
+  if (L > kRowCap) return;  // k_row_emit_long
   int out = offsets[warp];
   const unsigned le = 0xffffffffu >> (31 - lane);
   int runs_before = 0;  // heads in earlier chunks
@@ -186,6 +193,183 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_row_emit(int nrow, cons
   }
 }
 
+constexpr int kLongThreads = 1024;
+constexpr int kLongChunk = 4096;  // keys a CTA sorts in shared memory (32 KB)
+constexpr int kLongGrid = 148;    // CTAs over the long-row list (one per SM)
+
+IPCB_D void cas(unsigned long long* k, int i, int l, bool up) {
+  const unsigned long long a = k[i], c = k[l];
+  if ((a > c) == up) {
+    k[i] = c;
+    k[l] = a;
+  }
+}
+
+// the stages of stride < C of the bitonic merge sizes sz_lo..sz_hi, on each
+// C-key chunk of the row in shared memory (C = min(P, kLongChunk))
+IPCB_D void chunk_stages(unsigned long long* __restrict__ g, unsigned long long* __restrict__ sk, int P, int C,
+                         int sz_lo, int sz_hi) {
+  for (int c0 = 0; c0 < P; c0 += C) {
+    for (int i = threadIdx.x; i < C; i += kLongThreads) sk[i] = g[c0 + i];
+    __syncthreads();
+    for (int sz = sz_lo; sz <= sz_hi; sz <<= 1) {
+      for (int st = min(sz, C) >> 1; st > 0; st >>= 1) {
+        for (int i = threadIdx.x; i < C; i += kLongThreads) {
+          const int l = i ^ st;
+          if (l > i) cas(sk, i, l, ((c0 + i) & sz) == 0);
+        }
+        __syncthreads();
+      }
+    }
+    for (int i = threadIdx.x; i < C; i += kLongThreads) g[c0 + i] = sk[i];
+    __syncthreads();
+  }
+}
+
+// One CTA per long row (grid-stride over the list): bitonic sort of the
+// (col, id) keys padded to the power of two P >= L in lkeys (the row's region
+// [2 b, 2 b + P) lies inside [2 b, 2 b + 2 L), its own), then the sorted ids
+// back into the bucket and the distinct-column count into row_nnz.
+__global__ void __launch_bounds__(kLongThreads) k_row_sort_long(const int* __restrict__ long_rows,
+                                                                const int* __restrict__ n_long,
+                                                                const int* __restrict__ cols,
+                                                                const int* __restrict__ row_start,
+                                                                int* __restrict__ bucket,
+                                                                unsigned long long* __restrict__ lkeys,
+                                                                int* __restrict__ row_nnz) {
+  __shared__ unsigned long long sk[kLongChunk];
+  __shared__ int s_distinct;
+  const int n = *n_long;
+  for (int li = blockIdx.x; li < n; li += gridDim.x) {
+    const int r = long_rows[li];
+    const int b = row_start[r], L = row_start[r + 1] - b;
+    int P = 1;
+    while (P < L) P <<= 1;
+    const int C = P < kLongChunk ? P : kLongChunk;
+    unsigned long long* g = lkeys + 2LL * b;
+    for (int i = threadIdx.x; i < P; i += kLongThreads) g[i] = i < L ? ckey(cols, bucket[b + i]) : ~0ULL;
+    if (threadIdx.x == 0) s_distinct = 0;
+    __syncthreads();
+    chunk_stages(g, sk, P, C, 2, C);
+    for (int sz = 2 * C; sz <= P; sz <<= 1) {
+      for (int st = sz >> 1; st >= C; st >>= 1) {
+        for (int i = threadIdx.x; i < P; i += kLongThreads) {
+          const int l = i ^ st;
+          if (l > i) cas(g, i, l, (i & sz) == 0);
+        }
+        __syncthreads();
+      }
+      chunk_stages(g, sk, P, C, sz, sz);
+    }
+    int d = 0;
+    for (int i = threadIdx.x; i < L; i += kLongThreads) {
+      const unsigned long long k = g[i];
+      bucket[b + i] = (int)(unsigned)(k & 0xffffffffULL);
+      d += (i == 0 || (g[i - 1] >> 32) != (k >> 32)) ? 1 : 0;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+    if ((threadIdx.x & 31) == 0 && d) atomicAdd(&s_distinct, d);
+    __syncthreads();
+    if (threadIdx.x == 0) row_nnz[r] = s_distinct;
+    __syncthreads();
+  }
+}
+
+// One CTA per long row: warp w owns the runs whose first entry lies in its
+// slice [w L / 32, (w + 1) L / 32) and reduces them with the same segmented
+// scan as k_row_emit, reading past its slice end to finish its last run; a
+// block scan of the warps' run counts gives each warp's output position.
+template <class S>
+__global__ void __launch_bounds__(kLongThreads) k_row_emit_long(const int* __restrict__ long_rows,
+                                                                const int* __restrict__ n_long,
+                                                                const int* __restrict__ cols,
+                                                                const S* __restrict__ vals,
+                                                                const int* __restrict__ row_start,
+                                                                const int* __restrict__ bucket,
+                                                                const int* __restrict__ offsets,
+                                                                int* __restrict__ columns, S* __restrict__ values) {
+  __shared__ int s_runs[kLongThreads / 32];
+  const int n = *n_long;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nw = kLongThreads / 32;
+  for (int li = blockIdx.x; li < n; li += gridDim.x) {
+    const int r = long_rows[li];
+    const int b = row_start[r], L = row_start[r + 1] - b;
+    auto col_at = [&](int i) { return cols[bucket[b + i]]; };
+    auto is_head = [&](int i) { return i == 0 || col_at(i) != col_at(i - 1); };
+    // first head at or after the slice start (warp-parallel search)
+    auto first_head = [&](int from) {
+      for (int base = from; base < L; base += 32) {
+        const int i = base + lane;
+        const unsigned m = __ballot_sync(0xffffffffu, i < L && is_head(i));
+        if (m) return base + __ffs(m) - 1;
+      }
+      return L;
+    };
+    const int s0 = (int)((long long)L * w / nw), s1 = (int)((long long)L * (w + 1) / nw);
+    const int start = first_head(s0);
+    const int end = s1 >= L ? L : first_head(s1);
+    int heads = 0;
+    for (int base = start; base < end; base += 32) {
+      const int i = base + lane;
+      heads += __popc(__ballot_sync(0xffffffffu, i < end && is_head(i)));
+    }
+    if (lane == 0) s_runs[w] = heads;
+    __syncthreads();
+    int runs_before = 0;
+    for (int k = 0; k < w; ++k) runs_before += s_runs[k];
+    __syncthreads();
+    const int out = offsets[r];
+    const unsigned le = 0xffffffffu >> (31 - lane);
+    int prev_col = -1;
+    S carry[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) carry[q] = S(0);
+    for (int base = start; base < end; base += 32) {
+      const int i = base + lane;
+      const bool in = i < end;
+      const int t = in ? bucket[b + i] : 0;
+      const int c = in ? cols[t] : -1;
+      int cprev = __shfl_up_sync(0xffffffffu, c, 1);
+      if (lane == 0) cprev = base == start ? -1 : prev_col;
+      const bool head = in && (i == start || c != cprev);
+      int cnext = __shfl_down_sync(0xffffffffu, c, 1);
+      if (lane == 31) cnext = (i + 1 < end) ? cols[bucket[b + i + 1]] : -2;
+      const bool tail = in && (i == end - 1 || cnext != c);
+      S v[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) v[q] = in ? vals[9LL * t + q] : S(0);
+      if (lane == 0 && in && !head) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) v[q] = carry[q] + v[q];
+      }
+      int f = head ? 1 : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int nf = __shfl_up_sync(0xffffffffu, f, o);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+          const S nv = __shfl_up_sync(0xffffffffu, v[q], o);
+          if (lane >= o && !f) v[q] = nv + v[q];
+        }
+        if (lane >= o) f |= nf;
+      }
+      const unsigned hm = __ballot_sync(0xffffffffu, head);
+      const int u = runs_before + __popc(hm & le) - 1;
+      if (tail) {
+        columns[out + u] = c;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) values[9LL * (out + u) + q] = v[q];
+      }
+#pragma unroll
+      for (int q = 0; q < 9; ++q) carry[q] = __shfl_sync(0xffffffffu, v[q], 31);
+      prev_col = __shfl_sync(0xffffffffu, c, 31);
+      runs_before += __popc(hm);
+    }
+  }
+}
+
 __global__ void k_finish_offsets(int nrow, int* __restrict__ offsets, const int* __restrict__ total,
                                  int* __restrict__ nnz) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -229,18 +413,27 @@ int assemble(int nrow, int ncol, int n, const int* rows, const int* cols, const 
   int* total = (int*)p; p += 256;
   int* bucket = (int*)p; p += al(N * 4);
   int* tmp = (int*)p; p += al(N * 4);
+  int* long_rows = (int*)p; p += al(R * 4);
+  int* n_long = (int*)p; p += 256;
+  unsigned long long* lkeys = (unsigned long long*)p; p += al(2 * N * 8);
   void* scratch = p;
+  cudaMemsetAsync(n_long, 0, sizeof(int), st);
   cudaMemsetAsync(row_start, 0, R * sizeof(int), st);
   cudaMemsetAsync(cursor, 0, R * sizeof(int), st);
   int g = div_up(n, 256);
   k_row_count<S><<<g, 256, 0, st>>>(n, rows, cols, vals, nrow, ncol, row_start);
   scan::exclusive<int>(row_start, (int)R, scratch, total, st);  // row_start[nrow] = valid count
   k_row_scatter<S><<<g, 256, 0, st>>>(n, rows, cols, vals, nrow, ncol, row_start, cursor, bucket);
-  k_row_sort<<<div_up(nrow, kSortWarps), kSortWarps * 32, 0, st>>>(nrow, cols, row_start, bucket, tmp, offsets);
+  k_row_sort<<<div_up(nrow, kSortWarps), kSortWarps * 32, 0, st>>>(nrow, cols, row_start, bucket, tmp, offsets,
+                                                                     long_rows, n_long);
+  const int g_long = nrow < kLongGrid ? nrow : kLongGrid;
+  k_row_sort_long<<<g_long, kLongThreads, 0, st>>>(long_rows, n_long, cols, row_start, bucket, lkeys, offsets);
   scan::exclusive<int>(offsets, nrow, scratch, total, st);
   int gw = div_up(nrow, kWarpsPerBlock);
   k_finish_offsets<<<1, 32, 0, st>>>(nrow, offsets, total, nnz);
   k_row_emit<S><<<gw, kWarpsPerBlock * 32, 0, st>>>(nrow, cols, vals, row_start, bucket, offsets, columns, values);
+  k_row_emit_long<S><<<g_long, kLongThreads, 0, st>>>(long_rows, n_long, cols, vals, row_start, bucket, offsets,
+                                                      columns, values);
   return check_launch("ipcb_bsr_from_triplets");
 }
 
@@ -254,7 +447,7 @@ extern "C" {
 size_t ipcb_bsr_workspace(int n_trip, int nrow, int ncol) {
   (void)ncol;
   size_t R = (size_t)(nrow > 0 ? nrow : 0) + 1, N = (size_t)(n_trip > 0 ? n_trip : 1);
-  return 2 * al(R * 4) + 256 + 2 * al(N * 4) + scan::scratch_bytes((int)R);
+  return 3 * al(R * 4) + 512 + 2 * al(N * 4) + al(2 * N * 8) + scan::scratch_bytes((int)R);
 }
 
 int ipcb_bsr_from_triplets(int nrow, int ncol, int n_trip, const int* rows, const int* cols, const void* vals,
