@@ -426,14 +426,19 @@ int ipcb_mixed_pins(const ipcb_mixed* m, const void* q, const void* pin_rest, co
                     ipcb_stream s);
 
 /* ---- Batched Newton terms and fixed-pattern assembly (time_integrator_base.py:403-426,
- * dynamic_contacts.py:275-297, fem/fem.py:139-203) ----
+ * dynamic_contacts.py:275-297, fem/fem.py:139-203, affine_body_dynamics.py:88-141) ----
  * One persistent launch over all per-iteration terms: the EE records, the PT
- * records (counts read on the device: min(*cnt, capacity)) and the tets, in
- * that order, each with the outputs of ipcb_contact_hessian (EE at 0, PT at
- * offset n_ee) and ipcb_tet_hessian (t_rows/t_cols may be null); forces add
- * into `force`.  Work is taken from *queue (zeroed by the call) in tiles of
- * `tile` items per warp (a multiple of 32); blocks x threads (<= 128, multiple
- * of 32) is the persistent grid, with 145 * 32 scalars of shared memory per warp. */
+ * records (counts read on the device: min(*cnt, capacity)), the tets and the
+ * affine bodies' 16 (i, j) items, in that order, with the outputs of
+ * ipcb_contact_hessian_sorted (EE at 0, PT at offset n_ee; ee_ws / pt_ws are
+ * each list's ipcb_contact_hessian_workspace, the call runs the two ordering
+ * passes first), ipcb_tet_hessian (t_rows/t_cols may be null) and
+ * ipcb_abd_body_system (triplets a_rows/a_cols/a_vals, 16 per body, at rows
+ * body_row0 + 4 b + i; gradient rows written into a_grad; abd.n_bodies may
+ * be 0); forces add into `force`.  Work is taken from *queue (zeroed by the
+ * call) in tiles of `tile` items per warp (a multiple of 32); blocks x
+ * threads (<= 128, multiple of 32) is the persistent grid, with 145 * 32
+ * scalars of shared memory per warp. */
 typedef struct {
   int fp64;
   const void* x;
@@ -456,8 +461,18 @@ typedef struct {
   void* t_vals;
   void* force;
   int* queue;
+  void* ee_ws;
+  void* pt_ws;
+  ipcb_abd abd;
+  int body_row0;
+  double h2;
+  int* a_rows;
+  int* a_cols;
+  void* a_vals;
+  void* a_grad;
 } ipcb_terms;
-int ipcb_terms_launch(const ipcb_terms* terms, int blocks, int threads, int tile, ipcb_stream s);
+/* variant 0: the kernel's register budget allows 3 CTAs of 128 per SM; 1: 2 CTAs (255 registers) */
+int ipcb_terms_launch(const ipcb_terms* terms, int blocks, int threads, int tile, int variant, ipcb_stream s);
 /* slots[i] = position of block (rows[i], cols[i]) in a BSR pattern, -1 if absent */
 int ipcb_bsr_slots(int nrow, const int* offsets, const int* columns, int n, const int* rows, const int* cols,
                    int* slots, ipcb_stream s);

@@ -37,11 +37,18 @@ class Bodies(ctypes.Structure):
                 ("max_edges", c_int), ("max_tris", c_int), ("max_verts", c_int), ("frames", P), ("motion", P)]
 
 
+class Abd(ctypes.Structure):
+    _fields_ = [("n_bodies", c_int), ("fp64", c_int), ("q", P), ("q0", P), ("q_tilde", P), ("qdot", P), ("dx", P),
+                ("mass", P), ("volume", P), ("stiffness", P), ("fixed", P)]
+
+
 class Terms(ctypes.Structure):
     _fields_ = [("fp64", c_int), ("x", P), ("xcs", P), ("ee", Contacts), ("pt", Contacts), ("kappa", c_double),
                 ("c_rows", P), ("c_cols", P), ("c_vals", P), ("c_mask", P), ("material", c_int), ("tets", P),
                 ("n_tets", c_int), ("Bm", P), ("W", P), ("mu", c_double), ("lam", c_double), ("t_rows", P),
-                ("t_cols", P), ("t_vals", P), ("force", P), ("queue", P)]
+                ("t_cols", P), ("t_vals", P), ("force", P), ("queue", P), ("ee_ws", P), ("pt_ws", P),
+                ("abd", Abd), ("body_row0", c_int), ("h2", c_double), ("a_rows", P), ("a_cols", P), ("a_vals", P),
+                ("a_grad", P)]
 
 
 class LsState(ctypes.Structure):
@@ -54,11 +61,6 @@ class AlSet(ctypes.Structure):
     _fields_ = [("table_size", c_int), ("capacity", c_int), ("cell_start", P), ("a1a2b1b2", P), ("e0e1", P),
                 ("l0", P), ("alpha", P), ("lam", P), ("gamma", P), ("slack", P), ("mollifier", P), ("d0", P),
                 ("distance_type", P), ("grad", P)]
-
-
-class Abd(ctypes.Structure):
-    _fields_ = [("n_bodies", c_int), ("fp64", c_int), ("q", P), ("q0", P), ("q_tilde", P), ("qdot", P), ("dx", P),
-                ("mass", P), ("volume", P), ("stiffness", P), ("fixed", P)]
 
 
 class Mixed(ctypes.Structure):
@@ -144,7 +146,7 @@ SIGNATURES = {
     "ipcb_pcg_iterate": (c_int, [ctypes.POINTER(Pcg), c_int, P]),
     "ipcb_block_jacobi": (c_int, [c_int, P, P, P, P, c_int, P, P, P]),
     "ipcb_fsai_mirror": (c_int, [GP, P, P, P]),
-    "ipcb_terms_launch": (c_int, [ctypes.POINTER(Terms), c_int, c_int, c_int, P]),
+    "ipcb_terms_launch": (c_int, [ctypes.POINTER(Terms), c_int, c_int, c_int, c_int, P]),
     "ipcb_bsr_slots": (c_int, [c_int, P, P, c_int, P, P, P, P]),
     "ipcb_bsr_union_workspace": (c_size_t, [c_int]),
     "ipcb_bsr_union": (c_int, [c_int, P, P, P, P, P, P, P, P, P, c_int, P, P, P, c_size_t, P]),

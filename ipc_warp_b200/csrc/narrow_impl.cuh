@@ -622,6 +622,103 @@ IPCB_D void hessian_from_warp(const S* __restrict__ x, const S* __restrict__ xcs
   if (active && block_mask) block_mask[offset + i] = (unsigned short)mask;
 }
 
+// ---- class-sorted path: the records of the whole list are put in cost-class
+// order (most expensive first) before the Hessian kernel, so nearly every
+// warp runs one path.  The ordering pass also copies each record's float32
+// part, vertex ids and l0 to its sorted position, so the Hessian kernel reads
+// its inputs coalesced and only the positions are gathered.  Workspace:
+// [class counts int[4] | cursors int[4] | pad to 256 B | float4 pre[cap] |
+// int order[cap] | float4 sorted pre[cap] | int4 sorted ids[cap] | S sorted
+// l0[cap]], each array 256-byte aligned.
+template <class S, int KIND>
+__global__ void __launch_bounds__(256) k_classify(const S* __restrict__ x, const S* __restrict__ xcs, ipcb_contacts L,
+                                                  int n, float4* __restrict__ pre, int* __restrict__ counts) {
+  __shared__ int sc[4];
+  const int cnt = list_count<S>(L, n);
+  if ((int)(blockIdx.x * blockDim.x) >= cnt) return;  // the whole block
+  if (threadIdx.x < 4) sc[threadIdx.x] = 0;
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < cnt) {
+    const int4 id = __ldg(reinterpret_cast<const int4*>(L.a1a2b1b2) + i);
+    const S l0 = static_cast<const S*>(L.l0)[i];
+    const v3<S> xs[4] = {ldx(x, id.x), ldx(x, id.y), ldx(x, id.z), ldx(x, id.w)};
+    const Pre p = predicate<S, KIND>(xcs, id, l0, xs);
+    pre[i] = pack(p);
+    atomicAdd(&sc[p.cls()], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x < 4 && sc[threadIdx.x]) atomicAdd(counts + threadIdx.x, sc[threadIdx.x]);
+}
+
+template <class S>
+struct Sorted {
+  float4* pre;
+  int* order;
+  float4* spre;
+  int4* sids;
+  S* sl0;
+};
+
+// host side: the device addresses of the workspace's arrays
+template <class S>
+inline Sorted<S> sorted_ws(void* ws, int capacity) {
+  const size_t c = (size_t)(capacity < 1 ? 1 : capacity);
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+  char* p = (char*)ws + 256;
+  Sorted<S> r;
+  r.pre = (float4*)p;
+  p += al(c * 16);
+  r.order = (int*)p;
+  p += al(c * 4);
+  r.spre = (float4*)p;
+  p += al(c * 16);
+  r.sids = (int4*)p;
+  p += al(c * 16);
+  r.sl0 = (S*)p;
+  return r;
+}
+
+template <class S>
+__global__ void __launch_bounds__(256) k_class_order(ipcb_contacts L, int n, const int* __restrict__ counts,
+                                                     int* __restrict__ cursor, Sorted<S> W) {
+  __shared__ int sc[4], sbase[4];
+  const int cnt = list_count<S>(L, n);
+  if ((int)(blockIdx.x * blockDim.x) >= cnt) return;
+  if (threadIdx.x < 4) sc[threadIdx.x] = 0;
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int cls = -1, local = 0;
+  float4 pr = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (i < cnt) {
+    pr = W.pre[i];
+    cls = __float_as_int(pr.w) & 3;
+    local = atomicAdd(&sc[cls], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    // classes in the order 3, 2, 1, 0: the costliest records start first
+    const int k = threadIdx.x;
+    int start = 0;
+    for (int c = 3; c > k; --c) start += counts[c];
+    sbase[k] = sc[k] ? start + atomicAdd(cursor + k, sc[k]) : 0;
+  }
+  __syncthreads();
+  if (cls >= 0) {
+    const int pos = sbase[cls] + local;
+    W.order[pos] = i;
+    W.spre[pos] = pr;
+    W.sids[pos] = __ldg(reinterpret_cast<const int4*>(L.a1a2b1b2) + i);
+    W.sl0[pos] = static_cast<const S*>(L.l0)[i];
+  }
+}
+
+inline size_t sorted_workspace(int capacity) {
+  const size_t c = (size_t)(capacity < 1 ? 1 : capacity);
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+  return 256 + al(c * 16) + al(c * 4) + al(c * 16) + al(c * 16) + al(c * 8);
+}
+
 // One record of contact_hessian_ee / _pt: the float32 part, then the rest.
 template <class S, int KIND>
 IPCB_D void contact_hessian_item(const S* __restrict__ x, const S* __restrict__ xcs, const ipcb_contacts& L, int i,

@@ -180,6 +180,20 @@ class DevicePcg:
         return B["x"], st.it, rel, st.status
 
 
+def terms_candidates() -> list[tuple]:
+    """Schedules of the per-iteration terms: the per-kind kernels back to
+    back ("separate"), or the one persistent work-queue launch
+    (ipcb_terms_launch) as (register variant, blocks per SM, threads, tile)."""
+    shapes = [(0, bps, 128) for bps in (1, 2, 3)] + [(1, bps, 128) for bps in (1, 2)] + \
+        [(v, 4, 64) for v in (0, 1)]
+    return [("separate",)] + [(v, bps, th, tile) for (v, bps, th) in shapes for tile in (32, 64, 128)]
+
+
+def launch_terms(Tc, cfg, n_sm: int):
+    variant, bps, threads, tile = cfg
+    N.call("ipcb_terms_launch", ctypes.byref(Tc), bps * n_sm, threads, tile, variant, N.stream_handle())
+
+
 class FEMContactSolver(ContactBarrierMixin):
     """Deformable bodies (tet FEM) with IPC contact: RodComplexBC on the GPU."""
 
@@ -368,12 +382,13 @@ class FEMContactSolver(ContactBarrierMixin):
                             ws=torch.empty(N.size("ipcb_bsr_union_workspace", V), dtype=torch.uint8, device=dev))
         n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
         self._n_sm = n_sm
-        # schedules: the per-kind kernels back to back, or the one persistent
-        # work-queue launch at a (blocks/SM, threads, tile) shape; the fastest
-        # per workload bucket wins
-        cands = [("separate",)] + [(bps, th, tile) for (bps, th) in ((1, 128), (2, 128), (2, 64), (4, 64))
-                                   for tile in (32, 64, 128, 256)]
-        self._tuner = Autotuner("terms", cands)
+        self._tuner = Autotuner("terms", terms_candidates())
+
+    def _sorted_workspaces(self):
+        """Device workspaces of the class-sorted narrow phase, one per list."""
+        self._ws_ee = hessian_workspace(self.contacts_new, getattr(self, "_ws_ee", None))
+        self._ws_pt = hessian_workspace(self.contacts_pt, getattr(self, "_ws_pt", None))
+        return N.ptr(self._ws_ee), N.ptr(self._ws_pt)
 
     def _launch_terms(self, cfg, Tc):
         s = N.stream_handle()
@@ -392,8 +407,7 @@ class FEMContactSolver(ContactBarrierMixin):
                    N.ptr(self.tets), self.n_tets, N.ptr(self.Bm), N.ptr(self.W), self.mu, self.lam, None, None,
                    N.ptr(self._static["tet_vals"]), N.ptr(self.b), s)
             return
-        bps, threads, tile = cfg
-        N.call("ipcb_terms_launch", ctypes.byref(Tc), bps * self._n_sm, threads, tile, s)
+        launch_terms(Tc, cfg, self._n_sm)
 
     def _compute_A_queue(self) -> BsrMatrix:
         """Contact detection, then one persistent launch for the contact
@@ -416,7 +430,7 @@ class FEMContactSolver(ContactBarrierMixin):
                      self.contacts_new.c_struct(), self.contacts_pt.c_struct(), float(self.contact_stiffness),
                      N.ptr(t.rows), N.ptr(t.cols), N.ptr(t.vals), N.ptr(t.mask), self.material, N.ptr(self.tets),
                      self.n_tets, N.ptr(self.Bm), N.ptr(self.W), self.mu, self.lam, None, None, N.ptr(st["tet_vals"]),
-                     N.ptr(self.b), N.ptr(st["queue"]))
+                     N.ptr(self.b), N.ptr(st["queue"]), *self._sorted_workspaces())
         key = (int(self.dtype == torch.float64), bucket(n_ee + n_pt), bucket(self.n_tets))
         cfg = self._tuner.pick(key, lambda c: self._launch_terms(c, Tc), self.b.zero_)
         self._launch_terms(cfg, Tc)

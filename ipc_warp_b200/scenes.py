@@ -479,3 +479,111 @@ def screw_direction(sc: Scene, omega: float = 4.0, dt: float = 2e-3, seed: int =
     dx = x - x1
     dx += rng.normal(scale=0.05 * sc.dhat, size=dx.shape)
     return dx
+
+
+# --------------------------------------------- mixed affine + FEM wrecking balls
+@dataclass
+class MixedScene:
+    """Deformable tet bodies and affine bodies in one scene.
+
+    ``fem``: the tet bodies as a :class:`Scene` (vertices, tets, surface, body
+    ids).  ``bodies``: per affine body its world vertices (n, 3) and
+    outward faces (m, 3); ``fixed_bodies`` never move (the ground).
+    ``pins``: body -> (world point on the body at rest, world target,
+    stiffness), a pendulum rod as a quadratic penalty.  ``velocities``:
+    body -> (linear, angular) initial velocity."""
+    name: str
+    fem: Scene
+    bodies: list
+    fixed_bodies: list
+    pins: dict
+    velocities: dict
+    dhat: float
+    kappa: float
+    meta: dict = field(default_factory=dict)
+
+
+def ground_grid(quads: int, extent: float, origin=(0.0, 0.0, 0.0)):
+    """A flat square of quads x quads quads (2 triangles each) spanning
+    [0, extent]^2 in x-z at height origin[1], faces pointing up (+y)."""
+    n = quads + 1
+    g = np.linspace(0.0, extent, n)
+    X, Z = np.meshgrid(g, g, indexing="ij")
+    v = np.column_stack([X.ravel(), np.zeros(n * n), Z.ravel()]) + np.asarray(origin, np.float64)
+    i, j = np.meshgrid(np.arange(quads), np.arange(quads), indexing="ij")
+    a = (i * n + j).ravel()
+    b, c, d = a + n, a + n + 1, a + 1
+    # (a, d, c) and (a, c, b): counter-clockwise seen from +y
+    f = np.concatenate([np.column_stack([a, d, c]), np.column_stack([a, c, b])])
+    return v, f.astype(np.int64)
+
+
+def wrecking_balls(n_balls: int = 64, subdiv: int = 4, radius: float = 0.5, rope: float = 1.0,
+                   max_angle_deg: float = 60.0, stack=(2, 2, 2), cube_cells: int = 4, cube_size: float = 0.25,
+                   ground_quads: int = 100, station: float = 3.0, dhat: float = 1e-3, kappa: float = 1e10,
+                   pin_stiffness: float = 1e9, seed: int = 0) -> MixedScene:
+    """Batched affine + FEM wrecking balls: ``n_balls`` affine icospheres
+    (subdiv 4: 2562 vertices, 5120 triangles; radius 0.5) on pendulum pins,
+    each released from rest at a seeded angle uniform in [0, max_angle_deg]
+    towards a stack of FEM cubes (``stack`` cubes of cube_cells^3 hex cells,
+    5 tets/cell; 64 balls x 2x2x2 = 512 cubes) that rests on a fixed ground
+    of ground_quads^2 quads.  Each ball has its own station on a square
+    grid ``station`` apart; at the bottom of its swing the ball's centre is
+    ``radius + 0.05`` above the ground and 0.01 in front of its stack.
+    Neighbouring cubes and the lowest layer and the ground start 1.5 dhat
+    apart, inside the barrier."""
+    rng = np.random.default_rng(seed)
+    side = int(np.ceil(np.sqrt(n_balls)))
+    gap = 1.5 * dhat
+    ball_v, ball_f = icosphere(subdiv, radius)
+    cubes, bodies, pins, velocities = [], [], {}, {}
+    sx, sy, sz = stack
+    pitch = cube_size + gap
+    for k in range(n_balls):
+        cx, cz = (k // side) * station + 0.5 * station, (k % side) * station + 0.5 * station
+        low = radius + 0.05
+        pivot = np.array([cx, low + rope, cz])
+        th = np.radians(rng.uniform(0.0, max_angle_deg))
+        centre = pivot + rope * np.array([-np.sin(th), -np.cos(th), 0.0])
+        R = transform(rng.uniform(0, 360, 3))[:3, :3]
+        bodies.append((ball_v @ R.T + centre, ball_f.copy()))
+        pins[k] = (pivot.copy(), pivot.copy(), float(pin_stiffness))
+        x0 = cx + radius + 0.01
+        for a in range(sx):
+            for b in range(sy):
+                for c in range(sz):
+                    m = hex_grid_tets(cube_cells, cube_cells, cube_cells, size=(cube_size,) * 3)
+                    m.x = m.x + np.array([x0 + a * pitch, gap + b * pitch, cz - 0.5 * sz * pitch + c * pitch])
+                    cubes.append(m)
+    extent = side * station
+    bodies.append(ground_grid(ground_quads, extent))
+    fem = assemble(cubes, "wrecking_cubes", dhat, kappa)
+    return MixedScene(name=f"wrecking_balls_{n_balls}", fem=fem, bodies=bodies, fixed_bodies=[len(bodies) - 1],
+                      pins=pins, velocities=velocities, dhat=float(dhat), kappa=float(kappa),
+                      meta={"radius": radius, "rope": rope, "cube_size": cube_size, "stack": tuple(stack),
+                            "ground_quads": ground_quads})
+
+
+def mixed_touching(subdiv: int = 1, radius: float = 0.5, cube_cells: int = 2, cube_size: float = 1.0,
+                   dhat: float = 1e-3, gap_over_dhat: float = 0.6, kappa: float = 1e8, ground_quads: int = 4,
+                   pin_stiffness: float = 1e6) -> MixedScene:
+    """A small mixed scene with every kind of body pair inside the barrier:
+    two affine balls side by side, a FEM cube beside the first, all resting
+    on a fixed ground, every facing gap ``gap_over_dhat`` dhat (measured
+    between the meshes' extreme vertices).  Ball 0 hangs on a pin at its
+    top.  Body pairs: ball-ball, ball-cube, ball-ground, cube-ground."""
+    g = gap_over_dhat * dhat
+    v, f = icosphere(subdiv, radius)
+    lo = v.min(axis=0)
+    hi = v.max(axis=0)
+    a = v - np.array([0.0, lo[1] - g, 0.0])                 # resting g above y = 0
+    b = a + np.array([hi[0] - lo[0] + g, 0.0, 0.0])          # g to the right of ball 0
+    cube = hex_grid_tets(cube_cells, cube_cells, cube_cells, size=(cube_size,) * 3)
+    cube.x = cube.x + np.array([a[:, 0].min() - g - cube_size, g, -0.5 * cube_size])
+    span = 4.0 * (radius + cube_size)
+    ground = ground_grid(ground_quads, span, origin=(-0.5 * span, 0.0, -0.5 * span))
+    fem = assemble([cube], "touching_cube", dhat, kappa)
+    top = a.mean(axis=0) + np.array([0.0, radius, 0.0])
+    return MixedScene(name="mixed_touching", fem=fem, bodies=[(a, f.copy()), (b, f.copy()), ground],
+                      fixed_bodies=[2], pins={0: (top, top.copy(), float(pin_stiffness))}, velocities={},
+                      dhat=float(dhat), kappa=float(kappa), meta={})

@@ -45,6 +45,47 @@ def test_bsr_from_triplets(cuda, n_trip, nrow, fp64):
     assert np.abs(y - yref).max() <= (1e-10 if fp64 else 1e-4) * max(np.abs(yref).max(), 1.0)
 
 
+@pytest.mark.parametrize("lengths", [(1025, 2048, 3000), (5000, 70_000, 4097), (300_000,)])
+@pytest.mark.parametrize("fp64", [False, True])
+def test_bsr_long_rows(cuda, lengths, fp64):
+    """Rows longer than a warp's shared-memory sort (the unknown rows of an
+    affine body collect all its contacts) go through the CTA-per-row sort
+    and emit; mixed with ordinary short rows."""
+    rng = np.random.default_rng(sum(lengths))
+    dt = np.float64 if fp64 else np.float32
+    nrow = 4000
+    rows, cols = [], []
+    for k, L in enumerate(lengths):
+        r = 7 + 113 * k
+        rows.append(np.full(L, r))
+        # many duplicate columns, a few runs longer than a warp's slice
+        cols.append(np.concatenate([rng.integers(0, nrow, size=L - L // 4), np.full(L // 4, r)]))
+    rows.append(rng.integers(0, nrow, size=20_000))
+    cols.append(np.clip(rows[-1] + rng.integers(-3, 4, size=20_000), 0, nrow - 1))
+    rows = np.concatenate(rows).astype(np.int32)
+    cols = np.concatenate(cols).astype(np.int32)
+    perm = rng.permutation(len(rows))
+    rows, cols = rows[perm], cols[perm]
+    vals = rng.normal(size=(len(rows), 3, 3)).astype(dt)
+    vals[::11] = 0.0
+    tr = lambda a: torch.tensor(a, device=cuda)  # noqa: E731
+    A = bsr_from_triplets(nrow, nrow, tr(rows), tr(cols), tr(vals))
+    ref = scipy_from_triplets(nrow, nrow, rows, cols, vals)
+    keep = np.any(vals != 0, axis=(1, 2))
+    uniq = np.unique(rows[keep].astype(np.int64) * nrow + cols[keep])
+    assert A.nnz_sync() == len(uniq)
+    offs = A.offsets.cpu().numpy()
+    colsA = A.columns[: len(uniq)].cpu().numpy()
+    for k in range(len(lengths)):
+        r = 7 + 113 * k
+        assert np.all(np.diff(colsA[offs[r]:offs[r + 1]]) > 0)
+    d = A.to_scipy().tocsr() - ref
+    tol = 1e-12 if fp64 else 1e-5
+    assert (abs(d).max() if d.nnz else 0.0) <= tol * max(abs(ref).max(), 1.0) * (np.sqrt(max(lengths)) / 10 + 1)
+    B = bsr_from_triplets(nrow, nrow, tr(rows), tr(cols), tr(vals))
+    assert torch.equal(A.values[: A.nnz_sync()], B.values[: B.nnz_sync()])
+
+
 @pytest.mark.parametrize("idx", range(4))
 @pytest.mark.parametrize("fp64", [False, True])
 def test_contact_bsr_equals_generic_assembly(cuda, idx, fp64):

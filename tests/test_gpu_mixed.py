@@ -1,0 +1,158 @@
+"""Mixed FEM + affine-body Newton system (ipc_warp_b200.mixed, csrc/mixed.cu)
+against the CPU oracle oracle/mixed.py, and short trajectories of the
+wrecking-balls configuration that must stay intersection-free (gpu)."""
+import numpy as np
+import pytest
+import torch
+
+from ipc_warp_b200 import contact, scenes
+from ipc_warp_b200.mixed import MixedSolver
+from oracle import mixed as om
+from oracle import newton as on
+
+pytestmark = pytest.mark.gpu
+
+DTYPES = [torch.float32, torch.float64]
+TOL = {torch.float32: 1e-5, torch.float64: 1e-10}
+
+
+def _host(t):
+    return t.double().cpu().numpy()
+
+
+def _oracle(s: MixedSolver):
+    V = s.n_verts
+    p = on.Problem(xcs=_host(s.soup.xcs), tets=s.tets.cpu().numpy(), edges=s.soup.edges.cpu().numpy().reshape(-1, 2),
+                   triangles=s.soup.triangles.cpu().numpy().reshape(-1, 3), body=s.soup.body.cpu().numpy(),
+                   mass=np.zeros(V), fixed=np.zeros(V, bool), x_target=np.zeros((V, 3)), material=s.material,
+                   mu=s.mu, lam=s.lam, dhat=2.0 * contact._thickness, kappa=s.contact_stiffness, h=s.h, k_att=0.0,
+                   gravity=np.zeros(3), fp64=s.dtype == torch.float64, exclude_same_body=s.disable_self_collision)
+    m = om.Mixed(n_fem=s.n_fem, body=s.body_local.cpu().numpy(), fixed=s.abd_fixed.cpu().numpy(),
+                 rest=_host(s.soup.xcs), fem_mass=_host(s.fem_mass), M=_host(s.abd_mass).reshape(-1, 4, 4),
+                 volume=_host(s.abd_volume), stiffness=_host(s.abd_stiffness), pin_rest=_host(s.pin_rest),
+                 pin_target=_host(s.pin_target), pin_k=_host(s.pin_k))
+    return p, m
+
+
+def _solver(dtype, assembly="queue", affine_stiffness=1e5, **kw):
+    sc = scenes.mixed_touching(**kw)
+    return MixedSolver(sc, E=1e5, nu=0.4, h=1e-2, dtype=dtype, affine_stiffness=affine_stiffness, maxiter=2000,
+                       assembly=assembly)
+
+
+def _perturb(s: MixedSolver, seed, scale=2e-5):
+    rng = np.random.default_rng(seed)
+    q = _host(s.q)
+    d = scale * rng.normal(size=q.shape)
+    fixed = _host(s.abd_fixed).astype(bool)
+    for b in np.flatnonzero(fixed):
+        o = s.n_fem + 4 * b
+        d[o:o + 4] = 0
+    s.q.copy_(torch.tensor(q + d, dtype=s.dtype))
+    s._sync()
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_mixed_system_matches_oracle(cuda, dtype):
+    s = _solver(dtype)
+    _perturb(s, 1)
+    A = s.compute_A()
+    n_ee, n_pt = s.n_contacts, s.n_contacts_pt
+    assert n_ee + n_pt > 0
+    p, m = _oracle(s)
+    g_ref, A_ref, ne, npt = om.system(p, m, _host(s.q), _host(s.xt_f), _host(s.qt_a), x=_host(s.x))
+    assert (ne, npt) == (n_ee, n_pt)
+    # every body pair of the scene is in contact: ball-ball, ball-cube, ball-ground, cube-ground
+    body = s.soup.body.cpu().numpy()
+    recs = np.concatenate([s.contacts_new.records(n_ee)[:, :4].cpu().numpy(),
+                           s.contacts_pt.records(n_pt)[:, :4].cpu().numpy()])
+    pairs = {tuple(sorted(set(body[r].tolist()))) for r in recs}
+    assert {(1, 2), (0, 1), (1, 3), (2, 3), (0, 3)} <= pairs, pairs
+    Ad = A.to_scipy().toarray()
+    Ar = A_ref.toarray()
+    assert np.abs(Ad - Ar).max() <= TOL[dtype] * np.abs(Ar).max() * 10
+    g = _host(s.rhs)
+    assert np.abs(g - g_ref).max() <= TOL[dtype] * np.abs(g_ref).max() * 10
+    # the matrix is symmetric and its coupling blocks between the cube's
+    # unknowns and ball 0's are non-zero
+    assert np.abs(Ad - Ad.T).max() <= TOL[dtype] * np.abs(Ad).max() * 10
+    o = 3 * s.n_fem
+    assert np.abs(Ad[:o, o:o + 12]).max() > 0
+
+
+@pytest.mark.parametrize("cfg", [(0, 2, 128, 64), (1, 1, 128, 32), (0, 4, 64, 32)])
+def test_fused_terms_equal_per_kind_kernels(cuda, cfg):
+    """The persistent launch over contact records, tets and affine-body items
+    assembles the same matrix and gradient as the per-kind kernels."""
+    out = []
+    for assembly in ("separate", "queue"):
+        s = _solver(torch.float64, assembly=assembly)
+        _perturb(s, 3)
+        if assembly == "queue":
+            s._tuner.pick = lambda key, run, reset: cfg
+        A = s.compute_A()
+        assert s.n_contacts + s.n_contacts_pt > 0
+        out.append((A.to_scipy().toarray(), _host(s.rhs)))
+    (A0, g0), (A1, g1) = out
+    assert np.abs(A1 - A0).max() <= 1e-12 * np.abs(A0).max()
+    assert np.abs(g1 - g0).max() <= 1e-11 * np.abs(g0).max()
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_mixed_energy_matches_oracle(cuda, dtype):
+    s = _solver(dtype)
+    _perturb(s, 2)
+    e = s.total_energy()
+    p, m = _oracle(s)
+    ref = om.energy(p, m, _host(s.q), _host(s.xt_f), _host(s.qt_a), x=_host(s.x))
+    # float32: the body inertia and orthogonality sums run in float (as
+    # test_gpu_abd's energies), so the bound is theirs
+    assert abs(e - ref) <= (1e-4 if dtype == torch.float32 else 1e-10) * abs(ref) + 1e-12
+
+
+def test_mixed_newton_steps_rest(cuda):
+    """The touching scene under gravity: Newton converges every step, no
+    surface crossing, the pinned ball stays rigid, the ground does not move."""
+    s = _solver(torch.float64, affine_stiffness=1e8)
+    q0 = _host(s.q)
+    ground = s.n_fem + 4 * 2
+    for k in range(5):
+        st = s.step()
+        assert st.newton_iterations < s.max_newton, k
+        assert st.ccd_refusals == 0
+        assert s.edge_triangle_crossings()[0] == 0, k
+    q = _host(s.q)
+    assert np.isfinite(q).all()
+    assert np.abs(q[ground:ground + 4] - q0[ground:ground + 4]).max() == 0.0
+    assert s.orthogonality_error() < 1e-3
+
+
+def test_wrecking_balls_trajectory(cuda):
+    """Four balls of the wrecking-balls configuration, released at seeded
+    angles, strike their cube stacks: every step converges, no surface
+    crossing, the balls stay rigid, the ground stays put, and the balls
+    end up touching the cubes (affine-FEM contact records)."""
+    sc = scenes.wrecking_balls(n_balls=4, subdiv=3, cube_cells=3, ground_quads=16, max_angle_deg=60.0,
+                               kappa=1e10, seed=2)
+    s = MixedSolver(sc, E=5e5, nu=0.4, h=1e-2, dtype=torch.float32, maxiter=2000)
+    q0 = _host(s.q)
+    n_fem_bodies = int(sc.fem.body.max()) + 1
+    body = s.soup.body.cpu().numpy()
+    hit = False
+    for k in range(60):
+        st = s.step()
+        assert st.newton_iterations < s.max_newton, k
+        assert st.ccd_refusals == 0, k
+        assert s.edge_triangle_crossings()[0] == 0, k
+        n_ee, n_pt = s.n_contacts, s.n_contacts_pt
+        recs = np.concatenate([s.contacts_new.records(n_ee)[:, :4].cpu().numpy(),
+                               s.contacts_pt.records(n_pt)[:, :4].cpu().numpy()])
+        b = body[recs]
+        ball = ((b >= n_fem_bodies) & (b < n_fem_bodies + 4)).any(axis=1)
+        hit |= bool((ball & (b < n_fem_bodies).any(axis=1)).any())
+    q = _host(s.q)
+    assert np.isfinite(q).all()
+    g = s.n_fem + 4 * (len(sc.bodies) - 1)
+    assert np.abs(q[g:g + 4] - q0[g:g + 4]).max() == 0.0
+    assert s.orthogonality_error() < 1e-3
+    assert hit

@@ -1,5 +1,5 @@
 """Batched Newton terms (one persistent work-queue launch over the contact
-records and the tets) and the fixed-pattern assembly against the per-term
+records, the tets and the affine-body items) and the fixed-pattern assembly against the per-term
 kernels and the sort-based assembly; BSR pattern union against numpy;
 autotuner bookkeeping (gpu)."""
 import numpy as np
@@ -111,10 +111,11 @@ def test_autotuner_records_every_candidate(cuda):
     assert len(s._tuner.timings) == 1
 
 
-@pytest.mark.parametrize("cfg", [("separate",), (2, 128, 64), (4, 64, 32)])
+@pytest.mark.parametrize("cfg", [("separate",), (0, 2, 128, 64), (0, 4, 64, 32), (1, 1, 128, 32), (1, 2, 128, 128)])
 def test_every_schedule_assembles_the_same_matrix(cuda, cfg):
-    """The per-kind kernels and the persistent work-queue launch (with its
-    staged tet chunks) produce the same matrix and force."""
+    """The per-kind kernels and the persistent work-queue launch (its two
+    register variants, with staged tet chunks and class-sorted contact
+    chunks) produce the same matrix and force."""
     sc = small_scenes()[2]
     rng = np.random.default_rng(11)
     x = sc.x + rng.normal(scale=0.05 * sc.dhat, size=sc.x.shape)
