@@ -328,6 +328,51 @@ def newton_step_times(dev, torch, reps: int = 3, direct_reps: int = 1):
     return out
 
 
+WRECKING_WORKLOAD = "wrecking_balls_64_icospheres_2562v_512_nh_cubes_4x4x4_ground_100x100_dt1e-2_kappa1e10"
+
+
+def wrecking_balls_steps(dev, torch, before: int = 55, timed: int = 3):
+    """The batched affine + FEM wrecking balls (64 pendulum icospheres, 512
+    neo-Hookean cubes, fixed ground) in one mixed Newton solve: ``before``
+    untimed time steps (the balls swing into their cube stacks), then
+    ``timed`` steps timed with CUDA events, the phases of one Newton
+    iteration at the last state, and the intersection check."""
+    from ipc_warp_b200 import scenes
+    from ipc_warp_b200.mixed import MixedSolver
+
+    sc = scenes.wrecking_balls(n_balls=64)
+    s = MixedSolver(sc, E=5e5, nu=0.4, h=1e-2, dtype=torch.float32, device=dev, maxiter=2000)
+    for _ in range(before):
+        s.step()
+    steps = []
+    for _ in range(timed):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        st = s.step()
+        b.record()
+        torch.cuda.synchronize()
+        steps.append({"ms": a.elapsed_time(b), "newton_iterations": st.newton_iterations,
+                      "pcg_iterations": st.pcg_iterations, "records": s.n_contacts + s.n_contacts_pt})
+    s.prepare()
+    phase = {}
+    for name, fn in (("compute_A", s.compute_A), ("solve", s.solve), ("line_search", s.line_search)):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        phase[name] = round(a.elapsed_time(b), 3)
+    key = next(iter(s._tuner.best.values()), None) if s._tuner.best else None
+    return {"workload": WRECKING_WORKLOAD, "unknowns": s.nq, "vertices": s.n_verts, "tets": s.n_tets,
+            "bodies": s.n_bodies, "steps_before": before, "timed_steps": steps,
+            "ms_per_step": statistics.median(x["ms"] for x in steps), "newton_iteration_phase_ms": phase,
+            "terms_schedules": {k: list(v) for k, v in s._tuner.best.items()}, "last_schedule": key,
+            "edge_triangle_crossings": s.edge_triangle_crossings()[0],
+            "orthogonality_error": s.orthogonality_error()}
+
+
 def run_profile_solver(args):
     """Untimed launches of the Newton solve's kernels on the wound rod bundle
     (for ncu): two learned-factor builds (MPNN forward, row normalisation,
@@ -583,6 +628,7 @@ def run_ours(args):
     out = None
     if rank == 0:
         newton = None if args.no_newton else newton_step_times(dev, torch)
+        wrecking = None if args.no_newton else wrecking_balls_steps(dev, torch)
         sc = head.pop("sc")
         cfg = workload_config(args.workload, sc, head["pairs"])
         cfg.update({"n_ee": head["n_ee"], "n_pt": head["n_pt"], "ccd_candidates": head["ccd_candidates"],
@@ -596,7 +642,7 @@ def run_ours(args):
             "roofline_narrow": head["roofline_narrow"], "roofline_ccd": head["roofline_ccd"],
             "cpu_baseline": head["cpu_baseline"],
             "e2e": head["e2e"], "gpu_launches": head["gpu_launches"], "kernels": head["kernels"], "clocks": clocks,
-            "newton_step": newton,
+            "newton_step": newton, "wrecking_balls": wrecking,
         }
         if second is not None:
             second.pop("sc")
@@ -618,7 +664,7 @@ def main():
     ap.add_argument("--profile-only", action="store_true",
                     help="warmup + K steps only (for ncu launch lists); prints nothing")
     ap.add_argument("--no-newton", action="store_true",
-                    help="skip the Newton-step timing (learned-PCG / Jacobi-PCG / direct)")
+                    help="skip the Newton-step timing (learned-PCG / Jacobi-PCG / direct) and the wrecking balls")
     ap.add_argument("--profile-solver", action="store_true",
                     help="untimed Newton-solve kernels only (learned factor + PCG), for ncu; prints nothing")
     ap.add_argument("--workload", default=HEADLINE, choices=sorted(WORKLOADS),

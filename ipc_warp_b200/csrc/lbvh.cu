@@ -138,102 +138,80 @@ __global__ void k_karras(const unsigned* __restrict__ keys, const int* __restric
 // child to arrive at a node merges both slots and continues upward.  The .w
 // of a slot's hi entry carries the largest leaf rank (position in Morton
 // order) below the slot: a node's is its right child's.
-__global__ void k_refit(const float* __restrict__ lo, const float* __restrict__ hi, int n,
-                        const int* __restrict__ sorted, const int* __restrict__ parent, int cap,
-                        float4* __restrict__ nodes, unsigned* __restrict__ flags) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
+//
+// The refit also writes the 4-wide view (see traverse4) on the way up: entries
+// 2s and 2s + 1 of wide[node] belong to the node's side-s child -- the child's
+// own slot and an empty entry when the child is a leaf, the child's two slots
+// when it is internal.  The thread that writes its subtree's slot into `node`
+// knows both (an internal subtree's two slots are the ones it merged one level
+// below), so it writes that half of wide[node] with the slot, before the
+// fence: no loads and no separate gather pass over the nodes.
+struct Slot {
+  float4 lo, hi;
+};
+
+// entries 2 side and 2 side + 1 of the SoA wide node w
+IPCB_D void put_wide_half(float4* __restrict__ w, int side, const Slot& a, const Slot& b) {
+  float2* h = reinterpret_cast<float2*>(w) + side;
+  h[0] = make_float2(a.lo.x, b.lo.x);
+  h[2] = make_float2(a.lo.y, b.lo.y);
+  h[4] = make_float2(a.lo.z, b.lo.z);
+  h[6] = make_float2(a.hi.x, b.hi.x);
+  h[8] = make_float2(a.hi.y, b.hi.y);
+  h[10] = make_float2(a.hi.z, b.hi.z);
+  h[12] = make_float2(a.lo.w, b.lo.w);
+  h[14] = make_float2(a.hi.w, b.hi.w);
+}
+
+__global__ void __launch_bounds__(256) k_refit(const float* __restrict__ lo, const float* __restrict__ hi, int n,
+                                               const int* __restrict__ sorted, const int* __restrict__ parent,
+                                               int cap, float4* __restrict__ nodes, unsigned* __restrict__ flags,
+                                               float4* __restrict__ wide) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
-  int prim = sorted[k];
+  const int prim = sorted[k];
   float3 bl = make_float3(lo[3 * prim], lo[3 * prim + 1], lo[3 * prim + 2]);
   float3 bh = make_float3(hi[3 * prim], hi[3 * prim + 1], hi[3 * prim + 2]);
   int code = ~prim;
+  const Slot none{make_float4(3.4e38f, 3.4e38f, 3.4e38f, __int_as_float(-1)),
+                  make_float4(-3.4e38f, -3.4e38f, -3.4e38f, __int_as_float(-1))};
   if (n == 1) {
-    nodes[0] = make_float4(bl.x, bl.y, bl.z, __int_as_float(code));
-    nodes[1] = make_float4(bh.x, bh.y, bh.z, __int_as_float(0));
-    nodes[2] = make_float4(3.4e38f, 3.4e38f, 3.4e38f, __int_as_float(code));
-    nodes[3] = make_float4(-3.4e38f, -3.4e38f, -3.4e38f, __int_as_float(-1));
+    const Slot leaf{make_float4(bl.x, bl.y, bl.z, __int_as_float(code)), make_float4(bh.x, bh.y, bh.z, __int_as_float(0))};
+    const Slot second{make_float4(3.4e38f, 3.4e38f, 3.4e38f, __int_as_float(code)), none.hi};
+    nodes[0] = leaf.lo;
+    nodes[1] = leaf.hi;
+    nodes[2] = second.lo;
+    nodes[3] = second.hi;
+    put_wide_half(wide, 0, leaf, none);
+    put_wide_half(wide, 1, second, none);  // a leaf code with an empty box: never hit
     return;
   }
   int par = parent[cap + k];
   int last = k;  // largest leaf rank below the subtree being carried up
+  Slot c0 = none, c1 = none;  // the carried subtree's two slots (side order) when it is internal
   // Depth is bounded by the 30 Morton bits plus 32 index bits of the
   // tie-break; the loop bound only guards against a corrupted parent array.
   for (int level = 0; level < 128; ++level) {
-    int node = par >> 1, side = par & 1;
-    __stcg(nodes + 4 * node + 2 * side, make_float4(bl.x, bl.y, bl.z, __int_as_float(code)));
-    __stcg(nodes + 4 * node + 2 * side + 1, make_float4(bh.x, bh.y, bh.z, __int_as_float(last)));
+    const int node = par >> 1, side = par & 1;
+    const Slot own{make_float4(bl.x, bl.y, bl.z, __int_as_float(code)),
+                   make_float4(bh.x, bh.y, bh.z, __int_as_float(last))};
+    __stcg(nodes + 4 * node + 2 * side, own.lo);
+    __stcg(nodes + 4 * node + 2 * side + 1, own.hi);
+    if (code < 0) put_wide_half(wide + 8 * (size_t)node, side, own, none);
+    else put_wide_half(wide + 8 * (size_t)node, side, c0, c1);
     __threadfence();
-    unsigned old = atomicAdd(flags + node, 1u);
+    const unsigned old = atomicAdd(flags + node, 1u);
     if (old == 0) return;
     flags[node] = 0;
-    float4 sl = __ldcg(nodes + 4 * node + 2 * (1 - side));
-    float4 sh = __ldcg(nodes + 4 * node + 2 * (1 - side) + 1);
-    if (side == 0) last = __float_as_int(sh.w);
-    bl = make_float3(fminf(bl.x, sl.x), fminf(bl.y, sl.y), fminf(bl.z, sl.z));
-    bh = make_float3(fmaxf(bh.x, sh.x), fmaxf(bh.y, sh.y), fmaxf(bh.z, sh.z));
+    const Slot sib{__ldcg(nodes + 4 * node + 2 * (1 - side)), __ldcg(nodes + 4 * node + 2 * (1 - side) + 1)};
+    c0 = side == 0 ? own : sib;
+    c1 = side == 0 ? sib : own;
+    if (side == 0) last = __float_as_int(sib.hi.w);
+    bl = make_float3(fminf(bl.x, sib.lo.x), fminf(bl.y, sib.lo.y), fminf(bl.z, sib.lo.z));
+    bh = make_float3(fmaxf(bh.x, sib.hi.x), fmaxf(bh.y, sib.hi.y), fmaxf(bh.z, sib.hi.z));
     if (node == 0) return;
     code = node;
     par = parent[node];
-  }
-}
-
-// Gather the 4-wide view (see traverse4) from the refit binary nodes.  A
-// warp's 32 consecutive wide nodes (4 KB) are staged in shared memory and
-// stored as 8 fully coalesced 512-byte rows instead of 8 scattered 16-byte
-// stores per lane (the stage is padded to 9 vectors a lane: no bank conflict).
-__global__ void __launch_bounds__(256) k_widen(const float4* __restrict__ nodes, int n_int,
-                                               float4* __restrict__ wide) {
-  __shared__ float4 stage[8][32 * 9];
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31, warp0 = b - lane;
-  if (warp0 >= n_int) return;  // the whole warp
-  float4* sw = stage[threadIdx.x >> 5];
-  if (b < n_int) {
-    float lo[4][3], hi[4][3];
-    int code[4], last[4];
-    int m = 0;
-  #pragma unroll
-    for (int side = 0; side < 2; ++side) {
-      float4 slo = __ldcg(nodes + 4 * b + 2 * side), shi = __ldcg(nodes + 4 * b + 2 * side + 1);
-      int c = __float_as_int(slo.w);
-      if (c < 0) {
-        lo[m][0] = slo.x; lo[m][1] = slo.y; lo[m][2] = slo.z;
-        hi[m][0] = shi.x; hi[m][1] = shi.y; hi[m][2] = shi.z;
-        last[m] = __float_as_int(shi.w);
-        code[m++] = c;
-      } else {
-  #pragma unroll
-        for (int s2 = 0; s2 < 2; ++s2) {
-          float4 glo = __ldcg(nodes + 4 * c + 2 * s2), ghi = __ldcg(nodes + 4 * c + 2 * s2 + 1);
-          lo[m][0] = glo.x; lo[m][1] = glo.y; lo[m][2] = glo.z;
-          hi[m][0] = ghi.x; hi[m][1] = ghi.y; hi[m][2] = ghi.z;
-          last[m] = __float_as_int(ghi.w);
-          code[m++] = __float_as_int(glo.w);
-        }
-      }
-    }
-    for (int k = m; k < 4; ++k) {
-      lo[k][0] = lo[k][1] = lo[k][2] = 3.4e38f;
-      hi[k][0] = hi[k][1] = hi[k][2] = -3.4e38f;
-      code[k] = -1;
-      last[k] = -1;
-    }
-    float4* w = sw + 9 * lane;
-    w[0] = make_float4(lo[0][0], lo[1][0], lo[2][0], lo[3][0]);
-    w[1] = make_float4(lo[0][1], lo[1][1], lo[2][1], lo[3][1]);
-    w[2] = make_float4(lo[0][2], lo[1][2], lo[2][2], lo[3][2]);
-    w[3] = make_float4(hi[0][0], hi[1][0], hi[2][0], hi[3][0]);
-    w[4] = make_float4(hi[0][1], hi[1][1], hi[2][1], hi[3][1]);
-    w[5] = make_float4(hi[0][2], hi[1][2], hi[2][2], hi[3][2]);
-    *reinterpret_cast<int4*>(w + 6) = make_int4(code[0], code[1], code[2], code[3]);
-    *reinterpret_cast<int4*>(w + 7) = make_int4(last[0], last[1], last[2], last[3]);
-  }
-  __syncwarp();
-  // row r of the warp's output: vector u = 32 r + lane is vector u % 8 of node warp0 + u / 8
-#pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    const int u = 32 * r + lane, owner = u >> 3;
-    if (warp0 + owner < n_int) wide[8 * (size_t)warp0 + u] = sw[9 * owner + (u & 7)];
   }
 }
 
@@ -330,9 +308,7 @@ int ipcb_lbvh_build(ipcb_lbvh* bvh, const float* lower, const float* upper, int 
     k_karras<<<div_up(n - 1, 256), 256, 0, st>>>(bvh->keys, bvh->sorted, n, (float4*)bvh->nodes, bvh->parent,
                                                   bvh->capacity);
   k_refit<<<div_up(n, 256), 256, 0, st>>>(lower, upper, n, bvh->sorted, bvh->parent, bvh->capacity,
-                                           (float4*)bvh->nodes, bvh->flags);
-  int n_int = n > 1 ? n - 1 : 1;
-  k_widen<<<div_up(n_int, 256), 256, 0, st>>>((const float4*)bvh->nodes, n_int, (float4*)bvh->wide);
+                                           (float4*)bvh->nodes, bvh->flags, (float4*)bvh->wide);
   return check_launch("ipcb_lbvh_build");
 }
 
@@ -341,9 +317,8 @@ int ipcb_lbvh_refit(const ipcb_lbvh* bvh, const float* lower, const float* upper
   if (bvh->n == 0) return IPCB_OK;
   if (!lower || !upper) return IPCB_E_ARG;
   k_refit<<<div_up(bvh->n, 256), 256, 0, (cudaStream_t)s>>>(lower, upper, bvh->n, bvh->sorted, bvh->parent,
-                                                            bvh->capacity, (float4*)bvh->nodes, bvh->flags);
-  int n_int = bvh->n > 1 ? bvh->n - 1 : 1;
-  k_widen<<<div_up(n_int, 256), 256, 0, (cudaStream_t)s>>>((const float4*)bvh->nodes, n_int, (float4*)bvh->wide);
+                                                            bvh->capacity, (float4*)bvh->nodes, bvh->flags,
+                                                            (float4*)bvh->wide);
   return check_launch("ipcb_lbvh_refit");
 }
 

@@ -252,11 +252,16 @@ def backward(net: Net, sysm: System, tape: _Tape, dG: torch.Tensor, grad: torch.
 
 
 class Trainer:
-    """Adam on the Kaporin loss over a list of systems."""
+    """Adam on the Kaporin loss over a list of systems.  The gradient is
+    clipped to norm ``clip`` and a step whose loss or gradient is not finite
+    is skipped: one very stiff system in a batch can otherwise throw the
+    parameters far enough that the net collapses to the diagonal."""
 
-    def __init__(self, net: Net, lr: float = 1e-3, betas=(0.9, 0.999), eps: float = 1e-8):
+    def __init__(self, net: Net, lr: float = 1e-3, betas=(0.9, 0.999), eps: float = 1e-8, clip: float = 1.0):
         self.net = net
         self.lr, self.betas, self.eps = lr, betas, eps
+        self.clip = float(clip)
+        self.skipped = 0
         z = lambda: torch.zeros_like(net.params)
         self.m, self.v, self.grad = z(), z(), z()
         self.t = 0
@@ -270,6 +275,12 @@ class Trainer:
             dG = loss_grad(sysm, nz, weight=1.0 / len(batch))
             backward(self.net, sysm, tape, dG, self.grad)
             total += nz.loss / len(batch)
+        gn = float(self.grad.norm())
+        if not (math.isfinite(gn) and math.isfinite(total)):
+            self.skipped += 1
+            return total
+        if self.clip > 0 and gn > self.clip:
+            self.grad.mul_(self.clip / gn)
         self.t += 1
         N.call("ipcb_adam", self.net.params.numel(), N.ptr(self.net.params), N.ptr(self.grad), N.ptr(self.m),
                N.ptr(self.v), float(self.lr), float(self.betas[0]), float(self.betas[1]), float(self.eps), self.t,
