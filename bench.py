@@ -328,7 +328,7 @@ def newton_step_times(dev, torch, reps: int = 3, direct_reps: int = 1):
     return out
 
 
-WRECKING_WORKLOAD = "wrecking_balls_64_icospheres_2562v_512_nh_cubes_4x4x4_ground_100x100_dt1e-2_kappa1e10"
+WRECKING_WORKLOAD = "wrecking_balls_64_icospheres_2562v_512_nh_cubes_4x4x4_ground_100x100_dt1e-2_kappa1e12"
 
 
 def wrecking_balls_steps(dev, torch, before: int = 55, timed: int = 3):

@@ -702,6 +702,7 @@ int ipcb_fsai_apply(const ipcb_graph* g, const float* G, const float* scale, int
 typedef struct {
   double rz, rz_new, pAp, rr, bb, tol2, last_rr;
   int it, done, maxiter, status;
+  int arrived; /* blocks of the last kernel of an iteration that have finished (internal) */
 } ipcb_pcg_state;
 
 typedef struct {

@@ -80,7 +80,7 @@ class Tape(ctypes.Structure):
 class PcgState(ctypes.Structure):
     _fields_ = [("rz", c_double), ("rz_new", c_double), ("pAp", c_double), ("rr", c_double), ("bb", c_double),
                 ("tol2", c_double), ("last_rr", c_double), ("it", c_int), ("done", c_int), ("maxiter", c_int),
-                ("status", c_int)]
+                ("status", c_int), ("arrived", c_int)]
 
 
 class Pcg(ctypes.Structure):

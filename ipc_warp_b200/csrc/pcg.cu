@@ -5,9 +5,11 @@
 // at a time (or replays them as a CUDA graph) and reads one flag per batch.
 //
 // Per iteration: q = A p fused with p.q (warp per block row over the row's
-// contiguous values); x += alpha p, r -= alpha q with |r|^2; z = M^-1 r with
-// r.z (block Jacobi, or the two sweeps of the FSAI factor); p = z + beta p;
-// a one-thread kernel rotates the scalars and tests |r| <= tol |b|.
+// contiguous values); x += alpha p, r -= alpha q with |r|^2, fused with the
+// block-Jacobi z = D^-1 r and r.z (or, for the FSAI factor, followed by its
+// two sweeps); p = z + beta p, whose last block to finish rotates the
+// scalars and tests |r| <= tol |b|: three launches per iteration with block
+// Jacobi, four with the learned factor.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -39,6 +41,33 @@ __device__ __forceinline__ double block_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
   }
   return t;  // valid in thread 0
+}
+
+// two block sums at once (valid in thread 0)
+__device__ __forceinline__ void block_sum2(double& a, double& b) {
+  __shared__ double s[2][kBlock / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+    s[0][w] = a;
+    s[1][w] = b;
+  }
+  __syncthreads();
+  if (w == 0) {
+    double x = lane < (int)(blockDim.x >> 5) ? s[0][lane] : 0.0;
+    double y = lane < (int)(blockDim.x >> 5) ? s[1][lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      x += __shfl_down_sync(0xffffffffu, x, o);
+      y += __shfl_down_sync(0xffffffffu, y, o);
+    }
+    a = x;
+    b = y;
+  }
 }
 
 template <class T> __device__ __forceinline__ T ldv(const T* p) { return __ldg(p); }
@@ -149,6 +178,41 @@ __global__ void __launch_bounds__(kBlock) k_update_xr(int m, T* __restrict__ x, 
   if (threadIdx.x == 0) atomicAdd(&st->rr, part);
 }
 
+// x += alpha p ; r -= alpha q ; z = D^-1 r (block Jacobi), per block row ;
+// state.rr += r.r ; state.rz_new += r.z
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_update_xr_jacobi(int n, T* __restrict__ x, T* __restrict__ r,
+                                                             const T* __restrict__ p, const T* __restrict__ q,
+                                                             const T* __restrict__ dinv, T* __restrict__ z,
+                                                             ipcb_pcg_state* st) {
+  if (st->done) return;
+  const double alpha = st->pAp > 0.0 ? st->rz / st->pAp : 0.0;
+  double prr = 0.0, prz = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    T rv[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int k = 3 * i + c;
+      x[k] += (T)alpha * p[k];
+      rv[c] = r[k] - (T)alpha * q[k];
+      r[k] = rv[c];
+      prr += (double)rv[c] * rv[c];
+    }
+    const T* d = dinv + 9LL * i;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const T zc = d[3 * c] * rv[0] + d[3 * c + 1] * rv[1] + d[3 * c + 2] * rv[2];
+      z[3 * i + c] = zc;
+      prz += (double)rv[c] * zc;
+    }
+  }
+  block_sum2(prr, prz);
+  if (threadIdx.x == 0) {
+    atomicAdd(&st->rr, prr);
+    atomicAdd(&st->rz_new, prz);
+  }
+}
+
 // z = D^-1 r (block Jacobi) ; state.rz_new += r.z
 template <class T>
 __global__ void __launch_bounds__(kBlock) k_jacobi(int n, const T* __restrict__ dinv, const T* __restrict__ r,
@@ -224,19 +288,9 @@ __global__ void __launch_bounds__(kBlock) k_fsai_upper(int n, const int* __restr
   if (threadIdx.x == 0) atomicAdd(&st->rz_new, part);
 }
 
-// p = z + beta p (beta = rz_new / rz); with start != 0: p = z
-template <class T>
-__global__ void __launch_bounds__(kBlock) k_update_p(int m, const T* __restrict__ z, T* __restrict__ p,
-                                                     ipcb_pcg_state* st, int start) {
-  if (st->done) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
-  const double beta = start ? 0.0 : (st->rz != 0.0 ? st->rz_new / st->rz : 0.0);
-  p[i] = z[i] + (T)beta * (start ? (T)0 : p[i]);
-}
-
-__global__ void k_finish(ipcb_pcg_state* st, int start) {
-  if (st->done) return;
+// the end of an iteration (start: of the setup): rotate the scalars and
+// test convergence, breakdown and the iteration bound
+__device__ __forceinline__ void finish_state(ipcb_pcg_state* st, int start) {
   if (!start) {
     st->it += 1;
     if (st->rr <= st->tol2 * st->bb) st->done = 1;
@@ -253,6 +307,27 @@ __global__ void k_finish(ipcb_pcg_state* st, int start) {
   st->rz_new = 0.0;
   st->pAp = 0.0;
   st->rr = 0.0;
+}
+
+// p = z + beta p (beta = rz_new / rz; start: p = z); the last block to finish
+// (every block has read rz / rz_new by then) runs finish_state
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_update_p_finish(int m, const T* __restrict__ z, T* __restrict__ p,
+                                                            ipcb_pcg_state* st, int start) {
+  if (st->done) return;
+  const double beta = start ? 0.0 : (st->rz != 0.0 ? st->rz_new / st->rz : 0.0);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    p[i] = z[i] + (T)beta * (start ? (T)0 : p[i]);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const int k = atomicAdd(&st->arrived, 1);
+    if (k == (int)gridDim.x - 1) {
+      __threadfence();
+      st->arrived = 0;
+      finish_state(st, start);
+    }
+  }
 }
 
 // x = 0, r = b, bb = b.b
@@ -278,6 +353,7 @@ __global__ void k_state_init(ipcb_pcg_state* st, double tol, int maxiter) {
   st->done = 0;
   st->maxiter = maxiter;
   st->status = 0;
+  st->arrived = 0;
 }
 
 // inverse of the diagonal blocks
@@ -366,8 +442,7 @@ int start(const ipcb_pcg* P, double tol, int maxiter, cudaStream_t s) {
   k_state_init<<<1, 1, 0, s>>>(P->state, tol, maxiter);
   k_start<T><<<gridn(m), kBlock, 0, s>>>(m, (const T*)P->b, (T*)P->x, (T*)P->r, P->state);
   precond<T>(P, s);
-  k_update_p<T><<<gridn(m), kBlock, 0, s>>>(m, (const T*)P->z, (T*)P->p, P->state, 1);
-  k_finish<<<1, 1, 0, s>>>(P->state, 1);
+  k_update_p_finish<T><<<flat_grid(m), kBlock, 0, s>>>(m, (const T*)P->z, (T*)P->p, P->state, 1);
   return 0;
 }
 
@@ -377,10 +452,15 @@ int iterate(const ipcb_pcg* P, int k, cudaStream_t s) {
   for (int it = 0; it < k; ++it) {
     k_spmv_dot<T><<<warp_grid(n), kBlock, 0, s>>>(n, P->offsets, P->columns, (const T*)P->values, (const T*)P->p,
                                                      (T*)P->q, P->state);
-    k_update_xr<T><<<flat_grid(m), kBlock, 0, s>>>(m, (T*)P->x, (T*)P->r, (const T*)P->p, (const T*)P->q, P->state);
-    precond<T>(P, s);
-    k_update_p<T><<<gridn(m), kBlock, 0, s>>>(m, (const T*)P->z, (T*)P->p, P->state, 0);
-    k_finish<<<1, 1, 0, s>>>(P->state, 0);
+    if (P->precond == 0) {
+      k_update_xr_jacobi<T><<<flat_grid(n), kBlock, 0, s>>>(n, (T*)P->x, (T*)P->r, (const T*)P->p, (const T*)P->q,
+                                                            (const T*)P->dinv, (T*)P->z, P->state);
+    } else {
+      k_update_xr<T><<<flat_grid(m), kBlock, 0, s>>>(m, (T*)P->x, (T*)P->r, (const T*)P->p, (const T*)P->q,
+                                                     P->state);
+      precond<T>(P, s);
+    }
+    k_update_p_finish<T><<<flat_grid(m), kBlock, 0, s>>>(m, (const T*)P->z, (T*)P->p, P->state, 0);
   }
   return 0;
 }

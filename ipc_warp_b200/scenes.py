@@ -520,7 +520,7 @@ def ground_grid(quads: int, extent: float, origin=(0.0, 0.0, 0.0)):
 
 def wrecking_balls(n_balls: int = 64, subdiv: int = 4, radius: float = 0.5, rope: float = 1.0,
                    max_angle_deg: float = 60.0, stack=(2, 2, 2), cube_cells: int = 4, cube_size: float = 0.25,
-                   ground_quads: int = 100, station: float = 3.0, dhat: float = 1e-3, kappa: float = 1e10,
+                   ground_quads: int = 100, station: float = 3.0, dhat: float = 1e-3, kappa: float = 1e12,
                    pin_stiffness: float = 1e9, seed: int = 0) -> MixedScene:
     """Batched affine + FEM wrecking balls: ``n_balls`` affine icospheres
     (subdiv 4: 2562 vertices, 5120 triangles; radius 0.5) on pendulum pins,

@@ -133,7 +133,7 @@ def test_wrecking_balls_trajectory(cuda):
     crossing, the balls stay rigid, the ground stays put, and the balls
     end up touching the cubes (affine-FEM contact records)."""
     sc = scenes.wrecking_balls(n_balls=4, subdiv=3, cube_cells=3, ground_quads=16, max_angle_deg=60.0,
-                               kappa=1e10, seed=2)
+                               kappa=1e12, seed=2)
     s = MixedSolver(sc, E=5e5, nu=0.4, h=1e-2, dtype=torch.float32, maxiter=2000)
     q0 = _host(s.q)
     n_fem_bodies = int(sc.fem.body.max()) + 1
