@@ -6,7 +6,9 @@ library is missing or a call reports an error.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
+import gc
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -202,6 +204,20 @@ SIGNATURES = {
     "ipcb_contact_bsr_workspace": (c_size_t, [c_int, c_int]),
     "ipcb_contact_bsr": (c_int, [CP, c_int, CP, c_int, c_int, P, P, c_int, P, P, P, P, P, P, c_size_t, P]),
 }
+
+
+@contextlib.contextmanager
+def no_collection():
+    """Garbage collection off for a CUDA graph capture: an object collected
+    inside it (an earlier solver's graph, a tensor whose allocator queries
+    events) must not touch the capturing stream."""
+    was_on = gc.isenabled()
+    gc.disable()
+    try:
+        yield
+    finally:
+        if was_on:
+            gc.enable()
 
 
 class NativeError(RuntimeError):

@@ -18,6 +18,7 @@ from __future__ import annotations
 import ctypes
 import gc
 import math
+import warnings
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -27,8 +28,9 @@ from . import _native as N
 from . import contact as contact_mod
 from .autotune import Autotuner, bucket
 from .bsr import BsrMatrix, Triplets, bsr_from_triplets, bsr_mv, contact_bsr
-from .contact import Soup
-from .dynamic_contacts import ContactBarrierMixin, contact_hessian_ee, contact_hessian_pt, hessian_workspace
+from .contact import QUERY_FAILED, Soup
+from .dynamic_contacts import (ContactBarrierMixin, contact_hessian_ee, contact_hessian_pt, contact_hessian_pt_after,
+                               hessian_workspace)
 
 MATERIALS = {"snh": 0, "neo_hookean": 1, "nh": 1, "stvk": 2}
 
@@ -162,7 +164,7 @@ class DevicePcg:
         key = tuple(getattr(P, f) for f, _ in N.Pcg._fields_)
         if self.use_graph and key != self._key:
             self._graph = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(self._graph):
+            with N.no_collection(), torch.cuda.graph(self._graph):
                 N.call("ipcb_pcg_iterate", ctypes.byref(P), self.batch, N.stream_handle())
             self._key = key
         st = N.PcgState()
@@ -216,6 +218,9 @@ class FEMContactSolver(ContactBarrierMixin):
         # fixed-pattern assembly (csrc/terms.cu); "generic": per-term kernels
         # and a sort-based assembly of all triplets
         self.assembly = assembly
+        # queue assembly: replay compute_A from a CUDA graph (device-side
+        # counts, one host read) once a step-by-step call has sized the buffers
+        self.graph_compute_A = True
         self._static = None
         self.material = MATERIALS[material]
         self.mu, self.lam = lame(E, nu)
@@ -325,8 +330,137 @@ class FEMContactSolver(ContactBarrierMixin):
     def compute_A(self) -> BsrMatrix:
         """time_integrator_base.py:406-426 + dynamic_contacts.py:275-297."""
         if self.assembly == "queue":
+            if self.graph_compute_A and self.device.type == "cuda" and not getattr(self, "bvh_rebuild_interval", 0):
+                return self._compute_A_graph()
             return self._compute_A_queue()
         return self._compute_A_generic()
+
+    # ------------------------------------------ graph-replayed compute_A
+    def _graph_buffers(self):
+        """Buffers sized for the list capacities (so the captured launches
+        never need a count on the host): the contact triplets, the contact
+        BSR and the union (static pattern + 16 blocks per possible record)."""
+        st = self._static
+        ee, pt = self.contacts_new, self.contacts_pt
+        cap_rec = ee.capacity + pt.capacity
+        t = self.collision_triplets
+        if t is None or t.rows.shape[0] < 16 * cap_rec:
+            self.collision_triplets = Triplets.zeros(16 * cap_rec, self.dtype, self.device)
+        V = self.soup.n_verts
+        cap = st["nnz"] + 16 * cap_rec
+        A = getattr(self, "A", None)
+        if A is None or A.columns.shape[0] < cap or "a_rows" not in st or st["a_rows"].shape[0] < cap:
+            A = self.A = BsrMatrix(V, V, cap, self.dtype, self.device)
+            for k in ("a_rows", "src_a", "src_b"):
+                st[k] = torch.empty(cap, dtype=torch.int32, device=self.device)
+        if "graph_read" not in st:
+            st["graph_read"] = torch.zeros(4, dtype=torch.int32, pin_memory=True)
+        return min(A.columns.shape[0], st["a_rows"].shape[0])
+
+    def _enqueue_A(self, cfg, cap: int):
+        """compute_A's launches with every count read on the device: box
+        refits and the discrete queries, the per-iteration terms on schedule
+        ``cfg``, the contact BSR of the lists' capacities, the union with the
+        elastic pattern and its values; ends with the copy of the two list
+        counts and the two status words into pinned host memory."""
+        st = self._static
+        h2 = self.h * self.h
+        V = self.soup.n_verts
+        ee, pt = self.contacts_new, self.contacts_pt
+        t = self.collision_triplets
+        s = N.stream_handle()
+        self.b.zero_()
+        self.compute_V(ret=False)
+        self._status.zero_()
+        self.update_bvh()
+        self._launch_dcd("ee")
+        if self.has_triangles:
+            self._launch_dcd("pt")
+        else:
+            pt.cnt.zero_()
+        kappa = float(self.contact_stiffness)
+        if cfg[0] == "separate":
+            self._ws_ee = hessian_workspace(ee, getattr(self, "_ws_ee", None))
+            self._ws_pt = hessian_workspace(pt, getattr(self, "_ws_pt", None))
+            contact_hessian_ee(None, self.soup, ee, t, self.b, kappa, n=-1, ws=self._ws_ee)
+            contact_hessian_pt_after(None, self.soup, pt, t, self.b, ee, kappa, ws=self._ws_pt)
+            N.call("ipcb_tet_hessian", self.material, int(self.dtype == torch.float64), N.ptr(self.states.x),
+                   N.ptr(self.tets), self.n_tets, N.ptr(self.Bm), N.ptr(self.W), self.mu, self.lam, None, None,
+                   N.ptr(st["tet_vals"]), N.ptr(self.b), s)
+        else:
+            Tc = N.Terms(int(self.dtype == torch.float64), N.ptr(self.states.x), N.ptr(self.soup.xcs),
+                         ee.c_struct(), pt.c_struct(), kappa, N.ptr(t.rows), N.ptr(t.cols), N.ptr(t.vals),
+                         N.ptr(t.mask), self.material, N.ptr(self.tets), self.n_tets, N.ptr(self.Bm), N.ptr(self.W),
+                         self.mu, self.lam, None, None, N.ptr(st["tet_vals"]), N.ptr(self.b), N.ptr(st["queue"]),
+                         *self._sorted_workspaces())
+            launch_terms(Tc, cfg, self._n_sm)
+        C, _ = contact_bsr(ee, None, pt, None, V, t, out=getattr(self, "_C", None), status=st["status"],
+                           read_status=False)
+        self._C = C
+        S, A = st["S"], self.A
+        N.call("ipcb_bsr_union", V, N.ptr(S.offsets), N.ptr(S.columns), N.ptr(C.offsets), N.ptr(C.columns),
+               N.ptr(A.offsets), N.ptr(st["a_rows"]), N.ptr(A.columns), N.ptr(st["src_a"]), N.ptr(st["src_b"]), cap,
+               N.ptr(A.nnz_dev), N.ptr(st["status"]), N.ptr(st["ws"]), st["ws"].numel(), s)
+        N.call("ipcb_newton_values", int(self.dtype == torch.float64), N.ptr(A.nnz_dev), cap, N.ptr(st["a_rows"]),
+               N.ptr(A.columns), N.ptr(st["src_a"]), N.ptr(st["src_b"]), N.ptr(st["g_off"]), N.ptr(st["g_idx"]),
+               N.ptr(st["tet_vals"]), h2, N.ptr(st["diag"]), N.ptr(C.values), h2, N.ptr(A.values), s)
+        r = st["graph_read"]
+        r[0:1].copy_(ee.cnt, non_blocking=True)
+        r[1:2].copy_(pt.cnt, non_blocking=True)
+        r[2:3].copy_(st["status"], non_blocking=True)
+        r[3:4].copy_(self._status, non_blocking=True)
+
+    def _compute_A_graph(self) -> BsrMatrix:
+        """compute_A replayed from one CUDA graph with one host read.  The
+        first call (and any call after a list overflow, a row with too many
+        contact columns or a union over capacity) runs the step-by-step path,
+        which grows the lists and has the autotuner pick the terms schedule;
+        the sequence is then captured for the buffers and schedule of the
+        moment and replayed while they stay the same."""
+        st = self._static
+        g = getattr(self, "_A_graph", None)
+        if g is not None and g[0] == self._A_graph_key():
+            g[1].replay()
+            torch.cuda.current_stream().synchronize()
+            n_ee, n_pt, bst, qst = (int(v) for v in st["graph_read"])
+            ee, pt = self.contacts_new, self.contacts_pt
+            if n_ee <= ee.capacity and n_pt <= pt.capacity and not (bst & (4 | 16)):
+                self.n_contacts, self.n_contacts_pt = n_ee, n_pt
+                self.query_status = qst
+                if qst & QUERY_FAILED:
+                    warnings.warn(f"contact query ran out of its traversal bound (status {qst}): "
+                                  "the candidate lists may be incomplete", RuntimeWarning, stacklevel=2)
+                self.collision_hessian = self._C
+                return self.A
+            self._A_graph = None  # overflow: the step-by-step path grows and re-tunes
+        A = self._compute_A_queue()
+        n_ee, n_pt = self.n_contacts, self.n_contacts_pt
+        cfg = self._tuner.best.get(str((int(self.dtype == torch.float64), bucket(n_ee + n_pt), bucket(self.n_tets))))
+        if cfg is None:
+            return A
+        cap = self._graph_buffers()
+        graph = torch.cuda.CUDAGraph()
+        torch.cuda.synchronize()
+        with N.no_collection(), torch.cuda.graph(graph):
+            self._enqueue_A(cfg, cap)
+        self._A_graph = (self._A_graph_key(), graph, cfg)
+        # the capture recorded the launches without running them: run them now
+        # so that this call's results are the graph's (same matrix as above)
+        graph.replay()
+        torch.cuda.current_stream().synchronize()
+        self.collision_hessian = self._C
+        return self.A
+
+    def _A_graph_key(self):
+        """The buffers a captured compute_A reads and writes (the schedule is
+        kept as captured while they stay: a later workload bucket's choice
+        would cost a recapture per change of bucket)."""
+        st = self._static
+        ee, pt, t = self.contacts_new, self.contacts_pt, self.collision_triplets
+        return (ee.a1a2b1b2.data_ptr(), ee.capacity, pt.a1a2b1b2.data_ptr(), pt.capacity,
+                None if t is None else t.rows.data_ptr(), None if self.A is None else self.A.values.data_ptr(),
+                None if getattr(self, "_C", None) is None else self._C.values.data_ptr(),
+                st.get("a_rows").data_ptr() if "a_rows" in st else None, self.states.x.data_ptr())
 
     def _compute_A_generic(self) -> BsrMatrix:
         """Per-term kernels, then one sort-based assembly of every triplet."""

@@ -127,7 +127,7 @@ class ContactPipeline(ContactBarrierMixin):
             return
         g = torch.cuda.CUDAGraph()
         torch.cuda.synchronize()
-        with torch.cuda.graph(g):
+        with N.no_collection(), torch.cuda.graph(g):
             self._enqueue()
         self._graph = (key, g)
 

@@ -131,3 +131,28 @@ def test_every_schedule_assembles_the_same_matrix(cuda, cfg):
     (Dg, bg), (Dq, bq) = out
     assert np.abs(Dq - Dg).max() <= 1e-12 * np.abs(Dg).max()
     assert np.abs(bq - bg).max() <= 1e-11 * np.abs(bg).max()
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_graph_replayed_compute_A_equals_step_by_step(cuda, dtype):
+    """compute_A replayed from its CUDA graph (device-side counts, capacities,
+    one host read) assembles the matrix and force of the step-by-step path."""
+    sc = small_scenes()[2]
+    rng = np.random.default_rng(5)
+    x = sc.x + rng.normal(scale=0.05 * sc.dhat, size=sc.x.shape)
+    out = []
+    for graph in (False, True):
+        s = _solver(sc, dtype, "queue")
+        s.graph_compute_A = graph
+        s.states.x.copy_(torch.tensor(x, dtype=dtype))
+        s.compute_A()
+        A = s.compute_A()  # with graph: a replay
+        assert (getattr(s, "_A_graph", None) is not None) == graph
+        assert s.n_contacts + s.n_contacts_pt > 0
+        out.append((_dense(A), s.b.double().cpu().numpy().copy(), s.n_contacts, s.n_contacts_pt))
+    ((Dg, rg, cg), bg, *ng), ((Dq, rq, cq), bq, *nq) = out
+    assert ng == nq
+    assert np.array_equal(rg, rq) and np.array_equal(cg, cq)
+    tol = 1e-5 if dtype == torch.float32 else 1e-12
+    assert np.abs(Dq - Dg).max() <= tol * np.abs(Dg).max()
+    assert np.abs(bq - bg).max() <= tol * max(np.abs(bg).max(), 1e-30) * 10
