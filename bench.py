@@ -599,6 +599,61 @@ def measure(name, args, dev, world, rank, torch, dist, full: bool):
     return out
 
 
+def run_sharded(args):
+    """``--shard``: one scene split over the N ranks (ipc_warp_b200.sharded:
+    query ranges, force / energy / TOI exchanged over NCCL); K device-timed
+    steps after W warm-up steps, max over ranks; value = the scene's pairs
+    per second (strong scaling)."""
+    import torch
+    import torch.distributed as dist
+
+    from ipc_warp_b200.sharded import ShardedContactPipeline
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    sc = scene(args.workload)
+    dx = torch.tensor(direction(sc), dtype=torch.float32, device=dev)
+    pipe = ShardedContactPipeline.from_scene(sc, rank, world, dtype=torch.float32, device=dev)
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    for _ in range(max(args.warmup, 3)):
+        r = pipe.iteration(dx)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = []
+    for _ in range(args.steps):
+        flush_l2(flush)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        r = pipe.iteration(dx)
+        b.record()
+        evs.append((a, b))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    total = sum(a.elapsed_time(b) for a, b in evs)
+    if world > 1:
+        total, _ = max_over_ranks([total, total], dev)
+    pairs = r.n_ee_total + r.n_pt_total
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": pairs * args.steps / (total * 1e-3), "unit": "pairs/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
+                          "ms_per_step": total / args.steps, "higher_is_better": True, "scaling": "strong",
+                          "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                          "config": {"workload": args.workload, "pairs": pairs, "parallelism": f"sharded x{world}",
+                                     "l2": "flushed between steps (256 MiB write)"}}))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -674,6 +729,8 @@ def main():
                     help="thread turns of the screw and nut (12 = the benchmark workload; fewer for ncu captures)")
     ap.add_argument("--rods", type=int, default=4,
                     help="rods per side of the bundle (4 = the benchmark workload; smaller for ncu section captures)")
+    ap.add_argument("--shard", action="store_true",
+                    help="split the headline workload over the N ranks (strong scaling) instead of N replicas")
     ap.add_argument("--profile-newton", action="store_true",
                     help="untimed Newton iterations (learned PCG, device line search), for ncu; prints nothing")
     args = ap.parse_args()
@@ -688,6 +745,8 @@ def main():
         return
     if args.impl == "reference":
         run_reference(args)
+    elif args.shard:
+        run_sharded(args)
     else:
         run_ours(args)
 

@@ -153,6 +153,17 @@ int ipcb_dcd_ee(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* edge_bv
 /* query_order: optional int32[n_verts] vertex visiting order (NULL = 0..V-1) */
 int ipcb_dcd_pt(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* tri_bvh, float thickness, float query_pad,
                 int exclude_same_body, const int* query_order, ipcb_contacts* out, int* status, ipcb_stream s);
+/* One scene's queries split over several GPUs: the same queries restricted to
+ * the queries first .. first + count - 1 (EE: the edges of those Morton ranks
+ * in edge_bvh, and every pair is met by its lower-ranked edge, so disjoint
+ * rank ranges partition the pair set; PT: those vertices of the visiting
+ * order).  ipcb_dcd_ee / ipcb_dcd_pt are the full ranges. */
+int ipcb_dcd_ee_range(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* edge_bvh, float thickness,
+                      float query_pad, int exclude_same_body, int first, int count, ipcb_contacts* out, int* status,
+                      ipcb_stream s);
+int ipcb_dcd_pt_range(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* tri_bvh, float thickness,
+                      float query_pad, int exclude_same_body, const int* query_order, int first, int count,
+                      ipcb_contacts* out, int* status, ipcb_stream s);
 
 /* ---- narrow phase (dynamic_contacts.py:152-246 contact_hessian_ee/pt, 375-398 energy) ----
  * kind 0 = EE list, 1 = PT list.  n >= 0: number of records; n < 0: read
@@ -210,6 +221,14 @@ int ipcb_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* s
                        ipcb_stream s);
 int ipcb_point_triangle_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* swept_tri_bvh, double pad,
                             int exclude_same_body, void* toi, int* status, void* ws, size_t ws_bytes, ipcb_stream s);
+/* The CCD queries restricted to a range of queries, as ipcb_dcd_ee_range /
+ * ipcb_dcd_pt_range (EE: Morton ranks of swept_edge_bvh; PT: vertices). */
+int ipcb_edge_edge_toi_range(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* swept_edge_bvh,
+                             const float* lower, const float* upper, int exclude_same_body, int first, int count,
+                             void* toi, int* status, void* ws, size_t ws_bytes, ipcb_stream s);
+int ipcb_point_triangle_toi_range(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* swept_tri_bvh, double pad,
+                                  int exclude_same_body, int first, int count, void* toi, int* status, void* ws,
+                                  size_t ws_bytes, ipcb_stream s);
 /* new_intersections (contact.py:587-670; edge_edge_intersections /
  * point_triangle_intersections 371-442): the CCD queries above that also
  * append every pair whose time of impact is < 1 to `out` as a record

@@ -120,6 +120,8 @@ SIGNATURES = {
     "ipcb_swept_triangle_aabbs": (c_int, [SP, P, c_double, P, P, P]),
     "ipcb_dcd_ee": (c_int, [SP, P, BP, c_float, c_float, c_int, CP, P, P]),
     "ipcb_dcd_pt": (c_int, [SP, P, BP, c_float, c_float, c_int, P, CP, P, P]),
+    "ipcb_dcd_ee_range": (c_int, [SP, P, BP, c_float, c_float, c_int, c_int, c_int, CP, P, P]),
+    "ipcb_dcd_pt_range": (c_int, [SP, P, BP, c_float, c_float, c_int, P, c_int, c_int, CP, P, P]),
     "ipcb_contact_hessian": (c_int, [c_int, SP, CP, c_int, c_int, c_double, P, P, P, P, P, P]),
     "ipcb_contact_hessian_after": (c_int, [c_int, SP, CP, c_int, c_int, P, c_double, P, P, P, P, P, P]),
     "ipcb_contact_hessian_workspace": (c_size_t, [c_int]),
@@ -129,6 +131,8 @@ SIGNATURES = {
     "ipcb_toi_workspace": (c_size_t, [c_int]),
     "ipcb_edge_edge_toi": (c_int, [SP, P, BP, P, P, c_int, P, P, P, c_size_t, P]),
     "ipcb_point_triangle_toi": (c_int, [SP, P, BP, c_double, c_int, P, P, P, c_size_t, P]),
+    "ipcb_edge_edge_toi_range": (c_int, [SP, P, BP, P, P, c_int, c_int, c_int, P, P, P, c_size_t, P]),
+    "ipcb_point_triangle_toi_range": (c_int, [SP, P, BP, c_double, c_int, c_int, c_int, P, P, P, c_size_t, P]),
     "ipcb_collision_time": (c_int, [c_int, c_int, P, P, P, P, P]),
     "ipcb_cubic_roots": (c_int, [c_int, P, c_double, c_double, P, P, P, P]),
     "ipcb_mpnn_param_count": (c_int, []),

@@ -521,13 +521,14 @@ template <class S, bool FAST>
 __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, const S* __restrict__ x1,
                                                     const int* __restrict__ edges, const int* __restrict__ body,
                                                     const float4* __restrict__ nodes, const int* __restrict__ order,
-                                                    int n, const float* __restrict__ lo, const float* __restrict__ hi,
-                                                    int exclude, CandList cand, S* toi, int* status, Sink sink,
-                                                    const int* gate) {
+                                                    int n, int first, int count, const float* __restrict__ lo,
+                                                    const float* __restrict__ hi, int exclude, CandList cand, S* toi,
+                                                    int* status, Sink sink, const int* gate) {
   if (gate && *gate == 0) return;
   bool dropped = false;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  bool active = t < n;
+  // queries: the edges of Morton rank first .. first + count - 1
+  int t = first + blockIdx.x * blockDim.x + threadIdx.x;
+  bool active = t < first + count;
   int i = active ? __ldg(order + t) : 0;
   int2 ea = __ldg(reinterpret_cast<const int2*>(edges) + i);
   int bi = exclude ? __ldg(body + ea.x) : 0;
@@ -588,13 +589,14 @@ __global__ void __launch_bounds__(128) k_ee_collect(const S* __restrict__ x0, co
 template <class S, bool FAST>
 __global__ void __launch_bounds__(128) k_pt_collect(const S* __restrict__ x0, const S* __restrict__ x1,
                                                     const int* __restrict__ tris, const int* __restrict__ body,
-                                                    const float4* __restrict__ nodes, int n_tris, int nv, double pad,
-                                                    int exclude, CandList cand, S* toi, int* status, Sink sink,
-                                                    const int* gate) {
+                                                    const float4* __restrict__ nodes, int n_tris, int first, int count,
+                                                    double pad, int exclude, CandList cand, S* toi, int* status,
+                                                    Sink sink, const int* gate) {
   if (gate && *gate == 0) return;
   bool dropped = false;
-  int i0 = blockIdx.x * blockDim.x + threadIdx.x;
-  bool active = i0 < nv;
+  // queries: the vertices first .. first + count - 1
+  int i0 = first + blockIdx.x * blockDim.x + threadIdx.x;
+  bool active = i0 < first + count;
   int i = active ? i0 : 0;
   d3 a = ld(x0, i), b = ld(x1, i);
   int bi = exclude ? __ldg(body + i) : 0;
@@ -1091,36 +1093,35 @@ __global__ void k_cubic(int n, const double* __restrict__ coef, double x0, doubl
 // solves every pair of the query in place.
 template <class S>
 void run_ee(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, const float* lower, const float* upper,
-            int exclude, CandList c, void* toi, int* status, Sink sink, cudaStream_t st) {
+            int exclude, CandList c, void* toi, int* status, Sink sink, cudaStream_t st, int first, int count) {
   const int n = soup->n_edges;
-  const dim3 g(div_up(n, 128));
+  const dim3 g(div_up(count, 128));
   cudaMemsetAsync(c.count, 0, 2 * sizeof(int), st);
   k_ee_collect<S, true><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->edges, soup->body,
-                                           (const float4*)bvh->wide, bvh->sorted, n, lower, upper, exclude, c,
-                                           (S*)toi, status, sink, nullptr);
+                                           (const float4*)bvh->wide, bvh->sorted, n, first, count, lower, upper,
+                                           exclude, c, (S*)toi, status, sink, nullptr);
   solve_candidates<S, 0>((const S*)soup->x, (const S*)x1, soup->edges, c.count, c, (S*)toi, status, sink, st);
   CandList none = c;
   none.capacity = 0;
   k_ee_collect<S, false><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->edges, soup->body,
-                                            (const float4*)bvh->wide, bvh->sorted, n, lower, upper, exclude, none,
-                                            (S*)toi, status, sink, c.overflow);
+                                            (const float4*)bvh->wide, bvh->sorted, n, first, count, lower, upper,
+                                            exclude, none, (S*)toi, status, sink, c.overflow);
 }
 
 template <class S>
 void run_pt(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, double pad, int exclude, CandList c,
-            void* toi, int* status, Sink sink, cudaStream_t st) {
-  const int nv = soup->n_verts;
-  const dim3 g(div_up(nv, 128));
+            void* toi, int* status, Sink sink, cudaStream_t st, int first, int count) {
+  const dim3 g(div_up(count, 128));
   cudaMemsetAsync(c.count, 0, 2 * sizeof(int), st);
   k_pt_collect<S, true><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->triangles, soup->body,
-                                           (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude, c, (S*)toi,
-                                           status, sink, nullptr);
+                                           (const float4*)bvh->wide, soup->n_tris, first, count, pad, exclude, c,
+                                           (S*)toi, status, sink, nullptr);
   solve_candidates<S, 1>((const S*)soup->x, (const S*)x1, soup->triangles, c.count, c, (S*)toi, status, sink, st);
   CandList none = c;
   none.capacity = 0;
   k_pt_collect<S, false><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->triangles, soup->body,
-                                            (const float4*)bvh->wide, soup->n_tris, nv, pad, exclude, none, (S*)toi,
-                                            status, sink, c.overflow);
+                                            (const float4*)bvh->wide, soup->n_tris, first, count, pad, exclude, none,
+                                            (S*)toi, status, sink, c.overflow);
 }
 
 }  // namespace
@@ -1173,29 +1174,55 @@ int ipcb_swept_triangle_aabbs(const ipcb_soup* soup, const void* x1, double pad,
 
 size_t ipcb_toi_workspace(int capacity) { return kCandHeader + (size_t)(capacity > 0 ? capacity : 0) * kCandPerPair; }
 
-int ipcb_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, const float* lower,
-                       const float* upper, int exclude_same_body, void* toi, int* status, void* ws, size_t ws_bytes,
-                       ipcb_stream s) {
+int ipcb_edge_edge_toi_range(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, const float* lower,
+                             const float* upper, int exclude_same_body, int first, int count, void* toi, int* status,
+                             void* ws, size_t ws_bytes, ipcb_stream s) {
   if (!soup || !x1 || !bvh || !lower || !upper || !toi || !status || !ws || ws_bytes < kCandHeader ||
       bvh->n != soup->n_edges)
     return IPCB_E_ARG;
-  if (soup->n_edges == 0) return IPCB_OK;
+  const int n = soup->n_edges;
+  if (first < 0 || count < 0 || first > n || count > n - first) return IPCB_E_ARG;
+  if (count == 0) return IPCB_OK;
   const CandList c = cand_list(ws, ws_bytes);
-  if (soup->fp64) run_ee<double>(soup, x1, bvh, lower, upper, exclude_same_body, c, toi, status, Sink{}, (cudaStream_t)s);
-  else run_ee<float>(soup, x1, bvh, lower, upper, exclude_same_body, c, toi, status, Sink{}, (cudaStream_t)s);
+  if (soup->fp64)
+    run_ee<double>(soup, x1, bvh, lower, upper, exclude_same_body, c, toi, status, Sink{}, (cudaStream_t)s, first,
+                   count);
+  else
+    run_ee<float>(soup, x1, bvh, lower, upper, exclude_same_body, c, toi, status, Sink{}, (cudaStream_t)s, first,
+                  count);
   return check_launch("ipcb_edge_edge_toi");
+}
+
+int ipcb_edge_edge_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, const float* lower,
+                       const float* upper, int exclude_same_body, void* toi, int* status, void* ws, size_t ws_bytes,
+                       ipcb_stream s) {
+  if (!soup) return IPCB_E_ARG;
+  return ipcb_edge_edge_toi_range(soup, x1, bvh, lower, upper, exclude_same_body, 0, soup->n_edges, toi, status, ws,
+                                  ws_bytes, s);
+}
+
+int ipcb_point_triangle_toi_range(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, double pad,
+                                  int exclude_same_body, int first, int count, void* toi, int* status, void* ws,
+                                  size_t ws_bytes, ipcb_stream s) {
+  if (!soup || !x1 || !bvh || !toi || !status || !ws || ws_bytes < kCandHeader || bvh->n != soup->n_tris)
+    return IPCB_E_ARG;
+  const int nv = soup->n_verts;
+  if (first < 0 || count < 0 || first > nv || count > nv - first) return IPCB_E_ARG;
+  if (count == 0 || soup->n_tris == 0) return IPCB_OK;
+  const CandList c = cand_list(ws, ws_bytes);
+  if (soup->fp64)
+    run_pt<double>(soup, x1, bvh, pad, exclude_same_body, c, toi, status, Sink{}, (cudaStream_t)s, first, count);
+  else
+    run_pt<float>(soup, x1, bvh, pad, exclude_same_body, c, toi, status, Sink{}, (cudaStream_t)s, first, count);
+  return check_launch("ipcb_point_triangle_toi");
 }
 
 int ipcb_point_triangle_toi(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, double pad,
                             int exclude_same_body, void* toi, int* status, void* ws, size_t ws_bytes,
                             ipcb_stream s) {
-  if (!soup || !x1 || !bvh || !toi || !status || !ws || ws_bytes < kCandHeader || bvh->n != soup->n_tris)
-    return IPCB_E_ARG;
-  if (soup->n_verts == 0 || soup->n_tris == 0) return IPCB_OK;
-  const CandList c = cand_list(ws, ws_bytes);
-  if (soup->fp64) run_pt<double>(soup, x1, bvh, pad, exclude_same_body, c, toi, status, Sink{}, (cudaStream_t)s);
-  else run_pt<float>(soup, x1, bvh, pad, exclude_same_body, c, toi, status, Sink{}, (cudaStream_t)s);
-  return check_launch("ipcb_point_triangle_toi");
+  if (!soup) return IPCB_E_ARG;
+  return ipcb_point_triangle_toi_range(soup, x1, bvh, pad, exclude_same_body, 0, soup->n_verts, toi, status, ws,
+                                       ws_bytes, s);
 }
 
 int ipcb_edge_edge_intersections(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, const float* lower,
@@ -1208,8 +1235,11 @@ int ipcb_edge_edge_intersections(const ipcb_soup* soup, const void* x1, const ip
   if (soup->n_edges == 0) return IPCB_OK;
   const CandList c = cand_list(ws, ws_bytes);
   const Sink sink{*out, thickness * 2.0, 1};
-  if (soup->fp64) run_ee<double>(soup, x1, bvh, lower, upper, exclude_same_body, c, toi, status, sink, (cudaStream_t)s);
-  else run_ee<float>(soup, x1, bvh, lower, upper, exclude_same_body, c, toi, status, sink, (cudaStream_t)s);
+  const int n = soup->n_edges;
+  if (soup->fp64)
+    run_ee<double>(soup, x1, bvh, lower, upper, exclude_same_body, c, toi, status, sink, (cudaStream_t)s, 0, n);
+  else
+    run_ee<float>(soup, x1, bvh, lower, upper, exclude_same_body, c, toi, status, sink, (cudaStream_t)s, 0, n);
   return check_launch("ipcb_edge_edge_intersections");
 }
 
@@ -1223,8 +1253,11 @@ int ipcb_point_triangle_intersections(const ipcb_soup* soup, const void* x1, con
   if (soup->n_verts == 0 || soup->n_tris == 0) return IPCB_OK;
   const CandList c = cand_list(ws, ws_bytes);
   const Sink sink{*out, thickness * 2.0, 1};
-  if (soup->fp64) run_pt<double>(soup, x1, bvh, pad, exclude_same_body, c, toi, status, sink, (cudaStream_t)s);
-  else run_pt<float>(soup, x1, bvh, pad, exclude_same_body, c, toi, status, sink, (cudaStream_t)s);
+  const int nv = soup->n_verts;
+  if (soup->fp64)
+    run_pt<double>(soup, x1, bvh, pad, exclude_same_body, c, toi, status, sink, (cudaStream_t)s, 0, nv);
+  else
+    run_pt<float>(soup, x1, bvh, pad, exclude_same_body, c, toi, status, sink, (cudaStream_t)s, 0, nv);
   return check_launch("ipcb_point_triangle_intersections");
 }
 

@@ -93,10 +93,12 @@ IPCB_D int warp_max(int v) {
 template <class S>
 __global__ void __launch_bounds__(128) k_dcd_ee(const float4* __restrict__ x4, const int* __restrict__ edges,
                                                 const int* __restrict__ body, const float4* __restrict__ nodes,
-                                                const int* __restrict__ order, int n, float thickness, float qpad,
-                                                int exclude, ipcb_contacts out, int* status) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  bool active = t < n;
+                                                const int* __restrict__ order, int n, int first, int count,
+                                                float thickness, float qpad, int exclude, ipcb_contacts out,
+                                                int* status) {
+  // queries: the edges of Morton rank first .. first + count - 1
+  int t = first + blockIdx.x * blockDim.x + threadIdx.x;
+  bool active = t < first + count;
   int i = active ? __ldg(order + t) : 0;
   int2 ea = active ? __ldg(reinterpret_cast<const int2*>(edges) + i) : make_int2(0, 0);
   f3 p1 = load4(x4, ea.x), p2 = load4(x4, ea.y);
@@ -148,10 +150,12 @@ __global__ void __launch_bounds__(128) k_dcd_ee(const float4* __restrict__ x4, c
 template <class S>
 __global__ void __launch_bounds__(128) k_dcd_pt(const float4* __restrict__ x4, const int* __restrict__ tris,
                                                 const int* __restrict__ body, const float4* __restrict__ nodes,
-                                                int n_tris, const int* __restrict__ order, int nv, float thickness,
-                                                float qpad, int exclude, ipcb_contacts out, int* status) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  bool active = t < nv;
+                                                int n_tris, const int* __restrict__ order, int first, int count,
+                                                float thickness, float qpad, int exclude, ipcb_contacts out,
+                                                int* status) {
+  // queries: the vertices first .. first + count - 1 of the visiting order
+  int t = first + blockIdx.x * blockDim.x + threadIdx.x;
+  bool active = t < first + count;
   int i = active ? (order ? __ldg(order + t) : t) : 0;
   f3 p = load4(x4, i);
   int bi = exclude ? __ldg(body + i) : 0;
@@ -377,38 +381,55 @@ int ipcb_triangle_aabbs(const ipcb_soup* soup, const float* x4, float pad, float
   return check_launch("ipcb_triangle_aabbs");
 }
 
-int ipcb_dcd_ee(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* bvh, float thickness, float query_pad,
-                int exclude_same_body, ipcb_contacts* out, int* status, ipcb_stream s) {
+int ipcb_dcd_ee_range(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* bvh, float thickness,
+                      float query_pad, int exclude_same_body, int first, int count, ipcb_contacts* out, int* status,
+                      ipcb_stream s) {
   if (!soup || !x4 || !bvh || !out || !status || bvh->n != soup->n_edges) return IPCB_E_ARG;
   int n = soup->n_edges;
-  if (n == 0) return IPCB_OK;
-  dim3 grid(div_up(n, 128));
+  if (first < 0 || count < 0 || first > n || count > n - first) return IPCB_E_ARG;
+  if (count == 0) return IPCB_OK;
+  dim3 grid(div_up(count, 128));
   if (soup->fp64)
     k_dcd_ee<double><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->edges, soup->body,
-                                                        (const float4*)bvh->wide, bvh->sorted, n, thickness,
-                                                        query_pad, exclude_same_body, *out, status);
+                                                        (const float4*)bvh->wide, bvh->sorted, n, first, count,
+                                                        thickness, query_pad, exclude_same_body, *out, status);
   else
     k_dcd_ee<float><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->edges, soup->body,
-                                                       (const float4*)bvh->wide, bvh->sorted, n, thickness,
-                                                       query_pad, exclude_same_body, *out, status);
+                                                       (const float4*)bvh->wide, bvh->sorted, n, first, count,
+                                                       thickness, query_pad, exclude_same_body, *out, status);
   return check_launch("ipcb_dcd_ee");
+}
+
+int ipcb_dcd_ee(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* bvh, float thickness, float query_pad,
+                int exclude_same_body, ipcb_contacts* out, int* status, ipcb_stream s) {
+  if (!soup) return IPCB_E_ARG;
+  return ipcb_dcd_ee_range(soup, x4, bvh, thickness, query_pad, exclude_same_body, 0, soup->n_edges, out, status, s);
+}
+
+int ipcb_dcd_pt_range(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* bvh, float thickness,
+                      float query_pad, int exclude_same_body, const int* query_order, int first, int count,
+                      ipcb_contacts* out, int* status, ipcb_stream s) {
+  if (!soup || !x4 || !bvh || !out || !status || bvh->n != soup->n_tris) return IPCB_E_ARG;
+  int nv = soup->n_verts;
+  if (first < 0 || count < 0 || first > nv || count > nv - first) return IPCB_E_ARG;
+  if (count == 0 || soup->n_tris == 0) return IPCB_OK;
+  dim3 grid(div_up(count, 128));
+  if (soup->fp64)
+    k_dcd_pt<double><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->triangles, soup->body,
+                                                        (const float4*)bvh->wide, soup->n_tris, query_order, first,
+                                                        count, thickness, query_pad, exclude_same_body, *out, status);
+  else
+    k_dcd_pt<float><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->triangles, soup->body,
+                                                       (const float4*)bvh->wide, soup->n_tris, query_order, first,
+                                                       count, thickness, query_pad, exclude_same_body, *out, status);
+  return check_launch("ipcb_dcd_pt");
 }
 
 int ipcb_dcd_pt(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* bvh, float thickness, float query_pad,
                 int exclude_same_body, const int* query_order, ipcb_contacts* out, int* status, ipcb_stream s) {
-  if (!soup || !x4 || !bvh || !out || !status || bvh->n != soup->n_tris) return IPCB_E_ARG;
-  int nv = soup->n_verts;
-  if (nv == 0 || soup->n_tris == 0) return IPCB_OK;
-  dim3 grid(div_up(nv, 128));
-  if (soup->fp64)
-    k_dcd_pt<double><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->triangles, soup->body,
-                                                        (const float4*)bvh->wide, soup->n_tris, query_order, nv,
-                                                        thickness, query_pad, exclude_same_body, *out, status);
-  else
-    k_dcd_pt<float><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->triangles, soup->body,
-                                                       (const float4*)bvh->wide, soup->n_tris, query_order, nv,
-                                                       thickness, query_pad, exclude_same_body, *out, status);
-  return check_launch("ipcb_dcd_pt");
+  if (!soup) return IPCB_E_ARG;
+  return ipcb_dcd_pt_range(soup, x4, bvh, thickness, query_pad, exclude_same_body, query_order, 0, soup->n_verts,
+                           out, status, s);
 }
 
 
