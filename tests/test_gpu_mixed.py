@@ -156,3 +156,35 @@ def test_wrecking_balls_trajectory(cuda):
     assert np.abs(q[g:g + 4] - q0[g:g + 4]).max() == 0.0
     assert s.orthogonality_error() < 1e-3
     assert hit
+
+
+def test_mixed_system_matches_oracle_at_impact(cuda):
+    """The Newton matrix and gradient of the 4-ball wrecking-balls scene in
+    float64, taken at the first step where a ball touches its cubes, against
+    the oracle's J^T H J assembly (sparse comparison)."""
+    sc = scenes.wrecking_balls(n_balls=4, subdiv=3, cube_cells=3, ground_quads=16, max_angle_deg=60.0,
+                               kappa=1e12, seed=2)
+    s = MixedSolver(sc, E=5e5, nu=0.4, h=1e-2, dtype=torch.float64, maxiter=4000)
+    n_fem_bodies = int(sc.fem.body.max()) + 1
+    body = s.soup.body.cpu().numpy()
+    for k in range(80):
+        s.step()
+        s.prepare()
+        s.compute_A()
+        n_ee, n_pt = s.n_contacts, s.n_contacts_pt
+        recs = np.concatenate([s.contacts_new.records(n_ee)[:, :4].cpu().numpy(),
+                               s.contacts_pt.records(n_pt)[:, :4].cpu().numpy()])
+        b = body[recs]
+        ball = ((b >= n_fem_bodies) & (b < n_fem_bodies + 4)).any(axis=1)
+        if bool((ball & (b < n_fem_bodies).any(axis=1)).any()):
+            break
+    else:
+        pytest.fail("no ball reached its cubes")
+    p, m = _oracle(s)
+    g_ref, A_ref, ne, npt = om.system(p, m, _host(s.q), _host(s.xt_f), _host(s.qt_a), x=_host(s.x))
+    assert (ne, npt) == (s.n_contacts, s.n_contacts_pt)
+    d = (s.A.to_scipy().tocsr() - A_ref).tocoo()
+    scale = abs(A_ref).max()
+    assert (abs(d.data).max() if d.nnz else 0.0) <= 1e-9 * scale
+    g = _host(s.rhs)
+    assert np.abs(g - g_ref).max() <= 1e-9 * np.abs(g_ref).max()
