@@ -161,6 +161,11 @@ NARROW_BYTES = {"pt": 824, "ee": 872}
 # launches (k_contact_hessian_sorted) of one step: one-pass ncu capture of each
 # full workload
 NARROW_DRAM_BYTES_PER_STEP = {"rod_bundle": 464.2e6, "screw_nut": 169.6e6}
+# DRAM bytes (read + write) of the CCD edge-edge query per step -- k_ee_collect
+# (both passes), k_cand_bound, k_cand_bucket, k_cand_solve -- from one ncu pass
+# of dram__bytes_read.sum + dram__bytes_write.sum on the full workload (caches
+# flushed before each launch, so an upper bound on the in-step traffic)
+CCD_DRAM_BYTES_PER_STEP = {"rod_bundle": 41.6e6, "screw_nut": 342.1e6}
 
 
 def stage_times(pipe, dx, reps, torch):
@@ -459,6 +464,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(args.workload, sc, pairs),
+        "details": {"parallelism": f"{cores} host threads (OpenMP)"},
         "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": "port",
                          "sample": "full workload, one DCD+narrow+energy+BSR+CCD pass per step (C++ oracle, OpenMP)"},
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -466,10 +472,14 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+L2_NOTE = "GPU arm: L2 flushed between timed steps (256 MiB write)"
+
+
 def workload_config(name, sc, pairs):
-    """The config keys both arms report for a workload."""
+    """The config both arms report for a workload (identical keys and values;
+    run details go beside it, in ``details``)."""
     return {"workload": WORKLOADS[name], "verts": sc.n_verts, "edges": sc.n_edges, "tris": sc.n_tris,
-            "dhat": sc.dhat, "pairs": pairs}
+            "dhat": sc.dhat, "pairs": pairs, "l2": L2_NOTE}
 
 
 def max_over_ranks(values, device):
@@ -581,7 +591,7 @@ def measure(name, args, dev, world, rank, torch, dist, full: bool):
     ccd_achieved = ccd_algo / (st["ccd_query_ee"] * 1e-3) / 1e9
     ccd_roof = {"kernel": "k_ee_collect + k_cand_toi (CCD edge-edge query)", "bound": "hbm",
                 "achieved": ccd_achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                "frac": ccd_achieved / peak, "traffic": None, "algorithmic_bytes": ccd_algo,
+                "frac": ccd_achieved / peak, "traffic": CCD_DRAM_BYTES_PER_STEP[name], "algorithmic_bytes": ccd_algo,
                 "note": "bound by the double-precision root isolation and the dependent position gathers, "
                         "not by DRAM"}
     dominant = "ccd" if st["ccd_query_ee"] > narrow_ms else "narrow"
@@ -647,8 +657,8 @@ def run_sharded(args):
                           "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
                           "ms_per_step": total / args.steps, "higher_is_better": True, "scaling": "strong",
                           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                          "config": {"workload": args.workload, "pairs": pairs, "parallelism": f"sharded x{world}",
-                                     "l2": "flushed between steps (256 MiB write)"}}))
+                          "config": workload_config(args.workload, sc, pairs),
+                          "details": {"parallelism": f"sharded x{world}"}}))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -686,14 +696,13 @@ def run_ours(args):
         wrecking = None if args.no_newton else wrecking_balls_steps(dev, torch)
         sc = head.pop("sc")
         cfg = workload_config(args.workload, sc, head["pairs"])
-        cfg.update({"n_ee": head["n_ee"], "n_pt": head["n_pt"], "ccd_candidates": head["ccd_candidates"],
-                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
-                    "stage_ms": head["stage_ms"]})
+        details = {"n_ee": head["n_ee"], "n_pt": head["n_pt"], "ccd_candidates": head["ccd_candidates"],
+                   "parallelism": f"replicas x{world}", "stage_ms": head["stage_ms"]}
         out = {
             "metric": METRIC, "value": head["value"], "unit": "pairs/s",
             "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": head["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": cfg, "roofline": head["roofline"],
+            "data": "synthetic", "config": cfg, "details": details, "roofline": head["roofline"],
             "roofline_narrow": head["roofline_narrow"], "roofline_ccd": head["roofline_ccd"],
             "cpu_baseline": head["cpu_baseline"],
             "e2e": head["e2e"], "gpu_launches": head["gpu_launches"], "kernels": head["kernels"], "clocks": clocks,
