@@ -738,6 +738,12 @@ typedef struct {
   const void* b;
   void *x, *r, *z, *p, *q, *t;
   ipcb_pcg_state* state;
+  /* precond 0 with n_groups > 0 (a mixed FEM + affine-body system): rows
+   * n_point + 4 g .. + 3 form group g (one affine body's p, a0, a1, a2) and
+   * use the inverse of their 12x12 diagonal block, dinv_group scalar[144
+   * n_groups] from ipcb_group_jacobi; n = n_point + 4 n_groups. */
+  int n_point, n_groups;
+  const void* dinv_group;
 } ipcb_pcg;
 
 int ipcb_pcg_start(const ipcb_pcg* P, double tol, int maxiter, ipcb_stream s);
@@ -745,6 +751,11 @@ int ipcb_pcg_iterate(const ipcb_pcg* P, int k, ipcb_stream s);
 /* Inverse diagonal blocks (diag may be NULL: found by a row scan). */
 int ipcb_block_jacobi(int n, const int* offsets, const int* columns, const int* diag, const void* values, int fp64,
                       void* dinv, int* status, ipcb_stream s);
+/* Inverses of the 12x12 diagonal blocks of the row groups n_point + 4 g .. + 3
+ * (g < n_groups), row-major scalar[144 n_groups]; IPCB_STATUS_PATTERN when a
+ * block is singular (its inverse is then the identity). */
+int ipcb_group_jacobi(int n_point, int n_groups, const int* offsets, const int* columns, const void* values,
+                      int fp64, void* dinv_group, int* status, ipcb_stream s);
 /* bf16 copy of the FSAI factor for the apply: lower and diagonal blocks as
  * they are, upper slots holding the transposed lower block. */
 int ipcb_fsai_mirror(const ipcb_graph* g, const float* G, void* gh, ipcb_stream s);

@@ -88,7 +88,8 @@ class PcgState(ctypes.Structure):
 class Pcg(ctypes.Structure):
     _fields_ = [("n", c_int), ("fp64", c_int), ("precond", c_int), ("offsets", P), ("columns", P), ("values", P),
                 ("dinv", P), ("g_offsets", P), ("g_columns", P), ("diag", P), ("g", P), ("scale", P), ("b", P),
-                ("x", P), ("r", P), ("z", P), ("p", P), ("q", P), ("t", P), ("state", P)]
+                ("x", P), ("r", P), ("z", P), ("p", P), ("q", P), ("t", P), ("state", P), ("n_point", c_int),
+                ("n_groups", c_int), ("dinv_group", P)]
 
 
 SP, CP, BP = ctypes.POINTER(Soup), ctypes.POINTER(Contacts), ctypes.POINTER(Lbvh)
@@ -151,6 +152,7 @@ SIGNATURES = {
     "ipcb_pcg_start": (c_int, [ctypes.POINTER(Pcg), c_double, c_int, P]),
     "ipcb_pcg_iterate": (c_int, [ctypes.POINTER(Pcg), c_int, P]),
     "ipcb_block_jacobi": (c_int, [c_int, P, P, P, P, c_int, P, P, P]),
+    "ipcb_group_jacobi": (c_int, [c_int, c_int, P, P, P, c_int, P, P, P]),
     "ipcb_fsai_mirror": (c_int, [GP, P, P, P]),
     "ipcb_terms_launch": (c_int, [ctypes.POINTER(Terms), c_int, c_int, c_int, c_int, P]),
     "ipcb_bsr_slots": (c_int, [c_int, P, P, c_int, P, P, P, P]),

@@ -213,6 +213,154 @@ __global__ void __launch_bounds__(kBlock) k_update_xr_jacobi(int n, T* __restric
   }
 }
 
+// Item layout of the grouped update: items i < n_point are the 3x3 block
+// rows; from the next multiple of 32 on, 16 lanes per group (lanes 0..11 its
+// rows, 12..15 idle), so a warp holds two whole groups.
+__host__ __device__ inline int group_base(int n_point) { return (n_point + 31) & ~31; }
+__host__ __device__ inline long long group_items(int n_point, int n_groups) {
+  return group_base(n_point) + 16LL * ((n_groups + 1) & ~1);
+}
+
+// The same for a system with row groups (one affine body each): a group's
+// 16-lane half-warp updates its 12 rows of x and r, exchanges the new
+// residuals by shuffles, and lane c takes row c of the 12x12 inverse block.
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_update_xr_groups(int n_point, int n_groups, T* __restrict__ x,
+                                                             T* __restrict__ r, const T* __restrict__ p,
+                                                             const T* __restrict__ q, const T* __restrict__ dinv,
+                                                             const T* __restrict__ dinv_group, T* __restrict__ z,
+                                                             ipcb_pcg_state* st) {
+  if (st->done) return;
+  const double alpha = st->pAp > 0.0 ? st->rz / st->pAp : 0.0;
+  const int base = group_base(n_point);
+  const long long total = group_items(n_point, n_groups);
+  double prr = 0.0, prz = 0.0;
+  // total and the stride are multiples of 32: a warp runs the loop as a whole
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (i < n_point) {
+      T rv[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const long long k = 3 * i + c;
+        x[k] += (T)alpha * p[k];
+        rv[c] = r[k] - (T)alpha * q[k];
+        r[k] = rv[c];
+        prr += (double)rv[c] * rv[c];
+      }
+      const T* d = dinv + 9 * i;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const T zc = d[3 * c] * rv[0] + d[3 * c + 1] * rv[1] + d[3 * c + 2] * rv[2];
+        z[3 * i + c] = zc;
+        prz += (double)rv[c] * zc;
+      }
+    } else if (i >= base) {  // whole warps only (base is a multiple of 32)
+      const long long j = i - base;
+      const int g = (int)(j >> 4), c = (int)(j & 15);
+      const bool on = g < n_groups && c < 12;
+      const long long o = 3LL * n_point + 12LL * g + c;
+      T rv = T(0);
+      if (on) {
+        x[o] += (T)alpha * p[o];
+        rv = r[o] - (T)alpha * q[o];
+        r[o] = rv;
+        prr += (double)rv * rv;
+      }
+      const T* d = dinv_group + 144LL * g + 12 * c;
+      T zc = T(0);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) {
+        const T rk = __shfl_sync(0xffffffffu, rv, k, 16);
+        if (on) zc += d[k] * rk;
+      }
+      if (on) {
+        z[o] = zc;
+        prz += (double)rv * zc;
+      }
+    }
+  }
+  block_sum2(prr, prz);
+  if (threadIdx.x == 0) {
+    atomicAdd(&st->rr, prr);
+    atomicAdd(&st->rz_new, prz);
+  }
+}
+
+// z = (group) block-Jacobi r ; state.rz_new += r.z (the start of a solve)
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_jacobi_groups(int n_point, int n_groups, const T* __restrict__ dinv,
+                                                          const T* __restrict__ dinv_group, const T* __restrict__ r,
+                                                          T* __restrict__ z, ipcb_pcg_state* st) {
+  if (st->done) return;
+  double part = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_point + n_groups; i += gridDim.x * blockDim.x) {
+    const bool grp = i >= n_point;
+    const int w = grp ? 12 : 3;
+    const long long o = grp ? 3LL * n_point + 12LL * (i - n_point) : 3LL * i;
+    const T* d = grp ? dinv_group + 144LL * (i - n_point) : dinv + 9LL * i;
+    for (int c = 0; c < w; ++c) {
+      T zc = T(0);
+      for (int k = 0; k < w; ++k) zc += d[w * c + k] * r[o + k];
+      z[o + c] = zc;
+      part += (double)r[o + c] * zc;
+    }
+  }
+  part = block_sum(part);
+  if (threadIdx.x == 0) atomicAdd(&st->rz_new, part);
+}
+
+// one thread per group: gather the 16 3x3 blocks of rows / columns
+// n_point + 4 g .. + 3 from the BSR, invert the 12x12 in double (Gauss-Jordan,
+// partial pivoting)
+template <class T>
+__global__ void k_group_inverse(int n_point, int n_groups, const int* __restrict__ off, const int* __restrict__ cols,
+                                const T* __restrict__ vals, T* __restrict__ out, int* __restrict__ status) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_groups) return;
+  double a[12][24];
+  for (int i = 0; i < 12; ++i)
+    for (int j = 0; j < 24; ++j) a[i][j] = (j == 12 + i) ? 1.0 : 0.0;
+  const int r0 = n_point + 4 * g;
+  for (int bi = 0; bi < 4; ++bi) {
+    const int row = r0 + bi;
+    for (int k = off[row]; k < off[row + 1]; ++k) {
+      const int c = cols[k] - r0;
+      if (c < 0 || c >= 4) continue;
+      for (int u = 0; u < 3; ++u)
+        for (int v = 0; v < 3; ++v) a[3 * bi + u][3 * c + v] += (double)vals[9LL * k + 3 * u + v];
+    }
+  }
+  bool ok = true;
+  for (int c = 0; c < 12 && ok; ++c) {
+    int piv = c;
+    for (int i = c + 1; i < 12; ++i)
+      if (fabs(a[i][c]) > fabs(a[piv][c])) piv = i;
+    if (!(fabs(a[piv][c]) > 0.0)) {
+      ok = false;
+      break;
+    }
+    if (piv != c)
+      for (int j = 0; j < 24; ++j) {
+        const double t = a[c][j];
+        a[c][j] = a[piv][j];
+        a[piv][j] = t;
+      }
+    const double inv = 1.0 / a[c][c];
+    for (int j = 0; j < 24; ++j) a[c][j] *= inv;
+    for (int i = 0; i < 12; ++i) {
+      if (i == c) continue;
+      const double f = a[i][c];
+      if (f != 0.0)
+        for (int j = 0; j < 24; ++j) a[i][j] -= f * a[c][j];
+    }
+  }
+  T* d = out + 144LL * g;
+  if (!ok) atomicOr(status, IPCB_STATUS_PATTERN);
+  for (int i = 0; i < 12; ++i)
+    for (int j = 0; j < 12; ++j) d[12 * i + j] = ok ? (T)a[i][12 + j] : (T)(i == j ? 1.0 : 0.0);
+}
+
 // z = D^-1 r (block Jacobi) ; state.rz_new += r.z
 template <class T>
 __global__ void __launch_bounds__(kBlock) k_jacobi(int n, const T* __restrict__ dinv, const T* __restrict__ r,
@@ -425,7 +573,10 @@ int flat_grid(long long m) {
 template <class T>
 int precond(const ipcb_pcg* P, cudaStream_t s) {
   const int n = P->n;
-  if (P->precond == 0)
+  if (P->precond == 0 && P->n_groups > 0)
+    k_jacobi_groups<T><<<flat_grid(P->n_point + P->n_groups), kBlock, 0, s>>>(
+        P->n_point, P->n_groups, (const T*)P->dinv, (const T*)P->dinv_group, (const T*)P->r, (T*)P->z, P->state);
+  else if (P->precond == 0)
     k_jacobi<T><<<flat_grid(n), kBlock, 0, s>>>(n, (const T*)P->dinv, (const T*)P->r, (T*)P->z, P->state);
   else {
     k_fsai_lower<T><<<warp_grid(n), kBlock, 0, s>>>(n, P->g_offsets, P->diag, P->g_columns, (const bf16*)P->g,
@@ -452,7 +603,11 @@ int iterate(const ipcb_pcg* P, int k, cudaStream_t s) {
   for (int it = 0; it < k; ++it) {
     k_spmv_dot<T><<<warp_grid(n), kBlock, 0, s>>>(n, P->offsets, P->columns, (const T*)P->values, (const T*)P->p,
                                                      (T*)P->q, P->state);
-    if (P->precond == 0) {
+    if (P->precond == 0 && P->n_groups > 0) {
+      k_update_xr_groups<T><<<flat_grid(group_items(P->n_point, P->n_groups)), kBlock, 0, s>>>(
+          P->n_point, P->n_groups, (T*)P->x, (T*)P->r, (const T*)P->p, (const T*)P->q, (const T*)P->dinv,
+          (const T*)P->dinv_group, (T*)P->z, P->state);
+    } else if (P->precond == 0) {
       k_update_xr_jacobi<T><<<flat_grid(n), kBlock, 0, s>>>(n, (T*)P->x, (T*)P->r, (const T*)P->p, (const T*)P->q,
                                                             (const T*)P->dinv, (T*)P->z, P->state);
     } else {
@@ -469,6 +624,9 @@ bool pcg_ok(const ipcb_pcg* P) {
   if (!P || P->n <= 0 || !P->offsets || !P->columns || !P->values || !P->x || !P->r || !P->z || !P->p || !P->q ||
       !P->b || !P->state)
     return false;
+  if (P->n_groups < 0 || P->n_point < 0 || P->n_point > (1 << 30)) return false;
+  if (P->precond == 0 && P->n_groups > 0)
+    return P->dinv && P->dinv_group && P->n == P->n_point + 4 * P->n_groups;
   if (P->precond == 0) return P->dinv != nullptr;
   if (P->precond == 1) return P->g_offsets && P->g_columns && P->diag && P->g && P->scale && P->t;
   return false;
@@ -512,6 +670,21 @@ int ipcb_block_jacobi(int n, const int* offsets, const int* columns, const int* 
     k_block_jacobi<float><<<gridn(n), kBlock, 0, (cudaStream_t)s>>>(n, diag, offsets, columns, (const float*)values,
                                                                     (float*)dinv, status);
   return ipcb::check_launch("ipcb_block_jacobi");
+}
+
+int ipcb_group_jacobi(int n_point, int n_groups, const int* offsets, const int* columns, const void* values,
+                      int fp64, void* dinv_group, int* status, ipcb_stream s) {
+  if (n_point < 0 || n_groups < 0 || (n_groups && (!offsets || !columns || !values || !dinv_group || !status)))
+    return IPCB_E_ARG;
+  if (n_groups == 0) return IPCB_OK;
+  const int g = gridn(n_groups, 64);
+  if (fp64)
+    k_group_inverse<double><<<g, 64, 0, (cudaStream_t)s>>>(n_point, n_groups, offsets, columns,
+                                                           (const double*)values, (double*)dinv_group, status);
+  else
+    k_group_inverse<float><<<g, 64, 0, (cudaStream_t)s>>>(n_point, n_groups, offsets, columns, (const float*)values,
+                                                          (float*)dinv_group, status);
+  return ipcb::check_launch("ipcb_group_jacobi");
 }
 
 int ipcb_fsai_mirror(const ipcb_graph* g, const float* G, void* gh, ipcb_stream s) {

@@ -48,10 +48,17 @@ class MixedSolver(ContactBarrierMixin):
                  rho: float = 1000.0, density: float = 1000.0, affine_stiffness: float = 1e8,
                  gravity=(0.0, -9.8, 0.0), h: float = 1e-2, dtype=torch.float32, device="cuda",
                  vel_tol: float = 5e-2, max_newton: int = 100, tol: float = 1e-4, maxiter: int = 500,
-                 exclude_same_body: bool = True, direct_fallback: bool = True, assembly: str = "queue"):
+                 exclude_same_body: bool = True, direct_fallback: bool = True, assembly: str = "queue",
+                 preconditioner: str = "body_block"):
         if assembly not in ("queue", "separate"):
             raise ValueError(f"unknown assembly {assembly!r}")
+        if preconditioner not in ("body_block", "jacobi"):
+            raise ValueError(f"unknown preconditioner {preconditioner!r}")
         self.assembly = assembly
+        # "body_block": 3x3 blocks for the FEM vertices, the 12x12 diagonal
+        # block for each affine body's (p, a0, a1, a2); "jacobi": 3x3 blocks
+        # throughout
+        self.preconditioner = preconditioner
         self.h = float(h)
         self.dtype = dtype
         self.device = torch.device(device)
@@ -188,6 +195,7 @@ class MixedSolver(ContactBarrierMixin):
         self.A = None
         self.device_pcg = DevicePcg()
         self._dinv = None
+        self._dinv_group = None
         self.direct_solver = None
         self.stats = StepStats()
         self.frame = 0
@@ -348,8 +356,9 @@ class MixedSolver(ContactBarrierMixin):
         """Block-Jacobi PCG to the relative residual ``tol`` (device loop),
         the direct solve as fallback when it misses (time_integrator_base.py
         502-507)."""
-        M = JacobiPrecond(self.A, self._dinv)
-        self._dinv = M.dinv
+        groups = (self.n_fem, self.n_bodies) if self.preconditioner == "body_block" and self.n_bodies else None
+        M = JacobiPrecond(self.A, self._dinv, groups=groups, out_group=self._dinv_group)
+        self._dinv, self._dinv_group = M.dinv, M.dinv_group
         x, its, rel, status = self.device_pcg.solve(self.A, self.rhs, M, self.tol, self.maxiter)
         self.stats.pcg_iterations.append(its)
         dq = x

@@ -111,19 +111,38 @@ def pcg(A: BsrMatrix, b: torch.Tensor, precond, tol: float = 1e-6, maxiter: int 
 
 class JacobiPrecond:
     """Block-Jacobi preconditioner for DevicePcg (inverse diagonal blocks);
-    ``out`` reuses a buffer, so that a graph-replayed PCG keeps its pointers."""
+    ``out`` reuses a buffer, so that a graph-replayed PCG keeps its pointers.
+
+    ``groups=(n_point, n_groups)``: block rows n_point + 4 g .. + 3 form one
+    group (an affine body's p, a0, a1, a2) preconditioned by the inverse of
+    their 12x12 diagonal block (ipcb_group_jacobi); ``out_group`` reuses that
+    buffer."""
     kind = 0
 
-    def __init__(self, A: BsrMatrix, out: torch.Tensor | None = None):
+    def __init__(self, A: BsrMatrix, out: torch.Tensor | None = None, groups: tuple[int, int] | None = None,
+                 out_group: torch.Tensor | None = None):
         shape = (A.nrow, 3, 3)
         ok = out is not None and tuple(out.shape) == shape and out.dtype == A.dtype
         self.dinv = out if ok else torch.empty(shape, dtype=A.dtype, device=A.device)
         status = torch.zeros(1, dtype=torch.int32, device=A.device)
-        N.call("ipcb_block_jacobi", A.nrow, N.ptr(A.offsets), N.ptr(A.columns), None, N.ptr(A.values),
-               int(A.dtype == torch.float64), N.ptr(self.dinv), N.ptr(status), N.stream_handle())
+        fp64 = int(A.dtype == torch.float64)
+        N.call("ipcb_block_jacobi", A.nrow, N.ptr(A.offsets), N.ptr(A.columns), None, N.ptr(A.values), fp64,
+               N.ptr(self.dinv), N.ptr(status), N.stream_handle())
+        self.n_point, self.n_groups = groups if groups else (A.nrow, 0)
+        self.dinv_group = None
+        if self.n_groups:
+            if self.n_point + 4 * self.n_groups != A.nrow:
+                raise ValueError(f"groups {groups} do not cover {A.nrow} block rows")
+            gshape = (self.n_groups, 12, 12)
+            ok = out_group is not None and tuple(out_group.shape) == gshape and out_group.dtype == A.dtype
+            self.dinv_group = out_group if ok else torch.empty(gshape, dtype=A.dtype, device=A.device)
+            N.call("ipcb_group_jacobi", self.n_point, self.n_groups, N.ptr(A.offsets), N.ptr(A.columns),
+                   N.ptr(A.values), fp64, N.ptr(self.dinv_group), N.ptr(status), N.stream_handle())
 
     def fill(self, P):
         P.dinv = N.ptr(self.dinv)
+        P.n_point, P.n_groups = self.n_point, self.n_groups
+        P.dinv_group = N.ptr(self.dinv_group) if self.n_groups else None
 
 
 class DevicePcg:
