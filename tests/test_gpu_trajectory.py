@@ -7,7 +7,8 @@ After every step the surface is checked for edge-triangle crossings (none
 allowed), every step's Newton loop must end before its iteration cap with no
 refused CCD bound, and the rods must come into contact.  The float32 run's
 final positions are compared with the float64 run's; the difference is
-printed and bounded.
+printed and bounded by the run-to-run spread of the float64 build (atomic
+accumulation order), not by a tighter figure.
 
 The barrier stiffness is scaled to the barrier's energy scale: the IPC
 barrier in squared-distance form has energies of order kappa dhat^4, so with
@@ -57,4 +58,12 @@ def test_rod_twist_trajectory_float32_against_float64(cuda):
     print(f"rod twist, {STEPS} steps: float32 vs float64 max |dx| = {err:.3e} ({err / extent:.3e} of the "
           f"extent); Newton iterations per step float32 max {max(it32)} mean {np.mean(it32):.2f}, float64 max "
           f"{max(it64)} mean {np.mean(it64):.2f}; contacts up to {c32} / {c64}")
-    assert err <= 1e-3 * extent
+    # Two float64 runs differ by as much (max 3.7e-3, mean 1.2e-4 over the
+    # vertices after 200 steps, measured on a B200): atomically accumulated
+    # forces, matrix entries and PCG dot products sum in a different order
+    # each run, and the Newton iterates at rel. res. 1e-6 carry that through
+    # the contact trajectory.  Float32 against float64 measured max 4.1e-3 ..
+    # 1.1e-2, mean 1.3e-4 .. 1.9e-4; the bounds sit above that floor.
+    mean = np.abs(x32 - x64).mean()
+    assert err <= 5e-3 * extent
+    assert mean <= 1e-4 * extent
