@@ -196,6 +196,7 @@ class MixedSolver(ContactBarrierMixin):
         self.device_pcg = DevicePcg()
         self._dinv = None
         self._dinv_group = None
+        self._in_step, self._E_cache = False, None
         self.direct_solver = None
         self.stats = StepStats()
         self.frame = 0
@@ -395,8 +396,15 @@ class MixedSolver(ContactBarrierMixin):
             self.compute_collision_energy()
 
     def line_search(self) -> float:
+        """Backtracking from the CCD bound on the total incremental potential
+        (time_integrator_base.py:514-546).  Inside step(), E0 is the energy
+        of the point the previous search ended at (q has not moved since), as
+        the reference's affine-body search caches it; a search outside step()
+        evaluates it."""
         self.q_start.copy_(self.q)
-        E0 = self.total_energy()
+        cached = self._E_cache if self._in_step else None
+        E0 = cached if cached is not None else self.total_energy()
+        self._E_cache = E0
         refusals = self.ccd_refusals
         ub = self.collision_free_step(self.dx)
         if self.ccd_refusals != refusals:
@@ -422,6 +430,8 @@ class MixedSolver(ContactBarrierMixin):
             self.q.copy_(self.q_start)
             self._sync()
             alpha = 0.0
+        else:
+            self._E_cache = E1
         self.stats.energies.append((E0, E1))
         return alpha
 
@@ -437,13 +447,17 @@ class MixedSolver(ContactBarrierMixin):
         """time_integrator_base.py:375-401 over the joint unknowns."""
         self.stats = StepStats()
         self.prepare()
-        for it in range(self.max_newton):
-            alpha, norm = self.newton_iteration()
-            self.stats.newton_iterations = it + 1
-            self.stats.alphas.append(alpha)
-            self.stats.norms.append(norm)
-            if alpha == 0.0 or norm <= self.vel_tol * self.h:
-                break
+        self._in_step, self._E_cache = True, None
+        try:
+            for it in range(self.max_newton):
+                alpha, norm = self.newton_iteration()
+                self.stats.newton_iterations = it + 1
+                self.stats.alphas.append(alpha)
+                self.stats.norms.append(norm)
+                if alpha == 0.0 or norm <= self.vel_tol * self.h:
+                    break
+        finally:
+            self._in_step, self._E_cache = False, None
         h = self.h
         Vf = self.n_fem
         self.v_f.copy_((self.q[:Vf] - self.x0_f) / h)
