@@ -74,7 +74,8 @@ typedef struct {
   int n;          /* leaves currently built */
   int capacity;   /* leaves the memory was bound for */
   void* nodes;    /* float4[4*max(capacity-1,1)] */
-  int* parent;    /* int32[2*capacity]: internal j at j, leaf slot k at capacity+k; (parent<<1)|side */
+  int* parent;    /* int32[2*capacity]: internal j at j, leaf slot k at capacity+k; (parent<<1)|side, bit 31
+                   * set when the parent's leaf range lies in one 32-leaf block */
   int* sorted;    /* int32[capacity]: primitive of each leaf slot (Morton order) */
   unsigned* keys; /* uint32[capacity]: sorted Morton codes */
   unsigned* flags;/* uint32[capacity]: refit arrival counters (zero between calls) */

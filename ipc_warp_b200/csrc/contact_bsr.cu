@@ -6,8 +6,9 @@
 // (vertex ii of the record) and 4 consecutive blocks (columns = the record's 4
 // vertices).  A row's distinct columns are few (tens), so:
 //   1. thread per record: count the quads of each row and take each quad's
-//      arrival slot in its row (atomics); scan the counts; scatter the quad
-//      ids to their rows (arrival order)
+//      arrival slot in its row (atomics; a row's first arrival also appends
+//      the row to the list of touched rows); scan the counts; scatter the
+//      quad ids to their rows (arrival order)
 //   2. pass A, warp per row: sort the row's quad ids (so the order, and every
 //      sum below, is the same on every run), insert the columns of the
 //      non-zero blocks (the narrow phase's per-record block masks) into a
@@ -17,10 +18,15 @@
 //   4. pass B, warp per row: the row's blocks 32 at a time, grouped by column
 //      position within the warp and summed per group (shuffles), one
 //      shared-memory add per column and batch; a fixed order, so deterministic
+// Passes A and B run persistent warps that take the touched rows from a
+// counter: most vertices of a large scene have no contact, and a launch over
+// all rows would spend most of its blocks on empty ones.
 // A row with more than kHash distinct columns sets IPCB_STATUS_ROW_OVERFLOW
 // (the host then uses the generic assembly).
 #include "common.cuh"
 #include "scan.cuh"
+
+#include <algorithm>
 
 namespace ipcb {
 int check_launch(const char* where);
@@ -42,23 +48,39 @@ IPCB_D int comp(int4 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ?
 
 // nrec = {EE records, PT records}: host values, or min(*cnt, capacity) of
 // the lists read on the device (graph-capturable; no host read of the counts)
+// nrec[2]: touched rows; nrec[3], nrec[4]: the work counters of passes A, B
 __global__ void k_counts(const int* __restrict__ ee_cnt, int ee_n, const int* __restrict__ pt_cnt, int pt_n,
                          int* __restrict__ nrec) {
   nrec[0] = ee_cnt ? min(max(*ee_cnt, 0), ee_n) : ee_n;
   nrec[1] = pt_cnt ? min(max(*pt_cnt, 0), pt_n) : pt_n;
+  nrec[2] = nrec[3] = nrec[4] = 0;
 }
 
-__global__ void k_rec_slots(const int* __restrict__ nrec, const int* __restrict__ ee, const int* __restrict__ pt,
-                            int4* __restrict__ slots, int* __restrict__ row_cnt) {
+IPCB_D int arrive(int* __restrict__ row_cnt, int row, int* __restrict__ rows, int* __restrict__ nrows) {
+  const int s = atomicAdd(row_cnt + row, 1);
+  if (s == 0) rows[atomicAdd(nrows, 1)] = row;
+  return s;
+}
+
+__global__ void k_rec_slots(int* __restrict__ nrec, const int* __restrict__ ee, const int* __restrict__ pt,
+                            int4* __restrict__ slots, int* __restrict__ row_cnt, int* __restrict__ rows) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x, n_ee = nrec[0];
   if (p >= n_ee + nrec[1]) return;
   const int4 v = record_ids(ee, n_ee, pt, p);
   int4 s;
-  s.x = atomicAdd(row_cnt + v.x, 1);
-  s.y = atomicAdd(row_cnt + v.y, 1);
-  s.z = atomicAdd(row_cnt + v.z, 1);
-  s.w = atomicAdd(row_cnt + v.w, 1);
+  s.x = arrive(row_cnt, v.x, rows, nrec + 2);
+  s.y = arrive(row_cnt, v.y, rows, nrec + 2);
+  s.z = arrive(row_cnt, v.z, rows, nrec + 2);
+  s.w = arrive(row_cnt, v.w, rows, nrec + 2);
   slots[p] = s;
+}
+
+// the next touched row for this warp (one counter bump per row), -1 when done
+IPCB_D int next_row(int* __restrict__ work, const int* __restrict__ rows, int nrows, int lane) {
+  int r = 0;
+  if (lane == 0) r = atomicAdd(work, 1);
+  r = __shfl_sync(0xffffffffu, r, 0);
+  return r < nrows ? __ldg(rows + r) : -1;
 }
 
 __global__ void k_rec_scatter(const int* __restrict__ nrec, const int* __restrict__ ee, const int* __restrict__ pt,
@@ -173,23 +195,19 @@ IPCB_D unsigned quad_mask(const unsigned short* __restrict__ bmask, int q) {
 // sorted, and every quad gets its 4 column positions through a slot ->
 // position table.
 __global__ void __launch_bounds__(kWarps * 32, 12)
-    k_row_columns(int nrow, const int* __restrict__ qstart, int* __restrict__ qids, const int* __restrict__ ee,
-                  const int* __restrict__ nrec, const int* __restrict__ pt, const unsigned short* __restrict__ bmask,
-                  int* __restrict__ tmpcols, unsigned* __restrict__ qpos, int* __restrict__ row_nnz,
-                  int* __restrict__ status) {
+    k_row_columns(const int* __restrict__ rows, const int* __restrict__ qstart, int* __restrict__ qids,
+                  const int* __restrict__ ee, int* __restrict__ nrec, const int* __restrict__ pt,
+                  const unsigned short* __restrict__ bmask, int* __restrict__ tmpcols, unsigned* __restrict__ qpos,
+                  int* __restrict__ row_nnz, int* __restrict__ status) {
   __shared__ int sq[kWarps][kSmemQuads];
   __shared__ int tab[kWarps][kHash];
   __shared__ int scol[kWarps][kHash];
   __shared__ unsigned char slot_pos[kWarps][kHash];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int row = blockIdx.x * kWarps + w;
-  if (row >= nrow) return;
+  const int n_ee = nrec[0], nrows = nrec[2];
+  for (int row = next_row(nrec + 3, rows, nrows, lane); row >= 0; row = next_row(nrec + 3, rows, nrows, lane)) {
+  __syncwarp();  // the previous row's shared-memory reads are done
   const int b = qstart[row], n = qstart[row + 1] - b;
-  if (n == 0) {
-    if (lane == 0) row_nnz[row] = 0;
-    return;
-  }
-  const int n_ee = nrec[0];
   // the row's quads in quad-id order
   int nq2 = 32;
   while (nq2 < n) nq2 <<= 1;
@@ -281,6 +299,7 @@ __global__ void __launch_bounds__(kWarps * 32, 12)
     row_nnz[row] = cnt;
     if (bad) atomicOr(status, IPCB_STATUS_ROW_OVERFLOW);
   }
+  }
 }
 
 // pass B, warp per row: one 9-value accumulator per column in shared memory.
@@ -292,7 +311,8 @@ __global__ void __launch_bounds__(kWarps * 32, 12)
 // within a batch a fixed tree over the group's lanes), so the result is
 // deterministic, and each column takes one shared-memory add per batch.
 template <class S>
-__global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int* __restrict__ qstart,
+__global__ void __launch_bounds__(kWarps * 32) k_row_values(const int* __restrict__ rows, int* __restrict__ nrec,
+                                                            const int* __restrict__ qstart,
                                                             const int* __restrict__ qids,
                                                             const unsigned* __restrict__ qpos,
                                                             const S* __restrict__ vals,
@@ -306,12 +326,12 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int*
   constexpr int kVec = 36 * (int)sizeof(S) / 16;  // 16-byte vectors per quad
   const unsigned full = 0xffffffffu;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int row = blockIdx.x * kWarps + w;
-  if (row >= nrow) return;
+  const int nrows = nrec[2];
+  for (int row = next_row(nrec + 4, rows, nrows, lane); row >= 0; row = next_row(nrec + 4, rows, nrows, lane)) {
+  __syncwarp();  // the previous row's shared-memory reads are done
   int b = qstart[row], e = qstart[row + 1];
-  if (b == e) return;
   const int out = offsets[row], cnt = min(offsets[row + 1] - out, kHash);
-  if (cnt == 0) return;  // also a row pass A skipped (too many quads): its positions were not written
+  if (cnt == 0) continue;  // a row whose blocks are all zero
   for (int k = lane; k < cnt; k += 32) {
 #pragma unroll
     for (int t = 0; t < 9; ++t) sacc[w][9 * k + t] = S(0);
@@ -372,6 +392,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_values(int nrow, const int*
 #pragma unroll
     for (int t = 0; t < 9; ++t) values[9LL * (out + k) + t] = sacc[w][9 * k + t];
   }
+  }
 }
 
 __global__ void k_total(int nrow, int* __restrict__ offsets, const int* __restrict__ total, int* __restrict__ nnz) {
@@ -390,20 +411,26 @@ int assemble(int n_ee, int n_pt, const int* ee_cnt, const int* pt_cnt, int nv, c
   int* qids = (int*)p; p += al(NQ * 4);
   unsigned* qpos = (unsigned*)p; p += al(NQ * 4);
   int* qstart = (int*)p; p += al(R * 4);
+  int* rows = (int*)p; p += al(R * 4);
   int* tmpcols = (int*)p; p += al(NQ * 4 * 4);
   int* total = (int*)p; p += 256;
   int* nrec = (int*)p; p += 256;
   void* scratch = p;
   cudaMemsetAsync(qstart, 0, R * sizeof(int), st);
+  cudaMemsetAsync(offsets, 0, (size_t)nv * sizeof(int), st);  // rows without contact: no blocks
   k_counts<<<1, 1, 0, st>>>(ee_cnt, n_ee, pt_cnt, n_pt, nrec);
-  k_rec_slots<<<div_up(P, 256), 256, 0, st>>>(nrec, ee, pt, slots, qstart);
+  k_rec_slots<<<div_up(P, 256), 256, 0, st>>>(nrec, ee, pt, slots, qstart, rows);
   scan::exclusive<int>(qstart, (int)R, scratch, total, st);
   k_rec_scatter<<<div_up(P, 256), 256, 0, st>>>(nrec, ee, pt, slots, qstart, qids);
-  int g = div_up(nv, kWarps);
-  k_row_columns<<<g, kWarps * 32, 0, st>>>(nv, qstart, qids, ee, nrec, pt, bmask, tmpcols, qpos, offsets, status);
+  // persistent warps over the touched rows (at most min(nv, 4 P) of them)
+  const long long max_rows = std::min<long long>(nv, NQ);
+  const int ga = (int)std::min<long long>(148 * 12, div_up(max_rows, kWarps));
+  const int gb = (int)std::min<long long>(148 * 8, div_up(max_rows, kWarps));
+  k_row_columns<<<ga, kWarps * 32, 0, st>>>(rows, qstart, qids, ee, nrec, pt, bmask, tmpcols, qpos, offsets, status);
   scan::exclusive<int>(offsets, nv, scratch, total, st);
   k_total<<<1, 1, 0, st>>>(nv, offsets, total, nnz);
-  k_row_values<S><<<g, kWarps * 32, 0, st>>>(nv, qstart, qids, qpos, vals, tmpcols, offsets, columns, values);
+  k_row_values<S><<<gb, kWarps * 32, 0, st>>>(rows, nrec, qstart, qids, qpos, vals, tmpcols, offsets, columns,
+                                              values);
   return check_launch("ipcb_contact_bsr");
 }
 
@@ -416,7 +443,7 @@ extern "C" {
 
 size_t ipcb_contact_bsr_workspace(int n_records, int n_verts) {
   size_t NQ = 4 * (size_t)(n_records > 0 ? n_records : 1), R = (size_t)(n_verts > 0 ? n_verts : 0) + 1;
-  return al(NQ * 4) * 3 + al(R * 4) + al(NQ * 16) + 512 + scan::scratch_bytes((int)R);
+  return al(NQ * 4) * 3 + 2 * al(R * 4) + al(NQ * 16) + 512 + scan::scratch_bytes((int)R);
 }
 
 int ipcb_contact_bsr(const ipcb_contacts* ee, int n_ee, const ipcb_contacts* pt, int n_pt, int n_verts,

@@ -93,7 +93,12 @@ IPCB_D int delta(const unsigned* __restrict__ k, int n, int i, int j) {
   return __clz(a ^ b);
 }
 
-// One thread per internal node: range, split, child codes and parents.
+// Bit 31 of a parent entry: the parent's leaf range lies inside one 32-leaf
+// block, i.e. inside one warp of the refit.
+constexpr unsigned kLocalParent = 0x80000000u;
+
+// One thread per internal node: range, split, child codes and parents (with
+// the node's block-local bit).
 __global__ void k_karras(const unsigned* __restrict__ keys, const int* __restrict__ sorted, int n,
                          float4* __restrict__ nodes, int* __restrict__ parent, int cap) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -115,20 +120,22 @@ __global__ void k_karras(const unsigned* __restrict__ keys, const int* __restric
   }
   int g = i + s * d + min(d, 0);
   int first = min(i, j), last = max(i, j);
+  const unsigned loc = (first >> 5) == (last >> 5) ? kLocalParent : 0u;
+  const int up0 = (int)(((unsigned)i << 1) | loc), up1 = (int)(((unsigned)i << 1) | 1u | loc);
   int lcode, rcode;
   if (first == g) {
     lcode = ~sorted[g];
-    parent[cap + g] = (i << 1) | 0;
+    parent[cap + g] = up0;
   } else {
     lcode = g;
-    parent[g] = (i << 1) | 0;
+    parent[g] = up0;
   }
   if (last == g + 1) {
     rcode = ~sorted[g + 1];
-    parent[cap + g + 1] = (i << 1) | 1;
+    parent[cap + g + 1] = up1;
   } else {
     rcode = g + 1;
-    parent[g + 1] = (i << 1) | 1;
+    parent[g + 1] = up1;
   }
   nodes[4 * i + 0].w = __int_as_float(lcode);
   nodes[4 * i + 2].w = __int_as_float(rcode);
@@ -144,8 +151,16 @@ __global__ void k_karras(const unsigned* __restrict__ keys, const int* __restric
 // own slot and an empty entry when the child is a leaf, the child's two slots
 // when it is internal.  The thread that writes its subtree's slot into `node`
 // knows both (an internal subtree's two slots are the ones it merged one level
-// below), so it writes that half of wide[node] with the slot, before the
-// fence: no loads and no separate gather pass over the nodes.
+// below), so it writes that half of wide[node] with the slot: no loads and no
+// separate gather pass over the nodes.
+//
+// Two phases.  A node whose leaves lie in one 32-leaf block (kLocalParent in
+// the entries pointing to it) has both arrivals in the same warp (lane = leaf
+// rank mod 32), and its index -- one end of its range -- is in the block: the
+// warp meets there in rounds, each lane delivering its slot to shared memory,
+// one __syncwarp, and the side-0 lane of a node with both slots carrying it
+// up (no fence, no global atomic).  Above the blocks, the second of the two
+// arrivals found by a global atomic counter continues, after a fence.
 struct Slot {
   float4 lo, hi;
 };
@@ -163,21 +178,29 @@ IPCB_D void put_wide_half(float4* __restrict__ w, int side, const Slot& a, const
   h[14] = make_float2(a.hi.w, b.hi.w);
 }
 
-__global__ void __launch_bounds__(256) k_refit(const float* __restrict__ lo, const float* __restrict__ hi, int n,
-                                               const int* __restrict__ sorted, const int* __restrict__ parent,
-                                               int cap, float4* __restrict__ nodes, unsigned* __restrict__ flags,
-                                               float4* __restrict__ wide) {
+// 64-thread blocks: a warp whose lanes finish early frees its block slot
+// without waiting for warps still climbing (1.49M leaves: 211 us against 233
+// us with 8-warp blocks)
+constexpr int kRefitWarps = 2;
+
+__global__ void __launch_bounds__(32 * kRefitWarps) k_refit(const float* __restrict__ lo, const float* __restrict__ hi,
+                                                            int n, const int* __restrict__ sorted,
+                                                            const int* __restrict__ parent, int cap,
+                                                            float4* __restrict__ nodes, unsigned* __restrict__ flags,
+                                                            float4* __restrict__ wide) {
+  __shared__ Slot sslot[kRefitWarps][32][2];  // per warp: block-local node x side
+  __shared__ unsigned sarr[kRefitWarps][32];  // per warp: sides delivered to each block-local node
+  const unsigned full = 0xffffffffu;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  const int prim = sorted[k];
-  float3 bl = make_float3(lo[3 * prim], lo[3 * prim + 1], lo[3 * prim + 2]);
-  float3 bh = make_float3(hi[3 * prim], hi[3 * prim + 1], hi[3 * prim + 2]);
-  int code = ~prim;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const Slot none{make_float4(3.4e38f, 3.4e38f, 3.4e38f, __int_as_float(-1)),
                   make_float4(-3.4e38f, -3.4e38f, -3.4e38f, __int_as_float(-1))};
   if (n == 1) {
-    const Slot leaf{make_float4(bl.x, bl.y, bl.z, __int_as_float(code)), make_float4(bh.x, bh.y, bh.z, __int_as_float(0))};
-    const Slot second{make_float4(3.4e38f, 3.4e38f, 3.4e38f, __int_as_float(code)), none.hi};
+    if (k != 0) return;
+    const int prim = sorted[0];
+    const Slot leaf{make_float4(lo[3 * prim], lo[3 * prim + 1], lo[3 * prim + 2], __int_as_float(~prim)),
+                    make_float4(hi[3 * prim], hi[3 * prim + 1], hi[3 * prim + 2], __int_as_float(0))};
+    const Slot second{make_float4(3.4e38f, 3.4e38f, 3.4e38f, __int_as_float(~prim)), none.hi};
     nodes[0] = leaf.lo;
     nodes[1] = leaf.hi;
     nodes[2] = second.lo;
@@ -186,21 +209,85 @@ __global__ void __launch_bounds__(256) k_refit(const float* __restrict__ lo, con
     put_wide_half(wide, 1, second, none);  // a leaf code with an empty box: never hit
     return;
   }
-  int par = parent[cap + k];
-  int last = k;  // largest leaf rank below the subtree being carried up
+  sarr[w][lane] = 0u;
+  const int base = k & ~31;  // first leaf of this warp's block
+  bool carry = k < n;        // holds a subtree not yet delivered to its parent
+  float3 bl = make_float3(0.f, 0.f, 0.f), bh = bl;
+  int code = 0, par = 0, last = k;  // last: largest leaf rank below the carried subtree
+  if (carry) {
+    const int prim = sorted[k];
+    bl = make_float3(lo[3 * prim], lo[3 * prim + 1], lo[3 * prim + 2]);
+    bh = make_float3(hi[3 * prim], hi[3 * prim + 1], hi[3 * prim + 2]);
+    code = ~prim;
+    par = parent[cap + k];
+  }
   Slot c0 = none, c1 = none;  // the carried subtree's two slots (side order) when it is internal
-  // Depth is bounded by the 30 Morton bits plus 32 index bits of the
-  // tie-break; the loop bound only guards against a corrupted parent array.
+  __syncwarp();
+  // phase 1: the block-local nodes, in rounds over the whole warp (a block's
+  // subtree has depth < 32, so 32 rounds finish it; the bound also ends the
+  // loop on a corrupted parent array)
+  bool wait = false;  // delivered to a block-local node whose other side has not been seen
+  int wnode = 0, wside = 0, wpar = 0;  // wpar: the node's own parent entry, loaded on delivery
+  for (int round = 0; round < 40; ++round) {
+    int li = 32;
+    if (carry && ((unsigned)par & kLocalParent)) li = (int)((((unsigned)par & ~kLocalParent) >> 1)) - base;
+    const bool deliver = (unsigned)li < 32u;
+    if (!__any_sync(full, deliver || wait)) break;
+    if (deliver) {
+      const int node = base + li, side = par & 1;
+      if (side == 0 && node != 0) wpar = parent[node];  // needed if this lane carries the node on
+      const Slot own{make_float4(bl.x, bl.y, bl.z, __int_as_float(code)),
+                     make_float4(bh.x, bh.y, bh.z, __int_as_float(last))};
+      __stcg(nodes + 4 * node + 2 * side, own.lo);
+      __stcg(nodes + 4 * node + 2 * side + 1, own.hi);
+      if (code < 0) put_wide_half(wide + 8 * (size_t)node, side, own, none);
+      else put_wide_half(wide + 8 * (size_t)node, side, c0, c1);
+      sslot[w][li][side] = own;
+      atomicOr(&sarr[w][li], 1u << side);
+      carry = false;
+      wait = true;
+      wnode = node;
+      wside = side;
+    }
+    __syncwarp();
+    if (wait && sarr[w][wnode - base] == 3u) {
+      wait = false;
+      if (wside == 0) {  // both sides are in: the side-0 lane carries the node up
+        const Slot own{make_float4(bl.x, bl.y, bl.z, __int_as_float(code)),
+                       make_float4(bh.x, bh.y, bh.z, __int_as_float(last))};
+        const Slot sib = sslot[w][wnode - base][1];
+        c0 = own;
+        c1 = sib;
+        last = __float_as_int(sib.hi.w);
+        bl = make_float3(fminf(bl.x, sib.lo.x), fminf(bl.y, sib.lo.y), fminf(bl.z, sib.lo.z));
+        bh = make_float3(fmaxf(bh.x, sib.hi.x), fmaxf(bh.y, sib.hi.y), fmaxf(bh.z, sib.hi.z));
+        code = wnode;
+        if (wnode != 0) {
+          par = wpar;
+          carry = true;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  if (!carry) return;
+  // phase 2: the nodes above the blocks.  Depth is bounded by the 30 Morton
+  // bits plus 32 index bits of the tie-break; the loop bound only guards
+  // against a corrupted parent array.
+  // Per level only the slot the sibling reads is fenced; the parent entry is
+  // loaded and the wide half written outside the fence -> atomic -> sibling
+  // chain, which is the latency the climb to the root pays per level.
   for (int level = 0; level < 128; ++level) {
-    const int node = par >> 1, side = par & 1;
+    const int node = (int)(((unsigned)par & ~kLocalParent) >> 1), side = par & 1;
+    const int next = node != 0 ? parent[node] : 0;
     const Slot own{make_float4(bl.x, bl.y, bl.z, __int_as_float(code)),
                    make_float4(bh.x, bh.y, bh.z, __int_as_float(last))};
     __stcg(nodes + 4 * node + 2 * side, own.lo);
     __stcg(nodes + 4 * node + 2 * side + 1, own.hi);
-    if (code < 0) put_wide_half(wide + 8 * (size_t)node, side, own, none);
-    else put_wide_half(wide + 8 * (size_t)node, side, c0, c1);
     __threadfence();
     const unsigned old = atomicAdd(flags + node, 1u);
+    if (code < 0) put_wide_half(wide + 8 * (size_t)node, side, own, none);
+    else put_wide_half(wide + 8 * (size_t)node, side, c0, c1);
     if (old == 0) return;
     flags[node] = 0;
     const Slot sib{__ldcg(nodes + 4 * node + 2 * (1 - side)), __ldcg(nodes + 4 * node + 2 * (1 - side) + 1)};
@@ -211,7 +298,7 @@ __global__ void __launch_bounds__(256) k_refit(const float* __restrict__ lo, con
     bh = make_float3(fmaxf(bh.x, sib.hi.x), fmaxf(bh.y, sib.hi.y), fmaxf(bh.z, sib.hi.z));
     if (node == 0) return;
     code = node;
-    par = parent[node];
+    par = next;
   }
 }
 
@@ -307,7 +394,7 @@ int ipcb_lbvh_build(ipcb_lbvh* bvh, const float* lower, const float* upper, int 
   if (n > 1)
     k_karras<<<div_up(n - 1, 256), 256, 0, st>>>(bvh->keys, bvh->sorted, n, (float4*)bvh->nodes, bvh->parent,
                                                   bvh->capacity);
-  k_refit<<<div_up(n, 256), 256, 0, st>>>(lower, upper, n, bvh->sorted, bvh->parent, bvh->capacity,
+  k_refit<<<div_up(n, 32 * kRefitWarps), 32 * kRefitWarps, 0, st>>>(lower, upper, n, bvh->sorted, bvh->parent, bvh->capacity,
                                            (float4*)bvh->nodes, bvh->flags, (float4*)bvh->wide);
   return check_launch("ipcb_lbvh_build");
 }
@@ -316,7 +403,7 @@ int ipcb_lbvh_refit(const ipcb_lbvh* bvh, const float* lower, const float* upper
   if (!bvh || bvh->n < 0) return IPCB_E_ARG;
   if (bvh->n == 0) return IPCB_OK;
   if (!lower || !upper) return IPCB_E_ARG;
-  k_refit<<<div_up(bvh->n, 256), 256, 0, (cudaStream_t)s>>>(lower, upper, bvh->n, bvh->sorted, bvh->parent,
+  k_refit<<<div_up(bvh->n, 32 * kRefitWarps), 32 * kRefitWarps, 0, (cudaStream_t)s>>>(lower, upper, bvh->n, bvh->sorted, bvh->parent,
                                                             bvh->capacity, (float4*)bvh->nodes, bvh->flags,
                                                             (float4*)bvh->wide);
   return check_launch("ipcb_lbvh_refit");
