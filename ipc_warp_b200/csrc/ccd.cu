@@ -1095,15 +1095,15 @@ template <class S>
 void run_ee(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, const float* lower, const float* upper,
             int exclude, CandList c, void* toi, int* status, Sink sink, cudaStream_t st, int first, int count) {
   const int n = soup->n_edges;
-  const dim3 g(div_up(count, 128));
+  const dim3 g(div_up(count, 64));  // 64-thread blocks, as the discrete queries
   cudaMemsetAsync(c.count, 0, 2 * sizeof(int), st);
-  k_ee_collect<S, true><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->edges, soup->body,
+  k_ee_collect<S, true><<<g, 64, 0, st>>>((const S*)soup->x, (const S*)x1, soup->edges, soup->body,
                                            (const float4*)bvh->wide, bvh->sorted, n, first, count, lower, upper,
                                            exclude, c, (S*)toi, status, sink, nullptr);
   solve_candidates<S, 0>((const S*)soup->x, (const S*)x1, soup->edges, c.count, c, (S*)toi, status, sink, st);
   CandList none = c;
   none.capacity = 0;
-  k_ee_collect<S, false><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->edges, soup->body,
+  k_ee_collect<S, false><<<g, 64, 0, st>>>((const S*)soup->x, (const S*)x1, soup->edges, soup->body,
                                             (const float4*)bvh->wide, bvh->sorted, n, first, count, lower, upper,
                                             exclude, none, (S*)toi, status, sink, c.overflow);
 }
@@ -1111,15 +1111,15 @@ void run_ee(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, const f
 template <class S>
 void run_pt(const ipcb_soup* soup, const void* x1, const ipcb_lbvh* bvh, double pad, int exclude, CandList c,
             void* toi, int* status, Sink sink, cudaStream_t st, int first, int count) {
-  const dim3 g(div_up(count, 128));
+  const dim3 g(div_up(count, 64));
   cudaMemsetAsync(c.count, 0, 2 * sizeof(int), st);
-  k_pt_collect<S, true><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->triangles, soup->body,
+  k_pt_collect<S, true><<<g, 64, 0, st>>>((const S*)soup->x, (const S*)x1, soup->triangles, soup->body,
                                            (const float4*)bvh->wide, soup->n_tris, first, count, pad, exclude, c,
                                            (S*)toi, status, sink, nullptr);
   solve_candidates<S, 1>((const S*)soup->x, (const S*)x1, soup->triangles, c.count, c, (S*)toi, status, sink, st);
   CandList none = c;
   none.capacity = 0;
-  k_pt_collect<S, false><<<g, 128, 0, st>>>((const S*)soup->x, (const S*)x1, soup->triangles, soup->body,
+  k_pt_collect<S, false><<<g, 64, 0, st>>>((const S*)soup->x, (const S*)x1, soup->triangles, soup->body,
                                             (const float4*)bvh->wide, soup->n_tris, first, count, pad, exclude, none,
                                             (S*)toi, status, sink, c.overflow);
 }

@@ -388,13 +388,15 @@ int ipcb_dcd_ee_range(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* b
   int n = soup->n_edges;
   if (first < 0 || count < 0 || first > n || count > n - first) return IPCB_E_ARG;
   if (count == 0) return IPCB_OK;
-  dim3 grid(div_up(count, 128));
+  // 64-thread blocks: queries end at different depths, and a small block
+  // frees its slot sooner (measured a few percent faster than 128)
+  dim3 grid(div_up(count, 64));
   if (soup->fp64)
-    k_dcd_ee<double><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->edges, soup->body,
+    k_dcd_ee<double><<<grid, 64, 0, (cudaStream_t)s>>>((const float4*)x4, soup->edges, soup->body,
                                                         (const float4*)bvh->wide, bvh->sorted, n, first, count,
                                                         thickness, query_pad, exclude_same_body, *out, status);
   else
-    k_dcd_ee<float><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->edges, soup->body,
+    k_dcd_ee<float><<<grid, 64, 0, (cudaStream_t)s>>>((const float4*)x4, soup->edges, soup->body,
                                                        (const float4*)bvh->wide, bvh->sorted, n, first, count,
                                                        thickness, query_pad, exclude_same_body, *out, status);
   return check_launch("ipcb_dcd_ee");
@@ -413,13 +415,13 @@ int ipcb_dcd_pt_range(const ipcb_soup* soup, const float* x4, const ipcb_lbvh* b
   int nv = soup->n_verts;
   if (first < 0 || count < 0 || first > nv || count > nv - first) return IPCB_E_ARG;
   if (count == 0 || soup->n_tris == 0) return IPCB_OK;
-  dim3 grid(div_up(count, 128));
+  dim3 grid(div_up(count, 64));
   if (soup->fp64)
-    k_dcd_pt<double><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->triangles, soup->body,
+    k_dcd_pt<double><<<grid, 64, 0, (cudaStream_t)s>>>((const float4*)x4, soup->triangles, soup->body,
                                                         (const float4*)bvh->wide, soup->n_tris, query_order, first,
                                                         count, thickness, query_pad, exclude_same_body, *out, status);
   else
-    k_dcd_pt<float><<<grid, 128, 0, (cudaStream_t)s>>>((const float4*)x4, soup->triangles, soup->body,
+    k_dcd_pt<float><<<grid, 64, 0, (cudaStream_t)s>>>((const float4*)x4, soup->triangles, soup->body,
                                                        (const float4*)bvh->wide, soup->n_tris, query_order, first,
                                                        count, thickness, query_pad, exclude_same_body, *out, status);
   return check_launch("ipcb_dcd_pt");
