@@ -709,8 +709,11 @@ struct CandOrder {
 
 IPCB_D int bucket_of(float tl) { return min(kBuckets - 1, (int)(tl * (float)kBuckets)); }
 
+// 3 blocks per SM (at most 85 registers; 88 unbounded): the pass waits on
+// gathers of the pair's positions, and the extra warps hide them (screw and
+// nut edge-edge query 1.21 -> 1.14 ms)
 template <class S, int KIND>
-__global__ void __launch_bounds__(256) k_cand_bound(const S* __restrict__ x0, const S* __restrict__ x1,
+__global__ void __launch_bounds__(256, 3) k_cand_bound(const S* __restrict__ x0, const S* __restrict__ x1,
                                                     const int* __restrict__ prims, CandList cand, CandOrder o,
                                                     const int* skip_if) {
   __shared__ int sb[kBuckets];
