@@ -90,8 +90,11 @@ IPCB_D int warp_max(int v) {
 // warp's queries walk neighbouring subtrees.  Traversal only applies the cheap
 // filters and queues the surviving leaves; the exact closest-point test and
 // the append run afterwards with the warp converged.
+// 64-thread blocks, 14 per SM (at most 73 registers; 80 unbounded): more
+// warps in flight over the dependent node loads (screw and nut 0.568 ->
+// 0.539 ms; 64 registers spill and were slower)
 template <class S>
-__global__ void __launch_bounds__(128) k_dcd_ee(const float4* __restrict__ x4, const int* __restrict__ edges,
+__global__ void __launch_bounds__(64, 14) k_dcd_ee(const float4* __restrict__ x4, const int* __restrict__ edges,
                                                 const int* __restrict__ body, const float4* __restrict__ nodes,
                                                 const int* __restrict__ order, int n, int first, int count,
                                                 float thickness, float qpad, int exclude, ipcb_contacts out,
@@ -148,7 +151,7 @@ __global__ void __launch_bounds__(128) k_dcd_ee(const float4* __restrict__ x4, c
 }
 
 template <class S>
-__global__ void __launch_bounds__(128) k_dcd_pt(const float4* __restrict__ x4, const int* __restrict__ tris,
+__global__ void __launch_bounds__(64, 14) k_dcd_pt(const float4* __restrict__ x4, const int* __restrict__ tris,
                                                 const int* __restrict__ body, const float4* __restrict__ nodes,
                                                 int n_tris, const int* __restrict__ order, int first, int count,
                                                 float thickness, float qpad, int exclude, ipcb_contacts out,
