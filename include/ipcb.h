@@ -745,6 +745,9 @@ typedef struct {
    * n_groups] from ipcb_group_jacobi; n = n_point + 4 n_groups. */
   int n_point, n_groups;
   const void* dinv_group;
+  /* initial guess scalar[3n], or NULL for x = 0: ipcb_pcg_start copies it to
+   * x and starts from r = b - A x0 (the stopping test stays relative to |b|) */
+  const void* x0;
 } ipcb_pcg;
 
 int ipcb_pcg_start(const ipcb_pcg* P, double tol, int maxiter, ipcb_stream s);

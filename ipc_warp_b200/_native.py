@@ -89,7 +89,7 @@ class Pcg(ctypes.Structure):
     _fields_ = [("n", c_int), ("fp64", c_int), ("precond", c_int), ("offsets", P), ("columns", P), ("values", P),
                 ("dinv", P), ("g_offsets", P), ("g_columns", P), ("diag", P), ("g", P), ("scale", P), ("b", P),
                 ("x", P), ("r", P), ("z", P), ("p", P), ("q", P), ("t", P), ("state", P), ("n_point", c_int),
-                ("n_groups", c_int), ("dinv_group", P)]
+                ("n_groups", c_int), ("dinv_group", P), ("x0", P)]
 
 
 SP, CP, BP = ctypes.POINTER(Soup), ctypes.POINTER(Contacts), ctypes.POINTER(Lbvh)

@@ -494,6 +494,21 @@ __global__ void __launch_bounds__(kBlock) k_start(int m, const T* __restrict__ b
   if (threadIdx.x == 0) atomicAdd(&st->bb, part);
 }
 
+// the start from a guess: x = x0 was copied and q = A x0 computed; r = b - q
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_start_guess(int m, const T* __restrict__ b, const T* __restrict__ q,
+                                                        T* __restrict__ r, ipcb_pcg_state* st) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double part = 0.0;
+  if (i < m) {
+    const T bi = b[i];
+    r[i] = bi - q[i];
+    part = (double)bi * bi;
+  }
+  part = block_sum(part);
+  if (threadIdx.x == 0) atomicAdd(&st->bb, part);
+}
+
 __global__ void k_state_init(ipcb_pcg_state* st, double tol, int maxiter) {
   st->rz = st->rz_new = st->pAp = st->rr = st->bb = st->last_rr = 0.0;
   st->tol2 = tol * tol;
@@ -591,7 +606,15 @@ template <class T>
 int start(const ipcb_pcg* P, double tol, int maxiter, cudaStream_t s) {
   const int m = 3 * P->n;
   k_state_init<<<1, 1, 0, s>>>(P->state, tol, maxiter);
-  k_start<T><<<gridn(m), kBlock, 0, s>>>(m, (const T*)P->b, (T*)P->x, (T*)P->r, P->state);
+  if (P->x0) {
+    // the product's p.q lands in pAp, which the setup's finish_state clears
+    cudaMemcpyAsync(P->x, P->x0, (size_t)m * sizeof(T), cudaMemcpyDeviceToDevice, s);
+    k_spmv_dot<T><<<warp_grid(P->n), kBlock, 0, s>>>(P->n, P->offsets, P->columns, (const T*)P->values,
+                                                        (const T*)P->x, (T*)P->q, P->state);
+    k_start_guess<T><<<gridn(m), kBlock, 0, s>>>(m, (const T*)P->b, (const T*)P->q, (T*)P->r, P->state);
+  } else {
+    k_start<T><<<gridn(m), kBlock, 0, s>>>(m, (const T*)P->b, (T*)P->x, (T*)P->r, P->state);
+  }
   precond<T>(P, s);
   k_update_p_finish<T><<<flat_grid(m), kBlock, 0, s>>>(m, (const T*)P->z, (T*)P->p, P->state, 1);
   return 0;

@@ -160,14 +160,15 @@ class DevicePcg:
     def _buffers(self, n, dtype, device):
         if self._bufs is None or self._bufs["n"] != n or self._bufs["dtype"] != dtype:
             z = lambda: torch.zeros((n, 3), dtype=dtype, device=device)
-            self._bufs = dict(n=n, dtype=dtype, x=z(), r=z(), z=z(), p=z(), q=z(), t=z(), b=z(),
+            self._bufs = dict(n=n, dtype=dtype, x=z(), r=z(), z=z(), p=z(), q=z(), t=z(), b=z(), x0=z(),
                               state=torch.zeros(ctypes.sizeof(N.PcgState), dtype=torch.uint8, device=device),
                               host=torch.zeros(ctypes.sizeof(N.PcgState), dtype=torch.uint8).pin_memory())
         return self._bufs
 
-    def solve(self, A: BsrMatrix, b: torch.Tensor, M, tol: float, maxiter: int):
+    def solve(self, A: BsrMatrix, b: torch.Tensor, M, tol: float, maxiter: int, x0: torch.Tensor | None = None):
         """Returns (x, iterations, relative residual, status); x is a view of
-        an internal buffer (valid until the next solve)."""
+        an internal buffer (valid until the next solve).  x0: initial guess
+        (None: zero); the stopping test stays relative to |b|."""
         n = A.nrow
         B = self._buffers(n, A.dtype, A.device)
         B["b"].copy_(b)
@@ -178,9 +179,12 @@ class DevicePcg:
             setattr(P, k, N.ptr(B[k]))
         P.state = N.ptr(B["state"])
         M.fill(P)
+        if x0 is not None:
+            B["x0"].copy_(x0.reshape(n, 3))
+            P.x0 = N.ptr(B["x0"])
         self._P = P
         N.call("ipcb_pcg_start", ctypes.byref(P), float(tol), int(maxiter), N.stream_handle())
-        key = tuple(getattr(P, f) for f, _ in N.Pcg._fields_)
+        key = tuple(getattr(P, f) for f, _ in N.Pcg._fields_ if f != "x0")  # the loop never reads x0
         if self.use_graph and key != self._key:
             self._graph = torch.cuda.CUDAGraph()
             with N.no_collection(), torch.cuda.graph(self._graph):
@@ -197,6 +201,8 @@ class DevicePcg:
             st = N.PcgState.from_buffer_copy(B["host"].numpy().tobytes())
             if st.done:
                 break
+        if x0 is not None and not st.bb > 0:
+            B["x"].zero_()  # b = 0: the solution is 0, whatever the guess
         rel = math.sqrt(st.last_rr / st.bb) if st.bb > 0 else 0.0
         return B["x"], st.it, rel, st.status
 

@@ -236,3 +236,75 @@ def test_body_block_groups_must_cover_rows(cuda):
     s.compute_A()
     with pytest.raises(ValueError):
         JacobiPrecond(s.A, groups=(s.n_fem + 1, s.n_bodies))
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_group_jacobi_random_and_singular_blocks(cuda, fp64):
+    """ipcb_group_jacobi on a small block matrix: 2 point rows and 3 groups of
+    4 block rows; groups 0 and 2 get random SPD 12x12 blocks (their inverse
+    is returned), group 1 an all-zero block (singular: the identity is
+    returned and IPCB_STATUS_PATTERN is raised)."""
+    from ipc_warp_b200 import _native as N
+    from ipc_warp_b200.bsr import bsr_from_triplets
+
+    dtype = torch.float64 if fp64 else torch.float32
+    n_point, n_groups = 2, 3
+    nrow = n_point + 4 * n_groups
+    rng = np.random.default_rng(7)
+    dense = np.zeros((3 * nrow, 3 * nrow))
+    for i in range(n_point):
+        dense[3 * i:3 * i + 3, 3 * i:3 * i + 3] = np.eye(3) * (2.0 + i)
+    for g in (0, 2):
+        m = rng.normal(size=(12, 12))
+        o = 3 * n_point + 12 * g
+        dense[o:o + 12, o:o + 12] = m @ m.T + 12 * np.eye(12)
+    rows, cols, vals = [], [], []
+    for bi in range(nrow):
+        for bj in range(nrow):
+            blk = dense[3 * bi:3 * bi + 3, 3 * bj:3 * bj + 3]
+            if np.any(blk) or bi == bj:
+                rows.append(bi)
+                cols.append(bj)
+                vals.append(blk)
+    A = bsr_from_triplets(nrow, nrow, torch.tensor(rows, dtype=torch.int32, device=cuda),
+                          torch.tensor(cols, dtype=torch.int32, device=cuda),
+                          torch.tensor(np.array(vals), dtype=dtype, device=cuda))
+    out = torch.empty((n_groups, 12, 12), dtype=dtype, device=cuda)
+    status = torch.zeros(1, dtype=torch.int32, device=cuda)
+    N.call("ipcb_group_jacobi", n_point, n_groups, N.ptr(A.offsets), N.ptr(A.columns), N.ptr(A.values), int(fp64),
+           N.ptr(out), N.ptr(status), N.stream_handle())
+    got = out.double().cpu().numpy()
+    assert int(status.item()) & 16
+    assert np.array_equal(got[1], np.eye(12))
+    for g in (0, 2):
+        o = 3 * n_point + 12 * g
+        ref = np.linalg.inv(dense[o:o + 12, o:o + 12])
+        assert np.abs(got[g] - ref).max() <= (1e-12 if fp64 else 1e-6) * np.abs(ref).max()
+    # bad arguments are refused before any launch
+    with pytest.raises(N.NativeError):
+        N.call("ipcb_group_jacobi", -1, n_groups, N.ptr(A.offsets), N.ptr(A.columns), N.ptr(A.values), int(fp64),
+               N.ptr(out), N.ptr(status), N.stream_handle())
+
+
+def test_pcg_initial_guess(cuda):
+    """DevicePcg from an initial guess (ipcb_pcg.x0): the same solution to the
+    tolerance, fewer iterations from a close guess, and zero for b = 0."""
+    import scipy.sparse.linalg as sla
+
+    from ipc_warp_b200.newton import DevicePcg, JacobiPrecond
+
+    s = _solver(torch.float64)
+    _perturb(s, 5)
+    A = s.compute_A()
+    ref = sla.spsolve(A.to_scipy().tocsc(), _host(s.rhs).ravel())
+    M = JacobiPrecond(A, groups=(s.n_fem, s.n_bodies))
+    pcg = DevicePcg()
+    x, it0, rel, status = pcg.solve(A, s.rhs, M, 1e-8, 4000)
+    assert status == 0 and rel <= 1e-8
+    guess = torch.tensor(0.9 * ref.reshape(-1, 3), dtype=torch.float64, device=cuda)
+    x, it1, rel, status = pcg.solve(A, s.rhs, M, 1e-8, 4000, x0=guess)
+    assert status == 0 and rel <= 1e-8
+    assert np.abs(_host(x).ravel() - ref).max() <= 1e-5 * np.abs(ref).max()
+    assert it1 < it0, (it1, it0)
+    x, _, _, status = pcg.solve(A, torch.zeros_like(s.rhs), M, 1e-8, 4000, x0=guess)
+    assert status == 0 and not bool(x.any())
