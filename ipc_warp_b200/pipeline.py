@@ -66,10 +66,15 @@ class ContactPipeline(ContactBarrierMixin):
             self._side = torch.cuda.Stream(device=dev)
             self._ccd_e = torch.cuda.Stream(device=dev)
             self._ccd_t = torch.cuda.Stream(device=dev)
+            self._copy_in = torch.cuda.Stream(device=dev)
+            self._copy_out = torch.cuda.Stream(device=dev)
+            self._x1_done = torch.cuda.Event()
             self._ee_done = torch.cuda.Event()
             self._pt_done = torch.cuda.Event()
             self._toi_ws_pt = torch.empty_like(self._toi_ws)
         self._dx_buf = torch.zeros_like(soup.x_transformed)
+        self._host_io = None  # (x, dx, b) pinned host tensors during iteration_host
+        self._last_stepwise = False
         self._readback = {"counts": torch.zeros(4, dtype=torch.int32, pin_memory=pin),
                           "energy": torch.zeros(1, dtype=torch.float64, pin_memory=pin),
                           "toi": torch.zeros(1, dtype=soup.x_transformed.dtype, pin_memory=pin)}
@@ -105,8 +110,10 @@ class ContactPipeline(ContactBarrierMixin):
         h = self._readback
         ee, pt = self.contacts_new, self.contacts_pt
         n_ee, n_pt, st, qst = (int(v) for v in h["counts"])
+        self._last_stepwise = False
         if n_ee > ee.capacity or n_pt > pt.capacity or st & 4:
             self._graph = None
+            self._last_stepwise = True
             return self.iteration_stepwise()
         if self.use_graph and (self._graph is None or self._graph[0] != key):
             self._capture(self._graph_key())  # the eager pass may have (re)allocated buffers
@@ -118,9 +125,32 @@ class ContactPipeline(ContactBarrierMixin):
         ee, pt, t, H = self.contacts_new, self.contacts_pt, self.collision_triplets, self.collision_hessian
         ws = tuple(None if getattr(self, a, None) is None else getattr(self, a).data_ptr()
                    for a in ("_ws_ee", "_ws_pt"))
+        io = None if self._host_io is None else tuple(a.data_ptr() for a in self._host_io)
         return (ee.a1a2b1b2.data_ptr(), ee.capacity, pt.a1a2b1b2.data_ptr(), pt.capacity,
                 None if t is None else t.rows.data_ptr(), None if H is None else H.values.data_ptr(),
-                None if H is None else H._ws.data_ptr(), ws, getattr(self, "bvh_rebuild_interval", 0))
+                None if H is None else H._ws.data_ptr(), ws, io, getattr(self, "bvh_rebuild_interval", 0))
+
+    def iteration_host(self, x: torch.Tensor, dx: torch.Tensor, b: torch.Tensor) -> IterationResult:
+        """iteration() from host memory: positions x and direction dx (V, 3)
+        copied in, the contact force b copied out (pinned tensors of the
+        soup's dtype).  On a GPU the copies are part of the enqueued (and
+        graph-replayed) sequence: x first, dx on its own stream beside the
+        discrete queries (only the CCD reads it), and b as soon as the narrow
+        phase has written it, beside the BSR, energy and CCD stages."""
+        if self.device.type != "cuda":
+            self.soup.x_transformed.copy_(x)
+            res = self.iteration(dx.to(self.device))
+            b.copy_(self.b)
+            return res
+        self._host_io = (x, dx, b)
+        self.states.dx = self._dx_buf  # filled by the copy in the sequence
+        try:
+            res = self.iteration()
+        finally:
+            self._host_io = None
+        if self._last_stepwise:  # redone stage by stage: copy its force out
+            b.copy_(self.b)
+        return res
 
     def _capture(self, key):
         if key[-1]:  # periodic rebuilds alternate with refits: not one fixed sequence
@@ -155,12 +185,23 @@ class ContactPipeline(ContactBarrierMixin):
             t = self.collision_triplets = Triplets.zeros(16 * cap, self.soup.xcs.dtype, self.device)
         self._ws_ee = hessian_workspace(ee, getattr(self, "_ws_ee", None))
         self._ws_pt = hessian_workspace(pt, getattr(self, "_ws_pt", None))
+        io = self._host_io
+        if io is not None:
+            self.soup.x_transformed.copy_(io[0], non_blocking=True)
         self.compute_V(ret=False)
         self._pack()
         self.b.zero_()
-        N.call("ipcb_add_dx", soup, N.ptr(self._dx_buf), N.ptr(self.ccd_x1), N.stream_handle())
         self.ccd_toi.fill_(1.0)
         self._status.zero_()
+        if io is None:
+            N.call("ipcb_add_dx", soup, N.ptr(self._dx_buf), N.ptr(self.ccd_x1), N.stream_handle())
+        else:  # the direction crosses the bus beside the discrete queries
+            cin = self._copy_in
+            cin.wait_stream(main)
+            with torch.cuda.stream(cin):
+                self._dx_buf.copy_(io[1], non_blocking=True)
+                N.call("ipcb_add_dx", soup, N.ptr(self._dx_buf), N.ptr(self.ccd_x1), N.stream_handle())
+                self._x1_done.record(cin)
         side.wait_stream(main)
         with torch.cuda.stream(side):
             self._triangle_aabbs()
@@ -174,6 +215,8 @@ class ContactPipeline(ContactBarrierMixin):
         self._ee_done.record(main)
         with torch.cuda.stream(ccd_e):
             ccd_e.wait_event(self._ee_done)
+            if io is not None:
+                ccd_e.wait_event(self._x1_done)
             s1 = N.stream_handle()
             N.call("ipcb_swept_edge_aabbs", soup, N.ptr(self.ccd_x1), pad, N.ptr(self.ccd_edge_lower),
                    N.ptr(self.ccd_edge_upper), s1)
@@ -183,6 +226,8 @@ class ContactPipeline(ContactBarrierMixin):
                    N.ptr(self._status), N.ptr(self._toi_ws), self._toi_ws.numel(), s1)
         with torch.cuda.stream(ccd_t):
             ccd_t.wait_event(self._pt_done)
+            if io is not None:
+                ccd_t.wait_event(self._x1_done)
             s2 = N.stream_handle()
             N.call("ipcb_swept_triangle_aabbs", soup, N.ptr(self.ccd_x1), pad, N.ptr(self.ccd_triangle_lower),
                    N.ptr(self.ccd_triangle_upper), s2)
@@ -195,6 +240,11 @@ class ContactPipeline(ContactBarrierMixin):
             side.wait_event(self._ee_done)  # the PT records follow the EE count
             contact_hessian_pt_after(self.states, self.soup, pt, t, self.b, ee, kappa, ws=self._ws_pt)
         main.wait_stream(side)
+        if io is not None:  # the force is final: send it back beside the remaining stages
+            cout = self._copy_out
+            cout.wait_stream(main)
+            with torch.cuda.stream(cout):
+                io[2].copy_(self.b, non_blocking=True)
         H, _ = contact_bsr(ee, None, pt, None, self.soup.n_verts, t, out=self.collision_hessian,
                            status=self._bsr_status, read_status=False)
         self.collision_hessian = H
@@ -203,6 +253,9 @@ class ContactPipeline(ContactBarrierMixin):
         contact_energy_pt(self.states, self.soup, pt, e, kappa, n=-1)
         main.wait_stream(ccd_e)
         main.wait_stream(ccd_t)
+        if io is not None:
+            main.wait_stream(self._copy_in)
+            main.wait_stream(self._copy_out)
         self._copy_results(e)
 
     def _copy_results(self, e):
@@ -218,6 +271,10 @@ class ContactPipeline(ContactBarrierMixin):
     def _enqueue_serial(self):
         """_enqueue on one stream (periodic BVH rebuilds, or no triangles)."""
         ee, pt = self.contacts_new, self.contacts_pt
+        io = self._host_io
+        if io is not None:
+            self.soup.x_transformed.copy_(io[0], non_blocking=True)
+            self._dx_buf.copy_(io[1], non_blocking=True)
         self.compute_V(ret=False)
         self._status.zero_()
         self.update_bvh()
@@ -243,6 +300,8 @@ class ContactPipeline(ContactBarrierMixin):
         contact_energy_ee(self.states, self.soup, ee, e, kappa, n=-1)
         contact_energy_pt(self.states, self.soup, pt, e, kappa, n=-1)
         self._launch_ccd(self._dx_buf, reset_status=False)
+        if io is not None:
+            io[2].copy_(self.b, non_blocking=True)
         self._copy_results(e)
 
     def iteration_stepwise(self) -> IterationResult:

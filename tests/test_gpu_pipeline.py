@@ -73,3 +73,32 @@ def test_graph_replay_equals_stepwise(cuda):
         assert torch.equal(o, o2) and torch.equal(c, c2)
         assert ((v - v2).abs() <= 1e-5 * v2.abs().amax(dim=(1, 2), keepdim=True).clamp_min(1e-30)).all()
     assert pipe._graph is not None  # the later calls replayed it, each against its own direction
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_iteration_from_host_buffers(cuda, dtype):
+    """iteration_host (x and dx copied in, the force copied out inside the
+    enqueued and then graph-replayed sequence) gives iteration()'s result
+    from device tensors: first call eager, second and third replayed, the
+    third with other host contents in the same buffers."""
+    sc = small_scenes()[1]
+    pipe, dx = _pipe(sc, dtype, cuda)
+    ref_pipe, _ = _pipe(sc, dtype, cuda)
+    xh = torch.tensor(sc.x, dtype=dtype).pin_memory()
+    dxh = dx.cpu().pin_memory()
+    bh = torch.empty_like(xh).pin_memory()
+    tol = 1e-12 if dtype == torch.float64 else 1e-5
+    rng = np.random.default_rng(4)
+    for call in range(3):
+        if call == 2:  # new contents in the same pinned buffers: the replay must read them
+            xh.copy_(torch.tensor(sc.x + rng.normal(scale=0.05 * sc.dhat, size=sc.x.shape), dtype=dtype))
+            dxh.mul_(0.5)
+        r = pipe.iteration_host(xh, dxh, bh)
+        ref_pipe.soup.x_transformed.copy_(xh.to(cuda))
+        q = ref_pipe.iteration(dxh.to(cuda))
+        assert (r.n_ee, r.n_pt) == (q.n_ee, q.n_pt) and r.n_ee + r.n_pt > 0
+        assert r.alpha == q.alpha
+        assert r.energy == pytest.approx(q.energy, rel=1e-12 if dtype == torch.float64 else 1e-6)
+        b_ref = ref_pipe.b.double().cpu()
+        assert (bh.double() - b_ref).abs().max() <= tol * max(b_ref.abs().max().item(), 1e-300)
+    assert pipe._graph is not None  # the later calls replayed the captured sequence
