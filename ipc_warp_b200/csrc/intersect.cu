@@ -1,7 +1,7 @@
 // Intersection check of a surface state: every surface edge that crosses a
 // surface triangle (not sharing a vertex with it) is an intersection.  The
-// IPC invariant is that an accepted step never produces one; the north-star
-// test runs this after every step of a trajectory.
+// IPC invariant is that an accepted step never produces one; the trajectory
+// tests run this after every step.
 //
 // One thread per edge queries the triangle hierarchy (refit to the current
 // positions) with the edge's box padded by a relative 1e-6 (covers the

@@ -177,7 +177,7 @@ def test_narrow_phase_matches_reference_float32_build():
     float32 build on the narrow_fp64.npz scene rounded to float32
     (narrow_fp32.npz): the oracle's float mode (float32 gate and features,
     geometry and barrier in double) within 1e-5 per record, in the force
-    and in the energies -- the float32 tolerance of the north star."""
+    and in the energies -- the float32 parity tolerance of this library."""
     d = load("narrow_fp32.npz")
     d64 = load("narrow_fp64.npz")
     x, xcs, l0, kappa = d["x"], d["xcs"], d["l0"], float(d64["kappa"])
