@@ -542,6 +542,11 @@ int ipcb_ls_trial(const ipcb_ls_state* st, int fp64, int n_verts, const void* x_
 int ipcb_ls_accept(ipcb_ls_state* st, const double* acc, double h2, const ipcb_contacts* ee, const ipcb_contacts* pt,
                    unsigned long long cond_handle, ipcb_stream s);
 int ipcb_ls_finish(const ipcb_ls_state* st, int fp64, int n_verts, const void* x_tmp, void* x, ipcb_stream s);
+/* *acc += extra[0] + ... + extra[n-1], then extra[0 .. n) = 0 (one thread, in
+ * this order): folds energy terms accumulated apart (affine-body inertia and
+ * orthogonality, pins, FEM inertia) into the inertia slot of a line-search
+ * accumulator without a host read. */
+int ipcb_acc_fold(double* acc, double* extra, int n, ipcb_stream s);
 /* A CUDA graph with one WHILE conditional node: _begin creates it and starts
  * capturing stream s (not the legacy default stream) into the loop body
  * (*handle: the condition, 1 at the start of every launch); launches on s

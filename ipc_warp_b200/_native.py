@@ -165,6 +165,7 @@ SIGNATURES = {
     "ipcb_ls_trial": (c_int, [P, c_int, c_int, P, P, P, P, P]),
     "ipcb_ls_accept": (c_int, [P, P, c_double, CP, CP, ctypes.c_ulonglong, P]),
     "ipcb_ls_finish": (c_int, [P, c_int, c_int, P, P, P]),
+    "ipcb_acc_fold": (c_int, [P, P, c_int, P]),
     "ipcb_graph_while_begin": (c_int, [ctypes.POINTER(c_void_p), ctypes.POINTER(ctypes.c_ulonglong), P]),
     "ipcb_graph_while_end": (c_int, [c_void_p, P]),
     "ipcb_graph_launch": (c_int, [c_void_p, P]),

@@ -117,6 +117,15 @@ __global__ void k_ls_finish(const ipcb_ls_state* __restrict__ st, int n3, const 
   if (i < n3 && !st->accepted) x[i] = x_tmp[i];
 }
 
+__global__ void k_acc_fold(double* acc, double* extra, int n) {
+  double v = *acc;
+  for (int i = 0; i < n; ++i) {
+    v += extra[i];
+    extra[i] = 0.0;
+  }
+  *acc = v;
+}
+
 struct WhileGraph {
   cudaGraph_t graph = nullptr;
   cudaGraph_t body = nullptr;
@@ -184,6 +193,12 @@ int ipcb_ls_finish(const ipcb_ls_state* st, int fp64, int n_verts, const void* x
   if (fp64) k_ls_finish<double><<<div_up(n3, 256), 256, 0, str>>>(st, n3, (const double*)x_tmp, (double*)x);
   else k_ls_finish<float><<<div_up(n3, 256), 256, 0, str>>>(st, n3, (const float*)x_tmp, (float*)x);
   return check_launch("ipcb_ls_finish");
+}
+
+int ipcb_acc_fold(double* acc, double* extra, int n, ipcb_stream s) {
+  if (!acc || n < 0 || (n && !extra)) return IPCB_E_ARG;
+  k_acc_fold<<<1, 1, 0, (cudaStream_t)s>>>(acc, extra, n);
+  return check_launch("ipcb_acc_fold");
 }
 
 int ipcb_graph_while_begin(void** ctx, unsigned long long* handle, ipcb_stream s) {

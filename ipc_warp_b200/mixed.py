@@ -49,7 +49,7 @@ class MixedSolver(ContactBarrierMixin):
                  gravity=(0.0, -9.8, 0.0), h: float = 1e-2, dtype=torch.float32, device="cuda",
                  vel_tol: float = 5e-2, max_newton: int = 100, tol: float = 1e-4, maxiter: int = 500,
                  exclude_same_body: bool = True, direct_fallback: bool = True, assembly: str = "queue",
-                 preconditioner: str = "body_block"):
+                 preconditioner: str = "body_block", line_search_mode: str = "device"):
         if assembly not in ("queue", "separate"):
             raise ValueError(f"unknown assembly {assembly!r}")
         if preconditioner not in ("body_block", "jacobi"):
@@ -59,6 +59,11 @@ class MixedSolver(ContactBarrierMixin):
         # block for each affine body's (p, a0, a1, a2); "jacobi": 3x3 blocks
         # throughout
         self.preconditioner = preconditioner
+        if line_search_mode not in ("device", "host"):
+            raise ValueError(f"unknown line search mode {line_search_mode!r}")
+        self.line_search_mode = line_search_mode
+        self._ls = None
+        self._acc_cached = False
         self.h = float(h)
         self.dtype = dtype
         self.device = torch.device(device)
@@ -397,10 +402,159 @@ class MixedSolver(ContactBarrierMixin):
 
     def line_search(self) -> float:
         """Backtracking from the CCD bound on the total incremental potential
-        (time_integrator_base.py:514-546).  Inside step(), E0 is the energy
-        of the point the previous search ended at (q has not moved since), as
-        the reference's affine-body search caches it; a search outside step()
-        evaluates it."""
+        (time_integrator_base.py:514-546): on the device ("device", the
+        trials in one WHILE-graph launch, one host read) or on the host."""
+        if self.line_search_mode == "device":
+            return self._line_search_device()
+        return self._line_search_host()
+
+    # ---- device search: the FEM solver's ipcb_ls_* state machine over q
+    def _ls_buffers(self):
+        if self._ls is None:
+            dev = self.device
+            z = lambda n: torch.zeros(n, dtype=torch.float64, device=dev)  # noqa: E731
+            self._ls = dict(acc=z(3), acc0=z(3), extra=z(4),
+                            state=torch.zeros(ctypes.sizeof(N.LsState), dtype=torch.uint8, device=dev),
+                            host=torch.zeros(ctypes.sizeof(N.LsState), dtype=torch.uint8).pin_memory(),
+                            gravity=(ctypes.c_double * 3)(*self.gravity),
+                            stream=torch.cuda.Stream(device=dev), graph=None, key=None)
+        return self._ls
+
+    def _energy_launches(self, acc: torch.Tensor, detect: bool = True):
+        """Launches (no host read) adding the energy at the current q into
+        acc: [0] tet Psi, [1] barrier (both times h^2 in E), [2] FEM and body
+        inertia, h^2 orthogonality and pins -- the terms of total_energy.  The
+        contact lists are refilled by the DCD, their counts kept on the
+        device."""
+        s = N.stream_handle()
+        h2 = self.h * self.h
+        kappa = float(self.contact_stiffness)
+        if detect:
+            self.update_bvh()
+            self._launch_dcd("ee")
+            if self.has_triangles:
+                self._launch_dcd("pt")
+        soup = self.soup.c_struct()
+        base = acc.data_ptr()
+        N.call("ipcb_contact_energy", 0, ctypes.byref(soup), ctypes.byref(self.contacts_new.c_struct()), -1, kappa,
+               base + 8, s)
+        if self.has_triangles:
+            N.call("ipcb_contact_energy", 1, ctypes.byref(soup), ctypes.byref(self.contacts_pt.c_struct()), -1,
+                   kappa, base + 8, s)
+        if self.n_tets:
+            N.call("ipcb_tet_energy", self.material, self.fp64, N.ptr(self.x), N.ptr(self.tets), self.n_tets,
+                   N.ptr(self.Bm), N.ptr(self.W), self.mu, self.lam, base, s)
+        ls = self._ls
+        eb = ls["extra"].data_ptr()
+        if self.n_bodies:
+            N.call("ipcb_abd_body_energy", ctypes.byref(self._c_abd), h2, eb, s)
+            N.call("ipcb_mixed_pins", ctypes.byref(self._c_mixed), N.ptr(self.q), N.ptr(self.pin_rest),
+                   N.ptr(self.pin_target), N.ptr(self.pin_k), h2, None, None, None, None, eb + 16, s)
+        if self.n_fem:  # 1/2 m |q - x~|^2 with x~ = x0 + h v + h^2 g formed in double, as prepare() does
+            N.call("ipcb_ls_inertia", self.fp64, self.n_fem, N.ptr(self.q), N.ptr(self.x0_f), N.ptr(self.v_f),
+                   ls["gravity"], self.h, N.ptr(self.fem_mass), None, None, 0.0, eb + 24, s)
+        N.call("ipcb_acc_fold", base + 16, eb, 4, s)
+
+    def _ls_key(self):
+        ee, pt = self.contacts_new, self.contacts_pt
+        return (self.q.data_ptr(), self.q_start.data_ptr(), self.dq.data_ptr(), self.x.data_ptr(),
+                ee.a1a2b1b2.data_ptr(), ee.capacity, pt.a1a2b1b2.data_ptr(), pt.capacity)
+
+    def _ls_graph(self):
+        """The WHILE graph of one trial (q = q_start - alpha dq, x = J q, the
+        energy, the accept test), captured once per buffer set on a side
+        stream."""
+        ls = self._ls
+        key = self._ls_key()
+        if ls["graph"] is not None and ls["key"] == key:
+            return ls["graph"]
+        if ls["graph"] is not None:
+            N.lib().ipcb_graph_destroy(ls["graph"])
+            ls["graph"] = None
+        h2 = self.h * self.h
+        side = ls["stream"]
+        side.wait_stream(torch.cuda.current_stream())
+        ctx, handle = ctypes.c_void_p(), ctypes.c_ulonglong()
+        with N.no_collection(), torch.cuda.stream(side):
+            s = N.stream_handle()
+            N.call("ipcb_graph_while_begin", ctypes.byref(ctx), ctypes.byref(handle), s)
+            body_ok = False
+            try:
+                N.call("ipcb_ls_trial", N.ptr(ls["state"]), self.fp64, self.nq, N.ptr(self.q_start), N.ptr(self.dq),
+                       N.ptr(self.q), N.ptr(ls["acc"]), s)
+                self._sync()
+                self._energy_launches(ls["acc"])
+                # the accept kernel ends the body: it sets the loop condition
+                N.call("ipcb_ls_accept", N.ptr(ls["state"]), N.ptr(ls["acc"]), h2,
+                       ctypes.byref(self.contacts_new.c_struct()), ctypes.byref(self.contacts_pt.c_struct()),
+                       handle.value, s)
+                body_ok = True
+            finally:
+                end_rc = N.lib().ipcb_graph_while_end(ctx, s)
+                if not body_ok or end_rc != 0:
+                    N.lib().ipcb_graph_destroy(ctx)
+            if end_rc != 0:
+                raise N.NativeError("ipcb_graph_while_end failed: " + (N.lib().ipcb_last_error() or b"").decode())
+        torch.cuda.current_stream().wait_stream(side)
+        ls["graph"], ls["key"] = ctx, key
+        return ctx
+
+    def _line_search_device(self) -> float:
+        """E0 (inside step(): the terms of the point the previous search
+        ended at) and the CCD bound are launched, the WHILE graph runs the
+        trials, and the state is read once.  A contact list that overflows
+        during the search grows and the search reruns on the host."""
+        ls = self._ls_buffers()
+        h2 = self.h * self.h
+        s = N.stream_handle()
+        self.q_start.copy_(self.q)
+        if self._in_step and self._acc_cached:
+            ls["acc0"].copy_(ls["acc"])
+        else:
+            ls["acc0"].zero_()
+            self._energy_launches(ls["acc0"])
+        self._launch_ccd(self.dx)
+        eps = 1.1920928955078125e-7 if self.dtype == torch.float32 else 2.220446049250313e-16
+        N.call("ipcb_ls_begin", N.ptr(ls["state"]), N.ptr(self.ccd_toi), self.fp64, N.ptr(self._status),
+               N.ptr(ls["acc0"]), h2, eps, 64, ctypes.byref(self.contacts_new.c_struct()),
+               ctypes.byref(self.contacts_pt.c_struct()), s)
+        N.call("ipcb_graph_launch", self._ls_graph(), s)
+        N.call("ipcb_ls_finish", N.ptr(ls["state"]), self.fp64, self.nq, N.ptr(self.q_start), N.ptr(self.q), s)
+        self._sync()
+        ls["host"].copy_(ls["state"], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        st = N.LsState.from_buffer_copy(ls["host"].numpy().tobytes())
+        if st.overflow:
+            if st.max_ee > self.contacts_new.capacity:
+                self._grow_contact_list(self.contacts_new, st.max_ee)
+            if st.max_pt > self.contacts_pt.capacity:
+                self._grow_contact_list(self.contacts_pt, st.max_pt, point_triangle=True)
+            self.q.copy_(self.q_start)
+            self._sync()
+            self._acc_cached = False
+            return self._line_search_host()
+        self.query_status = st.refused
+        if st.refused:  # a CCD query ran out of its bounds: its TOI is no bound, no step
+            self.ccd_refusals += 1
+            self.stats.ccd_refusals += 1
+        if not st.accepted:  # q is back at q_start: its terms are E0's
+            ls["acc"].copy_(ls["acc0"])
+        self._acc_cached = True
+        self.stats.energies.append((st.E0, st.E1))
+        return st.alpha_accepted if st.accepted else 0.0
+
+    def __del__(self):
+        ls = getattr(self, "_ls", None)
+        if ls and ls.get("graph") is not None:
+            try:
+                N.lib().ipcb_graph_destroy(ls["graph"])
+            except Exception:
+                pass
+
+    def _line_search_host(self) -> float:
+        """Inside step(), E0 is the energy of the point the previous search
+        ended at (q has not moved since), as the reference's affine-body
+        search caches it; a search outside step() evaluates it."""
         self.q_start.copy_(self.q)
         cached = self._E_cache if self._in_step else None
         E0 = cached if cached is not None else self.total_energy()
@@ -447,7 +601,7 @@ class MixedSolver(ContactBarrierMixin):
         """time_integrator_base.py:375-401 over the joint unknowns."""
         self.stats = StepStats()
         self.prepare()
-        self._in_step, self._E_cache = True, None
+        self._in_step, self._E_cache, self._acc_cached = True, None, False
         try:
             for it in range(self.max_newton):
                 alpha, norm = self.newton_iteration()
@@ -457,7 +611,7 @@ class MixedSolver(ContactBarrierMixin):
                 if alpha == 0.0 or norm <= self.vel_tol * self.h:
                     break
         finally:
-            self._in_step, self._E_cache = False, None
+            self._in_step, self._E_cache, self._acc_cached = False, None, False
         h = self.h
         Vf = self.n_fem
         self.v_f.copy_((self.q[:Vf] - self.x0_f) / h)

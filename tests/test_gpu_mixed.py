@@ -308,3 +308,43 @@ def test_pcg_initial_guess(cuda):
     assert it1 < it0, (it1, it0)
     x, _, _, status = pcg.solve(A, torch.zeros_like(s.rhs), M, 1e-8, 4000, x0=guess)
     assert status == 0 and not bool(x.any())
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_device_line_search_matches_host(cuda, dtype):
+    """The mixed solver's line search on the device (trials in one WHILE-graph
+    launch) against the host loop from the same state and direction: the
+    same step and energies (to rounding), and the same q after it."""
+    out = []
+    for mode in ("host", "device"):
+        s = _solver(dtype)
+        s.line_search_mode = mode
+        _perturb(s, 8)
+        s.prepare()
+        s.compute_A()
+        s.solve()
+        alpha = s.line_search()
+        E0, E1 = s.stats.energies[-1]
+        out.append((alpha, E0, E1, _host(s.q)))
+    (ah, e0h, e1h, qh), (ad, e0d, e1d, qd) = out
+    tol = 1e-9 if dtype == torch.float64 else 1e-4
+    assert 0.0 < ah <= 1.0 and ad == pytest.approx(ah, rel=1e-12)
+    assert e0d == pytest.approx(e0h, rel=tol) and e1d == pytest.approx(e1h, rel=tol)
+    assert e1d < e0d
+    assert np.abs(qd - qh).max() <= (1e-12 if dtype == torch.float64 else 1e-5) * max(np.abs(qh).max(), 1.0)
+
+
+def test_device_line_search_steps_rest(cuda):
+    """A few steps of the touching scene with the device search: converged,
+    intersection-free, the ground does not move (as with the host search)."""
+    s = _solver(torch.float64, affine_stiffness=1e8)
+    assert s.line_search_mode == "device"
+    q0 = _host(s.q)
+    ground = s.n_fem + 4 * 2
+    for k in range(5):
+        st = s.step()
+        assert st.newton_iterations < s.max_newton, k
+        assert st.ccd_refusals == 0
+        assert s.edge_triangle_crossings()[0] == 0, k
+    q = _host(s.q)
+    assert np.abs(q[ground:ground + 4] - q0[ground:ground + 4]).max() == 0.0
