@@ -189,6 +189,18 @@ class MixedSolver(ContactBarrierMixin):
         self._tet = Triplets.zeros(16 * self.n_tets, dtype, dev)
         self._body = Triplets.zeros(16 * nb, dtype, dev)
         self._pin = Triplets.zeros(16 * nb, dtype, dev)
+        # the blocks of the fixed pattern in one array (tets | bodies | pins),
+        # so one gather map covers them all
+        nt16 = 16 * self.n_tets
+        self._fixed_vals = torch.zeros((nt16 + 32 * nb, 3, 3), dtype=dtype, device=dev)
+        self._tet.vals = self._fixed_vals[:nt16]
+        self._body.vals = self._fixed_vals[nt16:nt16 + 16 * nb]
+        self._pin.vals = self._fixed_vals[nt16 + 16 * nb:]
+        # assemble A as the union of the fixed pattern (FEM mass, tets, body
+        # blocks, pins; its slot map built once) and the reduced contact
+        # blocks, instead of sorting every triplet each iteration
+        self.fixed_pattern = True
+        self._static = None
         self._red = None
         self._red_ws = None
         self._red_n = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -328,6 +340,8 @@ class MixedSolver(ContactBarrierMixin):
                    N.ptr(g), None, s)
         N.call("ipcb_mixed_reduce_force", ctypes.byref(self._c_mixed), N.ptr(self.b), -h2, N.ptr(g), s)
         red = self._reduced_contact(n_rec, h2)
+        if self.fixed_pattern:
+            return self._assemble_union(red, h2)
         idx = torch.arange(Vf, dtype=torch.int32, device=self.device)
         eye = torch.eye(3, dtype=self.dtype, device=self.device)
         rows, cols, vals = [idx], [idx], [self.fem_mass.to(self.dtype)[:, None, None] * eye]
@@ -346,6 +360,72 @@ class MixedSolver(ContactBarrierMixin):
             vals.append(red.vals)
         self.A = bsr_from_triplets(self.nq, self.nq, torch.cat(rows), torch.cat(cols), torch.cat(vals), out=self.A)
         return self.A
+
+    def _static_pattern(self):
+        """Pattern of FEM mass + tets + body blocks + pins (their rows and
+        columns are the same every iteration) with the map from each slot to
+        the blocks of _fixed_vals that land on it, built once."""
+        dev = self.device
+        Vf, nb, nt16 = self.n_fem, self.n_bodies, 16 * self.n_tets
+        rows_g = torch.cat([self._tet.rows, self._body.rows, self._pin.rows])
+        cols_g = torch.cat([self._tet.cols, self._body.cols, self._pin.cols])
+        idx = torch.arange(self.nq, dtype=torch.int32, device=dev)
+        rows = torch.cat([idx, rows_g])
+        cols = torch.cat([idx, cols_g])
+        ones = torch.ones((rows.numel(), 3, 3), dtype=self.dtype, device=dev)
+        S = bsr_from_triplets(self.nq, self.nq, rows, cols, ones)
+        nnz = int(S.nnz_dev.item())
+        n_g = rows_g.numel()
+        slots = torch.empty(max(n_g, 1), dtype=torch.int32, device=dev)
+        N.call("ipcb_bsr_slots", self.nq, N.ptr(S.offsets), N.ptr(S.columns), n_g, N.ptr(rows_g), N.ptr(cols_g),
+               N.ptr(slots), N.stream_handle())
+        sl = slots[:n_g].long()
+        g_idx = torch.argsort(sl, stable=True).to(torch.int32)
+        g_off = torch.zeros(nnz + 1, dtype=torch.int32, device=dev)
+        g_off[1:] = torch.cumsum(torch.bincount(sl, minlength=nnz), 0).to(torch.int32)
+        diag = torch.zeros(self.nq, dtype=self.dtype, device=dev)
+        diag[:Vf] = self.fem_mass.to(self.dtype)
+        self._static = dict(S=S, nnz=nnz, g_off=g_off, g_idx=g_idx, diag=diag, n_fixed=nt16,
+                            status=torch.zeros(1, dtype=torch.int32, device=dev),
+                            ws=torch.empty(N.size("ipcb_bsr_union_workspace", self.nq), dtype=torch.uint8,
+                                           device=dev))
+
+    def _assemble_union(self, red, h2: float) -> BsrMatrix:
+        """A = union of the fixed pattern (values gathered in a fixed order:
+        h^2 times the tet blocks, the body and pin blocks, the FEM mass on
+        the diagonal) and the BSR of the reduced contact triplets."""
+        if self._static is None:
+            self._static_pattern()
+        st = self._static
+        s = N.stream_handle()
+        # ipcb_newton_values scales every gathered block by h^2: the body and
+        # pin blocks (unscaled terms) enter divided by it
+        self._fixed_vals[st["n_fixed"]:].mul_(1.0 / h2)
+        if red is None:
+            red = Triplets.zeros(1, self.dtype, self.device)  # one zero block at (0, 0)
+            n = 1
+        else:
+            n = red.rows.shape[0]
+        C = bsr_from_triplets(self.nq, self.nq, red.rows, red.cols, red.vals, count=n,
+                              out=getattr(self, "_C", None))
+        self._C = C
+        S = st["S"]
+        cap = st["nnz"] + max(int(C.nnz_dev.item()), 1)
+        A = self.A
+        if A is None or A.columns.shape[0] < cap or "a_rows" not in st or st["a_rows"].shape[0] < cap:
+            cap = cap + cap // 4
+            A = BsrMatrix(self.nq, self.nq, cap, self.dtype, self.device)
+            for k in ("a_rows", "src_a", "src_b"):
+                st[k] = torch.empty(cap, dtype=torch.int32, device=self.device)
+        cap = min(A.columns.shape[0], st["a_rows"].shape[0])
+        N.call("ipcb_bsr_union", self.nq, N.ptr(S.offsets), N.ptr(S.columns), N.ptr(C.offsets), N.ptr(C.columns),
+               N.ptr(A.offsets), N.ptr(st["a_rows"]), N.ptr(A.columns), N.ptr(st["src_a"]), N.ptr(st["src_b"]), cap,
+               N.ptr(A.nnz_dev), N.ptr(st["status"]), N.ptr(st["ws"]), st["ws"].numel(), s)
+        N.call("ipcb_newton_values", self.fp64, N.ptr(A.nnz_dev), cap, N.ptr(st["a_rows"]), N.ptr(A.columns),
+               N.ptr(st["src_a"]), N.ptr(st["src_b"]), N.ptr(st["g_off"]), N.ptr(st["g_idx"]),
+               N.ptr(self._fixed_vals), h2, N.ptr(st["diag"]), N.ptr(C.values), 1.0, N.ptr(A.values), s)
+        self.A = A
+        return A
 
     def compute_rhs(self) -> torch.Tensor:
         return self.rhs

@@ -348,3 +348,29 @@ def test_device_line_search_steps_rest(cuda):
         assert s.edge_triangle_crossings()[0] == 0, k
     q = _host(s.q)
     assert np.abs(q[ground:ground + 4] - q0[ground:ground + 4]).max() == 0.0
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_fixed_pattern_assembly_equals_sorted_assembly(cuda, dtype):
+    """A as the union of the fixed pattern (gathered FEM mass, tet, body and
+    pin blocks) and the reduced contact BSR equals the sort-based assembly
+    of all triplets, over two Newton iterations (the second reuses the slot
+    map)."""
+    mats = []
+    for fixed in (True, False):
+        s = _solver(dtype)
+        s.fixed_pattern = fixed
+        _perturb(s, 9)
+        s.prepare()
+        out = []
+        for it in range(2):
+            A = s.compute_A()
+            assert s.n_contacts + s.n_contacts_pt > 0
+            out.append(A.to_scipy().toarray())
+            if it == 0:
+                s.solve()
+                s.line_search()
+        mats.append(out)
+    tol = 1e-12 if dtype == torch.float64 else 1e-5
+    for a, b in zip(*mats):
+        assert np.abs(a - b).max() <= tol * np.abs(b).max()
