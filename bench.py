@@ -378,6 +378,28 @@ def wrecking_balls_steps(dev, torch, before: int = 55, timed: int = 3):
             "orthogonality_error": s.orthogonality_error()}
 
 
+def run_profile_mixed():
+    """One Newton iteration of the wrecking balls at an impact state (after
+    55 steps), between cudaProfilerStart/Stop (ncu --profile-from-start off)."""
+    import torch
+
+    from ipc_warp_b200 import scenes
+    from ipc_warp_b200.mixed import MixedSolver
+
+    dev = torch.device("cuda", 0)
+    s = MixedSolver(scenes.wrecking_balls(n_balls=64), E=5e5, nu=0.4, h=1e-2, dtype=torch.float32, device=dev,
+                    maxiter=2000)
+    for _ in range(55):
+        s.step()
+    s.prepare()
+    s.newton_iteration()  # buffers and graphs at this state
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    s.newton_iteration()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+
+
 def run_profile_solver(args):
     """Untimed launches of the Newton solve's kernels on the wound rod bundle
     (for ncu): two learned-factor builds (MPNN forward, row normalisation,
@@ -741,10 +763,16 @@ def main():
                     help="split the headline workload over the N ranks (strong scaling) instead of N replicas")
     ap.add_argument("--profile-newton", action="store_true",
                     help="untimed Newton iterations (learned PCG, device line search), for ncu; prints nothing")
+    ap.add_argument("--profile-mixed", action="store_true",
+                    help="wrecking balls: 55 untimed steps, then one Newton iteration between "
+                         "cudaProfilerStart/Stop, for ncu; prints nothing")
     args = ap.parse_args()
     global ROD_SIDE, TURNS
     ROD_SIDE = args.rods
     TURNS = args.turns
+    if args.profile_mixed:
+        run_profile_mixed()
+        return
     if args.profile_solver:
         run_profile_solver(args)
         return
