@@ -64,6 +64,7 @@ class MixedSolver(ContactBarrierMixin):
         self.line_search_mode = line_search_mode
         self._ls = None
         self._acc_cached = False
+        self._lists_at_q = False
         self.h = float(h)
         self.dtype = dtype
         self.device = torch.device(device)
@@ -227,6 +228,7 @@ class MixedSolver(ContactBarrierMixin):
     # ------------------------------------------------------------- maps
     def _sync(self):
         """x = J q for every soup vertex."""
+        self._lists_at_q = False  # q may have moved: the contact lists are not known to be current
         N.call("ipcb_mixed_map", ctypes.byref(self._c_mixed), N.ptr(self.q), N.ptr(self.x), N.stream_handle())
 
     def _vertex_direction(self):
@@ -316,8 +318,14 @@ class MixedSolver(ContactBarrierMixin):
         Vf, nb = self.n_fem, self.n_bodies
         s = N.stream_handle()
         self.b.zero_()
-        with self.profile_timer("detect collision"):
-            self.detect_collision()
+        if self._lists_at_q:
+            # the search that produced q evaluated its energy here: its
+            # detection (hierarchies refit, lists filled at q) is this one
+            self.n_contacts, self.n_contacts_pt = (
+                int(v) for v in torch.cat([self.contacts_new.cnt, self.contacts_pt.cnt]).tolist())
+        else:
+            with self.profile_timer("detect collision"):
+                self.detect_collision()
         n_ee, n_pt = self.n_contacts, self.n_contacts_pt
         n_rec = n_ee + n_pt
         if getattr(self, "collision_triplets", None) is None or self.collision_triplets.rows.shape[0] < 16 * n_rec:
@@ -620,6 +628,8 @@ class MixedSolver(ContactBarrierMixin):
         if not st.accepted:  # q is back at q_start: its terms are E0's
             ls["acc"].copy_(ls["acc0"])
         self._acc_cached = True
+        # the accepted trial, the last one run, detected the contacts at q
+        self._lists_at_q = bool(st.accepted)
         self.stats.energies.append((st.E0, st.E1))
         return st.alpha_accepted if st.accepted else 0.0
 
@@ -666,6 +676,7 @@ class MixedSolver(ContactBarrierMixin):
             alpha = 0.0
         else:
             self._E_cache = E1
+            self._lists_at_q = True  # total_energy at the accepted q detected its contacts
         self.stats.energies.append((E0, E1))
         return alpha
 
