@@ -94,15 +94,15 @@ __device__ __forceinline__ void ld9(const bf16* __restrict__ v, float (&a)[9]) {
   for (int q = 0; q < 9; ++q) a[q] = __bfloat162float(v[q]);
 }
 
-template <class T, class V>
+template <class T, class V, int L = kLanes>
 __device__ __forceinline__ void row_mv(const int* __restrict__ cols, const V* __restrict__ vals, int b, int e,
                                        const T* __restrict__ x, const float* __restrict__ xs, int transpose_at,
                                        T& o0, T& o1, T& o2) {
-  const int sub = threadIdx.x & (kLanes - 1);
+  const int sub = threadIdx.x & (L - 1);
   using A = typename std::conditional<std::is_same<V, double>::value, double, float>::type;
   T a0 = 0, a1 = 0, a2 = 0;
 #pragma unroll 2
-  for (int k = b + sub; k < e; k += kLanes) {
+  for (int k = b + sub; k < e; k += L) {
     const int c = __ldg(cols + k);
     A m[9];
     ld9(vals + 9LL * k, m);
@@ -123,7 +123,7 @@ __device__ __forceinline__ void row_mv(const int* __restrict__ cols, const V* __
     }
   }
 #pragma unroll
-  for (int o = kLanes / 2; o > 0; o >>= 1) {
+  for (int o = L / 2; o > 0; o >>= 1) {
     a0 += __shfl_xor_sync(0xffffffffu, a0, o);
     a1 += __shfl_xor_sync(0xffffffffu, a1, o);
     a2 += __shfl_xor_sync(0xffffffffu, a2, o);
@@ -382,6 +382,11 @@ __global__ void __launch_bounds__(kBlock) k_jacobi(int n, const T* __restrict__ 
   if (threadIdx.x == 0) atomicAdd(&st->rz_new, part);
 }
 
+// lanes per row of the factor sweeps: each reads half a row of the pattern
+// (measured on the wound rod bundle: 61.7 us an iteration with 4, 63.3 with
+// 8, 70.0 with 2)
+constexpr int kFsaiLanes = 4;
+
 // t = G_lower (S r)
 template <class T>
 __global__ void __launch_bounds__(kBlock) k_fsai_lower(int n, const int* __restrict__ off, const int* __restrict__ diag,
@@ -389,14 +394,14 @@ __global__ void __launch_bounds__(kBlock) k_fsai_lower(int n, const int* __restr
                                                        const float* __restrict__ scale, const T* __restrict__ r,
                                                        T* __restrict__ t, ipcb_pcg_state* st) {
   if (st->done) return;
-  const int sub = threadIdx.x & (kLanes - 1);
-  const int groups = (gridDim.x * blockDim.x) / kLanes;
+  const int sub = threadIdx.x & (kFsaiLanes - 1);
+  const int groups = (gridDim.x * blockDim.x) / kFsaiLanes;
   const int trips = (n + groups - 1) / groups;
-  int row = (blockIdx.x * blockDim.x + threadIdx.x) / kLanes;
+  int row = (blockIdx.x * blockDim.x + threadIdx.x) / kFsaiLanes;
   for (int it = 0; it < trips; ++it, row += groups) {
     const bool ok = row < n;
     T o0, o1, o2;
-    row_mv<T, bf16>(cols, g, ok ? off[row] : 0, ok ? diag[row] + 1 : 0, r, scale, -1, o0, o1, o2);
+    row_mv<T, bf16, kFsaiLanes>(cols, g, ok ? off[row] : 0, ok ? diag[row] + 1 : 0, r, scale, -1, o0, o1, o2);
     if (ok && sub == 0) {
       t[3 * row] = o0;
       t[3 * row + 1] = o1;
@@ -414,16 +419,16 @@ __global__ void __launch_bounds__(kBlock) k_fsai_upper(int n, const int* __restr
                                                        const T* __restrict__ r, T* __restrict__ z,
                                                        ipcb_pcg_state* st) {
   if (st->done) return;
-  const int sub = threadIdx.x & (kLanes - 1);
-  const int groups = (gridDim.x * blockDim.x) / kLanes;
+  const int sub = threadIdx.x & (kFsaiLanes - 1);
+  const int groups = (gridDim.x * blockDim.x) / kFsaiLanes;
   const int trips = (n + groups - 1) / groups;
   double part = 0.0;
-  int row = (blockIdx.x * blockDim.x + threadIdx.x) / kLanes;
+  int row = (blockIdx.x * blockDim.x + threadIdx.x) / kFsaiLanes;
   for (int it = 0; it < trips; ++it, row += groups) {
     const bool ok = row < n;
     T o0, o1, o2;
     const int d = ok ? diag[row] : 0;
-    row_mv<T, bf16>(cols, g, d, ok ? off[row + 1] : 0, t, nullptr, d, o0, o1, o2);
+    row_mv<T, bf16, kFsaiLanes>(cols, g, d, ok ? off[row + 1] : 0, t, nullptr, d, o0, o1, o2);
     if (ok && sub == 0) {
       const T z0 = o0 * (T)scale[3 * row], z1 = o1 * (T)scale[3 * row + 1], z2 = o2 * (T)scale[3 * row + 2];
       z[3 * row] = z0;
