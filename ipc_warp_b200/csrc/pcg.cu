@@ -310,55 +310,86 @@ __global__ void __launch_bounds__(kBlock) k_jacobi_groups(int n_point, int n_gro
   if (threadIdx.x == 0) atomicAdd(&st->rz_new, part);
 }
 
-// one thread per group: gather the 16 3x3 blocks of rows / columns
-// n_point + 4 g .. + 3 from the BSR, invert the 12x12 in double (Gauss-Jordan,
-// partial pivoting)
+// one warp per group: gather the 16 3x3 blocks of rows / columns
+// n_point + 4 g .. + 3 from the BSR into the warp's shared [12 | I] matrix,
+// then Gauss-Jordan in double with partial pivoting (the first largest pivot,
+// as a sequential scan picks), one row swap, scaling and elimination step per
+// column with the lanes over the entries
+constexpr int kInvWarps = 4;
+
 template <class T>
-__global__ void k_group_inverse(int n_point, int n_groups, const int* __restrict__ off, const int* __restrict__ cols,
-                                const T* __restrict__ vals, T* __restrict__ out, int* __restrict__ status) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= n_groups) return;
-  double a[12][24];
-  for (int i = 0; i < 12; ++i)
-    for (int j = 0; j < 24; ++j) a[i][j] = (j == 12 + i) ? 1.0 : 0.0;
+__global__ void __launch_bounds__(32 * kInvWarps) k_group_inverse(int n_point, int n_groups,
+                                                                 const int* __restrict__ off,
+                                                                 const int* __restrict__ cols,
+                                                                 const T* __restrict__ vals, T* __restrict__ out,
+                                                                 int* __restrict__ status) {
+  __shared__ double sa[kInvWarps][12][24];
+  const unsigned full = 0xffffffffu;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = blockIdx.x * kInvWarps + w;
+  if (g >= n_groups) return;  // the whole warp
+  double(&a)[12][24] = sa[w];
+  for (int e = lane; e < 12 * 24; e += 32) {
+    const int i = e / 24, j = e - 24 * i;
+    a[i][j] = (j == 12 + i) ? 1.0 : 0.0;
+  }
+  __syncwarp(full);
   const int r0 = n_point + 4 * g;
   for (int bi = 0; bi < 4; ++bi) {
     const int row = r0 + bi;
-    for (int k = off[row]; k < off[row + 1]; ++k) {
+    for (int k = off[row] + lane; k < off[row + 1]; k += 32) {  // a row's columns are distinct
       const int c = cols[k] - r0;
       if (c < 0 || c >= 4) continue;
       for (int u = 0; u < 3; ++u)
         for (int v = 0; v < 3; ++v) a[3 * bi + u][3 * c + v] += (double)vals[9LL * k + 3 * u + v];
     }
   }
+  __syncwarp(full);
   bool ok = true;
-  for (int c = 0; c < 12 && ok; ++c) {
-    int piv = c;
-    for (int i = c + 1; i < 12; ++i)
-      if (fabs(a[i][c]) > fabs(a[piv][c])) piv = i;
-    if (!(fabs(a[piv][c]) > 0.0)) {
+  for (int c = 0; c < 12; ++c) {
+    // pivot: the largest |a[i][c]| over i >= c, the smallest such i
+    double v = lane >= c && lane < 12 ? fabs(a[lane][c]) : -1.0;
+    int piv = lane;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(full, v, o);
+      const int op = __shfl_xor_sync(full, piv, o);
+      if (ov > v || (ov == v && op < piv)) {
+        v = ov;
+        piv = op;
+      }
+    }
+    if (!(v > 0.0)) {
       ok = false;
       break;
     }
-    if (piv != c)
-      for (int j = 0; j < 24; ++j) {
-        const double t = a[c][j];
-        a[c][j] = a[piv][j];
-        a[piv][j] = t;
-      }
-    const double inv = 1.0 / a[c][c];
-    for (int j = 0; j < 24; ++j) a[c][j] *= inv;
-    for (int i = 0; i < 12; ++i) {
-      if (i == c) continue;
-      const double f = a[i][c];
-      if (f != 0.0)
-        for (int j = 0; j < 24; ++j) a[i][j] -= f * a[c][j];
+    if (piv != c && lane < 24) {
+      const double t = a[c][lane];
+      a[c][lane] = a[piv][lane];
+      a[piv][lane] = t;
     }
+    __syncwarp(full);
+    const double inv = 1.0 / a[c][c];
+    __syncwarp(full);
+    if (lane < 24) a[c][lane] *= inv;
+    __syncwarp(full);
+    double f[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) f[i] = a[i][c];
+    __syncwarp(full);
+    if (lane < 24) {
+#pragma unroll
+      for (int i = 0; i < 12; ++i)
+        if (i != c && f[i] != 0.0) a[i][lane] -= f[i] * a[c][lane];
+    }
+    __syncwarp(full);
   }
   T* d = out + 144LL * g;
-  if (!ok) atomicOr(status, IPCB_STATUS_PATTERN);
-  for (int i = 0; i < 12; ++i)
-    for (int j = 0; j < 12; ++j) d[12 * i + j] = ok ? (T)a[i][12 + j] : (T)(i == j ? 1.0 : 0.0);
+  if (!ok && lane == 0) atomicOr(status, IPCB_STATUS_PATTERN);
+  for (int e = lane; e < 144; e += 32) {
+    const int i = e / 12, j = e - 12 * i;
+    d[e] = ok ? (T)a[i][12 + j] : (T)(i == j ? 1.0 : 0.0);
+  }
 }
 
 // z = D^-1 r (block Jacobi) ; state.rz_new += r.z
@@ -705,13 +736,15 @@ int ipcb_group_jacobi(int n_point, int n_groups, const int* offsets, const int* 
   if (n_point < 0 || n_groups < 0 || (n_groups && (!offsets || !columns || !values || !dinv_group || !status)))
     return IPCB_E_ARG;
   if (n_groups == 0) return IPCB_OK;
-  const int g = gridn(n_groups, 64);
+  const int g = gridn(n_groups, kInvWarps);
   if (fp64)
-    k_group_inverse<double><<<g, 64, 0, (cudaStream_t)s>>>(n_point, n_groups, offsets, columns,
-                                                           (const double*)values, (double*)dinv_group, status);
+    k_group_inverse<double><<<g, 32 * kInvWarps, 0, (cudaStream_t)s>>>(n_point, n_groups, offsets, columns,
+                                                                       (const double*)values, (double*)dinv_group,
+                                                                       status);
   else
-    k_group_inverse<float><<<g, 64, 0, (cudaStream_t)s>>>(n_point, n_groups, offsets, columns, (const float*)values,
-                                                          (float*)dinv_group, status);
+    k_group_inverse<float><<<g, 32 * kInvWarps, 0, (cudaStream_t)s>>>(n_point, n_groups, offsets, columns,
+                                                                      (const float*)values, (float*)dinv_group,
+                                                                      status);
   return ipcb::check_launch("ipcb_group_jacobi");
 }
 
