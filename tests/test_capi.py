@@ -37,6 +37,13 @@ def test_sizes_and_args_without_gpu():
     assert L.ipcb_sort_pairs_u32(None, None, -1, 8, None, 0, None) == 1
     assert L.ipcb_contact_hessian(5, None, None, 0, 0, 1.0, None, None, None, None, None, None) == 1
     assert L.ipcb_contact_hessian_after(1, None, None, -1, 0, None, 1.0, None, None, None, None, None, None) == 1
+    # line-search accumulator fold and body-block inverses: refused before any launch
+    assert L.ipcb_acc_fold(None, None, 1, None) == 1
+    assert L.ipcb_acc_fold(ctypes.c_void_p(16), None, 2, None) == 1
+    assert L.ipcb_acc_fold(ctypes.c_void_p(16), ctypes.c_void_p(16), -1, None) == 1
+    assert L.ipcb_group_jacobi(-1, 1, None, None, None, 0, None, None, None) == 1
+    assert L.ipcb_group_jacobi(4, 2, None, None, None, 0, None, None, None) == 1
+    assert L.ipcb_group_jacobi(4, 0, None, None, None, 0, None, None, None) == 0  # nothing to do
     # contact BSR: negative counts mean "read on the device" and need the lists' count words
     assert L.ipcb_contact_bsr_workspace(10, 5) > L.ipcb_contact_bsr_workspace(1, 5)
     ee = _native.Contacts(None, None, None, None, None, None, 4)  # capacity 4, no count word
